@@ -1,0 +1,226 @@
+/*
+ * FP64 periodic direct-sum oracles.  TEST INFRASTRUCTURE ONLY.
+ *
+ * Janus pair rule (src/lib.rs:94-121): same signs attract, opposite signs
+ * repel; acceleration of i = s_i * sum_j s_j m_j (x_j - x_i) / |r|^3 with G
+ * folded into m.  The periodic sum is split the way the TreePM force is:
+ *
+ *   long:  a_L(i) = s_i sum_{k != 0} (4 pi / V) exp(-k^2 r_s^2) / k^2
+ *                     * k * Im( exp(-i k.x_i) S(k) ),  S(k) = sum_j s_j m_j exp(i k.x_j)
+ *          (Ewald reciprocal sum; the k-sum stops where exp(-k^2 r_s^2) < tol)
+ *   short: a_S(i) = s_i sum_j sum_images s_j m_j r S(r_p) / r_p^3,
+ *          r_p^2 = r^2 + eps^2,  S(r) = erfc(r/2r_s) + r/(r_s sqrt(pi)) exp(-r^2/4r_s^2)
+ *          (pairs with |r| < r_trunc)
+ *
+ * With eps = 0 and r_trunc beyond the point where S vanishes this is the
+ * Ewald sum of Newtonian forces, independent of r_s.  Pass r_trunc = r_cut
+ * to evaluate the truncated TreePM split model exactly (no grid, no tree).
+ *
+ * Cost: the reciprocal sum is (number of k vectors) x (sources + targets);
+ * exp(i k.x) is built from per-axis powers, so each k costs two complex
+ * multiplies per particle.
+ */
+#include "oracle.h"
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+static inline double short_factor(double r, double r_s)
+{
+    double x = r / (2.0 * r_s);
+    return erfc(x) + (r / (r_s * sqrt(M_PI))) * exp(-x * x);
+}
+
+void orc_ewald_short(const double* pos, const double* mass,
+                     const int8_t* signs, int64_t n, const int64_t* idx,
+                     int64_t nt, double box, double r_s, double eps,
+                     double r_trunc, double* acc)
+{
+    /* cell list over sources with cells >= r_trunc when that gives >= 3 cells
+     * per axis; otherwise loop over all sources and all images in range */
+    int nc = (int)floor(box / r_trunc);
+    double half = box / 2.0;
+    int nimg = (int)ceil(r_trunc / box);  /* image shells needed */
+    if (nc >= 3 && r_trunc <= half) {
+        if (nc > 256) nc = 256;
+        int64_t ncell = (int64_t)nc * nc * nc;
+        int64_t* head = (int64_t*)malloc(sizeof(int64_t) * (size_t)ncell);
+        int64_t* next = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n > 0 ? n : 1));
+        for (int64_t c = 0; c < ncell; c++) head[c] = -1;
+        double cs = box / nc;
+        for (int64_t j = 0; j < n; j++) {
+            int c[3];
+            for (int d = 0; d < 3; d++) {
+                double g = floor((pos[3 * j + d] + half) / cs);
+                int gi = (int)g % nc; if (gi < 0) gi += nc;
+                c[d] = gi;
+            }
+            int64_t cid = c[0] + (int64_t)nc * (c[1] + (int64_t)nc * c[2]);
+            next[j] = head[cid]; head[cid] = j;
+        }
+#pragma omp parallel for schedule(dynamic, 64)
+        for (int64_t q = 0; q < nt; q++) {
+            int64_t i = idx[q];
+            double a[3] = {0, 0, 0};
+            int c[3];
+            for (int d = 0; d < 3; d++) {
+                double g = floor((pos[3 * i + d] + half) / cs);
+                int gi = (int)g % nc; if (gi < 0) gi += nc;
+                c[d] = gi;
+            }
+            for (int oz = -1; oz <= 1; oz++)
+                for (int oy = -1; oy <= 1; oy++)
+                    for (int ox = -1; ox <= 1; ox++) {
+                        int cx = (c[0] + ox + nc) % nc, cy = (c[1] + oy + nc) % nc, cz = (c[2] + oz + nc) % nc;
+                        for (int64_t j = head[cx + (int64_t)nc * (cy + (int64_t)nc * cz)]; j >= 0; j = next[j]) {
+                            if (j == i) continue;
+                            double r[3];
+                            for (int d = 0; d < 3; d++) {
+                                double dd = pos[3 * j + d] - pos[3 * i + d];
+                                dd -= box * floor(dd / box + 0.5);
+                                r[d] = dd;
+                            }
+                            double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+                            if (r2 >= r_trunc * r_trunc) continue;
+                            double rp2 = r2 + eps * eps;
+                            double rp = sqrt(rp2);
+                            double f = (double)signs[j] * mass[j] * short_factor(rp, r_s) / (rp2 * rp);
+                            a[0] += f * r[0]; a[1] += f * r[1]; a[2] += f * r[2];
+                        }
+                    }
+            double s = (double)signs[i];
+            acc[3 * q] = s * a[0]; acc[3 * q + 1] = s * a[1]; acc[3 * q + 2] = s * a[2];
+        }
+        free(head); free(next);
+        return;
+    }
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t q = 0; q < nt; q++) {
+        int64_t i = idx[q];
+        double a[3] = {0, 0, 0};
+        for (int64_t j = 0; j < n; j++) {
+            double r0[3];
+            for (int d = 0; d < 3; d++) {
+                double dd = pos[3 * j + d] - pos[3 * i + d];
+                dd -= box * floor(dd / box + 0.5);
+                r0[d] = dd;
+            }
+            for (int iz = -nimg; iz <= nimg; iz++)
+                for (int iy = -nimg; iy <= nimg; iy++)
+                    for (int ix = -nimg; ix <= nimg; ix++) {
+                        if (j == i && ix == 0 && iy == 0 && iz == 0) continue;
+                        double r[3] = {r0[0] + ix * box, r0[1] + iy * box, r0[2] + iz * box};
+                        double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+                        if (r2 >= r_trunc * r_trunc) continue;
+                        double rp2 = r2 + eps * eps;
+                        double rp = sqrt(rp2);
+                        double f = (double)signs[j] * mass[j] * short_factor(rp, r_s) / (rp2 * rp);
+                        a[0] += f * r[0]; a[1] += f * r[1]; a[2] += f * r[2];
+                    }
+        }
+        double s = (double)signs[i];
+        acc[3 * q] = s * a[0]; acc[3 * q + 1] = s * a[1]; acc[3 * q + 2] = s * a[2];
+    }
+}
+
+void orc_ewald_long(const double* pos, const double* mass, const int8_t* signs,
+                    int64_t n, const int64_t* idx, int64_t nt, double box,
+                    double r_s, double kcut_tol, double* acc)
+{
+    double dk = 2.0 * M_PI / box;
+    double kmax = sqrt(-log(kcut_tol)) / r_s;   /* exp(-k^2 r_s^2) = tol */
+    int nmax = (int)floor(kmax / dk);
+    if (nmax < 1) nmax = 1;
+    int W = nmax + 1;
+    double V = box * box * box;
+    /* list of half-space k vectors with weights 2 * (4 pi / V) e^{-k^2 r_s^2} / k^2 */
+    int64_t cap = (int64_t)(2 * nmax + 1) * (2 * nmax + 1) * (nmax + 1);
+    int* kv = (int*)malloc(sizeof(int) * 3 * (size_t)cap);
+    double* kw = (double*)malloc(sizeof(double) * (size_t)cap);
+    int64_t nk = 0;
+    for (int nx = 0; nx <= nmax; nx++)
+        for (int ny = -nmax; ny <= nmax; ny++)
+            for (int nz = -nmax; nz <= nmax; nz++) {
+                if (nx == 0 && (ny < 0 || (ny == 0 && nz <= 0))) continue;
+                double k2 = dk * dk * (double)(nx * nx + ny * ny + nz * nz);
+                if (k2 > kmax * kmax) continue;
+                kv[3 * nk] = nx; kv[3 * nk + 1] = ny; kv[3 * nk + 2] = nz;
+                kw[nk] = 2.0 * (4.0 * M_PI / V) * exp(-k2 * r_s * r_s) / k2;
+                nk++;
+            }
+    /* per-particle axis powers e^{i n theta_d}, n = 0..nmax */
+    int64_t np = n;
+    double* ex = (double*)malloc(sizeof(double) * 2 * (size_t)W * 3 * (size_t)(np > 0 ? np : 1));
+#pragma omp parallel for schedule(static)
+    for (int64_t j = 0; j < np; j++) {
+        for (int d = 0; d < 3; d++) {
+            double th = dk * pos[3 * j + d];
+            double* e = ex + 2 * (size_t)W * (3 * j + d);
+            for (int m = 0; m <= nmax; m++) { e[2 * m] = cos(m * th); e[2 * m + 1] = sin(m * th); }
+        }
+    }
+    /* structure factors S(k) = sum_j s_j m_j e^{i k.x_j} */
+    double* S = (double*)calloc(2 * (size_t)nk, sizeof(double));
+#pragma omp parallel
+    {
+        double* Sl = (double*)calloc(2 * (size_t)nk, sizeof(double));
+#pragma omp for schedule(static)
+        for (int64_t j = 0; j < np; j++) {
+            const double* e0 = ex + 2 * (size_t)W * (3 * j);
+            const double* e1 = e0 + 2 * W;
+            const double* e2 = e1 + 2 * W;
+            double q = (double)signs[j] * mass[j];
+            for (int64_t k = 0; k < nk; k++) {
+                int a = kv[3 * k], b = kv[3 * k + 1], c = kv[3 * k + 2];
+                double xr = e0[2 * a], xi = e0[2 * a + 1];
+                double yr = e1[2 * (b < 0 ? -b : b)], yi = e1[2 * (b < 0 ? -b : b) + 1];
+                if (b < 0) yi = -yi;
+                double zr = e2[2 * (c < 0 ? -c : c)], zi = e2[2 * (c < 0 ? -c : c) + 1];
+                if (c < 0) zi = -zi;
+                double pr = xr * yr - xi * yi, pi = xr * yi + xi * yr;
+                double er = pr * zr - pi * zi, ei = pr * zi + pi * zr;
+                Sl[2 * k] += q * er; Sl[2 * k + 1] += q * ei;
+            }
+        }
+#pragma omp critical
+        for (int64_t k = 0; k < 2 * nk; k++) S[k] += Sl[k];
+        free(Sl);
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t t = 0; t < nt; t++) {
+        int64_t i = idx[t];
+        const double* e0 = ex + 2 * (size_t)W * (3 * i);
+        const double* e1 = e0 + 2 * W;
+        const double* e2 = e1 + 2 * W;
+        double a0 = 0, a1 = 0, a2 = 0;
+        for (int64_t k = 0; k < nk; k++) {
+            int a = kv[3 * k], b = kv[3 * k + 1], c = kv[3 * k + 2];
+            double xr = e0[2 * a], xi = e0[2 * a + 1];
+            double yr = e1[2 * (b < 0 ? -b : b)], yi = e1[2 * (b < 0 ? -b : b) + 1];
+            if (b < 0) yi = -yi;
+            double zr = e2[2 * (c < 0 ? -c : c)], zi = e2[2 * (c < 0 ? -c : c) + 1];
+            if (c < 0) zi = -zi;
+            double pr = xr * yr - xi * yi, pi = xr * yi + xi * yr;
+            double er = pr * zr - pi * zi, ei = pr * zi + pi * zr;
+            /* Im(conj(E_i) S) */
+            double im = er * S[2 * k + 1] - ei * S[2 * k];
+            double f = kw[k] * im;
+            a0 += f * (dk * a); a1 += f * (dk * b); a2 += f * (dk * c);
+        }
+        double s = (double)signs[i];
+        acc[3 * t] = s * a0; acc[3 * t + 1] = s * a1; acc[3 * t + 2] = s * a2;
+    }
+    free(kv); free(kw); free(ex); free(S);
+}
+
+void orc_ewald_forces(const double* pos, const double* mass,
+                      const int8_t* signs, int64_t n, const int64_t* idx,
+                      int64_t nt, double box, double r_s, double eps,
+                      double r_trunc, double kcut_tol, double* acc)
+{
+    double* al = (double*)malloc(sizeof(double) * 3 * (size_t)(nt > 0 ? nt : 1));
+    orc_ewald_long(pos, mass, signs, n, idx, nt, box, r_s, kcut_tol, al);
+    orc_ewald_short(pos, mass, signs, n, idx, nt, box, r_s, eps, r_trunc, acc);
+    for (int64_t i = 0; i < 3 * nt; i++) acc[i] += al[i];
+    free(al);
+}

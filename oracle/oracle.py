@@ -1,0 +1,217 @@
+"""ctypes bindings for the CPU oracle (test infrastructure only).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline legs import
+this module.  It loads oracle/liboracle.so (C restatements of the reference
+path plus the FP64 Ewald oracles) and, when present, oracle/_ref/
+libref_twopass.so (the reference's own CUDA kernel source compiled for the
+host CPU).  Both are built by `make -C oracle` / `make -C oracle ref`.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_lib = None
+_ref = None
+
+f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+i8p = np.ctypeslib.ndpointer(np.int8, flags="C_CONTIGUOUS")
+i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
+u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+I64, I32, F32, F64 = C.c_int64, C.c_int, C.c_float, C.c_double
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            raise RuntimeError("oracle not built: run `make -C oracle`")
+        L = C.CDLL(path)
+        sig = {
+            "orc_morton30": [f32p, I64, F32, u32p],
+            "orc_sort_keys": [u32p, I64, i32p],
+            "orc_karras": [u32p, i32p, I64, i32p, i32p, i32p, i32p, i32p],
+            "orc_leaves_reduce": [f32p, I64, F32, F32, i32p, i32p, i32p, f32p, f32p, i32p],
+            "orc_ref_cic_scatter": [f32p, i8p, I64, I32, F32, F32, f64p, f64p],
+            "orc_ref_poisson": [f64p, f64p, I32, F64, F64, F64, I32],
+            "orc_ref_cic_gather": [f32p, i8p, I64, I32, F32, F32, F32, f64p, f64p, f32p],
+            "orc_ref_pm_forces": [f32p, i8p, I64, I32, F64, F64, F64, I32, f32p],
+            "orc_ref_quantize": [F64, F64, F64, F64, C.POINTER(F32), C.POINTER(F32),
+                                 C.POINTER(F32), C.POINTER(F32)],
+            "orc_ref_short_range": [f32p, i8p, I64, I32, f32p, f32p, i32p, i32p, i32p,
+                                    F32, F32, F32, F32, I32, f32p],
+            "orc_ref_total_forces": [f32p, i8p, I64, I32, F64, F64, F64, F64, F64, I32, f32p],
+            "orc_cpu_treepm_forces": [f64p, f64p, i8p, I64, F64, I32, F64, F64, F64, f64p],
+            "orc_cpu_treepm_last_times": [C.POINTER(F64), C.POINTER(F64)],
+            "orc_ewald_forces": [f64p, f64p, i8p, I64, i64p, I64, F64, F64, F64, F64, F64, f64p],
+            "orc_ewald_long": [f64p, f64p, i8p, I64, i64p, I64, F64, F64, F64, f64p],
+            "orc_ewald_short": [f64p, f64p, i8p, I64, i64p, I64, F64, F64, F64, F64, f64p],
+            "orc_acc_pm_forces": [f64p, f64p, i8p, I64, I32, F64, F64, I32, f64p],
+            "orc_acc_pm_grids": [f64p, f64p, i8p, I64, I32, F64, F64, I32, f64p, f64p, f64p],
+            "orc_fft3d": [f64p, I32, I32],
+        }
+        for name, args in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = None
+        L.orc_expand10.argtypes = [C.c_uint32]
+        L.orc_expand10.restype = C.c_uint32
+        _lib = L
+    return _lib
+
+
+def ref_available():
+    return os.path.exists(os.path.join(HERE, "_ref", "libref_twopass.so"))
+
+
+def ref():
+    """The reference kernels compiled for the host (oracle/_ref)."""
+    global _ref
+    if _ref is None:
+        path = os.path.join(HERE, "_ref", "libref_twopass.so")
+        if not os.path.exists(path):
+            raise RuntimeError("reference harness not built: run `make -C oracle ref`")
+        R = C.CDLL(path)
+        sig = {
+            "ref_morton": [f32p, I32, F32, u64p, i32p],
+            "ref_radix_sort": [u64p, i32p, I32],
+            "ref_karras": [u64p, I32, i32p, i32p, i32p, i32p, i32p],
+            "ref_leaves_reduce": [f32p, I32, F32, F32, i32p, i32p, i32p, i32p, i32p,
+                                  f32p, f32p, i32p],
+            "ref_cic_scatter": [f32p, i8p, f64p, f64p, I32, I32, F32, F32],
+            "ref_cic_gather": [f32p, i8p, f64p, f64p, f32p, I32, I32, F32, F32, F32],
+            "ref_apply_green": [f64p, I32, I32, I32, F64, F64, F64, I32],
+            "ref_normalize": [f64p, I32, F64],
+            "ref_pack_params": [F64, F64, F64, F64, C.POINTER(F32), C.POINTER(F32)],
+            "ref_short_range": [f32p, i8p, f32p, f32p, i32p, i32p, i32p, f32p, I32, F32, F32],
+            "ref_drift": [f32p, f32p, F32, F32, I32],
+            "ref_kick": [f32p, f32p, F32, I32, F32, F32],
+        }
+        for name, args in sig.items():
+            fn = getattr(R, name)
+            fn.argtypes = args
+            fn.restype = None
+        _ref = R
+    return _ref
+
+
+# ---------------------------------------------------------------- helpers
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+def morton30(pos, box_half):
+    pos = _c(pos, np.float32).reshape(-1, 3)
+    out = np.empty(len(pos), np.uint32)
+    lib().orc_morton30(pos.ravel(), len(pos), np.float32(box_half), out)
+    return out
+
+
+def build_tree(pos, box_half, mass):
+    """Reference LBVH over one species (positions in the species' own order).
+
+    Returns a dict with m30 (sorted), perm, pos_sorted, left, right, parent,
+    rl, rr, node_pos (2n-1, 7), node_mass, types."""
+    pos = _c(pos, np.float32).reshape(-1, 3)
+    n = len(pos)
+    nn = max(2 * n - 1, 1)
+    L = lib()
+    m30 = morton30(pos, box_half)
+    perm = np.empty(n, np.int32)
+    L.orc_sort_keys(m30, n, perm)
+    m30s = np.ascontiguousarray(m30[perm])
+    pos_s = np.ascontiguousarray(pos[perm])
+    left = np.zeros(nn, np.int32)
+    right = np.zeros(nn, np.int32)
+    parent = np.zeros(nn, np.int32)
+    rl = np.zeros(max(n - 1, 1), np.int32)
+    rr = np.zeros(max(n - 1, 1), np.int32)
+    L.orc_karras(m30s, perm, n, left, right, parent, rl, rr)
+    node_pos = np.zeros(7 * nn, np.float32)
+    node_mass = np.zeros(nn, np.float32)
+    types = np.zeros(nn, np.int32)
+    L.orc_leaves_reduce(pos_s.ravel(), n, np.float32(box_half), np.float32(mass),
+                        left, right, parent, node_pos, node_mass, types)
+    return dict(m30=m30s, perm=perm, pos_sorted=pos_s, left=left, right=right,
+                parent=parent, rl=rl[:max(n - 1, 0)], rr=rr[:max(n - 1, 0)],
+                node_pos=node_pos.reshape(nn, 7), node_mass=node_mass, types=types)
+
+
+def ref_quantize(theta, softening, r_cut, box):
+    a, b, c, d = F32(), F32(), F32(), F32()
+    lib().orc_ref_quantize(theta, softening, r_cut, box, C.byref(a), C.byref(b),
+                           C.byref(c), C.byref(d))
+    return a.value, b.value, c.value, d.value
+
+
+def ref_total_forces(pos_all, signs_all, M, box, theta, softening, r_cut,
+                     mass_factor, k_min=0):
+    """Reference GPU TreePM acceleration (PM + both trees), FP32 out."""
+    pos_all = _c(pos_all, np.float32).reshape(-1, 3)
+    signs_all = _c(signs_all, np.int8)
+    acc = np.zeros((len(pos_all), 3), np.float32)
+    lib().orc_ref_total_forces(pos_all.ravel(), signs_all, len(pos_all), M, box,
+                               theta, softening, r_cut, mass_factor, k_min, acc.ravel())
+    return acc
+
+
+def ref_pm_forces(pos_all, signs_all, M, box, mass_factor, r_cut, k_min=0):
+    pos_all = _c(pos_all, np.float32).reshape(-1, 3)
+    signs_all = _c(signs_all, np.int8)
+    out = np.zeros((len(pos_all), 3), np.float32)
+    lib().orc_ref_pm_forces(pos_all.ravel(), signs_all, len(pos_all), M, box,
+                            mass_factor, r_cut, k_min, out.ravel())
+    return out
+
+
+def cpu_treepm_forces(pos, mass, signs, r_cut, grid, box, theta, softening):
+    """Reference CPU TreePM (src/treepm) on all particles; returns (acc, t_update, t_forces)."""
+    pos = _c(pos, np.float64).reshape(-1, 3)
+    mass = _c(mass, np.float64)
+    signs = _c(signs, np.int8)
+    acc = np.zeros((len(pos), 3), np.float64)
+    L = lib()
+    L.orc_cpu_treepm_forces(pos.ravel(), mass, signs, len(pos), r_cut, grid, box,
+                            theta, softening, acc.ravel())
+    tu, tf = F64(), F64()
+    L.orc_cpu_treepm_last_times(C.byref(tu), C.byref(tf))
+    return acc, tu.value, tf.value
+
+
+def ewald_forces(pos, mass, signs, box, r_s, eps, r_trunc=None, idx=None,
+                 kcut_tol=1e-12, part="all"):
+    """FP64 periodic oracle on targets idx (default all).  part: all|long|short."""
+    pos = _c(pos, np.float64).reshape(-1, 3)
+    mass = _c(mass, np.float64)
+    signs = _c(signs, np.int8)
+    n = len(pos)
+    idx = np.arange(n, dtype=np.int64) if idx is None else _c(idx, np.int64)
+    if r_trunc is None:
+        r_trunc = 12.0 * r_s   # S(r) < 1e-14 beyond
+    acc = np.zeros((len(idx), 3), np.float64)
+    L = lib()
+    if part == "all":
+        L.orc_ewald_forces(pos.ravel(), mass, signs, n, idx, len(idx), box, r_s, eps,
+                           r_trunc, kcut_tol, acc.ravel())
+    elif part == "long":
+        L.orc_ewald_long(pos.ravel(), mass, signs, n, idx, len(idx), box, r_s, kcut_tol,
+                         acc.ravel())
+    else:
+        L.orc_ewald_short(pos.ravel(), mass, signs, n, idx, len(idx), box, r_s, eps,
+                          r_trunc, acc.ravel())
+    return acc
+
+
+def acc_pm_forces(pos, mass, signs, M, box, r_s, k_min=0):
+    pos = _c(pos, np.float64).reshape(-1, 3)
+    mass = _c(mass, np.float64)
+    signs = _c(signs, np.int8)
+    acc = np.zeros((len(pos), 3), np.float64)
+    lib().orc_acc_pm_forces(pos.ravel(), mass, signs, len(pos), M, box, r_s, k_min,
+                            acc.ravel())
+    return acc
