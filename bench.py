@@ -1,0 +1,328 @@
+#!/usr/bin/env python
+"""TreePM particle-steps/s of the bimetric (m+ / m-) step on a B200.
+
+Workload (one "step" = one full KDK TreePM step of every particle):
+  2 x 224^3 = 22,478,848 particles (11,239,424 m+, 11,239,424 m-) on a 224^3
+  lattice per species (the m- lattice offset by half a cell) with seeded
+  Zel'dovich displacements (P(k) ~ k^-2.5 exp(-(k/k_c)^2), k_c = half the
+  lattice Nyquist, rms 0.3 spacing, delta- = -delta+), L = 250 Mpc, PM grid
+  512^3, mu = M-/M+ = 19, theta = 0.5, r_s = 1.25 cells, r_cut = 4.5 r_s,
+  Plummer softening = mean spacing / 30, dt = 0.005 Gyr, Hubble drag from the
+  FP64 Janus expansion at z = 4.  Synthetic data; positions (360 MB per copy)
+  are larger than L2, so no flush is needed between steps.
+
+`python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]`
+prints ONE JSON line on rank 0.  N > 1 (torchrun): every rank advances its own
+independent box (different seed): replicas, weak scaling, no collective on the
+data path; time = max over ranks.
+
+--impl reference times the reference's CPU TreePM path (src/treepm/*.rs,
+restated in C under oracle/ because the Rust crate cannot be built here) on
+the host cores, each step a bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "janus-sim_b200"))
+
+METRIC = "TreePM particle-steps/s at 2x224^3"
+UNIT = "particle-steps/s"
+
+# flops per evaluated interaction of the walk (counted in k_walk_acc: pair
+# kernel incl. S(x) by A&S 7.1.26, one exp, one rcp and one rsqrt each
+# counted as one flop); quadrupole nodes cost more but are a minority
+FLOPS_PER_INTERACTION = 40.0
+
+
+def workload(n_side=224, L=250.0, M=512):
+    n_tot = 2 * n_side ** 3
+    r_s = 1.25 * L / M
+    return dict(n_side=n_side, L=L, M=M, mu=19.0, theta=0.5, r_s=r_s, r_cut=4.5 * r_s,
+                eps=(L / n_tot ** (1.0 / 3.0)) / 30.0, dt=0.005, z=4.0, n_total=n_tot)
+
+
+def hubble_at(z):
+    from janus_treepm import expansion
+    return expansion.state_at_redshift(z)[2]
+
+
+def dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_treepm_step(sample_div=4, seed=42, threads=None):
+    """One reference-CPU TreePM step (update + compute_all_forces + kick/drift)
+    on a bounded sample of the workload: the same density, r_s, r_cut,
+    softening and theta in a box of side L/sample_div (N/sample_div^3
+    particles, PM grid M/sample_div).  Returns (particles, seconds, cores)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from janus_treepm import ics
+    w = workload()
+    n_side = w["n_side"] // sample_div
+    L = w["L"] / sample_div
+    M = w["M"] // sample_div
+    pp, vp, pm, vm = ics.zeldovich_lattice(n_side, L, seed=seed)
+    pos = np.concatenate([pp, pm]).astype(np.float64)
+    vel = np.concatenate([vp, vm]).astype(np.float64)
+    n = len(pp)
+    mass = np.concatenate([np.full(n, 1.0), np.full(n, w["mu"])]) * 1e-3
+    sg = np.concatenate([np.ones(n, np.int8), -np.ones(n, np.int8)])
+    t0 = time.perf_counter()
+    acc, tu, tf = O.cpu_treepm_forces(pos, mass, sg, w["r_cut"], M, L, w["theta"], w["eps"])
+    vel += acc * w["dt"]
+    pos += vel * w["dt"]
+    dt = time.perf_counter() - t0
+    return len(pos), dt, (threads or os.cpu_count())
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return 0
+    w = workload()
+    div = args.cpu_sample_div
+    for _ in range(args.warmup if args.warmup < 1 else 1):
+        cpu_treepm_step(div)
+    tot_n, tot_t, cores = 0, 0.0, os.cpu_count()
+    for k in range(args.steps):
+        n, t, cores = cpu_treepm_step(div, seed=42 + k)
+        tot_n += n
+        tot_t += t
+    v = tot_n / tot_t
+    sample = (f"2x{w['n_side'] // div}^3 particles, L={w['L'] / div:g} Mpc, PM "
+              f"{w['M'] // div}^3 (the workload's density, r_s, r_cut, eps, theta in a box "
+              f"1/{div} the side); one full step per sample")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * w["n_total"] / v,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Zel'dovich lattice)",
+        "config": {"workload": "TreePM step 2x224^3, L=250 Mpc, PM 512^3, mu=19, theta=0.5",
+                   "reference_path": "src/treepm (TreePMForce update + compute_all_forces), "
+                                     "C restatement with OpenMP"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    import janus_treepm as J
+    from janus_treepm import ics
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist_
+        dist_.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    w = workload(args.n_side, 250.0 * args.n_side / 224.0, args.grid)
+    H = hubble_at(w["z"])
+    seed = 42 + rank
+    pp, vp, pm, vm = ics.zeldovich_lattice(w["n_side"], w["L"], seed=seed)
+    n = len(pp)
+    cfg = J.Config(box_L=w["L"], pm_grid=w["M"], theta=w["theta"], softening=w["eps"],
+                   r_s=w["r_s"], r_cut=w["r_cut"], mu=w["mu"], G_mass_plus=1.0e-3,
+                   mode=J.JT_ACCURATE, integrator=J.JT_KDK)
+    s = J.Solver(cfg)
+    s.set_state(pp, vp, pm, vm)
+    peak_fp32 = J.fp32_peak_tflops()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if ws > 1:
+            torch.distributed.barrier()
+
+    for _ in range(args.warmup):
+        s.step(w["dt"], H, 1.0, 1)
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    t_wall = time.perf_counter()
+    dev_ms = 0.0
+    stages = {}
+    for _ in range(args.steps):
+        s.step(w["dt"], H, 1.0, 1)
+        tm = s.timings()
+        dev_ms += tm["total_ms"]
+        for k, v in tm.items():
+            stages[k] = stages.get(k, 0.0) + v
+    barrier()
+    wall = time.perf_counter() - t_wall
+    clk = clocks.stop()
+    if ws > 1:
+        t = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        dev_ms = float(t.item())
+    K = args.steps
+    value = ws * 2 * n * K / (dev_ms * 1e-3)
+
+    # end to end through the C ABI with pinned host buffers: upload the state,
+    # one step, read the state back, every step
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    hp, hvp, hm, hvm = pin(pp), pin(vp), pin(pm), pin(vm)
+    op = [pin(np.zeros_like(pp)) for _ in range(4)]
+    s.set_state(hp, hvp, hm, hvm)
+    s.step(w["dt"], H, 1.0, 1)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(K):
+        s.set_state(hp, hvp, hm, hvm)
+        s.step(w["dt"], H, 1.0, 1)
+        a, b, c, d = s.get_state()
+    barrier()
+    e2e_t = time.perf_counter() - t0
+    if ws > 1:
+        t = torch.tensor([e2e_t], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_t = float(t.item())
+    e2e = ws * 2 * n * K / e2e_t
+    bytes_state = 2 * n * 3 * 4 * 2     # positions + velocities, both species
+
+    # roofline of the dominant kernel: the walk (FP32 pipe)
+    walk_ms = stages["walk_ms"] / K
+    inter = stages["interactions"] / K
+    achieved = inter * FLOPS_PER_INTERACTION / (walk_ms * 1e-3) / 1e12
+    Gc = w["M"] * w["M"] * (w["M"] // 2 + 1)
+    ks_ms = stages["kspace_ms"] / K
+    ks_gbs = 32.0 * Gc / (ks_ms * 1e-3) / 1e9
+    hbm_peak = 6550.7
+    try:
+        hbm_peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+        hbm_src = "measured"
+    except Exception:
+        hbm_src = "fallback"
+    walk_traffic = None
+    try:
+        prof = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        walk_traffic = prof.get("walk_bytes_per_particle", None)
+        if walk_traffic is not None:
+            walk_traffic = walk_traffic * 2 * n
+    except Exception:
+        pass
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        npart, tcpu, cores = cpu_treepm_step(args.cpu_sample_div)
+        cpu = {"value": npart / tcpu, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"one reference-CPU TreePM step (oracle/ref_cpu_treepm.c) on "
+                         f"2x{w['n_side'] // args.cpu_sample_div}^3 particles in a box "
+                         f"1/{args.cpu_sample_div} the side (same density, r_s, r_cut, "
+                         f"eps, theta), {tcpu:.1f} s"}
+    launches = stages.get("launches", 0)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K,
+            "warmup": args.warmup, "ms_per_step": dev_ms / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded Zel'dovich lattice)",
+            "config": {"workload": f"TreePM KDK step 2x{w['n_side']}^3, L={w['L']:g} Mpc, "
+                                   f"PM {w['M']}^3, mu=19, theta=0.5, r_s=1.25 cells, "
+                                   f"r_cut=4.5 r_s, accurate mode",
+                       "l2": "inputs larger than L2 (no flush)",
+                       "parallelism": "replicas" if ws > 1 else "single"},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": bytes_state * ws,
+                    "d2h_bytes_per_step": bytes_state * ws},
+            "roofline": {"bound": "fp32", "kernel": "k_walk_acc", "achieved": achieved,
+                         "peak": peak_fp32, "unit": "TFLOP/s", "frac": achieved / peak_fp32,
+                         "traffic": walk_traffic,
+                         "peak_source": "measured (jt_fp32_peak FMA kernel, same run)",
+                         "work": f"{inter:.4g} interactions x {FLOPS_PER_INTERACTION:g} flop"},
+            "roofline_hbm": {"bound": "hbm", "kernel": "k_kspace_acc", "achieved": ks_gbs,
+                             "peak": hbm_peak, "unit": "GB/s", "frac": ks_gbs / hbm_peak,
+                             "peak_source": hbm_src},
+            "stages_ms_per_step": {k: round(v / K, 4) for k, v in stages.items()
+                                   if k.endswith("_ms")},
+            "wall_ms_per_step": 1e3 * wall / K,
+            "clocks": clk,
+            "gpu_launches": int(launches),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n-side", type=int, default=224)
+    ap.add_argument("--grid", type=int, default=512)
+    ap.add_argument("--cpu-sample-div", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    ws, rank, local = dist()
+    if args.impl == "reference":
+        return run_reference(args, ws, rank)
+    return run_ours(args, ws, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

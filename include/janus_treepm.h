@@ -1,0 +1,163 @@
+/*
+ * janus_treepm.h -- C ABI of the B200 bimetric TreePM force-and-step engine.
+ *
+ * Two species of opposite gravitational mass (m+ and m-) in a periodic cube
+ * [-L/2, L/2)^3.  Same signs attract, opposite signs repel (janus-sim
+ * src/lib.rs:94-121).  Per-species particle arrays in, per-species
+ * accelerations out.  Arrays are AoS float3 (x,y,z per particle), the layout
+ * of the reference's Vec<f32> position/velocity buffers
+ * (src/nbody_gpu_twopass.rs:2159-2176).
+ *
+ * Conventions (the reference's FFI returns 0 or -1 after printing to stderr,
+ * cuda/cufft_wrapper.cu:13-27; here every entry point returns 0 or one of the
+ * negative JT_E* codes below and prints nothing):
+ *   - the caller owns every array it passes; `mem` says whether the pointers
+ *     are host (JT_MEM_HOST) or device (JT_MEM_DEVICE, current device) memory;
+ *   - a handle owns all its device state, cuFFT plans and a private stream;
+ *     handles are independent (no process-global state), one host thread per
+ *     handle at a time;
+ *   - every call returns after its GPU work has finished.
+ */
+#ifndef JANUS_TREEPM_H
+#define JANUS_TREEPM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- return codes ---- */
+#define JT_OK          0
+#define JT_EINVAL     -1   /* bad argument (the reference's only error value) */
+#define JT_ENOMEM     -2   /* device or host allocation failed */
+#define JT_ECUDA      -3   /* a CUDA or cuFFT call failed */
+#define JT_ETIMEDOUT  -4   /* a bounded device-side wait gave up */
+#define JT_ENOTIMPL   -5   /* feature not available in this build */
+#define JT_ESTATE     -6   /* call out of order (e.g. no particles set) */
+#define JT_EOVERFLOW  -7   /* a fixed-capacity device list overflowed */
+#define JT_EBUSY      -8   /* admission refused (batch / serve) */
+
+/* ---- memory kinds ---- */
+#define JT_MEM_HOST    0
+#define JT_MEM_DEVICE  1
+
+/* ---- force modes ---- */
+/* ACCURATE: signed-source PM with CIC deconvolution and spectral gradient,
+ * short-range factor erfc(x) + 2x/sqrt(pi) exp(-x^2), x = r / (2 r_s), Plummer
+ * softening, monopole + quadrupole nodes, hard cut at r_cut. */
+#define JT_ACCURATE    0
+/* RCOMPAT: the reference GPU formulas (src/nbody_gpu_twopass.rs:98-257,
+ * 1670-1811; cuda/cufft_wrapper.cu:148-208): finite-difference gradient of the
+ * undeconvolved potential, erfc-only short-range factor with r_s = r_cut/3,
+ * 16-bit quantised theta/softening and integer r_cut/box_half, warp-uniform
+ * opening decisions over groups of 32 particles of the concatenated
+ * [m+ ; m-] arrays, monopole nodes with the reference's cube geometry. */
+#define JT_RCOMPAT     1
+
+/* ---- integrators ---- */
+#define JT_KDK         0   /* kick(dt/2) drift(dt) force kick(dt/2) */
+#define JT_DKD_REF     1   /* drift(dt/2) force kick(dt) drift(dt/2), the
+                              reference's step_treepm_gpu order (:4518-4637) */
+
+/* Configuration.  Mirrors the reference's TreePM fields
+ * (TreePMForce{r_cut, r_s, softening, g_constant}, src/treepm/treepm_force.rs:
+ * 17-25; GpuNBodyTwoPass{theta, softening, box_size, pm_grid_size, pm_k_min,
+ * mass_factor}, src/nbody_gpu_twopass.rs:1874-1893). */
+typedef struct jt_config {
+    double box_L;        /* box side (Mpc); positions in [-L/2, L/2) */
+    int    pm_grid;      /* PM cells per side M, power of two, 8..1024 */
+    double theta;        /* Barnes-Hut opening angle */
+    double softening;    /* Plummer softening eps */
+    double r_s;          /* long/short split scale (ACCURATE; RCOMPAT uses r_cut/3) */
+    double r_cut;        /* short-range cutoff */
+    double mu;           /* total-mass ratio M- / M+ */
+    double G_mass_plus;  /* G * (mass of one m+ particle); m- = mu*m+*N+/N- */
+    int    k_min;        /* zero modes with max(|kx|,|ky|,|kz|) < k_min; 0 = off */
+    int    mode;         /* JT_ACCURATE | JT_RCOMPAT */
+    int    integrator;   /* JT_KDK | JT_DKD_REF */
+    int    reserved[5];  /* zero */
+} jt_config;
+
+typedef struct jt_handle jt_handle;
+
+/* Stage timings of the last jt_accel / jt_step call, milliseconds of device
+ * time (CUDA events on the handle's stream), summed over the call. */
+typedef struct jt_timings {
+    double sort_ms;      /* Morton keys + radix sort + reorder */
+    double tree_ms;      /* Karras nodes + bottom-up moments */
+    double deposit_ms;   /* CIC deposit of the signed source */
+    double fft_ms;       /* R2C + k-space kernel + C2R */
+    double kspace_ms;    /* the fused k-space kernel alone (part of fft_ms) */
+    double walk_ms;      /* PM interpolation + short-range walk (+ kick) */
+    double kick_drift_ms;/* kick/drift kernels outside the walk */
+    double total_ms;     /* whole call */
+    int64_t interactions;/* pair + node interactions counted by the walk */
+    int64_t launches;    /* kernels launched by the library (incl. cuFFT's) */
+} jt_timings;
+
+/* Create a handle on the current CUDA device.  Replaces the constructor and
+ * setters of GpuNBodyTwoPass (src/nbody_gpu_twopass.rs:2159-2336) and
+ * TreePMForce::new (src/treepm/treepm_force.rs:35-49). */
+int  jt_create(const jt_config* cfg, jt_handle** out);
+
+/* Load both species.  Replaces GpuNBodyTwoPass::with_custom_ics (:2159-2303)
+ * with per-species arrays (the reference takes one array plus i8 signs; the
+ * m+ array here is its sign>0 subset in order, the m- array its sign<0 subset).
+ * vel_* may be NULL (zero velocities).  n_p or n_m may be 0. */
+int  jt_set_state(jt_handle* h,
+                  const float* pos_p, const float* vel_p, size_t n_p,
+                  const float* pos_m, const float* vel_m, size_t n_m,
+                  int mem);
+
+/* The reference's layout: one array and i8 signs (+1 / -1), exactly the
+ * arguments of with_custom_ics.  RCOMPAT groups warps in this array order. */
+int  jt_set_state_signed(jt_handle* h, const float* pos, const float* vel,
+                         const int8_t* signs, size_t n, int mem);
+
+/* Accelerations at the current positions (force only; the parity entry
+ * point).  Replaces compute_short_range_forces + the PM half of
+ * step_treepm_gpu (:3961-4138, :4530-4600) and TreePMForce::
+ * compute_all_forces (src/treepm/treepm_force.rs:124-131).  Outputs in the
+ * caller's order; either pointer may be NULL. */
+int  jt_accel(jt_handle* h, float* acc_p, float* acc_m, int mem);
+/* Same, for a state loaded with jt_set_state_signed: acc in that order. */
+int  jt_accel_signed(jt_handle* h, float* acc, int mem);
+
+/* Advance nsteps steps of length dt.  Kick: v += (a - H v dtau_per_dt) dt,
+ * the reference's kick_f32 (:50-64) with hubble = H; drift x += v dt with
+ * one periodic wrap (:33-48).  Replaces step_treepm_gpu(dt, r_cut, hubble,
+ * dtau_per_dt) (:4486-4649); r_cut comes from the config. */
+int  jt_step(jt_handle* h, double dt, double hubble, double dtau_per_dt, int nsteps);
+
+/* Read the state back in the caller's order (get_particles, :5470).  Any
+ * pointer may be NULL. */
+int  jt_get_state(jt_handle* h, float* pos_p, float* vel_p, float* pos_m,
+                  float* vel_m, int mem);
+int  jt_get_state_signed(jt_handle* h, float* pos, float* vel, int mem);
+
+/* Topology of one species' tree built at the current positions with the
+ * reference's keys ((morton30 << 32) | index in the species array), in the
+ * reference's numbering (internal 0..n-2, leaves n-1..2n-2;
+ * build_bvh_tp :407-447): morton[n] (sorted 30-bit codes), perm[n] (species
+ * index of each sorted position), left/right/parent[2n-1] (leaf entries of
+ * left/right are 0; parent[0] = -1).  species: 0 = m+, 1 = m-.  Host memory. */
+int  jt_debug_tree(jt_handle* h, int species, uint32_t* morton, int32_t* perm,
+                   int32_t* left, int32_t* right, int32_t* parent);
+
+int  jt_get_timings(jt_handle* h, jt_timings* t);
+int  jt_counts(jt_handle* h, size_t* n_p, size_t* n_m);
+void jt_destroy(jt_handle* h);
+const char* jt_strerror(int code);
+/* FP32 FMA throughput of the current device (TFLOP/s), measured by a
+ * register-only FMA kernel: the roofline denominator for the walk.  No
+ * counterpart in the reference. */
+int  jt_fp32_peak(int iters, double* tflops);
+/* Library version string, e.g. "janus-treepm-b200 0.1 sm_100a". */
+const char* jt_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

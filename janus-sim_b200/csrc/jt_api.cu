@@ -1,0 +1,795 @@
+// C ABI of the engine: handle, state, force and step pipelines.
+//
+// One handle = one simulation box on the current device with its own stream,
+// cuFFT plans and buffers (the reference keeps process-global cuFFT plans and
+// k-space buffers, cuda/cufft_wrapper.cu:30-32, 319-320, and synchronises the
+// device after every launch; here nothing is global and a call synchronises
+// its own stream once, at the end).
+//
+// Force pipeline (jt_accel, and every step):
+//   per species: Morton keys -> onesweep sort -> reorder state -> Karras nodes
+//   -> bottom-up moments;  memset rho -> signed CIC deposit -> R2C -> fused
+//   k-space kernel -> batched C2R;  walk (PM interpolation + both trees, +
+//   kick in the accurate step).
+#include "jt_internal.cuh"
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <algorithm>
+#include <new>
+#include <vector>
+
+struct jt_handle {
+    jt_config cfg;
+    int device = 0;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev[10] = {};
+    int64_t n[2] = {0, 0};
+    float mass[2] = {0.f, 0.f};
+    bool have_state = false;
+    bool signed_layout = false;
+    bool acc_valid = false;
+    int64_t cap[2] = {0, 0};
+    float4 *pos[2] = {}, *vel[2] = {}, *acc[2] = {}, *pos_b[2] = {}, *vel_b[2] = {};
+    int *id[2] = {}, *id_b[2] = {}, *gmap[2] = {};
+    jt_tree_dev tree[2] = {};
+    jt_sort_ws ws = {};
+    uint64_t* key64 = nullptr;
+    jt_pm_dev pm = {};
+    float4* pos_caller = nullptr;
+    float4* acc_caller = nullptr;
+    int8_t* sign_caller = nullptr;
+    int* rank_buf = nullptr;
+    void* stage = nullptr;
+    size_t stage_bytes = 0;
+    unsigned* d_err = nullptr;
+    unsigned long long* d_inter = nullptr;
+    jt_timings tm = {};
+    int64_t launches_per_force = 0;
+};
+
+namespace {
+
+bool cuda_ok(cudaError_t e) { return e == cudaSuccess; }
+
+#define JT_TRY(x)                      \
+    do {                               \
+        int _r = (x);                  \
+        if (_r != JT_OK) return _r;    \
+    } while (0)
+#define JT_CU(x)                                   \
+    do {                                           \
+        if ((x) != cudaSuccess) return JT_ECUDA;   \
+    } while (0)
+#define JT_FFT(x)                                   \
+    do {                                            \
+        if ((x) != CUFFT_SUCCESS) return JT_ECUDA;  \
+    } while (0)
+
+template <class T>
+int dalloc(T** p, size_t count)
+{
+    *p = nullptr;
+    if (count == 0) count = 1;
+    return cuda_ok(cudaMalloc((void**)p, sizeof(T) * count)) ? JT_OK : JT_ENOMEM;
+}
+
+template <class T>
+void dfree(T*& p)
+{
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+}
+
+bool is_pow2(int m) { return m > 0 && (m & (m - 1)) == 0; }
+
+int validate(const jt_config* c)
+{
+    if (!c) return JT_EINVAL;
+    if (!(c->box_L > 0.0) || !std::isfinite(c->box_L)) return JT_EINVAL;
+    if (!is_pow2(c->pm_grid) || c->pm_grid < 8 || c->pm_grid > 1024) return JT_EINVAL;
+    if (!(c->theta >= 0.0) || !std::isfinite(c->theta)) return JT_EINVAL;
+    if (!(c->softening >= 0.0) || !std::isfinite(c->softening)) return JT_EINVAL;
+    if (!(c->r_cut > 0.0) || c->r_cut >= 0.5 * c->box_L) return JT_EINVAL;
+    if (c->mode == JT_ACCURATE && !(c->r_s > 0.0)) return JT_EINVAL;
+    if (!(c->mu >= 0.0) || !std::isfinite(c->mu)) return JT_EINVAL;
+    if (!(c->G_mass_plus > 0.0) || !std::isfinite(c->G_mass_plus)) return JT_EINVAL;
+    if (c->k_min < 0) return JT_EINVAL;
+    if (c->mode != JT_ACCURATE && c->mode != JT_RCOMPAT) return JT_EINVAL;
+    if (c->integrator != JT_KDK && c->integrator != JT_DKD_REF) return JT_EINVAL;
+    return JT_OK;
+}
+
+void free_particles(jt_handle* h)
+{
+    for (int s = 0; s < 2; s++) {
+        dfree(h->pos[s]); dfree(h->vel[s]); dfree(h->acc[s]);
+        dfree(h->pos_b[s]); dfree(h->vel_b[s]);
+        dfree(h->id[s]); dfree(h->id_b[s]); dfree(h->gmap[s]);
+        jt_tree_dev& t = h->tree[s];
+        dfree(t.child); dfree(t.parent); dfree(t.flag); dfree(t.com); dfree(t.bmin);
+        dfree(t.bmax); dfree(t.quad0); dfree(t.quad1); dfree(t.m30); dfree(t.tie);
+        t = jt_tree_dev{};
+        h->cap[s] = 0;
+    }
+    jt_sort_ws_free(&h->ws);
+    dfree(h->key64);
+    dfree(h->pos_caller); dfree(h->acc_caller); dfree(h->sign_caller); dfree(h->rank_buf);
+    if (h->stage) cudaFree(h->stage);
+    h->stage = nullptr;
+    h->stage_bytes = 0;
+}
+
+int alloc_particles(jt_handle* h, int64_t n0, int64_t n1)
+{
+    if (h->stage && h->cap[0] == n0 && h->cap[1] == n1) return JT_OK;  // same sizes: reuse
+    free_particles(h);
+    int64_t nn[2] = {n0, n1};
+    for (int s = 0; s < 2; s++) {
+        int64_t n = nn[s], nodes = n > 0 ? 2 * n - 1 : 1;
+        JT_TRY(dalloc(&h->pos[s], n)); JT_TRY(dalloc(&h->vel[s], n)); JT_TRY(dalloc(&h->acc[s], n));
+        JT_TRY(dalloc(&h->pos_b[s], n)); JT_TRY(dalloc(&h->vel_b[s], n));
+        JT_TRY(dalloc(&h->id[s], n)); JT_TRY(dalloc(&h->id_b[s], n)); JT_TRY(dalloc(&h->gmap[s], n));
+        jt_tree_dev& t = h->tree[s];
+        JT_TRY(dalloc(&t.child, nodes)); JT_TRY(dalloc(&t.parent, nodes));
+        JT_TRY(dalloc(&t.flag, n > 1 ? n - 1 : 1));
+        JT_TRY(dalloc(&t.com, nodes)); JT_TRY(dalloc(&t.bmin, nodes)); JT_TRY(dalloc(&t.bmax, nodes));
+        JT_TRY(dalloc(&t.quad0, nodes)); JT_TRY(dalloc(&t.quad1, nodes));
+        JT_TRY(dalloc(&t.m30, n)); JT_TRY(dalloc(&t.tie, n));
+        t.n = n;
+        h->cap[s] = n;
+    }
+    int64_t nmax = n0 > n1 ? n0 : n1;
+    if (jt_sort_ws_alloc(&h->ws, nmax > 0 ? nmax : 1, 8) != 0) return JT_ENOMEM;
+    JT_TRY(dalloc(&h->key64, nmax));
+    int64_t na = n0 + n1;
+    JT_TRY(dalloc(&h->pos_caller, na)); JT_TRY(dalloc(&h->acc_caller, na));
+    JT_TRY(dalloc(&h->sign_caller, na)); JT_TRY(dalloc(&h->rank_buf, na));
+    h->stage_bytes = sizeof(float) * 3 * (size_t)(na > 0 ? na : 1) * 2;
+    if (!cuda_ok(cudaMalloc(&h->stage, h->stage_bytes))) return JT_ENOMEM;
+    return JT_OK;
+}
+
+int alloc_pm(jt_handle* h)
+{
+    jt_pm_dev& pm = h->pm;
+    int M = h->cfg.pm_grid;
+    pm.M = M;
+    pm.L = h->cfg.box_L;
+    int64_t G = (int64_t)M * M * M, Gc = (int64_t)M * M * (M / 2 + 1);
+    bool rc = h->cfg.mode == JT_RCOMPAT;
+    JT_TRY(dalloc(&pm.rho, G));
+    if (!rc) JT_TRY(dalloc(&pm.rho_k, Gc));
+    // accurate: 3 spectra + the per-axis factor table (M float4 = 2M complex)
+    JT_TRY(dalloc(&pm.force_k, rc ? Gc : 3 * Gc + 2 * (int64_t)M));
+    JT_TRY(dalloc(&pm.force, rc ? G : 3 * G));
+    JT_FFT(cufftPlan3d(&pm.plan_r2c, M, M, M, CUFFT_R2C));
+    if (rc) {
+        JT_FFT(cufftPlan3d(&pm.plan_c2r, M, M, M, CUFFT_C2R));
+    } else {
+        int dims[3] = {M, M, M};
+        JT_FFT(cufftPlanMany(&pm.plan_c2r, 3, dims, nullptr, 1, (int)Gc, nullptr, 1, (int)G,
+                             CUFFT_C2R, 3));
+        // per-axis factors: k_n, gradient factor (0 at Nyquist), exp(-k^2 r_s^2)/sinc^4, |n|
+        std::vector<float> tab(4 * (size_t)M);
+        double dk = 2.0 * M_PI / h->cfg.box_L, rs = h->cfg.r_s;
+        for (int n = 0; n < M; n++) {
+            int ni = n <= M / 2 ? n : n - M;
+            double k = dk * ni;
+            double u = M_PI * ni / M;
+            double sinc = ni == 0 ? 1.0 : std::sin(u) / u;
+            double f = std::exp(-k * k * rs * rs) / (sinc * sinc * sinc * sinc);
+            tab[4 * n] = (float)k;
+            tab[4 * n + 1] = (n == M / 2) ? 0.0f : (float)k;
+            tab[4 * n + 2] = (float)f;
+            tab[4 * n + 3] = (float)(ni < 0 ? -ni : ni);
+        }
+        JT_CU(cudaMemcpy(pm.force_k + 3 * Gc, tab.data(), sizeof(float) * tab.size(),
+                         cudaMemcpyHostToDevice));
+    }
+    JT_FFT(cufftSetStream(pm.plan_r2c, h->st));
+    JT_FFT(cufftSetStream(pm.plan_c2r, h->st));
+    pm.plans_ready = 1;
+    return JT_OK;
+}
+
+void free_pm(jt_handle* h)
+{
+    jt_pm_dev& pm = h->pm;
+    if (pm.plans_ready) {
+        cufftDestroy(pm.plan_r2c);
+        cufftDestroy(pm.plan_c2r);
+    }
+    dfree(pm.rho); dfree(pm.rho_k); dfree(pm.force_k); dfree(pm.force);
+    pm = jt_pm_dev{};
+}
+
+int id_bits(int64_t n)
+{
+    int b = 0;
+    while (b < 32 && ((int64_t)1 << b) < n) b++;
+    return b;
+}
+
+// Sort both species by Morton key, reorder the state, build both trees.
+// rc_keys: the reference's 64-bit keys (m30 << 32 | caller index), else m30.
+int build_trees(jt_handle* h, bool rc_keys, bool rc_nodes)
+{
+    float box_half = (float)(h->cfg.box_L / 2.0);
+    for (int s = 0; s < 2; s++) {
+        int64_t n = h->n[s];
+        if (n == 0) continue;
+        jt_tree_dev& t = h->tree[s];
+        if (rc_keys) {
+            jt_launch_morton(h->pos[s], h->id[s], n, box_half, nullptr, h->key64, h->ws.vals, h->st);
+            int shifts[8], np = 0;
+            int ib = id_bits(n);
+            for (int b = 0; b < ib; b += 8) shifts[np++] = b;
+            for (int b = 32; b < 62; b += 8) shifts[np++] = b;
+            JT_TRY(jt_radix_sort_u64(h->key64, h->ws.vals, n, shifts, np, &h->ws, h->d_err, h->st));
+            jt_launch_split_keys(h->key64, n, t.m30, t.tie, h->st);
+        } else {
+            jt_launch_morton(h->pos[s], h->id[s], n, box_half, t.m30, nullptr, h->ws.vals, h->st);
+            const int shifts[4] = {0, 8, 16, 24};
+            JT_TRY(jt_radix_sort_u32(t.m30, h->ws.vals, n, shifts, 4, &h->ws, h->d_err, h->st));
+        }
+        jt_launch_reorder(h->ws.vals, n, h->pos[s], h->pos_b[s], h->vel[s], h->vel_b[s], h->id[s],
+                          h->id_b[s], h->st);
+        std::swap(h->pos[s], h->pos_b[s]);
+        std::swap(h->vel[s], h->vel_b[s]);
+        std::swap(h->id[s], h->id_b[s]);
+        t.n = n;
+    }
+    cudaEventRecord(h->ev[1], h->st);
+    for (int s = 0; s < 2; s++) {
+        int64_t n = h->n[s];
+        if (n == 0) continue;
+        jt_tree_dev tk = h->tree[s];
+        if (!rc_keys) tk.tie = nullptr;  // tie = sorted position
+        jt_launch_karras(tk, h->st);
+        jt_launch_moments(h->tree[s], h->pos[s], h->mass[s], box_half, rc_nodes ? 1 : 0, h->st);
+    }
+    return cudaGetLastError() == cudaSuccess ? JT_OK : JT_ECUDA;
+}
+
+int check_device_error(jt_handle* h)
+{
+    unsigned e = 0;
+    JT_CU(cudaMemcpyAsync(&e, h->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, h->st));
+    JT_CU(cudaStreamSynchronize(h->st));
+    if (e) {
+        cudaMemsetAsync(h->d_err, 0, sizeof(unsigned), h->st);
+        cudaStreamSynchronize(h->st);
+        if (e & JT_ERRBIT_LOOKBACK) return JT_ETIMEDOUT;
+        return JT_EOVERFLOW;
+    }
+    return JT_OK;
+}
+
+float elapsed(cudaEvent_t a, cudaEvent_t b)
+{
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) return 0.f;
+    return ms;
+}
+
+// Compute accelerations at the current positions into acc[s] (internal order).
+// kick_dt/drag: closing kick fused into the accurate walk (0 = none).
+int compute_forces(jt_handle* h, float kick_dt, float drag)
+{
+    const jt_config& c = h->cfg;
+    const bool rc = c.mode == JT_RCOMPAT;
+    cudaStream_t st = h->st;
+    int M = c.pm_grid;
+    int64_t G = (int64_t)M * M * M;
+    cudaEventRecord(h->ev[0], st);
+    JT_TRY(build_trees(h, rc, rc));
+    cudaEventRecord(h->ev[2], st);
+    JT_CU(cudaMemsetAsync(h->pm.rho, 0, sizeof(float) * G, st));
+    if (rc) {
+        for (int s = 0; s < 2; s++)
+            jt_launch_to_caller(h->pos[s], h->id[s], h->gmap[s], h->n[s], h->pos_caller, st);
+        double cell = c.box_L / M;
+        jt_launch_rcompat_deposit(h->pos_caller, h->sign_caller, h->n[0] + h->n[1], h->mass,
+                                  h->pm.rho, M, (float)(c.box_L / 2.0), (float)(M / c.box_L),
+                                  (float)(1.0 / (cell * cell * cell)), st);
+    } else {
+        double h3 = std::pow(c.box_L / M, 3.0);
+        jt_launch_deposit(h->pos[0], h->n[0], (float)(h->mass[0] / h3), h->pos[1], h->n[1],
+                          (float)(-h->mass[1] / h3), h->pm.rho, M, (float)c.box_L, 0, st);
+    }
+    cudaEventRecord(h->ev[3], st);
+    if (rc) {
+        JT_FFT(cufftExecR2C(h->pm.plan_r2c, h->pm.rho, h->pm.force_k));
+        cudaEventRecord(h->ev[4], st);
+        jt_launch_kspace(nullptr, h->pm.force_k, M, c.box_L, c.r_cut / 3.0, c.k_min, 1, st);
+        cudaEventRecord(h->ev[5], st);
+        JT_FFT(cufftExecC2R(h->pm.plan_c2r, h->pm.force_k, h->pm.force));
+    } else {
+        JT_FFT(cufftExecR2C(h->pm.plan_r2c, h->pm.rho, h->pm.rho_k));
+        cudaEventRecord(h->ev[4], st);
+        jt_launch_kspace(h->pm.rho_k, h->pm.force_k, M, c.box_L, c.r_s, c.k_min, 0, st);
+        cudaEventRecord(h->ev[5], st);
+        JT_FFT(cufftExecC2R(h->pm.plan_c2r, h->pm.force_k, h->pm.force));
+    }
+    cudaEventRecord(h->ev[6], st);
+    if (rc) {
+        float tq, sq, rq, bq;
+        {
+            // host packing of the reference (:4079-4082, :1932-1937) and the
+            // kernel's unpacking (:1684-1694)
+            auto sat = [](double v) -> unsigned {
+                return v <= 0.0 ? 0u : (v >= 4294967295.0 ? 0xFFFFFFFFu : (unsigned)v);
+            };
+            unsigned ti = sat(c.theta * 1000.0), si = sat(c.softening * 1000.0);
+            unsigned ri = sat(c.r_cut), bi = sat(c.box_L / 2.0);
+            ti = ti > 0xFFFF ? 0xFFFF : ti; si = si > 0xFFFF ? 0xFFFF : si;
+            ri = ri > 0xFFFF ? 0xFFFF : ri; bi = bi > 0xFFFF ? 0xFFFF : bi;
+            tq = (float)ti / 1000.0f; sq = (float)si / 1000.0f; rq = (float)ri; bq = (float)bi;
+        }
+        jt_rc_params P;
+        P.theta2 = tq * tq;
+        P.eps2 = sq * sq;
+        P.r_cut = rq;
+        P.box_half_q = bq;
+        P.r_s = rq / 3.0f;
+        P.box_half = (float)(c.box_L / 2.0);
+        P.inv_cell = (float)(M / c.box_L);
+        P.cell = (float)(c.box_L / M);
+        P.M = M;
+        P.mass[0] = h->mass[0];
+        P.mass[1] = h->mass[1];
+        const float4* sp2[2] = {h->pos[0], h->pos[1]};
+        jt_launch_walk_rcompat(P, h->pos_caller, h->sign_caller, h->n[0] + h->n[1], sp2, h->n,
+                               h->tree, h->pm.force, h->acc_caller, h->d_err, st);
+        for (int s = 0; s < 2; s++)
+            jt_launch_from_caller(h->acc_caller, h->id[s], h->gmap[s], h->n[s], h->acc[s], st);
+        if (kick_dt != 0.0f)
+            for (int s = 0; s < 2; s++) jt_launch_kick(h->vel[s], h->acc[s], h->n[s], kick_dt, drag, st);
+    } else {
+        jt_walk_params P;
+        P.L = (float)c.box_L;
+        P.halfL = (float)(c.box_L / 2.0);
+        P.theta2 = (float)(c.theta * c.theta);
+        P.rc = (float)c.r_cut;
+        P.rc2 = (float)(c.r_cut * c.r_cut);
+        P.eps2 = (float)(c.softening * c.softening);
+        P.c = (float)(1.0 / (2.0 * c.r_s));
+        P.mass[0] = h->mass[0];
+        P.mass[1] = h->mass[1];
+        P.M = M;
+        P.h_inv = (float)(M / c.box_L);
+        const float4* p2[2] = {h->pos[0], h->pos[1]};
+        float4* a2[2] = {h->acc[0], h->acc[1]};
+        float4* v2[2] = {h->vel[0], h->vel[1]};
+        jt_launch_walk_accurate(P, p2, h->n, h->tree, h->pm.force, a2, v2, kick_dt, drag,
+                                h->d_inter, h->d_err, st);
+    }
+    cudaEventRecord(h->ev[7], st);
+    JT_CU(cudaGetLastError());
+    h->acc_valid = true;
+    return JT_OK;
+}
+
+void accumulate_timings(jt_handle* h)
+{
+    // ev0 start, ev1 (last species) karras start, ev2 trees done, ev3 deposit
+    // done, ev4 R2C done, ev5 k-space done, ev6 C2R done, ev7 walk done
+    h->tm.sort_ms += elapsed(h->ev[0], h->ev[1]);
+    h->tm.tree_ms += elapsed(h->ev[1], h->ev[2]);
+    h->tm.deposit_ms += elapsed(h->ev[2], h->ev[3]);
+    h->tm.fft_ms += elapsed(h->ev[3], h->ev[6]);
+    h->tm.kspace_ms += elapsed(h->ev[4], h->ev[5]);
+    h->tm.walk_ms += elapsed(h->ev[6], h->ev[7]);
+}
+
+int fetch_inter(jt_handle* h)
+{
+    unsigned long long v = 0;
+    JT_CU(cudaMemcpyAsync(&v, h->d_inter, sizeof(v), cudaMemcpyDeviceToHost, h->st));
+    JT_CU(cudaStreamSynchronize(h->st));
+    h->tm.interactions += (int64_t)v;
+    JT_CU(cudaMemsetAsync(h->d_inter, 0, sizeof(v), h->st));
+    return JT_OK;
+}
+
+void set_masses(jt_handle* h)
+{
+    double mp = h->cfg.G_mass_plus;
+    double mm = h->n[1] > 0 ? h->cfg.mu * mp * (double)h->n[0] / (double)h->n[1] : 0.0;
+    if (h->n[0] == 0) mm = h->cfg.mu * mp;  // no m+ particles: m- per particle = mu * m+
+    h->mass[0] = (float)mp;
+    h->mass[1] = (float)mm;
+}
+
+int copy_in(jt_handle* h, const void* src, size_t bytes, int mem, void** dev)
+{
+    if (mem == JT_MEM_DEVICE) {
+        *dev = const_cast<void*>(src);
+        return JT_OK;
+    }
+    if (bytes > h->stage_bytes) return JT_EINVAL;
+    JT_CU(cudaMemcpyAsync(h->stage, src, bytes, cudaMemcpyHostToDevice, h->st));
+    *dev = h->stage;
+    return JT_OK;
+}
+
+int write_out(jt_handle* h, const float4* src, const int* id, const int* gmap, int64_t n,
+              float* dst, int mem)
+{
+    if (!dst || n == 0) return JT_OK;
+    float* target = mem == JT_MEM_DEVICE ? dst : (float*)h->stage;
+    jt_launch_aos_out(src, id, gmap, n, target, h->st);
+    if (mem == JT_MEM_HOST)
+        JT_CU(cudaMemcpyAsync(dst, h->stage, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, h->st));
+    return JT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* jt_version(void) { return "janus-treepm-b200 0.1 sm_100a"; }
+
+const char* jt_strerror(int code)
+{
+    switch (code) {
+    case JT_OK: return "ok";
+    case JT_EINVAL: return "invalid argument";
+    case JT_ENOMEM: return "out of memory";
+    case JT_ECUDA: return "CUDA or cuFFT error";
+    case JT_ETIMEDOUT: return "device wait timed out";
+    case JT_ENOTIMPL: return "not implemented";
+    case JT_ESTATE: return "call out of order";
+    case JT_EOVERFLOW: return "device list overflow";
+    case JT_EBUSY: return "admission refused";
+    default: return "unknown error";
+    }
+}
+
+int jt_create(const jt_config* cfg, jt_handle** out)
+{
+    if (!out) return JT_EINVAL;
+    *out = nullptr;
+    JT_TRY(validate(cfg));
+    jt_handle* h = new (std::nothrow) jt_handle();
+    if (!h) return JT_ENOMEM;
+    h->cfg = *cfg;
+    int r = JT_OK;
+    if (cudaGetDevice(&h->device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
+        delete h;
+        return JT_ECUDA;
+    }
+    for (auto& e : h->ev) cudaEventCreate(&e);
+    if (cudaMalloc(&h->d_err, sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&h->d_inter, sizeof(unsigned long long)) != cudaSuccess) r = JT_ENOMEM;
+    if (r == JT_OK) {
+        cudaMemset(h->d_err, 0, sizeof(unsigned));
+        cudaMemset(h->d_inter, 0, sizeof(unsigned long long));
+        r = alloc_pm(h);
+    }
+    if (r != JT_OK) {
+        jt_destroy(h);
+        return r;
+    }
+    *out = h;
+    return JT_OK;
+}
+
+void jt_destroy(jt_handle* h)
+{
+    if (!h) return;
+    if (h->st) cudaStreamSynchronize(h->st);
+    free_particles(h);
+    free_pm(h);
+    if (h->d_err) cudaFree(h->d_err);
+    if (h->d_inter) cudaFree(h->d_inter);
+    for (auto& e : h->ev)
+        if (e) cudaEventDestroy(e);
+    if (h->st) cudaStreamDestroy(h->st);
+    delete h;
+}
+
+int jt_set_state(jt_handle* h, const float* pos_p, const float* vel_p, size_t n_p,
+                 const float* pos_m, const float* vel_m, size_t n_m, int mem)
+{
+    if (!h || (mem != JT_MEM_HOST && mem != JT_MEM_DEVICE)) return JT_EINVAL;
+    if ((n_p && !pos_p) || (n_m && !pos_m)) return JT_EINVAL;
+    if (n_p + n_m == 0) return JT_EINVAL;
+    if (n_p >= (size_t)1 << 30 || n_m >= (size_t)1 << 30) return JT_EINVAL;
+    h->have_state = false;
+    h->acc_valid = false;
+    JT_TRY(alloc_particles(h, (int64_t)n_p, (int64_t)n_m));
+    h->n[0] = (int64_t)n_p;
+    h->n[1] = (int64_t)n_m;
+    set_masses(h);
+    const float* pp[2] = {pos_p, pos_m};
+    const float* vv[2] = {vel_p, vel_m};
+    for (int s = 0; s < 2; s++) {
+        int64_t n = h->n[s];
+        if (n == 0) continue;
+        void* d = nullptr;
+        JT_TRY(copy_in(h, pp[s], sizeof(float) * 3 * n, mem, &d));
+        jt_launch_aos_in((const float*)d, n, h->pos[s], h->id[s], h->st);
+        if (vv[s]) {
+            JT_TRY(copy_in(h, vv[s], sizeof(float) * 3 * n, mem, &d));
+            jt_launch_aos_in((const float*)d, n, h->vel[s], nullptr, h->st);
+        } else {
+            JT_CU(cudaMemsetAsync(h->vel[s], 0, sizeof(float4) * n, h->st));
+        }
+        // caller layout: [m+ ; m-]
+        std::vector<int> g(n);
+        for (int64_t i = 0; i < n; i++) g[i] = (int)(i + (s == 1 ? h->n[0] : 0));
+        JT_CU(cudaMemcpyAsync(h->gmap[s], g.data(), sizeof(int) * n, cudaMemcpyHostToDevice, h->st));
+        JT_CU(cudaStreamSynchronize(h->st));
+    }
+    std::vector<int8_t> sg((size_t)(h->n[0] + h->n[1]));
+    for (int64_t i = 0; i < h->n[0] + h->n[1]; i++) sg[i] = i < h->n[0] ? 1 : -1;
+    if (!sg.empty())
+        JT_CU(cudaMemcpyAsync(h->sign_caller, sg.data(), sg.size(), cudaMemcpyHostToDevice, h->st));
+    JT_CU(cudaStreamSynchronize(h->st));
+    h->signed_layout = false;
+    h->have_state = true;
+    return JT_OK;
+}
+
+int jt_set_state_signed(jt_handle* h, const float* pos, const float* vel, const int8_t* signs,
+                        size_t n, int mem)
+{
+    if (!h || !pos || !signs || n == 0 || (mem != JT_MEM_HOST && mem != JT_MEM_DEVICE))
+        return JT_EINVAL;
+    if (n >= (size_t)1 << 30) return JT_EINVAL;
+    std::vector<int8_t> sg(n);
+    if (mem == JT_MEM_DEVICE) {
+        JT_CU(cudaMemcpy(sg.data(), signs, n, cudaMemcpyDeviceToHost));
+    } else {
+        std::memcpy(sg.data(), signs, n);
+    }
+    std::vector<int> rank(n);
+    int64_t c[2] = {0, 0};
+    for (size_t i = 0; i < n; i++) {
+        if (sg[i] != 1 && sg[i] != -1) return JT_EINVAL;
+        int s = sg[i] > 0 ? 0 : 1;
+        rank[i] = (int)c[s]++;
+    }
+    h->have_state = false;
+    h->acc_valid = false;
+    JT_TRY(alloc_particles(h, c[0], c[1]));
+    h->n[0] = c[0];
+    h->n[1] = c[1];
+    set_masses(h);
+    JT_CU(cudaMemcpyAsync(h->rank_buf, rank.data(), sizeof(int) * n, cudaMemcpyHostToDevice, h->st));
+    JT_CU(cudaMemcpyAsync(h->sign_caller, sg.data(), n, cudaMemcpyHostToDevice, h->st));
+    const float* dpos = pos;
+    const float* dvel = vel;
+    if (mem == JT_MEM_HOST) {
+        float* stg = (float*)h->stage;
+        JT_CU(cudaMemcpyAsync(stg, pos, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, h->st));
+        dpos = stg;
+        if (vel) {
+            JT_CU(cudaMemcpyAsync(stg + 3 * n, vel, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, h->st));
+            dvel = stg + 3 * n;
+        }
+    }
+    jt_launch_split_signed(dpos, dvel, h->sign_caller, (int64_t)n, h->rank_buf, h->pos[0], h->vel[0],
+                           h->id[0], h->gmap[0], h->pos[1], h->vel[1], h->id[1], h->gmap[1], h->st);
+    JT_CU(cudaStreamSynchronize(h->st));
+    JT_CU(cudaGetLastError());
+    h->signed_layout = true;
+    h->have_state = true;
+    return JT_OK;
+}
+
+int jt_accel(jt_handle* h, float* acc_p, float* acc_m, int mem)
+{
+    if (!h || (mem != JT_MEM_HOST && mem != JT_MEM_DEVICE)) return JT_EINVAL;
+    if (!h->have_state) return JT_ESTATE;
+    h->tm = jt_timings{};
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    cudaEventRecord(t0, h->st);
+    int r = compute_forces(h, 0.0f, 0.0f);
+    if (r == JT_OK) {
+        if (!h->signed_layout) {
+            r = write_out(h, h->acc[0], h->id[0], nullptr, h->n[0], acc_p, mem);
+            if (r == JT_OK) {
+                // the host path reuses the staging buffer: finish the first copy
+                if (mem == JT_MEM_HOST) cudaStreamSynchronize(h->st);
+                r = write_out(h, h->acc[1], h->id[1], nullptr, h->n[1], acc_m, mem);
+            }
+        } else {
+            r = JT_EINVAL;  // state loaded with the signed layout: use jt_accel_signed
+        }
+    }
+    cudaEventRecord(t1, h->st);
+    int e = check_device_error(h);
+    if (r == JT_OK) r = e;
+    if (r == JT_OK) {
+        accumulate_timings(h);
+        h->tm.total_ms = elapsed(t0, t1);
+        fetch_inter(h);
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    return r;
+}
+
+int jt_accel_signed(jt_handle* h, float* acc, int mem)
+{
+    if (!h || !acc || (mem != JT_MEM_HOST && mem != JT_MEM_DEVICE)) return JT_EINVAL;
+    if (!h->have_state) return JT_ESTATE;
+    h->tm = jt_timings{};
+    int r = compute_forces(h, 0.0f, 0.0f);
+    if (r == JT_OK) {
+        int64_t na = h->n[0] + h->n[1];
+        float* target = mem == JT_MEM_DEVICE ? acc : (float*)h->stage;
+        for (int s = 0; s < 2; s++)
+            jt_launch_aos_out(h->acc[s], h->id[s], h->gmap[s], h->n[s], target, h->st);
+        if (mem == JT_MEM_HOST)
+            cudaMemcpyAsync(acc, h->stage, sizeof(float) * 3 * na, cudaMemcpyDeviceToHost, h->st);
+    }
+    int e = check_device_error(h);
+    if (r == JT_OK) r = e;
+    if (r == JT_OK) {
+        accumulate_timings(h);
+        fetch_inter(h);
+    }
+    return r;
+}
+
+int jt_step(jt_handle* h, double dt, double hubble, double dtau_per_dt, int nsteps)
+{
+    if (!h || nsteps < 0 || !std::isfinite(dt) || !std::isfinite(hubble) || !std::isfinite(dtau_per_dt))
+        return JT_EINVAL;
+    if (!h->have_state) return JT_ESTATE;
+    if (nsteps == 0) return JT_OK;
+    h->tm = jt_timings{};
+    const jt_config& c = h->cfg;
+    // FP64 step factors, applied in FP32
+    const double drag_d = hubble * dtau_per_dt;
+    const float drag = (float)drag_d;
+    const float L = (float)c.box_L, halfL = (float)(c.box_L / 2.0);
+    cudaEvent_t t0, t1, k0, k1;
+    cudaEventCreate(&t0); cudaEventCreate(&t1); cudaEventCreate(&k0); cudaEventCreate(&k1);
+    cudaEventRecord(t0, h->st);
+    int r = JT_OK;
+    double kd_ms = 0.0;
+    if (c.integrator == JT_KDK) {
+        const float half = (float)(0.5 * dt), full = (float)dt;
+        if (!h->acc_valid) {
+            r = compute_forces(h, 0.0f, 0.0f);
+            if (r == JT_OK) { r = check_device_error(h); if (r == JT_OK) accumulate_timings(h); }
+        }
+        for (int k = 0; k < nsteps && r == JT_OK; k++) {
+            cudaEventRecord(k0, h->st);
+            for (int s = 0; s < 2; s++) {
+                jt_launch_kick(h->vel[s], h->acc[s], h->n[s], half, drag, h->st);
+                jt_launch_drift(h->pos[s], h->vel[s], h->n[s], full, L, halfL, h->st);
+            }
+            cudaEventRecord(k1, h->st);
+            r = compute_forces(h, half, drag);
+            if (r != JT_OK) break;
+            r = check_device_error(h);
+            if (r != JT_OK) break;
+            accumulate_timings(h);
+            kd_ms += elapsed(k0, k1);
+        }
+    } else {
+        const float half = (float)(0.5 * dt), full = (float)dt;
+        for (int k = 0; k < nsteps && r == JT_OK; k++) {
+            cudaEventRecord(k0, h->st);
+            for (int s = 0; s < 2; s++)
+                jt_launch_drift(h->pos[s], h->vel[s], h->n[s], half, L, halfL, h->st);
+            cudaEventRecord(k1, h->st);
+            r = compute_forces(h, 0.0f, 0.0f);
+            if (r != JT_OK) break;
+            for (int s = 0; s < 2; s++) {
+                jt_launch_kick(h->vel[s], h->acc[s], h->n[s], full, drag, h->st);
+                jt_launch_drift(h->pos[s], h->vel[s], h->n[s], half, L, halfL, h->st);
+            }
+            r = check_device_error(h);
+            if (r != JT_OK) break;
+            accumulate_timings(h);
+            kd_ms += elapsed(k0, k1);
+            h->acc_valid = false;  // acc belongs to the half-drifted positions
+        }
+    }
+    cudaEventRecord(t1, h->st);
+    if (cudaStreamSynchronize(h->st) != cudaSuccess && r == JT_OK) r = JT_ECUDA;
+    if (r == JT_OK) {
+        h->tm.total_ms = elapsed(t0, t1);
+        h->tm.kick_drift_ms = kd_ms;
+        fetch_inter(h);
+    }
+    cudaEventDestroy(t0); cudaEventDestroy(t1); cudaEventDestroy(k0); cudaEventDestroy(k1);
+    return r;
+}
+
+int jt_get_state(jt_handle* h, float* pos_p, float* vel_p, float* pos_m, float* vel_m, int mem)
+{
+    if (!h || (mem != JT_MEM_HOST && mem != JT_MEM_DEVICE)) return JT_EINVAL;
+    if (!h->have_state) return JT_ESTATE;
+    float* outs[2][2] = {{pos_p, vel_p}, {pos_m, vel_m}};
+    for (int s = 0; s < 2; s++) {
+        for (int q = 0; q < 2; q++) {
+            JT_TRY(write_out(h, q == 0 ? h->pos[s] : h->vel[s], h->id[s], nullptr, h->n[s],
+                             outs[s][q], mem));
+            JT_CU(cudaStreamSynchronize(h->st));
+        }
+    }
+    return JT_OK;
+}
+
+int jt_get_state_signed(jt_handle* h, float* pos, float* vel, int mem)
+{
+    if (!h || (mem != JT_MEM_HOST && mem != JT_MEM_DEVICE)) return JT_EINVAL;
+    if (!h->have_state) return JT_ESTATE;
+    int64_t na = h->n[0] + h->n[1];
+    float* outs[2] = {pos, vel};
+    for (int q = 0; q < 2; q++) {
+        if (!outs[q]) continue;
+        float* target = mem == JT_MEM_DEVICE ? outs[q] : (float*)h->stage;
+        for (int s = 0; s < 2; s++)
+            jt_launch_aos_out(q == 0 ? h->pos[s] : h->vel[s], h->id[s], h->gmap[s], h->n[s], target, h->st);
+        if (mem == JT_MEM_HOST)
+            JT_CU(cudaMemcpyAsync(outs[q], h->stage, sizeof(float) * 3 * na, cudaMemcpyDeviceToHost, h->st));
+        JT_CU(cudaStreamSynchronize(h->st));
+    }
+    return JT_OK;
+}
+
+int jt_debug_tree(jt_handle* h, int species, uint32_t* morton, int32_t* perm, int32_t* left,
+                  int32_t* right, int32_t* parent)
+{
+    if (!h || species < 0 || species > 1) return JT_EINVAL;
+    if (!h->have_state) return JT_ESTATE;
+    int64_t n = h->n[species];
+    if (n == 0) return JT_OK;
+    jt_tree_dev& t = h->tree[species];
+    float box_half = (float)(h->cfg.box_L / 2.0);
+    // reference keys at the current positions, without moving the state
+    jt_launch_morton(h->pos[species], h->id[species], n, box_half, nullptr, h->key64, h->ws.vals, h->st);
+    int shifts[8], np = 0;
+    for (int b = 0; b < id_bits(n); b += 8) shifts[np++] = b;
+    for (int b = 32; b < 62; b += 8) shifts[np++] = b;
+    JT_TRY(jt_radix_sort_u64(h->key64, h->ws.vals, n, shifts, np, &h->ws, h->d_err, h->st));
+    jt_launch_split_keys(h->key64, n, t.m30, t.tie, h->st);
+    jt_tree_dev tk = t;
+    tk.n = n;
+    jt_launch_karras(tk, h->st);
+    JT_TRY(check_device_error(h));
+    int64_t nn = 2 * n - 1;
+    std::vector<int2> ch(nn);
+    if (morton) JT_CU(cudaMemcpy(morton, t.m30, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost));
+    if (perm) JT_CU(cudaMemcpy(perm, t.tie, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+    JT_CU(cudaMemcpy(ch.data(), t.child, sizeof(int2) * nn, cudaMemcpyDeviceToHost));
+    if (parent) JT_CU(cudaMemcpy(parent, t.parent, sizeof(int32_t) * nn, cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < nn; i++) {
+        if (left) left[i] = ch[i].x;
+        if (right) right[i] = ch[i].y;
+    }
+    // the tree arrays no longer describe the state order; the next force
+    // evaluation rebuilds them
+    return JT_OK;
+}
+
+int jt_get_timings(jt_handle* h, jt_timings* t)
+{
+    if (!h || !t) return JT_EINVAL;
+    *t = h->tm;
+    return JT_OK;
+}
+
+int jt_counts(jt_handle* h, size_t* n_p, size_t* n_m)
+{
+    if (!h) return JT_EINVAL;
+    if (n_p) *n_p = (size_t)h->n[0];
+    if (n_m) *n_m = (size_t)h->n[1];
+    return JT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,722 @@
+// Short-range tree walk (+ PM interpolation, + kick), and the step kernels.
+//
+// ACCURATE walk (k_walk_acc): one warp per group of 32 Morton-consecutive
+// target particles of one species; both species' trees are walked in the same
+// launch.  The warp tests up to 32 nodes at once (breadth-batched traversal
+// from a per-warp stack in shared memory): a node whose AABB lies farther than
+// r_cut from the group's AABB (periodic) is dropped; a leaf becomes a direct
+// interaction; an internal node whose size l satisfies l < theta * d, with d
+// the distance from the group's AABB to the node's centre of mass, becomes a
+// monopole + quadrupole interaction; otherwise its two children are pushed.
+// Accepted entries are compacted with ballots into shared-memory lists that
+// all 32 lanes evaluate against their own particle once 32 entries are
+// queued.  Far-field (node) sums are Kahan-compensated.  The PM acceleration
+// is interpolated first (CIC of the three force grids) and the kick is
+// applied in the epilogue, so acc is written once.
+//
+// Pair force (G folded into m):  a_i += s_i s_j m_j S(r_p) r / r_p^3 for
+// |r| < r_cut, r_p^2 = r^2 + eps^2, S(x) = erfc(x) + 2x/sqrt(pi) e^{-x^2},
+// x = r_p/(2 r_s): the exact short-range complement of the Gaussian-filtered
+// PM force.  The reference (src/nbody_gpu_twopass.rs:1776-1785) uses erfc(x)
+// alone, which drops 0.42 of the Newtonian force at r = 2 r_s.
+//
+// RCOMPAT walk (k_walk_rc): the reference's forces_treepm_short_range
+// (:1670-1811) semantics for 32 particles of the caller-order array per warp:
+// one node at a time from a 128-entry stack (pushes only while sp < 127);
+// skip when every lane has r - hs > r_cut; monopole when every lane accepts
+// (leaf or 4 hs^2 < theta^2 r^2); otherwise descend.  Float expressions are
+// evaluated without contraction, in the reference's order.
+#include "jt_internal.cuh"
+
+namespace {
+
+constexpr int kWarps = JT_WARPS_PER_BLOCK;
+constexpr int kStackCap = 1536;
+constexpr int kListCap = 64;
+
+struct WalkWarpSmem {
+    int stack[kStackCap];
+    float4 dsrc[kListCap];
+    float4 acom[kListCap];
+    float4 aq0[kListCap];
+    float2 aq1[kListCap];
+};
+
+struct Acc3 {
+    float x, y, z;
+};
+
+__device__ __forceinline__ void kahan_add(float& s, float& c, float v)
+{
+    float y = v - c;
+    float t = s + y;
+    c = (t - s) - y;
+    s = t;
+}
+
+__device__ __forceinline__ float warp_min(float v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ float warp_max(float v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__device__ __forceinline__ float gap1(float d, float ext)
+{
+    float g = fabsf(d) - ext;
+    return g > 0.0f ? g : 0.0f;
+}
+
+struct WalkArgs {
+    jt_walk_params p;
+    const float4* pos[2];
+    int64_t n[2];
+    jt_tree_dev tree[2];
+    const float* force3;
+    float4* acc[2];
+    float4* vel[2];
+    float kick_dt, kick_drag;
+    int64_t groups0, groups1;
+    unsigned long long* inter;
+    unsigned* err;
+};
+
+// evaluate `cnt` queued direct sources against this lane's particle
+__device__ __forceinline__ void eval_direct(const float4* __restrict__ src, int cnt, float px,
+                                            float py, float pz, const jt_walk_params& P,
+                                            float fac, Acc3& a)
+{
+    for (int j = 0; j < cnt; j++) {
+        float4 q = src[j];
+        float dx = jt_wrap(q.x - px, P.L, P.halfL);
+        float dy = jt_wrap(q.y - py, P.L, P.halfL);
+        float dz = jt_wrap(q.z - pz, P.L, P.halfL);
+        float r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 < P.rc2 && r2 > 0.0f) {
+            float rp2 = r2 + P.eps2;
+            float ri = rsqrtf(rp2);
+            float x = rp2 * ri * P.c;
+            float g = fac * jt_split_S(x) * ri * ri * ri;
+            a.x += g * dx;
+            a.y += g * dy;
+            a.z += g * dz;
+        }
+    }
+}
+
+// evaluate `cnt` queued nodes (monopole + quadrupole), Kahan-compensated
+__device__ __forceinline__ void eval_approx(const float4* __restrict__ cm, const float4* __restrict__ q0s,
+                                            const float2* __restrict__ q1s, int cnt, float px,
+                                            float py, float pz, const jt_walk_params& P, float sgn,
+                                            Acc3& s, Acc3& c)
+{
+    for (int j = 0; j < cnt; j++) {
+        float4 m = cm[j];
+        float dx = jt_wrap(m.x - px, P.L, P.halfL);
+        float dy = jt_wrap(m.y - py, P.L, P.halfL);
+        float dz = jt_wrap(m.z - pz, P.L, P.halfL);
+        float r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 < P.rc2) {
+            float rp2 = r2 + P.eps2;
+            float ri = rsqrtf(rp2);
+            float x = rp2 * ri * P.c;
+            jt_sfac f = jt_split_S2(x, P.c);
+            float ri2 = ri * ri, ri3 = ri2 * ri;
+            float g = f.S * ri3;
+            float G1 = (f.dS - 3.0f * f.S * ri) * ri2 * ri2;
+            float G2 = (f.d2S - 7.0f * f.dS * ri + 15.0f * f.S * ri2) * ri2 * ri3;
+            float4 a = q0s[j];  // xx yy zz xy
+            float2 b = q1s[j];  // xz yz
+            float qx = a.x * dx + a.w * dy + b.x * dz;
+            float qy = a.w * dx + a.y * dy + b.y * dz;
+            float qz = b.x * dx + b.y * dy + a.z * dz;
+            float dqd = dx * qx + dy * qy + dz * qz;
+            float tr = a.x + a.y + a.z;
+            float coef = sgn * (m.w * g + 0.5f * G1 * tr + 0.5f * G2 * dqd);
+            float g1s = sgn * G1;
+            kahan_add(s.x, c.x, coef * dx + g1s * qx);
+            kahan_add(s.y, c.y, coef * dy + g1s * qy);
+            kahan_add(s.z, c.z, coef * dz + g1s * qz);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kWarps * 32) k_walk_acc(WalkArgs A)
+{
+    __shared__ WalkWarpSmem smem_all[kWarps];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    WalkWarpSmem& S = smem_all[wib];
+    const int64_t gw = (int64_t)blockIdx.x * kWarps + wib;
+    int s;
+    int64_t grp;
+    if (gw < A.groups0) { s = 0; grp = gw; }
+    else if (gw < A.groups0 + A.groups1) { s = 1; grp = gw - A.groups0; }
+    else return;  // whole warp
+    const jt_walk_params& P = A.p;
+    const int64_t ns = A.n[s];
+    const int64_t i = grp * 32 + lane;
+    const bool valid = i < ns;
+    const float4 p = A.pos[s][valid ? i : grp * 32];
+    const float sgn_s = s == 0 ? 1.0f : -1.0f;
+    const unsigned lt = (1u << lane) - 1u;
+
+    // group AABB
+    float lox = warp_min(p.x), loy = warp_min(p.y), loz = warp_min(p.z);
+    float hix = warp_max(p.x), hiy = warp_max(p.y), hiz = warp_max(p.z);
+    float gcx = 0.5f * (lox + hix), gcy = 0.5f * (loy + hiy), gcz = 0.5f * (loz + hiz);
+    float ghx = 0.5f * (hix - lox), ghy = 0.5f * (hiy - loy), ghz = 0.5f * (hiz - loz);
+
+    // PM interpolation (CIC of the three force grids)
+    Acc3 pm = {0.f, 0.f, 0.f};
+    {
+        const int M = P.M, mask = M - 1;
+        const int64_t G = (int64_t)M * M * M, MM = (int64_t)M * M;
+        float gx = (p.x + P.halfL) * P.h_inv, gy = (p.y + P.halfL) * P.h_inv,
+              gz = (p.z + P.halfL) * P.h_inv;
+        float fx0 = floorf(gx), fy0 = floorf(gy), fz0 = floorf(gz);
+        float fx = gx - fx0, fy = gy - fy0, fz = gz - fz0;
+        int ix = (int)fx0 & mask, iy = (int)fy0 & mask, iz = (int)fz0 & mask;
+        int ixs[2] = {ix, (ix + 1) & mask}, iys[2] = {iy, (iy + 1) & mask},
+            izs[2] = {iz, (iz + 1) & mask};
+        float wx[2] = {1.f - fx, fx}, wy[2] = {1.f - fy, fy}, wz[2] = {1.f - fz, fz};
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            int dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
+            int64_t id = ixs[dx] + iys[dy] * (int64_t)M + izs[dz] * MM;
+            float w = wx[dx] * wy[dy] * wz[dz];
+            pm.x += w * __ldg(A.force3 + id);
+            pm.y += w * __ldg(A.force3 + G + id);
+            pm.z += w * __ldg(A.force3 + 2 * G + id);
+        }
+    }
+
+    Acc3 near = {0.f, 0.f, 0.f}, far = {0.f, 0.f, 0.f}, comp = {0.f, 0.f, 0.f};
+    unsigned long long inter = 0;
+    const unsigned nvalid = __popc(__ballot_sync(0xffffffffu, valid));
+
+    for (int t = 0; t < 2; t++) {
+        const int64_t nt = A.n[t];
+        if (nt == 0) continue;
+        const jt_tree_dev T = A.tree[t];
+        const float4* __restrict__ tpos = A.pos[t];
+        const float sgn = (s == t) ? 1.0f : -1.0f;
+        const float fac_direct = sgn * P.mass[t];
+        const int64_t leaf0 = nt - 1;
+        int sp = 1, nD = 0, nA = 0;
+        if (lane == 0) S.stack[0] = 0;
+        __syncwarp();
+        while (sp > 0) {
+            const int k = sp < 32 ? sp : 32;
+            int node = lane < k ? S.stack[sp - k + lane] : -1;
+            sp -= k;
+            __syncwarp();
+            if (node >= 2 * nt - 1) {  // never expected: keeps a corrupted id off the loads
+                atomicOr(A.err, JT_ERRBIT_STACK);
+                node = -1;
+            }
+            int act = 0;  // 1 push, 2 direct, 3 approx
+            float4 pay = make_float4(0.f, 0.f, 0.f, 0.f), pq0 = pay;
+            float2 pq1 = make_float2(0.f, 0.f);
+            int2 ch = make_int2(0, 0);
+            if (node >= 0) {
+                if (node >= leaf0) {
+                    float4 q = tpos[node - leaf0];
+                    float dx = jt_wrap(q.x - gcx, P.L, P.halfL);
+                    float dy = jt_wrap(q.y - gcy, P.L, P.halfL);
+                    float dz = jt_wrap(q.z - gcz, P.L, P.halfL);
+                    float gx = gap1(dx, ghx), gy = gap1(dy, ghy), gz = gap1(dz, ghz);
+                    if (gx * gx + gy * gy + gz * gz <= P.rc2) {
+                        act = 2;
+                        pay = make_float4(gcx + dx, gcy + dy, gcz + dz, 0.f);
+                    }
+                } else {
+                    float4 lo = T.bmin[node], hi = T.bmax[node];
+                    float nhx = 0.5f * (hi.x - lo.x), nhy = 0.5f * (hi.y - lo.y),
+                          nhz = 0.5f * (hi.z - lo.z);
+                    float dx = jt_wrap(0.5f * (hi.x + lo.x) - gcx, P.L, P.halfL);
+                    float dy = jt_wrap(0.5f * (hi.y + lo.y) - gcy, P.L, P.halfL);
+                    float dz = jt_wrap(0.5f * (hi.z + lo.z) - gcz, P.L, P.halfL);
+                    float gx = gap1(dx, ghx + nhx), gy = gap1(dy, ghy + nhy),
+                          gz = gap1(dz, ghz + nhz);
+                    if (gx * gx + gy * gy + gz * gz <= P.rc2) {
+                        float4 cm = T.com[node];
+                        float mx = jt_wrap(cm.x - gcx, P.L, P.halfL);
+                        float my = jt_wrap(cm.y - gcy, P.L, P.halfL);
+                        float mz = jt_wrap(cm.z - gcz, P.L, P.halfL);
+                        float ax = gap1(mx, ghx), ay = gap1(my, ghy), az = gap1(mz, ghz);
+                        float dm2 = ax * ax + ay * ay + az * az;
+                        float size = 2.0f * fmaxf(fmaxf(nhx, nhy), nhz);
+                        if (size * size < P.theta2 * dm2) {
+                            act = 3;
+                            pay = make_float4(gcx + mx, gcy + my, gcz + mz, cm.w);
+                            pq0 = T.quad0[node];
+                            pq1 = T.quad1[node];
+                        } else {
+                            act = 1;
+                            ch = T.child[node];
+                        }
+                    }
+                }
+            }
+            const unsigned mpush = __ballot_sync(0xffffffffu, act == 1);
+            const unsigned mdir = __ballot_sync(0xffffffffu, act == 2);
+            const unsigned mapp = __ballot_sync(0xffffffffu, act == 3);
+            if (act == 1) {
+                int at = sp + 2 * __popc(mpush & lt);
+                if (at + 1 < kStackCap) {
+                    S.stack[at] = ch.y;
+                    S.stack[at + 1] = ch.x;
+                } else {
+                    atomicOr(A.err, JT_ERRBIT_STACK);
+                }
+            } else if (act == 2) {
+                S.dsrc[nD + __popc(mdir & lt)] = pay;
+            } else if (act == 3) {
+                int at = nA + __popc(mapp & lt);
+                S.acom[at] = pay;
+                S.aq0[at] = pq0;
+                S.aq1[at] = pq1;
+            }
+            {
+                // lanes whose pair fitted wrote it; they are a prefix in lane order
+                int room = (kStackCap - sp) / 2;
+                int np = __popc(mpush);
+                sp += 2 * (np < room ? np : room);
+            }
+            nD += __popc(mdir);
+            nA += __popc(mapp);
+            __syncwarp();
+            while (nD >= 32) {
+                eval_direct(S.dsrc, 32, p.x, p.y, p.z, P, fac_direct, near);
+                inter += 32ull * nvalid;
+                __syncwarp();
+                float4 tmp = S.dsrc[32 + lane];
+                __syncwarp();
+                if (lane < nD - 32) S.dsrc[lane] = tmp;
+                nD -= 32;
+                __syncwarp();
+            }
+            while (nA >= 32) {
+                eval_approx(S.acom, S.aq0, S.aq1, 32, p.x, p.y, p.z, P, sgn, far, comp);
+                inter += 32ull * nvalid;
+                __syncwarp();
+                float4 t0 = S.acom[32 + lane], t1 = S.aq0[32 + lane];
+                float2 t2 = S.aq1[32 + lane];
+                __syncwarp();
+                if (lane < nA - 32) {
+                    S.acom[lane] = t0;
+                    S.aq0[lane] = t1;
+                    S.aq1[lane] = t2;
+                }
+                nA -= 32;
+                __syncwarp();
+            }
+        }
+        if (nD > 0) {
+            eval_direct(S.dsrc, nD, p.x, p.y, p.z, P, fac_direct, near);
+            inter += (unsigned long long)nD * nvalid;
+        }
+        if (nA > 0) {
+            eval_approx(S.acom, S.aq0, S.aq1, nA, p.x, p.y, p.z, P, sgn, far, comp);
+            inter += (unsigned long long)nA * nvalid;
+        }
+        __syncwarp();
+    }
+
+    if (valid) {
+        float ax = sgn_s * pm.x + near.x + (far.x - comp.x);
+        float ay = sgn_s * pm.y + near.y + (far.y - comp.y);
+        float az = sgn_s * pm.z + near.z + (far.z - comp.z);
+        A.acc[s][i] = make_float4(ax, ay, az, 0.f);
+        if (A.kick_dt != 0.0f) {
+            float4 v = A.vel[s][i];
+            v.x += (ax - A.kick_drag * v.x) * A.kick_dt;
+            v.y += (ay - A.kick_drag * v.y) * A.kick_dt;
+            v.z += (az - A.kick_drag * v.z) * A.kick_dt;
+            A.vel[s][i] = v;
+        }
+    }
+    if (lane == 0 && A.inter) atomicAdd(A.inter, inter);
+}
+
+// ------------------------------------------------------------------ RCOMPAT
+struct RcArgs {
+    jt_rc_params p;
+    const float4* pos;      // caller order, both species
+    const int8_t* sg;
+    int64_t n_all;
+    int64_t n[2];
+    jt_tree_dev tree[2];
+    const float* phi;
+    float4* acc;
+    unsigned* err;
+};
+
+__device__ __forceinline__ float rc_wrap(float d, float bh)
+{
+    if (d > bh) d = __fsub_rn(d, __fmul_rn(2.0f, bh));
+    if (d < -bh) d = __fadd_rn(d, __fmul_rn(2.0f, bh));
+    return d;
+}
+
+__global__ void __launch_bounds__(kWarps * 32) k_walk_rc(RcArgs A)
+{
+    __shared__ int stack_all[kWarps][128];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    int* stack = stack_all[wib];
+    const int64_t tid = ((int64_t)blockIdx.x * kWarps + wib) * 32 + lane;
+    const int64_t wbase = tid - lane;
+    if (wbase >= A.n_all) return;  // whole warp
+    const jt_rc_params& P = A.p;
+    const bool valid = tid < A.n_all;
+    const int64_t st = valid ? tid : 0;
+    const float4 p = A.pos[st];
+    const int my_sign = A.sg[st] > 0 ? 1 : -1;
+    float res[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+
+    for (int t = 0; t < 2; t++) {
+        const int64_t nt = A.n[t];
+        if (nt == 0) continue;
+        const jt_tree_dev T = A.tree[t];
+        const int tree_sign = t == 0 ? 1 : -1;
+        const float sf = (my_sign == tree_sign) ? 1.0f : -1.0f;
+        float ax = 0.f, ay = 0.f, az = 0.f;
+        int sp = 0;
+        if (lane == 0) stack[0] = 0;
+        sp = 1;
+        __syncwarp();
+        while (sp > 0) {
+            const int node = stack[sp - 1];
+            --sp;
+            __syncwarp();
+            const bool leaf = node >= nt - 1;
+            const float4 b = T.bmin[node];   // cx cy cz hs
+            const float4 cm = T.com[node];   // comx comy comz m
+            float dx = rc_wrap(__fsub_rn(b.x, p.x), P.box_half_q);
+            float dy = rc_wrap(__fsub_rn(b.y, p.y), P.box_half_q);
+            float dz = rc_wrap(__fsub_rn(b.z, p.z), P.box_half_q);
+            float r2 = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)),
+                                           __fmul_rn(dz, dz)), 1e-20f);
+            float r = __fsqrt_rn(r2);
+            bool beyond = __fsub_rn(r, b.w) > P.r_cut;
+            if (__all_sync(0xffffffffu, beyond)) continue;
+            bool approx = leaf || (__fmul_rn(__fmul_rn(4.0f, b.w), b.w) < __fmul_rn(P.theta2, r2));
+            if (__all_sync(0xffffffffu, approx)) {
+                if (valid) {
+                    float ddx = rc_wrap(__fsub_rn(cm.x, p.x), P.box_half_q);
+                    float ddy = rc_wrap(__fsub_rn(cm.y, p.y), P.box_half_q);
+                    float ddz = rc_wrap(__fsub_rn(cm.z, p.z), P.box_half_q);
+                    float rp2 = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)),
+                                                    __fmul_rn(ddz, ddz)), P.eps2);
+                    float rp = __fsqrt_rn(rp2);
+                    float arg = __fdiv_rn(rp, __fmul_rn(2.0f, P.r_s));
+                    float ef = erfcf(arg);
+                    if (ef > 1e-6f) {
+                        float irp3 = __fdiv_rn(1.0f, __fmul_rn(rp, rp2));
+                        float f = __fmul_rn(__fmul_rn(__fmul_rn(sf, cm.w), irp3), ef);
+                        ax = __fadd_rn(ax, __fmul_rn(f, ddx));
+                        ay = __fadd_rn(ay, __fmul_rn(f, ddy));
+                        az = __fadd_rn(az, __fmul_rn(f, ddz));
+                    }
+                }
+            } else {
+                // not every lane accepts (a leaf is always accepted): lane 0
+                // pushes right then left while sp < 127; sp is warp-uniform
+                int2 ch = T.child[node];
+                if (ch.y >= 0 && sp < 127) { if (lane == 0) stack[sp] = ch.y; ++sp; }
+                if (ch.x >= 0 && sp < 127) { if (lane == 0) stack[sp] = ch.x; ++sp; }
+            }
+            __syncwarp();
+        }
+        res[t][0] = ax; res[t][1] = ay; res[t][2] = az;
+    }
+
+    if (!valid) return;
+    // PM: central differences of the signed potential at the 8 CIC nodes
+    // (cic_gather, :162-257); F = -s grad(phi)
+    const int M = P.M;
+    float gx = __fmul_rn(__fadd_rn(p.x, P.box_half), P.inv_cell);
+    float gy = __fmul_rn(__fadd_rn(p.y, P.box_half), P.inv_cell);
+    float gz = __fmul_rn(__fadd_rn(p.z, P.box_half), P.inv_cell);
+    float Mf = (float)M;
+    gx = fmodf(__fadd_rn(gx, Mf), Mf);
+    gy = fmodf(__fadd_rn(gy, Mf), Mf);
+    gz = fmodf(__fadd_rn(gz, Mf), Mf);
+    int ix = (int)gx, iy = (int)gy, iz = (int)gz;
+    float fx = __fsub_rn(gx, (float)ix), fy = __fsub_rn(gy, (float)iy), fz = __fsub_rn(gz, (float)iz);
+    float wx[2] = {__fsub_rn(1.0f, fx), fx}, wy[2] = {__fsub_rn(1.0f, fy), fy},
+          wz[2] = {__fsub_rn(1.0f, fz), fz};
+    // positions outside the box (or NaN) still index inside the grid
+    ix = ((ix % M) + M) % M; iy = ((iy % M) + M) % M; iz = ((iz % M) + M) % M;
+    float inv_2h = __fdiv_rn(0.5f, P.cell);
+    float sgn = (float)my_sign;
+    float Fx = 0.f, Fy = 0.f, Fz = 0.f;
+    const float* phi = A.phi;
+#define RCIDX(a, b, c) ((int64_t)(a) + (int64_t)M * ((int64_t)(b) + (int64_t)M * (int64_t)(c)))
+    for (int di = 0; di < 2; di++)
+        for (int dj = 0; dj < 2; dj++)
+            for (int dk = 0; dk < 2; dk++) {
+                int ci = (ix + di) % M, cj = (iy + dj) % M, ck = (iz + dk) % M;
+                float w = __fmul_rn(__fmul_rn(wx[di], wy[dj]), wz[dk]);
+                int cip = (ci + 1) % M, cim = (ci + M - 1) % M;
+                int cjp = (cj + 1) % M, cjm = (cj + M - 1) % M;
+                int ckp = (ck + 1) % M, ckm = (ck + M - 1) % M;
+                float ddx = __fmul_rn(__fsub_rn(phi[RCIDX(cip, cj, ck)], phi[RCIDX(cim, cj, ck)]), inv_2h);
+                float ddy = __fmul_rn(__fsub_rn(phi[RCIDX(ci, cjp, ck)], phi[RCIDX(ci, cjm, ck)]), inv_2h);
+                float ddz = __fmul_rn(__fsub_rn(phi[RCIDX(ci, cj, ckp)], phi[RCIDX(ci, cj, ckm)]), inv_2h);
+                Fx = __fadd_rn(Fx, __fmul_rn(w, -__fmul_rn(sgn, ddx)));
+                Fy = __fadd_rn(Fy, __fmul_rn(w, -__fmul_rn(sgn, ddy)));
+                Fz = __fadd_rn(Fz, __fmul_rn(w, -__fmul_rn(sgn, ddz)));
+            }
+#undef RCIDX
+    // acc = (tree+ + tree-) + pm, the reference's accumulation order
+    float ax = __fadd_rn(__fadd_rn(res[0][0], res[1][0]), Fx);
+    float ay = __fadd_rn(__fadd_rn(res[0][1], res[1][1]), Fy);
+    float az = __fadd_rn(__fadd_rn(res[0][2], res[1][2]), Fz);
+    A.acc[tid] = make_float4(ax, ay, az, 0.f);
+}
+
+// ------------------------------------------------------------------ step kernels
+__global__ void k_kick(float4* __restrict__ vel, const float4* __restrict__ acc, int64_t n, float dt,
+                       float drag)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 v = vel[i], a = acc[i];
+    v.x += (a.x - drag * v.x) * dt;
+    v.y += (a.y - drag * v.y) * dt;
+    v.z += (a.z - drag * v.z) * dt;
+    vel[i] = v;
+}
+
+// drift with one periodic wrap (drift_f32, :33-48)
+__global__ void k_drift(float4* __restrict__ pos, const float4* __restrict__ vel, int64_t n, float dt,
+                        float L, float halfL)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 p = pos[i], v = vel[i];
+    p.x += v.x * dt;
+    p.y += v.y * dt;
+    p.z += v.z * dt;
+    p.x = p.x > halfL ? p.x - L : p.x;
+    p.x = p.x < -halfL ? p.x + L : p.x;
+    p.y = p.y > halfL ? p.y - L : p.y;
+    p.y = p.y < -halfL ? p.y + L : p.y;
+    p.z = p.z > halfL ? p.z - L : p.z;
+    p.z = p.z < -halfL ? p.z + L : p.z;
+    pos[i] = p;
+}
+
+__global__ void k_to_caller(const float4* __restrict__ src, const int* __restrict__ id,
+                            const int* __restrict__ gmap, int64_t n, float4* __restrict__ dst)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    dst[gmap[id[i]]] = src[i];
+}
+
+__global__ void k_aos_out(const float4* __restrict__ src, const int* __restrict__ id,
+                          const int* __restrict__ gmap, int64_t n, float* __restrict__ dst)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 v = src[i];
+    int64_t k = id ? id[i] : i;
+    if (gmap) k = gmap[k];
+    int64_t o = 3 * k;
+    dst[o] = v.x;
+    dst[o + 1] = v.y;
+    dst[o + 2] = v.z;
+}
+
+__global__ void k_from_caller(const float4* __restrict__ src, const int* __restrict__ id,
+                              const int* __restrict__ gmap, int64_t n, float4* __restrict__ dst)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    dst[i] = src[gmap[id[i]]];
+}
+
+__global__ void k_aos_in(const float* __restrict__ src, int64_t n, float4* __restrict__ dst,
+                         int* __restrict__ id)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    dst[i] = src ? make_float4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0.f)
+                 : make_float4(0.f, 0.f, 0.f, 0.f);
+    if (id) id[i] = (int)i;
+}
+
+__global__ void k_split_signed(const float* __restrict__ pos, const float* __restrict__ vel,
+                               const int8_t* __restrict__ sg, int64_t n, const int* __restrict__ rank,
+                               float4* pos_p, float4* vel_p, int* id_p, int* gmap_p, float4* pos_m,
+                               float4* vel_m, int* id_m, int* gmap_m)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int r = rank[i];
+    float4 p = make_float4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], 0.f);
+    float4 v = vel ? make_float4(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2], 0.f)
+                   : make_float4(0.f, 0.f, 0.f, 0.f);
+    if (sg[i] > 0) {
+        pos_p[r] = p; vel_p[r] = v; id_p[r] = r; gmap_p[r] = (int)i;
+    } else {
+        pos_m[r] = p; vel_m[r] = v; id_m[r] = r; gmap_m[r] = (int)i;
+    }
+}
+
+}  // namespace
+
+void jt_launch_walk_accurate(const jt_walk_params& p, const float4* const pos[2], const int64_t n[2],
+                             const jt_tree_dev tree[2], const float* force3, float4* const acc[2],
+                             float4* const vel[2], float kick_dt, float kick_drag,
+                             unsigned long long* inter, unsigned* d_err, cudaStream_t st)
+{
+    WalkArgs A;
+    A.p = p;
+    for (int s = 0; s < 2; s++) {
+        A.pos[s] = pos[s];
+        A.n[s] = n[s];
+        A.tree[s] = tree[s];
+        A.acc[s] = acc[s];
+        A.vel[s] = vel[s];
+    }
+    A.force3 = force3;
+    A.kick_dt = kick_dt;
+    A.kick_drag = kick_drag;
+    A.groups0 = (n[0] + 31) / 32;
+    A.groups1 = (n[1] + 31) / 32;
+    A.inter = inter;
+    A.err = d_err;
+    int64_t warps = A.groups0 + A.groups1;
+    if (warps == 0) return;
+    k_walk_acc<<<(unsigned)((warps + kWarps - 1) / kWarps), kWarps * 32, 0, st>>>(A);
+}
+
+void jt_launch_walk_rcompat(const jt_rc_params& p, const float4* pos_caller, const int8_t* sign_caller,
+                            int64_t n_all, const float4* const spos[2], const int64_t n[2],
+                            const jt_tree_dev tree[2], const float* phi, float4* acc_caller,
+                            unsigned* d_err, cudaStream_t st)
+{
+    (void)spos;
+    RcArgs A;
+    A.p = p;
+    A.pos = pos_caller;
+    A.sg = sign_caller;
+    A.n_all = n_all;
+    for (int s = 0; s < 2; s++) {
+        A.n[s] = n[s];
+        A.tree[s] = tree[s];
+    }
+    A.phi = phi;
+    A.acc = acc_caller;
+    A.err = d_err;
+    int64_t warps = (n_all + 31) / 32;
+    if (warps == 0) return;
+    k_walk_rc<<<(unsigned)((warps + kWarps - 1) / kWarps), kWarps * 32, 0, st>>>(A);
+}
+
+void jt_launch_kick(float4* vel, const float4* acc, int64_t n, float dt, float drag, cudaStream_t st)
+{
+    if (n <= 0) return;
+    k_kick<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(vel, acc, n, dt, drag);
+}
+
+void jt_launch_drift(float4* pos, const float4* vel, int64_t n, float dt, float L, float halfL,
+                     cudaStream_t st)
+{
+    if (n <= 0) return;
+    k_drift<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(pos, vel, n, dt, L, halfL);
+}
+
+void jt_launch_to_caller(const float4* src, const int* id, const int* gmap, int64_t n, float4* dst,
+                         cudaStream_t st)
+{
+    if (n <= 0) return;
+    k_to_caller<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(src, id, gmap, n, dst);
+}
+
+void jt_launch_aos_out(const float4* src, const int* id, const int* gmap, int64_t n, float* dst_aos,
+                       cudaStream_t st)
+{
+    if (n <= 0) return;
+    k_aos_out<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(src, id, gmap, n, dst_aos);
+}
+
+void jt_launch_from_caller(const float4* src_caller, const int* id, const int* gmap, int64_t n,
+                           float4* dst, cudaStream_t st)
+{
+    if (n <= 0) return;
+    k_from_caller<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(src_caller, id, gmap, n, dst);
+}
+
+void jt_launch_aos_in(const float* src_aos, int64_t n, float4* dst, int* id, cudaStream_t st)
+{
+    if (n <= 0) return;
+    k_aos_in<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(src_aos, n, dst, id);
+}
+
+void jt_launch_split_signed(const float* pos_aos, const float* vel_aos, const int8_t* sg, int64_t n,
+                            const int* rank, float4* pos_p, float4* vel_p, int* id_p, int* gmap_p,
+                            float4* pos_m, float4* vel_m, int* id_m, int* gmap_m, cudaStream_t st)
+{
+    if (n <= 0) return;
+    k_split_signed<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(pos_aos, vel_aos, sg, n, rank, pos_p,
+                                                                vel_p, id_p, gmap_p, pos_m, vel_m,
+                                                                id_m, gmap_m);
+}
+
+// ------------------------------------------------------------------ FP32 peak probe
+// Independent FMA chains (8 per thread) with no memory traffic: the FP32
+// roofline denominator of the walk, measured on the device it runs on.
+namespace {
+__global__ void k_fma_peak(float* out, int iters, float a, float b)
+{
+    float x0 = threadIdx.x * 1e-3f, x1 = x0 + 1.f, x2 = x0 + 2.f, x3 = x0 + 3.f;
+    float x4 = x0 + 4.f, x5 = x0 + 5.f, x6 = x0 + 6.f, x7 = x0 + 7.f;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+            x0 = fmaf(x0, a, b); x1 = fmaf(x1, a, b); x2 = fmaf(x2, a, b); x3 = fmaf(x3, a, b);
+            x4 = fmaf(x4, a, b); x5 = fmaf(x5, a, b); x6 = fmaf(x6, a, b); x7 = fmaf(x7, a, b);
+        }
+    }
+    float s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+    if (s == 1.2345f) out[0] = s;  // keeps the chains alive
+}
+}  // namespace
+
+extern "C" int jt_fp32_peak(int iters, double* tflops)
+{
+    if (!tflops || iters <= 0) return JT_EINVAL;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return JT_ECUDA;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    float* out = nullptr;
+    if (cudaMalloc(&out, sizeof(float)) != cudaSuccess) return JT_ENOMEM;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    dim3 grid(sms * 8), block(256);
+    k_fma_peak<<<grid, block>>>(out, 16, 0.9999f, 1e-4f);  // warm-up
+    cudaEventRecord(e0);
+    k_fma_peak<<<grid, block>>>(out, iters, 0.9999f, 1e-4f);
+    cudaEventRecord(e1);
+    cudaError_t err = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    if (err != cudaSuccess || ms <= 0.f) return JT_ECUDA;
+    double flops = 2.0 * 8.0 * 16.0 * (double)iters * grid.x * block.x;
+    *tflops = flops / (ms * 1e-3) / 1e12;
+    return JT_OK;
+}

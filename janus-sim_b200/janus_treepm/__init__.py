@@ -1,0 +1,418 @@
+"""Host-side mirror of the janus-sim TreePM interface over the B200 engine.
+
+The engine is libjanus_treepm.so (CUDA for sm_100a, built in-tree by
+`make -C janus-sim_b200`); this module binds its C ABI (include/janus_treepm.h)
+with ctypes and offers the reference's two call shapes:
+
+* ``GpuNBodyTwoPass`` -- src/nbody_gpu_twopass.rs: ``with_custom_ics(pos, vel,
+  signs, box_size)``, ``set_theta``, ``set_softening``, ``set_mass_factor``,
+  ``set_pm_k_min``, ``step_treepm_gpu(dt, r_cut, hubble, dtau_per_dt)``,
+  ``compute_forces()``, ``get_particles()``.
+* ``TreePMForce`` -- src/treepm/treepm_force.rs: ``TreePMForce(r_cut,
+  grid_size, box_size, theta, softening)``, ``update(particles)``,
+  ``compute_all_forces(particles)``.
+
+Errors raise ``JanusError`` carrying the library's negative code (the
+reference returns ``Result<_, Box<dyn Error>>``).  There is no CPU fallback:
+if the library is missing or no CUDA device is present, every call raises.
+"""
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG_ROOT = os.path.dirname(HERE)
+LIB_PATH = os.path.join(PKG_ROOT, "libjanus_treepm.so")
+
+JT_OK, JT_EINVAL, JT_ENOMEM, JT_ECUDA, JT_ETIMEDOUT = 0, -1, -2, -3, -4
+JT_ENOTIMPL, JT_ESTATE, JT_EOVERFLOW, JT_EBUSY = -5, -6, -7, -8
+JT_MEM_HOST, JT_MEM_DEVICE = 0, 1
+JT_ACCURATE, JT_RCOMPAT = 0, 1
+JT_KDK, JT_DKD_REF = 0, 1
+
+EXPORTED = [
+    "jt_create", "jt_set_state", "jt_set_state_signed", "jt_accel", "jt_accel_signed",
+    "jt_step", "jt_get_state", "jt_get_state_signed", "jt_debug_tree", "jt_get_timings",
+    "jt_counts", "jt_destroy", "jt_strerror", "jt_version", "jt_fp32_peak",
+]
+
+
+class JanusError(RuntimeError):
+    def __init__(self, code, what=""):
+        self.code = code
+        msg = _strerror(code)
+        super().__init__(f"{what}: {msg} ({code})" if what else f"{msg} ({code})")
+
+
+class jt_config(C.Structure):
+    _fields_ = [
+        ("box_L", C.c_double), ("pm_grid", C.c_int), ("theta", C.c_double),
+        ("softening", C.c_double), ("r_s", C.c_double), ("r_cut", C.c_double),
+        ("mu", C.c_double), ("G_mass_plus", C.c_double), ("k_min", C.c_int),
+        ("mode", C.c_int), ("integrator", C.c_int), ("reserved", C.c_int * 5),
+    ]
+
+
+class jt_timings(C.Structure):
+    _fields_ = [
+        ("sort_ms", C.c_double), ("tree_ms", C.c_double), ("deposit_ms", C.c_double),
+        ("fft_ms", C.c_double), ("kspace_ms", C.c_double), ("walk_ms", C.c_double),
+        ("kick_drift_ms", C.c_double), ("total_ms", C.c_double),
+        ("interactions", C.c_int64), ("launches", C.c_int64),
+    ]
+
+
+_lib = None
+
+
+def library():
+    """Load libjanus_treepm.so (raises if it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} not built: run `make -C janus-sim_b200`")
+    L = C.CDLL(LIB_PATH)
+    vp, fp, i8p = C.c_void_p, C.c_void_p, C.c_void_p
+    H = C.c_void_p
+    L.jt_create.argtypes = [C.POINTER(jt_config), C.POINTER(H)]
+    L.jt_set_state.argtypes = [H, fp, fp, C.c_size_t, fp, fp, C.c_size_t, C.c_int]
+    L.jt_set_state_signed.argtypes = [H, fp, fp, i8p, C.c_size_t, C.c_int]
+    L.jt_accel.argtypes = [H, fp, fp, C.c_int]
+    L.jt_accel_signed.argtypes = [H, fp, C.c_int]
+    L.jt_step.argtypes = [H, C.c_double, C.c_double, C.c_double, C.c_int]
+    L.jt_get_state.argtypes = [H, fp, fp, fp, fp, C.c_int]
+    L.jt_get_state_signed.argtypes = [H, fp, fp, C.c_int]
+    L.jt_debug_tree.argtypes = [H, C.c_int, vp, vp, vp, vp, vp]
+    L.jt_get_timings.argtypes = [H, C.POINTER(jt_timings)]
+    L.jt_counts.argtypes = [H, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]
+    L.jt_destroy.argtypes = [H]
+    L.jt_destroy.restype = None
+    L.jt_strerror.argtypes = [C.c_int]
+    L.jt_strerror.restype = C.c_char_p
+    L.jt_fp32_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
+    L.jt_version.argtypes = []
+    L.jt_version.restype = C.c_char_p
+    for name in EXPORTED:
+        if name not in ("jt_destroy", "jt_strerror", "jt_version"):
+            getattr(L, name).restype = C.c_int
+    _lib = L
+    return L
+
+
+def _strerror(code):
+    try:
+        return library().jt_strerror(code).decode()
+    except Exception:
+        return "error"
+
+
+def _check(code, what):
+    if code != JT_OK:
+        raise JanusError(code, what)
+
+
+def _f32(a, n3=True):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if n3:
+        a = a.reshape(-1, 3)
+    return a
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+@dataclass
+class Config:
+    """Solver configuration (the fields of jt_config)."""
+    box_L: float
+    pm_grid: int
+    theta: float = 0.5
+    softening: float = 0.1
+    r_s: float = 0.0            # 0 -> 1.25 PM cells
+    r_cut: float = 0.0          # 0 -> 4.5 r_s
+    mu: float = 1.0             # M- / M+
+    G_mass_plus: float = 1.0    # G * mass of one m+ particle
+    k_min: int = 0
+    mode: int = JT_ACCURATE
+    integrator: int = JT_KDK
+
+    def resolved(self):
+        c = Config(**self.__dict__)
+        if c.r_s <= 0:
+            c.r_s = 1.25 * c.box_L / c.pm_grid
+        if c.r_cut <= 0:
+            c.r_cut = 4.5 * c.r_s
+        return c
+
+    def to_c(self):
+        c = self.resolved()
+        s = jt_config()
+        s.box_L, s.pm_grid, s.theta, s.softening = c.box_L, c.pm_grid, c.theta, c.softening
+        s.r_s, s.r_cut, s.mu, s.G_mass_plus = c.r_s, c.r_cut, c.mu, c.G_mass_plus
+        s.k_min, s.mode, s.integrator = c.k_min, c.mode, c.integrator
+        return s
+
+
+class Solver:
+    """One simulation box on the current CUDA device (a jt_handle)."""
+
+    def __init__(self, config: Config):
+        self.config = config.resolved()
+        self._h = C.c_void_p()
+        cfg = self.config.to_c()
+        _check(library().jt_create(C.byref(cfg), C.byref(self._h)), "jt_create")
+        self._signed = False
+        self.n = (0, 0)
+
+    def close(self):
+        if self._h:
+            library().jt_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- state
+    def set_state(self, pos_p, vel_p, pos_m, vel_m):
+        pos_p = _f32(pos_p) if pos_p is not None else np.zeros((0, 3), np.float32)
+        pos_m = _f32(pos_m) if pos_m is not None else np.zeros((0, 3), np.float32)
+        vel_p = None if vel_p is None else _f32(vel_p)
+        vel_m = None if vel_m is None else _f32(vel_m)
+        _check(library().jt_set_state(self._h, _ptr(pos_p), _ptr(vel_p), len(pos_p), _ptr(pos_m),
+                                      _ptr(vel_m), len(pos_m), JT_MEM_HOST), "jt_set_state")
+        self._signed = False
+        self.n = (len(pos_p), len(pos_m))
+
+    def set_state_signed(self, pos, vel, signs):
+        pos = _f32(pos)
+        vel = None if vel is None else _f32(vel)
+        signs = np.ascontiguousarray(signs, dtype=np.int8)
+        _check(library().jt_set_state_signed(self._h, _ptr(pos), _ptr(vel), _ptr(signs), len(pos),
+                                             JT_MEM_HOST), "jt_set_state_signed")
+        self._signed = True
+        n_p = int((signs > 0).sum())
+        self.n = (n_p, len(signs) - n_p)
+
+    def set_state_device(self, pos_p, vel_p, pos_m, vel_m):
+        """Device (torch CUDA float32 (n,3) contiguous) tensors; vel may be None."""
+        def dp(t):
+            return None if t is None else C.c_void_p(t.data_ptr())
+        n_p = 0 if pos_p is None else pos_p.shape[0]
+        n_m = 0 if pos_m is None else pos_m.shape[0]
+        _check(library().jt_set_state(self._h, dp(pos_p), dp(vel_p), n_p, dp(pos_m), dp(vel_m),
+                                      n_m, JT_MEM_DEVICE), "jt_set_state")
+        self._signed = False
+        self.n = (n_p, n_m)
+
+    def accel(self):
+        """Accelerations (acc_p (n+,3), acc_m (n-,3)) or, after set_state_signed, one array."""
+        if self._signed:
+            out = np.zeros((sum(self.n), 3), np.float32)
+            _check(library().jt_accel_signed(self._h, _ptr(out), JT_MEM_HOST), "jt_accel_signed")
+            return out
+        ap = np.zeros((self.n[0], 3), np.float32)
+        am = np.zeros((self.n[1], 3), np.float32)
+        _check(library().jt_accel(self._h, _ptr(ap), _ptr(am), JT_MEM_HOST), "jt_accel")
+        return ap, am
+
+    def accel_device(self, acc_p, acc_m):
+        def dp(t):
+            return None if t is None else C.c_void_p(t.data_ptr())
+        _check(library().jt_accel(self._h, dp(acc_p), dp(acc_m), JT_MEM_DEVICE), "jt_accel")
+
+    def step(self, dt, hubble=0.0, dtau_per_dt=1.0, nsteps=1):
+        _check(library().jt_step(self._h, dt, hubble, dtau_per_dt, nsteps), "jt_step")
+
+    def get_state(self):
+        if self._signed:
+            pos = np.zeros((sum(self.n), 3), np.float32)
+            vel = np.zeros((sum(self.n), 3), np.float32)
+            _check(library().jt_get_state_signed(self._h, _ptr(pos), _ptr(vel), JT_MEM_HOST),
+                   "jt_get_state_signed")
+            return pos, vel
+        pp = np.zeros((self.n[0], 3), np.float32)
+        vp = np.zeros((self.n[0], 3), np.float32)
+        pm = np.zeros((self.n[1], 3), np.float32)
+        vm = np.zeros((self.n[1], 3), np.float32)
+        _check(library().jt_get_state(self._h, _ptr(pp), _ptr(vp), _ptr(pm), _ptr(vm), JT_MEM_HOST),
+               "jt_get_state")
+        return pp, vp, pm, vm
+
+    def debug_tree(self, species):
+        n = self.n[species]
+        nn = max(2 * n - 1, 1)
+        morton = np.zeros(max(n, 1), np.uint32)
+        perm = np.zeros(max(n, 1), np.int32)
+        left = np.zeros(nn, np.int32)
+        right = np.zeros(nn, np.int32)
+        parent = np.zeros(nn, np.int32)
+        _check(library().jt_debug_tree(self._h, species, _ptr(morton), _ptr(perm), _ptr(left),
+                                       _ptr(right), _ptr(parent)), "jt_debug_tree")
+        return dict(morton=morton[:n], perm=perm[:n], left=left, right=right, parent=parent)
+
+    def timings(self):
+        t = jt_timings()
+        _check(library().jt_get_timings(self._h, C.byref(t)), "jt_get_timings")
+        return {k: getattr(t, k) for k, _ in jt_timings._fields_}
+
+
+# --------------------------------------------------------------------------
+# The reference's call shapes
+# --------------------------------------------------------------------------
+class GpuNBodyTwoPass:
+    """src/nbody_gpu_twopass.rs GpuNBodyTwoPass over the B200 engine.
+
+    Defaults follow with_custom_ics (:2303-2336): theta 0.5, softening 0.1,
+    pm_grid 256, k_min 0, mass_factor = G_cosmo * 0.3 * rho_crit * L^3 / N
+    (:2320-2330).  Forces use the reference formulas (RCOMPAT) unless
+    ``mode=JT_ACCURATE`` is passed; the step is the reference's
+    drift-kick-drift (JT_DKD_REF) unless ``integrator=JT_KDK``.
+    """
+
+    def __init__(self, pos, vel, signs, box_size, mode=JT_RCOMPAT, integrator=JT_DKD_REF,
+                 pm_grid=256):
+        pos = _f32(pos)
+        n = len(pos)
+        self.box_size = float(box_size)
+        self.theta = 0.5
+        self.softening = 0.1
+        self.pm_grid = pm_grid
+        self.pm_k_min = 0
+        g_cosmo, rho_crit, omega_m = 4.499e-15, 2.775e11, 0.3
+        self.mass_factor = g_cosmo * omega_m * rho_crit * self.box_size ** 3 / n
+        self.mode = mode
+        self.integrator = integrator
+        self._pos = pos
+        self._vel = None if vel is None else _f32(vel)
+        self._signs = np.ascontiguousarray(signs, dtype=np.int8)
+        self._solver = None
+        self._r_cut = None
+        self._dirty_state = True
+
+    @classmethod
+    def with_custom_ics(cls, pos, vel, signs, box_size, **kw):
+        return cls(pos, vel, signs, box_size, **kw)
+
+    def set_theta(self, t):
+        self._sync_state()
+        self.theta = float(t)
+        self._solver = None
+
+    def set_softening(self, e):
+        self._sync_state()
+        self.softening = float(e)
+        self._solver = None
+
+    def set_mass_factor(self, mf):
+        self._sync_state()
+        self.mass_factor = float(mf)
+        self._solver = None
+
+    def set_pm_k_min(self, k):
+        self._sync_state()
+        self.pm_k_min = int(k)
+        self._solver = None
+
+    def _sync_state(self):
+        if self._solver is not None:
+            self._pos, self._vel = self._solver.get_state()
+
+    def _ensure(self, r_cut):
+        if self._solver is not None and self._r_cut == r_cut:
+            return
+        self._sync_state()
+        n_p = int((self._signs > 0).sum())
+        n_m = len(self._signs) - n_p
+        mu = (n_m / n_p) if n_p else 1.0   # equal per-particle mass = mass_factor
+        cfg = Config(box_L=self.box_size, pm_grid=self.pm_grid, theta=self.theta,
+                     softening=self.softening, r_s=r_cut / 3.0, r_cut=r_cut, mu=mu,
+                     G_mass_plus=self.mass_factor, k_min=self.pm_k_min, mode=self.mode,
+                     integrator=self.integrator)
+        self._solver = Solver(cfg)
+        self._solver.set_state_signed(self._pos, self._vel, self._signs)
+        self._r_cut = r_cut
+
+    def compute_forces(self, r_cut):
+        """Accelerations of all particles in the with_custom_ics order."""
+        self._ensure(r_cut)
+        return self._solver.accel()
+
+    def step_treepm_gpu(self, dt, r_cut, hubble, dtau_per_dt):
+        self._ensure(r_cut)
+        self._solver.step(dt, hubble, dtau_per_dt, 1)
+
+    def get_particles(self):
+        """(pos, vel, signs) in the with_custom_ics order."""
+        self._sync_state()
+        vel = self._vel if self._vel is not None else np.zeros_like(self._pos)
+        return self._pos.copy(), vel.copy(), self._signs.copy()
+
+
+@dataclass
+class Particle:
+    """src/nbody.rs Particle {pos, vel, mass, sign} (sign +1 / -1)."""
+    pos: tuple
+    vel: tuple = (0.0, 0.0, 0.0)
+    mass: float = 1.0
+    sign: int = 1
+
+
+class TreePMForce:
+    """src/treepm/treepm_force.rs TreePMForce over the B200 engine.
+
+    new(r_cut, grid_size, box_size, theta, softening); r_s = r_cut / 3 and G = 1
+    as in the reference (:35-49).  Each species' particles must share one mass
+    (the engine stores one mass per species).  Positions in [-L/2, L/2).
+    """
+
+    def __init__(self, r_cut, grid_size, box_size, theta, softening, mode=JT_ACCURATE):
+        self.r_cut = float(r_cut)
+        self.r_s = self.r_cut / 3.0
+        self.grid_size = int(grid_size)
+        self.box_size = float(box_size)
+        self.theta = float(theta)
+        self.softening = float(softening)
+        self.g_constant = 1.0
+        self.mode = mode
+        self._solver = None
+        self._order = None
+
+    def update(self, particles):
+        pos = np.array([p.pos for p in particles], np.float64).reshape(-1, 3)
+        sg = np.array([1 if p.sign > 0 else -1 for p in particles], np.int8)
+        mass = np.array([abs(p.mass) for p in particles], np.float64)
+        mp = mass[sg > 0]
+        mm = mass[sg < 0]
+        if (len(mp) and np.ptp(mp) > 1e-12 * mp.max()) or (len(mm) and np.ptp(mm) > 1e-12 * mm.max()):
+            raise JanusError(JT_EINVAL, "TreePMForce.update: one mass per species")
+        m_plus = float(mp[0]) if len(mp) else 1.0
+        m_minus = float(mm[0]) if len(mm) else m_plus
+        mu = (m_minus * len(mm)) / (m_plus * len(mp)) if len(mp) else m_minus / m_plus
+        cfg = Config(box_L=self.box_size, pm_grid=self.grid_size, theta=self.theta,
+                     softening=self.softening, r_s=self.r_s, r_cut=self.r_cut, mu=mu,
+                     G_mass_plus=self.g_constant * m_plus, mode=self.mode)
+        self._solver = Solver(cfg)
+        self._solver.set_state_signed(pos.astype(np.float32), None, sg)
+
+    def compute_all_forces(self, particles=None):
+        if self._solver is None:
+            raise JanusError(JT_ESTATE, "TreePMForce.compute_all_forces before update")
+        return self._solver.accel().astype(np.float64)
+
+
+def version():
+    return library().jt_version().decode()
+
+
+def fp32_peak_tflops(iters=4096):
+    """Measured FP32 FMA throughput of the current device."""
+    v = C.c_double()
+    _check(library().jt_fp32_peak(iters, C.byref(v)), "jt_fp32_peak")
+    return v.value

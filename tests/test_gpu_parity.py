@@ -1,0 +1,168 @@
+"""GPU parity through the C ABI (janus-sim_b200/libjanus_treepm.so).
+
+Bars:
+  * Morton codes, sort permutation and LBVH topology: bit-exact against the
+    oracle restatement of the reference build (pinned to the reference's own
+    kernels in tests/test_oracle.py);
+  * compatibility-mode accelerations against the oracle restatement of the
+    reference's GPU forces: p99 relative error <= 1e-5 (the engine evaluates
+    the same float expressions; the PM runs in FP32 where the reference runs
+    FP64, and CUDA's erfcf differs from the host's by an ulp);
+  * accurate-mode accelerations against the FP64 exact split-model sum (same
+    r_s, softening and r_cut, no grid, no tree): p99 relative error <= 2e-3
+    and median <= 3e-4 at theta = 0.5 (the remaining error is the PM grid's
+    and the tree's);
+  * the m- response is the exact sign flip of the m+ response (bitwise).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _mods():
+    import janus_treepm as J
+    import oracle as O
+    return J, O
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b, axis=1) / np.maximum(np.linalg.norm(b, axis=1), 1e-30)
+
+
+def _uniform(n, L, seed):
+    rng = np.random.default_rng(seed)
+    return ((rng.random((n, 3)) - 0.5) * L).astype(np.float32)
+
+
+@pytest.mark.parametrize("n_p,n_m,collide", [(5000, 3001, False), (4096, 4096, True),
+                                             (1, 2, False), (33, 0, False)])
+def test_tree_topology_bitexact(n_p, n_m, collide):
+    J, O = _mods()
+    L = 64.0
+    pp = _uniform(n_p, L, 1)
+    pm = _uniform(n_m, L, 2)
+    if collide:
+        # many particles per 10-bit Morton cell: exercises the index tie-break
+        cell = L / 1024
+        pp = ((np.floor(pp / (128 * cell)) + 0.3) * 128 * cell).astype(np.float32)
+        pm = ((np.floor(pm / (128 * cell)) + 0.6) * 128 * cell).astype(np.float32)
+    s = J.Solver(J.Config(box_L=L, pm_grid=32, mode=J.JT_ACCURATE))
+    s.set_state(pp, None, pm if n_m else None, None)
+    for sp, pos in ((0, pp), (1, pm)):
+        n = len(pos)
+        if n == 0:
+            continue
+        got = s.debug_tree(sp)
+        ref = O.build_tree(pos, np.float32(L / 2), 1.0)
+        assert np.array_equal(got["morton"], ref["m30"])
+        assert np.array_equal(got["perm"], ref["perm"])
+        if n > 1:
+            assert np.array_equal(got["left"][:n - 1], ref["left"][:n - 1])
+            assert np.array_equal(got["right"][:n - 1], ref["right"][:n - 1])
+        assert np.array_equal(got["parent"][:2 * n - 1], ref["parent"][:2 * n - 1])
+    s.close()
+
+
+@pytest.mark.parametrize("n,M,L,interleave", [(2048, 32, 64.0, False), (3000, 32, 50.0, True)])
+def test_rcompat_matches_reference_forces(n, M, L, interleave):
+    J, O = _mods()
+    rng = np.random.default_rng(7)
+    pos = _uniform(n, L, 3)
+    if interleave:
+        sg = np.where(rng.random(n) < 0.4, 1, -1).astype(np.int8)
+    else:
+        sg = np.concatenate([np.ones(n // 2, np.int8), -np.ones(n - n // 2, np.int8)])
+    theta, eps, r_cut, mf = 0.5, 0.052913, 5.625, 0.01
+    s = J.Solver(J.Config(box_L=L, pm_grid=M, theta=theta, softening=eps, r_s=r_cut / 3,
+                          r_cut=r_cut, mu=(sg < 0).sum() / (sg > 0).sum(), G_mass_plus=mf,
+                          mode=J.JT_RCOMPAT))
+    s.set_state_signed(pos, None, sg)
+    got = s.accel()
+    ref = O.ref_total_forces(pos, sg, M, L, theta, eps, r_cut, mf)
+    rel = _rel(got, ref)
+    assert np.percentile(rel, 99) <= 1e-5, np.percentile(rel, [50, 99, 100])
+    assert rel.max() <= 1e-3
+    s.close()
+
+
+@pytest.mark.parametrize("n,M,L,mu", [(4096, 32, 32.0, 19.0), (8192, 64, 64.0, 1.0)])
+def test_accurate_matches_exact_split_model(n, M, L, mu):
+    J, O = _mods()
+    pp = _uniform(n, L, 11)
+    pm = _uniform(n, L, 12)
+    r_s = 1.25 * L / M
+    r_cut = 4.5 * r_s
+    eps = (L / (2 * n) ** (1 / 3)) / 30
+    s = J.Solver(J.Config(box_L=L, pm_grid=M, theta=0.5, softening=eps, r_s=r_s, r_cut=r_cut,
+                          mu=mu, G_mass_plus=1.0, mode=J.JT_ACCURATE))
+    s.set_state(pp, None, pm, None)
+    ap, am = s.accel()
+    pos = np.concatenate([pp, pm]).astype(np.float64)
+    mass = np.concatenate([np.full(n, 1.0), np.full(n, mu)])
+    sg = np.concatenate([np.ones(n, np.int8), -np.ones(n, np.int8)])
+    ex = O.ewald_forces(pos, mass, sg, L, r_s, eps, r_trunc=r_cut)
+    rel = _rel(np.concatenate([ap, am]), ex)
+    p50, p99 = np.percentile(rel, [50, 99])
+    assert p99 <= 2e-3 and p50 <= 3e-4, (p50, p99)
+    s.close()
+
+
+def test_minus_response_is_exact_sign_flip():
+    J, O = _mods()
+    n, L = 3000, 40.0
+    pp = _uniform(n, L, 5)
+    s = J.Solver(J.Config(box_L=L, pm_grid=32, mu=1.0, mode=J.JT_ACCURATE))
+    s.set_state(pp, None, pp.copy(), None)
+    ap, am = s.accel()
+    assert np.array_equal(am, -ap)
+    s.close()
+
+
+def test_kdk_steps_repeat_within_rounding():
+    """Three KDK steps twice from the same state agree to FP32 rounding (the
+    deposit sums with float atomics, whose order varies run to run)."""
+    J, O = _mods()
+    n, L, mu = 4096, 32.0, 3.0
+    pp = _uniform(n, L, 21)
+    pm = _uniform(n, L, 22)
+    s = J.Solver(J.Config(box_L=L, pm_grid=32, mu=mu, G_mass_plus=1e-3, mode=J.JT_ACCURATE))
+    s.set_state(pp, None, pm, None)
+    s.step(0.01, 0.0, 1.0, 3)
+    a1 = s.get_state()
+    s.set_state(pp, None, pm, None)
+    s.step(0.01, 0.0, 1.0, 3)
+    a2 = s.get_state()
+    for x, y in zip(a1, a2):
+        assert np.isfinite(x).all()
+        assert np.abs(x - y).max() <= 1e-5 * max(np.abs(y).max(), 1e-12)
+    s.close()
+
+
+def test_kdk_matches_host_integration_of_device_forces():
+    """One KDK step equals kick/drift applied on the host to jt_accel's
+    accelerations (v += a dt/2; x += v dt; wrap; v += a' dt/2)."""
+    J, O = _mods()
+    n, L, dt, H = 2048, 32.0, 0.02, 0.1
+    pp = _uniform(n, L, 31)
+    pm = _uniform(n, L, 32)
+    rng = np.random.default_rng(3)
+    vp = (rng.standard_normal((n, 3)) * 0.5).astype(np.float32)
+    vm = (rng.standard_normal((n, 3)) * 0.5).astype(np.float32)
+    s = J.Solver(J.Config(box_L=L, pm_grid=32, mu=2.0, G_mass_plus=1e-2, mode=J.JT_ACCURATE))
+    s.set_state(pp, vp, pm, vm)
+    a0p, a0m = s.accel()
+    half = lambda v, a: v + (a - H * v) * (dt / 2)
+    wrap = lambda x: np.where(x > L / 2, x - L, np.where(x < -L / 2, x + L, x))
+    v1p, v1m = half(vp, a0p), half(vm, a0m)
+    x1p, x1m = wrap(pp + v1p * dt), wrap(pm + v1m * dt)
+    s.step(dt, H, 1.0, 1)
+    gp, gvp, gm, gvm = s.get_state()
+    assert np.abs(gp - x1p).max() < 1e-4
+    s2 = J.Solver(J.Config(box_L=L, pm_grid=32, mu=2.0, G_mass_plus=1e-2, mode=J.JT_ACCURATE))
+    s2.set_state(x1p, None, x1m, None)
+    a1p, a1m = s2.accel()
+    assert np.abs(gvp - half(v1p, a1p)).max() < 1e-4 * max(1.0, np.abs(gvp).max())
+    assert np.abs(gvm - half(v1m, a1m)).max() < 1e-4 * max(1.0, np.abs(gvm).max())
+    s.close()
+    s2.close()
