@@ -77,7 +77,14 @@ typedef struct jt_config {
     int    k_min;        /* zero modes with max(|kx|,|ky|,|kz|) < k_min; 0 = off */
     int    mode;         /* JT_ACCURATE | JT_RCOMPAT */
     int    integrator;   /* JT_KDK | JT_DKD_REF */
-    int    reserved[5];  /* zero */
+    /* ACCURATE mass assignment: 0 = default (TSC), 2 = CIC, 3 = TSC.  CIC at
+     * r_s = 1.25 cells leaves ~1e-2 relative long-range force errors (FP64
+     * oracle); TSC with interlacing reaches ~5e-4 at p99. */
+    int    pm_order;
+    /* ACCURATE interlacing (second grid shifted by half a cell, odd aliases
+     * cancel): 0 = default (on), 1 = on, 2 = off. */
+    int    pm_interlace;
+    int    reserved[3];  /* zero */
 } jt_config;
 
 typedef struct jt_handle jt_handle;
@@ -93,8 +100,11 @@ typedef struct jt_timings {
     double walk_ms;      /* PM interpolation + short-range walk (+ kick) */
     double kick_drift_ms;/* kick/drift kernels outside the walk */
     double total_ms;     /* whole call */
-    int64_t interactions;/* pair + node interactions counted by the walk */
-    int64_t launches;    /* kernels launched by the library (incl. cuFFT's) */
+    int64_t interactions;/* pair + node interactions evaluated by the walk */
+    int64_t launches;    /* kernels launched by the library (cuFFT's not counted) */
+    int64_t pair_interactions;  /* particle pairs inside r_cut */
+    int64_t node_interactions;  /* multipole node interactions */
+    int64_t candidates;         /* particle candidates distance-tested */
 } jt_timings;
 
 /* Create a handle on the current CUDA device.  Replaces the constructor and
@@ -124,6 +134,13 @@ int  jt_set_state_signed(jt_handle* h, const float* pos, const float* vel,
 int  jt_accel(jt_handle* h, float* acc_p, float* acc_m, int mem);
 /* Same, for a state loaded with jt_set_state_signed: acc in that order. */
 int  jt_accel_signed(jt_handle* h, float* acc, int mem);
+/* One part of the acceleration: JT_PART_PM (long range only, the reference's
+ * pm_only mode, TreePMForce::new_pm_only src/treepm/treepm_force.rs:52-63),
+ * JT_PART_SHORT (tree only), JT_PART_ALL (= jt_accel).  Per-species output. */
+#define JT_PART_ALL    3
+#define JT_PART_PM     1
+#define JT_PART_SHORT  2
+int  jt_accel_part(jt_handle* h, int part, float* acc_p, float* acc_m, int mem);
 
 /* Advance nsteps steps of length dt.  Kick: v += (a - H v dtau_per_dt) dt,
  * the reference's kick_f32 (:50-64) with hubble = H; drift x += v dt with

@@ -45,7 +45,7 @@ struct jt_handle {
     void* stage = nullptr;
     size_t stage_bytes = 0;
     unsigned* d_err = nullptr;
-    unsigned long long* d_inter = nullptr;
+    unsigned long long* d_stats = nullptr;   // pairs, nodes, candidates
     jt_timings tm = {};
     int64_t launches_per_force = 0;
 };
@@ -99,6 +99,8 @@ int validate(const jt_config* c)
     if (c->k_min < 0) return JT_EINVAL;
     if (c->mode != JT_ACCURATE && c->mode != JT_RCOMPAT) return JT_EINVAL;
     if (c->integrator != JT_KDK && c->integrator != JT_DKD_REF) return JT_EINVAL;
+    if (c->pm_order != 0 && c->pm_order != 2 && c->pm_order != 3) return JT_EINVAL;
+    if (c->pm_interlace < 0 || c->pm_interlace > 2) return JT_EINVAL;
     return JT_OK;
 }
 
@@ -109,7 +111,7 @@ void free_particles(jt_handle* h)
         dfree(h->pos_b[s]); dfree(h->vel_b[s]);
         dfree(h->id[s]); dfree(h->id_b[s]); dfree(h->gmap[s]);
         jt_tree_dev& t = h->tree[s];
-        dfree(t.child); dfree(t.parent); dfree(t.flag); dfree(t.com); dfree(t.bmin);
+        dfree(t.child); dfree(t.range); dfree(t.parent); dfree(t.flag); dfree(t.com); dfree(t.bmin);
         dfree(t.bmax); dfree(t.quad0); dfree(t.quad1); dfree(t.m30); dfree(t.tie);
         t = jt_tree_dev{};
         h->cap[s] = 0;
@@ -134,6 +136,7 @@ int alloc_particles(jt_handle* h, int64_t n0, int64_t n1)
         JT_TRY(dalloc(&h->id[s], n)); JT_TRY(dalloc(&h->id_b[s], n)); JT_TRY(dalloc(&h->gmap[s], n));
         jt_tree_dev& t = h->tree[s];
         JT_TRY(dalloc(&t.child, nodes)); JT_TRY(dalloc(&t.parent, nodes));
+        JT_TRY(dalloc(&t.range, n > 1 ? n - 1 : 1));
         JT_TRY(dalloc(&t.flag, n > 1 ? n - 1 : 1));
         JT_TRY(dalloc(&t.com, nodes)); JT_TRY(dalloc(&t.bmin, nodes)); JT_TRY(dalloc(&t.bmax, nodes));
         JT_TRY(dalloc(&t.quad0, nodes)); JT_TRY(dalloc(&t.quad1, nodes));
@@ -155,39 +158,53 @@ int alloc_particles(jt_handle* h, int64_t n0, int64_t n1)
 int alloc_pm(jt_handle* h)
 {
     jt_pm_dev& pm = h->pm;
-    int M = h->cfg.pm_grid;
+    const jt_config& c = h->cfg;
+    int M = c.pm_grid;
     pm.M = M;
-    pm.L = h->cfg.box_L;
+    pm.L = c.box_L;
+    bool rc = c.mode == JT_RCOMPAT;
+    pm.order = rc ? 2 : (c.pm_order == 0 ? 3 : c.pm_order);
+    pm.ngrid = rc ? 1 : (c.pm_interlace == 2 ? 1 : 2);
     int64_t G = (int64_t)M * M * M, Gc = (int64_t)M * M * (M / 2 + 1);
-    bool rc = h->cfg.mode == JT_RCOMPAT;
-    JT_TRY(dalloc(&pm.rho, G));
-    if (!rc) JT_TRY(dalloc(&pm.rho_k, Gc));
-    // accurate: 3 spectra + the per-axis factor table (M float4 = 2M complex)
-    JT_TRY(dalloc(&pm.force_k, rc ? Gc : 3 * Gc + 2 * (int64_t)M));
-    JT_TRY(dalloc(&pm.force, rc ? G : 3 * G));
-    JT_FFT(cufftPlan3d(&pm.plan_r2c, M, M, M, CUFFT_R2C));
+    int NG = pm.ngrid;
+    JT_TRY(dalloc(&pm.rho, NG * G));
+    if (!rc) JT_TRY(dalloc(&pm.rho_k, NG * Gc));
+    // accurate: 3*NG spectra + two per-axis tables (2M float4 = 4M complex)
+    JT_TRY(dalloc(&pm.force_k, rc ? Gc : 3 * NG * Gc + 4 * (int64_t)M));
+    JT_TRY(dalloc(&pm.force, rc ? G : 3 * NG * G));
+    int T = jt_pm_tile_edge(M);
+    int64_t ntiles = (int64_t)(M / T) * (M / T) * (M / T);
+    JT_TRY(dalloc(&pm.ranges, ntiles));
+    int dims[3] = {M, M, M};
     if (rc) {
+        JT_FFT(cufftPlan3d(&pm.plan_r2c, M, M, M, CUFFT_R2C));
         JT_FFT(cufftPlan3d(&pm.plan_c2r, M, M, M, CUFFT_C2R));
     } else {
-        int dims[3] = {M, M, M};
+        JT_FFT(cufftPlanMany(&pm.plan_r2c, 3, dims, nullptr, 1, (int)G, nullptr, 1, (int)Gc,
+                             CUFFT_R2C, NG));
         JT_FFT(cufftPlanMany(&pm.plan_c2r, 3, dims, nullptr, 1, (int)Gc, nullptr, 1, (int)G,
-                             CUFFT_C2R, 3));
-        // per-axis factors: k_n, gradient factor (0 at Nyquist), exp(-k^2 r_s^2)/sinc^4, |n|
-        std::vector<float> tab(4 * (size_t)M);
-        double dk = 2.0 * M_PI / h->cfg.box_L, rs = h->cfg.r_s;
+                             CUFFT_C2R, 3 * NG));
+        // per-axis tables: ta = {k, gradient k (0 at Nyquist), exp(-k^2 r_s^2)/sinc^(2 order), |n|}
+        //                  tb = {cos(k h/2), sin(k h/2), 0, 0}
+        std::vector<float> tab(8 * (size_t)M);
+        double dk = 2.0 * M_PI / c.box_L, rs = c.r_s, hh = c.box_L / M;
         for (int n = 0; n < M; n++) {
             int ni = n <= M / 2 ? n : n - M;
             double k = dk * ni;
             double u = M_PI * ni / M;
             double sinc = ni == 0 ? 1.0 : std::sin(u) / u;
-            double f = std::exp(-k * k * rs * rs) / (sinc * sinc * sinc * sinc);
+            double f = std::exp(-k * k * rs * rs) / std::pow(sinc, 2.0 * pm.order);
             tab[4 * n] = (float)k;
             tab[4 * n + 1] = (n == M / 2) ? 0.0f : (float)k;
             tab[4 * n + 2] = (float)f;
             tab[4 * n + 3] = (float)(ni < 0 ? -ni : ni);
+            tab[4 * (M + n)] = (float)std::cos(0.5 * k * hh);
+            tab[4 * (M + n) + 1] = (float)std::sin(0.5 * k * hh);
+            tab[4 * (M + n) + 2] = 0.0f;
+            tab[4 * (M + n) + 3] = 0.0f;
         }
-        JT_CU(cudaMemcpy(pm.force_k + 3 * Gc, tab.data(), sizeof(float) * tab.size(),
-                         cudaMemcpyHostToDevice));
+        pm.tabs = reinterpret_cast<float4*>(pm.force_k + 3 * NG * Gc);
+        JT_CU(cudaMemcpy(pm.tabs, tab.data(), sizeof(float) * tab.size(), cudaMemcpyHostToDevice));
     }
     JT_FFT(cufftSetStream(pm.plan_r2c, h->st));
     JT_FFT(cufftSetStream(pm.plan_c2r, h->st));
@@ -202,7 +219,7 @@ void free_pm(jt_handle* h)
         cufftDestroy(pm.plan_r2c);
         cufftDestroy(pm.plan_c2r);
     }
-    dfree(pm.rho); dfree(pm.rho_k); dfree(pm.force_k); dfree(pm.force);
+    dfree(pm.rho); dfree(pm.rho_k); dfree(pm.force_k); dfree(pm.force); dfree(pm.ranges);
     pm = jt_pm_dev{};
 }
 
@@ -277,7 +294,7 @@ float elapsed(cudaEvent_t a, cudaEvent_t b)
 
 // Compute accelerations at the current positions into acc[s] (internal order).
 // kick_dt/drag: closing kick fused into the accurate walk (0 = none).
-int compute_forces(jt_handle* h, float kick_dt, float drag)
+int compute_forces(jt_handle* h, float kick_dt, float drag, int parts = JT_PART_ALL)
 {
     const jt_config& c = h->cfg;
     const bool rc = c.mode == JT_RCOMPAT;
@@ -287,7 +304,7 @@ int compute_forces(jt_handle* h, float kick_dt, float drag)
     cudaEventRecord(h->ev[0], st);
     JT_TRY(build_trees(h, rc, rc));
     cudaEventRecord(h->ev[2], st);
-    JT_CU(cudaMemsetAsync(h->pm.rho, 0, sizeof(float) * G, st));
+    JT_CU(cudaMemsetAsync(h->pm.rho, 0, sizeof(float) * G * h->pm.ngrid, st));
     if (rc) {
         for (int s = 0; s < 2; s++)
             jt_launch_to_caller(h->pos[s], h->id[s], h->gmap[s], h->n[s], h->pos_caller, st);
@@ -297,20 +314,23 @@ int compute_forces(jt_handle* h, float kick_dt, float drag)
                                   (float)(1.0 / (cell * cell * cell)), st);
     } else {
         double h3 = std::pow(c.box_L / M, 3.0);
-        jt_launch_deposit(h->pos[0], h->n[0], (float)(h->mass[0] / h3), h->pos[1], h->n[1],
-                          (float)(-h->mass[1] / h3), h->pm.rho, M, (float)c.box_L, 0, st);
+        jt_launch_tile_ranges(h->tree[0].m30, h->n[0], h->tree[1].m30, h->n[1], M, h->pm.ranges, st);
+        JT_TRY(jt_launch_deposit_tiled(h->pos[0], (float)(h->mass[0] / h3), h->pos[1],
+                                       (float)(-h->mass[1] / h3), h->pm.ranges, h->pm.rho, M,
+                                       (float)c.box_L, h->pm.order, h->pm.ngrid, st));
     }
     cudaEventRecord(h->ev[3], st);
     if (rc) {
         JT_FFT(cufftExecR2C(h->pm.plan_r2c, h->pm.rho, h->pm.force_k));
         cudaEventRecord(h->ev[4], st);
-        jt_launch_kspace(nullptr, h->pm.force_k, M, c.box_L, c.r_cut / 3.0, c.k_min, 1, st);
+        jt_launch_kspace(nullptr, h->pm.force_k, M, c.box_L, c.r_cut / 3.0, c.k_min, 1, 0, nullptr, st);
         cudaEventRecord(h->ev[5], st);
         JT_FFT(cufftExecC2R(h->pm.plan_c2r, h->pm.force_k, h->pm.force));
     } else {
         JT_FFT(cufftExecR2C(h->pm.plan_r2c, h->pm.rho, h->pm.rho_k));
         cudaEventRecord(h->ev[4], st);
-        jt_launch_kspace(h->pm.rho_k, h->pm.force_k, M, c.box_L, c.r_s, c.k_min, 0, st);
+        jt_launch_kspace(h->pm.rho_k, h->pm.force_k, M, c.box_L, c.r_s, c.k_min, 0,
+                         h->pm.ngrid == 2, h->pm.tabs, st);
         cudaEventRecord(h->ev[5], st);
         JT_FFT(cufftExecC2R(h->pm.plan_c2r, h->pm.force_k, h->pm.force));
     }
@@ -341,6 +361,7 @@ int compute_forces(jt_handle* h, float kick_dt, float drag)
         P.M = M;
         P.mass[0] = h->mass[0];
         P.mass[1] = h->mass[1];
+        P.parts = parts;
         const float4* sp2[2] = {h->pos[0], h->pos[1]};
         jt_launch_walk_rcompat(P, h->pos_caller, h->sign_caller, h->n[0] + h->n[1], sp2, h->n,
                                h->tree, h->pm.force, h->acc_caller, h->d_err, st);
@@ -361,11 +382,14 @@ int compute_forces(jt_handle* h, float kick_dt, float drag)
         P.mass[1] = h->mass[1];
         P.M = M;
         P.h_inv = (float)(M / c.box_L);
+        P.order = h->pm.order;
+        P.ngrid = h->pm.ngrid;
+        P.parts = parts;
         const float4* p2[2] = {h->pos[0], h->pos[1]};
         float4* a2[2] = {h->acc[0], h->acc[1]};
         float4* v2[2] = {h->vel[0], h->vel[1]};
         jt_launch_walk_accurate(P, p2, h->n, h->tree, h->pm.force, a2, v2, kick_dt, drag,
-                                h->d_inter, h->d_err, st);
+                                h->d_stats, h->d_err, st);
     }
     cudaEventRecord(h->ev[7], st);
     JT_CU(cudaGetLastError());
@@ -387,11 +411,14 @@ void accumulate_timings(jt_handle* h)
 
 int fetch_inter(jt_handle* h)
 {
-    unsigned long long v = 0;
-    JT_CU(cudaMemcpyAsync(&v, h->d_inter, sizeof(v), cudaMemcpyDeviceToHost, h->st));
+    unsigned long long v[3] = {0, 0, 0};
+    JT_CU(cudaMemcpyAsync(v, h->d_stats, sizeof(v), cudaMemcpyDeviceToHost, h->st));
     JT_CU(cudaStreamSynchronize(h->st));
-    h->tm.interactions += (int64_t)v;
-    JT_CU(cudaMemsetAsync(h->d_inter, 0, sizeof(v), h->st));
+    h->tm.pair_interactions += (int64_t)v[0];
+    h->tm.node_interactions += (int64_t)v[1];
+    h->tm.candidates += (int64_t)v[2];
+    h->tm.interactions += (int64_t)(v[0] + v[1]);
+    JT_CU(cudaMemsetAsync(h->d_stats, 0, sizeof(v), h->st));
     return JT_OK;
 }
 
@@ -465,10 +492,10 @@ int jt_create(const jt_config* cfg, jt_handle** out)
     }
     for (auto& e : h->ev) cudaEventCreate(&e);
     if (cudaMalloc(&h->d_err, sizeof(unsigned)) != cudaSuccess ||
-        cudaMalloc(&h->d_inter, sizeof(unsigned long long)) != cudaSuccess) r = JT_ENOMEM;
+        cudaMalloc(&h->d_stats, 3 * sizeof(unsigned long long)) != cudaSuccess) r = JT_ENOMEM;
     if (r == JT_OK) {
         cudaMemset(h->d_err, 0, sizeof(unsigned));
-        cudaMemset(h->d_inter, 0, sizeof(unsigned long long));
+        cudaMemset(h->d_stats, 0, 3 * sizeof(unsigned long long));
         r = alloc_pm(h);
     }
     if (r != JT_OK) {
@@ -486,7 +513,7 @@ void jt_destroy(jt_handle* h)
     free_particles(h);
     free_pm(h);
     if (h->d_err) cudaFree(h->d_err);
-    if (h->d_inter) cudaFree(h->d_inter);
+    if (h->d_stats) cudaFree(h->d_stats);
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
     if (h->st) cudaStreamDestroy(h->st);
@@ -585,14 +612,21 @@ int jt_set_state_signed(jt_handle* h, const float* pos, const float* vel, const 
 
 int jt_accel(jt_handle* h, float* acc_p, float* acc_m, int mem)
 {
+    return jt_accel_part(h, JT_PART_ALL, acc_p, acc_m, mem);
+}
+
+int jt_accel_part(jt_handle* h, int part, float* acc_p, float* acc_m, int mem)
+{
     if (!h || (mem != JT_MEM_HOST && mem != JT_MEM_DEVICE)) return JT_EINVAL;
+    if (part < 1 || part > 3) return JT_EINVAL;
     if (!h->have_state) return JT_ESTATE;
     h->tm = jt_timings{};
     cudaEvent_t t0, t1;
     cudaEventCreate(&t0);
     cudaEventCreate(&t1);
     cudaEventRecord(t0, h->st);
-    int r = compute_forces(h, 0.0f, 0.0f);
+    int r = compute_forces(h, 0.0f, 0.0f, part);
+    if (part != JT_PART_ALL) h->acc_valid = false;
     if (r == JT_OK) {
         if (!h->signed_layout) {
             r = write_out(h, h->acc[0], h->id[0], nullptr, h->n[0], acc_p, mem);

@@ -34,6 +34,7 @@
 struct jt_tree_dev {
     int64_t n;         // particles (leaves)
     int2* child;
+    int2* range;       // internal node i: sorted particle range [first, last]
     int* parent;
     int* flag;         // arrival counters for the bottom-up pass
     float4* com;
@@ -93,6 +94,32 @@ __device__ __forceinline__ jt_sfac jt_split_S2(float x, float c)
     return s;
 }
 
+// Mass-assignment stencil along one axis at grid coordinate g (nodes at
+// integers): returns the first node index and fills ORDER weights.
+//   ORDER 2 (CIC): nodes floor(g), +1; weights 1-f, f
+//   ORDER 3 (TSC): nodes c-1, c, c+1 with c = nearest node, d = g - c;
+//                  weights (1/2)(1/2-d)^2, 3/4-d^2, (1/2)(1/2+d)^2
+// Deposit and interpolation use the same stencil, so the scheme exerts no
+// self-force and conserves momentum.
+template <int ORDER>
+__device__ __forceinline__ int jt_stencil(float g, float* w)
+{
+    if (ORDER == 2) {
+        float f0 = floorf(g);
+        float f = g - f0;
+        w[0] = 1.0f - f;
+        w[1] = f;
+        return (int)f0;
+    } else {
+        float c = floorf(g + 0.5f);
+        float d = g - c;
+        w[0] = 0.5f * (0.5f - d) * (0.5f - d);
+        w[1] = 0.75f - d * d;
+        w[2] = 0.5f * (0.5f + d) * (0.5f + d);
+        return (int)c - 1;
+    }
+}
+
 __device__ __forceinline__ float jt_wrap(float d, float L, float halfL)
 {
     // minimum image for |d| < 1.5 L
@@ -130,10 +157,14 @@ void jt_launch_moments(jt_tree_dev t, const float4* pos, float mass, float box_h
 struct jt_pm_dev {
     int M;
     double L;
-    float* rho;
-    cufftComplex* rho_k;
-    cufftComplex* force_k;   // 3 spectra (ACCURATE) or 1 (RCOMPAT potential)
-    float* force;            // 3 grids (ACCURATE) or 1 potential grid (RCOMPAT)
+    int order;               // 2 = CIC, 3 = TSC (accurate); 2 in compatibility mode
+    int ngrid;               // 1, or 2 with interlacing
+    float* rho;              // ngrid grids
+    cufftComplex* rho_k;     // ngrid spectra
+    cufftComplex* force_k;   // 3*ngrid spectra + axis tables (ACCURATE) or 1 (RCOMPAT)
+    float4* tabs;            // 2*M float4 axis tables (inside force_k)
+    float* force;            // 3*ngrid grids (ACCURATE) or 1 potential grid (RCOMPAT)
+    int4* ranges;            // per-tile particle ranges
     cufftHandle plan_r2c, plan_c2r;
     int plans_ready;
 };
@@ -141,7 +172,15 @@ void jt_launch_deposit(const float4* pos0, int64_t n0, float q0, const float4* p
                        int64_t n1, float q1, float* rho, int M, float L, int rcompat,
                        cudaStream_t st);
 void jt_launch_kspace(const cufftComplex* rho_k, cufftComplex* out, int M, double L,
-                      double r_s, int k_min, int rcompat, cudaStream_t st);
+                      double r_s, int k_min, int rcompat, int interlace, const float4* tabs,
+                      cudaStream_t st);
+int jt_pm_tile_edge(int M);
+// per-tile particle ranges [x,y) of species 0 and [z,w) of species 1
+void jt_launch_tile_ranges(const uint32_t* m0, int64_t n0, const uint32_t* m1, int64_t n1,
+                           int M, int4* ranges, cudaStream_t st);
+int jt_launch_deposit_tiled(const float4* pos0, float q0, const float4* pos1, float q1,
+                            const int4* ranges, float* rho, int M, float L, int order,
+                            int ngrid, cudaStream_t st);
 
 // walk (jt_walk.cu)
 struct jt_walk_params {
@@ -153,18 +192,24 @@ struct jt_walk_params {
     float mass[2];      // per-species particle mass (G folded in)
     int M;
     float h_inv;        // M / L
+    int order;          // PM assignment order (2 CIC, 3 TSC)
+    int ngrid;          // PM grids (2 with interlacing)
+    int parts;          // JT_PART_* bits: 1 = PM, 2 = tree
 };
+// stats[0] pair interactions inside r_cut, [1] node (multipole) interactions,
+// [2] candidate particles distance-tested
 void jt_launch_walk_accurate(const jt_walk_params& p, const float4* const pos[2],
                              const int64_t n[2], const jt_tree_dev tree[2],
                              const float* force3, float4* const acc[2],
                              float4* const vel[2], float kick_dt, float kick_drag,
-                             unsigned long long* inter, unsigned* d_err, cudaStream_t st);
+                             unsigned long long* stats, unsigned* d_err, cudaStream_t st);
 
 struct jt_rc_params {
     float theta2, eps2, r_cut, box_half_q, r_s;   // quantised tree parameters
     float box_half, inv_cell, cell;               // PM (float) as the reference
     int M;
     float mass[2];
+    int parts;                                    // JT_PART_* bits
 };
 void jt_launch_walk_rcompat(const jt_rc_params& p, const float4* pos_caller,
                             const int8_t* sign_caller, int64_t n_all,

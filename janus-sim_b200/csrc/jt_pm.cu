@@ -1,4 +1,4 @@
-// Particle-mesh kernels: signed CIC deposit and the fused k-space kernel.
+// Particle-mesh kernels: signed mass deposit and the fused k-space kernel.
 //
 // Reference: cic_scatter (src/nbody_gpu_twopass.rs:98-158) deposits counts of
 // each species into two f64 grids with CAS-loop atomics; cufft_solve_device
@@ -8,18 +8,140 @@
 //
 // Here: one FP32 grid holds the signed source rho = sum_j s_j m_j W / h^3 of
 // both species (the reference's F+ = -grad phi+ + grad phi- is the same linear
-// combination), deposited with native float reductions by particles in Morton
-// order; one R2C; ONE k-space kernel applies Green x Gaussian filter (x CIC
-// deconvolution x spectral gradient in the accurate mode) and the 1/M^3
-// normalisation and writes the three force spectra; one batched C2R (batch 3)
-// produces the three force grids.  The compatibility mode writes the potential
-// spectrum only (the reference's Green, r_s = r_cut/3, k_min filter) and
-// differentiates in real space as the reference does.
+// combination).  Accurate mode:
+//   * deposit: one CTA per Morton-aligned tile of T^3 cells.  Particles are
+//     kept in Morton order, so a tile's particles are one contiguous range of
+//     each species' array; the CTA accumulates them into a shared-memory copy
+//     of the tile plus a one-cell halo with shared-memory float atomics and
+//     flushes it to the grid with coalesced global reductions.  CIC (8 cells)
+//     or TSC (27 cells); with interlacing a second grid whose nodes sit half a
+//     cell higher on every axis receives the same particles.
+//   * one (batched) R2C; ONE k-space kernel combines the interlaced spectra,
+//     applies -4 pi/k^2 x exp(-k^2 r_s^2) x 1/U(k)^2 (U = sinc^order per axis)
+//     x 1/M^3, takes the spectral gradient -i k, and writes the three force
+//     spectra (six with interlacing, the second three phase-shifted to the
+//     shifted nodes); modes on a Nyquist plane are dropped (their weight is
+//     exp(-(pi r_s/h)^2) ~ 2e-7 at r_s = 1.25 h); one batched C2R.
+// Compatibility mode writes the potential spectrum only (the reference's
+// Green, r_s = r_cut/3, k_min filter) and differentiates in real space as the
+// reference does.
 #include "jt_internal.cuh"
 
 namespace {
 
-// ---- accurate deposit: nodes at -L/2 + i h, floor-based CIC, wrap by mask
+// ---------------------------------------------------------------- helpers
+__device__ __forceinline__ uint32_t compact3(uint32_t x)
+{
+    x &= 0x09249249u;
+    x = (x ^ (x >> 2)) & 0x030C30C3u;
+    x = (x ^ (x >> 4)) & 0x0300F00Fu;
+    x = (x ^ (x >> 8)) & 0x030000FFu;
+    x = (x ^ (x >> 16)) & 0x000003FFu;
+    return x;
+}
+
+__device__ __forceinline__ int64_t lower_bound_tile(const uint32_t* __restrict__ m30, int64_t n,
+                                                    uint32_t key, int shift)
+{
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+        int64_t mid = (lo + hi) >> 1;
+        if ((m30[mid] >> shift) < key) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void k_tile_ranges(const uint32_t* __restrict__ m0, int64_t n0,
+                              const uint32_t* __restrict__ m1, int64_t n1, int shift, int ntiles,
+                              int4* __restrict__ ranges)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntiles) return;
+    int4 r;
+    r.x = (int)lower_bound_tile(m0, n0, (uint32_t)t, shift);
+    r.y = (int)lower_bound_tile(m0, n0, (uint32_t)t + 1, shift);
+    r.z = (int)lower_bound_tile(m1, n1, (uint32_t)t, shift);
+    r.w = (int)lower_bound_tile(m1, n1, (uint32_t)t + 1, shift);
+    ranges[t] = r;
+}
+
+constexpr int kTileEdge = 16;
+
+template <int ORDER, int NG>
+__global__ void __launch_bounds__(256)
+k_deposit_tiled(const float4* __restrict__ pos0, float q0, const float4* __restrict__ pos1, float q1,
+                const int4* __restrict__ ranges, int shift, int T, float* __restrict__ rho, int M,
+                float halfL, float hinv)
+{
+    extern __shared__ float tile[];
+    const int S = T + 3;               // cells [origin-1, origin+T+1]
+    const int S3 = S * S * S;
+    // tile id = Morton code of the tile (m30 >> shift); its first cell, minus the halo
+    const uint32_t t = blockIdx.x;
+    (void)shift;
+    const int bx = (int)compact3(t) * T - 1;
+    const int by = (int)compact3(t >> 1) * T - 1;
+    const int bz = (int)compact3(t >> 2) * T - 1;
+    for (int c = threadIdx.x; c < NG * S3; c += blockDim.x) tile[c] = 0.0f;
+    __syncthreads();
+    const int4 r = ranges[t];
+    const int mask = M - 1;
+    const int64_t G = (int64_t)M * M * M;
+    const int n0 = r.y - r.x, n1 = r.w - r.z;
+    for (int k = threadIdx.x; k < n0 + n1; k += blockDim.x) {
+        float4 p;
+        float q;
+        if (k < n0) { p = pos0[r.x + k]; q = q0; } else { p = pos1[r.z + k - n0]; q = q1; }
+        float gx = (p.x + halfL) * hinv, gy = (p.y + halfL) * hinv, gz = (p.z + halfL) * hinv;
+#pragma unroll
+        for (int b = 0; b < NG; b++) {
+            float sh = 0.5f * b;
+            float wx[ORDER], wy[ORDER], wz[ORDER];
+            int ix = jt_stencil<ORDER>(gx - sh, wx);
+            int iy = jt_stencil<ORDER>(gy - sh, wy);
+            int iz = jt_stencil<ORDER>(gz - sh, wz);
+            int lx = ix - bx, ly = iy - by, lz = iz - bz;
+            bool inside = lx >= 0 && ly >= 0 && lz >= 0 && lx + ORDER <= S && ly + ORDER <= S &&
+                          lz + ORDER <= S;
+            if (inside) {
+                float* tb_ = tile + b * S3;
+#pragma unroll
+                for (int c = 0; c < ORDER; c++)
+#pragma unroll
+                    for (int bb = 0; bb < ORDER; bb++) {
+                        float wyz = q * wz[c] * wy[bb];
+                        float* row = tb_ + ((lz + c) * S + (ly + bb)) * S + lx;
+#pragma unroll
+                        for (int a = 0; a < ORDER; a++) atomicAdd(row + a, wyz * wx[a]);
+                    }
+            } else {
+                // particle outside its Morton tile's box (float rounding at a tile
+                // edge or a position outside the box): reduce straight into the grid
+                float* gb = rho + b * G;
+#pragma unroll
+                for (int c = 0; c < ORDER; c++)
+#pragma unroll
+                    for (int bb = 0; bb < ORDER; bb++) {
+                        float wyz = q * wz[c] * wy[bb];
+                        int64_t row = ((int64_t)((iz + c) & mask) * M + ((iy + bb) & mask)) * M;
+#pragma unroll
+                        for (int a = 0; a < ORDER; a++) atomicAdd(gb + row + ((ix + a) & mask), wyz * wx[a]);
+                    }
+            }
+        }
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < NG * S3; c += blockDim.x) {
+        float v = tile[c];
+        if (v == 0.0f) continue;
+        int b = c / S3, rem = c - b * S3;
+        int lz = rem / (S * S), ly = (rem / S) % S, lx = rem % S;
+        int64_t idx = ((int64_t)((bz + lz) & mask) * M + ((by + ly) & mask)) * M + ((bx + lx) & mask);
+        atomicAdd(rho + b * G + idx, v);
+    }
+}
+
+// ---- plain deposit (no tiling): CIC, one grid -- used for tiny grids
 __global__ void k_deposit(const float4* __restrict__ pos0, int64_t n0, float q0,
                           const float4* __restrict__ pos1, int64_t n1, float q1,
                           float* __restrict__ rho, int M, float halfL, float hinv)
@@ -85,36 +207,58 @@ __global__ void k_deposit_rc(const float4* __restrict__ pos, const int8_t* __res
             }
 }
 
-// per-axis factors of the accurate Green's function (separable):
-//   ax[n] = { k_n, grad factor (0 at Nyquist), exp(-k_n^2 r_s^2) / sinc^4(pi n / M), |n| }
+// Accurate k-space kernel.  Per-axis tables (index n = 0..M-1):
+//   ta[n] = { k_n, gradient factor k_n, exp(-k_n^2 r_s^2) / sinc^(2 order)(pi n/M), |n| }
+//   tb[n] = { cos(k_n h/2), sin(k_n h/2), 0, 0 }   (interlacing phase)
+template <bool IL>
 __global__ void k_kspace_acc(const float2* __restrict__ rho_k, float2* __restrict__ out, int M,
-                             const float4* __restrict__ axis, float norm, int k_min,
-                             int64_t Gc)
+                             const float4* __restrict__ ta, const float4* __restrict__ tb,
+                             float norm, int k_min, int64_t Gc)
 {
     int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= Gc) return;
-    int Mh = M / 2 + 1;
-    int kx = (int)(idx % Mh);
-    int64_t r = idx / Mh;
-    int ky = (int)(r % M);
-    int kz = (int)(r / M);
-    float4 ax = __ldg(&axis[kx]), ay = __ldg(&axis[ky]), az = __ldg(&axis[kz]);
-    float k2 = ax.x * ax.x + ay.x * ay.x + az.x * az.x;
-    int kmax = max(max((int)ax.w, (int)ay.w), (int)az.w);
-    float2 z = rho_k[idx];
-    float2 o0 = make_float2(0.f, 0.f), o1 = o0, o2 = o0;
-    if (k2 > 0.0f && kmax >= k_min) {
-        // -4 pi / k^2 * filter * deconvolution * 1/M^3
+    const int Mh = M / 2 + 1;
+    const int kx = (int)(idx % Mh);
+    const int64_t r = idx / Mh;
+    const int ky = (int)(r % M);
+    const int kz = (int)(r / M);
+    const float4 ax = __ldg(&ta[kx]), ay = __ldg(&ta[ky]), az = __ldg(&ta[kz]);
+    const float k2 = ax.x * ax.x + ay.x * ay.x + az.x * az.x;
+    const int half = M / 2;
+    const int nx = (int)ax.w, ny = (int)ay.w, nz = (int)az.w;
+    const int kmax = max(max(nx, ny), nz);
+    const bool keep = k2 > 0.0f && kmax >= k_min && nx != half && ny != half && nz != half;
+    float2 F0 = make_float2(0.f, 0.f), F1 = F0, F2 = F0;
+    float er = 1.0f, ei = 0.0f;  // exp(+i theta), theta = (kx + ky + kz) h / 2
+    if (keep) {
+        float2 z = rho_k[idx];
+        if (IL) {
+            float4 bx = __ldg(&tb[kx]), by = __ldg(&tb[ky]), bz = __ldg(&tb[kz]);
+            // exp(+i theta) = prod (c + i s)
+            float pr = bx.x * by.x - bx.y * by.y, pi = bx.x * by.y + bx.y * by.x;
+            er = pr * bz.x - pi * bz.y;
+            ei = pr * bz.y + pi * bz.x;
+            float2 w = rho_k[Gc + idx];
+            // rho = (rhoA + rhoB exp(-i theta)) / 2
+            z.x = 0.5f * (z.x + (w.x * er + w.y * ei));
+            z.y = 0.5f * (z.y + (w.y * er - w.x * ei));
+        }
         float green = -12.566370614f * norm * (ax.z * ay.z * az.z) / k2;
         float pr = z.x * green, pi = z.y * green;
         // a_d(k) = -i k_d phi(k) = k_d (pi, -pr)
-        o0 = make_float2(ax.y * pi, -ax.y * pr);
-        o1 = make_float2(ay.y * pi, -ay.y * pr);
-        o2 = make_float2(az.y * pi, -az.y * pr);
+        F0 = make_float2(ax.y * pi, -ax.y * pr);
+        F1 = make_float2(ay.y * pi, -ay.y * pr);
+        F2 = make_float2(az.y * pi, -az.y * pr);
     }
-    out[idx] = o0;
-    out[Gc + idx] = o1;
-    out[2 * Gc + idx] = o2;
+    out[idx] = F0;
+    out[Gc + idx] = F1;
+    out[2 * Gc + idx] = F2;
+    if (IL) {
+        // forces at the shifted nodes: multiply by exp(+i theta)
+        out[3 * Gc + idx] = make_float2(F0.x * er - F0.y * ei, F0.x * ei + F0.y * er);
+        out[4 * Gc + idx] = make_float2(F1.x * er - F1.y * ei, F1.x * ei + F1.y * er);
+        out[5 * Gc + idx] = make_float2(F2.x * er - F2.y * ei, F2.x * ei + F2.y * er);
+    }
 }
 
 // the reference's apply_green_kernel + normalisation, FP32, in place:
@@ -144,6 +288,53 @@ __global__ void k_kspace_rc(float2* __restrict__ data, int M, float dk, float rs
 
 }  // namespace
 
+int jt_pm_tile_edge(int M) { return M < kTileEdge ? M : kTileEdge; }
+
+void jt_launch_tile_ranges(const uint32_t* m0, int64_t n0, const uint32_t* m1, int64_t n1, int M,
+                           int4* ranges, cudaStream_t st)
+{
+    int T = jt_pm_tile_edge(M);
+    int W = 1024 / M * T;  // tile edge in Morton cells (power of two)
+    int lw = 0;
+    while ((1 << lw) < W) lw++;
+    int shift = 3 * lw;
+    int ntiles = (M / T) * (M / T) * (M / T);
+    k_tile_ranges<<<(ntiles + 255) / 256, 256, 0, st>>>(m0, n0, m1, n1, shift, ntiles, ranges);
+}
+
+int jt_launch_deposit_tiled(const float4* pos0, float q0, const float4* pos1, float q1,
+                            const int4* ranges, float* rho, int M, float L, int order, int ngrid,
+                            cudaStream_t st)
+{
+    int T = jt_pm_tile_edge(M);
+    int W = 1024 / M * T;
+    int lw = 0;
+    while ((1 << lw) < W) lw++;
+    int shift = 3 * lw;
+    int ntiles = (M / T) * (M / T) * (M / T);
+    int S = T + 3;
+    size_t smem = sizeof(float) * (size_t)ngrid * S * S * S;
+    float halfL = 0.5f * L, hinv = (float)M / L;
+#define JT_DEP(O, NG)                                                                          \
+    do {                                                                                       \
+        static bool attr = false;                                                              \
+        if (!attr) {                                                                           \
+            cudaFuncSetAttribute(k_deposit_tiled<O, NG>,                                       \
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);      \
+            attr = true;                                                                       \
+        }                                                                                      \
+        k_deposit_tiled<O, NG><<<ntiles, 256, smem, st>>>(pos0, q0, pos1, q1, ranges, shift, T, \
+                                                          rho, M, halfL, hinv);                \
+    } while (0)
+    if (order == 2 && ngrid == 1) JT_DEP(2, 1);
+    else if (order == 2 && ngrid == 2) JT_DEP(2, 2);
+    else if (order == 3 && ngrid == 1) JT_DEP(3, 1);
+    else if (order == 3 && ngrid == 2) JT_DEP(3, 2);
+    else return JT_EINVAL;
+#undef JT_DEP
+    return cudaGetLastError() == cudaSuccess ? JT_OK : JT_ECUDA;
+}
+
 void jt_launch_deposit(const float4* pos0, int64_t n0, float q0, const float4* pos1, int64_t n1,
                        float q1, float* rho, int M, float L, int rcompat, cudaStream_t st)
 {
@@ -163,9 +354,8 @@ void jt_launch_rcompat_deposit(const float4* pos_caller, const int8_t* sign_call
         pos_caller, sign_caller, n_all, mass[0], mass[1], rho, M, box_half, inv_cell, inv_vol);
 }
 
-// axis table: computed on the host in double, stored as float4 per index
 void jt_launch_kspace(const cufftComplex* rho_k, cufftComplex* out, int M, double L, double r_s,
-                      int k_min, int rcompat, cudaStream_t st)
+                      int k_min, int rcompat, int interlace, const float4* tabs, cudaStream_t st)
 {
     int64_t Gc = (int64_t)M * M * (M / 2 + 1);
     float norm = (float)(1.0 / ((double)M * M * M));
@@ -175,7 +365,10 @@ void jt_launch_kspace(const cufftComplex* rho_k, cufftComplex* out, int M, doubl
                                        (float)(r_s * r_s), norm, k_min, Gc);
         return;
     }
-    // the axis table lives right after the three spectra (allocated by the caller)
-    const float4* axis = reinterpret_cast<const float4*>(out + 3 * Gc);
-    k_kspace_acc<<<g, 256, 0, st>>>((const float2*)rho_k, (float2*)out, M, axis, norm, k_min, Gc);
+    if (interlace)
+        k_kspace_acc<true><<<g, 256, 0, st>>>((const float2*)rho_k, (float2*)out, M, tabs, tabs + M,
+                                              norm, k_min, Gc);
+    else
+        k_kspace_acc<false><<<g, 256, 0, st>>>((const float2*)rho_k, (float2*)out, M, tabs, tabs + M,
+                                               norm, k_min, Gc);
 }

@@ -41,7 +41,8 @@ __device__ __forceinline__ int tdelta(const uint32_t* m30, const uint32_t* tie, 
 }
 
 __global__ void k_karras(const uint32_t* __restrict__ m30, const uint32_t* __restrict__ tie,
-                         int64_t n, int2* __restrict__ child, int* __restrict__ parent)
+                         int64_t n, int2* __restrict__ child, int* __restrict__ parent,
+                         int2* __restrict__ range)
 {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
@@ -76,6 +77,7 @@ __global__ void k_karras(const uint32_t* __restrict__ m30, const uint32_t* __res
     int64_t lc = (first == gamma) ? (n - 1 + first) : gamma;
     int64_t rc = (gamma + 1 == last) ? (n - 1 + last) : (gamma + 1);
     child[i] = make_int2((int)lc, (int)rc);
+    if (range) range[i] = make_int2((int)first, (int)last);
     parent[lc] = (int)i;
     parent[rc] = (int)i;
 }
@@ -171,7 +173,7 @@ void jt_launch_karras(jt_tree_dev t, cudaStream_t st)
     cudaMemsetAsync(t.child, 0, sizeof(int2) * nn, st);
     if (t.n >= 2)
         k_karras<<<(unsigned)((t.n - 1 + 255) / 256), 256, 0, st>>>(t.m30, t.tie, t.n, t.child,
-                                                                   t.parent);
+                                                                   t.parent, t.range);
 }
 
 void jt_launch_moments(jt_tree_dev t, const float4* pos, float mass, float box_half, int rcompat,

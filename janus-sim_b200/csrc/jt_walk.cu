@@ -31,15 +31,26 @@
 namespace {
 
 constexpr int kWarps = JT_WARPS_PER_BLOCK;
-constexpr int kStackCap = 1536;
-constexpr int kListCap = 64;
+#ifndef JT_WALK_STACK
+#define JT_WALK_STACK 384
+#endif
+#ifndef JT_WALK_BUCKET
+#define JT_WALK_BUCKET 32
+#endif
+constexpr int kStackCap = JT_WALK_STACK;   // per-warp traversal stack (node ids)
+constexpr int kBucket = JT_WALK_BUCKET;    // nodes with <= kBucket particles are streamed as ranges
+constexpr int kRangeCap = 64;     // queued ranges
+constexpr int kCandCap = 64;      // candidate particle buffer
+constexpr int kApproxCap = 64;    // queued multipole nodes
 
 struct WalkWarpSmem {
     int stack[kStackCap];
-    float4 dsrc[kListCap];
-    float4 acom[kListCap];
-    float4 aq0[kListCap];
-    float2 aq1[kListCap];
+    int2 rng[kRangeCap];          // (first sorted index, count)
+    float4 rsh[kRangeCap];        // periodic shift of the range (multiples of L)
+    float4 cand[kCandCap];        // shifted candidate positions
+    float4 acom[kApproxCap];      // shifted COM + mass
+    float4 aq0[kApproxCap];       // Qxx Qyy Qzz Qxy
+    float2 aq1[kApproxCap];       // Qxz Qyz
 };
 
 struct Acc3 {
@@ -83,46 +94,75 @@ struct WalkArgs {
     float4* vel[2];
     float kick_dt, kick_drag;
     int64_t groups0, groups1;
-    unsigned long long* inter;
+    unsigned long long* stats;
     unsigned* err;
 };
 
-// evaluate `cnt` queued direct sources against this lane's particle
-__device__ __forceinline__ void eval_direct(const float4* __restrict__ src, int cnt, float px,
-                                            float py, float pz, const jt_walk_params& P,
-                                            float fac, Acc3& a)
+// Pair interactions of this lane's particle with a chunk of cnt candidates:
+// a distance mask first (8 flops per candidate), then the full split-force
+// kernel only for candidates inside r_cut.  WRAP applies the minimum image
+// per pair (groups wider than L/8; otherwise candidates were shifted to the
+// group's image when queued).
+template <bool WRAP>
+__device__ __forceinline__ int eval_chunk(const float4* __restrict__ cand, int cnt, float px, float py,
+                                          float pz, bool valid, const jt_walk_params& P, float fac,
+                                          Acc3& a)
 {
+    unsigned m = 0;
+#pragma unroll 8
     for (int j = 0; j < cnt; j++) {
-        float4 q = src[j];
-        float dx = jt_wrap(q.x - px, P.L, P.halfL);
-        float dy = jt_wrap(q.y - py, P.L, P.halfL);
-        float dz = jt_wrap(q.z - pz, P.L, P.halfL);
-        float r2 = dx * dx + dy * dy + dz * dz;
-        if (r2 < P.rc2 && r2 > 0.0f) {
-            float rp2 = r2 + P.eps2;
-            float ri = rsqrtf(rp2);
-            float x = rp2 * ri * P.c;
-            float g = fac * jt_split_S(x) * ri * ri * ri;
-            a.x += g * dx;
-            a.y += g * dy;
-            a.z += g * dz;
+        float4 q = cand[j];
+        float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
+        if (WRAP) {
+            dx = jt_wrap(dx, P.L, P.halfL);
+            dy = jt_wrap(dy, P.L, P.halfL);
+            dz = jt_wrap(dz, P.L, P.halfL);
         }
+        float r2 = dx * dx + dy * dy + dz * dz;
+        m |= ((r2 < P.rc2) & (r2 > 0.0f) ? 1u : 0u) << j;
     }
+    if (!valid) m = 0;
+    const int hits = __popc(m);
+    while (m) {
+        const int j = __ffs(m) - 1;
+        m &= m - 1;
+        float4 q = cand[j];
+        float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
+        if (WRAP) {
+            dx = jt_wrap(dx, P.L, P.halfL);
+            dy = jt_wrap(dy, P.L, P.halfL);
+            dz = jt_wrap(dz, P.L, P.halfL);
+        }
+        float rp2 = dx * dx + dy * dy + dz * dz + P.eps2;
+        float ri = rsqrtf(rp2);
+        float x = rp2 * ri * P.c;
+        float g = fac * jt_split_S(x) * ri * ri * ri;
+        a.x += g * dx;
+        a.y += g * dy;
+        a.z += g * dz;
+    }
+    return hits;
 }
 
-// evaluate `cnt` queued nodes (monopole + quadrupole), Kahan-compensated
-__device__ __forceinline__ void eval_approx(const float4* __restrict__ cm, const float4* __restrict__ q0s,
-                                            const float2* __restrict__ q1s, int cnt, float px,
-                                            float py, float pz, const jt_walk_params& P, float sgn,
-                                            Acc3& s, Acc3& c)
+// multipole (monopole + quadrupole) interactions, Kahan-compensated
+template <bool WRAP>
+__device__ __forceinline__ int eval_approx(const float4* __restrict__ cm, const float4* __restrict__ q0s,
+                                           const float2* __restrict__ q1s, int cnt, float px, float py,
+                                           float pz, bool valid, const jt_walk_params& P, float sgn,
+                                           Acc3& s, Acc3& c)
 {
+    int hits = 0;
     for (int j = 0; j < cnt; j++) {
         float4 m = cm[j];
-        float dx = jt_wrap(m.x - px, P.L, P.halfL);
-        float dy = jt_wrap(m.y - py, P.L, P.halfL);
-        float dz = jt_wrap(m.z - pz, P.L, P.halfL);
+        float dx = m.x - px, dy = m.y - py, dz = m.z - pz;
+        if (WRAP) {
+            dx = jt_wrap(dx, P.L, P.halfL);
+            dy = jt_wrap(dy, P.L, P.halfL);
+            dz = jt_wrap(dz, P.L, P.halfL);
+        }
         float r2 = dx * dx + dy * dy + dz * dz;
-        if (r2 < P.rc2) {
+        if (valid && r2 < P.rc2) {
+            hits++;
             float rp2 = r2 + P.eps2;
             float ri = rsqrtf(rp2);
             float x = rp2 * ri * P.c;
@@ -145,8 +185,200 @@ __device__ __forceinline__ void eval_approx(const float4* __restrict__ cm, const
             kahan_add(s.z, c.z, coef * dz + g1s * qz);
         }
     }
+    return hits;
 }
 
+// Stream the queued ranges [0, nr) into the candidate buffer, evaluating every
+// full chunk of 32.  The next range's particles are loaded while the current
+// one is appended (one coalesced float4 load per lane per range).
+template <bool WRAP>
+__device__ __forceinline__ void drain_ranges(WalkWarpSmem& S, int nr, int& nc,
+                                             const float4* __restrict__ tpos, int lane, float px,
+                                             float py, float pz, bool valid, const jt_walk_params& P,
+                                             float fac, Acc3& near, unsigned long long& pairs,
+                                             unsigned long long& cands)
+{
+    if (nr <= 0) return;
+    int2 r0 = S.rng[0];
+    float4 nxt = lane < r0.y ? tpos[r0.x + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int r = 0; r < nr; r++) {
+        const int2 rr = S.rng[r];
+        const float4 sh = S.rsh[r];
+        const float4 cur = nxt;
+        if (r + 1 < nr) {
+            const int2 rn = S.rng[r + 1];
+            nxt = lane < rn.y ? tpos[rn.x + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        if (lane < rr.y) S.cand[nc + lane] = make_float4(cur.x + sh.x, cur.y + sh.y, cur.z + sh.z, 0.f);
+        nc += rr.y;
+        __syncwarp();
+        if (nc >= 32) {
+            pairs += eval_chunk<WRAP>(S.cand, 32, px, py, pz, valid, P, fac, near);
+            cands += 32;
+            __syncwarp();
+            float4 t = S.cand[32 + lane];
+            __syncwarp();
+            if (lane < nc - 32) S.cand[lane] = t;
+            nc -= 32;
+            __syncwarp();
+        }
+    }
+}
+
+template <int ORDER, int NG, bool WRAP>
+__device__ __forceinline__ void walk_trees(const WalkArgs& A, WalkWarpSmem& S, int s, int lane,
+                                           const float4& p, bool valid, float gcx, float gcy,
+                                           float gcz, float ghx, float ghy, float ghz, Acc3& near,
+                                           Acc3& far, Acc3& comp, unsigned long long& pairs,
+                                           unsigned long long& nodes, unsigned long long& cands)
+{
+    const jt_walk_params& P = A.p;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int t = 0; t < 2; t++) {
+        const int64_t nt = A.n[t];
+        if (nt == 0 || !(P.parts & 2)) continue;
+        const jt_tree_dev T = A.tree[t];
+        const float4* __restrict__ tpos = A.pos[t];
+        const float sgn = (s == t) ? 1.0f : -1.0f;
+        const float fac_direct = sgn * P.mass[t];
+        const int64_t leaf0 = nt - 1;
+        int sp = 1, nR = 0, nA = 0, nc = 0;
+        if (lane == 0) S.stack[0] = 0;
+        __syncwarp();
+        while (sp > 0) {
+            const int k = sp < 32 ? sp : 32;
+            int node = lane < k ? S.stack[sp - k + lane] : -1;
+            sp -= k;
+            __syncwarp();
+            if (node >= 2 * nt - 1) {  // never expected: keeps a corrupted id off the loads
+                atomicOr(A.err, JT_ERRBIT_STACK);
+                node = -1;
+            }
+            int act = 0;  // 1 open, 2 range, 3 multipole
+            float4 pay = make_float4(0.f, 0.f, 0.f, 0.f), pq0 = pay;
+            float2 pq1 = make_float2(0.f, 0.f);
+            int2 ch = make_int2(0, 0), rg = make_int2(0, 0);
+            if (node >= 0) {
+                float lox, loy, loz, hix, hiy, hiz;
+                int first, count;
+                if (node >= leaf0) {
+                    first = (int)(node - leaf0);
+                    count = 1;
+                    float4 q = tpos[first];
+                    lox = hix = q.x; loy = hiy = q.y; loz = hiz = q.z;
+                } else {
+                    int2 r = T.range[node];
+                    first = r.x;
+                    count = r.y - r.x + 1;
+                    float4 lo = T.bmin[node], hi = T.bmax[node];
+                    lox = lo.x; loy = lo.y; loz = lo.z; hix = hi.x; hiy = hi.y; hiz = hi.z;
+                }
+                float nhx = 0.5f * (hix - lox), nhy = 0.5f * (hiy - loy), nhz = 0.5f * (hiz - loz);
+                float cx = 0.5f * (hix + lox), cy = 0.5f * (hiy + loy), cz = 0.5f * (hiz + loz);
+                float dx = jt_wrap(cx - gcx, P.L, P.halfL);
+                float dy = jt_wrap(cy - gcy, P.L, P.halfL);
+                float dz = jt_wrap(cz - gcz, P.L, P.halfL);
+                float gx = gap1(dx, ghx + nhx), gy = gap1(dy, ghy + nhy), gz = gap1(dz, ghz + nhz);
+                if (gx * gx + gy * gy + gz * gz <= P.rc2) {
+                    bool accepted = false;
+                    if (count > 1) {
+                        float4 cm = T.com[node];
+                        float mx = jt_wrap(cm.x - gcx, P.L, P.halfL);
+                        float my = jt_wrap(cm.y - gcy, P.L, P.halfL);
+                        float mz = jt_wrap(cm.z - gcz, P.L, P.halfL);
+                        float ax = gap1(mx, ghx), ay = gap1(my, ghy), az = gap1(mz, ghz);
+                        float dm2 = ax * ax + ay * ay + az * az;
+                        float size = 2.0f * fmaxf(fmaxf(nhx, nhy), nhz);
+                        if (size * size < P.theta2 * dm2) {
+                            accepted = true;
+                            act = 3;
+                            pay = make_float4(gcx + mx, gcy + my, gcz + mz, cm.w);
+                            pq0 = T.quad0[node];
+                            pq1 = T.quad1[node];
+                        }
+                    }
+                    if (!accepted) {
+                        if (count <= kBucket) {
+                            act = 2;
+                            rg = make_int2(first, count);
+                            // shift that moves the node to the group's periodic image
+                            pay = make_float4((gcx + dx) - cx, (gcy + dy) - cy, (gcz + dz) - cz, 0.f);
+                        } else {
+                            act = 1;
+                            ch = T.child[node];
+                        }
+                    }
+                }
+            }
+            const unsigned mopen = __ballot_sync(0xffffffffu, act == 1);
+            const unsigned mrng = __ballot_sync(0xffffffffu, act == 2);
+            const unsigned mapp = __ballot_sync(0xffffffffu, act == 3);
+            if (act == 1) {
+                int at = sp + 2 * __popc(mopen & lt);
+                if (at + 1 < kStackCap) {
+                    S.stack[at] = ch.y;
+                    S.stack[at + 1] = ch.x;
+                } else {
+                    atomicOr(A.err, JT_ERRBIT_STACK);
+                }
+            } else if (act == 2) {
+                int at = nR + __popc(mrng & lt);
+                S.rng[at] = rg;
+                S.rsh[at] = pay;
+            } else if (act == 3) {
+                int at = nA + __popc(mapp & lt);
+                S.acom[at] = pay;
+                S.aq0[at] = pq0;
+                S.aq1[at] = pq1;
+            }
+            {
+                int room = (kStackCap - sp) / 2;
+                int no = __popc(mopen);
+                sp += 2 * (no < room ? no : room);
+            }
+            nR += __popc(mrng);
+            nA += __popc(mapp);
+            __syncwarp();
+            if (nR >= 32) {
+                drain_ranges<WRAP>(S, 32, nc, tpos, lane, p.x, p.y, p.z, valid, P, fac_direct, near,
+                                   pairs, cands);
+                __syncwarp();
+                int2 r2 = S.rng[32 + lane];
+                float4 s2 = S.rsh[32 + lane];
+                __syncwarp();
+                if (lane < nR - 32) { S.rng[lane] = r2; S.rsh[lane] = s2; }
+                nR -= 32;
+                __syncwarp();
+            }
+            if (nA >= 32) {
+                nodes += eval_approx<WRAP>(S.acom, S.aq0, S.aq1, 32, p.x, p.y, p.z, valid, P, sgn, far, comp);
+                __syncwarp();
+                float4 t0 = S.acom[32 + lane], t1 = S.aq0[32 + lane];
+                float2 t2 = S.aq1[32 + lane];
+                __syncwarp();
+                if (lane < nA - 32) {
+                    S.acom[lane] = t0;
+                    S.aq0[lane] = t1;
+                    S.aq1[lane] = t2;
+                }
+                nA -= 32;
+                __syncwarp();
+            }
+        }
+        drain_ranges<WRAP>(S, nR, nc, tpos, lane, p.x, p.y, p.z, valid, P, fac_direct, near, pairs,
+                           cands);
+        __syncwarp();
+        if (nc > 0) {
+            pairs += eval_chunk<WRAP>(S.cand, nc, p.x, p.y, p.z, valid, P, fac_direct, near);
+            cands += nc;
+        }
+        if (nA > 0)
+            nodes += eval_approx<WRAP>(S.acom, S.aq0, S.aq1, nA, p.x, p.y, p.z, valid, P, sgn, far, comp);
+        __syncwarp();
+    }
+}
+
+template <int ORDER, int NG>
 __global__ void __launch_bounds__(kWarps * 32) k_walk_acc(WalkArgs A)
 {
     __shared__ WalkWarpSmem smem_all[kWarps];
@@ -164,7 +396,6 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk_acc(WalkArgs A)
     const bool valid = i < ns;
     const float4 p = A.pos[s][valid ? i : grp * 32];
     const float sgn_s = s == 0 ? 1.0f : -1.0f;
-    const unsigned lt = (1u << lane) - 1u;
 
     // group AABB
     float lox = warp_min(p.x), loy = warp_min(p.y), loz = warp_min(p.z);
@@ -172,162 +403,51 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk_acc(WalkArgs A)
     float gcx = 0.5f * (lox + hix), gcy = 0.5f * (loy + hiy), gcz = 0.5f * (loz + hiz);
     float ghx = 0.5f * (hix - lox), ghy = 0.5f * (hiy - loy), ghz = 0.5f * (hiz - loz);
 
-    // PM interpolation (CIC of the three force grids)
+    // PM interpolation: the deposit's stencil on every grid (the interlaced
+    // grid's nodes sit half a cell higher), averaged over the grids
     Acc3 pm = {0.f, 0.f, 0.f};
-    {
+    if (P.parts & 1) {
         const int M = P.M, mask = M - 1;
-        const int64_t G = (int64_t)M * M * M, MM = (int64_t)M * M;
-        float gx = (p.x + P.halfL) * P.h_inv, gy = (p.y + P.halfL) * P.h_inv,
-              gz = (p.z + P.halfL) * P.h_inv;
-        float fx0 = floorf(gx), fy0 = floorf(gy), fz0 = floorf(gz);
-        float fx = gx - fx0, fy = gy - fy0, fz = gz - fz0;
-        int ix = (int)fx0 & mask, iy = (int)fy0 & mask, iz = (int)fz0 & mask;
-        int ixs[2] = {ix, (ix + 1) & mask}, iys[2] = {iy, (iy + 1) & mask},
-            izs[2] = {iz, (iz + 1) & mask};
-        float wx[2] = {1.f - fx, fx}, wy[2] = {1.f - fy, fy}, wz[2] = {1.f - fz, fz};
+        const int64_t G = (int64_t)M * M * M;
+        const float gx = (p.x + P.halfL) * P.h_inv, gy = (p.y + P.halfL) * P.h_inv,
+                    gz = (p.z + P.halfL) * P.h_inv;
 #pragma unroll
-        for (int c = 0; c < 8; c++) {
-            int dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
-            int64_t id = ixs[dx] + iys[dy] * (int64_t)M + izs[dz] * MM;
-            float w = wx[dx] * wy[dy] * wz[dz];
-            pm.x += w * __ldg(A.force3 + id);
-            pm.y += w * __ldg(A.force3 + G + id);
-            pm.z += w * __ldg(A.force3 + 2 * G + id);
+        for (int b = 0; b < NG; b++) {
+            const float sh = 0.5f * b;
+            float wx[ORDER], wy[ORDER], wz[ORDER];
+            const int ix = jt_stencil<ORDER>(gx - sh, wx);
+            const int iy = jt_stencil<ORDER>(gy - sh, wy);
+            const int iz = jt_stencil<ORDER>(gz - sh, wz);
+            const float* __restrict__ F = A.force3 + (int64_t)b * 3 * G;
+#pragma unroll
+            for (int c = 0; c < ORDER; c++)
+#pragma unroll
+                for (int bb = 0; bb < ORDER; bb++) {
+                    const float wyz = wz[c] * wy[bb];
+                    const int64_t row = ((int64_t)((iz + c) & mask) * M + ((iy + bb) & mask)) * M;
+#pragma unroll
+                    for (int a = 0; a < ORDER; a++) {
+                        const int64_t id = row + ((ix + a) & mask);
+                        const float w = wyz * wx[a];
+                        pm.x += w * __ldg(F + id);
+                        pm.y += w * __ldg(F + G + id);
+                        pm.z += w * __ldg(F + 2 * G + id);
+                    }
+                }
         }
+        if (NG == 2) { pm.x *= 0.5f; pm.y *= 0.5f; pm.z *= 0.5f; }
     }
 
     Acc3 near = {0.f, 0.f, 0.f}, far = {0.f, 0.f, 0.f}, comp = {0.f, 0.f, 0.f};
-    unsigned long long inter = 0;
-    const unsigned nvalid = __popc(__ballot_sync(0xffffffffu, valid));
-
-    for (int t = 0; t < 2; t++) {
-        const int64_t nt = A.n[t];
-        if (nt == 0) continue;
-        const jt_tree_dev T = A.tree[t];
-        const float4* __restrict__ tpos = A.pos[t];
-        const float sgn = (s == t) ? 1.0f : -1.0f;
-        const float fac_direct = sgn * P.mass[t];
-        const int64_t leaf0 = nt - 1;
-        int sp = 1, nD = 0, nA = 0;
-        if (lane == 0) S.stack[0] = 0;
-        __syncwarp();
-        while (sp > 0) {
-            const int k = sp < 32 ? sp : 32;
-            int node = lane < k ? S.stack[sp - k + lane] : -1;
-            sp -= k;
-            __syncwarp();
-            if (node >= 2 * nt - 1) {  // never expected: keeps a corrupted id off the loads
-                atomicOr(A.err, JT_ERRBIT_STACK);
-                node = -1;
-            }
-            int act = 0;  // 1 push, 2 direct, 3 approx
-            float4 pay = make_float4(0.f, 0.f, 0.f, 0.f), pq0 = pay;
-            float2 pq1 = make_float2(0.f, 0.f);
-            int2 ch = make_int2(0, 0);
-            if (node >= 0) {
-                if (node >= leaf0) {
-                    float4 q = tpos[node - leaf0];
-                    float dx = jt_wrap(q.x - gcx, P.L, P.halfL);
-                    float dy = jt_wrap(q.y - gcy, P.L, P.halfL);
-                    float dz = jt_wrap(q.z - gcz, P.L, P.halfL);
-                    float gx = gap1(dx, ghx), gy = gap1(dy, ghy), gz = gap1(dz, ghz);
-                    if (gx * gx + gy * gy + gz * gz <= P.rc2) {
-                        act = 2;
-                        pay = make_float4(gcx + dx, gcy + dy, gcz + dz, 0.f);
-                    }
-                } else {
-                    float4 lo = T.bmin[node], hi = T.bmax[node];
-                    float nhx = 0.5f * (hi.x - lo.x), nhy = 0.5f * (hi.y - lo.y),
-                          nhz = 0.5f * (hi.z - lo.z);
-                    float dx = jt_wrap(0.5f * (hi.x + lo.x) - gcx, P.L, P.halfL);
-                    float dy = jt_wrap(0.5f * (hi.y + lo.y) - gcy, P.L, P.halfL);
-                    float dz = jt_wrap(0.5f * (hi.z + lo.z) - gcz, P.L, P.halfL);
-                    float gx = gap1(dx, ghx + nhx), gy = gap1(dy, ghy + nhy),
-                          gz = gap1(dz, ghz + nhz);
-                    if (gx * gx + gy * gy + gz * gz <= P.rc2) {
-                        float4 cm = T.com[node];
-                        float mx = jt_wrap(cm.x - gcx, P.L, P.halfL);
-                        float my = jt_wrap(cm.y - gcy, P.L, P.halfL);
-                        float mz = jt_wrap(cm.z - gcz, P.L, P.halfL);
-                        float ax = gap1(mx, ghx), ay = gap1(my, ghy), az = gap1(mz, ghz);
-                        float dm2 = ax * ax + ay * ay + az * az;
-                        float size = 2.0f * fmaxf(fmaxf(nhx, nhy), nhz);
-                        if (size * size < P.theta2 * dm2) {
-                            act = 3;
-                            pay = make_float4(gcx + mx, gcy + my, gcz + mz, cm.w);
-                            pq0 = T.quad0[node];
-                            pq1 = T.quad1[node];
-                        } else {
-                            act = 1;
-                            ch = T.child[node];
-                        }
-                    }
-                }
-            }
-            const unsigned mpush = __ballot_sync(0xffffffffu, act == 1);
-            const unsigned mdir = __ballot_sync(0xffffffffu, act == 2);
-            const unsigned mapp = __ballot_sync(0xffffffffu, act == 3);
-            if (act == 1) {
-                int at = sp + 2 * __popc(mpush & lt);
-                if (at + 1 < kStackCap) {
-                    S.stack[at] = ch.y;
-                    S.stack[at + 1] = ch.x;
-                } else {
-                    atomicOr(A.err, JT_ERRBIT_STACK);
-                }
-            } else if (act == 2) {
-                S.dsrc[nD + __popc(mdir & lt)] = pay;
-            } else if (act == 3) {
-                int at = nA + __popc(mapp & lt);
-                S.acom[at] = pay;
-                S.aq0[at] = pq0;
-                S.aq1[at] = pq1;
-            }
-            {
-                // lanes whose pair fitted wrote it; they are a prefix in lane order
-                int room = (kStackCap - sp) / 2;
-                int np = __popc(mpush);
-                sp += 2 * (np < room ? np : room);
-            }
-            nD += __popc(mdir);
-            nA += __popc(mapp);
-            __syncwarp();
-            while (nD >= 32) {
-                eval_direct(S.dsrc, 32, p.x, p.y, p.z, P, fac_direct, near);
-                inter += 32ull * nvalid;
-                __syncwarp();
-                float4 tmp = S.dsrc[32 + lane];
-                __syncwarp();
-                if (lane < nD - 32) S.dsrc[lane] = tmp;
-                nD -= 32;
-                __syncwarp();
-            }
-            while (nA >= 32) {
-                eval_approx(S.acom, S.aq0, S.aq1, 32, p.x, p.y, p.z, P, sgn, far, comp);
-                inter += 32ull * nvalid;
-                __syncwarp();
-                float4 t0 = S.acom[32 + lane], t1 = S.aq0[32 + lane];
-                float2 t2 = S.aq1[32 + lane];
-                __syncwarp();
-                if (lane < nA - 32) {
-                    S.acom[lane] = t0;
-                    S.aq0[lane] = t1;
-                    S.aq1[lane] = t2;
-                }
-                nA -= 32;
-                __syncwarp();
-            }
-        }
-        if (nD > 0) {
-            eval_direct(S.dsrc, nD, p.x, p.y, p.z, P, fac_direct, near);
-            inter += (unsigned long long)nD * nvalid;
-        }
-        if (nA > 0) {
-            eval_approx(S.acom, S.aq0, S.aq1, nA, p.x, p.y, p.z, P, sgn, far, comp);
-            inter += (unsigned long long)nA * nvalid;
-        }
-        __syncwarp();
-    }
+    unsigned long long pairs = 0, nodes = 0, cands = 0;
+    // groups wider than L/8 take the minimum image per pair
+    const bool wide = fmaxf(fmaxf(ghx, ghy), ghz) > 0.125f * P.L;
+    if (wide)
+        walk_trees<ORDER, NG, true>(A, S, s, lane, p, valid, gcx, gcy, gcz, ghx, ghy, ghz, near, far,
+                                    comp, pairs, nodes, cands);
+    else
+        walk_trees<ORDER, NG, false>(A, S, s, lane, p, valid, gcx, gcy, gcz, ghx, ghy, ghz, near, far,
+                                     comp, pairs, nodes, cands);
 
     if (valid) {
         float ax = sgn_s * pm.x + near.x + (far.x - comp.x);
@@ -342,7 +462,18 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk_acc(WalkArgs A)
             A.vel[s][i] = v;
         }
     }
-    if (lane == 0 && A.inter) atomicAdd(A.inter, inter);
+    if (A.stats) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
+            nodes += __shfl_xor_sync(0xffffffffu, nodes, o);
+        }
+        if (lane == 0) {
+            atomicAdd(A.stats, pairs);
+            atomicAdd(A.stats + 1, nodes);
+            atomicAdd(A.stats + 2, cands * 32ull);
+        }
+    }
 }
 
 // ------------------------------------------------------------------ RCOMPAT
@@ -382,7 +513,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk_rc(RcArgs A)
 
     for (int t = 0; t < 2; t++) {
         const int64_t nt = A.n[t];
-        if (nt == 0) continue;
+        if (nt == 0 || !(P.parts & 2)) continue;
         const jt_tree_dev T = A.tree[t];
         const int tree_sign = t == 0 ? 1 : -1;
         const float sf = (my_sign == tree_sign) ? 1.0f : -1.0f;
@@ -458,6 +589,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk_rc(RcArgs A)
     float sgn = (float)my_sign;
     float Fx = 0.f, Fy = 0.f, Fz = 0.f;
     const float* phi = A.phi;
+    if (P.parts & 1)
 #define RCIDX(a, b, c) ((int64_t)(a) + (int64_t)M * ((int64_t)(b) + (int64_t)M * (int64_t)(c)))
     for (int di = 0; di < 2; di++)
         for (int dj = 0; dj < 2; dj++)
@@ -577,7 +709,7 @@ __global__ void k_split_signed(const float* __restrict__ pos, const float* __res
 void jt_launch_walk_accurate(const jt_walk_params& p, const float4* const pos[2], const int64_t n[2],
                              const jt_tree_dev tree[2], const float* force3, float4* const acc[2],
                              float4* const vel[2], float kick_dt, float kick_drag,
-                             unsigned long long* inter, unsigned* d_err, cudaStream_t st)
+                             unsigned long long* stats, unsigned* d_err, cudaStream_t st)
 {
     WalkArgs A;
     A.p = p;
@@ -593,11 +725,15 @@ void jt_launch_walk_accurate(const jt_walk_params& p, const float4* const pos[2]
     A.kick_drag = kick_drag;
     A.groups0 = (n[0] + 31) / 32;
     A.groups1 = (n[1] + 31) / 32;
-    A.inter = inter;
+    A.stats = stats;
     A.err = d_err;
     int64_t warps = A.groups0 + A.groups1;
     if (warps == 0) return;
-    k_walk_acc<<<(unsigned)((warps + kWarps - 1) / kWarps), kWarps * 32, 0, st>>>(A);
+    unsigned g = (unsigned)((warps + kWarps - 1) / kWarps);
+    if (p.order == 3 && p.ngrid == 2) k_walk_acc<3, 2><<<g, kWarps * 32, 0, st>>>(A);
+    else if (p.order == 3) k_walk_acc<3, 1><<<g, kWarps * 32, 0, st>>>(A);
+    else if (p.ngrid == 2) k_walk_acc<2, 2><<<g, kWarps * 32, 0, st>>>(A);
+    else k_walk_acc<2, 1><<<g, kWarps * 32, 0, st>>>(A);
 }
 
 void jt_launch_walk_rcompat(const jt_rc_params& p, const float4* pos_caller, const int8_t* sign_caller,

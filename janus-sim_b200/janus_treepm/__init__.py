@@ -24,18 +24,20 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 PKG_ROOT = os.path.dirname(HERE)
-LIB_PATH = os.path.join(PKG_ROOT, "libjanus_treepm.so")
+# JANUS_TREEPM_LIB selects another build of the same library (for A/B timing)
+LIB_PATH = os.environ.get("JANUS_TREEPM_LIB", os.path.join(PKG_ROOT, "libjanus_treepm.so"))
 
 JT_OK, JT_EINVAL, JT_ENOMEM, JT_ECUDA, JT_ETIMEDOUT = 0, -1, -2, -3, -4
 JT_ENOTIMPL, JT_ESTATE, JT_EOVERFLOW, JT_EBUSY = -5, -6, -7, -8
 JT_MEM_HOST, JT_MEM_DEVICE = 0, 1
 JT_ACCURATE, JT_RCOMPAT = 0, 1
 JT_KDK, JT_DKD_REF = 0, 1
+JT_PART_PM, JT_PART_SHORT, JT_PART_ALL = 1, 2, 3
 
 EXPORTED = [
     "jt_create", "jt_set_state", "jt_set_state_signed", "jt_accel", "jt_accel_signed",
     "jt_step", "jt_get_state", "jt_get_state_signed", "jt_debug_tree", "jt_get_timings",
-    "jt_counts", "jt_destroy", "jt_strerror", "jt_version", "jt_fp32_peak",
+    "jt_counts", "jt_destroy", "jt_strerror", "jt_version", "jt_fp32_peak", "jt_accel_part",
 ]
 
 
@@ -51,7 +53,8 @@ class jt_config(C.Structure):
         ("box_L", C.c_double), ("pm_grid", C.c_int), ("theta", C.c_double),
         ("softening", C.c_double), ("r_s", C.c_double), ("r_cut", C.c_double),
         ("mu", C.c_double), ("G_mass_plus", C.c_double), ("k_min", C.c_int),
-        ("mode", C.c_int), ("integrator", C.c_int), ("reserved", C.c_int * 5),
+        ("mode", C.c_int), ("integrator", C.c_int), ("pm_order", C.c_int),
+        ("pm_interlace", C.c_int), ("reserved", C.c_int * 3),
     ]
 
 
@@ -61,6 +64,8 @@ class jt_timings(C.Structure):
         ("fft_ms", C.c_double), ("kspace_ms", C.c_double), ("walk_ms", C.c_double),
         ("kick_drift_ms", C.c_double), ("total_ms", C.c_double),
         ("interactions", C.c_int64), ("launches", C.c_int64),
+        ("pair_interactions", C.c_int64), ("node_interactions", C.c_int64),
+        ("candidates", C.c_int64),
     ]
 
 
@@ -82,6 +87,7 @@ def library():
     L.jt_set_state_signed.argtypes = [H, fp, fp, i8p, C.c_size_t, C.c_int]
     L.jt_accel.argtypes = [H, fp, fp, C.c_int]
     L.jt_accel_signed.argtypes = [H, fp, C.c_int]
+    L.jt_accel_part.argtypes = [H, C.c_int, fp, fp, C.c_int]
     L.jt_step.argtypes = [H, C.c_double, C.c_double, C.c_double, C.c_int]
     L.jt_get_state.argtypes = [H, fp, fp, fp, fp, C.c_int]
     L.jt_get_state_signed.argtypes = [H, fp, fp, C.c_int]
@@ -139,6 +145,8 @@ class Config:
     k_min: int = 0
     mode: int = JT_ACCURATE
     integrator: int = JT_KDK
+    pm_order: int = 0           # 0 -> TSC (accurate); 2 CIC; 3 TSC
+    pm_interlace: int = 0       # 0 -> on (accurate); 1 on; 2 off
 
     def resolved(self):
         c = Config(**self.__dict__)
@@ -154,6 +162,7 @@ class Config:
         s.box_L, s.pm_grid, s.theta, s.softening = c.box_L, c.pm_grid, c.theta, c.softening
         s.r_s, s.r_cut, s.mu, s.G_mass_plus = c.r_s, c.r_cut, c.mu, c.G_mass_plus
         s.k_min, s.mode, s.integrator = c.k_min, c.mode, c.integrator
+        s.pm_order, s.pm_interlace = c.pm_order, c.pm_interlace
         return s
 
 
@@ -220,6 +229,14 @@ class Solver:
         ap = np.zeros((self.n[0], 3), np.float32)
         am = np.zeros((self.n[1], 3), np.float32)
         _check(library().jt_accel(self._h, _ptr(ap), _ptr(am), JT_MEM_HOST), "jt_accel")
+        return ap, am
+
+    def accel_part(self, part):
+        """JT_PART_PM (long range only), JT_PART_SHORT (tree only) or JT_PART_ALL."""
+        ap = np.zeros((self.n[0], 3), np.float32)
+        am = np.zeros((self.n[1], 3), np.float32)
+        _check(library().jt_accel_part(self._h, part, _ptr(ap), _ptr(am), JT_MEM_HOST),
+               "jt_accel_part")
         return ap, am
 
     def accel_device(self, acc_p, acc_m):

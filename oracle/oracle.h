@@ -136,6 +136,10 @@ void orc_ewald_short(const double* pos, const double* mass,
 void orc_acc_pm_forces(const double* pos, const double* mass,
                        const int8_t* signs, int64_t n, int M, double box,
                        double r_s, int k_min, double* acc);
+/* Same with assignment order (2 CIC, 3 TSC) and ngrid (1, or 2 interlaced). */
+void orc_acc_pm_forces2(const double* pos, const double* mass,
+                        const int8_t* signs, int64_t n, int M, double box,
+                        double r_s, int k_min, int order, int ngrid, double* acc);
 /* The three long-range force grids of the accurate formulation for the
  * signed source (acc of a + particle), index x + M*(y + M*z). */
 void orc_acc_pm_grids(const double* pos, const double* mass,

@@ -53,6 +53,7 @@ def lib():
             "orc_ewald_short": [f64p, f64p, i8p, I64, i64p, I64, F64, F64, F64, F64, f64p],
             "orc_acc_pm_forces": [f64p, f64p, i8p, I64, I32, F64, F64, I32, f64p],
             "orc_acc_pm_grids": [f64p, f64p, i8p, I64, I32, F64, F64, I32, f64p, f64p, f64p],
+            "orc_acc_pm_forces2": [f64p, f64p, i8p, I64, I32, F64, F64, I32, I32, I32, f64p],
             "orc_fft3d": [f64p, I32, I32],
         }
         for name, args in sig.items():
@@ -207,11 +208,12 @@ def ewald_forces(pos, mass, signs, box, r_s, eps, r_trunc=None, idx=None,
     return acc
 
 
-def acc_pm_forces(pos, mass, signs, M, box, r_s, k_min=0):
+def acc_pm_forces(pos, mass, signs, M, box, r_s, k_min=0, order=2, interlace=False):
+    """FP64 PM acceleration (long range only) in the accurate formulation."""
     pos = _c(pos, np.float64).reshape(-1, 3)
     mass = _c(mass, np.float64)
     signs = _c(signs, np.int8)
     acc = np.zeros((len(pos), 3), np.float64)
-    lib().orc_acc_pm_forces(pos.ravel(), mass, signs, len(pos), M, box, r_s, k_min,
-                            acc.ravel())
+    lib().orc_acc_pm_forces2(pos.ravel(), mass, signs, len(pos), M, box, r_s, k_min, order,
+                             2 if interlace else 1, acc.ravel())
     return acc

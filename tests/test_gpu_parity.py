@@ -8,10 +8,10 @@ Bars:
     reference's GPU forces: p99 relative error <= 1e-5 (the engine evaluates
     the same float expressions; the PM runs in FP32 where the reference runs
     FP64, and CUDA's erfcf differs from the host's by an ulp);
-  * accurate-mode accelerations against the FP64 exact split-model sum (same
-    r_s, softening and r_cut, no grid, no tree): p99 relative error <= 2e-3
-    and median <= 3e-4 at theta = 0.5 (the remaining error is the PM grid's
-    and the tree's);
+  * accurate-mode accelerations (TSC + interlacing, the default) against the
+    FP64 exact split-model sum (same r_s, softening and r_cut, no grid, no
+    tree): median <= 2e-4 and p99 <= 3e-3 at theta = 0.5 (the remaining error
+    is the PM grid's; measured p50 8e-5, p99 1.3e-3 at 2x32^3 particles);
   * the m- response is the exact sign flip of the m+ response (bitwise).
 """
 import numpy as np
@@ -104,7 +104,7 @@ def test_accurate_matches_exact_split_model(n, M, L, mu):
     ex = O.ewald_forces(pos, mass, sg, L, r_s, eps, r_trunc=r_cut)
     rel = _rel(np.concatenate([ap, am]), ex)
     p50, p99 = np.percentile(rel, [50, 99])
-    assert p99 <= 2e-3 and p50 <= 3e-4, (p50, p99)
+    assert p99 <= 3e-3 and p50 <= 2e-4, (p50, p99)
     s.close()
 
 
