@@ -139,6 +139,98 @@ def cpu_treepm_step(sample_div=4, seed=42, threads=None):
     return len(pos), dt, (threads or os.cpu_count())
 
 
+def ensemble_boxes(n_boxes=64, seed=7):
+    """The batched-ensemble workload: n_boxes independent boxes, n per species
+    log-uniform in [16, 96] (N = n^3 per species), L ~ U(50, 300) Mpc, PM grid
+    = next power of two >= 2n (32..256), mu ~ U(5, 30), eta ~ U(1.00, 1.10)
+    (eta enters only the expansion factors, not the force path), seeded
+    Zel'dovich ICs (seed 1000 + box), cfg1's theta / r_s / r_cut / softening
+    rules and mass density."""
+    rng = np.random.default_rng(seed)
+    boxes = []
+    for b in range(n_boxes):
+        n = int(round(np.exp(rng.uniform(np.log(16), np.log(96)))))
+        L = float(rng.uniform(50.0, 300.0))
+        M = 1 << int(np.ceil(np.log2(2 * n)))
+        mu = float(rng.uniform(5.0, 30.0))
+        eta = float(rng.uniform(1.0, 1.1))
+        boxes.append(dict(n=n, L=L, M=M, mu=mu, eta=eta, seed=1000 + b))
+    return boxes
+
+
+def box_config(J, bx):
+    r_s = 1.25 * bx["L"] / bx["M"]
+    spacing = bx["L"] / bx["n"]
+    # cfg1's mass per particle scaled to the same mean density
+    gm = 1.0e-3 * (spacing / (250.0 / 224.0)) ** 3
+    return J.Config(box_L=bx["L"], pm_grid=bx["M"], theta=0.5,
+                    softening=bx["L"] / (2 * bx["n"] ** 3) ** (1.0 / 3.0) / 30.0, r_s=r_s,
+                    r_cut=4.5 * r_s, mu=bx["mu"], G_mass_plus=gm, mode=J.JT_ACCURATE,
+                    integrator=J.JT_KDK)
+
+
+def run_ensemble(J, ics, n_boxes, steps, warmup, H, dt):
+    """Batched steps of the ensemble vs the same boxes one at a time through
+    single handles (the plain path).  Device time of each call from its CUDA
+    events; wall time beside it."""
+    import torch
+    boxes = ensemble_boxes(n_boxes)
+    states = [ics.zeldovich_lattice(bx["n"], bx["L"], seed=bx["seed"]) for bx in boxes]
+    n_part = sum(2 * bx["n"] ** 3 for bx in boxes)
+    # batched
+    B = J.Batch()
+    ids = [B.add(box_config(J, bx), *st) for bx, st in zip(boxes, states)]
+    for _ in range(warmup):
+        B.step(ids, dt, H, 1.0, 1)
+    torch.cuda.synchronize()
+    dev, t0 = 0.0, time.perf_counter()
+    stages = {}
+    for _ in range(steps):
+        B.step(ids, dt, H, 1.0, 1)
+        tm = B.timings()
+        dev += tm["total_ms"]
+        for k, v in tm.items():
+            stages[k] = stages.get(k, 0.0) + v
+    torch.cuda.synchronize()
+    wall_b = time.perf_counter() - t0
+    mem = B.memory()
+    B.close()
+    # plain: one handle per box, stepped one after another
+    solvers = []
+    for bx, st in zip(boxes, states):
+        s = J.Solver(box_config(J, bx))
+        s.set_state(*st)
+        solvers.append(s)
+    for _ in range(warmup):
+        for s in solvers:
+            s.step(dt, H, 1.0, 1)
+    torch.cuda.synchronize()
+    dev_p, t0 = 0.0, time.perf_counter()
+    for _ in range(steps):
+        for s in solvers:
+            s.step(dt, H, 1.0, 1)
+            dev_p += s.timings()["total_ms"]
+    torch.cuda.synchronize()
+    wall_p = time.perf_counter() - t0
+    for s in solvers:
+        s.close()
+    v_b = n_part * steps / (dev * 1e-3)
+    v_p = n_part * steps / (dev_p * 1e-3)
+    return {
+        "workload": f"{n_boxes} boxes, n per species log-uniform 16..96 ({n_part} particles), "
+                    f"L U(50,300), PM 32..256, mu U(5,30)",
+        "value": v_b, "unit": UNIT, "ms_per_step": dev / steps,
+        "wall_value": n_part * steps / wall_b,
+        "plain_value": v_p, "plain_ms_per_step": dev_p / steps,
+        "plain_wall_value": n_part * steps / wall_p,
+        "speedup_vs_plain": v_b / v_p, "speedup_vs_plain_wall": wall_p / wall_b,
+        "launches_per_step": stages.get("launches", 0) / steps,
+        "stages_ms_per_step": {k: round(v / steps, 4) for k, v in stages.items() if k.endswith("_ms")},
+        "device_bytes": {"persistent": mem[0], "scratch": mem[1]},
+        "steps": steps,
+    }
+
+
 def run_reference(args, ws, rank):
     if rank != 0:
         return 0
@@ -277,6 +369,9 @@ def run_ours(args, ws, rank, local):
                          f"1/{args.cpu_sample_div} the side (same density, r_s, r_cut, "
                          f"eps, theta), {tcpu:.1f} s"}
     launches = stages.get("launches", 0)
+    ensemble = None
+    if rank == 0 and ws == 1 and args.ensemble_boxes > 0:
+        ensemble = run_ensemble(J, ics, args.ensemble_boxes, args.ensemble_steps, 3, H, w["dt"])
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K,
@@ -305,6 +400,7 @@ def run_ours(args, ws, rank, local):
             "clocks": clk,
             "gpu_launches": int(launches),
             "cpu_baseline": cpu,
+            "ensemble": ensemble,
         }
         print(json.dumps(line), flush=True)
     s.close()
@@ -323,6 +419,8 @@ def main():
     ap.add_argument("--grid", type=int, default=512)
     ap.add_argument("--cpu-sample-div", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ensemble-boxes", type=int, default=64)
+    ap.add_argument("--ensemble-steps", type=int, default=5)
     args = ap.parse_args()
     ws, rank, local = dist()
     if args.impl == "reference":

@@ -164,6 +164,11 @@ int  jt_debug_tree(jt_handle* h, int species, uint32_t* morton, int32_t* perm,
                    int32_t* left, int32_t* right, int32_t* parent);
 
 int  jt_get_timings(jt_handle* h, jt_timings* t);
+/* Walk phase counters accumulated since jt_create (traversal iterations,
+ * ranges streamed, candidate chunks, pair-loop trips); non-zero only in a
+ * diagnostic build compiled with -DJT_WALK_COUNT.  No counterpart in the
+ * reference. */
+int  jt_walk_counters(jt_handle* h, int64_t* out4);
 int  jt_counts(jt_handle* h, size_t* n_p, size_t* n_m);
 void jt_destroy(jt_handle* h);
 const char* jt_strerror(int code);
@@ -173,6 +178,53 @@ const char* jt_strerror(int code);
 int  jt_fp32_peak(int iters, double* tflops);
 /* Library version string, e.g. "janus-treepm-b200 0.1 sm_100a". */
 const char* jt_version(void);
+
+/* ---- batched ensembles ----
+ * A batch advances many independent boxes with one kernel launch per stage
+ * over the work of all chosen boxes, and one batched cuFFT R2C/C2R per
+ * distinct grid size.  It replaces the reference's one-process-per-box
+ * parameter scans (optim/run_tour.py:40-48, scripts/run_scan_mu.sh driving
+ * step_treepm_gpu once per box).  Boxes may differ in particle counts, box
+ * size, grid, theta, softening, r_s, r_cut, mu and step; all boxes of one
+ * batch share pm_order, pm_interlace and k_min, and must be JT_ACCURATE with
+ * JT_KDK.  Every call synchronises the batch's own stream before it returns. */
+typedef struct jt_batch jt_batch;
+
+/* Per-box step arguments of jt_batch_step (one entry per listed box). */
+typedef struct jt_step_args {
+    double dt;           /* step length */
+    double hubble;       /* H of the kick drag term v += (a - H v dtau) dt */
+    double dtau_per_dt;  /* the reference's dtau factor (step_treepm_gpu) */
+} jt_step_args;
+
+int  jt_batch_create(jt_batch** out);
+void jt_batch_destroy(jt_batch* b);
+/* Add one box (per-species arrays as jt_set_state); *box_id receives its id.
+ * JT_EINVAL if the config is not batchable or disagrees with the batch's
+ * shared fields; JT_ENOMEM if its state does not fit on the device. */
+int  jt_batch_add(jt_batch* b, const jt_config* cfg,
+                  const float* pos_p, const float* vel_p, size_t n_p,
+                  const float* pos_m, const float* vel_m, size_t n_m,
+                  int mem, int* box_id);
+/* Free one box's device state; its id may be reused by a later add. */
+int  jt_batch_remove(jt_batch* b, int box_id);
+/* Accelerations of the listed boxes at their current positions (JT_PART_*). */
+int  jt_batch_forces(jt_batch* b, const int* box_ids, int n_ids, int part);
+/* nsteps KDK steps of the listed boxes, args[k] for box_ids[k]. */
+int  jt_batch_step(jt_batch* b, const int* box_ids, int n_ids,
+                   const jt_step_args* args, int nsteps);
+/* Per-box read-back in the caller's species order (NULL pointers skipped). */
+int  jt_batch_get_accel(jt_batch* b, int box_id, float* acc_p, float* acc_m, int mem);
+int  jt_batch_get_state(jt_batch* b, int box_id, float* pos_p, float* vel_p,
+                        float* pos_m, float* vel_m, int mem);
+int  jt_batch_box_info(jt_batch* b, int box_id, size_t* n_p, size_t* n_m, size_t* bytes);
+/* Device bytes held: persistent box state, and the grow-only per-pass scratch. */
+int  jt_batch_memory(jt_batch* b, size_t* persistent, size_t* scratch);
+/* Device bytes one box would need (no device work): its persistent state and
+ * its share of the per-pass scratch.  The serving loop's admission control. */
+int  jt_batch_estimate(const jt_config* cfg, size_t n_p, size_t n_m,
+                       size_t* persistent, size_t* scratch);
+int  jt_batch_get_timings(jt_batch* b, jt_timings* t);
 
 #ifdef __cplusplus
 }

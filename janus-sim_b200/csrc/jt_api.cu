@@ -6,12 +6,15 @@
 // device after every launch; here nothing is global and a call synchronises
 // its own stream once, at the end).
 //
-// Force pipeline (jt_accel, and every step):
-//   per species: Morton keys -> onesweep sort -> reorder state -> Karras nodes
-//   -> bottom-up moments;  memset rho -> signed CIC deposit -> R2C -> fused
-//   k-space kernel -> batched C2R;  walk (PM interpolation + both trees, +
-//   kick in the accurate step).
-#include "jt_internal.cuh"
+// JT_ACCURATE handles are a batch of one box (jt_batch.cu): the same
+// one-launch-per-stage pipeline that advances ensembles, so a single box and a
+// box inside a batch run identical kernels.  JT_RCOMPAT handles keep the
+// reference's caller-order, 64-bit-key formulation here:
+//   per species: Morton keys (m30 << 32 | index) -> onesweep sort -> reorder
+//   -> Karras nodes -> cube moments;  memset rho -> CIC deposit in caller
+//   order -> R2C -> Green's function -> C2R (potential);  warp-uniform walk
+//   with finite-difference PM gradient.
+#include "jt_batch.h"
 
 #include <cmath>
 #include <cstdio>
@@ -47,8 +50,39 @@ struct jt_handle {
     unsigned* d_err = nullptr;
     unsigned long long* d_stats = nullptr;   // pairs, nodes, candidates
     jt_timings tm = {};
-    int64_t launches_per_force = 0;
+    int64_t phase[4] = {0, 0, 0, 0};   // walk phase counters of a diagnostic build
+    // JT_ACCURATE: the particle state lives in box `box_id` of `batch`
+    jt_batch* batch = nullptr;
+    int box_id = -1;
+    bool dbg_ready = false;            // debug-tree buffers (accurate mode)
 };
+
+namespace {
+
+// The particle arrays of a handle (internal order).  In accurate mode they
+// belong to the batch box and change after every force pass (the reorder
+// swaps buffers), so take a fresh view after each pass.
+struct Parts {
+    float4* pos[2];
+    float4* vel[2];
+    float4* acc[2];
+    int* id[2];
+};
+
+Parts parts_of(jt_handle* h)
+{
+    Parts p;
+    jt_box_state* b = h->batch ? jtb_box(h->batch, h->box_id) : nullptr;
+    for (int s = 0; s < 2; s++) {
+        p.pos[s] = b ? b->pos[s] : h->pos[s];
+        p.vel[s] = b ? b->vel[s] : h->vel[s];
+        p.acc[s] = b ? b->acc[s] : h->acc[s];
+        p.id[s] = b ? b->id[s] : h->id[s];
+    }
+    return p;
+}
+
+}  // namespace
 
 namespace {
 
@@ -104,36 +138,43 @@ int validate(const jt_config* c)
     return JT_OK;
 }
 
+void free_trees(jt_handle* h)
+{
+    for (int s = 0; s < 2; s++) {
+        jt_tree_dev& t = h->tree[s];
+        dfree(t.child); dfree(t.range); dfree(t.parent); dfree(t.flag); dfree(t.com); dfree(t.bmin);
+        dfree(t.bmax); dfree(t.quad0); dfree(t.quad1); dfree(t.m30); dfree(t.tie);
+        t = jt_tree_dev{};
+    }
+    jt_sort_ws_free(&h->ws);
+    dfree(h->key64);
+    h->dbg_ready = false;
+}
+
 void free_particles(jt_handle* h)
 {
     for (int s = 0; s < 2; s++) {
         dfree(h->pos[s]); dfree(h->vel[s]); dfree(h->acc[s]);
         dfree(h->pos_b[s]); dfree(h->vel_b[s]);
         dfree(h->id[s]); dfree(h->id_b[s]); dfree(h->gmap[s]);
-        jt_tree_dev& t = h->tree[s];
-        dfree(t.child); dfree(t.range); dfree(t.parent); dfree(t.flag); dfree(t.com); dfree(t.bmin);
-        dfree(t.bmax); dfree(t.quad0); dfree(t.quad1); dfree(t.m30); dfree(t.tie);
-        t = jt_tree_dev{};
         h->cap[s] = 0;
     }
-    jt_sort_ws_free(&h->ws);
-    dfree(h->key64);
+    free_trees(h);
+    if (h->batch && h->box_id >= 0) jt_batch_remove(h->batch, h->box_id);
+    h->box_id = -1;
     dfree(h->pos_caller); dfree(h->acc_caller); dfree(h->sign_caller); dfree(h->rank_buf);
     if (h->stage) cudaFree(h->stage);
     h->stage = nullptr;
     h->stage_bytes = 0;
 }
 
-int alloc_particles(jt_handle* h, int64_t n0, int64_t n1)
+// Trees, sort workspace and 64-bit keys for both species (RCOMPAT force
+// passes, and jt_debug_tree in either mode).
+int alloc_trees(jt_handle* h, int64_t n0, int64_t n1)
 {
-    if (h->stage && h->cap[0] == n0 && h->cap[1] == n1) return JT_OK;  // same sizes: reuse
-    free_particles(h);
     int64_t nn[2] = {n0, n1};
     for (int s = 0; s < 2; s++) {
         int64_t n = nn[s], nodes = n > 0 ? 2 * n - 1 : 1;
-        JT_TRY(dalloc(&h->pos[s], n)); JT_TRY(dalloc(&h->vel[s], n)); JT_TRY(dalloc(&h->acc[s], n));
-        JT_TRY(dalloc(&h->pos_b[s], n)); JT_TRY(dalloc(&h->vel_b[s], n));
-        JT_TRY(dalloc(&h->id[s], n)); JT_TRY(dalloc(&h->id_b[s], n)); JT_TRY(dalloc(&h->gmap[s], n));
         jt_tree_dev& t = h->tree[s];
         JT_TRY(dalloc(&t.child, nodes)); JT_TRY(dalloc(&t.parent, nodes));
         JT_TRY(dalloc(&t.range, n > 1 ? n - 1 : 1));
@@ -142,19 +183,49 @@ int alloc_particles(jt_handle* h, int64_t n0, int64_t n1)
         JT_TRY(dalloc(&t.quad0, nodes)); JT_TRY(dalloc(&t.quad1, nodes));
         JT_TRY(dalloc(&t.m30, n)); JT_TRY(dalloc(&t.tie, n));
         t.n = n;
-        h->cap[s] = n;
     }
     int64_t nmax = n0 > n1 ? n0 : n1;
     if (jt_sort_ws_alloc(&h->ws, nmax > 0 ? nmax : 1, 8) != 0) return JT_ENOMEM;
     JT_TRY(dalloc(&h->key64, nmax));
-    int64_t na = n0 + n1;
-    JT_TRY(dalloc(&h->pos_caller, na)); JT_TRY(dalloc(&h->acc_caller, na));
-    JT_TRY(dalloc(&h->sign_caller, na)); JT_TRY(dalloc(&h->rank_buf, na));
-    h->stage_bytes = sizeof(float) * 3 * (size_t)(na > 0 ? na : 1) * 2;
-    if (!cuda_ok(cudaMalloc(&h->stage, h->stage_bytes))) return JT_ENOMEM;
+    h->dbg_ready = true;
     return JT_OK;
 }
 
+int alloc_particles(jt_handle* h, int64_t n0, int64_t n1)
+{
+    if (h->stage && h->cap[0] == n0 && h->cap[1] == n1) {  // same sizes: reuse
+        if (h->batch) {
+            jt_box_state* b = jtb_box(h->batch, h->box_id);
+            if (b) b->acc_valid = false;
+        }
+        return JT_OK;
+    }
+    free_particles(h);
+    int64_t nn[2] = {n0, n1};
+    for (int s = 0; s < 2; s++) JT_TRY(dalloc(&h->gmap[s], nn[s]));
+    if (h->batch) {
+        JT_TRY(jtb_add_empty(h->batch, &h->cfg, n0, n1, &h->box_id));
+    } else {
+        for (int s = 0; s < 2; s++) {
+            int64_t n = nn[s];
+            JT_TRY(dalloc(&h->pos[s], n)); JT_TRY(dalloc(&h->vel[s], n)); JT_TRY(dalloc(&h->acc[s], n));
+            JT_TRY(dalloc(&h->pos_b[s], n)); JT_TRY(dalloc(&h->vel_b[s], n));
+            JT_TRY(dalloc(&h->id[s], n)); JT_TRY(dalloc(&h->id_b[s], n));
+        }
+        JT_TRY(alloc_trees(h, n0, n1));
+    }
+    int64_t na = n0 + n1;
+    JT_TRY(dalloc(&h->pos_caller, h->batch ? 1 : na)); JT_TRY(dalloc(&h->acc_caller, h->batch ? 1 : na));
+    JT_TRY(dalloc(&h->sign_caller, na)); JT_TRY(dalloc(&h->rank_buf, na));
+    h->stage_bytes = sizeof(float) * 3 * (size_t)(na > 0 ? na : 1) * 2;
+    if (!cuda_ok(cudaMalloc(&h->stage, h->stage_bytes))) return JT_ENOMEM;
+    h->cap[0] = n0;
+    h->cap[1] = n1;
+    return JT_OK;
+}
+
+// RCOMPAT PM: one CIC grid, its spectrum (Green's function applied in
+// place) and the potential grid.
 int alloc_pm(jt_handle* h)
 {
     jt_pm_dev& pm = h->pm;
@@ -162,53 +233,20 @@ int alloc_pm(jt_handle* h)
     int M = c.pm_grid;
     pm.M = M;
     pm.L = c.box_L;
-    bool rc = c.mode == JT_RCOMPAT;
-    pm.order = rc ? 2 : (c.pm_order == 0 ? 3 : c.pm_order);
-    pm.ngrid = rc ? 1 : (c.pm_interlace == 2 ? 1 : 2);
+    pm.order = 2;
+    pm.ngrid = 1;
     int64_t G = (int64_t)M * M * M, Gc = (int64_t)M * M * (M / 2 + 1);
-    int NG = pm.ngrid;
-    JT_TRY(dalloc(&pm.rho, NG * G));
-    if (!rc) JT_TRY(dalloc(&pm.rho_k, NG * Gc));
-    // accurate: 3*NG spectra + two per-axis tables (2M float4 = 4M complex)
-    JT_TRY(dalloc(&pm.force_k, rc ? Gc : 3 * NG * Gc + 4 * (int64_t)M));
-    JT_TRY(dalloc(&pm.force, rc ? G : 3 * NG * G));
-    int T = jt_pm_tile_edge(M);
-    int64_t ntiles = (int64_t)(M / T) * (M / T) * (M / T);
-    JT_TRY(dalloc(&pm.ranges, ntiles));
-    int dims[3] = {M, M, M};
-    if (rc) {
-        JT_FFT(cufftPlan3d(&pm.plan_r2c, M, M, M, CUFFT_R2C));
-        JT_FFT(cufftPlan3d(&pm.plan_c2r, M, M, M, CUFFT_C2R));
-    } else {
-        JT_FFT(cufftPlanMany(&pm.plan_r2c, 3, dims, nullptr, 1, (int)G, nullptr, 1, (int)Gc,
-                             CUFFT_R2C, NG));
-        JT_FFT(cufftPlanMany(&pm.plan_c2r, 3, dims, nullptr, 1, (int)Gc, nullptr, 1, (int)G,
-                             CUFFT_C2R, 3 * NG));
-        // per-axis tables: ta = {k, gradient k (0 at Nyquist), exp(-k^2 r_s^2)/sinc^(2 order), |n|}
-        //                  tb = {cos(k h/2), sin(k h/2), 0, 0}
-        std::vector<float> tab(8 * (size_t)M);
-        double dk = 2.0 * M_PI / c.box_L, rs = c.r_s, hh = c.box_L / M;
-        for (int n = 0; n < M; n++) {
-            int ni = n <= M / 2 ? n : n - M;
-            double k = dk * ni;
-            double u = M_PI * ni / M;
-            double sinc = ni == 0 ? 1.0 : std::sin(u) / u;
-            double f = std::exp(-k * k * rs * rs) / std::pow(sinc, 2.0 * pm.order);
-            tab[4 * n] = (float)k;
-            tab[4 * n + 1] = (n == M / 2) ? 0.0f : (float)k;
-            tab[4 * n + 2] = (float)f;
-            tab[4 * n + 3] = (float)(ni < 0 ? -ni : ni);
-            tab[4 * (M + n)] = (float)std::cos(0.5 * k * hh);
-            tab[4 * (M + n) + 1] = (float)std::sin(0.5 * k * hh);
-            tab[4 * (M + n) + 2] = 0.0f;
-            tab[4 * (M + n) + 3] = 0.0f;
-        }
-        pm.tabs = reinterpret_cast<float4*>(pm.force_k + 3 * NG * Gc);
-        JT_CU(cudaMemcpy(pm.tabs, tab.data(), sizeof(float) * tab.size(), cudaMemcpyHostToDevice));
+    JT_TRY(dalloc(&pm.rho, G));
+    JT_TRY(dalloc(&pm.force_k, Gc));
+    JT_TRY(dalloc(&pm.force, G));
+    JT_FFT(cufftPlan3d(&pm.plan_r2c, M, M, M, CUFFT_R2C));
+    if (cufftPlan3d(&pm.plan_c2r, M, M, M, CUFFT_C2R) != CUFFT_SUCCESS) {
+        cufftDestroy(pm.plan_r2c);
+        return JT_ECUDA;
     }
+    pm.plans_ready = 1;
     JT_FFT(cufftSetStream(pm.plan_r2c, h->st));
     JT_FFT(cufftSetStream(pm.plan_c2r, h->st));
-    pm.plans_ready = 1;
     return JT_OK;
 }
 
@@ -219,7 +257,7 @@ void free_pm(jt_handle* h)
         cufftDestroy(pm.plan_r2c);
         cufftDestroy(pm.plan_c2r);
     }
-    dfree(pm.rho); dfree(pm.rho_k); dfree(pm.force_k); dfree(pm.force); dfree(pm.ranges);
+    dfree(pm.rho); dfree(pm.force_k); dfree(pm.force);
     pm = jt_pm_dev{};
 }
 
@@ -230,43 +268,38 @@ int id_bits(int64_t n)
     return b;
 }
 
-// Sort both species by Morton key, reorder the state, build both trees.
-// rc_keys: the reference's 64-bit keys (m30 << 32 | caller index), else m30.
-int build_trees(jt_handle* h, bool rc_keys, bool rc_nodes)
+// RCOMPAT: sort both species by the reference's 64-bit Morton key
+// (m30 << 32 | caller index), reorder the state, build both trees with the
+// reference's cube node geometry.
+int build_trees(jt_handle* h)
 {
     float box_half = (float)(h->cfg.box_L / 2.0);
     for (int s = 0; s < 2; s++) {
         int64_t n = h->n[s];
         if (n == 0) continue;
         jt_tree_dev& t = h->tree[s];
-        if (rc_keys) {
-            jt_launch_morton(h->pos[s], h->id[s], n, box_half, nullptr, h->key64, h->ws.vals, h->st);
-            int shifts[8], np = 0;
-            int ib = id_bits(n);
-            for (int b = 0; b < ib; b += 8) shifts[np++] = b;
-            for (int b = 32; b < 62; b += 8) shifts[np++] = b;
-            JT_TRY(jt_radix_sort_u64(h->key64, h->ws.vals, n, shifts, np, &h->ws, h->d_err, h->st));
-            jt_launch_split_keys(h->key64, n, t.m30, t.tie, h->st);
-        } else {
-            jt_launch_morton(h->pos[s], h->id[s], n, box_half, t.m30, nullptr, h->ws.vals, h->st);
-            const int shifts[4] = {0, 8, 16, 24};
-            JT_TRY(jt_radix_sort_u32(t.m30, h->ws.vals, n, shifts, 4, &h->ws, h->d_err, h->st));
-        }
+        jt_launch_morton(h->pos[s], h->id[s], n, box_half, nullptr, h->key64, h->ws.vals, h->st);
+        int shifts[8], np = 0;
+        int ib = id_bits(n);
+        for (int b = 0; b < ib; b += 8) shifts[np++] = b;
+        for (int b = 32; b < 62; b += 8) shifts[np++] = b;
+        JT_TRY(jt_radix_sort_u64(h->key64, h->ws.vals, n, shifts, np, &h->ws, h->d_err, h->st));
+        jt_launch_split_keys(h->key64, n, t.m30, t.tie, h->st);
         jt_launch_reorder(h->ws.vals, n, h->pos[s], h->pos_b[s], h->vel[s], h->vel_b[s], h->id[s],
                           h->id_b[s], h->st);
         std::swap(h->pos[s], h->pos_b[s]);
         std::swap(h->vel[s], h->vel_b[s]);
         std::swap(h->id[s], h->id_b[s]);
         t.n = n;
+        h->tm.launches += 5 + np;   // morton, hist, scan, np onesweep passes, split, reorder
     }
     cudaEventRecord(h->ev[1], h->st);
     for (int s = 0; s < 2; s++) {
         int64_t n = h->n[s];
         if (n == 0) continue;
-        jt_tree_dev tk = h->tree[s];
-        if (!rc_keys) tk.tie = nullptr;  // tie = sorted position
-        jt_launch_karras(tk, h->st);
-        jt_launch_moments(h->tree[s], h->pos[s], h->mass[s], box_half, rc_nodes ? 1 : 0, h->st);
+        jt_launch_karras(h->tree[s], h->st);
+        jt_launch_moments_rc(h->tree[s], h->pos[s], h->mass[s], box_half, h->st);
+        h->tm.launches += (n > 1 ? 1 : 0) + 1;
     }
     return cudaGetLastError() == cudaSuccess ? JT_OK : JT_ECUDA;
 }
@@ -292,108 +325,70 @@ float elapsed(cudaEvent_t a, cudaEvent_t b)
     return ms;
 }
 
-// Compute accelerations at the current positions into acc[s] (internal order).
-// kick_dt/drag: closing kick fused into the accurate walk (0 = none).
-int compute_forces(jt_handle* h, float kick_dt, float drag, int parts = JT_PART_ALL)
+// RCOMPAT accelerations at the current positions into acc[s] (internal
+// order); kick_dt/drag: a kick applied after the walk (0 = none).
+int compute_forces_rc(jt_handle* h, float kick_dt, float drag, int parts = JT_PART_ALL)
 {
     const jt_config& c = h->cfg;
-    const bool rc = c.mode == JT_RCOMPAT;
     cudaStream_t st = h->st;
     int M = c.pm_grid;
     int64_t G = (int64_t)M * M * M;
     cudaEventRecord(h->ev[0], st);
-    JT_TRY(build_trees(h, rc, rc));
+    JT_TRY(build_trees(h));
     cudaEventRecord(h->ev[2], st);
-    JT_CU(cudaMemsetAsync(h->pm.rho, 0, sizeof(float) * G * h->pm.ngrid, st));
-    if (rc) {
-        for (int s = 0; s < 2; s++)
-            jt_launch_to_caller(h->pos[s], h->id[s], h->gmap[s], h->n[s], h->pos_caller, st);
-        double cell = c.box_L / M;
-        jt_launch_rcompat_deposit(h->pos_caller, h->sign_caller, h->n[0] + h->n[1], h->mass,
-                                  h->pm.rho, M, (float)(c.box_L / 2.0), (float)(M / c.box_L),
-                                  (float)(1.0 / (cell * cell * cell)), st);
-    } else {
-        double h3 = std::pow(c.box_L / M, 3.0);
-        jt_launch_tile_ranges(h->tree[0].m30, h->n[0], h->tree[1].m30, h->n[1], M, h->pm.ranges, st);
-        JT_TRY(jt_launch_deposit_tiled(h->pos[0], (float)(h->mass[0] / h3), h->pos[1],
-                                       (float)(-h->mass[1] / h3), h->pm.ranges, h->pm.rho, M,
-                                       (float)c.box_L, h->pm.order, h->pm.ngrid, st));
-    }
+    JT_CU(cudaMemsetAsync(h->pm.rho, 0, sizeof(float) * G, st));
+    for (int s = 0; s < 2; s++)
+        jt_launch_to_caller(h->pos[s], h->id[s], h->gmap[s], h->n[s], h->pos_caller, st);
+    double cell = c.box_L / M;
+    jt_launch_rcompat_deposit(h->pos_caller, h->sign_caller, h->n[0] + h->n[1], h->mass, h->pm.rho, M,
+                              (float)(c.box_L / 2.0), (float)(M / c.box_L),
+                              (float)(1.0 / (cell * cell * cell)), st);
     cudaEventRecord(h->ev[3], st);
-    if (rc) {
-        JT_FFT(cufftExecR2C(h->pm.plan_r2c, h->pm.rho, h->pm.force_k));
-        cudaEventRecord(h->ev[4], st);
-        jt_launch_kspace(nullptr, h->pm.force_k, M, c.box_L, c.r_cut / 3.0, c.k_min, 1, 0, nullptr, st);
-        cudaEventRecord(h->ev[5], st);
-        JT_FFT(cufftExecC2R(h->pm.plan_c2r, h->pm.force_k, h->pm.force));
-    } else {
-        JT_FFT(cufftExecR2C(h->pm.plan_r2c, h->pm.rho, h->pm.rho_k));
-        cudaEventRecord(h->ev[4], st);
-        jt_launch_kspace(h->pm.rho_k, h->pm.force_k, M, c.box_L, c.r_s, c.k_min, 0,
-                         h->pm.ngrid == 2, h->pm.tabs, st);
-        cudaEventRecord(h->ev[5], st);
-        JT_FFT(cufftExecC2R(h->pm.plan_c2r, h->pm.force_k, h->pm.force));
-    }
+    JT_FFT(cufftExecR2C(h->pm.plan_r2c, h->pm.rho, h->pm.force_k));
+    cudaEventRecord(h->ev[4], st);
+    jt_launch_kspace_rc(h->pm.force_k, M, c.box_L, c.r_cut / 3.0, c.k_min, st);
+    cudaEventRecord(h->ev[5], st);
+    JT_FFT(cufftExecC2R(h->pm.plan_c2r, h->pm.force_k, h->pm.force));
     cudaEventRecord(h->ev[6], st);
-    if (rc) {
-        float tq, sq, rq, bq;
-        {
-            // host packing of the reference (:4079-4082, :1932-1937) and the
-            // kernel's unpacking (:1684-1694)
-            auto sat = [](double v) -> unsigned {
-                return v <= 0.0 ? 0u : (v >= 4294967295.0 ? 0xFFFFFFFFu : (unsigned)v);
-            };
-            unsigned ti = sat(c.theta * 1000.0), si = sat(c.softening * 1000.0);
-            unsigned ri = sat(c.r_cut), bi = sat(c.box_L / 2.0);
-            ti = ti > 0xFFFF ? 0xFFFF : ti; si = si > 0xFFFF ? 0xFFFF : si;
-            ri = ri > 0xFFFF ? 0xFFFF : ri; bi = bi > 0xFFFF ? 0xFFFF : bi;
-            tq = (float)ti / 1000.0f; sq = (float)si / 1000.0f; rq = (float)ri; bq = (float)bi;
-        }
-        jt_rc_params P;
-        P.theta2 = tq * tq;
-        P.eps2 = sq * sq;
-        P.r_cut = rq;
-        P.box_half_q = bq;
-        P.r_s = rq / 3.0f;
-        P.box_half = (float)(c.box_L / 2.0);
-        P.inv_cell = (float)(M / c.box_L);
-        P.cell = (float)(c.box_L / M);
-        P.M = M;
-        P.mass[0] = h->mass[0];
-        P.mass[1] = h->mass[1];
-        P.parts = parts;
-        const float4* sp2[2] = {h->pos[0], h->pos[1]};
-        jt_launch_walk_rcompat(P, h->pos_caller, h->sign_caller, h->n[0] + h->n[1], sp2, h->n,
-                               h->tree, h->pm.force, h->acc_caller, h->d_err, st);
-        for (int s = 0; s < 2; s++)
-            jt_launch_from_caller(h->acc_caller, h->id[s], h->gmap[s], h->n[s], h->acc[s], st);
-        if (kick_dt != 0.0f)
-            for (int s = 0; s < 2; s++) jt_launch_kick(h->vel[s], h->acc[s], h->n[s], kick_dt, drag, st);
-    } else {
-        jt_walk_params P;
-        P.L = (float)c.box_L;
-        P.halfL = (float)(c.box_L / 2.0);
-        P.theta2 = (float)(c.theta * c.theta);
-        P.rc = (float)c.r_cut;
-        P.rc2 = (float)(c.r_cut * c.r_cut);
-        P.eps2 = (float)(c.softening * c.softening);
-        P.c = (float)(1.0 / (2.0 * c.r_s));
-        P.mass[0] = h->mass[0];
-        P.mass[1] = h->mass[1];
-        P.M = M;
-        P.h_inv = (float)(M / c.box_L);
-        P.order = h->pm.order;
-        P.ngrid = h->pm.ngrid;
-        P.parts = parts;
-        const float4* p2[2] = {h->pos[0], h->pos[1]};
-        float4* a2[2] = {h->acc[0], h->acc[1]};
-        float4* v2[2] = {h->vel[0], h->vel[1]};
-        jt_launch_walk_accurate(P, p2, h->n, h->tree, h->pm.force, a2, v2, kick_dt, drag,
-                                h->d_stats, h->d_err, st);
+    float tq, sq, rq, bq;
+    {
+        // host packing of the reference (:4079-4082, :1932-1937) and the
+        // kernel's unpacking (:1684-1694)
+        auto sat = [](double v) -> unsigned {
+            return v <= 0.0 ? 0u : (v >= 4294967295.0 ? 0xFFFFFFFFu : (unsigned)v);
+        };
+        unsigned ti = sat(c.theta * 1000.0), si = sat(c.softening * 1000.0);
+        unsigned ri = sat(c.r_cut), bi = sat(c.box_L / 2.0);
+        ti = ti > 0xFFFF ? 0xFFFF : ti; si = si > 0xFFFF ? 0xFFFF : si;
+        ri = ri > 0xFFFF ? 0xFFFF : ri; bi = bi > 0xFFFF ? 0xFFFF : bi;
+        tq = (float)ti / 1000.0f; sq = (float)si / 1000.0f; rq = (float)ri; bq = (float)bi;
     }
+    jt_rc_params P;
+    P.theta2 = tq * tq;
+    P.eps2 = sq * sq;
+    P.r_cut = rq;
+    P.box_half_q = bq;
+    P.r_s = rq / 3.0f;
+    P.box_half = (float)(c.box_L / 2.0);
+    P.inv_cell = (float)(M / c.box_L);
+    P.cell = (float)(c.box_L / M);
+    P.M = M;
+    P.mass[0] = h->mass[0];
+    P.mass[1] = h->mass[1];
+    P.parts = parts;
+    const float4* sp2[2] = {h->pos[0], h->pos[1]};
+    jt_launch_walk_rcompat(P, h->pos_caller, h->sign_caller, h->n[0] + h->n[1], sp2, h->n, h->tree,
+                           h->pm.force, h->acc_caller, h->d_err, st);
+    for (int s = 0; s < 2; s++)
+        jt_launch_from_caller(h->acc_caller, h->id[s], h->gmap[s], h->n[s], h->acc[s], st);
+    if (kick_dt != 0.0f)
+        for (int s = 0; s < 2; s++) jt_launch_kick(h->vel[s], h->acc[s], h->n[s], kick_dt, drag, st);
     cudaEventRecord(h->ev[7], st);
     JT_CU(cudaGetLastError());
-    h->acc_valid = true;
+    const int nsp = (h->n[0] > 0) + (h->n[1] > 0);
+    // to_caller, from_caller (and kick) per species; deposit, k-space, walk
+    h->tm.launches += (kick_dt != 0.0f ? 3 : 2) * nsp + 3;
+    h->acc_valid = parts == JT_PART_ALL;
     return JT_OK;
 }
 
@@ -411,13 +406,14 @@ void accumulate_timings(jt_handle* h)
 
 int fetch_inter(jt_handle* h)
 {
-    unsigned long long v[3] = {0, 0, 0};
+    unsigned long long v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     JT_CU(cudaMemcpyAsync(v, h->d_stats, sizeof(v), cudaMemcpyDeviceToHost, h->st));
     JT_CU(cudaStreamSynchronize(h->st));
     h->tm.pair_interactions += (int64_t)v[0];
     h->tm.node_interactions += (int64_t)v[1];
     h->tm.candidates += (int64_t)v[2];
     h->tm.interactions += (int64_t)(v[0] + v[1]);
+    for (int i = 0; i < 4; i++) h->phase[i] += (int64_t)v[3 + i];
     JT_CU(cudaMemsetAsync(h->d_stats, 0, sizeof(v), h->st));
     return JT_OK;
 }
@@ -485,18 +481,30 @@ int jt_create(const jt_config* cfg, jt_handle** out)
     if (!h) return JT_ENOMEM;
     h->cfg = *cfg;
     int r = JT_OK;
-    if (cudaGetDevice(&h->device) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaGetDevice(&h->device) != cudaSuccess) {
+        delete h;
+        return JT_ECUDA;
+    }
+    if (cfg->mode == JT_ACCURATE) {
+        // a batch of one box; the handle issues its own launches on the
+        // batch's stream so that everything stays in stream order
+        r = jt_batch_create(&h->batch);
+        if (r != JT_OK) {
+            delete h;
+            return r;
+        }
+        h->st = jtb_stream(h->batch);
+    } else if (cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking) != cudaSuccess) {
         delete h;
         return JT_ECUDA;
     }
     for (auto& e : h->ev) cudaEventCreate(&e);
     if (cudaMalloc(&h->d_err, sizeof(unsigned)) != cudaSuccess ||
-        cudaMalloc(&h->d_stats, 3 * sizeof(unsigned long long)) != cudaSuccess) r = JT_ENOMEM;
+        cudaMalloc(&h->d_stats, 8 * sizeof(unsigned long long)) != cudaSuccess) r = JT_ENOMEM;
     if (r == JT_OK) {
         cudaMemset(h->d_err, 0, sizeof(unsigned));
-        cudaMemset(h->d_stats, 0, 3 * sizeof(unsigned long long));
-        r = alloc_pm(h);
+        cudaMemset(h->d_stats, 0, 8 * sizeof(unsigned long long));
+        if (!h->batch) r = alloc_pm(h);
     }
     if (r != JT_OK) {
         jt_destroy(h);
@@ -516,7 +524,11 @@ void jt_destroy(jt_handle* h)
     if (h->d_stats) cudaFree(h->d_stats);
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
-    if (h->st) cudaStreamDestroy(h->st);
+    if (h->batch) {
+        jt_batch_destroy(h->batch);   // owns the stream
+    } else if (h->st) {
+        cudaStreamDestroy(h->st);
+    }
     delete h;
 }
 
@@ -533,6 +545,7 @@ int jt_set_state(jt_handle* h, const float* pos_p, const float* vel_p, size_t n_
     h->n[0] = (int64_t)n_p;
     h->n[1] = (int64_t)n_m;
     set_masses(h);
+    const Parts P = parts_of(h);
     const float* pp[2] = {pos_p, pos_m};
     const float* vv[2] = {vel_p, vel_m};
     for (int s = 0; s < 2; s++) {
@@ -540,12 +553,12 @@ int jt_set_state(jt_handle* h, const float* pos_p, const float* vel_p, size_t n_
         if (n == 0) continue;
         void* d = nullptr;
         JT_TRY(copy_in(h, pp[s], sizeof(float) * 3 * n, mem, &d));
-        jt_launch_aos_in((const float*)d, n, h->pos[s], h->id[s], h->st);
+        jt_launch_aos_in((const float*)d, n, P.pos[s], P.id[s], h->st);
         if (vv[s]) {
             JT_TRY(copy_in(h, vv[s], sizeof(float) * 3 * n, mem, &d));
-            jt_launch_aos_in((const float*)d, n, h->vel[s], nullptr, h->st);
+            jt_launch_aos_in((const float*)d, n, P.vel[s], nullptr, h->st);
         } else {
-            JT_CU(cudaMemsetAsync(h->vel[s], 0, sizeof(float4) * n, h->st));
+            JT_CU(cudaMemsetAsync(P.vel[s], 0, sizeof(float4) * n, h->st));
         }
         // caller layout: [m+ ; m-]
         std::vector<int> g(n);
@@ -558,6 +571,7 @@ int jt_set_state(jt_handle* h, const float* pos_p, const float* vel_p, size_t n_
     if (!sg.empty())
         JT_CU(cudaMemcpyAsync(h->sign_caller, sg.data(), sg.size(), cudaMemcpyHostToDevice, h->st));
     JT_CU(cudaStreamSynchronize(h->st));
+    JT_CU(cudaGetLastError());
     h->signed_layout = false;
     h->have_state = true;
     return JT_OK;
@@ -601,14 +615,49 @@ int jt_set_state_signed(jt_handle* h, const float* pos, const float* vel, const 
             dvel = stg + 3 * n;
         }
     }
-    jt_launch_split_signed(dpos, dvel, h->sign_caller, (int64_t)n, h->rank_buf, h->pos[0], h->vel[0],
-                           h->id[0], h->gmap[0], h->pos[1], h->vel[1], h->id[1], h->gmap[1], h->st);
+    const Parts P = parts_of(h);
+    jt_launch_split_signed(dpos, dvel, h->sign_caller, (int64_t)n, h->rank_buf, P.pos[0], P.vel[0],
+                           P.id[0], h->gmap[0], P.pos[1], P.vel[1], P.id[1], h->gmap[1], h->st);
     JT_CU(cudaStreamSynchronize(h->st));
     JT_CU(cudaGetLastError());
     h->signed_layout = true;
     h->have_state = true;
     return JT_OK;
 }
+
+namespace {
+
+// One force evaluation at the current positions (no kick), any mode.
+int force_only(jt_handle* h, int part)
+{
+    if (h->batch) {
+        jtb_reset_timings(h->batch);
+        return jtb_force_pass(h->batch, &h->box_id, 1, part, 0.0f, nullptr);
+    }
+    return compute_forces_rc(h, 0.0f, 0.0f, part);
+}
+
+// Wait for the call's work, read the device error word, collect timings.
+int finish_call(jt_handle* h, int r, cudaEvent_t t0, cudaEvent_t t1)
+{
+    int e;
+    if (h->batch) {
+        e = jtb_finish(h->batch);
+        if (e == JT_OK) jt_batch_get_timings(h->batch, &h->tm);
+        for (int i = 0; i < 4; i++) h->phase[i] = jtb_phase(h->batch, i);
+    } else {
+        e = check_device_error(h);
+        if (e == JT_OK) {
+            accumulate_timings(h);
+            fetch_inter(h);
+        }
+    }
+    if (r == JT_OK) r = e;
+    if (r == JT_OK && t0 && t1) h->tm.total_ms = elapsed(t0, t1);
+    return r;
+}
+
+}  // namespace
 
 int jt_accel(jt_handle* h, float* acc_p, float* acc_m, int mem)
 {
@@ -620,32 +669,27 @@ int jt_accel_part(jt_handle* h, int part, float* acc_p, float* acc_m, int mem)
     if (!h || (mem != JT_MEM_HOST && mem != JT_MEM_DEVICE)) return JT_EINVAL;
     if (part < 1 || part > 3) return JT_EINVAL;
     if (!h->have_state) return JT_ESTATE;
+    if (h->signed_layout) return JT_EINVAL;  // state loaded with the signed layout: jt_accel_signed
     h->tm = jt_timings{};
     cudaEvent_t t0, t1;
     cudaEventCreate(&t0);
     cudaEventCreate(&t1);
     cudaEventRecord(t0, h->st);
-    int r = compute_forces(h, 0.0f, 0.0f, part);
-    if (part != JT_PART_ALL) h->acc_valid = false;
+    int r = force_only(h, part);
+    cudaEventRecord(t1, h->st);
     if (r == JT_OK) {
-        if (!h->signed_layout) {
-            r = write_out(h, h->acc[0], h->id[0], nullptr, h->n[0], acc_p, mem);
-            if (r == JT_OK) {
-                // the host path reuses the staging buffer: finish the first copy
-                if (mem == JT_MEM_HOST) cudaStreamSynchronize(h->st);
-                r = write_out(h, h->acc[1], h->id[1], nullptr, h->n[1], acc_m, mem);
-            }
-        } else {
-            r = JT_EINVAL;  // state loaded with the signed layout: use jt_accel_signed
+        const Parts P = parts_of(h);
+        r = write_out(h, P.acc[0], P.id[0], nullptr, h->n[0], acc_p, mem);
+        if (r == JT_OK) {
+            // the host path reuses the staging buffer: finish the first copy
+            if (mem == JT_MEM_HOST) cudaStreamSynchronize(h->st);
+            r = write_out(h, P.acc[1], P.id[1], nullptr, h->n[1], acc_m, mem);
         }
     }
-    cudaEventRecord(t1, h->st);
-    int e = check_device_error(h);
-    if (r == JT_OK) r = e;
-    if (r == JT_OK) {
-        accumulate_timings(h);
-        h->tm.total_ms = elapsed(t0, t1);
-        fetch_inter(h);
+    r = finish_call(h, r, t0, t1);
+    if (part != JT_PART_ALL) {
+        h->acc_valid = false;
+        if (h->batch) jtb_box(h->batch, h->box_id)->acc_valid = false;
     }
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
@@ -657,22 +701,16 @@ int jt_accel_signed(jt_handle* h, float* acc, int mem)
     if (!h || !acc || (mem != JT_MEM_HOST && mem != JT_MEM_DEVICE)) return JT_EINVAL;
     if (!h->have_state) return JT_ESTATE;
     h->tm = jt_timings{};
-    int r = compute_forces(h, 0.0f, 0.0f);
+    int r = force_only(h, JT_PART_ALL);
     if (r == JT_OK) {
+        const Parts P = parts_of(h);
         int64_t na = h->n[0] + h->n[1];
         float* target = mem == JT_MEM_DEVICE ? acc : (float*)h->stage;
-        for (int s = 0; s < 2; s++)
-            jt_launch_aos_out(h->acc[s], h->id[s], h->gmap[s], h->n[s], target, h->st);
+        for (int s = 0; s < 2; s++) jt_launch_aos_out(P.acc[s], P.id[s], h->gmap[s], h->n[s], target, h->st);
         if (mem == JT_MEM_HOST)
             cudaMemcpyAsync(acc, h->stage, sizeof(float) * 3 * na, cudaMemcpyDeviceToHost, h->st);
     }
-    int e = check_device_error(h);
-    if (r == JT_OK) r = e;
-    if (r == JT_OK) {
-        accumulate_timings(h);
-        fetch_inter(h);
-    }
-    return r;
+    return finish_call(h, r, nullptr, nullptr);
 }
 
 int jt_step(jt_handle* h, double dt, double hubble, double dtau_per_dt, int nsteps)
@@ -683,20 +721,43 @@ int jt_step(jt_handle* h, double dt, double hubble, double dtau_per_dt, int nste
     if (nsteps == 0) return JT_OK;
     h->tm = jt_timings{};
     const jt_config& c = h->cfg;
+    if (h->batch && c.integrator == JT_KDK) {
+        jt_step_args a;
+        a.dt = dt;
+        a.hubble = hubble;
+        a.dtau_per_dt = dtau_per_dt;
+        int r = jt_batch_step(h->batch, &h->box_id, 1, &a, nsteps);
+        jt_batch_get_timings(h->batch, &h->tm);
+        for (int i = 0; i < 4; i++) h->phase[i] = jtb_phase(h->batch, i);
+        return r;
+    }
     // FP64 step factors, applied in FP32
     const double drag_d = hubble * dtau_per_dt;
     const float drag = (float)drag_d;
     const float L = (float)c.box_L, halfL = (float)(c.box_L / 2.0);
+    const float half = (float)(0.5 * dt), full = (float)dt;
     cudaEvent_t t0, t1, k0, k1;
     cudaEventCreate(&t0); cudaEventCreate(&t1); cudaEventCreate(&k0); cudaEventCreate(&k1);
     cudaEventRecord(t0, h->st);
     int r = JT_OK;
     double kd_ms = 0.0;
+    jt_timings acc_tm = {};
+    auto add_pass = [&](void) {
+        // stage times of one force pass (batch timings are per pass)
+        if (!h->batch) return;
+        jt_timings t;
+        jt_batch_get_timings(h->batch, &t);
+        acc_tm.sort_ms += t.sort_ms; acc_tm.tree_ms += t.tree_ms; acc_tm.deposit_ms += t.deposit_ms;
+        acc_tm.fft_ms += t.fft_ms; acc_tm.kspace_ms += t.kspace_ms; acc_tm.walk_ms += t.walk_ms;
+        acc_tm.interactions += t.interactions; acc_tm.launches += t.launches;
+        acc_tm.pair_interactions += t.pair_interactions; acc_tm.node_interactions += t.node_interactions;
+        acc_tm.candidates += t.candidates;
+    };
     if (c.integrator == JT_KDK) {
-        const float half = (float)(0.5 * dt), full = (float)dt;
+        // RCOMPAT kick-drift-kick (the accurate handle went through the batch)
         if (!h->acc_valid) {
-            r = compute_forces(h, 0.0f, 0.0f);
-            if (r == JT_OK) { r = check_device_error(h); if (r == JT_OK) accumulate_timings(h); }
+            r = compute_forces_rc(h, 0.0f, 0.0f);
+            if (r == JT_OK) r = finish_call(h, r, nullptr, nullptr);
         }
         for (int k = 0; k < nsteps && r == JT_OK; k++) {
             cudaEventRecord(k0, h->st);
@@ -705,39 +766,38 @@ int jt_step(jt_handle* h, double dt, double hubble, double dtau_per_dt, int nste
                 jt_launch_drift(h->pos[s], h->vel[s], h->n[s], full, L, halfL, h->st);
             }
             cudaEventRecord(k1, h->st);
-            r = compute_forces(h, half, drag);
+            r = compute_forces_rc(h, half, drag);
             if (r != JT_OK) break;
-            r = check_device_error(h);
-            if (r != JT_OK) break;
-            accumulate_timings(h);
+            r = finish_call(h, r, nullptr, nullptr);
             kd_ms += elapsed(k0, k1);
         }
     } else {
-        const float half = (float)(0.5 * dt), full = (float)dt;
+        // the reference's drift(dt/2) force kick(dt) drift(dt/2)
         for (int k = 0; k < nsteps && r == JT_OK; k++) {
             cudaEventRecord(k0, h->st);
-            for (int s = 0; s < 2; s++)
-                jt_launch_drift(h->pos[s], h->vel[s], h->n[s], half, L, halfL, h->st);
+            Parts P = parts_of(h);
+            for (int s = 0; s < 2; s++) jt_launch_drift(P.pos[s], P.vel[s], h->n[s], half, L, halfL, h->st);
             cudaEventRecord(k1, h->st);
-            r = compute_forces(h, 0.0f, 0.0f);
+            r = force_only(h, JT_PART_ALL);
             if (r != JT_OK) break;
+            P = parts_of(h);
             for (int s = 0; s < 2; s++) {
-                jt_launch_kick(h->vel[s], h->acc[s], h->n[s], full, drag, h->st);
-                jt_launch_drift(h->pos[s], h->vel[s], h->n[s], half, L, halfL, h->st);
+                jt_launch_kick(P.vel[s], P.acc[s], h->n[s], full, drag, h->st);
+                jt_launch_drift(P.pos[s], P.vel[s], h->n[s], half, L, halfL, h->st);
             }
-            r = check_device_error(h);
-            if (r != JT_OK) break;
-            accumulate_timings(h);
+            r = finish_call(h, r, nullptr, nullptr);
+            add_pass();
             kd_ms += elapsed(k0, k1);
             h->acc_valid = false;  // acc belongs to the half-drifted positions
+            if (h->batch) jtb_box(h->batch, h->box_id)->acc_valid = false;
         }
     }
     cudaEventRecord(t1, h->st);
     if (cudaStreamSynchronize(h->st) != cudaSuccess && r == JT_OK) r = JT_ECUDA;
+    if (h->batch) h->tm = acc_tm;
     if (r == JT_OK) {
         h->tm.total_ms = elapsed(t0, t1);
         h->tm.kick_drift_ms = kd_ms;
-        fetch_inter(h);
     }
     cudaEventDestroy(t0); cudaEventDestroy(t1); cudaEventDestroy(k0); cudaEventDestroy(k1);
     return r;
@@ -747,11 +807,11 @@ int jt_get_state(jt_handle* h, float* pos_p, float* vel_p, float* pos_m, float* 
 {
     if (!h || (mem != JT_MEM_HOST && mem != JT_MEM_DEVICE)) return JT_EINVAL;
     if (!h->have_state) return JT_ESTATE;
+    const Parts P = parts_of(h);
     float* outs[2][2] = {{pos_p, vel_p}, {pos_m, vel_m}};
     for (int s = 0; s < 2; s++) {
         for (int q = 0; q < 2; q++) {
-            JT_TRY(write_out(h, q == 0 ? h->pos[s] : h->vel[s], h->id[s], nullptr, h->n[s],
-                             outs[s][q], mem));
+            JT_TRY(write_out(h, q == 0 ? P.pos[s] : P.vel[s], P.id[s], nullptr, h->n[s], outs[s][q], mem));
             JT_CU(cudaStreamSynchronize(h->st));
         }
     }
@@ -762,13 +822,14 @@ int jt_get_state_signed(jt_handle* h, float* pos, float* vel, int mem)
 {
     if (!h || (mem != JT_MEM_HOST && mem != JT_MEM_DEVICE)) return JT_EINVAL;
     if (!h->have_state) return JT_ESTATE;
+    const Parts P = parts_of(h);
     int64_t na = h->n[0] + h->n[1];
     float* outs[2] = {pos, vel};
     for (int q = 0; q < 2; q++) {
         if (!outs[q]) continue;
         float* target = mem == JT_MEM_DEVICE ? outs[q] : (float*)h->stage;
         for (int s = 0; s < 2; s++)
-            jt_launch_aos_out(q == 0 ? h->pos[s] : h->vel[s], h->id[s], h->gmap[s], h->n[s], target, h->st);
+            jt_launch_aos_out(q == 0 ? P.pos[s] : P.vel[s], P.id[s], h->gmap[s], h->n[s], target, h->st);
         if (mem == JT_MEM_HOST)
             JT_CU(cudaMemcpyAsync(outs[q], h->stage, sizeof(float) * 3 * na, cudaMemcpyDeviceToHost, h->st));
         JT_CU(cudaStreamSynchronize(h->st));
@@ -783,10 +844,12 @@ int jt_debug_tree(jt_handle* h, int species, uint32_t* morton, int32_t* perm, in
     if (!h->have_state) return JT_ESTATE;
     int64_t n = h->n[species];
     if (n == 0) return JT_OK;
+    if (!h->dbg_ready) JT_TRY(alloc_trees(h, h->n[0], h->n[1]));
+    const Parts P = parts_of(h);
     jt_tree_dev& t = h->tree[species];
     float box_half = (float)(h->cfg.box_L / 2.0);
     // reference keys at the current positions, without moving the state
-    jt_launch_morton(h->pos[species], h->id[species], n, box_half, nullptr, h->key64, h->ws.vals, h->st);
+    jt_launch_morton(P.pos[species], P.id[species], n, box_half, nullptr, h->key64, h->ws.vals, h->st);
     int shifts[8], np = 0;
     for (int b = 0; b < id_bits(n); b += 8) shifts[np++] = b;
     for (int b = 32; b < 62; b += 8) shifts[np++] = b;
@@ -806,8 +869,16 @@ int jt_debug_tree(jt_handle* h, int species, uint32_t* morton, int32_t* perm, in
         if (left) left[i] = ch[i].x;
         if (right) right[i] = ch[i].y;
     }
-    // the tree arrays no longer describe the state order; the next force
-    // evaluation rebuilds them
+    // RCOMPAT: the tree arrays no longer describe the state order; the next
+    // force evaluation rebuilds them
+    h->acc_valid = false;
+    return JT_OK;
+}
+
+int jt_walk_counters(jt_handle* h, int64_t* out4)
+{
+    if (!h || !out4) return JT_EINVAL;
+    for (int i = 0; i < 4; i++) out4[i] = h->phase[i];
     return JT_OK;
 }
 

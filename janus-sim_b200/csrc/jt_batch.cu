@@ -1,0 +1,886 @@
+// Batched engine: many independent boxes advanced with ONE launch per stage.
+//
+// The reference runs parameter scans one box at a time, one process per
+// configuration (optim/run_tour.py:40-48, scripts/run_scan_mu.sh), each box
+// paying its own ~40 launches and host synchronisations per step
+// (src/nbody_gpu_twopass.rs:4486-4649).  Here a jt_batch holds any number of
+// boxes (uneven particle counts, box sizes, PM grids, mu); a step over a
+// chosen subset of them runs every stage as one launch over the flattened
+// work of all chosen boxes (segments = box x species, jt_internal.cuh), with
+// cuFFT plans bucketed by grid size (one batched R2C and one batched C2R per
+// distinct M).  Only particle state persists per box; trees, sort workspaces
+// and PM grids are per-pass scratch in grow-only pools, so boxes can join and
+// leave between steps (the serving loop admits and evicts jobs this way).
+//
+// Per force pass (stream order, no host synchronisation inside):
+//   memset sort status -> morton, hist, scan, 4 onesweep passes, reorder
+//   (8 launches over all segments) -> karras, moments (2) -> memset rho per
+//   grid bucket -> tile ranges, tiled deposit (2) -> R2C per bucket ->
+//   k-space (1) -> C2R per bucket -> walk with fused closing kick (1).
+#include "jt_batch.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <new>
+#include <vector>
+
+namespace {
+
+#define JT_TRY(x)                   \
+    do {                            \
+        int _r = (x);               \
+        if (_r != JT_OK) return _r; \
+    } while (0)
+#define JT_CU(x)                                 \
+    do {                                         \
+        if ((x) != cudaSuccess) return JT_ECUDA; \
+    } while (0)
+#define JT_FFT(x)                                  \
+    do {                                           \
+        if ((x) != CUFFT_SUCCESS) return JT_ECUDA; \
+    } while (0)
+
+template <class T>
+int dalloc(T** p, size_t count)
+{
+    *p = nullptr;
+    if (count == 0) count = 1;
+    return cudaMalloc((void**)p, sizeof(T) * count) == cudaSuccess ? JT_OK : JT_ENOMEM;
+}
+template <class T>
+void dfree(T*& p)
+{
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+}
+
+// grow-only device array (25% headroom on growth)
+template <class T>
+struct Pool {
+    T* p = nullptr;
+    size_t cap = 0;
+    int ensure(size_t n, bool* grew)
+    {
+        if (n <= cap) return JT_OK;
+        size_t want = std::max(n, cap + cap / 4);
+        dfree(p);
+        cap = 0;
+        JT_TRY(dalloc(&p, want));
+        cap = want;
+        *grew = true;
+        return JT_OK;
+    }
+    size_t bytes() const { return cap * sizeof(T); }
+    void release()
+    {
+        dfree(p);
+        cap = 0;
+    }
+};
+
+int box_order(const jt_config& c) { return c.pm_order == 0 ? 3 : c.pm_order; }
+int box_ngrid(const jt_config& c) { return c.pm_interlace == 2 ? 1 : 2; }
+
+struct Bucket {                 // PM scratch of the boxes with grid M in a pass
+    int M = 0;
+    int cap = 0;                // boxes the arrays hold
+    float* rho = nullptr;
+    float2* rho_k = nullptr;
+    float2* force_k = nullptr;
+    float* force = nullptr;
+    int4* ranges = nullptr;
+    std::map<int, std::pair<cufftHandle, cufftHandle>> plans;   // count -> (r2c, c2r)
+    void free_arrays()
+    {
+        dfree(rho); dfree(rho_k); dfree(force_k); dfree(force); dfree(ranges);
+        cap = 0;
+    }
+    void release()
+    {
+        free_arrays();
+        for (auto& kv : plans) {
+            cufftDestroy(kv.second.first);
+            cufftDestroy(kv.second.second);
+        }
+        plans.clear();
+    }
+};
+
+size_t grid_bytes(int64_t M, int ngrid)
+{
+    int64_t G = M * M * M, Gc = M * M * (M / 2 + 1);
+    int T = jt_pm_tile_edge((int)M);
+    int64_t nt = (M / T) * (M / T) * (M / T);
+    return (size_t)(ngrid * (G * 4 + Gc * 8) + 3 * ngrid * (Gc * 8 + G * 4) + nt * 16);
+}
+
+// The tables of one pass, packed into one host buffer and uploaded once.
+struct Plan {
+    std::vector<int> ids;                 // boxes of this pass
+    std::vector<jt_seg_dev> pre, post;    // segments before / after the reorder
+    std::vector<jt_box_dev> bx;
+    std::vector<int64_t> pprefix, iprefix, tprefix, gprefix, ptprefix, kprefix;
+    int64_t npart = 0, ninternal = 0, nsorttiles = 0, ngroups = 0, npmtiles = 0, nmodes = 0;
+    std::map<int, std::vector<int>> by_M; // M -> boxes (positions in ids)
+    int maxT = 1;
+    const jt_seg_dev* d_pre = nullptr;
+    const jt_seg_dev* d_post = nullptr;
+    const jt_box_dev* d_bx = nullptr;
+    const int64_t *d_pp = nullptr, *d_ip = nullptr, *d_tp = nullptr, *d_gp = nullptr, *d_ptp = nullptr,
+                  *d_kp = nullptr;
+};
+
+float elapsed(cudaEvent_t a, cudaEvent_t b)
+{
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) return 0.f;
+    return ms;
+}
+
+}  // namespace
+
+struct jt_batch {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    std::vector<jt_box_state*> boxes;
+    int order = 0, ngrid = 0, k_min = -1;   // shared by every box of the batch
+    Pool<int2> child, range;
+    Pool<int> parent, flag;
+    Pool<float4> com, bmin, bmax, quad0;
+    Pool<float2> quad1;
+    Pool<uint32_t> m30, vals, vals_alt, keys_alt, hist, status, tickets;
+    Pool<unsigned char> desc;           // device copy of the pass's tables
+    unsigned char* hdesc = nullptr;     // pinned host staging of the tables
+    size_t hdesc_cap = 0;
+    cudaEvent_t desc_done = nullptr;    // the last upload from hdesc finished
+    std::map<int, Bucket> buckets;
+    unsigned* d_err = nullptr;
+    unsigned long long* d_stats = nullptr;
+    cudaEvent_t ev[8] = {};
+    bool pending = false;               // a pass's events await jtb_finish
+    jt_timings tm = {};
+    int64_t phase[4] = {0, 0, 0, 0};
+    Plan plan;
+};
+
+namespace {
+
+int box_alloc(jt_box_state* b)
+{
+    size_t bytes = 0;
+    for (int s = 0; s < 2; s++) {
+        int64_t n = b->n[s];
+        JT_TRY(dalloc(&b->pos[s], n)); JT_TRY(dalloc(&b->vel[s], n)); JT_TRY(dalloc(&b->acc[s], n));
+        JT_TRY(dalloc(&b->pos_b[s], n)); JT_TRY(dalloc(&b->vel_b[s], n));
+        JT_TRY(dalloc(&b->id[s], n)); JT_TRY(dalloc(&b->id_b[s], n));
+        bytes += (size_t)n * (5 * sizeof(float4) + 2 * sizeof(int));
+    }
+    const int M = b->M;
+    JT_TRY(dalloc(&b->tabs, 2 * (size_t)M));
+    // per-axis tables: ta = {k, gradient k (0 at Nyquist), exp(-k^2 r_s^2)/sinc^(2 order), |n|}
+    //                  tb = {cos(k h/2), sin(k h/2), 0, 0} (interlacing phase)
+    std::vector<float> tab(8 * (size_t)M);
+    const jt_config& c = b->cfg;
+    double dk = 2.0 * M_PI / c.box_L, rs = c.r_s, hh = c.box_L / M;
+    for (int n = 0; n < M; n++) {
+        int ni = n <= M / 2 ? n : n - M;
+        double k = dk * ni;
+        double u = M_PI * ni / M;
+        double sinc = ni == 0 ? 1.0 : std::sin(u) / u;
+        double f = std::exp(-k * k * rs * rs) / std::pow(sinc, 2.0 * b->order);
+        tab[4 * n] = (float)k;
+        tab[4 * n + 1] = (n == M / 2) ? 0.0f : (float)k;
+        tab[4 * n + 2] = (float)f;
+        tab[4 * n + 3] = (float)(ni < 0 ? -ni : ni);
+        tab[4 * (M + n)] = (float)std::cos(0.5 * k * hh);
+        tab[4 * (M + n) + 1] = (float)std::sin(0.5 * k * hh);
+        tab[4 * (M + n) + 2] = 0.0f;
+        tab[4 * (M + n) + 3] = 0.0f;
+    }
+    JT_CU(cudaMemcpy(b->tabs, tab.data(), sizeof(float) * tab.size(), cudaMemcpyHostToDevice));
+    b->bytes = bytes + sizeof(float4) * 2 * (size_t)M;
+    return JT_OK;
+}
+
+void box_release(jt_box_state* b)
+{
+    for (int s = 0; s < 2; s++) {
+        dfree(b->pos[s]); dfree(b->vel[s]); dfree(b->acc[s]); dfree(b->pos_b[s]); dfree(b->vel_b[s]);
+        dfree(b->id[s]); dfree(b->id_b[s]);
+    }
+    dfree(b->tabs);
+}
+
+int tile_shift_of(int M)
+{
+    int T = jt_pm_tile_edge(M);
+    int W = 1024 / M * T;  // tile edge in Morton cells (power of two)
+    int lw = 0;
+    while ((1 << lw) < W) lw++;
+    return 3 * lw;
+}
+
+int bucket_ensure(jt_batch* B, Bucket& k, int M, int count)
+{
+    k.M = M;
+    const int ngrid = B->ngrid;
+    const int64_t G = (int64_t)M * M * M, Gc = (int64_t)M * M * (M / 2 + 1);
+    if (count > k.cap) {
+        k.free_arrays();
+        int T = jt_pm_tile_edge(M);
+        int64_t nt = (int64_t)(M / T) * (M / T) * (M / T);
+        JT_TRY(dalloc(&k.rho, (size_t)count * ngrid * G));
+        JT_TRY(dalloc(&k.rho_k, (size_t)count * ngrid * Gc));
+        JT_TRY(dalloc(&k.force_k, (size_t)count * 3 * ngrid * Gc));
+        JT_TRY(dalloc(&k.force, (size_t)count * 3 * ngrid * G));
+        JT_TRY(dalloc(&k.ranges, (size_t)count * nt));
+        k.cap = count;
+    }
+    if (!k.plans.count(count)) {
+        int dims[3] = {M, M, M};
+        cufftHandle r2c, c2r;
+        JT_FFT(cufftPlanMany(&r2c, 3, dims, nullptr, 1, (int)G, nullptr, 1, (int)Gc, CUFFT_R2C,
+                             ngrid * count));
+        if (cufftPlanMany(&c2r, 3, dims, nullptr, 1, (int)Gc, nullptr, 1, (int)G, CUFFT_C2R,
+                          3 * ngrid * count) != CUFFT_SUCCESS) {
+            cufftDestroy(r2c);
+            return JT_ECUDA;
+        }
+        cufftSetStream(r2c, B->st);
+        cufftSetStream(c2r, B->st);
+        k.plans[count] = {r2c, c2r};
+    }
+    return JT_OK;
+}
+
+template <class T>
+size_t put(std::vector<unsigned char>& buf, const std::vector<T>& v)
+{
+    size_t off = (buf.size() + 15) & ~(size_t)15;
+    buf.resize(off + sizeof(T) * v.size());
+    if (!v.empty()) std::memcpy(buf.data() + off, v.data(), sizeof(T) * v.size());
+    return off;
+}
+
+// Size the scratch pools for the listed boxes, lay out their segments and
+// boxes, and upload every table in one copy.
+int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* steps, Plan& P)
+{
+    P = Plan();
+    P.ids = ids;
+    const int nb = (int)ids.size();
+    const int ST = jt_sort_tile_size();
+    int64_t nodes = 0, parts = 0, stiles = 0;
+    int nseg = 0;
+    for (int k = 0; k < nb; k++) {
+        jt_box_state* b = B->boxes[ids[k]];
+        for (int s = 0; s < 2; s++) {
+            int64_t n = b->n[s];
+            if (n == 0) continue;
+            nodes += 2 * n - 1;
+            parts += n;
+            stiles += (n + ST - 1) / ST;
+            nseg++;
+        }
+    }
+    bool grew = false;
+    JT_TRY(B->child.ensure(nodes, &grew)); JT_TRY(B->parent.ensure(nodes, &grew));
+    JT_TRY(B->range.ensure(parts, &grew)); JT_TRY(B->flag.ensure(parts, &grew));
+    JT_TRY(B->com.ensure(nodes, &grew)); JT_TRY(B->bmin.ensure(nodes, &grew));
+    JT_TRY(B->bmax.ensure(nodes, &grew)); JT_TRY(B->quad0.ensure(nodes, &grew));
+    JT_TRY(B->quad1.ensure(nodes, &grew));
+    JT_TRY(B->m30.ensure(parts, &grew)); JT_TRY(B->vals.ensure(parts, &grew));
+    JT_TRY(B->vals_alt.ensure(parts, &grew)); JT_TRY(B->keys_alt.ensure(parts, &grew));
+    JT_TRY(B->hist.ensure((size_t)nseg * 4 * 256, &grew));
+    JT_TRY(B->status.ensure((size_t)stiles * 4 * 256, &grew));
+    JT_TRY(B->tickets.ensure(4, &grew));
+    for (int k = 0; k < nb; k++) P.by_M[B->boxes[ids[k]]->M].push_back(k);
+    for (auto& kv : P.by_M) JT_TRY(bucket_ensure(B, B->buckets[kv.first], kv.first, (int)kv.second.size()));
+    std::vector<int> slot(nb);
+    for (auto& kv : P.by_M)
+        for (size_t q = 0; q < kv.second.size(); q++) slot[kv.second[q]] = (int)q;
+
+    int64_t o_node = 0, o_part = 0, o_tile = 0;
+    P.pprefix.push_back(0); P.iprefix.push_back(0); P.tprefix.push_back(0); P.gprefix.push_back(0);
+    P.ptprefix.push_back(0); P.kprefix.push_back(0);
+    P.bx.resize(nb);
+    for (int k = 0; k < nb; k++) {
+        jt_box_state* b = B->boxes[ids[k]];
+        const jt_config& c = b->cfg;
+        const int M = b->M;
+        jt_box_dev& d = P.bx[k];
+        std::memset(&d, 0, sizeof(d));
+        d.L = (float)c.box_L;
+        d.halfL = (float)(c.box_L / 2.0);
+        d.box_half = (float)(c.box_L / 2.0);
+        d.h_inv = (float)(M / c.box_L);
+        d.rc2 = (float)(c.r_cut * c.r_cut);
+        d.eps2 = (float)(c.softening * c.softening);
+        d.c = (float)(1.0 / (2.0 * c.r_s));
+        d.theta2 = (float)(c.theta * c.theta);
+        d.mass[0] = b->mass[0];
+        d.mass[1] = b->mass[1];
+        d.kick_drag = steps ? steps[k].drag : 0.0f;
+        d.dt = steps ? steps[k].dt : 0.0f;
+        d.M = M;
+        d.order = b->order;
+        d.ngrid = b->ngrid;
+        d.T = jt_pm_tile_edge(M);
+        d.tile_shift = tile_shift_of(M);
+        d.ntiles = (M / d.T) * (M / d.T) * (M / d.T);
+        P.maxT = std::max(P.maxT, d.T);
+        Bucket& K = B->buckets[M];
+        const int q = slot[k];
+        const int64_t G = (int64_t)M * M * M, Gc = (int64_t)M * M * (M / 2 + 1);
+        d.rho = K.rho + (size_t)q * b->ngrid * G;
+        d.rho_k = K.rho_k + (size_t)q * b->ngrid * Gc;
+        d.force_k = K.force_k + (size_t)q * 3 * b->ngrid * Gc;
+        d.force = K.force + (size_t)q * 3 * b->ngrid * G;
+        d.tabs = b->tabs;
+        d.ranges = K.ranges + (size_t)q * d.ntiles;
+        d.seg[0] = d.seg[1] = -1;
+        for (int s = 0; s < 2; s++) {
+            const int64_t n = b->n[s];
+            if (n == 0) continue;
+            jt_seg_dev g;
+            std::memset(&g, 0, sizeof(g));
+            g.n = n;
+            g.box = k;
+            g.species = s;
+            g.tree.n = n;
+            g.tree.child = B->child.p + o_node;
+            g.tree.parent = B->parent.p + o_node;
+            g.tree.com = B->com.p + o_node;
+            g.tree.bmin = B->bmin.p + o_node;
+            g.tree.bmax = B->bmax.p + o_node;
+            g.tree.quad0 = B->quad0.p + o_node;
+            g.tree.quad1 = B->quad1.p + o_node;
+            g.tree.range = B->range.p + o_part;
+            g.tree.flag = B->flag.p + o_part;
+            g.tree.m30 = B->m30.p + o_part;
+            g.tree.tie = nullptr;   // Karras ties broken by sorted position
+            g.vals = B->vals.p + o_part;
+            g.vals_alt = B->vals_alt.p + o_part;
+            g.keys_alt = B->keys_alt.p + o_part;
+            g.hist = B->hist.p + (size_t)P.pre.size() * 4 * 256;
+            g.status = B->status.p + (size_t)o_tile * 4 * 256;
+            d.seg[s] = (int)P.pre.size();
+            jt_seg_dev pre = g, post = g;
+            pre.pos = b->pos[s]; pre.vel = b->vel[s]; pre.acc = b->acc[s];
+            pre.pos_b = b->pos_b[s]; pre.vel_b = b->vel_b[s]; pre.id = b->id[s]; pre.id_b = b->id_b[s];
+            post.pos = b->pos_b[s]; post.vel = b->vel_b[s]; post.acc = b->acc[s];
+            post.pos_b = b->pos[s]; post.vel_b = b->vel[s]; post.id = b->id_b[s]; post.id_b = b->id[s];
+            P.pre.push_back(pre);
+            P.post.push_back(post);
+            const int64_t t = (n + ST - 1) / ST;
+            o_node += 2 * n - 1;
+            o_part += n;
+            o_tile += t;
+            P.pprefix.push_back(P.pprefix.back() + n);
+            P.iprefix.push_back(P.iprefix.back() + (n - 1));
+            P.tprefix.push_back(P.tprefix.back() + t);
+            P.gprefix.push_back(P.gprefix.back() + (n + 31) / 32);
+        }
+        P.ptprefix.push_back(P.ptprefix.back() + d.ntiles);
+        P.kprefix.push_back(P.kprefix.back() + Gc);
+    }
+    P.npart = P.pprefix.back();
+    P.ninternal = P.iprefix.back();
+    P.nsorttiles = P.tprefix.back();
+    P.ngroups = P.gprefix.back();
+    P.npmtiles = P.ptprefix.back();
+    P.nmodes = P.kprefix.back();
+
+    std::vector<unsigned char> buf;
+    size_t o_pre = put(buf, P.pre), o_post = put(buf, P.post), o_bx = put(buf, P.bx);
+    size_t o_pp = put(buf, P.pprefix), o_ip = put(buf, P.iprefix), o_tp = put(buf, P.tprefix);
+    size_t o_gp = put(buf, P.gprefix), o_ptp = put(buf, P.ptprefix), o_kp = put(buf, P.kprefix);
+    JT_TRY(B->desc.ensure(buf.size(), &grew));
+    // the previous upload may still read the staging buffer
+    JT_CU(cudaEventSynchronize(B->desc_done));
+    if (buf.size() > B->hdesc_cap) {
+        if (B->hdesc) cudaFreeHost(B->hdesc);
+        B->hdesc = nullptr;
+        B->hdesc_cap = 0;
+        if (cudaMallocHost((void**)&B->hdesc, buf.size() * 2) != cudaSuccess) return JT_ENOMEM;
+        B->hdesc_cap = buf.size() * 2;
+    }
+    std::memcpy(B->hdesc, buf.data(), buf.size());
+    JT_CU(cudaMemcpyAsync(B->desc.p, B->hdesc, buf.size(), cudaMemcpyHostToDevice, B->st));
+    JT_CU(cudaEventRecord(B->desc_done, B->st));
+    unsigned char* d = B->desc.p;
+    P.d_pre = (const jt_seg_dev*)(d + o_pre);
+    P.d_post = (const jt_seg_dev*)(d + o_post);
+    P.d_bx = (const jt_box_dev*)(d + o_bx);
+    P.d_pp = (const int64_t*)(d + o_pp);
+    P.d_ip = (const int64_t*)(d + o_ip);
+    P.d_tp = (const int64_t*)(d + o_tp);
+    P.d_gp = (const int64_t*)(d + o_gp);
+    P.d_ptp = (const int64_t*)(d + o_ptp);
+    P.d_kp = (const int64_t*)(d + o_kp);
+    return JT_OK;
+}
+
+// One force pass over the plan's boxes; afterwards every box's state sits in
+// its former b-buffers (pointers swapped here and in the plan).
+int force_pass(jt_batch* B, Plan& P, int parts, float kick_frac)
+{
+    cudaStream_t st = B->st;
+    const int nseg = (int)P.pre.size(), nbox = (int)P.bx.size();
+    cudaEventRecord(B->ev[0], st);
+    JT_CU(cudaMemsetAsync(B->hist.p, 0, sizeof(uint32_t) * (size_t)nseg * 4 * 256, st));
+    JT_CU(cudaMemsetAsync(B->status.p, 0, sizeof(uint32_t) * (size_t)P.nsorttiles * 4 * 256, st));
+    JT_CU(cudaMemsetAsync(B->tickets.p, 0, sizeof(uint32_t) * 4, st));
+    JT_TRY(jt_b_sort_reorder(P.d_pre, P.d_bx, nseg, P.d_pp, P.npart, P.d_tp, P.nsorttiles, B->tickets.p,
+                             B->d_err, st));
+    cudaEventRecord(B->ev[1], st);
+    jt_b_build_trees(P.d_post, P.d_bx, nseg, P.d_ip, P.ninternal, P.d_pp, P.npart, st);
+    cudaEventRecord(B->ev[2], st);
+    for (auto& kv : P.by_M) {
+        const int64_t M = kv.first, G = M * M * M;
+        JT_CU(cudaMemsetAsync(B->buckets[kv.first].rho, 0, sizeof(float) * kv.second.size() * B->ngrid * G, st));
+    }
+    jt_b_tile_ranges(P.d_post, P.d_bx, P.d_ptp, nbox, P.npmtiles, st);
+    JT_TRY(jt_b_deposit(P.d_post, P.d_bx, P.d_ptp, nbox, P.npmtiles, B->order, B->ngrid, P.maxT, st));
+    cudaEventRecord(B->ev[3], st);
+    for (auto& kv : P.by_M) {
+        Bucket& K = B->buckets[kv.first];
+        JT_FFT(cufftExecR2C(K.plans[(int)kv.second.size()].first, K.rho, (cufftComplex*)K.rho_k));
+    }
+    cudaEventRecord(B->ev[4], st);
+    jt_b_kspace(P.d_bx, P.d_kp, nbox, P.nmodes, B->ngrid == 2, B->k_min, st);
+    cudaEventRecord(B->ev[5], st);
+    for (auto& kv : P.by_M) {
+        Bucket& K = B->buckets[kv.first];
+        JT_FFT(cufftExecC2R(K.plans[(int)kv.second.size()].second, (cufftComplex*)K.force_k, K.force));
+    }
+    cudaEventRecord(B->ev[6], st);
+    JT_TRY(jt_b_walk(P.d_post, P.d_bx, P.d_gp, nseg, P.ngroups, B->order, B->ngrid, parts, kick_frac,
+                     B->d_stats, B->d_err, st));
+    cudaEventRecord(B->ev[7], st);
+    B->pending = true;
+    B->tm.launches += (P.npart > 0 ? 8 : 0) + (P.ninternal > 0 ? 1 : 0) + (P.npart > 0 ? 1 : 0) +
+                      (P.npmtiles > 0 ? 2 : 0) + (P.nmodes > 0 ? 1 : 0) + (P.ngroups > 0 ? 1 : 0);
+    for (int id : P.ids) {
+        jt_box_state* b = B->boxes[id];
+        for (int s = 0; s < 2; s++) {
+            std::swap(b->pos[s], b->pos_b[s]);
+            std::swap(b->vel[s], b->vel_b[s]);
+            std::swap(b->id[s], b->id_b[s]);
+        }
+        b->acc_valid = parts == JT_PART_ALL;
+    }
+    std::swap(P.pre, P.post);
+    std::swap(P.d_pre, P.d_post);
+    return cudaGetLastError() == cudaSuccess ? JT_OK : JT_ECUDA;
+}
+
+int finish(jt_batch* B)
+{
+    unsigned e = 0;
+    unsigned long long v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    JT_CU(cudaMemcpyAsync(&e, B->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, B->st));
+    JT_CU(cudaMemcpyAsync(v, B->d_stats, sizeof(v), cudaMemcpyDeviceToHost, B->st));
+    JT_CU(cudaStreamSynchronize(B->st));
+    if (e) {
+        for (jt_box_state* b : B->boxes)
+            if (b) b->acc_valid = false;
+        cudaMemsetAsync(B->d_err, 0, sizeof(unsigned), B->st);
+        cudaMemsetAsync(B->d_stats, 0, sizeof(v), B->st);
+        cudaStreamSynchronize(B->st);
+        B->pending = false;
+        return (e & JT_ERRBIT_LOOKBACK) ? JT_ETIMEDOUT : JT_EOVERFLOW;
+    }
+    if (B->pending) {
+        B->tm.sort_ms += elapsed(B->ev[0], B->ev[1]);
+        B->tm.tree_ms += elapsed(B->ev[1], B->ev[2]);
+        B->tm.deposit_ms += elapsed(B->ev[2], B->ev[3]);
+        B->tm.fft_ms += elapsed(B->ev[3], B->ev[6]);
+        B->tm.kspace_ms += elapsed(B->ev[4], B->ev[5]);
+        B->tm.walk_ms += elapsed(B->ev[6], B->ev[7]);
+        B->pending = false;
+    }
+    B->tm.pair_interactions += (int64_t)v[0];
+    B->tm.node_interactions += (int64_t)v[1];
+    B->tm.candidates += (int64_t)v[2];
+    B->tm.interactions += (int64_t)(v[0] + v[1]);
+    for (int i = 0; i < 4; i++) B->phase[i] += (int64_t)v[3 + i];
+    JT_CU(cudaMemsetAsync(B->d_stats, 0, sizeof(v), B->st));
+    return JT_OK;
+}
+
+int valid_ids(jt_batch* B, const int* ids, int n, std::vector<int>& out)
+{
+    out.clear();
+    if (!ids || n <= 0) return JT_EINVAL;
+    std::vector<char> seen(B->boxes.size(), 0);
+    for (int k = 0; k < n; k++) {
+        int id = ids[k];
+        if (id < 0 || id >= (int)B->boxes.size() || !B->boxes[id] || seen[id]) return JT_EINVAL;
+        seen[id] = 1;
+        out.push_back(id);
+    }
+    return JT_OK;
+}
+
+int validate_box_config(const jt_config* c)
+{
+    auto pow2 = [](int m) { return m > 0 && (m & (m - 1)) == 0; };
+    if (!c) return JT_EINVAL;
+    if (c->mode != JT_ACCURATE || c->integrator != JT_KDK) return JT_EINVAL;
+    if (!(c->box_L > 0.0) || !std::isfinite(c->box_L)) return JT_EINVAL;
+    if (!pow2(c->pm_grid) || c->pm_grid < 8 || c->pm_grid > 1024) return JT_EINVAL;
+    if (!(c->theta >= 0.0) || !std::isfinite(c->theta)) return JT_EINVAL;
+    if (!(c->softening >= 0.0) || !std::isfinite(c->softening)) return JT_EINVAL;
+    if (!(c->r_cut > 0.0) || c->r_cut >= 0.5 * c->box_L) return JT_EINVAL;
+    if (!(c->r_s > 0.0) || !std::isfinite(c->r_s)) return JT_EINVAL;
+    if (!(c->mu >= 0.0) || !std::isfinite(c->mu)) return JT_EINVAL;
+    if (!(c->G_mass_plus > 0.0) || !std::isfinite(c->G_mass_plus)) return JT_EINVAL;
+    if (c->k_min < 0) return JT_EINVAL;
+    if (c->pm_order != 0 && c->pm_order != 2 && c->pm_order != 3) return JT_EINVAL;
+    if (c->pm_interlace < 0 || c->pm_interlace > 2) return JT_EINVAL;
+    return JT_OK;
+}
+
+bool box_id_ok(jt_batch* B, int id) { return B && id >= 0 && id < (int)B->boxes.size() && B->boxes[id]; }
+
+// AoS float3 out of a box (caller order of the species array).
+int read_out(jt_batch* B, const float4* src, const int* id, int64_t n, float* dst, int mem)
+{
+    if (!dst || n == 0) return JT_OK;
+    if (mem == JT_MEM_DEVICE) {
+        jt_launch_aos_out(src, id, nullptr, n, dst, B->st);
+        return JT_OK;
+    }
+    float* stage = nullptr;
+    if (cudaMalloc(&stage, sizeof(float) * 3 * n) != cudaSuccess) return JT_ENOMEM;
+    jt_launch_aos_out(src, id, nullptr, n, stage, B->st);
+    cudaError_t e = cudaMemcpyAsync(dst, stage, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, B->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(B->st);
+    cudaFree(stage);
+    return e == cudaSuccess ? JT_OK : JT_ECUDA;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- internal
+int jtb_add_empty(jt_batch* B, const jt_config* cfg, int64_t n_p, int64_t n_m, int* box_id)
+{
+    if (!B || !box_id || n_p < 0 || n_m < 0 || n_p + n_m == 0) return JT_EINVAL;
+    if (n_p >= (int64_t)1 << 30 || n_m >= (int64_t)1 << 30) return JT_EINVAL;
+    JT_TRY(validate_box_config(cfg));
+    const int order = box_order(*cfg), ngrid = box_ngrid(*cfg);
+    bool empty = true;
+    for (auto* b : B->boxes) empty = empty && !b;
+    if (!empty && (order != B->order || ngrid != B->ngrid || cfg->k_min != B->k_min)) return JT_EINVAL;
+    jt_box_state* b = new (std::nothrow) jt_box_state();
+    if (!b) return JT_ENOMEM;
+    b->cfg = *cfg;
+    b->n[0] = n_p;
+    b->n[1] = n_m;
+    // per-particle masses: m+ = G_mass_plus, m- = mu m+ N+/N- (mu = M-/M+)
+    double mp = cfg->G_mass_plus;
+    double mm = n_m > 0 ? cfg->mu * mp * (double)n_p / (double)n_m : 0.0;
+    if (n_p == 0) mm = cfg->mu * mp;
+    b->mass[0] = (float)mp;
+    b->mass[1] = (float)mm;
+    b->M = cfg->pm_grid;
+    b->order = order;
+    b->ngrid = ngrid;
+    int r = box_alloc(b);
+    if (r != JT_OK) {
+        box_release(b);
+        delete b;
+        return r;
+    }
+    int slot = -1;
+    for (size_t k = 0; k < B->boxes.size(); k++)
+        if (!B->boxes[k]) { slot = (int)k; break; }
+    if (slot < 0) {
+        slot = (int)B->boxes.size();
+        B->boxes.push_back(nullptr);
+    }
+    B->boxes[slot] = b;
+    B->order = order;
+    B->ngrid = ngrid;
+    B->k_min = cfg->k_min;
+    *box_id = slot;
+    return JT_OK;
+}
+
+jt_box_state* jtb_box(jt_batch* B, int box_id) { return box_id_ok(B, box_id) ? B->boxes[box_id] : nullptr; }
+
+cudaStream_t jtb_stream(jt_batch* B) { return B ? B->st : nullptr; }
+
+int jtb_force_pass(jt_batch* B, const int* ids, int n_ids, int parts, float kick_frac, const jt_box_step* steps)
+{
+    if (!B || parts < 1 || parts > 3) return JT_EINVAL;
+    std::vector<int> v;
+    JT_TRY(valid_ids(B, ids, n_ids, v));
+    JT_TRY(build_plan(B, v, steps, B->plan));
+    return force_pass(B, B->plan, parts, kick_frac);
+}
+
+int jtb_finish(jt_batch* B) { return B ? finish(B) : JT_EINVAL; }
+
+void jtb_reset_timings(jt_batch* B)
+{
+    if (B) B->tm = jt_timings{};
+}
+
+int64_t jtb_phase(jt_batch* B, int i) { return B && i >= 0 && i < 4 ? B->phase[i] : 0; }
+
+// ---------------------------------------------------------------- C ABI
+extern "C" {
+
+int jt_batch_create(jt_batch** out)
+{
+    if (!out) return JT_EINVAL;
+    *out = nullptr;
+    jt_batch* B = new (std::nothrow) jt_batch();
+    if (!B) return JT_ENOMEM;
+    if (cudaGetDevice(&B->device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&B->st, cudaStreamNonBlocking) != cudaSuccess) {
+        delete B;
+        return JT_ECUDA;
+    }
+    for (auto& e : B->ev) cudaEventCreate(&e);
+    cudaEventCreateWithFlags(&B->desc_done, cudaEventDisableTiming);
+    if (cudaMalloc(&B->d_err, sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&B->d_stats, 8 * sizeof(unsigned long long)) != cudaSuccess) {
+        jt_batch_destroy(B);
+        return JT_ENOMEM;
+    }
+    cudaMemset(B->d_err, 0, sizeof(unsigned));
+    cudaMemset(B->d_stats, 0, 8 * sizeof(unsigned long long));
+    *out = B;
+    return JT_OK;
+}
+
+void jt_batch_destroy(jt_batch* B)
+{
+    if (!B) return;
+    if (B->st) cudaStreamSynchronize(B->st);
+    for (auto* b : B->boxes)
+        if (b) { box_release(b); delete b; }
+    B->child.release(); B->range.release(); B->parent.release(); B->flag.release();
+    B->com.release(); B->bmin.release(); B->bmax.release(); B->quad0.release(); B->quad1.release();
+    B->m30.release(); B->vals.release(); B->vals_alt.release(); B->keys_alt.release();
+    B->hist.release(); B->status.release(); B->tickets.release(); B->desc.release();
+    for (auto& kv : B->buckets) kv.second.release();
+    if (B->hdesc) cudaFreeHost(B->hdesc);
+    if (B->d_err) cudaFree(B->d_err);
+    if (B->d_stats) cudaFree(B->d_stats);
+    for (auto& e : B->ev)
+        if (e) cudaEventDestroy(e);
+    if (B->desc_done) cudaEventDestroy(B->desc_done);
+    if (B->st) cudaStreamDestroy(B->st);
+    delete B;
+}
+
+int jt_batch_add(jt_batch* B, const jt_config* cfg, const float* pos_p, const float* vel_p, size_t n_p,
+                 const float* pos_m, const float* vel_m, size_t n_m, int mem, int* box_id)
+{
+    if (!B || !cfg || !box_id || (mem != JT_MEM_HOST && mem != JT_MEM_DEVICE)) return JT_EINVAL;
+    if ((n_p && !pos_p) || (n_m && !pos_m)) return JT_EINVAL;
+    if (n_p >= (size_t)1 << 30 || n_m >= (size_t)1 << 30) return JT_EINVAL;
+    int id = -1;
+    JT_TRY(jtb_add_empty(B, cfg, (int64_t)n_p, (int64_t)n_m, &id));
+    jt_box_state* b = B->boxes[id];
+    const float* pp[2] = {pos_p, pos_m};
+    const float* vv[2] = {vel_p, vel_m};
+    int r = JT_OK;
+    float* stage = nullptr;
+    if (mem == JT_MEM_HOST && cudaMalloc(&stage, sizeof(float) * 3 * std::max(n_p, n_m)) != cudaSuccess)
+        r = JT_ENOMEM;
+    for (int s = 0; s < 2 && r == JT_OK; s++) {
+        const int64_t n = b->n[s];
+        if (n == 0) continue;
+        const float* src = pp[s];
+        if (mem == JT_MEM_HOST) {
+            if (cudaMemcpyAsync(stage, src, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, B->st) != cudaSuccess)
+                r = JT_ECUDA;
+            src = stage;
+        }
+        jt_launch_aos_in(src, n, b->pos[s], b->id[s], B->st);
+        if (vv[s]) {
+            const float* vs = vv[s];
+            if (mem == JT_MEM_HOST) {
+                cudaStreamSynchronize(B->st);
+                if (cudaMemcpyAsync(stage, vs, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, B->st) != cudaSuccess)
+                    r = JT_ECUDA;
+                vs = stage;
+            }
+            jt_launch_aos_in(vs, n, b->vel[s], nullptr, B->st);
+        } else {
+            cudaMemsetAsync(b->vel[s], 0, sizeof(float4) * n, B->st);
+        }
+        if (cudaStreamSynchronize(B->st) != cudaSuccess) r = JT_ECUDA;
+    }
+    if (stage) cudaFree(stage);
+    if (r == JT_OK && cudaGetLastError() != cudaSuccess) r = JT_ECUDA;
+    if (r != JT_OK) {
+        jt_batch_remove(B, id);
+        return r;
+    }
+    *box_id = id;
+    return JT_OK;
+}
+
+int jt_batch_remove(jt_batch* B, int box_id)
+{
+    if (!box_id_ok(B, box_id)) return JT_EINVAL;
+    cudaStreamSynchronize(B->st);
+    box_release(B->boxes[box_id]);
+    delete B->boxes[box_id];
+    B->boxes[box_id] = nullptr;
+    return JT_OK;
+}
+
+int jt_batch_forces(jt_batch* B, const int* ids, int n_ids, int part)
+{
+    if (!B || part < 1 || part > 3) return JT_EINVAL;
+    B->tm = jt_timings{};
+    cudaEvent_t t0, t1;
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    cudaEventRecord(t0, B->st);
+    int r = jtb_force_pass(B, ids, n_ids, part, 0.0f, nullptr);
+    cudaEventRecord(t1, B->st);
+    int e = finish(B);
+    if (r == JT_OK) r = e;
+    if (r == JT_OK) B->tm.total_ms = elapsed(t0, t1);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    return r;
+}
+
+int jt_batch_step(jt_batch* B, const int* ids, int n_ids, const jt_step_args* args, int nsteps)
+{
+    if (!B || nsteps < 0 || !args) return JT_EINVAL;
+    std::vector<int> v;
+    JT_TRY(valid_ids(B, ids, n_ids, v));
+    std::vector<jt_box_step> steps(v.size());
+    for (size_t k = 0; k < v.size(); k++) {
+        const jt_step_args& a = args[k];
+        if (!std::isfinite(a.dt) || !std::isfinite(a.hubble) || !std::isfinite(a.dtau_per_dt)) return JT_EINVAL;
+        // FP64 step factors, applied in FP32 (kicks and drifts use 0.5 dt and
+        // dt; halving a float is exact)
+        steps[k].dt = (float)a.dt;
+        steps[k].drag = (float)(a.hubble * a.dtau_per_dt);
+    }
+    if (nsteps == 0) return JT_OK;
+    B->tm = jt_timings{};
+    cudaEvent_t t0, t1, k0, k1;
+    cudaEventCreate(&t0); cudaEventCreate(&t1); cudaEventCreate(&k0); cudaEventCreate(&k1);
+    cudaEventRecord(t0, B->st);
+    int r = JT_OK;
+    bool all_valid = true;
+    for (int id : v) all_valid = all_valid && B->boxes[id]->acc_valid;
+    if (!all_valid) {
+        r = jtb_force_pass(B, v.data(), (int)v.size(), JT_PART_ALL, 0.0f, steps.data());
+        if (r == JT_OK) r = finish(B);
+    }
+    Plan& P = B->plan;
+    if (r == JT_OK) r = build_plan(B, v, steps.data(), P);
+    double kd = 0.0;
+    for (int k = 0; k < nsteps && r == JT_OK; k++) {
+        cudaEventRecord(k0, B->st);
+        if (k == 0) jt_b_kick(P.d_pre, P.d_bx, P.d_pp, (int)P.pre.size(), P.npart, 0.5f, B->st);
+        jt_b_drift(P.d_pre, P.d_bx, P.d_pp, (int)P.pre.size(), P.npart, 1.0f, B->st);
+        B->tm.launches += (k == 0 ? 2 : 1);
+        cudaEventRecord(k1, B->st);
+        // closing half kick, merged with the next step's opening half kick
+        r = force_pass(B, P, JT_PART_ALL, k + 1 < nsteps ? 1.0f : 0.5f);
+        if (r != JT_OK) break;
+        r = finish(B);
+        if (r != JT_OK) break;
+        kd += elapsed(k0, k1);
+    }
+    cudaEventRecord(t1, B->st);
+    if (cudaStreamSynchronize(B->st) != cudaSuccess && r == JT_OK) r = JT_ECUDA;
+    if (r == JT_OK) {
+        B->tm.total_ms = elapsed(t0, t1);
+        B->tm.kick_drift_ms = kd;
+    }
+    cudaEventDestroy(t0); cudaEventDestroy(t1); cudaEventDestroy(k0); cudaEventDestroy(k1);
+    return r;
+}
+
+int jt_batch_get_accel(jt_batch* B, int box_id, float* acc_p, float* acc_m, int mem)
+{
+    if (!box_id_ok(B, box_id) || (mem != JT_MEM_HOST && mem != JT_MEM_DEVICE)) return JT_EINVAL;
+    jt_box_state* b = B->boxes[box_id];
+    if (!b->acc_valid) return JT_ESTATE;
+    JT_TRY(read_out(B, b->acc[0], b->id[0], b->n[0], acc_p, mem));
+    JT_TRY(read_out(B, b->acc[1], b->id[1], b->n[1], acc_m, mem));
+    JT_CU(cudaStreamSynchronize(B->st));
+    return JT_OK;
+}
+
+int jt_batch_get_state(jt_batch* B, int box_id, float* pos_p, float* vel_p, float* pos_m, float* vel_m, int mem)
+{
+    if (!box_id_ok(B, box_id) || (mem != JT_MEM_HOST && mem != JT_MEM_DEVICE)) return JT_EINVAL;
+    jt_box_state* b = B->boxes[box_id];
+    JT_TRY(read_out(B, b->pos[0], b->id[0], b->n[0], pos_p, mem));
+    JT_TRY(read_out(B, b->vel[0], b->id[0], b->n[0], vel_p, mem));
+    JT_TRY(read_out(B, b->pos[1], b->id[1], b->n[1], pos_m, mem));
+    JT_TRY(read_out(B, b->vel[1], b->id[1], b->n[1], vel_m, mem));
+    JT_CU(cudaStreamSynchronize(B->st));
+    return JT_OK;
+}
+
+int jt_batch_box_info(jt_batch* B, int box_id, size_t* n_p, size_t* n_m, size_t* bytes)
+{
+    if (!box_id_ok(B, box_id)) return JT_EINVAL;
+    jt_box_state* b = B->boxes[box_id];
+    if (n_p) *n_p = (size_t)b->n[0];
+    if (n_m) *n_m = (size_t)b->n[1];
+    if (bytes) *bytes = b->bytes;
+    return JT_OK;
+}
+
+int jt_batch_memory(jt_batch* B, size_t* persistent, size_t* scratch)
+{
+    if (!B) return JT_EINVAL;
+    size_t p = 0, s = 0;
+    for (auto* b : B->boxes)
+        if (b) p += b->bytes;
+    s += B->child.bytes() + B->range.bytes() + B->parent.bytes() + B->flag.bytes() + B->com.bytes() +
+         B->bmin.bytes() + B->bmax.bytes() + B->quad0.bytes() + B->quad1.bytes() + B->m30.bytes() +
+         B->vals.bytes() + B->vals_alt.bytes() + B->keys_alt.bytes() + B->hist.bytes() + B->status.bytes() +
+         B->tickets.bytes() + B->desc.bytes();
+    for (auto& kv : B->buckets) s += (size_t)kv.second.cap * grid_bytes(kv.first, B->ngrid);
+    if (persistent) *persistent = p;
+    if (scratch) *scratch = s;
+    return JT_OK;
+}
+
+int jt_batch_estimate(const jt_config* cfg, size_t n_p, size_t n_m, size_t* persistent, size_t* scratch)
+{
+    if (validate_box_config(cfg) != JT_OK) return JT_EINVAL;
+    const size_t n = n_p + n_m;
+    const int64_t M = cfg->pm_grid;
+    if (persistent) *persistent = n * (5 * sizeof(float4) + 2 * sizeof(int)) + 2 * (size_t)M * sizeof(float4);
+    if (scratch) {
+        // tree: 2n nodes (child, parent, com, bmin, bmax, quad0, quad1) and n
+        // (range, flag); sort: m30, vals, vals_alt, keys_alt and the look-back
+        // words (4 passes x 256 per 4096-element tile); PM grids of one box
+        size_t tree = 2 * n * (sizeof(int2) + sizeof(int) + 4 * sizeof(float4) + sizeof(float2)) +
+                      n * (sizeof(int2) + sizeof(int));
+        size_t sort = n * 4 * sizeof(uint32_t) + (n / 4096 + 2) * 4 * 256 * sizeof(uint32_t);
+        *scratch = tree + sort + grid_bytes(M, box_ngrid(*cfg));
+    }
+    return JT_OK;
+}
+
+int jt_batch_get_timings(jt_batch* B, jt_timings* t)
+{
+    if (!B || !t) return JT_EINVAL;
+    *t = B->tm;
+    return JT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,42 @@
+// Internal interface of the batched engine (jt_batch.cu) used by the
+// single-box handle (jt_api.cu): an accurate-mode handle is a batch of one box
+// whose particle buffers it fills and reads itself.
+#pragma once
+#include "jt_internal.cuh"
+
+// Persistent device state of one box of a batch.  The reorder of every force
+// pass moves the state into the b-buffers and the host swaps the pointers, so
+// callers must re-read pos/vel/id after each pass.
+struct jt_box_state {
+    jt_config cfg;
+    int64_t n[2] = {0, 0};
+    float mass[2] = {0.f, 0.f};
+    float4 *pos[2] = {}, *vel[2] = {}, *acc[2] = {}, *pos_b[2] = {}, *vel_b[2] = {};
+    int *id[2] = {}, *id_b[2] = {};
+    float4* tabs = nullptr;      // per-axis k tables (2M float4)
+    bool acc_valid = false;      // acc belongs to the current positions
+    int M = 0, order = 3, ngrid = 2;
+    size_t bytes = 0;            // device bytes held by this box
+};
+
+// Per-box step arguments of a batched force pass (kick fused into the walk).
+struct jt_box_step {
+    float dt;       // the box's step; kicks/drifts apply a fraction of it
+    float drag;     // H * dtau_per_dt
+};
+
+// Allocate a box whose particle arrays the caller fills (pos/vel/id on the
+// batch's stream); n_p + n_m > 0.  The config must be ACCURATE.
+int jtb_add_empty(jt_batch* B, const jt_config* cfg, int64_t n_p, int64_t n_m, int* box_id);
+jt_box_state* jtb_box(jt_batch* B, int box_id);
+cudaStream_t jtb_stream(jt_batch* B);
+// Enqueue one force pass (sort, trees, PM, walk) over the listed boxes;
+// kick_frac != 0 fuses the closing kick (kick_frac * dt) into the walk.  No
+// host synchronisation; stage times are added to the batch's timings when
+// jtb_finish is called.
+int jtb_force_pass(jt_batch* B, const int* ids, int n_ids, int parts, float kick_frac,
+                   const jt_box_step* steps);
+// Synchronise, read the device error word and add the pass's stage times.
+int jtb_finish(jt_batch* B);
+void jtb_reset_timings(jt_batch* B);
+int64_t jtb_phase(jt_batch* B, int i);

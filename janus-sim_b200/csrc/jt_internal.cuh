@@ -58,6 +58,61 @@ struct jt_sort_ws {
     int max_passes;
 };
 
+// ---------------------------------------------------------------- batches
+// A batch advances several independent boxes with ONE launch per stage.
+// Work is described by segments (one per box and species) and boxes; every
+// batched kernel maps its flattened work items (particles, tiles, nodes,
+// 32-particle groups) to a segment or box through an exclusive prefix table
+// (jt_find: binary search, log2(#segments) steps).  A single box is the batch
+// of one (two segments).
+struct jt_seg_dev {
+    float4* pos;          // state, Morton order of the last build
+    float4* vel;
+    float4* acc;
+    float4* pos_b;        // reorder targets (swapped after each build)
+    float4* vel_b;
+    int* id;
+    int* id_b;
+    int64_t n;
+    jt_tree_dev tree;     // tree.m30 doubles as the sort key array
+    uint32_t* vals;       // sort values (permutation) and its ping-pong
+    uint32_t* vals_alt;
+    uint32_t* keys_alt;
+    uint32_t* hist;       // [4][256] digit counts -> bases
+    uint32_t* status;     // [4][tiles][256] look-back words
+    int box;              // owning box
+    int species;          // 0 = m+, 1 = m-
+};
+
+struct jt_box_dev {
+    float L, halfL, h_inv;
+    float rc2, eps2, c, theta2;
+    float mass[2];
+    float box_half;       // float(L/2), the reference's Morton box_half
+    float kick_drag;      // H * dtau of the current step
+    float dt;             // step of this box (kicks and drifts take a fraction of it)
+    int M, order, ngrid;
+    int T, tile_shift, ntiles;
+    float* rho;           // ngrid grids
+    float2* rho_k;        // ngrid spectra
+    float2* force_k;      // 3*ngrid spectra
+    const float4* tabs;   // 2*M per-axis k tables
+    float* force;         // 3*ngrid force grids
+    int4* ranges;         // per-tile particle ranges of both species
+    int seg[2];           // segment index of each species (-1: none)
+};
+
+__device__ __forceinline__ int jt_find(const int64_t* __restrict__ prefix, int count, int64_t i)
+{
+    // largest b with prefix[b] <= i (prefix[0] = 0, prefix[count] = total)
+    int lo = 0, hi = count - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= i) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
 // ---------------------------------------------------------------- math
 // Short-range factor of the Gaussian split (potential erfc(r/2r_s)/r):
 //   S(x) = erfc(x) + (2/sqrt(pi)) x exp(-x^2),  x = r / (2 r_s).
@@ -70,7 +125,7 @@ __device__ __forceinline__ float jt_erfc_as(float x, float e)
     const float p = 0.3275911f;
     const float a1 = 0.254829592f, a2 = -0.284496736f, a3 = 1.421413741f,
                 a4 = -1.453152027f, a5 = 1.061405429f;
-    float t = __frcp_rn(fmaf(p, x, 1.0f));
+    float t = __fdividef(1.0f, fmaf(p, x, 1.0f));   // fast reciprocal; t in (0, 1]
     float poly = fmaf(t, fmaf(t, fmaf(t, fmaf(t, a5, a4), a3), a2), a1);
     return t * poly * e;
 }
@@ -137,8 +192,6 @@ void jt_launch_morton(const float4* pos, const int* id, int64_t n, float box_hal
                       uint32_t* key32, uint64_t* key64, uint32_t* vals, cudaStream_t st);
 // Stable LSD onesweep sort of (key, val) in place (keys/vals ping-pong through
 // ws); shifts = bit offsets of the 8-bit digits, low to high.
-int jt_radix_sort_u32(uint32_t* keys, uint32_t* vals, int64_t n, const int* shifts,
-                      int npass, jt_sort_ws* ws, unsigned* d_err, cudaStream_t st);
 int jt_radix_sort_u64(uint64_t* keys, uint32_t* vals, int64_t n, const int* shifts,
                       int npass, jt_sort_ws* ws, unsigned* d_err, cudaStream_t st);
 // gather state by permutation: out[i] = in[perm[i]]
@@ -148,39 +201,46 @@ void jt_launch_reorder(const uint32_t* perm, int64_t n, const float4* pos_in,
 void jt_launch_split_keys(const uint64_t* key64, int64_t n, uint32_t* m30, uint32_t* tie,
                           cudaStream_t st);
 
+// batched sort (jt_sort.cu): per-segment hist/status must be zeroed and the
+// 4 tickets reset by the caller before the call
+int jt_b_sort_reorder(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, int nseg,
+                      const int64_t* d_pprefix, int64_t ntotal, const int64_t* d_tprefix,
+                      int64_t ntiles, uint32_t* d_tickets, unsigned* d_err, cudaStream_t st);
+int jt_sort_tile_size();
+
 // tree (jt_tree.cu)
 void jt_launch_karras(jt_tree_dev t, cudaStream_t st);
-void jt_launch_moments(jt_tree_dev t, const float4* pos, float mass, float box_half,
-                       int rcompat, cudaStream_t st);
+void jt_launch_moments_rc(jt_tree_dev t, const float4* pos, float mass, float box_half,
+                          cudaStream_t st);
 
-// PM (jt_pm.cu)
+// batched tree build over segments (jt_tree.cu)
+void jt_b_build_trees(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, int nseg,
+                      const int64_t* d_iprefix, int64_t ninternal, const int64_t* d_pprefix,
+                      int64_t nleaves, cudaStream_t st);
+
+// RCOMPAT PM (jt_pm.cu): one CIC grid of the caller-order particles, the
+// reference's Green's function in place, C2R to the potential.
 struct jt_pm_dev {
     int M;
     double L;
-    int order;               // 2 = CIC, 3 = TSC (accurate); 2 in compatibility mode
-    int ngrid;               // 1, or 2 with interlacing
-    float* rho;              // ngrid grids
-    cufftComplex* rho_k;     // ngrid spectra
-    cufftComplex* force_k;   // 3*ngrid spectra + axis tables (ACCURATE) or 1 (RCOMPAT)
-    float4* tabs;            // 2*M float4 axis tables (inside force_k)
-    float* force;            // 3*ngrid grids (ACCURATE) or 1 potential grid (RCOMPAT)
-    int4* ranges;            // per-tile particle ranges
+    int order;               // 2 (CIC)
+    int ngrid;               // 1
+    float* rho;
+    cufftComplex* force_k;   // potential spectrum
+    float* force;            // potential grid
     cufftHandle plan_r2c, plan_c2r;
     int plans_ready;
 };
-void jt_launch_deposit(const float4* pos0, int64_t n0, float q0, const float4* pos1,
-                       int64_t n1, float q1, float* rho, int M, float L, int rcompat,
-                       cudaStream_t st);
-void jt_launch_kspace(const cufftComplex* rho_k, cufftComplex* out, int M, double L,
-                      double r_s, int k_min, int rcompat, int interlace, const float4* tabs,
-                      cudaStream_t st);
+void jt_launch_kspace_rc(cufftComplex* data, int M, double L, double r_s, int k_min, cudaStream_t st);
 int jt_pm_tile_edge(int M);
-// per-tile particle ranges [x,y) of species 0 and [z,w) of species 1
-void jt_launch_tile_ranges(const uint32_t* m0, int64_t n0, const uint32_t* m1, int64_t n1,
-                           int M, int4* ranges, cudaStream_t st);
-int jt_launch_deposit_tiled(const float4* pos0, float q0, const float4* pos1, float q1,
-                            const int4* ranges, float* rho, int M, float L, int order,
-                            int ngrid, cudaStream_t st);
+
+// batched PM stages (jt_pm.cu)
+void jt_b_tile_ranges(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_tprefix,
+                      int nbox, int64_t ntiles, cudaStream_t st);
+int jt_b_deposit(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_tprefix,
+                 int nbox, int64_t ntiles, int order, int ngrid, int T, cudaStream_t st);
+void jt_b_kspace(const jt_box_dev* d_boxes, const int64_t* d_kprefix, int nbox, int64_t nmodes,
+                 int interlace, int k_min, cudaStream_t st);
 
 // walk (jt_walk.cu)
 struct jt_walk_params {
@@ -196,13 +256,19 @@ struct jt_walk_params {
     int ngrid;          // PM grids (2 with interlacing)
     int parts;          // JT_PART_* bits: 1 = PM, 2 = tree
 };
+// Batched accurate walk over every segment's 32-particle groups (gprefix);
 // stats[0] pair interactions inside r_cut, [1] node (multipole) interactions,
 // [2] candidate particles distance-tested
-void jt_launch_walk_accurate(const jt_walk_params& p, const float4* const pos[2],
-                             const int64_t n[2], const jt_tree_dev tree[2],
-                             const float* force3, float4* const acc[2],
-                             float4* const vel[2], float kick_dt, float kick_drag,
-                             unsigned long long* stats, unsigned* d_err, cudaStream_t st);
+int jt_b_walk(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_gprefix, int nseg,
+              int64_t ngroups, int order, int ngrid, int parts, float kick_frac,
+              unsigned long long* stats, unsigned* d_err, cudaStream_t st);
+
+// kick v += (a - drag v) frac*dt and drift x += v frac*dt with each box's own
+// dt and drag (jt_box_dev)
+void jt_b_kick(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_prefix, int nseg,
+               int64_t ntotal, float frac, cudaStream_t st);
+void jt_b_drift(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_prefix, int nseg,
+                int64_t ntotal, float frac, cudaStream_t st);
 
 struct jt_rc_params {
     float theta2, eps2, r_cut, box_half_q, r_s;   // quantised tree parameters

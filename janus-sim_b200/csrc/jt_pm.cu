@@ -51,126 +51,7 @@ __device__ __forceinline__ int64_t lower_bound_tile(const uint32_t* __restrict__
     return lo;
 }
 
-__global__ void k_tile_ranges(const uint32_t* __restrict__ m0, int64_t n0,
-                              const uint32_t* __restrict__ m1, int64_t n1, int shift, int ntiles,
-                              int4* __restrict__ ranges)
-{
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= ntiles) return;
-    int4 r;
-    r.x = (int)lower_bound_tile(m0, n0, (uint32_t)t, shift);
-    r.y = (int)lower_bound_tile(m0, n0, (uint32_t)t + 1, shift);
-    r.z = (int)lower_bound_tile(m1, n1, (uint32_t)t, shift);
-    r.w = (int)lower_bound_tile(m1, n1, (uint32_t)t + 1, shift);
-    ranges[t] = r;
-}
-
 constexpr int kTileEdge = 16;
-
-template <int ORDER, int NG>
-__global__ void __launch_bounds__(256)
-k_deposit_tiled(const float4* __restrict__ pos0, float q0, const float4* __restrict__ pos1, float q1,
-                const int4* __restrict__ ranges, int shift, int T, float* __restrict__ rho, int M,
-                float halfL, float hinv)
-{
-    extern __shared__ float tile[];
-    const int S = T + 3;               // cells [origin-1, origin+T+1]
-    const int S3 = S * S * S;
-    // tile id = Morton code of the tile (m30 >> shift); its first cell, minus the halo
-    const uint32_t t = blockIdx.x;
-    (void)shift;
-    const int bx = (int)compact3(t) * T - 1;
-    const int by = (int)compact3(t >> 1) * T - 1;
-    const int bz = (int)compact3(t >> 2) * T - 1;
-    for (int c = threadIdx.x; c < NG * S3; c += blockDim.x) tile[c] = 0.0f;
-    __syncthreads();
-    const int4 r = ranges[t];
-    const int mask = M - 1;
-    const int64_t G = (int64_t)M * M * M;
-    const int n0 = r.y - r.x, n1 = r.w - r.z;
-    for (int k = threadIdx.x; k < n0 + n1; k += blockDim.x) {
-        float4 p;
-        float q;
-        if (k < n0) { p = pos0[r.x + k]; q = q0; } else { p = pos1[r.z + k - n0]; q = q1; }
-        float gx = (p.x + halfL) * hinv, gy = (p.y + halfL) * hinv, gz = (p.z + halfL) * hinv;
-#pragma unroll
-        for (int b = 0; b < NG; b++) {
-            float sh = 0.5f * b;
-            float wx[ORDER], wy[ORDER], wz[ORDER];
-            int ix = jt_stencil<ORDER>(gx - sh, wx);
-            int iy = jt_stencil<ORDER>(gy - sh, wy);
-            int iz = jt_stencil<ORDER>(gz - sh, wz);
-            int lx = ix - bx, ly = iy - by, lz = iz - bz;
-            bool inside = lx >= 0 && ly >= 0 && lz >= 0 && lx + ORDER <= S && ly + ORDER <= S &&
-                          lz + ORDER <= S;
-            if (inside) {
-                float* tb_ = tile + b * S3;
-#pragma unroll
-                for (int c = 0; c < ORDER; c++)
-#pragma unroll
-                    for (int bb = 0; bb < ORDER; bb++) {
-                        float wyz = q * wz[c] * wy[bb];
-                        float* row = tb_ + ((lz + c) * S + (ly + bb)) * S + lx;
-#pragma unroll
-                        for (int a = 0; a < ORDER; a++) atomicAdd(row + a, wyz * wx[a]);
-                    }
-            } else {
-                // particle outside its Morton tile's box (float rounding at a tile
-                // edge or a position outside the box): reduce straight into the grid
-                float* gb = rho + b * G;
-#pragma unroll
-                for (int c = 0; c < ORDER; c++)
-#pragma unroll
-                    for (int bb = 0; bb < ORDER; bb++) {
-                        float wyz = q * wz[c] * wy[bb];
-                        int64_t row = ((int64_t)((iz + c) & mask) * M + ((iy + bb) & mask)) * M;
-#pragma unroll
-                        for (int a = 0; a < ORDER; a++) atomicAdd(gb + row + ((ix + a) & mask), wyz * wx[a]);
-                    }
-            }
-        }
-    }
-    __syncthreads();
-    for (int c = threadIdx.x; c < NG * S3; c += blockDim.x) {
-        float v = tile[c];
-        if (v == 0.0f) continue;
-        int b = c / S3, rem = c - b * S3;
-        int lz = rem / (S * S), ly = (rem / S) % S, lx = rem % S;
-        int64_t idx = ((int64_t)((bz + lz) & mask) * M + ((by + ly) & mask)) * M + ((bx + lx) & mask);
-        atomicAdd(rho + b * G + idx, v);
-    }
-}
-
-// ---- plain deposit (no tiling): CIC, one grid -- used for tiny grids
-__global__ void k_deposit(const float4* __restrict__ pos0, int64_t n0, float q0,
-                          const float4* __restrict__ pos1, int64_t n1, float q1,
-                          float* __restrict__ rho, int M, float halfL, float hinv)
-{
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n0 + n1) return;
-    float4 p;
-    float q;
-    if (i < n0) { p = pos0[i]; q = q0; } else { p = pos1[i - n0]; q = q1; }
-    float gx = (p.x + halfL) * hinv, gy = (p.y + halfL) * hinv, gz = (p.z + halfL) * hinv;
-    float fx0 = floorf(gx), fy0 = floorf(gy), fz0 = floorf(gz);
-    float fx = gx - fx0, fy = gy - fy0, fz = gz - fz0;
-    int mask = M - 1;
-    int ix = (int)fx0 & mask, iy = (int)fy0 & mask, iz = (int)fz0 & mask;
-    int ix1 = (ix + 1) & mask, iy1 = (iy + 1) & mask, iz1 = (iz + 1) & mask;
-    int64_t MM = (int64_t)M * M;
-    int64_t r00 = (int64_t)iy * M + (int64_t)iz * MM, r10 = (int64_t)iy1 * M + (int64_t)iz * MM;
-    int64_t r01 = (int64_t)iy * M + (int64_t)iz1 * MM, r11 = (int64_t)iy1 * M + (int64_t)iz1 * MM;
-    float wx0 = 1.0f - fx, wy0 = 1.0f - fy, wz0 = 1.0f - fz;
-    float a00 = q * wy0 * wz0, a10 = q * fy * wz0, a01 = q * wy0 * fz, a11 = q * fy * fz;
-    atomicAdd(rho + r00 + ix, a00 * wx0);
-    atomicAdd(rho + r00 + ix1, a00 * fx);
-    atomicAdd(rho + r10 + ix, a10 * wx0);
-    atomicAdd(rho + r10 + ix1, a10 * fx);
-    atomicAdd(rho + r01 + ix, a01 * wx0);
-    atomicAdd(rho + r01 + ix1, a01 * fx);
-    atomicAdd(rho + r11 + ix, a11 * wx0);
-    atomicAdd(rho + r11 + ix1, a11 * fx);
-}
 
 // ---- compatibility deposit: the reference's coordinates and weights
 // (fmodf wrap, (int) truncation, weight wx*wy*wz in float), signed mass
@@ -207,60 +88,6 @@ __global__ void k_deposit_rc(const float4* __restrict__ pos, const int8_t* __res
             }
 }
 
-// Accurate k-space kernel.  Per-axis tables (index n = 0..M-1):
-//   ta[n] = { k_n, gradient factor k_n, exp(-k_n^2 r_s^2) / sinc^(2 order)(pi n/M), |n| }
-//   tb[n] = { cos(k_n h/2), sin(k_n h/2), 0, 0 }   (interlacing phase)
-template <bool IL>
-__global__ void k_kspace_acc(const float2* __restrict__ rho_k, float2* __restrict__ out, int M,
-                             const float4* __restrict__ ta, const float4* __restrict__ tb,
-                             float norm, int k_min, int64_t Gc)
-{
-    int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= Gc) return;
-    const int Mh = M / 2 + 1;
-    const int kx = (int)(idx % Mh);
-    const int64_t r = idx / Mh;
-    const int ky = (int)(r % M);
-    const int kz = (int)(r / M);
-    const float4 ax = __ldg(&ta[kx]), ay = __ldg(&ta[ky]), az = __ldg(&ta[kz]);
-    const float k2 = ax.x * ax.x + ay.x * ay.x + az.x * az.x;
-    const int half = M / 2;
-    const int nx = (int)ax.w, ny = (int)ay.w, nz = (int)az.w;
-    const int kmax = max(max(nx, ny), nz);
-    const bool keep = k2 > 0.0f && kmax >= k_min && nx != half && ny != half && nz != half;
-    float2 F0 = make_float2(0.f, 0.f), F1 = F0, F2 = F0;
-    float er = 1.0f, ei = 0.0f;  // exp(+i theta), theta = (kx + ky + kz) h / 2
-    if (keep) {
-        float2 z = rho_k[idx];
-        if (IL) {
-            float4 bx = __ldg(&tb[kx]), by = __ldg(&tb[ky]), bz = __ldg(&tb[kz]);
-            // exp(+i theta) = prod (c + i s)
-            float pr = bx.x * by.x - bx.y * by.y, pi = bx.x * by.y + bx.y * by.x;
-            er = pr * bz.x - pi * bz.y;
-            ei = pr * bz.y + pi * bz.x;
-            float2 w = rho_k[Gc + idx];
-            // rho = (rhoA + rhoB exp(-i theta)) / 2
-            z.x = 0.5f * (z.x + (w.x * er + w.y * ei));
-            z.y = 0.5f * (z.y + (w.y * er - w.x * ei));
-        }
-        float green = -12.566370614f * norm * (ax.z * ay.z * az.z) / k2;
-        float pr = z.x * green, pi = z.y * green;
-        // a_d(k) = -i k_d phi(k) = k_d (pi, -pr)
-        F0 = make_float2(ax.y * pi, -ax.y * pr);
-        F1 = make_float2(ay.y * pi, -ay.y * pr);
-        F2 = make_float2(az.y * pi, -az.y * pr);
-    }
-    out[idx] = F0;
-    out[Gc + idx] = F1;
-    out[2 * Gc + idx] = F2;
-    if (IL) {
-        // forces at the shifted nodes: multiply by exp(+i theta)
-        out[3 * Gc + idx] = make_float2(F0.x * er - F0.y * ei, F0.x * ei + F0.y * er);
-        out[4 * Gc + idx] = make_float2(F1.x * er - F1.y * ei, F1.x * ei + F1.y * er);
-        out[5 * Gc + idx] = make_float2(F2.x * er - F2.y * ei, F2.x * ei + F2.y * er);
-    }
-}
-
 // the reference's apply_green_kernel + normalisation, FP32, in place:
 // -4 pi / k^2 * exp(-k^2 r_s^2) * 1/M^3; modes with max|k_i| < k_min and k = 0 zeroed
 __global__ void k_kspace_rc(float2* __restrict__ data, int M, float dk, float rs2, float norm,
@@ -290,61 +117,6 @@ __global__ void k_kspace_rc(float2* __restrict__ data, int M, float dk, float rs
 
 int jt_pm_tile_edge(int M) { return M < kTileEdge ? M : kTileEdge; }
 
-void jt_launch_tile_ranges(const uint32_t* m0, int64_t n0, const uint32_t* m1, int64_t n1, int M,
-                           int4* ranges, cudaStream_t st)
-{
-    int T = jt_pm_tile_edge(M);
-    int W = 1024 / M * T;  // tile edge in Morton cells (power of two)
-    int lw = 0;
-    while ((1 << lw) < W) lw++;
-    int shift = 3 * lw;
-    int ntiles = (M / T) * (M / T) * (M / T);
-    k_tile_ranges<<<(ntiles + 255) / 256, 256, 0, st>>>(m0, n0, m1, n1, shift, ntiles, ranges);
-}
-
-int jt_launch_deposit_tiled(const float4* pos0, float q0, const float4* pos1, float q1,
-                            const int4* ranges, float* rho, int M, float L, int order, int ngrid,
-                            cudaStream_t st)
-{
-    int T = jt_pm_tile_edge(M);
-    int W = 1024 / M * T;
-    int lw = 0;
-    while ((1 << lw) < W) lw++;
-    int shift = 3 * lw;
-    int ntiles = (M / T) * (M / T) * (M / T);
-    int S = T + 3;
-    size_t smem = sizeof(float) * (size_t)ngrid * S * S * S;
-    float halfL = 0.5f * L, hinv = (float)M / L;
-#define JT_DEP(O, NG)                                                                          \
-    do {                                                                                       \
-        static bool attr = false;                                                              \
-        if (!attr) {                                                                           \
-            cudaFuncSetAttribute(k_deposit_tiled<O, NG>,                                       \
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);      \
-            attr = true;                                                                       \
-        }                                                                                      \
-        k_deposit_tiled<O, NG><<<ntiles, 256, smem, st>>>(pos0, q0, pos1, q1, ranges, shift, T, \
-                                                          rho, M, halfL, hinv);                \
-    } while (0)
-    if (order == 2 && ngrid == 1) JT_DEP(2, 1);
-    else if (order == 2 && ngrid == 2) JT_DEP(2, 2);
-    else if (order == 3 && ngrid == 1) JT_DEP(3, 1);
-    else if (order == 3 && ngrid == 2) JT_DEP(3, 2);
-    else return JT_EINVAL;
-#undef JT_DEP
-    return cudaGetLastError() == cudaSuccess ? JT_OK : JT_ECUDA;
-}
-
-void jt_launch_deposit(const float4* pos0, int64_t n0, float q0, const float4* pos1, int64_t n1,
-                       float q1, float* rho, int M, float L, int rcompat, cudaStream_t st)
-{
-    (void)rcompat;
-    int64_t n = n0 + n1;
-    if (n <= 0) return;
-    k_deposit<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(pos0, n0, q0, pos1, n1, q1, rho, M,
-                                                           0.5f * L, (float)M / L);
-}
-
 void jt_launch_rcompat_deposit(const float4* pos_caller, const int8_t* sign_caller, int64_t n_all,
                                const float mass[2], float* rho, int M, float box_half,
                                float inv_cell, float inv_vol, cudaStream_t st)
@@ -354,21 +126,233 @@ void jt_launch_rcompat_deposit(const float4* pos_caller, const int8_t* sign_call
         pos_caller, sign_caller, n_all, mass[0], mass[1], rho, M, box_half, inv_cell, inv_vol);
 }
 
-void jt_launch_kspace(const cufftComplex* rho_k, cufftComplex* out, int M, double L, double r_s,
-                      int k_min, int rcompat, int interlace, const float4* tabs, cudaStream_t st)
+void jt_launch_kspace_rc(cufftComplex* data, int M, double L, double r_s, int k_min, cudaStream_t st)
 {
     int64_t Gc = (int64_t)M * M * (M / 2 + 1);
     float norm = (float)(1.0 / ((double)M * M * M));
     unsigned g = (unsigned)((Gc + 255) / 256);
-    if (rcompat) {
-        k_kspace_rc<<<g, 256, 0, st>>>((float2*)out, M, (float)(2.0 * 3.14159265358979323846 / L),
-                                       (float)(r_s * r_s), norm, k_min, Gc);
-        return;
+    k_kspace_rc<<<g, 256, 0, st>>>((float2*)data, M, (float)(2.0 * 3.14159265358979323846 / L),
+                                   (float)(r_s * r_s), norm, k_min, Gc);
+}
+
+// ======================================================================
+// Batched versions over boxes: one launch per stage for the whole batch.
+// ======================================================================
+namespace {
+
+__global__ void k_b_tile_ranges(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ boxes,
+                                const int64_t* __restrict__ tprefix, int nbox)
+{
+    int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= tprefix[nbox]) return;
+    const int b = jt_find(tprefix, nbox, q);
+    const jt_box_dev& B = boxes[b];
+    const uint32_t t = (uint32_t)(q - tprefix[b]);
+    int4 r = make_int4(0, 0, 0, 0);
+    if (B.seg[0] >= 0) {
+        const jt_seg_dev& S = segs[B.seg[0]];
+        r.x = (int)lower_bound_tile(S.tree.m30, S.n, t, B.tile_shift);
+        r.y = (int)lower_bound_tile(S.tree.m30, S.n, t + 1, B.tile_shift);
     }
-    if (interlace)
-        k_kspace_acc<true><<<g, 256, 0, st>>>((const float2*)rho_k, (float2*)out, M, tabs, tabs + M,
-                                              norm, k_min, Gc);
-    else
-        k_kspace_acc<false><<<g, 256, 0, st>>>((const float2*)rho_k, (float2*)out, M, tabs, tabs + M,
-                                               norm, k_min, Gc);
+    if (B.seg[1] >= 0) {
+        const jt_seg_dev& S = segs[B.seg[1]];
+        r.z = (int)lower_bound_tile(S.tree.m30, S.n, t, B.tile_shift);
+        r.w = (int)lower_bound_tile(S.tree.m30, S.n, t + 1, B.tile_shift);
+    }
+    B.ranges[t] = r;
+}
+
+// Tiled deposit: one CTA per Morton-aligned tile of T^3 cells of one box.
+// The tile's particles are one contiguous range of each species' sorted
+// array (B.ranges); they are accumulated into a shared-memory copy of the
+// tile plus a halo (edge S = T + 3 holds every TSC stencil of a particle
+// inside the tile, including the interlaced grid's half-cell shift) with
+// shared-memory float atomics, then flushed with one global reduction per
+// non-zero cell.  Stencils that leave the halo (a particle outside its tile
+// after the drift) go straight to the grid.
+template <int ORDER, int NG>
+__global__ void __launch_bounds__(256)
+k_b_deposit(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ boxes,
+            const int64_t* __restrict__ tprefix, int nbox)
+{
+    extern __shared__ float tile[];
+    const int64_t q = blockIdx.x;
+    const int b = jt_find(tprefix, nbox, q);
+    const jt_box_dev& B = boxes[b];
+    const uint32_t t = (uint32_t)(q - tprefix[b]);
+    const int T = B.T, M = B.M;
+    const int S = T + 3;
+    const int S3 = S * S * S;
+    const int bx = (int)compact3(t) * T - 1;
+    const int by = (int)compact3(t >> 1) * T - 1;
+    const int bz = (int)compact3(t >> 2) * T - 1;
+    for (int c = threadIdx.x; c < NG * S3; c += blockDim.x) tile[c] = 0.0f;
+    __syncthreads();
+    const int4 r = B.ranges[t];
+    const int mask = M - 1;
+    const int64_t G = (int64_t)M * M * M;
+    const int n0 = r.y - r.x, n1 = r.w - r.z;
+    const float halfL = B.halfL, hinv = B.h_inv;
+    const float inv_vol = hinv * hinv * hinv;
+    const float q0 = B.mass[0] * inv_vol, q1 = -B.mass[1] * inv_vol;
+    const float4* pos0 = B.seg[0] >= 0 ? segs[B.seg[0]].pos : nullptr;
+    const float4* pos1 = B.seg[1] >= 0 ? segs[B.seg[1]].pos : nullptr;
+    float* rho = B.rho;
+    for (int k = threadIdx.x; k < n0 + n1; k += blockDim.x) {
+        float4 p;
+        float qq;
+        if (k < n0) { p = pos0[r.x + k]; qq = q0; } else { p = pos1[r.z + k - n0]; qq = q1; }
+        float gx = (p.x + halfL) * hinv, gy = (p.y + halfL) * hinv, gz = (p.z + halfL) * hinv;
+#pragma unroll
+        for (int g = 0; g < NG; g++) {
+            float sh = 0.5f * g;
+            float wx[ORDER], wy[ORDER], wz[ORDER];
+            int ix = jt_stencil<ORDER>(gx - sh, wx);
+            int iy = jt_stencil<ORDER>(gy - sh, wy);
+            int iz = jt_stencil<ORDER>(gz - sh, wz);
+            int lx = ix - bx, ly = iy - by, lz = iz - bz;
+            bool inside = lx >= 0 && ly >= 0 && lz >= 0 && lx + ORDER <= S && ly + ORDER <= S &&
+                          lz + ORDER <= S;
+            if (inside) {
+                float* tb_ = tile + g * S3;
+#pragma unroll
+                for (int c = 0; c < ORDER; c++)
+#pragma unroll
+                    for (int bb = 0; bb < ORDER; bb++) {
+                        float wyz = qq * wz[c] * wy[bb];
+                        float* row = tb_ + ((lz + c) * S + (ly + bb)) * S + lx;
+#pragma unroll
+                        for (int a = 0; a < ORDER; a++) atomicAdd(row + a, wyz * wx[a]);
+                    }
+            } else {
+                float* gb = rho + g * G;
+#pragma unroll
+                for (int c = 0; c < ORDER; c++)
+#pragma unroll
+                    for (int bb = 0; bb < ORDER; bb++) {
+                        float wyz = qq * wz[c] * wy[bb];
+                        int64_t row = ((int64_t)((iz + c) & mask) * M + ((iy + bb) & mask)) * M;
+#pragma unroll
+                        for (int a = 0; a < ORDER; a++) atomicAdd(gb + row + ((ix + a) & mask), wyz * wx[a]);
+                    }
+            }
+        }
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < NG * S3; c += blockDim.x) {
+        float v = tile[c];
+        if (v == 0.0f) continue;
+        int g = c / S3, rem = c - g * S3;
+        int lz = rem / (S * S), ly = (rem / S) % S, lx = rem % S;
+        int64_t idx = ((int64_t)((bz + lz) & mask) * M + ((by + ly) & mask)) * M + ((bx + lx) & mask);
+        atomicAdd(rho + g * G + idx, v);
+    }
+}
+
+// Fused k-space kernel, one thread per complex mode of one box.  Per-axis
+// tables (index n = 0..M-1):
+//   ta[n] = { k_n, gradient factor k_n (0 on the Nyquist plane),
+//             exp(-k_n^2 r_s^2) / sinc^(2 order)(pi n/M), |n| }
+//   tb[n] = { cos(k_n h/2), sin(k_n h/2), 0, 0 }   (interlacing phase)
+// With interlacing rho = (rhoA + rhoB exp(-i theta)) / 2, theta = (kx+ky+kz) h/2,
+// and the second set of force spectra is multiplied by exp(+i theta) so that
+// its C2R gives the forces at the shifted nodes.  a_d(k) = -i k_d phi(k).
+template <bool IL>
+__global__ void k_b_kspace(const jt_box_dev* __restrict__ boxes, const int64_t* __restrict__ kprefix,
+                           int nbox, int k_min)
+{
+    int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= kprefix[nbox]) return;
+    const int b = jt_find(kprefix, nbox, q);
+    const jt_box_dev& B = boxes[b];
+    const int64_t idx = q - kprefix[b];
+    const int M = B.M;
+    const int64_t Gc = (int64_t)M * M * (M / 2 + 1);
+    const float norm = 1.0f / ((float)M * (float)M * (float)M);
+    const float4* ta = B.tabs;
+    const float4* tb = B.tabs + M;
+    const float2* rho_k = B.rho_k;
+    float2* out = B.force_k;
+    const int Mh = M / 2 + 1;
+    const int kx = (int)(idx % Mh);
+    const int64_t r = idx / Mh;
+    const int ky = (int)(r % M);
+    const int kz = (int)(r / M);
+    const float4 ax = __ldg(&ta[kx]), ay = __ldg(&ta[ky]), az = __ldg(&ta[kz]);
+    const float k2 = ax.x * ax.x + ay.x * ay.x + az.x * az.x;
+    const int half = M / 2;
+    const int nx = (int)ax.w, ny = (int)ay.w, nz = (int)az.w;
+    const int kmax = max(max(nx, ny), nz);
+    const bool keep = k2 > 0.0f && kmax >= k_min && nx != half && ny != half && nz != half;
+    float2 F0 = make_float2(0.f, 0.f), F1 = F0, F2 = F0;
+    float er = 1.0f, ei = 0.0f;
+    if (keep) {
+        float2 z = rho_k[idx];
+        if (IL) {
+            float4 bx = __ldg(&tb[kx]), by = __ldg(&tb[ky]), bz = __ldg(&tb[kz]);
+            float pr = bx.x * by.x - bx.y * by.y, pi = bx.x * by.y + bx.y * by.x;
+            er = pr * bz.x - pi * bz.y;
+            ei = pr * bz.y + pi * bz.x;
+            float2 w = rho_k[Gc + idx];
+            z.x = 0.5f * (z.x + (w.x * er + w.y * ei));
+            z.y = 0.5f * (z.y + (w.y * er - w.x * ei));
+        }
+        float green = -12.566370614f * norm * (ax.z * ay.z * az.z) / k2;
+        float pr = z.x * green, pi = z.y * green;
+        F0 = make_float2(ax.y * pi, -ax.y * pr);
+        F1 = make_float2(ay.y * pi, -ay.y * pr);
+        F2 = make_float2(az.y * pi, -az.y * pr);
+    }
+    out[idx] = F0;
+    out[Gc + idx] = F1;
+    out[2 * Gc + idx] = F2;
+    if (IL) {
+        out[3 * Gc + idx] = make_float2(F0.x * er - F0.y * ei, F0.x * ei + F0.y * er);
+        out[4 * Gc + idx] = make_float2(F1.x * er - F1.y * ei, F1.x * ei + F1.y * er);
+        out[5 * Gc + idx] = make_float2(F2.x * er - F2.y * ei, F2.x * ei + F2.y * er);
+    }
+}
+
+}  // namespace
+
+void jt_b_tile_ranges(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_tprefix,
+                      int nbox, int64_t ntiles, cudaStream_t st)
+{
+    if (ntiles <= 0) return;
+    k_b_tile_ranges<<<(unsigned)((ntiles + 255) / 256), 256, 0, st>>>(d_segs, d_boxes, d_tprefix, nbox);
+}
+
+// all boxes of a batch share order, ngrid and the tile edge T
+int jt_b_deposit(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_tprefix,
+                 int nbox, int64_t ntiles, int order, int ngrid, int T, cudaStream_t st)
+{
+    if (ntiles <= 0) return JT_OK;
+    int S = T + 3;
+    size_t smem = sizeof(float) * (size_t)ngrid * S * S * S;
+#define JT_BDEP(O, NG)                                                                        \
+    do {                                                                                      \
+        static bool attr = false;                                                             \
+        if (!attr) {                                                                          \
+            cudaFuncSetAttribute(k_b_deposit<O, NG>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                 96 * 1024);                                                  \
+            attr = true;                                                                      \
+        }                                                                                     \
+        k_b_deposit<O, NG><<<(unsigned)ntiles, 256, smem, st>>>(d_segs, d_boxes, d_tprefix, nbox); \
+    } while (0)
+    if (order == 2 && ngrid == 1) JT_BDEP(2, 1);
+    else if (order == 2 && ngrid == 2) JT_BDEP(2, 2);
+    else if (order == 3 && ngrid == 1) JT_BDEP(3, 1);
+    else if (order == 3 && ngrid == 2) JT_BDEP(3, 2);
+    else return JT_EINVAL;
+#undef JT_BDEP
+    return cudaGetLastError() == cudaSuccess ? JT_OK : JT_ECUDA;
+}
+
+void jt_b_kspace(const jt_box_dev* d_boxes, const int64_t* d_kprefix, int nbox, int64_t nmodes,
+                 int interlace, int k_min, cudaStream_t st)
+{
+    if (nmodes <= 0) return;
+    unsigned g = (unsigned)((nmodes + 255) / 256);
+    if (interlace) k_b_kspace<true><<<g, 256, 0, st>>>(d_boxes, d_kprefix, nbox, k_min);
+    else k_b_kspace<false><<<g, 256, 0, st>>>(d_boxes, d_kprefix, nbox, k_min);
 }

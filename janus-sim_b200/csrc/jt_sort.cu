@@ -341,12 +341,6 @@ void jt_launch_morton(const float4* pos, const int* id, int64_t n, float box_hal
     k_morton<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(pos, id, n, box_half, key32, key64, vals);
 }
 
-int jt_radix_sort_u32(uint32_t* keys, uint32_t* vals, int64_t n, const int* shifts, int npass,
-                      jt_sort_ws* ws, unsigned* d_err, cudaStream_t st)
-{
-    return radix_sort<uint32_t>(keys, vals, n, shifts, npass, ws, d_err, st);
-}
-
 int jt_radix_sort_u64(uint64_t* keys, uint32_t* vals, int64_t n, const int* shifts, int npass,
                       jt_sort_ws* ws, unsigned* d_err, cudaStream_t st)
 {
@@ -368,3 +362,234 @@ void jt_launch_split_keys(const uint64_t* key64, int64_t n, uint32_t* m30, uint3
     if (n <= 0) return;
     k_split_keys<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(key64, n, m30, tie);
 }
+
+// ======================================================================
+// Batched (segmented) versions: one launch per stage for every segment
+// (box x species) of a batch.  A segment's keys are its tree.m30 array.
+// ======================================================================
+namespace {
+
+__global__ void k_b_morton(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ boxes,
+                           const int64_t* __restrict__ prefix, int nseg)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= prefix[nseg]) return;
+    const int g = jt_find(prefix, nseg, i);
+    const int64_t j = i - prefix[g];
+    const jt_seg_dev& S = segs[g];
+    const float box_half = boxes[S.box].box_half;
+    float4 p = S.pos[j];
+    float scale = 1024.0f / (2.0f * box_half);
+    float x = __fmul_rn(__fadd_rn(p.x, box_half), scale);
+    float y = __fmul_rn(__fadd_rn(p.y, box_half), scale);
+    float z = __fmul_rn(__fadd_rn(p.z, box_half), scale);
+    uint32_t ix = min(__float2uint_rz(x), 0x3FFu);
+    uint32_t iy = min(__float2uint_rz(y), 0x3FFu);
+    uint32_t iz = min(__float2uint_rz(z), 0x3FFu);
+    S.tree.m30[j] = spread10(ix) | (spread10(iy) << 1) | (spread10(iz) << 2);
+    S.vals[j] = (uint32_t)j;
+}
+
+// per-segment histograms of the 4 digit positions (blocks over sort tiles)
+__global__ void __launch_bounds__(256) k_b_hist(const jt_seg_dev* __restrict__ segs,
+                                                const int64_t* __restrict__ tprefix, int nseg)
+{
+    __shared__ uint32_t s[4][256];
+    const int64_t tile = blockIdx.x;
+    const int g = jt_find(tprefix, nseg, tile);
+    const jt_seg_dev& S = segs[g];
+    const int64_t lt = tile - tprefix[g];
+    for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) (&s[0][0])[i] = 0;
+    __syncthreads();
+    const int64_t b0 = lt * kSortTile, b1 = min((int64_t)S.n, b0 + kSortTile);
+    for (int64_t i = b0 + threadIdx.x; i < b1; i += blockDim.x) {
+        uint32_t k = S.tree.m30[i];
+#pragma unroll
+        for (int p = 0; p < 4; p++) atomicAdd(&s[p][(k >> (8 * p)) & 0xFFu], 1u);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < 4; p++) {
+        uint32_t c = s[p][threadIdx.x];
+        if (c) atomicAdd(&S.hist[p * 256 + threadIdx.x], c);
+    }
+}
+
+// exclusive scan of each (segment, pass) histogram: block = 4 * segment + pass
+__global__ void k_b_scan(const jt_seg_dev* __restrict__ segs)
+{
+    __shared__ uint32_t wsum[8];
+    uint32_t* h = segs[blockIdx.x >> 2].hist + (blockIdx.x & 3) * 256;
+    int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    uint32_t v = h[t], x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    uint32_t add = 0;
+    for (int i = 0; i < w; i++) add += wsum[i];
+    h[t] = x - v + add;
+}
+
+// One onesweep pass over every segment.  Tickets (atomic, global over the
+// batch) are handed out in segment-then-tile order, so a tile only waits for
+// tiles of its own segment that already hold lower tickets.  Even passes read
+// (m30, vals) and write (keys_alt, vals_alt); odd passes the reverse.
+__global__ void __launch_bounds__(kSortThreads)
+k_b_onesweep(const jt_seg_dev* __restrict__ segs, const int64_t* __restrict__ tprefix, int nseg,
+             int pass, uint32_t* __restrict__ ticket, unsigned* err)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SortSmem<uint32_t>& S = *reinterpret_cast<SortSmem<uint32_t>*>(smem_raw);
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    if (t == 0) S.tile = (int)atomicAdd(ticket, 1u);
+    for (int i = t; i < kSortWarps * 256; i += kSortThreads) (&S.whist[0][0])[i] = 0;
+    __syncthreads();
+    const int64_t gt = S.tile;
+    const int g = jt_find(tprefix, nseg, gt);
+    const jt_seg_dev& G = segs[g];
+    const int tile = (int)(gt - tprefix[g]);
+    const int64_t n = G.n;
+    const int shift = 8 * pass;
+    const uint32_t* kin = (pass & 1) ? G.keys_alt : G.tree.m30;
+    uint32_t* kout = (pass & 1) ? G.tree.m30 : G.keys_alt;
+    const uint32_t* vin = (pass & 1) ? G.vals_alt : G.vals;
+    uint32_t* vout = (pass & 1) ? G.vals : G.vals_alt;
+    const uint32_t* base = G.hist + pass * 256;
+    const int64_t ntiles = (n + kSortTile - 1) / kSortTile;
+    uint32_t* status = G.status + (int64_t)pass * ntiles * 256;
+    const int64_t seg0 = (int64_t)tile * kSortTile + warp * (32 * kSortItems);
+
+    uint32_t k[kSortItems], v[kSortItems], rank[kSortItems];
+#pragma unroll
+    for (int j = 0; j < kSortItems; j++) {
+        int64_t idx = seg0 + j * 32 + lane;
+        bool ok = idx < n;
+        k[j] = ok ? kin[idx] : 0u;
+        v[j] = ok ? vin[idx] : 0u;
+    }
+    const uint32_t lt_mask = (1u << lane) - 1u;
+#pragma unroll
+    for (int j = 0; j < kSortItems; j++) {
+        bool ok = (seg0 + j * 32 + lane) < n;
+        uint32_t d = (k[j] >> shift) & 0xFFu;
+        uint32_t peers = __match_any_sync(0xffffffffu, ok ? d : (0x100u + lane));
+        int leader = __ffs(peers) - 1;
+        uint32_t old = 0;
+        if (ok && lane == leader) {
+            old = S.whist[warp][d];
+            S.whist[warp][d] = old + __popc(peers);
+        }
+        old = __shfl_sync(0xffffffffu, old, leader);
+        rank[j] = old + __popc(peers & lt_mask);
+        __syncwarp();
+    }
+    __syncthreads();
+    uint32_t count = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; w++) {
+        uint32_t c = S.whist[w][t];
+        S.whist[w][t] = count;
+        count += c;
+    }
+    uint32_t* row = status + (int64_t)tile * 256;
+    st_relaxed(row + t, (tile == 0 ? kFlagInc : kFlagAgg) | count);
+    uint32_t x = count;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) S.wsum[warp] = x;
+    __syncthreads();
+    uint32_t add = 0;
+    for (int i = 0; i < warp; i++) add += S.wsum[i];
+    S.tile_start[t] = x - count + add;
+    uint32_t excl = 0;
+    if (tile > 0) {
+        int p = tile - 1;
+        int spins = 0;
+        for (;;) {
+            uint32_t wv = ld_relaxed(status + (int64_t)p * 256 + t);
+            uint32_t flag = wv & ~kValMask;
+            if (flag == 0u) {
+                if (++spins > kLookbackLimit) { atomicOr(err, JT_ERRBIT_LOOKBACK); break; }
+                if (spins > 64) __nanosleep(32);
+                continue;
+            }
+            excl += wv & kValMask;
+            if (flag == kFlagInc || p == 0) break;
+            --p;
+        }
+        st_relaxed(row + t, kFlagInc | (excl + count));
+    }
+    S.gofs[t] = base[t] + excl;
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kSortItems; j++) {
+        bool ok = (seg0 + j * 32 + lane) < n;
+        if (ok) {
+            uint32_t d = (k[j] >> shift) & 0xFFu;
+            uint32_t pos = S.tile_start[d] + S.whist[warp][d] + rank[j];
+            S.keys[pos] = k[j];
+            S.vals[pos] = v[j];
+        }
+    }
+    __syncthreads();
+    int64_t rem = n - (int64_t)tile * kSortTile;
+    int tile_n = rem < kSortTile ? (int)rem : kSortTile;
+    for (int e = t; e < tile_n; e += kSortThreads) {
+        uint32_t key = S.keys[e];
+        uint32_t d = (key >> shift) & 0xFFu;
+        uint32_t dst = S.gofs[d] + (uint32_t)e - S.tile_start[d];
+        kout[dst] = key;
+        vout[dst] = S.vals[e];
+    }
+}
+
+__global__ void k_b_reorder(const jt_seg_dev* __restrict__ segs, const int64_t* __restrict__ prefix,
+                            int nseg)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= prefix[nseg]) return;
+    const int g = jt_find(prefix, nseg, i);
+    const int64_t j = i - prefix[g];
+    const jt_seg_dev& S = segs[g];
+    uint32_t s = S.vals[j];
+    S.pos_b[j] = S.pos[s];
+    S.vel_b[j] = S.vel[s];
+    S.id_b[j] = S.id[s];
+}
+
+}  // namespace
+
+// Sort every segment's particles by 30-bit Morton key (4 onesweep passes) and
+// gather their state into the ping-pong buffers (the caller swaps them).
+// pprefix: particles per segment; tprefix: sort tiles per segment (host and
+// device copies); ws: per-pass ticket counters.
+int jt_b_sort_reorder(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, int nseg,
+                      const int64_t* d_pprefix, int64_t ntotal, const int64_t* d_tprefix,
+                      int64_t ntiles, uint32_t* d_tickets, unsigned* d_err, cudaStream_t st)
+{
+    if (ntotal <= 0) return JT_OK;
+    unsigned g = (unsigned)((ntotal + 255) / 256);
+    k_b_morton<<<g, 256, 0, st>>>(d_segs, d_boxes, d_pprefix, nseg);
+    k_b_hist<<<(unsigned)ntiles, 256, 0, st>>>(d_segs, d_tprefix, nseg);
+    k_b_scan<<<4 * nseg, 256, 0, st>>>(d_segs);
+    size_t smem = sizeof(SortSmem<uint32_t>);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_b_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    for (int p = 0; p < 4; p++)
+        k_b_onesweep<<<(unsigned)ntiles, kSortThreads, smem, st>>>(d_segs, d_tprefix, nseg, p,
+                                                                   d_tickets + p, d_err);
+    k_b_reorder<<<g, 256, 0, st>>>(d_segs, d_pprefix, nseg);
+    return cudaGetLastError() == cudaSuccess ? JT_OK : JT_ECUDA;
+}
+
+int jt_sort_tile_size() { return kSortTile; }

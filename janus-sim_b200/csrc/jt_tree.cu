@@ -176,16 +176,135 @@ void jt_launch_karras(jt_tree_dev t, cudaStream_t st)
                                                                    t.parent, t.range);
 }
 
-void jt_launch_moments(jt_tree_dev t, const float4* pos, float mass, float box_half, int rcompat,
-                       cudaStream_t st)
+// RCOMPAT node moments (the accurate path builds its moments in k_b_moments)
+void jt_launch_moments_rc(jt_tree_dev t, const float4* pos, float mass, float box_half, cudaStream_t st)
 {
     if (t.n <= 0) return;
     cudaMemsetAsync(t.flag, 0, sizeof(int) * (t.n > 1 ? t.n - 1 : 1), st);
     unsigned g = (unsigned)((t.n + 255) / 256);
-    if (rcompat)
-        k_moments<true><<<g, 256, 0, st>>>(t.n, pos, mass, box_half, t.child, t.parent, t.flag,
-                                           t.com, t.bmin, t.bmax, t.quad0, t.quad1);
-    else
-        k_moments<false><<<g, 256, 0, st>>>(t.n, pos, mass, box_half, t.child, t.parent, t.flag,
-                                            t.com, t.bmin, t.bmax, t.quad0, t.quad1);
+    k_moments<true><<<g, 256, 0, st>>>(t.n, pos, mass, box_half, t.child, t.parent, t.flag, t.com, t.bmin,
+                                       t.bmax, t.quad0, t.quad1);
+}
+
+// ======================================================================
+// Batched versions over segments (accurate mode: tie = sorted position).
+// ======================================================================
+namespace {
+
+// internal nodes of every segment; iprefix counts n-1 per segment.  Node 0's
+// parent is set to -1 and each internal node's arrival flag is cleared here,
+// so no separate reset pass is needed.
+__global__ void k_b_karras(const jt_seg_dev* __restrict__ segs, const int64_t* __restrict__ iprefix,
+                           int nseg)
+{
+    int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= iprefix[nseg]) return;
+    const int g = jt_find(iprefix, nseg, q);
+    const int64_t i = q - iprefix[g];
+    const jt_seg_dev& S = segs[g];
+    const jt_tree_dev& T = S.tree;
+    const int64_t n = S.n;
+    const uint32_t* m30 = T.m30;
+    int64_t first, last;
+    if (i == 0) {
+        first = 0;
+        last = n - 1;
+        T.parent[0] = -1;
+    } else {
+        int dl = tdelta(m30, nullptr, n, i, i - 1);
+        int dr = tdelta(m30, nullptr, n, i, i + 1);
+        int d = (dr > dl) ? 1 : -1;
+        int dmin = (d > 0) ? dl : dr;
+        int64_t lmax = 2;
+        while (tdelta(m30, nullptr, n, i, i + lmax * d) > dmin) lmax *= 2;
+        int64_t l = 0;
+        for (int64_t t = lmax / 2; t >= 1; t /= 2)
+            if (tdelta(m30, nullptr, n, i, i + (l + t) * d) > dmin) l += t;
+        int64_t j = i + l * d;
+        first = d > 0 ? i : j;
+        last = d > 0 ? j : i;
+    }
+    int64_t gamma = first;
+    if (first != last) {
+        int dn = tdelta(m30, nullptr, n, first, last);
+        int64_t s = 0, t = last - first;
+        while (t > 1) {
+            t = (t + 1) / 2;
+            if (tdelta(m30, nullptr, n, first, first + s + t) > dn) s += t;
+        }
+        gamma = first + s;
+    }
+    int64_t lc = (first == gamma) ? (n - 1 + first) : gamma;
+    int64_t rc = (gamma + 1 == last) ? (n - 1 + last) : (gamma + 1);
+    T.child[i] = make_int2((int)lc, (int)rc);
+    T.range[i] = make_int2((int)first, (int)last);
+    T.flag[i] = 0;
+    T.parent[lc] = (int)i;
+    T.parent[rc] = (int)i;
+}
+
+// leaves of every segment (particle masses from the box table)
+__global__ void k_b_moments(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ boxes,
+                            const int64_t* __restrict__ pprefix, int nseg)
+{
+    int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= pprefix[nseg]) return;
+    const int g = jt_find(pprefix, nseg, q);
+    const int64_t j = q - pprefix[g];
+    const jt_seg_dev& S = segs[g];
+    const jt_tree_dev& T = S.tree;
+    const int64_t n = S.n;
+    const float mass = boxes[S.box].mass[S.species];
+    int64_t node = n - 1 + j;
+    float4 p = S.pos[j];
+    T.com[node] = make_float4(p.x, p.y, p.z, mass);
+    T.bmin[node] = make_float4(p.x, p.y, p.z, 0.0f);
+    T.bmax[node] = make_float4(p.x, p.y, p.z, 0.0f);
+    T.quad0[node] = make_float4(0.f, 0.f, 0.f, 0.f);
+    T.quad1[node] = make_float2(0.f, 0.f);
+    int cur = n > 1 ? T.parent[node] : -1;
+    while (cur >= 0) {
+        __threadfence();
+        if (atomicAdd(&T.flag[cur], 1) == 0) return;
+        int2 ch = __ldcg(&T.child[cur]);
+        float4 cl = __ldcg(&T.com[ch.x]);
+        float4 cr = __ldcg(&T.com[ch.y]);
+        float ml = cl.w, mr = cr.w, m = ml + mr;
+        float inv = 1.0f / m;
+        float cx = (ml * cl.x + mr * cr.x) * inv;
+        float cy = (ml * cl.y + mr * cr.y) * inv;
+        float cz = (ml * cl.z + mr * cr.z) * inv;
+        float4 lo_l = __ldcg(&T.bmin[ch.x]), lo_r = __ldcg(&T.bmin[ch.y]);
+        float4 hi_l = __ldcg(&T.bmax[ch.x]), hi_r = __ldcg(&T.bmax[ch.y]);
+        float4 ql0 = __ldcg(&T.quad0[ch.x]), qr0 = __ldcg(&T.quad0[ch.y]);
+        float2 ql1 = __ldcg(&T.quad1[ch.x]), qr1 = __ldcg(&T.quad1[ch.y]);
+        float dlx = cl.x - cx, dly = cl.y - cy, dlz = cl.z - cz;
+        float drx = cr.x - cx, dry = cr.y - cy, drz = cr.z - cz;
+        float4 q0;
+        q0.x = ql0.x + qr0.x + ml * dlx * dlx + mr * drx * drx;
+        q0.y = ql0.y + qr0.y + ml * dly * dly + mr * dry * dry;
+        q0.z = ql0.z + qr0.z + ml * dlz * dlz + mr * drz * drz;
+        q0.w = ql0.w + qr0.w + ml * dlx * dly + mr * drx * dry;
+        float2 q1;
+        q1.x = ql1.x + qr1.x + ml * dlx * dlz + mr * drx * drz;
+        q1.y = ql1.y + qr1.y + ml * dly * dlz + mr * dry * drz;
+        T.com[cur] = make_float4(cx, cy, cz, m);
+        T.bmin[cur] = make_float4(fminf(lo_l.x, lo_r.x), fminf(lo_l.y, lo_r.y), fminf(lo_l.z, lo_r.z), 0.0f);
+        T.bmax[cur] = make_float4(fmaxf(hi_l.x, hi_r.x), fmaxf(hi_l.y, hi_r.y), fmaxf(hi_l.z, hi_r.z), 0.0f);
+        T.quad0[cur] = q0;
+        T.quad1[cur] = q1;
+        cur = T.parent[cur];
+    }
+}
+
+}  // namespace
+
+void jt_b_build_trees(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, int nseg,
+                      const int64_t* d_iprefix, int64_t ninternal, const int64_t* d_pprefix,
+                      int64_t nleaves, cudaStream_t st)
+{
+    if (ninternal > 0)
+        k_b_karras<<<(unsigned)((ninternal + 255) / 256), 256, 0, st>>>(d_segs, d_iprefix, nseg);
+    if (nleaves > 0)
+        k_b_moments<<<(unsigned)((nleaves + 255) / 256), 256, 0, st>>>(d_segs, d_boxes, d_pprefix, nseg);
 }

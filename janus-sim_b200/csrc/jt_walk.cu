@@ -46,7 +46,7 @@ constexpr int kApproxCap = 64;    // queued multipole nodes
 struct WalkWarpSmem {
     int stack[kStackCap];
     int2 rng[kRangeCap];          // (first sorted index, count)
-    float4 rsh[kRangeCap];        // periodic shift of the range (multiples of L)
+    char4 rsh[kRangeCap];         // periodic shift of the range, in box lengths (-1, 0, 1)
     float4 cand[kCandCap];        // shifted candidate positions
     float4 acom[kApproxCap];      // shifted COM + mass
     float4 aq0[kApproxCap];       // Qxx Qyy Qzz Qxy
@@ -56,6 +56,14 @@ struct WalkWarpSmem {
 struct Acc3 {
     float x, y, z;
 };
+
+// Phase counters of a diagnostic build (-DJT_WALK_COUNT): traversal
+// iterations, ranges streamed, chunks evaluated, pair-loop trip counts (the
+// warp's maximum over lanes).  Compiled out of the product build.
+struct WalkCount {
+    unsigned long long iters, ranges, chunks, trips;
+};
+
 
 __device__ __forceinline__ void kahan_add(float& s, float& c, float v)
 {
@@ -85,32 +93,30 @@ __device__ __forceinline__ float gap1(float d, float ext)
 }
 
 struct WalkArgs {
-    jt_walk_params p;
-    const float4* pos[2];
-    int64_t n[2];
-    jt_tree_dev tree[2];
-    const float* force3;
-    float4* acc[2];
-    float4* vel[2];
-    float kick_dt, kick_drag;
-    int64_t groups0, groups1;
+    const jt_seg_dev* segs;
+    const jt_box_dev* boxes;
+    const int64_t* gprefix;   // 32-particle groups per segment
+    int nseg;
+    int parts;                // JT_PART_* bits
+    float kick_frac;          // closing kick fused into the epilogue: this fraction
+                              // of each box's dt (0 = none)
     unsigned long long* stats;
     unsigned* err;
 };
 
-// Pair interactions of this lane's particle with a chunk of cnt candidates:
-// a distance mask first (8 flops per candidate), then the full split-force
-// kernel only for candidates inside r_cut.  WRAP applies the minimum image
-// per pair (groups wider than L/8; otherwise candidates were shifted to the
-// group's image when queued).
-template <bool WRAP>
-__device__ __forceinline__ int eval_chunk(const float4* __restrict__ cand, int cnt, float px, float py,
-                                          float pz, bool valid, const jt_walk_params& P, float fac,
-                                          Acc3& a)
+// Pair interactions of this lane's target with a chunk of candidates: a
+// distance mask first (8 flops per candidate, fully unrolled for a full chunk
+// of 32), then the split-force kernel only for candidates inside r_cut.
+// WRAP applies the minimum image per pair (groups wider than L/8; otherwise
+// candidates were shifted to the group's image when queued).
+template <bool WRAP, int CNT>
+__device__ __forceinline__ unsigned chunk_mask(const float4* __restrict__ cand, int cnt, float px,
+                                               float py, float pz, const jt_walk_params& P)
 {
     unsigned m = 0;
-#pragma unroll 8
-    for (int j = 0; j < cnt; j++) {
+#pragma unroll
+    for (int j = 0; j < (CNT > 0 ? CNT : 32); j++) {
+        if (CNT == 0 && j >= cnt) break;
         float4 q = cand[j];
         float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
         if (WRAP) {
@@ -119,27 +125,51 @@ __device__ __forceinline__ int eval_chunk(const float4* __restrict__ cand, int c
             dz = jt_wrap(dz, P.L, P.halfL);
         }
         float r2 = dx * dx + dy * dy + dz * dz;
-        m |= ((r2 < P.rc2) & (r2 > 0.0f) ? 1u : 0u) << j;
+        if (r2 < P.rc2) m |= 1u << j;
     }
+    return m;
+}
+
+template <bool WRAP>
+__device__ __forceinline__ int eval_chunk(WalkWarpSmem& S, int cnt, int lane, float px, float py,
+                                          float pz, bool valid, const jt_walk_params& P, float fac,
+                                          WalkCount& wc, Acc3& a)
+{
+    wc.chunks++;
+    (void)lane;
+    const float4* __restrict__ cand = S.cand;
+    unsigned m = cnt == 32 ? chunk_mask<WRAP, 32>(cand, 32, px, py, pz, P)
+                           : chunk_mask<WRAP, 0>(cand, cnt, px, py, pz, P);
     if (!valid) m = 0;
-    const int hits = __popc(m);
+#ifdef JT_WALK_COUNT
+    {
+        int t = __popc(m);
+        for (int o = 16; o > 0; o >>= 1) t = max(t, __shfl_xor_sync(0xffffffffu, t, o));
+        wc.trips += t;
+    }
+#endif
+    int hits = 0;
     while (m) {
         const int j = __ffs(m) - 1;
         m &= m - 1;
-        float4 q = cand[j];
+        const float4 q = cand[j];
         float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
         if (WRAP) {
             dx = jt_wrap(dx, P.L, P.halfL);
             dy = jt_wrap(dy, P.L, P.halfL);
             dz = jt_wrap(dz, P.L, P.halfL);
         }
-        float rp2 = dx * dx + dy * dy + dz * dz + P.eps2;
-        float ri = rsqrtf(rp2);
-        float x = rp2 * ri * P.c;
-        float g = fac * jt_split_S(x) * ri * ri * ri;
-        a.x += g * dx;
-        a.y += g * dy;
-        a.z += g * dz;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 > 0.0f) {   // not the target itself (or an exact duplicate)
+            hits++;
+            const float rp2 = r2 + P.eps2;
+            const float ri = rsqrtf(rp2);
+            const float x = rp2 * ri * P.c;
+            const float g = fac * jt_split_S(x) * ri * ri * ri;
+            a.x += g * dx;
+            a.y += g * dy;
+            a.z += g * dz;
+        }
     }
     return hits;
 }
@@ -196,14 +226,16 @@ __device__ __forceinline__ void drain_ranges(WalkWarpSmem& S, int nr, int& nc,
                                              const float4* __restrict__ tpos, int lane, float px,
                                              float py, float pz, bool valid, const jt_walk_params& P,
                                              float fac, Acc3& near, unsigned long long& pairs,
-                                             unsigned long long& cands)
+                                             unsigned long long& cands, WalkCount& wc)
 {
     if (nr <= 0) return;
+    wc.ranges += nr;
     int2 r0 = S.rng[0];
     float4 nxt = lane < r0.y ? tpos[r0.x + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
     for (int r = 0; r < nr; r++) {
         const int2 rr = S.rng[r];
-        const float4 sh = S.rsh[r];
+        const char4 sc = S.rsh[r];
+        const float4 sh = make_float4(sc.x * P.L, sc.y * P.L, sc.z * P.L, 0.f);
         const float4 cur = nxt;
         if (r + 1 < nr) {
             const int2 rn = S.rng[r + 1];
@@ -213,7 +245,7 @@ __device__ __forceinline__ void drain_ranges(WalkWarpSmem& S, int nr, int& nc,
         nc += rr.y;
         __syncwarp();
         if (nc >= 32) {
-            pairs += eval_chunk<WRAP>(S.cand, 32, px, py, pz, valid, P, fac, near);
+            pairs += eval_chunk<WRAP>(S, 32, lane, px, py, pz, valid, P, fac, wc, near);
             cands += 32;
             __syncwarp();
             float4 t = S.cand[32 + lane];
@@ -226,19 +258,23 @@ __device__ __forceinline__ void drain_ranges(WalkWarpSmem& S, int nr, int& nc,
 }
 
 template <int ORDER, int NG, bool WRAP>
-__device__ __forceinline__ void walk_trees(const WalkArgs& A, WalkWarpSmem& S, int s, int lane,
+__device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& B,
+                                           const jt_walk_params& P, WalkWarpSmem& S, int s, int lane,
                                            const float4& p, bool valid, float gcx, float gcy,
                                            float gcz, float ghx, float ghy, float ghz, Acc3& near,
                                            Acc3& far, Acc3& comp, unsigned long long& pairs,
-                                           unsigned long long& nodes, unsigned long long& cands)
+                                           unsigned long long& nodes, unsigned long long& cands,
+                                           WalkCount& wc)
 {
-    const jt_walk_params& P = A.p;
     const unsigned lt = (1u << lane) - 1u;
     for (int t = 0; t < 2; t++) {
-        const int64_t nt = A.n[t];
-        if (nt == 0 || !(P.parts & 2)) continue;
-        const jt_tree_dev T = A.tree[t];
-        const float4* __restrict__ tpos = A.pos[t];
+        const int tg = B.seg[t];
+        if (tg < 0 || !(P.parts & 2)) continue;
+        const jt_seg_dev& TS = A.segs[tg];
+        const int64_t nt = TS.n;
+        if (nt == 0) continue;
+        const jt_tree_dev T = TS.tree;
+        const float4* __restrict__ tpos = TS.pos;
         const float sgn = (s == t) ? 1.0f : -1.0f;
         const float fac_direct = sgn * P.mass[t];
         const int64_t leaf0 = nt - 1;
@@ -246,6 +282,7 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, WalkWarpSmem& S, i
         if (lane == 0) S.stack[0] = 0;
         __syncwarp();
         while (sp > 0) {
+            wc.iters++;
             const int k = sp < 32 ? sp : 32;
             int node = lane < k ? S.stack[sp - k + lane] : -1;
             sp -= k;
@@ -301,8 +338,9 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, WalkWarpSmem& S, i
                         if (count <= kBucket) {
                             act = 2;
                             rg = make_int2(first, count);
-                            // shift that moves the node to the group's periodic image
-                            pay = make_float4((gcx + dx) - cx, (gcy + dy) - cy, (gcz + dz) - cz, 0.f);
+                            // shift (in box lengths) that moves the node to the group's image
+                            pay = make_float4(rintf(((gcx + dx) - cx) / P.L), rintf(((gcy + dy) - cy) / P.L),
+                                              rintf(((gcz + dz) - cz) / P.L), 0.f);
                         } else {
                             act = 1;
                             ch = T.child[node];
@@ -324,7 +362,7 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, WalkWarpSmem& S, i
             } else if (act == 2) {
                 int at = nR + __popc(mrng & lt);
                 S.rng[at] = rg;
-                S.rsh[at] = pay;
+                S.rsh[at] = make_char4((signed char)pay.x, (signed char)pay.y, (signed char)pay.z, 0);
             } else if (act == 3) {
                 int at = nA + __popc(mapp & lt);
                 S.acom[at] = pay;
@@ -341,10 +379,10 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, WalkWarpSmem& S, i
             __syncwarp();
             if (nR >= 32) {
                 drain_ranges<WRAP>(S, 32, nc, tpos, lane, p.x, p.y, p.z, valid, P, fac_direct, near,
-                                   pairs, cands);
+                                   pairs, cands, wc);
                 __syncwarp();
                 int2 r2 = S.rng[32 + lane];
-                float4 s2 = S.rsh[32 + lane];
+                char4 s2 = S.rsh[32 + lane];
                 __syncwarp();
                 if (lane < nR - 32) { S.rng[lane] = r2; S.rsh[lane] = s2; }
                 nR -= 32;
@@ -366,10 +404,10 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, WalkWarpSmem& S, i
             }
         }
         drain_ranges<WRAP>(S, nR, nc, tpos, lane, p.x, p.y, p.z, valid, P, fac_direct, near, pairs,
-                           cands);
+                           cands, wc);
         __syncwarp();
         if (nc > 0) {
-            pairs += eval_chunk<WRAP>(S.cand, nc, p.x, p.y, p.z, valid, P, fac_direct, near);
+            pairs += eval_chunk<WRAP>(S, nc, lane, p.x, p.y, p.z, valid, P, fac_direct, wc, near);
             cands += nc;
         }
         if (nA > 0)
@@ -378,23 +416,31 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, WalkWarpSmem& S, i
     }
 }
 
+#ifndef JT_WALK_MINBLOCKS
+#define JT_WALK_MINBLOCKS 6
+#endif
+
 template <int ORDER, int NG>
-__global__ void __launch_bounds__(kWarps * 32) k_walk_acc(WalkArgs A)
+__global__ void __launch_bounds__(kWarps * 32, JT_WALK_MINBLOCKS) k_walk_acc(WalkArgs A)
 {
     __shared__ WalkWarpSmem smem_all[kWarps];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     WalkWarpSmem& S = smem_all[wib];
     const int64_t gw = (int64_t)blockIdx.x * kWarps + wib;
-    int s;
-    int64_t grp;
-    if (gw < A.groups0) { s = 0; grp = gw; }
-    else if (gw < A.groups0 + A.groups1) { s = 1; grp = gw - A.groups0; }
-    else return;  // whole warp
-    const jt_walk_params& P = A.p;
-    const int64_t ns = A.n[s];
+    if (gw >= A.gprefix[A.nseg]) return;  // whole warp
+    const int g = jt_find(A.gprefix, A.nseg, gw);
+    const int64_t grp = gw - A.gprefix[g];
+    const jt_seg_dev& SG = A.segs[g];
+    const jt_box_dev& B = A.boxes[SG.box];
+    const int s = SG.species;
+    jt_walk_params P;
+    P.L = B.L; P.halfL = B.halfL; P.theta2 = B.theta2; P.rc2 = B.rc2; P.rc = sqrtf(B.rc2);
+    P.eps2 = B.eps2; P.c = B.c; P.mass[0] = B.mass[0]; P.mass[1] = B.mass[1];
+    P.M = B.M; P.h_inv = B.h_inv; P.order = ORDER; P.ngrid = NG; P.parts = A.parts;
+    const int64_t ns = SG.n;
     const int64_t i = grp * 32 + lane;
     const bool valid = i < ns;
-    const float4 p = A.pos[s][valid ? i : grp * 32];
+    const float4 p = SG.pos[valid ? i : grp * 32];
     const float sgn_s = s == 0 ? 1.0f : -1.0f;
 
     // group AABB
@@ -418,7 +464,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk_acc(WalkArgs A)
             const int ix = jt_stencil<ORDER>(gx - sh, wx);
             const int iy = jt_stencil<ORDER>(gy - sh, wy);
             const int iz = jt_stencil<ORDER>(gz - sh, wz);
-            const float* __restrict__ F = A.force3 + (int64_t)b * 3 * G;
+            const float* __restrict__ F = B.force + (int64_t)b * 3 * G;
 #pragma unroll
             for (int c = 0; c < ORDER; c++)
 #pragma unroll
@@ -440,26 +486,28 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk_acc(WalkArgs A)
 
     Acc3 near = {0.f, 0.f, 0.f}, far = {0.f, 0.f, 0.f}, comp = {0.f, 0.f, 0.f};
     unsigned long long pairs = 0, nodes = 0, cands = 0;
+    WalkCount wc = {0, 0, 0, 0};
     // groups wider than L/8 take the minimum image per pair
     const bool wide = fmaxf(fmaxf(ghx, ghy), ghz) > 0.125f * P.L;
     if (wide)
-        walk_trees<ORDER, NG, true>(A, S, s, lane, p, valid, gcx, gcy, gcz, ghx, ghy, ghz, near, far,
-                                    comp, pairs, nodes, cands);
+        walk_trees<ORDER, NG, true>(A, B, P, S, s, lane, p, valid, gcx, gcy, gcz, ghx, ghy, ghz, near,
+                                    far, comp, pairs, nodes, cands, wc);
     else
-        walk_trees<ORDER, NG, false>(A, S, s, lane, p, valid, gcx, gcy, gcz, ghx, ghy, ghz, near, far,
-                                     comp, pairs, nodes, cands);
+        walk_trees<ORDER, NG, false>(A, B, P, S, s, lane, p, valid, gcx, gcy, gcz, ghx, ghy, ghz, near,
+                                     far, comp, pairs, nodes, cands, wc);
 
     if (valid) {
         float ax = sgn_s * pm.x + near.x + (far.x - comp.x);
         float ay = sgn_s * pm.y + near.y + (far.y - comp.y);
         float az = sgn_s * pm.z + near.z + (far.z - comp.z);
-        A.acc[s][i] = make_float4(ax, ay, az, 0.f);
-        if (A.kick_dt != 0.0f) {
-            float4 v = A.vel[s][i];
-            v.x += (ax - A.kick_drag * v.x) * A.kick_dt;
-            v.y += (ay - A.kick_drag * v.y) * A.kick_dt;
-            v.z += (az - A.kick_drag * v.z) * A.kick_dt;
-            A.vel[s][i] = v;
+        SG.acc[i] = make_float4(ax, ay, az, 0.f);
+        if (A.kick_frac != 0.0f) {
+            const float drag = B.kick_drag, kdt = A.kick_frac * B.dt;
+            float4 v = SG.vel[i];
+            v.x += (ax - drag * v.x) * kdt;
+            v.y += (ay - drag * v.y) * kdt;
+            v.z += (az - drag * v.z) * kdt;
+            SG.vel[i] = v;
         }
     }
     if (A.stats) {
@@ -472,6 +520,12 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk_acc(WalkArgs A)
             atomicAdd(A.stats, pairs);
             atomicAdd(A.stats + 1, nodes);
             atomicAdd(A.stats + 2, cands * 32ull);
+#ifdef JT_WALK_COUNT
+            atomicAdd(A.stats + 3, wc.iters);
+            atomicAdd(A.stats + 4, wc.ranges);
+            atomicAdd(A.stats + 5, wc.chunks);
+            atomicAdd(A.stats + 6, wc.trips);
+#endif
         }
     }
 }
@@ -706,34 +760,27 @@ __global__ void k_split_signed(const float* __restrict__ pos, const float* __res
 
 }  // namespace
 
-void jt_launch_walk_accurate(const jt_walk_params& p, const float4* const pos[2], const int64_t n[2],
-                             const jt_tree_dev tree[2], const float* force3, float4* const acc[2],
-                             float4* const vel[2], float kick_dt, float kick_drag,
-                             unsigned long long* stats, unsigned* d_err, cudaStream_t st)
+int jt_b_walk(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_gprefix, int nseg,
+              int64_t ngroups, int order, int ngrid, int parts, float kick_frac,
+              unsigned long long* stats, unsigned* d_err, cudaStream_t st)
 {
+    if (ngroups <= 0) return JT_OK;
     WalkArgs A;
-    A.p = p;
-    for (int s = 0; s < 2; s++) {
-        A.pos[s] = pos[s];
-        A.n[s] = n[s];
-        A.tree[s] = tree[s];
-        A.acc[s] = acc[s];
-        A.vel[s] = vel[s];
-    }
-    A.force3 = force3;
-    A.kick_dt = kick_dt;
-    A.kick_drag = kick_drag;
-    A.groups0 = (n[0] + 31) / 32;
-    A.groups1 = (n[1] + 31) / 32;
+    A.segs = d_segs;
+    A.boxes = d_boxes;
+    A.gprefix = d_gprefix;
+    A.nseg = nseg;
+    A.parts = parts;
+    A.kick_frac = kick_frac;
     A.stats = stats;
     A.err = d_err;
-    int64_t warps = A.groups0 + A.groups1;
-    if (warps == 0) return;
-    unsigned g = (unsigned)((warps + kWarps - 1) / kWarps);
-    if (p.order == 3 && p.ngrid == 2) k_walk_acc<3, 2><<<g, kWarps * 32, 0, st>>>(A);
-    else if (p.order == 3) k_walk_acc<3, 1><<<g, kWarps * 32, 0, st>>>(A);
-    else if (p.ngrid == 2) k_walk_acc<2, 2><<<g, kWarps * 32, 0, st>>>(A);
-    else k_walk_acc<2, 1><<<g, kWarps * 32, 0, st>>>(A);
+    unsigned g = (unsigned)((ngroups + kWarps - 1) / kWarps);
+    if (order == 3 && ngrid == 2) k_walk_acc<3, 2><<<g, kWarps * 32, 0, st>>>(A);
+    else if (order == 3 && ngrid == 1) k_walk_acc<3, 1><<<g, kWarps * 32, 0, st>>>(A);
+    else if (order == 2 && ngrid == 2) k_walk_acc<2, 2><<<g, kWarps * 32, 0, st>>>(A);
+    else if (order == 2 && ngrid == 1) k_walk_acc<2, 1><<<g, kWarps * 32, 0, st>>>(A);
+    else return JT_EINVAL;
+    return cudaGetLastError() == cudaSuccess ? JT_OK : JT_ECUDA;
 }
 
 void jt_launch_walk_rcompat(const jt_rc_params& p, const float4* pos_caller, const int8_t* sign_caller,
@@ -855,4 +902,63 @@ extern "C" int jt_fp32_peak(int iters, double* tflops)
     double flops = 2.0 * 8.0 * 16.0 * (double)iters * grid.x * block.x;
     *tflops = flops / (ms * 1e-3) / 1e12;
     return JT_OK;
+}
+
+// ------------------------------------------------------------------ batched step kernels
+namespace {
+
+// v += (a - drag_b v) dt over every segment's particles (drag per box)
+__global__ void k_b_kick(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ boxes,
+                         const int64_t* __restrict__ prefix, int nseg, float frac)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= prefix[nseg]) return;
+    const int g = jt_find(prefix, nseg, i);
+    const int64_t j = i - prefix[g];
+    const jt_seg_dev& S = segs[g];
+    const float drag = boxes[S.box].kick_drag, dt = frac * boxes[S.box].dt;
+    float4 v = S.vel[j], a = S.acc[j];
+    v.x += (a.x - drag * v.x) * dt;
+    v.y += (a.y - drag * v.y) * dt;
+    v.z += (a.z - drag * v.z) * dt;
+    S.vel[j] = v;
+}
+
+// x += v dt with one periodic wrap per axis (box side per box)
+__global__ void k_b_drift(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ boxes,
+                          const int64_t* __restrict__ prefix, int nseg, float frac)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= prefix[nseg]) return;
+    const int g = jt_find(prefix, nseg, i);
+    const int64_t j = i - prefix[g];
+    const jt_seg_dev& S = segs[g];
+    const float L = boxes[S.box].L, halfL = boxes[S.box].halfL, dt = frac * boxes[S.box].dt;
+    float4 p = S.pos[j], v = S.vel[j];
+    p.x += v.x * dt;
+    p.y += v.y * dt;
+    p.z += v.z * dt;
+    p.x = p.x > halfL ? p.x - L : p.x;
+    p.x = p.x < -halfL ? p.x + L : p.x;
+    p.y = p.y > halfL ? p.y - L : p.y;
+    p.y = p.y < -halfL ? p.y + L : p.y;
+    p.z = p.z > halfL ? p.z - L : p.z;
+    p.z = p.z < -halfL ? p.z + L : p.z;
+    S.pos[j] = p;
+}
+
+}  // namespace
+
+void jt_b_kick(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_prefix, int nseg,
+               int64_t ntotal, float frac, cudaStream_t st)
+{
+    if (ntotal <= 0) return;
+    k_b_kick<<<(unsigned)((ntotal + 255) / 256), 256, 0, st>>>(d_segs, d_boxes, d_prefix, nseg, frac);
+}
+
+void jt_b_drift(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_prefix, int nseg,
+                int64_t ntotal, float frac, cudaStream_t st)
+{
+    if (ntotal <= 0) return;
+    k_b_drift<<<(unsigned)((ntotal + 255) / 256), 256, 0, st>>>(d_segs, d_boxes, d_prefix, nseg, frac);
 }

@@ -38,6 +38,10 @@ EXPORTED = [
     "jt_create", "jt_set_state", "jt_set_state_signed", "jt_accel", "jt_accel_signed",
     "jt_step", "jt_get_state", "jt_get_state_signed", "jt_debug_tree", "jt_get_timings",
     "jt_counts", "jt_destroy", "jt_strerror", "jt_version", "jt_fp32_peak", "jt_accel_part",
+    "jt_walk_counters",
+    "jt_batch_create", "jt_batch_destroy", "jt_batch_add", "jt_batch_remove", "jt_batch_forces",
+    "jt_batch_step", "jt_batch_get_accel", "jt_batch_get_state", "jt_batch_box_info",
+    "jt_batch_memory", "jt_batch_estimate", "jt_batch_get_timings",
 ]
 
 
@@ -67,6 +71,10 @@ class jt_timings(C.Structure):
         ("pair_interactions", C.c_int64), ("node_interactions", C.c_int64),
         ("candidates", C.c_int64),
     ]
+
+
+class jt_step_args(C.Structure):
+    _fields_ = [("dt", C.c_double), ("hubble", C.c_double), ("dtau_per_dt", C.c_double)]
 
 
 _lib = None
@@ -99,10 +107,26 @@ def library():
     L.jt_strerror.argtypes = [C.c_int]
     L.jt_strerror.restype = C.c_char_p
     L.jt_fp32_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
+    L.jt_walk_counters.argtypes = [H, C.POINTER(C.c_int64)]
     L.jt_version.argtypes = []
     L.jt_version.restype = C.c_char_p
+    szp = C.POINTER(C.c_size_t)
+    L.jt_batch_create.argtypes = [C.POINTER(H)]
+    L.jt_batch_destroy.argtypes = [H]
+    L.jt_batch_destroy.restype = None
+    L.jt_batch_add.argtypes = [H, C.POINTER(jt_config), fp, fp, C.c_size_t, fp, fp, C.c_size_t, C.c_int,
+                               C.POINTER(C.c_int)]
+    L.jt_batch_remove.argtypes = [H, C.c_int]
+    L.jt_batch_forces.argtypes = [H, C.POINTER(C.c_int), C.c_int, C.c_int]
+    L.jt_batch_step.argtypes = [H, C.POINTER(C.c_int), C.c_int, C.POINTER(jt_step_args), C.c_int]
+    L.jt_batch_get_accel.argtypes = [H, C.c_int, fp, fp, C.c_int]
+    L.jt_batch_get_state.argtypes = [H, C.c_int, fp, fp, fp, fp, C.c_int]
+    L.jt_batch_box_info.argtypes = [H, C.c_int, szp, szp, szp]
+    L.jt_batch_memory.argtypes = [H, szp, szp]
+    L.jt_batch_estimate.argtypes = [C.POINTER(jt_config), C.c_size_t, C.c_size_t, szp, szp]
+    L.jt_batch_get_timings.argtypes = [H, C.POINTER(jt_timings)]
     for name in EXPORTED:
-        if name not in ("jt_destroy", "jt_strerror", "jt_version"):
+        if name not in ("jt_destroy", "jt_strerror", "jt_version", "jt_batch_destroy"):
             getattr(L, name).restype = C.c_int
     _lib = L
     return L
@@ -274,9 +298,113 @@ class Solver:
                                        _ptr(right), _ptr(parent)), "jt_debug_tree")
         return dict(morton=morton[:n], perm=perm[:n], left=left, right=right, parent=parent)
 
+    def walk_counters(self):
+        """(iterations, ranges, chunks, trips) of a -DJT_WALK_COUNT build."""
+        v = (C.c_int64 * 4)()
+        _check(library().jt_walk_counters(self._h, v), "jt_walk_counters")
+        return tuple(v)
+
     def timings(self):
         t = jt_timings()
         _check(library().jt_get_timings(self._h, C.byref(t)), "jt_get_timings")
+        return {k: getattr(t, k) for k, _ in jt_timings._fields_}
+
+
+class Batch:
+    """Many independent boxes stepped together (a jt_batch).
+
+    Every stage of a force pass is one kernel launch over the work of all the
+    boxes passed to ``forces``/``step`` (one batched cuFFT per grid size), in
+    place of the reference's one-process-per-box scans.  Boxes keep their own
+    Config (all accurate/KDK with the same pm_order, pm_interlace, k_min).
+    """
+
+    def __init__(self):
+        self._b = C.c_void_p()
+        _check(library().jt_batch_create(C.byref(self._b)), "jt_batch_create")
+        self.boxes = {}
+
+    def close(self):
+        if self._b:
+            library().jt_batch_destroy(self._b)
+            self._b = C.c_void_p()
+            self.boxes = {}
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def estimate(config: Config, n_p, n_m):
+        """(persistent, scratch) device bytes of one box; no device work."""
+        cfg = config.resolved().to_c()
+        a, b = C.c_size_t(), C.c_size_t()
+        _check(library().jt_batch_estimate(C.byref(cfg), n_p, n_m, C.byref(a), C.byref(b)),
+               "jt_batch_estimate")
+        return a.value, b.value
+
+    def add(self, config: Config, pos_p, vel_p, pos_m, vel_m):
+        """Add one box (host arrays); returns its id."""
+        pos_p = _f32(pos_p) if pos_p is not None else np.zeros((0, 3), np.float32)
+        pos_m = _f32(pos_m) if pos_m is not None else np.zeros((0, 3), np.float32)
+        vel_p = None if vel_p is None else _f32(vel_p)
+        vel_m = None if vel_m is None else _f32(vel_m)
+        cfg = config.resolved().to_c()
+        bid = C.c_int(-1)
+        _check(library().jt_batch_add(self._b, C.byref(cfg), _ptr(pos_p), _ptr(vel_p), len(pos_p),
+                                      _ptr(pos_m), _ptr(vel_m), len(pos_m), JT_MEM_HOST,
+                                      C.byref(bid)), "jt_batch_add")
+        self.boxes[bid.value] = (len(pos_p), len(pos_m))
+        return bid.value
+
+    def remove(self, box_id):
+        _check(library().jt_batch_remove(self._b, box_id), "jt_batch_remove")
+        self.boxes.pop(box_id, None)
+
+    @staticmethod
+    def _ids(ids):
+        arr = (C.c_int * len(ids))(*ids)
+        return arr, len(ids)
+
+    def forces(self, ids, part=JT_PART_ALL):
+        arr, n = self._ids(ids)
+        _check(library().jt_batch_forces(self._b, arr, n, part), "jt_batch_forces")
+
+    def step(self, ids, dt, hubble=0.0, dtau_per_dt=1.0, nsteps=1):
+        """nsteps KDK steps; dt/hubble/dtau_per_dt scalars or one per box."""
+        arr, n = self._ids(ids)
+        dts = np.broadcast_to(np.asarray(dt, np.float64), (n,))
+        hs = np.broadcast_to(np.asarray(hubble, np.float64), (n,))
+        ds = np.broadcast_to(np.asarray(dtau_per_dt, np.float64), (n,))
+        args = (jt_step_args * n)(*[jt_step_args(float(dts[k]), float(hs[k]), float(ds[k]))
+                                    for k in range(n)])
+        _check(library().jt_batch_step(self._b, arr, n, args, nsteps), "jt_batch_step")
+
+    def accel(self, box_id):
+        n_p, n_m = self.boxes[box_id]
+        ap = np.zeros((n_p, 3), np.float32)
+        am = np.zeros((n_m, 3), np.float32)
+        _check(library().jt_batch_get_accel(self._b, box_id, _ptr(ap), _ptr(am), JT_MEM_HOST),
+               "jt_batch_get_accel")
+        return ap, am
+
+    def get_state(self, box_id):
+        n_p, n_m = self.boxes[box_id]
+        out = [np.zeros((n, 3), np.float32) for n in (n_p, n_p, n_m, n_m)]
+        _check(library().jt_batch_get_state(self._b, box_id, *[_ptr(a) for a in out], JT_MEM_HOST),
+               "jt_batch_get_state")
+        return tuple(out)
+
+    def memory(self):
+        a, b = C.c_size_t(), C.c_size_t()
+        _check(library().jt_batch_memory(self._b, C.byref(a), C.byref(b)), "jt_batch_memory")
+        return a.value, b.value
+
+    def timings(self):
+        t = jt_timings()
+        _check(library().jt_batch_get_timings(self._b, C.byref(t)), "jt_batch_get_timings")
         return {k: getattr(t, k) for k, _ in jt_timings._fields_}
 
 

@@ -1,0 +1,164 @@
+"""Batched ensembles on the GPU: each box's result is the same alone and in
+the mix.
+
+A jt_batch runs every stage as one launch over the work of all its boxes
+(uneven particle counts, box sizes, grids, mu, steps).  A box stepped alone
+through a single handle and the same box stepped inside a batch of uneven
+boxes run the same kernels on the same inputs; the only differences come from
+the order of floating-point atomics in the deposit (PM force, ~1e-7
+relative).  Tolerances: forces max |a_batch - a_alone| <= 2e-5 x
+rms|a_alone|; after 3 KDK steps positions and velocities within 1e-6 x L and
+1e-4 x rms|v| (a particle whose Morton key flips on a last-bit position
+difference sees a different tree, which stays far inside these bounds over
+three steps).
+"""
+import numpy as np
+import pytest
+
+import janus_treepm as J
+
+pytestmark = pytest.mark.gpu
+
+FORCE_TOL = 2e-5
+POS_TOL_L = 1e-6
+VEL_TOL = 1e-4
+
+
+def make_box(seed, n_side_p, n_side_m, L, M, mu, theta=0.5):
+    rng = np.random.default_rng(seed)
+    n_p, n_m = n_side_p ** 3, n_side_m ** 3
+    pp = rng.uniform(-L / 2, L / 2, (n_p, 3)).astype(np.float32)
+    pm = rng.uniform(-L / 2, L / 2, (n_m, 3)).astype(np.float32)
+    vp = rng.normal(0, 0.5, (n_p, 3)).astype(np.float32)
+    vm = rng.normal(0, 0.5, (n_m, 3)).astype(np.float32)
+    spacing = L / max(n_p + n_m, 1) ** (1 / 3)
+    cfg = J.Config(box_L=L, pm_grid=M, theta=theta, softening=spacing / 30, mu=mu,
+                   G_mass_plus=1e-3 * (L / 64.0) ** 3)
+    return cfg, pp, vp, pm, vm
+
+
+BOXES = [
+    # seed, n+ side, n- side, L, M, mu
+    (1, 16, 16, 64.0, 32, 19.0),
+    (2, 20, 12, 120.0, 64, 5.0),
+    (3, 9, 24, 50.0, 64, 30.0),
+    (4, 24, 24, 300.0, 64, 11.0),
+    (5, 12, 0, 80.0, 32, 19.0),       # no m- particles
+    (6, 1, 2, 40.0, 32, 3.0),         # tiny box: 1 m+, 8 m-
+    (7, 30, 30, 200.0, 128, 7.0),
+]
+
+
+def _alone_forces(box):
+    cfg, pp, vp, pm, vm = make_box(*box)
+    s = J.Solver(cfg)
+    s.set_state(pp, vp, pm, vm)
+    ap, am = s.accel()
+    s.close()
+    return ap, am
+
+
+def _cmp(a, b, tol):
+    if len(a) == 0:
+        return
+    rms = float(np.sqrt(np.mean(np.sum(b.astype(np.float64) ** 2, axis=1))))
+    err = float(np.max(np.abs(a.astype(np.float64) - b)))
+    assert err <= tol * rms, (err, rms)
+
+
+def test_forces_same_alone_and_in_the_mix():
+    B = J.Batch()
+    ids = []
+    for box in BOXES:
+        cfg, pp, vp, pm, vm = make_box(*box)
+        ids.append(B.add(cfg, pp, vp, pm, vm))
+    B.forces(ids)
+    t = B.timings()
+    assert t["launches"] == 14          # one launch per stage for all seven boxes
+    assert t["pair_interactions"] > 0
+    for bid, box in zip(ids, BOXES):
+        ap, am = B.accel(bid)
+        rp, rm = _alone_forces(box)
+        assert np.all(np.isfinite(ap)) and np.all(np.isfinite(am))
+        _cmp(ap, rp, FORCE_TOL)
+        _cmp(am, rm, FORCE_TOL)
+    B.close()
+
+
+def test_subset_forces_match_full_batch():
+    B = J.Batch()
+    ids = [B.add(*make_box(*box)) for box in BOXES]
+    B.forces(ids)
+    full = {i: B.accel(i) for i in ids}
+    sub = ids[1::2]
+    B.forces(sub)
+    for i in sub:
+        ap, am = B.accel(i)
+        _cmp(ap, full[i][0], FORCE_TOL)
+        _cmp(am, full[i][1], FORCE_TOL)
+    B.close()
+
+
+def test_steps_same_alone_and_in_the_mix():
+    dts = [0.01, 0.02, 0.005, 0.01, 0.015, 0.01, 0.02]
+    hub = [0.0, 0.1, 0.05, 0.2, 0.0, 0.0, 0.07]
+    B = J.Batch()
+    ids = []
+    for box in BOXES:
+        cfg, pp, vp, pm, vm = make_box(*box)
+        ids.append(B.add(cfg, pp, vp, pm, vm))
+    B.step(ids, dts, hub, 1.0, nsteps=3)
+    for k, (bid, box) in enumerate(zip(ids, BOXES)):
+        cfg, pp, vp, pm, vm = make_box(*box)
+        s = J.Solver(cfg)
+        s.set_state(pp, vp, pm, vm)
+        s.step(dts[k], hub[k], 1.0, 3)
+        ref = s.get_state()
+        s.close()
+        got = B.get_state(bid)
+        for q, (g, r) in enumerate(zip(got, ref)):
+            if len(r) == 0:
+                continue
+            d = np.abs(g.astype(np.float64) - r)
+            if q % 2 == 0:                                # positions (periodic)
+                d = np.minimum(d, cfg.box_L - d)
+                assert float(d.max()) <= POS_TOL_L * cfg.box_L, (k, q, float(d.max()))
+            else:
+                rms = float(np.sqrt(np.mean(np.sum(r.astype(np.float64) ** 2, axis=1))))
+                assert float(d.max()) <= VEL_TOL * rms, (k, q, float(d.max()), rms)
+    B.close()
+
+
+def test_remove_and_reuse_slot():
+    B = J.Batch()
+    a = B.add(*make_box(*BOXES[0]))
+    b = B.add(*make_box(*BOXES[1]))
+    B.forces([a, b])
+    ref_b = B.accel(b)
+    B.remove(a)
+    c = B.add(*make_box(*BOXES[3]))
+    assert c == a                      # freed id reused
+    B.forces([b, c])
+    got_b = B.accel(b)
+    _cmp(got_b[0], ref_b[0], FORCE_TOL)
+    _cmp(got_b[1], ref_b[1], FORCE_TOL)
+    pers, scratch = B.memory()
+    est = sum(sum(J.Batch.estimate(make_box(*BOXES[i])[0], BOXES[i][1] ** 3, BOXES[i][2] ** 3))
+              for i in (1, 3))
+    assert pers > 0 and scratch > 0 and est > 0
+    B.close()
+
+
+def test_batch_rejects_mismatched_shared_fields():
+    B = J.Batch()
+    B.add(*make_box(*BOXES[0]))
+    cfg, pp, vp, pm, vm = make_box(*BOXES[1])
+    cfg.pm_interlace = 2               # the batch's boxes are interlaced
+    with pytest.raises(J.JanusError) as e:
+        B.add(cfg, pp, vp, pm, vm)
+    assert e.value.code == J.JT_EINVAL
+    with pytest.raises(J.JanusError):
+        B.forces([0, 0])               # duplicate id
+    with pytest.raises(J.JanusError):
+        B.forces([5])                  # unknown id
+    B.close()
