@@ -226,6 +226,32 @@ int  jt_batch_estimate(const jt_config* cfg, size_t n_p, size_t n_m,
                        size_t* persistent, size_t* scratch);
 int  jt_batch_get_timings(jt_batch* b, jt_timings* t);
 
+/* ---- allocation-free Morton sort ----
+ * The reference's Morton keys of n positions already on the device (float3
+ * array, box [-L/2, L/2)), sorted by the key (morton30 << 32) | index: writes
+ * morton_out[n] (sorted 30-bit codes) and perm_out[n] (index of each sorted
+ * position) to device memory -- the morton/perm outputs of jt_debug_tree.
+ * Every byte of scratch of its onesweep radix sort lives in one fixed
+ * file-scope static device array of JT_STATIC_SORT_BYTES (6.5 MiB); the call
+ * allocates nothing (no cudaMalloc, cudaFree or allocating library call).
+ * n must be 1..JT_STATIC_SORT_MAX, else JT_EINVAL.  stream: a cudaStream_t,
+ * or NULL for the legacy default stream; the call synchronises that stream
+ * before it returns (it reads the sort's error word: JT_ETIMEDOUT if a
+ * bounded device wait gave up).
+ * For callers that cannot allocate: code running inside a fixed HBM budget
+ * (a served job's admission control counts every device byte it holds) and
+ * code that must not synchronise the whole device (cudaMalloc and cudaFree
+ * do, stalling every other stream on it).
+ * The static array keeps the last call's contents; calls that overlap in
+ * time (several threads or streams) race on it and must be serialised by the
+ * caller; make the first call on each device before any stream capture,
+ * since that call looks up the array's address (cudaGetSymbolAddress, once
+ * per device).  No counterpart in the reference. */
+#define JT_STATIC_SORT_MAX    262144
+#define JT_STATIC_SORT_BYTES  6824448
+int  jt_morton_sort_static(const float* pos, size_t n, double box_L,
+                           uint32_t* morton_out, int32_t* perm_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

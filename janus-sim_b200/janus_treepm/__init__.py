@@ -41,8 +41,9 @@ EXPORTED = [
     "jt_walk_counters",
     "jt_batch_create", "jt_batch_destroy", "jt_batch_add", "jt_batch_remove", "jt_batch_forces",
     "jt_batch_step", "jt_batch_get_accel", "jt_batch_get_state", "jt_batch_box_info",
-    "jt_batch_memory", "jt_batch_estimate", "jt_batch_get_timings",
+    "jt_batch_memory", "jt_batch_estimate", "jt_batch_get_timings", "jt_morton_sort_static",
 ]
+JT_STATIC_SORT_MAX = 262144
 
 
 class JanusError(RuntimeError):
@@ -125,6 +126,7 @@ def library():
     L.jt_batch_memory.argtypes = [H, szp, szp]
     L.jt_batch_estimate.argtypes = [C.POINTER(jt_config), C.c_size_t, C.c_size_t, szp, szp]
     L.jt_batch_get_timings.argtypes = [H, C.POINTER(jt_timings)]
+    L.jt_morton_sort_static.argtypes = [vp, C.c_size_t, C.c_double, vp, vp, vp]
     for name in EXPORTED:
         if name not in ("jt_destroy", "jt_strerror", "jt_version", "jt_batch_destroy"):
             getattr(L, name).restype = C.c_int
@@ -308,6 +310,13 @@ class Solver:
         t = jt_timings()
         _check(library().jt_get_timings(self._h, C.byref(t)), "jt_get_timings")
         return {k: getattr(t, k) for k, _ in jt_timings._fields_}
+
+
+def morton_sort_static(pos_ptr, n, box_L, morton_ptr, perm_ptr, stream=None):
+    """jt_morton_sort_static on device pointers (ints or None): sorted Morton
+    codes and permutation with no device allocation (n <= JT_STATIC_SORT_MAX)."""
+    _check(library().jt_morton_sort_static(pos_ptr, n, box_L, morton_ptr, perm_ptr, stream),
+           "jt_morton_sort_static")
 
 
 class Batch:
