@@ -457,8 +457,19 @@ int force_pass(jt_batch* B, Plan& P, int parts, float kick_frac)
         JT_FFT(cufftExecC2R(K.plans[(int)kv.second.size()].second, (cufftComplex*)K.force_k, K.force));
     }
     cudaEventRecord(B->ev[6], st);
-    JT_TRY(jt_b_walk(P.d_post, P.d_bx, P.d_gp, nseg, P.ngroups, B->order, B->ngrid, parts, kick_frac,
-                     B->d_stats, B->d_err, st));
+    jt_tree_dev pool = {};
+    pool.child = B->child.p;
+    pool.range = B->range.p;
+    pool.parent = B->parent.p;
+    pool.flag = B->flag.p;
+    pool.com = B->com.p;
+    pool.bmin = B->bmin.p;
+    pool.bmax = B->bmax.p;
+    pool.quad0 = B->quad0.p;
+    pool.quad1 = B->quad1.p;
+    pool.m30 = B->m30.p;
+    JT_TRY(jt_b_walk(P.d_post, P.d_bx, P.d_gp, nseg, P.ngroups, pool, B->order, B->ngrid, parts,
+                     kick_frac, B->d_stats, B->d_err, st));
     cudaEventRecord(B->ev[7], st);
     B->pending = true;
     B->tm.launches += (P.npart > 0 ? 8 : 0) + (P.ninternal > 0 ? 1 : 0) + (P.npart > 0 ? 1 : 0) +

@@ -257,10 +257,12 @@ struct jt_walk_params {
     int parts;          // JT_PART_* bits: 1 = PM, 2 = tree
 };
 // Batched accurate walk over every segment's 32-particle groups (gprefix);
+// every segment's tree arrays lie inside the arrays of `pool` (node arrays at
+// a per-segment node offset, range at its particle offset, both < 2^31);
 // stats[0] pair interactions inside r_cut, [1] node (multipole) interactions,
 // [2] candidate particles distance-tested
 int jt_b_walk(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_gprefix, int nseg,
-              int64_t ngroups, int order, int ngrid, int parts, float kick_frac,
+              int64_t ngroups, const jt_tree_dev& pool, int order, int ngrid, int parts, float kick_frac,
               unsigned long long* stats, unsigned* d_err, cudaStream_t st);
 
 // kick v += (a - drag v) frac*dt and drift x += v frac*dt with each box's own

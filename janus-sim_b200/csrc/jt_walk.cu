@@ -98,6 +98,8 @@ struct WalkArgs {
     const int64_t* gprefix;   // 32-particle groups per segment
     int nseg;
     int parts;                // JT_PART_* bits
+    jt_tree_dev pool;         // base of every tree array: a segment's tree is
+                              // pool + its node offset (range: + particle offset)
     float kick_frac;          // closing kick fused into the epilogue: this fraction
                               // of each box's dt (0 = none)
     unsigned long long* stats;
@@ -225,8 +227,8 @@ template <bool WRAP>
 __device__ __forceinline__ void drain_ranges(WalkWarpSmem& S, int nr, int& nc,
                                              const float4* __restrict__ tpos, int lane, float px,
                                              float py, float pz, bool valid, const jt_walk_params& P,
-                                             float fac, Acc3& near, unsigned long long& pairs,
-                                             unsigned long long& cands, WalkCount& wc)
+                                             float fac, Acc3& near, unsigned& pairs,
+                                             unsigned& cands, WalkCount& wc)
 {
     if (nr <= 0) return;
     wc.ranges += nr;
@@ -262,8 +264,8 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& 
                                            const jt_walk_params& P, WalkWarpSmem& S, int s, int lane,
                                            const float4& p, bool valid, float gcx, float gcy,
                                            float gcz, float ghx, float ghy, float ghz, Acc3& near,
-                                           Acc3& far, Acc3& comp, unsigned long long& pairs,
-                                           unsigned long long& nodes, unsigned long long& cands,
+                                           Acc3& far, Acc3& comp, unsigned& pairs,
+                                           unsigned& nodes, unsigned& cands,
                                            WalkCount& wc)
 {
     const unsigned lt = (1u << lane) - 1u;
@@ -271,13 +273,16 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& 
         const int tg = B.seg[t];
         if (tg < 0 || !(P.parts & 2)) continue;
         const jt_seg_dev& TS = A.segs[tg];
-        const int64_t nt = TS.n;
+        const int nt = (int)TS.n;   // < 2^30 per species
         if (nt == 0) continue;
-        const jt_tree_dev T = TS.tree;
+        // node arrays through the pool bases (kernel parameters, no
+        // registers) plus two 32-bit offsets
+        const int noff = (int)(TS.tree.com - A.pool.com);
+        const int roff = (int)(TS.tree.range - A.pool.range);
         const float4* __restrict__ tpos = TS.pos;
         const float sgn = (s == t) ? 1.0f : -1.0f;
-        const float fac_direct = sgn * P.mass[t];
-        const int64_t leaf0 = nt - 1;
+        const float fac_direct = sgn * (t == 0 ? P.mass[0] : P.mass[1]);   // no dynamic index into a local array
+        const int leaf0 = nt - 1;
         int sp = 1, nR = 0, nA = 0, nc = 0;
         if (lane == 0) S.stack[0] = 0;
         __syncwarp();
@@ -304,10 +309,10 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& 
                     float4 q = tpos[first];
                     lox = hix = q.x; loy = hiy = q.y; loz = hiz = q.z;
                 } else {
-                    int2 r = T.range[node];
+                    int2 r = A.pool.range[roff + node];
                     first = r.x;
                     count = r.y - r.x + 1;
-                    float4 lo = T.bmin[node], hi = T.bmax[node];
+                    float4 lo = A.pool.bmin[noff + node], hi = A.pool.bmax[noff + node];
                     lox = lo.x; loy = lo.y; loz = lo.z; hix = hi.x; hiy = hi.y; hiz = hi.z;
                 }
                 float nhx = 0.5f * (hix - lox), nhy = 0.5f * (hiy - loy), nhz = 0.5f * (hiz - loz);
@@ -319,7 +324,7 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& 
                 if (gx * gx + gy * gy + gz * gz <= P.rc2) {
                     bool accepted = false;
                     if (count > 1) {
-                        float4 cm = T.com[node];
+                        float4 cm = A.pool.com[noff + node];
                         float mx = jt_wrap(cm.x - gcx, P.L, P.halfL);
                         float my = jt_wrap(cm.y - gcy, P.L, P.halfL);
                         float mz = jt_wrap(cm.z - gcz, P.L, P.halfL);
@@ -330,8 +335,8 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& 
                             accepted = true;
                             act = 3;
                             pay = make_float4(gcx + mx, gcy + my, gcz + mz, cm.w);
-                            pq0 = T.quad0[node];
-                            pq1 = T.quad1[node];
+                            pq0 = A.pool.quad0[noff + node];
+                            pq1 = A.pool.quad1[noff + node];
                         }
                     }
                     if (!accepted) {
@@ -343,7 +348,7 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& 
                                               rintf(((gcz + dz) - cz) / P.L), 0.f);
                         } else {
                             act = 1;
-                            ch = T.child[node];
+                            ch = A.pool.child[noff + node];
                         }
                     }
                 }
@@ -485,7 +490,7 @@ __global__ void __launch_bounds__(kWarps * 32, JT_WALK_MINBLOCKS) k_walk_acc(Wal
     }
 
     Acc3 near = {0.f, 0.f, 0.f}, far = {0.f, 0.f, 0.f}, comp = {0.f, 0.f, 0.f};
-    unsigned long long pairs = 0, nodes = 0, cands = 0;
+    unsigned pairs = 0, nodes = 0, cands = 0;   // per lane (warp totals < 2^32)
     WalkCount wc = {0, 0, 0, 0};
     // groups wider than L/8 take the minimum image per pair
     const bool wide = fmaxf(fmaxf(ghx, ghy), ghz) > 0.125f * P.L;
@@ -517,9 +522,9 @@ __global__ void __launch_bounds__(kWarps * 32, JT_WALK_MINBLOCKS) k_walk_acc(Wal
             nodes += __shfl_xor_sync(0xffffffffu, nodes, o);
         }
         if (lane == 0) {
-            atomicAdd(A.stats, pairs);
-            atomicAdd(A.stats + 1, nodes);
-            atomicAdd(A.stats + 2, cands * 32ull);
+            atomicAdd(A.stats, (unsigned long long)pairs);
+            atomicAdd(A.stats + 1, (unsigned long long)nodes);
+            atomicAdd(A.stats + 2, (unsigned long long)cands * 32ull);
 #ifdef JT_WALK_COUNT
             atomicAdd(A.stats + 3, wc.iters);
             atomicAdd(A.stats + 4, wc.ranges);
@@ -761,8 +766,8 @@ __global__ void k_split_signed(const float* __restrict__ pos, const float* __res
 }  // namespace
 
 int jt_b_walk(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_gprefix, int nseg,
-              int64_t ngroups, int order, int ngrid, int parts, float kick_frac,
-              unsigned long long* stats, unsigned* d_err, cudaStream_t st)
+              int64_t ngroups, const jt_tree_dev& pool, int order, int ngrid, int parts,
+              float kick_frac, unsigned long long* stats, unsigned* d_err, cudaStream_t st)
 {
     if (ngroups <= 0) return JT_OK;
     WalkArgs A;
@@ -772,6 +777,7 @@ int jt_b_walk(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t
     A.nseg = nseg;
     A.parts = parts;
     A.kick_frac = kick_frac;
+    A.pool = pool;
     A.stats = stats;
     A.err = d_err;
     unsigned g = (unsigned)((ngroups + kWarps - 1) / kWarps);
