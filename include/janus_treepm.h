@@ -44,9 +44,10 @@ extern "C" {
 #define JT_MEM_DEVICE  1
 
 /* ---- force modes ---- */
-/* ACCURATE: signed-source PM with CIC deconvolution and spectral gradient,
- * short-range factor erfc(x) + 2x/sqrt(pi) exp(-x^2), x = r / (2 r_s), Plummer
- * softening, monopole + quadrupole nodes, hard cut at r_cut. */
+/* ACCURATE: signed-source PM (TSC assignment with interlacing by default,
+ * deconvolved, Gaussian long-range filter, spectral gradient), short-range
+ * factor erfc(x) + 2x/sqrt(pi) exp(-x^2), x = r / (2 r_s), Plummer softening,
+ * monopole + quadrupole nodes, hard cut at r_cut. */
 #define JT_ACCURATE    0
 /* RCOMPAT: the reference GPU formulas (src/nbody_gpu_twopass.rs:98-257,
  * 1670-1811; cuda/cufft_wrapper.cu:148-208): finite-difference gradient of the
@@ -225,6 +226,68 @@ int  jt_batch_memory(jt_batch* b, size_t* persistent, size_t* scratch);
 int  jt_batch_estimate(const jt_config* cfg, size_t n_p, size_t n_m,
                        size_t* persistent, size_t* scratch);
 int  jt_batch_get_timings(jt_batch* b, jt_timings* t);
+
+/* on != 0: jt_batch_step replays each step as a CUDA graph, captured once
+ * per set of boxes (two graphs: the reorder's ping-pong buffers alternate)
+ * and recaptured when a box joins or leaves or a scratch pool grows.  The
+ * graphs keep the two half kicks of consecutive steps separate (kick dt/2,
+ * drift, forces + kick dt/2).  Stage timings are not collected inside
+ * graphs (total_ms is). */
+int  jt_batch_set_graphs(jt_batch* b, int on);
+/* Release the batch's per-pass scratch pools and cuFFT plans (they grow
+ * back on the next pass); persistent box state is kept. */
+int  jt_batch_trim(jt_batch* b);
+
+/* ---- serving loop ----
+ * Simulation jobs (one box each) admitted onto the device by an HBM budget,
+ * their step requests served by continuous batching: every batched step
+ * advances each resident job with a pending request by one KDK step in one
+ * launch per stage; requests arriving meanwhile join the next step.  A job
+ * that has taken all its steps is evicted to pinned host memory; idle
+ * resident jobs are swapped out to make room for waiting ones.  No
+ * counterpart in the reference (it runs one process per box). */
+typedef struct jt_server jt_server;
+typedef struct jt_serve_stats {
+    int64_t requests_served;
+    int64_t batched_steps;
+    int64_t particle_steps;
+    int64_t admitted;          /* admissions (a swapped-out job counts again) */
+    int64_t evicted;           /* jobs finished and evicted to host memory */
+    int64_t admission_waits;   /* admission attempts that did not fit */
+    double  p50_latency_s;     /* per step request: completion - arrival */
+    double  p99_latency_s;
+    double  max_latency_s;
+    double  busy_s;            /* wall time inside batched steps */
+    int64_t peak_device_bytes; /* batch memory after a step, maximum */
+    int64_t max_jobs_per_step;
+    int64_t swapped_out;       /* idle jobs moved to host to admit others */
+} jt_serve_stats;
+
+#define JT_JOB_QUEUED    0
+#define JT_JOB_RESIDENT  1
+#define JT_JOB_DONE      2
+
+int  jt_server_create(size_t hbm_budget_bytes, jt_server** out);
+void jt_server_destroy(jt_server* s);
+/* Register a job (host arrays copied to pinned memory; nothing on the device
+ * until a request admits it).  JT_EBUSY if it can never fit the budget. */
+int  jt_server_add_job(jt_server* s, const jt_config* cfg,
+                       const float* pos_p, const float* vel_p, size_t n_p,
+                       const float* pos_m, const float* vel_m, size_t n_m,
+                       int steps_total, const jt_step_args* args, int* job_id);
+/* One step request for a job at t_arrival seconds on the server clock
+ * (negative = now). */
+int  jt_server_request(jt_server* s, int job, double t_arrival);
+double jt_server_clock(jt_server* s);
+/* Admit what fits, run one batched step; *served = requests it served. */
+int  jt_server_poll(jt_server* s, int* served);
+/* Replay an arrival schedule (t ascending, seconds from the call) in real
+ * time until every request is served; JT_EBUSY if some can never be. */
+int  jt_server_serve(jt_server* s, const double* t, const int* job, int n);
+int  jt_server_job_state(jt_server* s, int job, int* state, int* steps_done);
+int  jt_server_get_state(jt_server* s, int job, float* pos_p, float* vel_p,
+                         float* pos_m, float* vel_m);
+int  jt_server_stats(jt_server* s, jt_serve_stats* out);
 
 /* ---- allocation-free Morton sort ----
  * The reference's Morton keys of n positions already on the device (float3

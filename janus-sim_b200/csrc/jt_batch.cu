@@ -125,6 +125,7 @@ struct Plan {
     int64_t npart = 0, ninternal = 0, nsorttiles = 0, ngroups = 0, npmtiles = 0, nmodes = 0;
     std::map<int, std::vector<int>> by_M; // M -> boxes (positions in ids)
     int maxT = 1;
+    size_t table_bytes = 0;
     const jt_seg_dev* d_pre = nullptr;
     const jt_seg_dev* d_post = nullptr;
     const jt_box_dev* d_bx = nullptr;
@@ -163,6 +164,19 @@ struct jt_batch {
     jt_timings tm = {};
     int64_t phase[4] = {0, 0, 0, 0};
     Plan plan;
+    // CUDA graphs of one step (opt-in, jt_batch_set_graphs)
+    uint64_t gen = 0;                   // bumps when an address a captured plan holds may change
+    bool use_graphs = false;
+    struct {
+        std::vector<int> ids;
+        uint64_t gen = ~0ull;
+        Plan plan;                      // its tables live in gdesc
+        cudaGraphExec_t exec[2] = {nullptr, nullptr};
+        const float4* pre0 = nullptr;   // first segment's pos at parity 0
+        int box0 = -1, sp0 = 0;
+        int64_t launches = 0;           // kernels per replay
+    } gc;
+    Pool<unsigned char> gdesc;
 };
 
 namespace {
@@ -228,6 +242,7 @@ int bucket_ensure(jt_batch* B, Bucket& k, int M, int count)
     const int ngrid = B->ngrid;
     const int64_t G = (int64_t)M * M * M, Gc = (int64_t)M * M * (M / 2 + 1);
     if (count > k.cap) {
+        B->gen++;
         k.free_arrays();
         int T = jt_pm_tile_edge(M);
         int64_t nt = (int64_t)(M / T) * (M / T) * (M / T);
@@ -393,6 +408,7 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
     P.npmtiles = P.ptprefix.back();
     P.nmodes = P.kprefix.back();
 
+    if (grew) B->gen++;
     std::vector<unsigned char> buf;
     size_t o_pre = put(buf, P.pre), o_post = put(buf, P.post), o_bx = put(buf, P.bx);
     size_t o_pp = put(buf, P.pprefix), o_ip = put(buf, P.iprefix), o_tp = put(buf, P.tprefix);
@@ -420,6 +436,7 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
     P.d_gp = (const int64_t*)(d + o_gp);
     P.d_ptp = (const int64_t*)(d + o_ptp);
     P.d_kp = (const int64_t*)(d + o_kp);
+    P.table_bytes = buf.size();
     return JT_OK;
 }
 
@@ -576,6 +593,99 @@ int read_out(jt_batch* B, const float4* src, const int* id, int64_t n, float* ds
 
 }  // namespace
 
+void drop_graphs(jt_batch* B)
+{
+    for (auto& e : B->gc.exec)
+        if (e) {
+            cudaGraphExecDestroy(e);
+            e = nullptr;
+        }
+    B->gc.ids.clear();
+    B->gc.gen = ~0ull;
+}
+
+void swap_state(jt_batch* B, const std::vector<int>& v)
+{
+    for (int id : v) {
+        jt_box_state* b = B->boxes[id];
+        for (int s = 0; s < 2; s++) {
+            std::swap(b->pos[s], b->pos_b[s]);
+            std::swap(b->vel[s], b->vel_b[s]);
+            std::swap(b->id[s], b->id_b[s]);
+        }
+    }
+}
+
+// Capture one KDK step of boxes v -- kick(dt/2), drift(dt), force pass with
+// the closing kick(dt/2) fused into the walk -- as two CUDA graphs, one per
+// parity of the ping-pong buffers (the reorder of every pass swaps them).
+// The graphs read a private copy of the step's tables (gdesc), so other
+// passes may rebuild the batch's own tables freely; any change of a device
+// address the tables hold bumps B->gen and invalidates the graphs.
+int capture_graphs(jt_batch* B, const std::vector<int>& v, const jt_box_step* steps)
+{
+    drop_graphs(B);
+    Plan P;
+    JT_TRY(build_plan(B, v, steps, P));
+    bool grew = false;
+    JT_TRY(B->gdesc.ensure(P.table_bytes, &grew));
+    JT_CU(cudaMemcpyAsync(B->gdesc.p, B->desc.p, P.table_bytes, cudaMemcpyDeviceToDevice, B->st));
+    auto rebase = [&](const void* p) -> const void* {
+        return B->gdesc.p + ((const unsigned char*)p - B->desc.p);
+    };
+    P.d_pre = (const jt_seg_dev*)rebase(P.d_pre);
+    P.d_post = (const jt_seg_dev*)rebase(P.d_post);
+    P.d_bx = (const jt_box_dev*)rebase(P.d_bx);
+    P.d_pp = (const int64_t*)rebase(P.d_pp);
+    P.d_ip = (const int64_t*)rebase(P.d_ip);
+    P.d_tp = (const int64_t*)rebase(P.d_tp);
+    P.d_gp = (const int64_t*)rebase(P.d_gp);
+    P.d_ptp = (const int64_t*)rebase(P.d_ptp);
+    P.d_kp = (const int64_t*)rebase(P.d_kp);
+    const jt_timings saved = B->tm;
+    const jt_box_state* b0 = B->boxes[v[0]];
+    const int sp0 = b0->n[0] > 0 ? 0 : 1;
+    const float4* pre0 = b0->pos[sp0];
+    int r = JT_OK;
+    for (int parity = 0; parity < 2 && r == JT_OK; parity++) {
+        if (cudaStreamBeginCapture(B->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            r = JT_ECUDA;
+            break;
+        }
+        jt_b_kick(P.d_pre, P.d_bx, P.d_pp, (int)P.pre.size(), P.npart, 0.5f, B->st);
+        jt_b_drift(P.d_pre, P.d_bx, P.d_pp, (int)P.pre.size(), P.npart, 1.0f, B->st);
+        int rf = force_pass(B, P, JT_PART_ALL, 0.5f);   // swaps the boxes' buffers and P
+        cudaGraph_t g = nullptr;
+        cudaError_t ec = cudaStreamEndCapture(B->st, &g);
+        if (rf != JT_OK || ec != cudaSuccess || !g) {
+            if (g) cudaGraphDestroy(g);
+            r = rf != JT_OK ? rf : JT_ECUDA;
+            break;
+        }
+        if (cudaGraphInstantiate(&B->gc.exec[parity], g, 0) != cudaSuccess) r = JT_ECUDA;
+        cudaGraphDestroy(g);
+    }
+    const int64_t per_pass = B->tm.launches - saved.launches;
+    B->tm = saved;
+    B->pending = false;
+    cudaGetLastError();
+    // nothing ran during the captures: if they left the host pointers
+    // swapped an odd number of times, swap them back
+    if (b0->pos[sp0] != pre0) swap_state(B, v);
+    if (r != JT_OK) {
+        drop_graphs(B);
+        return r;
+    }
+    B->gc.launches = per_pass / 2 + 2;
+    B->gc.ids = v;
+    B->gc.gen = B->gen;
+    B->gc.plan = P;
+    B->gc.box0 = v[0];
+    B->gc.sp0 = sp0;
+    B->gc.pre0 = pre0;
+    return JT_OK;
+}
+
 // ---------------------------------------------------------------- internal
 int jtb_add_empty(jt_batch* B, const jt_config* cfg, int64_t n_p, int64_t n_m, int* box_id)
 {
@@ -614,6 +724,7 @@ int jtb_add_empty(jt_batch* B, const jt_config* cfg, int64_t n_p, int64_t n_m, i
         B->boxes.push_back(nullptr);
     }
     B->boxes[slot] = b;
+    B->gen++;
     B->order = order;
     B->ngrid = ngrid;
     B->k_min = cfg->k_min;
@@ -680,6 +791,8 @@ void jt_batch_destroy(jt_batch* B)
     B->com.release(); B->bmin.release(); B->bmax.release(); B->quad0.release(); B->quad1.release();
     B->m30.release(); B->vals.release(); B->vals_alt.release(); B->keys_alt.release();
     B->hist.release(); B->status.release(); B->tickets.release(); B->desc.release();
+    drop_graphs(B);
+    B->gdesc.release();
     for (auto& kv : B->buckets) kv.second.release();
     if (B->hdesc) cudaFreeHost(B->hdesc);
     if (B->d_err) cudaFree(B->d_err);
@@ -745,6 +858,7 @@ int jt_batch_remove(jt_batch* B, int box_id)
     if (!box_id_ok(B, box_id)) return JT_EINVAL;
     cudaStreamSynchronize(B->st);
     box_release(B->boxes[box_id]);
+    B->gen++;
     delete B->boxes[box_id];
     B->boxes[box_id] = nullptr;
     return JT_OK;
@@ -794,9 +908,34 @@ int jt_batch_step(jt_batch* B, const int* ids, int n_ids, const jt_step_args* ar
         r = jtb_force_pass(B, v.data(), (int)v.size(), JT_PART_ALL, 0.0f, steps.data());
         if (r == JT_OK) r = finish(B);
     }
-    Plan& P = B->plan;
-    if (r == JT_OK) r = build_plan(B, v, steps.data(), P);
     double kd = 0.0;
+    if (r == JT_OK && B->use_graphs) {
+        if (B->gc.gen != B->gen || B->gc.ids != v) r = capture_graphs(B, v, steps.data());
+        if (r == JT_OK) {
+            // this call's dt and drag into the graphs' box table
+            Plan& G = B->gc.plan;
+            for (size_t k = 0; k < v.size(); k++) {
+                G.bx[k].dt = steps[k].dt;
+                G.bx[k].kick_drag = steps[k].drag;
+            }
+            r = cudaMemcpyAsync((void*)G.d_bx, G.bx.data(), sizeof(jt_box_dev) * G.bx.size(),
+                                cudaMemcpyHostToDevice, B->st) == cudaSuccess ? JT_OK : JT_ECUDA;
+        }
+        for (int k = 0; k < nsteps && r == JT_OK; k++) {
+            const int parity = B->boxes[B->gc.box0]->pos[B->gc.sp0] == B->gc.pre0 ? 0 : 1;
+            if (cudaGraphLaunch(B->gc.exec[parity], B->st) != cudaSuccess) {
+                r = JT_ECUDA;
+                break;
+            }
+            swap_state(B, v);
+            for (int id : v) B->boxes[id]->acc_valid = true;
+            B->tm.launches += B->gc.launches;
+        }
+        if (r == JT_OK) r = finish(B);
+        nsteps = 0;   // all steps ran as graphs
+    }
+    Plan& P = B->plan;
+    if (r == JT_OK && nsteps > 0) r = build_plan(B, v, steps.data(), P);
     for (int k = 0; k < nsteps && r == JT_OK; k++) {
         cudaEventRecord(k0, B->st);
         if (k == 0) jt_b_kick(P.d_pre, P.d_bx, P.d_pp, (int)P.pre.size(), P.npart, 0.5f, B->st);
@@ -884,6 +1023,28 @@ int jt_batch_estimate(const jt_config* cfg, size_t n_p, size_t n_m, size_t* pers
         size_t sort = n * 4 * sizeof(uint32_t) + (n / 4096 + 2) * 4 * 256 * sizeof(uint32_t);
         *scratch = tree + sort + grid_bytes(M, box_ngrid(*cfg));
     }
+    return JT_OK;
+}
+
+int jt_batch_set_graphs(jt_batch* B, int on)
+{
+    if (!B) return JT_EINVAL;
+    B->use_graphs = on != 0;
+    if (!on) drop_graphs(B);
+    return JT_OK;
+}
+
+int jt_batch_trim(jt_batch* B)
+{
+    if (!B) return JT_EINVAL;
+    if (cudaStreamSynchronize(B->st) != cudaSuccess) return JT_ECUDA;
+    B->child.release(); B->range.release(); B->parent.release(); B->flag.release();
+    B->com.release(); B->bmin.release(); B->bmax.release(); B->quad0.release(); B->quad1.release();
+    B->m30.release(); B->vals.release(); B->vals_alt.release(); B->keys_alt.release();
+    B->hist.release(); B->status.release(); B->tickets.release();
+    for (auto& kv : B->buckets) kv.second.release();
+    B->buckets.clear();
+    B->gen++;
     return JT_OK;
 }
 

@@ -42,7 +42,11 @@ EXPORTED = [
     "jt_batch_create", "jt_batch_destroy", "jt_batch_add", "jt_batch_remove", "jt_batch_forces",
     "jt_batch_step", "jt_batch_get_accel", "jt_batch_get_state", "jt_batch_box_info",
     "jt_batch_memory", "jt_batch_estimate", "jt_batch_get_timings", "jt_morton_sort_static",
+    "jt_batch_trim", "jt_batch_set_graphs", "jt_server_create", "jt_server_destroy",
+    "jt_server_add_job", "jt_server_request", "jt_server_clock", "jt_server_poll", "jt_server_serve",
+    "jt_server_job_state", "jt_server_get_state", "jt_server_stats",
 ]
+JT_JOB_QUEUED, JT_JOB_RESIDENT, JT_JOB_DONE = 0, 1, 2
 JT_STATIC_SORT_MAX = 262144
 
 
@@ -76,6 +80,16 @@ class jt_timings(C.Structure):
 
 class jt_step_args(C.Structure):
     _fields_ = [("dt", C.c_double), ("hubble", C.c_double), ("dtau_per_dt", C.c_double)]
+
+
+class jt_serve_stats(C.Structure):
+    _fields_ = [
+        ("requests_served", C.c_int64), ("batched_steps", C.c_int64), ("particle_steps", C.c_int64),
+        ("admitted", C.c_int64), ("evicted", C.c_int64), ("admission_waits", C.c_int64),
+        ("p50_latency_s", C.c_double), ("p99_latency_s", C.c_double), ("max_latency_s", C.c_double),
+        ("busy_s", C.c_double), ("peak_device_bytes", C.c_int64), ("max_jobs_per_step", C.c_int64),
+        ("swapped_out", C.c_int64),
+    ]
 
 
 _lib = None
@@ -127,8 +141,24 @@ def library():
     L.jt_batch_estimate.argtypes = [C.POINTER(jt_config), C.c_size_t, C.c_size_t, szp, szp]
     L.jt_batch_get_timings.argtypes = [H, C.POINTER(jt_timings)]
     L.jt_morton_sort_static.argtypes = [vp, C.c_size_t, C.c_double, vp, vp, vp]
+    L.jt_batch_trim.argtypes = [H]
+    L.jt_batch_set_graphs.argtypes = [H, C.c_int]
+    L.jt_server_create.argtypes = [C.c_size_t, C.POINTER(H)]
+    L.jt_server_destroy.argtypes = [H]
+    L.jt_server_destroy.restype = None
+    L.jt_server_add_job.argtypes = [H, C.POINTER(jt_config), fp, fp, C.c_size_t, fp, fp, C.c_size_t,
+                                    C.c_int, C.POINTER(jt_step_args), C.POINTER(C.c_int)]
+    L.jt_server_request.argtypes = [H, C.c_int, C.c_double]
+    L.jt_server_clock.argtypes = [H]
+    L.jt_server_clock.restype = C.c_double
+    L.jt_server_poll.argtypes = [H, C.POINTER(C.c_int)]
+    L.jt_server_serve.argtypes = [H, vp, vp, C.c_int]
+    L.jt_server_job_state.argtypes = [H, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.jt_server_get_state.argtypes = [H, C.c_int, fp, fp, fp, fp]
+    L.jt_server_stats.argtypes = [H, C.POINTER(jt_serve_stats)]
     for name in EXPORTED:
-        if name not in ("jt_destroy", "jt_strerror", "jt_version", "jt_batch_destroy"):
+        if name not in ("jt_destroy", "jt_strerror", "jt_version", "jt_batch_destroy",
+                        "jt_server_destroy", "jt_server_clock"):
             getattr(L, name).restype = C.c_int
     _lib = L
     return L
@@ -328,10 +358,20 @@ class Batch:
     Config (all accurate/KDK with the same pm_order, pm_interlace, k_min).
     """
 
-    def __init__(self):
+    def __init__(self, graphs=False):
         self._b = C.c_void_p()
         _check(library().jt_batch_create(C.byref(self._b)), "jt_batch_create")
         self.boxes = {}
+        if graphs:
+            self.set_graphs(True)
+
+    def set_graphs(self, on):
+        """Replay each batched step as a CUDA graph (captured per set of boxes)."""
+        _check(library().jt_batch_set_graphs(self._b, 1 if on else 0), "jt_batch_set_graphs")
+
+    def trim(self):
+        """Release the per-pass scratch pools (they regrow on the next pass)."""
+        _check(library().jt_batch_trim(self._b), "jt_batch_trim")
 
     def close(self):
         if self._b:
@@ -415,6 +455,79 @@ class Batch:
         t = jt_timings()
         _check(library().jt_batch_get_timings(self._b, C.byref(t)), "jt_batch_get_timings")
         return {k: getattr(t, k) for k, _ in jt_timings._fields_}
+
+
+class Server:
+    """Serving loop over a batch (a jt_server): jobs admitted by an HBM budget,
+    step requests served by continuous batching, finished jobs evicted to
+    pinned host memory, idle jobs swapped out to make room."""
+
+    def __init__(self, hbm_budget_bytes):
+        self._s = C.c_void_p()
+        _check(library().jt_server_create(int(hbm_budget_bytes), C.byref(self._s)), "jt_server_create")
+        self.jobs = {}
+
+    def close(self):
+        if self._s:
+            library().jt_server_destroy(self._s)
+            self._s = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_job(self, config: Config, pos_p, vel_p, pos_m, vel_m, steps, dt, hubble=0.0,
+                dtau_per_dt=1.0):
+        pos_p = _f32(pos_p) if pos_p is not None else np.zeros((0, 3), np.float32)
+        pos_m = _f32(pos_m) if pos_m is not None else np.zeros((0, 3), np.float32)
+        vel_p = None if vel_p is None else _f32(vel_p)
+        vel_m = None if vel_m is None else _f32(vel_m)
+        cfg = config.resolved().to_c()
+        args = jt_step_args(float(dt), float(hubble), float(dtau_per_dt))
+        jid = C.c_int(-1)
+        _check(library().jt_server_add_job(self._s, C.byref(cfg), _ptr(pos_p), _ptr(vel_p), len(pos_p),
+                                           _ptr(pos_m), _ptr(vel_m), len(pos_m), int(steps),
+                                           C.byref(args), C.byref(jid)), "jt_server_add_job")
+        self.jobs[jid.value] = (len(pos_p), len(pos_m))
+        return jid.value
+
+    def request(self, job, t_arrival=-1.0):
+        _check(library().jt_server_request(self._s, job, float(t_arrival)), "jt_server_request")
+
+    def clock(self):
+        return library().jt_server_clock(self._s)
+
+    def poll(self):
+        """Admit what fits and run one batched step; returns requests served."""
+        n = C.c_int(0)
+        _check(library().jt_server_poll(self._s, C.byref(n)), "jt_server_poll")
+        return n.value
+
+    def serve(self, t, jobs):
+        """Replay arrival times t (seconds, ascending) of requests for jobs."""
+        t = np.ascontiguousarray(t, np.float64)
+        jobs = np.ascontiguousarray(jobs, np.int32)
+        _check(library().jt_server_serve(self._s, _ptr(t), _ptr(jobs), len(t)), "jt_server_serve")
+
+    def job_state(self, job):
+        st, done = C.c_int(), C.c_int()
+        _check(library().jt_server_job_state(self._s, job, C.byref(st), C.byref(done)),
+               "jt_server_job_state")
+        return st.value, done.value
+
+    def get_state(self, job):
+        n_p, n_m = self.jobs[job]
+        out = [np.zeros((n, 3), np.float32) for n in (n_p, n_p, n_m, n_m)]
+        _check(library().jt_server_get_state(self._s, job, *[_ptr(a) for a in out]),
+               "jt_server_get_state")
+        return tuple(out)
+
+    def stats(self):
+        st = jt_serve_stats()
+        _check(library().jt_server_stats(self._s, C.byref(st)), "jt_server_stats")
+        return {k: getattr(st, k) for k, _ in jt_serve_stats._fields_}
 
 
 # --------------------------------------------------------------------------

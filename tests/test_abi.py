@@ -21,7 +21,7 @@ HEADER = os.path.join(ROOT, "include", "janus_treepm.h")
 def declared_functions():
     text = open(HEADER).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    names = re.findall(r"^\s*(?:int|void|const char\*)\s+(jt_\w+)\s*\(", text, flags=re.M)
+    names = re.findall(r"^\s*(?:int|void|double|const char\*)\s+(jt_\w+)\s*\(", text, flags=re.M)
     return sorted(set(names))
 
 
@@ -97,3 +97,26 @@ def test_config_defaults_follow_the_workload_convention():
     c = J.Config(box_L=250.0, pm_grid=512).resolved()
     assert abs(c.r_s - 1.25 * 250.0 / 512) < 1e-12
     assert abs(c.r_cut - 4.5 * c.r_s) < 1e-12
+
+
+def test_batch_estimate_needs_no_device():
+    import janus_treepm as J
+    cfg = J.Config(box_L=100.0, pm_grid=64)
+    p1, s1 = J.Batch.estimate(cfg, 10_000, 10_000)
+    p2, s2 = J.Batch.estimate(cfg, 20_000, 20_000)
+    assert 0 < p1 < p2 and 0 < s1 < s2
+    # persistent state: 5 float4 + 2 int per particle, plus the k tables
+    assert p1 == 20_000 * (5 * 16 + 8) + 2 * 64 * 16
+    bad = J.Config(box_L=100.0, pm_grid=64, mode=J.JT_RCOMPAT).resolved().to_c()
+    a, b = C.c_size_t(), C.c_size_t()
+    assert J.library().jt_batch_estimate(C.byref(bad), 10, 10, C.byref(a), C.byref(b)) == J.JT_EINVAL
+
+
+def test_server_rejects_bad_arguments_without_a_device():
+    import janus_treepm as J
+    L = J.library()
+    h = C.c_void_p()
+    assert L.jt_server_create(0, C.byref(h)) == J.JT_EINVAL
+    assert L.jt_server_poll(None, None) == J.JT_EINVAL
+    assert L.jt_server_request(None, 0, 0.0) == J.JT_EINVAL
+    L.jt_server_destroy(None)

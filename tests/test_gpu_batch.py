@@ -162,3 +162,33 @@ def test_batch_rejects_mismatched_shared_fields():
     with pytest.raises(J.JanusError):
         B.forces([5])                  # unknown id
     B.close()
+
+
+def test_graph_replay_matches_plain_launches():
+    dts = [0.01, 0.02, 0.005, 0.01, 0.015, 0.01, 0.02]
+    hub = [0.0, 0.1, 0.05, 0.2, 0.0, 0.0, 0.07]
+    A, G = J.Batch(), J.Batch(graphs=True)
+    ia = [A.add(*make_box(*box)) for box in BOXES]
+    ig = [G.add(*make_box(*box)) for box in BOXES]
+    # odd and even step counts (both graph parities), a dt change between
+    # calls, and a subset (a second capture) in between
+    for n, scale in ((3, 1.0), (2, 0.5)):
+        A.step(ia, [d * scale for d in dts], hub, 1.0, nsteps=n)
+        G.step(ig, [d * scale for d in dts], hub, 1.0, nsteps=n)
+        A.step(ia[:3], dts[:3], hub[:3], 1.0, nsteps=1)
+        G.step(ig[:3], dts[:3], hub[:3], 1.0, nsteps=1)
+    assert G.timings()["launches"] > 0
+    for k, box in enumerate(BOXES):
+        L = make_box(*box)[0].box_L
+        for q, (g, r) in enumerate(zip(G.get_state(ig[k]), A.get_state(ia[k]))):
+            if len(r) == 0:
+                continue
+            d = np.abs(g.astype(np.float64) - r)
+            if q % 2 == 0:
+                d = np.minimum(d, L - d)
+                assert float(d.max()) <= POS_TOL_L * L, (k, q, float(d.max()))
+            else:
+                rms = float(np.sqrt(np.mean(np.sum(r.astype(np.float64) ** 2, axis=1))))
+                assert float(d.max()) <= VEL_TOL * rms, (k, q, float(d.max()), rms)
+    A.close()
+    G.close()

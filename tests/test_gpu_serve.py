@@ -1,0 +1,133 @@
+"""Serving loop on the GPU: jobs admitted by an HBM budget, step requests
+served by continuous batching, each job's result the same alone and in the mix.
+
+A job served alone (the only job on the server) and the same job served among
+others (Poisson arrivals interleaved, a budget that forces admission waits
+and swap-outs to pinned host memory) takes the same KDK steps on the same
+kernels; the differences come only from the order of floating-point atomics
+in the deposit.  Tolerance after all steps: positions within 1e-6 x L,
+velocities within 1e-4 x rms|v| (the batch tests' bounds).
+"""
+import numpy as np
+import pytest
+
+import janus_treepm as J
+
+pytestmark = pytest.mark.gpu
+
+POS_TOL_L = 1e-6
+VEL_TOL = 1e-4
+GiB = 1 << 30
+
+
+def job_spec(seed):
+    rng = np.random.default_rng(seed)
+    n_side = int(rng.integers(10, 26))
+    L = float(rng.uniform(50.0, 200.0))
+    M = 1 << int(np.ceil(np.log2(2 * n_side)))
+    mu = float(rng.uniform(5.0, 30.0))
+    n = n_side ** 3
+    pp = rng.uniform(-L / 2, L / 2, (n, 3)).astype(np.float32)
+    pm = rng.uniform(-L / 2, L / 2, (n, 3)).astype(np.float32)
+    vp = rng.normal(0, 0.3, (n, 3)).astype(np.float32)
+    vm = rng.normal(0, 0.3, (n, 3)).astype(np.float32)
+    cfg = J.Config(box_L=L, pm_grid=M, theta=0.5, softening=L / (2 * n) ** (1 / 3) / 30, mu=mu,
+                   G_mass_plus=1e-3 * (L / n_side / 1.116) ** 3)
+    dt = float(rng.uniform(0.005, 0.02))
+    hub = float(rng.uniform(0.0, 0.1))
+    return cfg, (pp, vp, pm, vm), dt, hub
+
+
+def _same(got, ref, L):
+    for q, (g, r) in enumerate(zip(got, ref)):
+        if len(r) == 0:
+            continue
+        d = np.abs(g.astype(np.float64) - r)
+        if q % 2 == 0:
+            d = np.minimum(d, L - d)
+            assert float(d.max()) <= POS_TOL_L * L, (q, float(d.max()))
+        else:
+            rms = float(np.sqrt(np.mean(np.sum(r.astype(np.float64) ** 2, axis=1))))
+            assert float(d.max()) <= VEL_TOL * rms, (q, float(d.max()), rms)
+
+
+def serve_alone(seed, steps):
+    cfg, st, dt, hub = job_spec(seed)
+    S = J.Server(8 * GiB)
+    j = S.add_job(cfg, *st, steps=steps, dt=dt, hubble=hub)
+    for _ in range(steps):
+        S.request(j)
+        assert S.poll() == 1
+    assert S.job_state(j) == (J.JT_JOB_DONE, steps)
+    out = S.get_state(j)
+    S.close()
+    return out, cfg
+
+
+def test_each_job_same_alone_and_in_the_mix():
+    seeds = [101, 102, 103, 104, 105, 106]
+    steps = 3
+    S = J.Server(8 * GiB)
+    jobs = {}
+    for sd in seeds:
+        cfg, st, dt, hub = job_spec(sd)
+        jobs[S.add_job(cfg, *st, steps=steps, dt=dt, hubble=hub)] = sd
+    # Poisson arrivals: every job's requests interleaved with the others'
+    rng = np.random.default_rng(5)
+    reqs = [j for j in jobs for _ in range(steps)]
+    rng.shuffle(reqs)
+    t = np.cumsum(rng.exponential(0.002, len(reqs)))
+    S.serve(t, reqs)
+    stats = S.stats()
+    assert stats["requests_served"] == len(reqs)
+    assert stats["evicted"] == len(seeds)
+    assert stats["max_jobs_per_step"] >= 2          # requests of different jobs were batched
+    assert stats["p99_latency_s"] >= stats["p50_latency_s"] > 0
+    for j, sd in jobs.items():
+        assert S.job_state(j) == (J.JT_JOB_DONE, steps)
+        ref, cfg = serve_alone(sd, steps)
+        _same(S.get_state(j), ref, cfg.box_L)
+    S.close()
+
+
+def test_budget_forces_swaps_but_results_hold():
+    steps = 2
+    need_of = lambda sp: sum(J.Batch.estimate(sp[0], len(sp[1][0]), len(sp[1][2])))
+    # job 0 is the smallest; the budget holds the largest job plus half of
+    # job 0, so admitting the largest must swap out job 0 while it is idle
+    seeds = sorted([201, 202, 203, 204], key=lambda sd: need_of(job_spec(sd)))
+    specs = [job_spec(sd) for sd in seeds]
+    need = [need_of(sp) for sp in specs]
+    budget = max(need) + need[0] // 2
+    S = J.Server(budget)
+    ids = [S.add_job(cfg, *st, steps=steps, dt=dt, hubble=hub) for cfg, st, dt, hub in specs]
+    # job 0 takes one step and goes idle; the others then arrive; job 0's
+    # second request comes last, after it has been swapped out
+    S.request(ids[0])
+    assert S.poll() == 1
+    for j in ids[1:]:
+        for _ in range(steps):
+            S.request(j)
+    while S.poll():
+        pass
+    S.request(ids[0])
+    while S.poll():
+        pass
+    st = S.stats()
+    assert st["requests_served"] == steps * len(ids)
+    assert st["swapped_out"] >= 1
+    assert st["admitted"] >= len(ids) + 1          # job 0 came back after its swap-out
+    for j, sd in zip(ids, seeds):
+        assert S.job_state(j) == (J.JT_JOB_DONE, steps)
+        ref, cfg = serve_alone(sd, steps)
+        _same(S.get_state(j), ref, cfg.box_L)
+    S.close()
+
+
+def test_job_that_never_fits_is_refused():
+    cfg, st, dt, hub = job_spec(301)
+    S = J.Server(1 << 20)                 # 1 MiB
+    with pytest.raises(J.JanusError) as e:
+        S.add_job(cfg, *st, steps=1, dt=dt)
+    assert e.value.code == J.JT_EBUSY
+    S.close()
