@@ -194,6 +194,16 @@ def run_ensemble(J, ics, n_boxes, steps, warmup, H, dt):
     torch.cuda.synchronize()
     wall_b = time.perf_counter() - t0
     mem = B.memory()
+    # the same steps replayed as CUDA graphs (captured once for the set)
+    B.set_graphs(True)
+    B.step(ids, dt, H, 1.0, 1)
+    torch.cuda.synchronize()
+    dev_g, t0 = 0.0, time.perf_counter()
+    for _ in range(steps):
+        B.step(ids, dt, H, 1.0, 1)
+        dev_g += B.timings()["total_ms"]
+    torch.cuda.synchronize()
+    wall_g = time.perf_counter() - t0
     B.close()
     # plain: one handle per box, stepped one after another
     solvers = []
@@ -221,6 +231,7 @@ def run_ensemble(J, ics, n_boxes, steps, warmup, H, dt):
                     f"L U(50,300), PM 32..256, mu U(5,30)",
         "value": v_b, "unit": UNIT, "ms_per_step": dev / steps,
         "wall_value": n_part * steps / wall_b,
+        "graph_value": n_part * steps / (dev_g * 1e-3), "graph_wall_value": n_part * steps / wall_g,
         "plain_value": v_p, "plain_ms_per_step": dev_p / steps,
         "plain_wall_value": n_part * steps / wall_p,
         "speedup_vs_plain": v_b / v_p, "speedup_vs_plain_wall": wall_p / wall_b,
@@ -228,6 +239,64 @@ def run_ensemble(J, ics, n_boxes, steps, warmup, H, dt):
         "stages_ms_per_step": {k: round(v / steps, 4) for k, v in stages.items() if k.endswith("_ms")},
         "device_bytes": {"persistent": mem[0], "scratch": mem[1]},
         "steps": steps,
+    }
+
+
+def run_serving(J, ics, n_small, n_big, steps, rate_frac, capacity_ps, H, dt, budget_gb=150.0,
+                seed=11):
+    """The serving workload: n_small jobs sized as the ensemble boxes plus
+    n_big jobs of 2x256^3 (L = 300 Mpc, PM 512^3), each wanting `steps` KDK
+    steps, admitted by an HBM budget.  Step requests arrive as one Poisson
+    stream at rate_frac x the capacity estimated from the batched ensemble's
+    particle-steps/s; request k of a job comes in round k (every job's k-th
+    request before any (k+1)-th), jobs in a random order per round.  The big
+    jobs share one Zel'dovich realisation, each moved by a random periodic
+    shift and axis permutation (generating eight 256^3 fields would take
+    minutes of host time)."""
+    rng = np.random.default_rng(seed)
+    small = ensemble_boxes(n_small, seed=seed)
+    S = J.Server(int(budget_gb * (1 << 30)))
+    parts = []
+    for bx in small:
+        st = ics.zeldovich_lattice(bx["n"], bx["L"], seed=bx["seed"])
+        S.add_job(box_config(J, bx), *st, steps=steps, dt=dt, hubble=H)
+        parts.append(2 * bx["n"] ** 3)
+    if n_big:
+        big_base = ics.zeldovich_lattice(256, 300.0, seed=seed)
+        bigbx = dict(n=256, L=300.0, M=512, mu=19.0)
+        for b in range(n_big):
+            shift = rng.uniform(-150.0, 150.0, 3).astype(np.float32)
+            perm = rng.permutation(3)
+            st = []
+            for k, a in enumerate(big_base):
+                a = a[:, perm]
+                if k % 2 == 0:
+                    a = ((a + shift + 150.0) % 300.0 - 150.0).astype(np.float32)
+                st.append(np.ascontiguousarray(a))
+            S.add_job(box_config(J, bigbx), *st, steps=steps, dt=dt, hubble=H)
+            parts.append(2 * 256 ** 3)
+        del big_base
+    n_jobs = len(parts)
+    rate = rate_frac * capacity_ps / float(np.mean(parts))     # requests per second
+    order = np.concatenate([rng.permutation(n_jobs) for _ in range(steps)])
+    t = np.cumsum(rng.exponential(1.0 / rate, len(order)))
+    t -= t[0]
+    t0 = time.perf_counter()
+    S.serve(t, order)
+    wall = time.perf_counter() - t0
+    st = S.stats()
+    S.close()
+    total_ps = float(sum(parts) * steps)
+    return {
+        "workload": f"{n_small} ensemble-style jobs + {n_big} jobs of 2x256^3 (L=300, PM 512^3), "
+                    f"{steps} steps each, {budget_gb:g} GB HBM budget, Poisson arrivals",
+        "arrival_rate_per_s": rate, "rate_vs_capacity": rate_frac,
+        "value": total_ps / wall, "unit": UNIT, "makespan_s": wall,
+        "p50_latency_ms": 1e3 * st["p50_latency_s"], "p99_latency_ms": 1e3 * st["p99_latency_s"],
+        "max_latency_ms": 1e3 * st["max_latency_s"], "gpu_busy_frac": st["busy_s"] / wall,
+        "requests": int(st["requests_served"]), "batched_steps": int(st["batched_steps"]),
+        "max_jobs_per_step": int(st["max_jobs_per_step"]), "admission_waits": int(st["admission_waits"]),
+        "swapped_out": int(st["swapped_out"]), "peak_device_gb": st["peak_device_bytes"] / 1e9,
     }
 
 
@@ -370,8 +439,15 @@ def run_ours(args, ws, rank, local):
                          f"eps, theta), {tcpu:.1f} s"}
     launches = stages.get("launches", 0)
     ensemble = None
+    serving = None
     if rank == 0 and ws == 1 and args.ensemble_boxes > 0:
         ensemble = run_ensemble(J, ics, args.ensemble_boxes, args.ensemble_steps, 3, H, w["dt"])
+        if args.serve_jobs > 0:
+            serving = [run_serving(J, ics, args.serve_jobs, args.serve_big, args.serve_steps, float(r),
+                                   ensemble["value"], H, w["dt"])
+                       for r in args.serve_rates.split(",")]
+            for sv in serving:
+                sv["vs_plain_ensemble"] = sv["value"] / ensemble["plain_value"]
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K,
@@ -401,6 +477,7 @@ def run_ours(args, ws, rank, local):
             "gpu_launches": int(launches),
             "cpu_baseline": cpu,
             "ensemble": ensemble,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     s.close()
@@ -421,6 +498,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ensemble-boxes", type=int, default=64)
     ap.add_argument("--ensemble-steps", type=int, default=5)
+    ap.add_argument("--serve-jobs", type=int, default=256)
+    ap.add_argument("--serve-big", type=int, default=8)
+    ap.add_argument("--serve-steps", type=int, default=2)
+    ap.add_argument("--serve-rates", default="1.0")
     args = ap.parse_args()
     ws, rank, local = dist()
     if args.impl == "reference":
