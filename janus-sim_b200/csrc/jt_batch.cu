@@ -7,7 +7,7 @@
 // boxes (uneven particle counts, box sizes, PM grids, mu); a step over a
 // chosen subset of them runs every stage as one launch over the flattened
 // work of all chosen boxes (segments = box x species, jt_internal.cuh), with
-// cuFFT plans bucketed by grid size (one batched R2C and one batched C2R per
+// cuFFT plans bucketed by grid size (batched R2C and C2R per
 // distinct M).  Only particle state persists per box; trees, sort workspaces
 // and PM grids are per-pass scratch in grow-only pools, so boxes can join and
 // leave between steps (the serving loop admits and evicts jobs this way).
@@ -91,7 +91,9 @@ struct Bucket {                 // PM scratch of the boxes with grid M in a pass
     float2* force_k = nullptr;
     float* force = nullptr;
     int4* ranges = nullptr;
-    std::map<int, std::pair<cufftHandle, cufftHandle>> plans;   // count -> (r2c, c2r)
+    // batched plans by transform count: r2c[b], c2r[b] transform b grids
+    // per execution (at most fft_chunk(M) each, see below)
+    std::map<int, cufftHandle> r2c, c2r;
     void free_arrays()
     {
         dfree(rho); dfree(rho_k); dfree(force_k); dfree(force); dfree(ranges);
@@ -100,11 +102,10 @@ struct Bucket {                 // PM scratch of the boxes with grid M in a pass
     void release()
     {
         free_arrays();
-        for (auto& kv : plans) {
-            cufftDestroy(kv.second.first);
-            cufftDestroy(kv.second.second);
-        }
-        plans.clear();
+        for (auto& kv : r2c) cufftDestroy(kv.second);
+        for (auto& kv : c2r) cufftDestroy(kv.second);
+        r2c.clear();
+        c2r.clear();
     }
 };
 
@@ -236,6 +237,30 @@ int tile_shift_of(int M)
     return 3 * lw;
 }
 
+// Grids per cuFFT execution: at most 2^27 real elements (one 512^3 grid,
+// eight 256^3, ...), which keeps every plan inside cuFFT's 32-bit sizes and
+// bounds its work area; a bucket's transforms run as consecutive chunks.
+int fft_chunk(int M)
+{
+    const int64_t G = (int64_t)M * M * M;
+    const int64_t c = ((int64_t)1 << 27) / G;
+    return c < 1 ? 1 : (int)c;
+}
+
+int make_plan(jt_batch* B, std::map<int, cufftHandle>& pl, int M, int batch, bool r2c)
+{
+    if (batch <= 0 || pl.count(batch)) return JT_OK;
+    const int64_t G = (int64_t)M * M * M, Gc = (int64_t)M * M * (M / 2 + 1);
+    int dims[3] = {M, M, M};
+    cufftHandle h;
+    cufftResult e = r2c ? cufftPlanMany(&h, 3, dims, nullptr, 1, (int)G, nullptr, 1, (int)Gc, CUFFT_R2C, batch)
+                        : cufftPlanMany(&h, 3, dims, nullptr, 1, (int)Gc, nullptr, 1, (int)G, CUFFT_C2R, batch);
+    if (e != CUFFT_SUCCESS) return e == CUFFT_ALLOC_FAILED ? JT_ENOMEM : JT_ECUDA;
+    cufftSetStream(h, B->st);
+    pl[batch] = h;
+    return JT_OK;
+}
+
 int bucket_ensure(jt_batch* B, Bucket& k, int M, int count)
 {
     k.M = M;
@@ -253,19 +278,41 @@ int bucket_ensure(jt_batch* B, Bucket& k, int M, int count)
         JT_TRY(dalloc(&k.ranges, (size_t)count * nt));
         k.cap = count;
     }
-    if (!k.plans.count(count)) {
-        int dims[3] = {M, M, M};
-        cufftHandle r2c, c2r;
-        JT_FFT(cufftPlanMany(&r2c, 3, dims, nullptr, 1, (int)G, nullptr, 1, (int)Gc, CUFFT_R2C,
-                             ngrid * count));
-        if (cufftPlanMany(&c2r, 3, dims, nullptr, 1, (int)Gc, nullptr, 1, (int)G, CUFFT_C2R,
-                          3 * ngrid * count) != CUFFT_SUCCESS) {
-            cufftDestroy(r2c);
+    // plans for the full chunk and the remainder of both transform counts
+    const int ch = fft_chunk(M);
+    const int nr = ngrid * count, nc = 3 * ngrid * count;
+    JT_TRY(make_plan(B, k.r2c, M, std::min(ch, nr), true));
+    JT_TRY(make_plan(B, k.r2c, M, nr % ch, true));
+    JT_TRY(make_plan(B, k.c2r, M, std::min(ch, nc), false));
+    JT_TRY(make_plan(B, k.c2r, M, nc % ch, false));
+    return JT_OK;
+}
+
+// Run n transforms of a bucket in chunks of at most fft_chunk(M).
+int exec_r2c(Bucket& K, int n)
+{
+    const int64_t G = (int64_t)K.M * K.M * K.M, Gc = (int64_t)K.M * K.M * (K.M / 2 + 1);
+    const int ch = fft_chunk(K.M);
+    for (int off = 0; off < n; off += ch) {
+        const int b = std::min(ch, n - off);
+        auto it = K.r2c.find(b);
+        if (it == K.r2c.end()) return JT_ECUDA;   // bucket_ensure made every size a pass uses
+        if (cufftExecR2C(it->second, K.rho + off * G, (cufftComplex*)(K.rho_k + off * Gc)) != CUFFT_SUCCESS)
             return JT_ECUDA;
-        }
-        cufftSetStream(r2c, B->st);
-        cufftSetStream(c2r, B->st);
-        k.plans[count] = {r2c, c2r};
+    }
+    return JT_OK;
+}
+
+int exec_c2r(Bucket& K, int n)
+{
+    const int64_t G = (int64_t)K.M * K.M * K.M, Gc = (int64_t)K.M * K.M * (K.M / 2 + 1);
+    const int ch = fft_chunk(K.M);
+    for (int off = 0; off < n; off += ch) {
+        const int b = std::min(ch, n - off);
+        auto it = K.c2r.find(b);
+        if (it == K.c2r.end()) return JT_ECUDA;
+        if (cufftExecC2R(it->second, (cufftComplex*)(K.force_k + off * Gc), K.force + off * G) != CUFFT_SUCCESS)
+            return JT_ECUDA;
     }
     return JT_OK;
 }
@@ -464,14 +511,14 @@ int force_pass(jt_batch* B, Plan& P, int parts, float kick_frac)
     cudaEventRecord(B->ev[3], st);
     for (auto& kv : P.by_M) {
         Bucket& K = B->buckets[kv.first];
-        JT_FFT(cufftExecR2C(K.plans[(int)kv.second.size()].first, K.rho, (cufftComplex*)K.rho_k));
+        JT_TRY(exec_r2c(K, B->ngrid * (int)kv.second.size()));
     }
     cudaEventRecord(B->ev[4], st);
     jt_b_kspace(P.d_bx, P.d_kp, nbox, P.nmodes, B->ngrid == 2, B->k_min, st);
     cudaEventRecord(B->ev[5], st);
     for (auto& kv : P.by_M) {
         Bucket& K = B->buckets[kv.first];
-        JT_FFT(cufftExecC2R(K.plans[(int)kv.second.size()].second, (cufftComplex*)K.force_k, K.force));
+        JT_TRY(exec_c2r(K, 3 * B->ngrid * (int)kv.second.size()));
     }
     cudaEventRecord(B->ev[6], st);
     jt_tree_dev pool = {};
