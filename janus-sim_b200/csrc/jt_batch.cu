@@ -47,7 +47,10 @@ int dalloc(T** p, size_t count)
 {
     *p = nullptr;
     if (count == 0) count = 1;
-    return cudaMalloc((void**)p, sizeof(T) * count) == cudaSuccess ? JT_OK : JT_ENOMEM;
+    if (cudaMalloc((void**)p, sizeof(T) * count) == cudaSuccess) return JT_OK;
+    *p = nullptr;
+    cudaGetLastError();   // an allocation failure is not sticky: keep it out of later checks
+    return JT_ENOMEM;
 }
 template <class T>
 void dfree(T*& p)
@@ -56,7 +59,7 @@ void dfree(T*& p)
     p = nullptr;
 }
 
-// grow-only device array (25% headroom on growth)
+// grow-only device array (1/16 headroom on growth)
 template <class T>
 struct Pool {
     T* p = nullptr;
@@ -64,7 +67,7 @@ struct Pool {
     int ensure(size_t n, bool* grew)
     {
         if (n <= cap) return JT_OK;
-        size_t want = std::max(n, cap + cap / 4);
+        size_t want = std::max(n, cap + cap / 16);
         dfree(p);
         cap = 0;
         JT_TRY(dalloc(&p, want));
@@ -178,6 +181,10 @@ struct jt_batch {
         int64_t launches = 0;           // kernels per replay
     } gc;
     Pool<unsigned char> gdesc;
+    // one cuFFT work area shared by every plan (they run in stream order)
+    Pool<unsigned char> fftws;
+    size_t fft_need = 0;
+    bool fft_dirty = false;
 };
 
 namespace {
@@ -253,10 +260,22 @@ int make_plan(jt_batch* B, std::map<int, cufftHandle>& pl, int M, int batch, boo
     const int64_t G = (int64_t)M * M * M, Gc = (int64_t)M * M * (M / 2 + 1);
     int dims[3] = {M, M, M};
     cufftHandle h;
-    cufftResult e = r2c ? cufftPlanMany(&h, 3, dims, nullptr, 1, (int)G, nullptr, 1, (int)Gc, CUFFT_R2C, batch)
-                        : cufftPlanMany(&h, 3, dims, nullptr, 1, (int)Gc, nullptr, 1, (int)G, CUFFT_C2R, batch);
-    if (e != CUFFT_SUCCESS) return e == CUFFT_ALLOC_FAILED ? JT_ENOMEM : JT_ECUDA;
+    if (cufftCreate(&h) != CUFFT_SUCCESS) return JT_ECUDA;
+    // the work area is the batch's shared one (set once all plans exist)
+    cufftSetAutoAllocation(h, 0);
+    size_t ws = 0;
+    cufftResult e = r2c ? cufftMakePlanMany(h, 3, dims, nullptr, 1, (int)G, nullptr, 1, (int)Gc, CUFFT_R2C,
+                                            batch, &ws)
+                        : cufftMakePlanMany(h, 3, dims, nullptr, 1, (int)Gc, nullptr, 1, (int)G, CUFFT_C2R,
+                                            batch, &ws);
+    if (e != CUFFT_SUCCESS) {
+        cufftDestroy(h);
+        cudaGetLastError();
+        return e == CUFFT_ALLOC_FAILED ? JT_ENOMEM : JT_ECUDA;
+    }
     cufftSetStream(h, B->st);
+    B->fft_need = std::max(B->fft_need, ws);
+    B->fft_dirty = true;
     pl[batch] = h;
     return JT_OK;
 }
@@ -360,6 +379,18 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
     JT_TRY(B->tickets.ensure(4, &grew));
     for (int k = 0; k < nb; k++) P.by_M[B->boxes[ids[k]]->M].push_back(k);
     for (auto& kv : P.by_M) JT_TRY(bucket_ensure(B, B->buckets[kv.first], kv.first, (int)kv.second.size()));
+    if (B->fft_dirty || B->fftws.cap < B->fft_need) {
+        bool ws_grew = false;
+        JT_TRY(B->fftws.ensure(B->fft_need, &ws_grew));
+        if (ws_grew) B->gen++;
+        for (auto& kv : B->buckets) {
+            for (auto& q : kv.second.r2c)
+                if (cufftSetWorkArea(q.second, B->fftws.p) != CUFFT_SUCCESS) return JT_ECUDA;
+            for (auto& q : kv.second.c2r)
+                if (cufftSetWorkArea(q.second, B->fftws.p) != CUFFT_SUCCESS) return JT_ECUDA;
+        }
+        B->fft_dirty = false;
+    }
     std::vector<int> slot(nb);
     for (auto& kv : P.by_M)
         for (size_t q = 0; q < kv.second.size(); q++) slot[kv.second[q]] = (int)q;
@@ -841,6 +872,7 @@ void jt_batch_destroy(jt_batch* B)
     drop_graphs(B);
     B->gdesc.release();
     for (auto& kv : B->buckets) kv.second.release();
+    B->fftws.release();
     if (B->hdesc) cudaFreeHost(B->hdesc);
     if (B->d_err) cudaFree(B->d_err);
     if (B->d_stats) cudaFree(B->d_stats);
@@ -1048,7 +1080,7 @@ int jt_batch_memory(jt_batch* B, size_t* persistent, size_t* scratch)
     s += B->child.bytes() + B->range.bytes() + B->parent.bytes() + B->flag.bytes() + B->com.bytes() +
          B->bmin.bytes() + B->bmax.bytes() + B->quad0.bytes() + B->quad1.bytes() + B->m30.bytes() +
          B->vals.bytes() + B->vals_alt.bytes() + B->keys_alt.bytes() + B->hist.bytes() + B->status.bytes() +
-         B->tickets.bytes() + B->desc.bytes();
+         B->tickets.bytes() + B->desc.bytes() + B->fftws.bytes() + B->gdesc.bytes();
     for (auto& kv : B->buckets) s += (size_t)kv.second.cap * grid_bytes(kv.first, B->ngrid);
     if (persistent) *persistent = p;
     if (scratch) *scratch = s;
@@ -1085,12 +1117,16 @@ int jt_batch_trim(jt_batch* B)
 {
     if (!B) return JT_EINVAL;
     if (cudaStreamSynchronize(B->st) != cudaSuccess) return JT_ECUDA;
+    drop_graphs(B);
     B->child.release(); B->range.release(); B->parent.release(); B->flag.release();
     B->com.release(); B->bmin.release(); B->bmax.release(); B->quad0.release(); B->quad1.release();
     B->m30.release(); B->vals.release(); B->vals_alt.release(); B->keys_alt.release();
     B->hist.release(); B->status.release(); B->tickets.release();
     for (auto& kv : B->buckets) kv.second.release();
     B->buckets.clear();
+    B->fftws.release();
+    B->fft_need = 0;
+    B->fft_dirty = false;
     B->gen++;
     return JT_OK;
 }

@@ -116,9 +116,15 @@ int evict(jt_server* S, Job& j, bool final)
     return JT_OK;
 }
 
+// Budget test for admitting j: persistent state of every resident job and j,
+// plus their per-pass scratch with the pools' 1/16 growth headroom, plus the
+// batch's shared cuFFT work area (at most 2^27 complex elements, 1 GiB).
+constexpr size_t kFftWorkAllowance = (size_t)1 << 30;
+
 bool fits(jt_server* S, const Job& j)
 {
-    return S->resident_persistent + j.persistent + S->resident_scratch + j.scratch <= S->budget;
+    const size_t scratch = S->resident_scratch + j.scratch;
+    return S->resident_persistent + j.persistent + scratch + scratch / 16 + kFftWorkAllowance <= S->budget;
 }
 
 int admit_waiting(jt_server* S)
@@ -156,6 +162,11 @@ int admit_waiting(jt_server* S)
             if (r != JT_OK) return r;
         }
         int r = admit(S, j);
+        if (r == JT_ENOMEM) {
+            // scratch pools held for an earlier mix: release them and retry
+            r = jt_batch_trim(S->B);
+            if (r == JT_OK) r = admit(S, j);
+        }
         if (r == JT_ENOMEM) break;     // the device disagrees with the estimate: retry later
         if (r != JT_OK) return r;
     }
@@ -179,12 +190,23 @@ int step_once(jt_server* S, int* served)
     if (ids.empty()) return JT_OK;
     const double a = now_s();
     int r = jt_batch_step(S->B, ids.data(), (int)ids.size(), args.data(), 1);
+    if (r == JT_ENOMEM) {
+        // the pass could not grow its scratch (pools sized for an earlier
+        // mix of jobs, fragmentation): release every pool and retry once;
+        // no kernel ran before the allocation failed
+        r = jt_batch_trim(S->B);
+        if (r == JT_OK) r = jt_batch_step(S->B, ids.data(), (int)ids.size(), args.data(), 1);
+    }
     if (r != JT_OK) return r;
     const double done = now_s();
     S->busy_s += done - a;
     S->steps++;
     S->max_resident = std::max(S->max_resident, (int)ids.size());
-    S->peak_device = std::max(S->peak_device, device_bytes(S));
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess)
+        S->peak_device = std::max(S->peak_device, total_b - free_b);   // whole device, context included
+    else
+        S->peak_device = std::max(S->peak_device, device_bytes(S));
     for (int k : jix) {
         Job& j = S->jobs[k];
         S->lat.push_back(done - S->t0 - j.pending.front());
@@ -259,7 +281,8 @@ int jt_server_add_job(jt_server* S, const jt_config* cfg, const float* pos_p, co
     j.args = *args;
     int r = jt_batch_estimate(cfg, n_p, n_m, &j.persistent, &j.scratch);
     if (r != JT_OK) return r;
-    if (j.persistent + j.scratch > S->budget) return JT_EBUSY;   // can never fit
+    if (j.persistent + j.scratch + j.scratch / 16 + kFftWorkAllowance > S->budget)
+        return JT_EBUSY;   // can never fit
     const size_t floats = 6 * (n_p + n_m);
     if (cudaMallocHost((void**)&j.host, sizeof(float) * floats) != cudaSuccess) return JT_ENOMEM;
     float* h = j.host;
