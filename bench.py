@@ -43,6 +43,7 @@ UNIT = "particle-steps/s"
 # of every candidate is overhead and is not counted as useful work.
 FLOPS_PAIR = 40.0
 FLOPS_NODE = 100.0
+WALK_DRAM_BYTES_PER_PARTICLE = 615.0
 
 
 def workload(n_side=224, L=250.0, M=512):
@@ -420,15 +421,10 @@ def run_ours(args, ws, rank, local):
         hbm_src = "measured"
     except Exception:
         hbm_src = "fallback"
-    walk_traffic = None
-    try:
-        prof = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
-        walk_traffic = prof.get("walk_bytes_per_particle", None)
-        if walk_traffic is not None:
-            walk_traffic = walk_traffic * 2 * n
-    except Exception:
-        pass
-
+    # DRAM bytes of one walk launch per particle, from ncu on the 2x112^3 case
+    # (profiles/k_walk_acc_2x112.md: 1.728 GB for 2,809,856 particles); the
+    # walk's traffic grows with N (particles, trees and PM grids scale alike)
+    walk_traffic = WALK_DRAM_BYTES_PER_PARTICLE * 2 * n if args.grid * 224 == 512 * args.n_side else None
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         npart, tcpu, cores = cpu_treepm_step(args.cpu_sample_div)
@@ -443,11 +439,15 @@ def run_ours(args, ws, rank, local):
     if rank == 0 and ws == 1 and args.ensemble_boxes > 0:
         ensemble = run_ensemble(J, ics, args.ensemble_boxes, args.ensemble_steps, 3, H, w["dt"])
         if args.serve_jobs > 0:
-            serving = [run_serving(J, ics, args.serve_jobs, args.serve_big, args.serve_steps, float(r),
-                                   ensemble["value"], H, w["dt"])
-                       for r in args.serve_rates.split(",")]
-            for sv in serving:
-                sv["vs_plain_ensemble"] = sv["value"] / ensemble["plain_value"]
+            serving = []
+            for r in args.serve_rates.split(","):
+                try:
+                    sv = run_serving(J, ics, args.serve_jobs, args.serve_big, args.serve_steps, float(r),
+                                     ensemble["value"], H, w["dt"])
+                    sv["vs_plain_ensemble"] = sv["value"] / ensemble["plain_value"]
+                except J.JanusError as e:
+                    sv = {"rate_vs_capacity": float(r), "error": str(e)}
+                serving.append(sv)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K,
