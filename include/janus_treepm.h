@@ -275,6 +275,10 @@ int  jt_server_add_job(jt_server* s, const jt_config* cfg,
                        const float* pos_p, const float* vel_p, size_t n_p,
                        const float* pos_m, const float* vel_m, size_t n_m,
                        int steps_total, const jt_step_args* args, int* job_id);
+/* Budget bytes a job needs when it is the only one resident: persistent
+ * state, per-pass scratch with the pools' growth headroom and the cuFFT work
+ * area (no device work). */
+int  jt_server_job_need(const jt_config* cfg, size_t n_p, size_t n_m, size_t* bytes);
 /* One step request for a job at t_arrival seconds on the server clock
  * (negative = now). */
 int  jt_server_request(jt_server* s, int job, double t_arrival);

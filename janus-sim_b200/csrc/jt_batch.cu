@@ -42,12 +42,32 @@ namespace {
         if ((x) != CUFFT_SUCCESS) return JT_ECUDA; \
     } while (0)
 
+// Device memory of a batch comes from its own stream-ordered pool
+// (cudaMallocFromPoolAsync / cudaFreeAsync on the batch's stream), which
+// keeps freed blocks for reuse: admitting and evicting boxes, growing pools
+// and trimming them never synchronise the device.  Every entry point that
+// may allocate or free sets the batch as the calling thread's allocation
+// context (AllocScope); a batch is used by one host thread at a time.
+struct AllocCtx {
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t st = nullptr;
+};
+thread_local const AllocCtx* t_alloc = nullptr;
+
+struct AllocScope {
+    const AllocCtx* prev;
+    explicit AllocScope(const AllocCtx* c) : prev(t_alloc) { t_alloc = c; }
+    ~AllocScope() { t_alloc = prev; }
+};
+
 template <class T>
 int dalloc(T** p, size_t count)
 {
     *p = nullptr;
+    if (!t_alloc) return JT_EINVAL;
     if (count == 0) count = 1;
-    if (cudaMalloc((void**)p, sizeof(T) * count) == cudaSuccess) return JT_OK;
+    if (cudaMallocFromPoolAsync((void**)p, sizeof(T) * count, t_alloc->pool, t_alloc->st) == cudaSuccess)
+        return JT_OK;
     *p = nullptr;
     cudaGetLastError();   // an allocation failure is not sticky: keep it out of later checks
     return JT_ENOMEM;
@@ -55,7 +75,7 @@ int dalloc(T** p, size_t count)
 template <class T>
 void dfree(T*& p)
 {
-    if (p) cudaFree((void*)p);
+    if (p && t_alloc) cudaFreeAsync((void*)p, t_alloc->st);
     p = nullptr;
 }
 
@@ -149,6 +169,8 @@ float elapsed(cudaEvent_t a, cudaEvent_t b)
 struct jt_batch {
     int device = 0;
     cudaStream_t st = nullptr;
+    AllocCtx actx;                      // its memory pool and stream
+    Pool<float> stage;                  // host <-> device staging of AoS arrays
     std::vector<jt_box_state*> boxes;
     int order = 0, ngrid = 0, k_min = -1;   // shared by every box of the batch
     Pool<int2> child, range;
@@ -660,12 +682,11 @@ int read_out(jt_batch* B, const float4* src, const int* id, int64_t n, float* ds
         jt_launch_aos_out(src, id, nullptr, n, dst, B->st);
         return JT_OK;
     }
-    float* stage = nullptr;
-    if (cudaMalloc(&stage, sizeof(float) * 3 * n) != cudaSuccess) return JT_ENOMEM;
-    jt_launch_aos_out(src, id, nullptr, n, stage, B->st);
-    cudaError_t e = cudaMemcpyAsync(dst, stage, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, B->st);
+    bool grew = false;
+    JT_TRY(B->stage.ensure(3 * (size_t)n, &grew));
+    jt_launch_aos_out(src, id, nullptr, n, B->stage.p, B->st);
+    cudaError_t e = cudaMemcpyAsync(dst, B->stage.p, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, B->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(B->st);
-    cudaFree(stage);
     return e == cudaSuccess ? JT_OK : JT_ECUDA;
 }
 
@@ -768,6 +789,7 @@ int capture_graphs(jt_batch* B, const std::vector<int>& v, const jt_box_step* st
 int jtb_add_empty(jt_batch* B, const jt_config* cfg, int64_t n_p, int64_t n_m, int* box_id)
 {
     if (!B || !box_id || n_p < 0 || n_m < 0 || n_p + n_m == 0) return JT_EINVAL;
+    AllocScope scope(&B->actx);
     if (n_p >= (int64_t)1 << 30 || n_m >= (int64_t)1 << 30) return JT_EINVAL;
     JT_TRY(validate_box_config(cfg));
     const int order = box_order(*cfg), ngrid = box_ngrid(*cfg);
@@ -817,6 +839,7 @@ cudaStream_t jtb_stream(jt_batch* B) { return B ? B->st : nullptr; }
 int jtb_force_pass(jt_batch* B, const int* ids, int n_ids, int parts, float kick_frac, const jt_box_step* steps)
 {
     if (!B || parts < 1 || parts > 3) return JT_EINVAL;
+    AllocScope scope(&B->actx);
     std::vector<int> v;
     JT_TRY(valid_ids(B, ids, n_ids, v));
     JT_TRY(build_plan(B, v, steps, B->plan));
@@ -846,6 +869,19 @@ int jt_batch_create(jt_batch** out)
         delete B;
         return JT_ECUDA;
     }
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = B->device;
+    if (cudaMemPoolCreate(&B->actx.pool, &props) != cudaSuccess) {
+        cudaStreamDestroy(B->st);
+        delete B;
+        return JT_ECUDA;
+    }
+    // keep freed blocks for reuse (jt_batch_trim returns them to the device)
+    uint64_t keep = ~(uint64_t)0;
+    cudaMemPoolSetAttribute(B->actx.pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    B->actx.st = B->st;
     for (auto& e : B->ev) cudaEventCreate(&e);
     cudaEventCreateWithFlags(&B->desc_done, cudaEventDisableTiming);
     if (cudaMalloc(&B->d_err, sizeof(unsigned)) != cudaSuccess ||
@@ -862,6 +898,7 @@ int jt_batch_create(jt_batch** out)
 void jt_batch_destroy(jt_batch* B)
 {
     if (!B) return;
+    AllocScope scope(&B->actx);
     if (B->st) cudaStreamSynchronize(B->st);
     for (auto* b : B->boxes)
         if (b) { box_release(b); delete b; }
@@ -873,12 +910,15 @@ void jt_batch_destroy(jt_batch* B)
     B->gdesc.release();
     for (auto& kv : B->buckets) kv.second.release();
     B->fftws.release();
+    B->stage.release();
     if (B->hdesc) cudaFreeHost(B->hdesc);
     if (B->d_err) cudaFree(B->d_err);
     if (B->d_stats) cudaFree(B->d_stats);
     for (auto& e : B->ev)
         if (e) cudaEventDestroy(e);
     if (B->desc_done) cudaEventDestroy(B->desc_done);
+    if (B->st) cudaStreamSynchronize(B->st);
+    if (B->actx.pool) cudaMemPoolDestroy(B->actx.pool);
     if (B->st) cudaStreamDestroy(B->st);
     delete B;
 }
@@ -887,6 +927,7 @@ int jt_batch_add(jt_batch* B, const jt_config* cfg, const float* pos_p, const fl
                  const float* pos_m, const float* vel_m, size_t n_m, int mem, int* box_id)
 {
     if (!B || !cfg || !box_id || (mem != JT_MEM_HOST && mem != JT_MEM_DEVICE)) return JT_EINVAL;
+    AllocScope scope(&B->actx);
     if ((n_p && !pos_p) || (n_m && !pos_m)) return JT_EINVAL;
     if (n_p >= (size_t)1 << 30 || n_m >= (size_t)1 << 30) return JT_EINVAL;
     int id = -1;
@@ -896,8 +937,11 @@ int jt_batch_add(jt_batch* B, const jt_config* cfg, const float* pos_p, const fl
     const float* vv[2] = {vel_p, vel_m};
     int r = JT_OK;
     float* stage = nullptr;
-    if (mem == JT_MEM_HOST && cudaMalloc(&stage, sizeof(float) * 3 * std::max(n_p, n_m)) != cudaSuccess)
-        r = JT_ENOMEM;
+    if (mem == JT_MEM_HOST) {
+        bool grew = false;
+        r = B->stage.ensure(3 * std::max(n_p, n_m), &grew);
+        stage = B->stage.p;
+    }
     for (int s = 0; s < 2 && r == JT_OK; s++) {
         const int64_t n = b->n[s];
         if (n == 0) continue;
@@ -922,7 +966,6 @@ int jt_batch_add(jt_batch* B, const jt_config* cfg, const float* pos_p, const fl
         }
         if (cudaStreamSynchronize(B->st) != cudaSuccess) r = JT_ECUDA;
     }
-    if (stage) cudaFree(stage);
     if (r == JT_OK && cudaGetLastError() != cudaSuccess) r = JT_ECUDA;
     if (r != JT_OK) {
         jt_batch_remove(B, id);
@@ -935,6 +978,7 @@ int jt_batch_add(jt_batch* B, const jt_config* cfg, const float* pos_p, const fl
 int jt_batch_remove(jt_batch* B, int box_id)
 {
     if (!box_id_ok(B, box_id)) return JT_EINVAL;
+    AllocScope scope(&B->actx);
     cudaStreamSynchronize(B->st);
     box_release(B->boxes[box_id]);
     B->gen++;
@@ -946,6 +990,7 @@ int jt_batch_remove(jt_batch* B, int box_id)
 int jt_batch_forces(jt_batch* B, const int* ids, int n_ids, int part)
 {
     if (!B || part < 1 || part > 3) return JT_EINVAL;
+    AllocScope scope(&B->actx);
     B->tm = jt_timings{};
     cudaEvent_t t0, t1;
     cudaEventCreate(&t0);
@@ -964,6 +1009,7 @@ int jt_batch_forces(jt_batch* B, const int* ids, int n_ids, int part)
 int jt_batch_step(jt_batch* B, const int* ids, int n_ids, const jt_step_args* args, int nsteps)
 {
     if (!B || nsteps < 0 || !args) return JT_EINVAL;
+    AllocScope scope(&B->actx);
     std::vector<int> v;
     JT_TRY(valid_ids(B, ids, n_ids, v));
     std::vector<jt_box_step> steps(v.size());
@@ -1041,6 +1087,7 @@ int jt_batch_step(jt_batch* B, const int* ids, int n_ids, const jt_step_args* ar
 int jt_batch_get_accel(jt_batch* B, int box_id, float* acc_p, float* acc_m, int mem)
 {
     if (!box_id_ok(B, box_id) || (mem != JT_MEM_HOST && mem != JT_MEM_DEVICE)) return JT_EINVAL;
+    AllocScope scope(&B->actx);
     jt_box_state* b = B->boxes[box_id];
     if (!b->acc_valid) return JT_ESTATE;
     JT_TRY(read_out(B, b->acc[0], b->id[0], b->n[0], acc_p, mem));
@@ -1052,6 +1099,7 @@ int jt_batch_get_accel(jt_batch* B, int box_id, float* acc_p, float* acc_m, int 
 int jt_batch_get_state(jt_batch* B, int box_id, float* pos_p, float* vel_p, float* pos_m, float* vel_m, int mem)
 {
     if (!box_id_ok(B, box_id) || (mem != JT_MEM_HOST && mem != JT_MEM_DEVICE)) return JT_EINVAL;
+    AllocScope scope(&B->actx);
     jt_box_state* b = B->boxes[box_id];
     JT_TRY(read_out(B, b->pos[0], b->id[0], b->n[0], pos_p, mem));
     JT_TRY(read_out(B, b->vel[0], b->id[0], b->n[0], vel_p, mem));
@@ -1080,7 +1128,7 @@ int jt_batch_memory(jt_batch* B, size_t* persistent, size_t* scratch)
     s += B->child.bytes() + B->range.bytes() + B->parent.bytes() + B->flag.bytes() + B->com.bytes() +
          B->bmin.bytes() + B->bmax.bytes() + B->quad0.bytes() + B->quad1.bytes() + B->m30.bytes() +
          B->vals.bytes() + B->vals_alt.bytes() + B->keys_alt.bytes() + B->hist.bytes() + B->status.bytes() +
-         B->tickets.bytes() + B->desc.bytes() + B->fftws.bytes() + B->gdesc.bytes();
+         B->tickets.bytes() + B->desc.bytes() + B->fftws.bytes() + B->gdesc.bytes() + B->stage.bytes();
     for (auto& kv : B->buckets) s += (size_t)kv.second.cap * grid_bytes(kv.first, B->ngrid);
     if (persistent) *persistent = p;
     if (scratch) *scratch = s;
@@ -1116,6 +1164,7 @@ int jt_batch_set_graphs(jt_batch* B, int on)
 int jt_batch_trim(jt_batch* B)
 {
     if (!B) return JT_EINVAL;
+    AllocScope scope(&B->actx);
     if (cudaStreamSynchronize(B->st) != cudaSuccess) return JT_ECUDA;
     drop_graphs(B);
     B->child.release(); B->range.release(); B->parent.release(); B->flag.release();
@@ -1127,7 +1176,11 @@ int jt_batch_trim(jt_batch* B)
     B->fftws.release();
     B->fft_need = 0;
     B->fft_dirty = false;
+    B->stage.release();
     B->gen++;
+    // hand the freed blocks back to the device
+    if (cudaStreamSynchronize(B->st) != cudaSuccess) return JT_ECUDA;
+    cudaMemPoolTrimTo(B->actx.pool, 0);
     return JT_OK;
 }
 

@@ -249,6 +249,7 @@ struct jt_walk_params {
     float rc2, rc;
     float eps2;
     float c;            // 1 / (2 r_s)
+    float c2s;          // c^2 scaled to the walk's S table index (y / dy)
     float mass[2];      // per-species particle mass (G folded in)
     int M;
     float h_inv;        // M / L

@@ -46,6 +46,7 @@ struct Job {
     int state = kQueued;
     int box = -1;
     size_t persistent = 0, scratch = 0;
+    size_t fft_ws = 0;             // cuFFT work area its grids may need
     std::deque<double> pending;    // arrival times of outstanding step requests
     double last_served = -1.0;     // server clock of the last step it took
 };
@@ -116,15 +117,28 @@ int evict(jt_server* S, Job& j, bool final)
     return JT_OK;
 }
 
-// Budget test for admitting j: persistent state of every resident job and j,
-// plus their per-pass scratch with the pools' 1/16 growth headroom, plus the
-// batch's shared cuFFT work area (at most 2^27 complex elements, 1 GiB).
-constexpr size_t kFftWorkAllowance = (size_t)1 << 30;
+// cuFFT work area a job's transforms may need: one execution covers at most
+// 2^27 real elements (jt_batch.cu), so at most 2^27 complex elements.
+size_t fft_ws_of(const jt_config& c)
+{
+    const size_t G = (size_t)c.pm_grid * c.pm_grid * c.pm_grid;
+    return 8 * std::min((size_t)6 * G, (size_t)1 << 27);
+}
+
+// Device bytes of a set of jobs: persistent state, per-pass scratch with the
+// pools' 1/16 growth headroom, and the batch's shared cuFFT work area (the
+// largest any of them needs).
+size_t need_of(size_t persistent, size_t scratch, size_t fft_ws)
+{
+    return persistent + scratch + scratch / 16 + fft_ws;
+}
 
 bool fits(jt_server* S, const Job& j)
 {
-    const size_t scratch = S->resident_scratch + j.scratch;
-    return S->resident_persistent + j.persistent + scratch + scratch / 16 + kFftWorkAllowance <= S->budget;
+    size_t ws = j.fft_ws;
+    for (const Job& q : S->jobs)
+        if (q.state == kResident) ws = std::max(ws, q.fft_ws);
+    return need_of(S->resident_persistent + j.persistent, S->resident_scratch + j.scratch, ws) <= S->budget;
 }
 
 int admit_waiting(jt_server* S)
@@ -281,8 +295,8 @@ int jt_server_add_job(jt_server* S, const jt_config* cfg, const float* pos_p, co
     j.args = *args;
     int r = jt_batch_estimate(cfg, n_p, n_m, &j.persistent, &j.scratch);
     if (r != JT_OK) return r;
-    if (j.persistent + j.scratch + j.scratch / 16 + kFftWorkAllowance > S->budget)
-        return JT_EBUSY;   // can never fit
+    j.fft_ws = fft_ws_of(*cfg);
+    if (need_of(j.persistent, j.scratch, j.fft_ws) > S->budget) return JT_EBUSY;   // can never fit
     const size_t floats = 6 * (n_p + n_m);
     if (cudaMallocHost((void**)&j.host, sizeof(float) * floats) != cudaSuccess) return JT_ENOMEM;
     float* h = j.host;
@@ -294,6 +308,16 @@ int jt_server_add_job(jt_server* S, const jt_config* cfg, const float* pos_p, co
     else std::memset(h + 6 * n_p + 3 * n_m, 0, sizeof(float) * 3 * n_m);
     S->jobs.push_back(j);
     *job_id = (int)S->jobs.size() - 1;
+    return JT_OK;
+}
+
+int jt_server_job_need(const jt_config* cfg, size_t n_p, size_t n_m, size_t* bytes)
+{
+    if (!cfg || !bytes) return JT_EINVAL;
+    size_t p = 0, s = 0;
+    int r = jt_batch_estimate(cfg, n_p, n_m, &p, &s);
+    if (r != JT_OK) return r;
+    *bytes = need_of(p, s, fft_ws_of(*cfg));
     return JT_OK;
 }
 

@@ -28,6 +28,9 @@
 // evaluated without contraction, in the reference's order.
 #include "jt_internal.cuh"
 
+#include <cmath>
+#include <vector>
+
 namespace {
 
 constexpr int kWarps = JT_WARPS_PER_BLOCK;
@@ -91,6 +94,20 @@ __device__ __forceinline__ float gap1(float d, float ext)
     float g = fabsf(d) - ext;
     return g > 0.0f ? g : 0.0f;
 }
+
+// Tabulated short-range factor for pair interactions (JT_WALK_STAB = 1):
+// S as a function of y = x^2 = (r^2 + eps^2) / (2 r_s)^2 on a uniform grid
+// of kStab points over [0, 16] (x <= 4; S(4) ~ 5e-7), each entry holding
+// (S(y_i), S(y_{i+1}) - S(y_i)) for linear interpolation.  It replaces the
+// exp and reciprocal of the closed form (two MUFU operations per pair) by
+// one L1-resident float2 load; interpolation error <= 3e-5 near y = 0 and
+// ~1e-6 elsewhere.  Filled once per device from the host's erfc and exp.
+#ifndef JT_WALK_STAB
+#define JT_WALK_STAB 1
+#endif
+constexpr int kStab = 4096;
+constexpr float kStabYMax = 16.0f;
+__device__ float2 g_stab[kStab];
 
 struct WalkArgs {
     const jt_seg_dev* segs;
@@ -166,8 +183,15 @@ __device__ __forceinline__ int eval_chunk(WalkWarpSmem& S, int cnt, int lane, fl
             hits++;
             const float rp2 = r2 + P.eps2;
             const float ri = rsqrtf(rp2);
-            const float x = rp2 * ri * P.c;
-            const float g = fac * jt_split_S(x) * ri * ri * ri;
+#if JT_WALK_STAB
+            const float t = fminf(rp2 * P.c2s, (float)kStab - 1.5f);   // y / dy
+            const int k = (int)t;
+            const float2 ab = __ldg(&g_stab[k]);
+            const float S = fmaf(ab.y, t - (float)k, ab.x);
+#else
+            const float S = jt_split_S(rp2 * ri * P.c);
+#endif
+            const float g = fac * S * ri * ri * ri;
             a.x += g * dx;
             a.y += g * dy;
             a.z += g * dz;
@@ -441,6 +465,7 @@ __global__ void __launch_bounds__(kWarps * 32, JT_WALK_MINBLOCKS) k_walk_acc(Wal
     jt_walk_params P;
     P.L = B.L; P.halfL = B.halfL; P.theta2 = B.theta2; P.rc2 = B.rc2; P.rc = sqrtf(B.rc2);
     P.eps2 = B.eps2; P.c = B.c; P.mass[0] = B.mass[0]; P.mass[1] = B.mass[1];
+    P.c2s = B.c * B.c * ((float)kStab / kStabYMax);
     P.M = B.M; P.h_inv = B.h_inv; P.order = ORDER; P.ngrid = NG; P.parts = A.parts;
     const int64_t ns = SG.n;
     const int64_t i = grp * 32 + lane;
@@ -765,11 +790,40 @@ __global__ void k_split_signed(const float* __restrict__ pos, const float* __res
 
 }  // namespace
 
+namespace {
+
+// Fill g_stab on the current device once (host double erfc/exp).
+int stab_ready()
+{
+#if JT_WALK_STAB
+    static bool done[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return JT_ECUDA;
+    if (done[dev]) return JT_OK;
+    std::vector<float2> tab(kStab);
+    const double dy = (double)kStabYMax / kStab;
+    auto S = [](double y) {
+        const double x = std::sqrt(y);
+        return std::erfc(x) + 1.1283791670955126 * x * std::exp(-y);
+    };
+    for (int i = 0; i < kStab; i++) {
+        const double a = S(i * dy), b = S((i + 1) * dy);
+        tab[i] = make_float2((float)a, (float)(b - a));
+    }
+    if (cudaMemcpyToSymbol(g_stab, tab.data(), sizeof(float2) * kStab) != cudaSuccess) return JT_ECUDA;
+    done[dev] = true;
+#endif
+    return JT_OK;
+}
+
+}  // namespace
+
 int jt_b_walk(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_gprefix, int nseg,
               int64_t ngroups, const jt_tree_dev& pool, int order, int ngrid, int parts,
               float kick_frac, unsigned long long* stats, unsigned* d_err, cudaStream_t st)
 {
     if (ngroups <= 0) return JT_OK;
+    if (int r = stab_ready()) return r;
     WalkArgs A;
     A.segs = d_segs;
     A.boxes = d_boxes;

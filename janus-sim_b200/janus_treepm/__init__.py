@@ -44,7 +44,7 @@ EXPORTED = [
     "jt_batch_memory", "jt_batch_estimate", "jt_batch_get_timings", "jt_morton_sort_static",
     "jt_batch_trim", "jt_batch_set_graphs", "jt_server_create", "jt_server_destroy",
     "jt_server_add_job", "jt_server_request", "jt_server_clock", "jt_server_poll", "jt_server_serve",
-    "jt_server_job_state", "jt_server_get_state", "jt_server_stats",
+    "jt_server_job_state", "jt_server_get_state", "jt_server_stats", "jt_server_job_need",
 ]
 JT_JOB_QUEUED, JT_JOB_RESIDENT, JT_JOB_DONE = 0, 1, 2
 JT_STATIC_SORT_MAX = 262144
@@ -156,6 +156,7 @@ def library():
     L.jt_server_job_state.argtypes = [H, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.jt_server_get_state.argtypes = [H, C.c_int, fp, fp, fp, fp]
     L.jt_server_stats.argtypes = [H, C.POINTER(jt_serve_stats)]
+    L.jt_server_job_need.argtypes = [C.POINTER(jt_config), C.c_size_t, C.c_size_t, C.POINTER(C.c_size_t)]
     for name in EXPORTED:
         if name not in ("jt_destroy", "jt_strerror", "jt_version", "jt_batch_destroy",
                         "jt_server_destroy", "jt_server_clock"):
@@ -492,6 +493,14 @@ class Server:
                                            C.byref(args), C.byref(jid)), "jt_server_add_job")
         self.jobs[jid.value] = (len(pos_p), len(pos_m))
         return jid.value
+
+    @staticmethod
+    def job_need(config: Config, n_p, n_m):
+        """Budget bytes one job needs alone (no device work)."""
+        cfg = config.resolved().to_c()
+        b = C.c_size_t()
+        _check(library().jt_server_job_need(C.byref(cfg), n_p, n_m, C.byref(b)), "jt_server_job_need")
+        return b.value
 
     def request(self, job, t_arrival=-1.0):
         _check(library().jt_server_request(self._s, job, float(t_arrival)), "jt_server_request")

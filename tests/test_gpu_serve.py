@@ -92,7 +92,7 @@ def test_each_job_same_alone_and_in_the_mix():
 
 def test_budget_forces_swaps_but_results_hold():
     steps = 2
-    need_of = lambda sp: sum(J.Batch.estimate(sp[0], len(sp[1][0]), len(sp[1][2])))
+    need_of = lambda sp: J.Server.job_need(sp[0], len(sp[1][0]), len(sp[1][2]))
     # job 0 is the smallest; the budget holds the largest job plus half of
     # job 0, so admitting the largest must swap out job 0 while it is idle
     seeds = sorted([201, 202, 203, 204], key=lambda sd: need_of(job_spec(sd)))
