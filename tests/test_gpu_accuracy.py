@@ -1,0 +1,75 @@
+"""Force accuracy on clustered data (the configs[2] shape), theta swept.
+
+configs[2] is 2x128^3 particles in L = 100 Mpc on a 256^3 grid: 80% in 512
+Plummer spheres (scale radii log-uniform 0.05-1 Mpc, species alternating by
+sphere) plus 20% uniform background.  Here the same density, cell size,
+r_s = 1.25 cells, r_cut = 4.5 r_s and softening in a box half the side:
+2x64^3 particles, L = 50 Mpc, PM 128^3.  On 8192 sampled targets:
+
+* short range (the tree walk, JT_PART_SHORT) against the FP64 direct sum of
+  the same truncated split kernel (oracle/ewald.c, part "short"), for
+  theta = 0.3, 0.5, 0.7: the Barnes-Hut + FP32 error;
+* long range (JT_PART_PM) against the FP64 restatement of the same PM scheme
+  (oracle/acc_pm.c, TSC with interlacing): the FP32 error of the PM path.
+
+Errors are |a - a_ref| / |a_total| per target, a_total = FP64 short + FP64
+PM.  Bars: p99 <= 1e-3 for the PM path and for the walk at theta <= 0.5;
+p99 <= 3e-3 at theta = 0.7.
+"""
+import json
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+pytestmark = pytest.mark.gpu
+
+L, M, NSIDE = 50.0, 128, 64
+BARS = {0.3: 1e-3, 0.5: 1e-3, 0.7: 3e-3}
+
+
+def _setup():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import janus_treepm as J
+    from janus_treepm import ics
+    n = NSIDE ** 3
+    pp, pm = ics.plummer_spheres(n, L, n_spheres=64, seed=7)
+    r_s = 1.25 * L / M
+    eps = (L / (2 * n) ** (1 / 3)) / 30
+    pos = np.concatenate([pp, pm]).astype(np.float64)
+    mass = np.concatenate([np.full(n, 1.0), np.full(n, 19.0)]) * 1e-3
+    sg = np.concatenate([np.ones(n, np.int8), -np.ones(n, np.int8)])
+    idx = np.random.default_rng(3).choice(2 * n, 8192, replace=False)
+    return O, J, pp, pm, pos, mass, sg, idx, r_s, eps, n
+
+
+def test_clustered_accuracy_theta_sweep():
+    O, J, pp, pm, pos, mass, sg, idx, r_s, eps, n = _setup()
+    r_cut = 4.5 * r_s
+    short_ref = O.ewald_forces(pos, mass, sg, L, r_s, eps, r_trunc=r_cut, idx=idx, part="short")
+    pm_ref = O.acc_pm_forces(pos, mass, sg, M, L, r_s, order=3, interlace=True)[idx]
+    tot = np.linalg.norm(short_ref + pm_ref, axis=1)
+    report = {}
+    for theta in (0.3, 0.5, 0.7):
+        s = J.Solver(J.Config(box_L=L, pm_grid=M, theta=theta, softening=eps, r_s=r_s, r_cut=r_cut,
+                              mu=19.0, G_mass_plus=1e-3, mode=J.JT_ACCURATE))
+        s.set_state(pp, None, pm, None)
+        sp, sm = s.accel_part(J.JT_PART_SHORT)
+        short = np.concatenate([sp, sm])[idx]
+        if theta == 0.5:
+            lp, lm = s.accel_part(J.JT_PART_PM)
+            lng = np.concatenate([lp, lm])[idx]
+            e = np.linalg.norm(lng - pm_ref, axis=1) / tot
+            report["pm_vs_fp64_pm"] = [float(x) for x in np.percentile(e, [50, 99])]
+        t = s.timings()
+        s.close()
+        e = np.linalg.norm(short - short_ref, axis=1) / tot
+        report[f"walk_theta_{theta}"] = [float(x) for x in np.percentile(e, [50, 99])] + \
+            [int(t["node_interactions"]), int(t["pair_interactions"])]
+    print("ACCURACY_CFG2", json.dumps(report))
+    assert report["pm_vs_fp64_pm"][1] <= 1e-3, report
+    for theta, bar in BARS.items():
+        assert report[f"walk_theta_{theta}"][1] <= bar, (theta, report)
