@@ -243,62 +243,108 @@ def run_ensemble(J, ics, n_boxes, steps, warmup, H, dt):
     }
 
 
-def run_serving(J, ics, n_small, n_big, steps, rate_frac, capacity_ps, H, dt, budget_gb=150.0,
-                seed=11):
-    """The serving workload: n_small jobs sized as the ensemble boxes plus
-    n_big jobs of 2x256^3 (L = 300 Mpc, PM 512^3), each wanting `steps` KDK
-    steps, admitted by an HBM budget.  Step requests arrive as one Poisson
-    stream at rate_frac x the capacity estimated from the batched ensemble's
-    particle-steps/s; request k of a job comes in round k (every job's k-th
-    request before any (k+1)-th), jobs in a random order per round.  The big
-    jobs share one Zel'dovich realisation, each moved by a random periodic
-    shift and axis permutation (generating eight 256^3 fields would take
-    minutes of host time)."""
+def serving_jobs(J, ics, n_small, n_big, H, dt, seed=11):
+    """The serving workload's jobs: n_small boxes sized as the ensemble's plus
+    n_big boxes of 2x256^3 (L = 300 Mpc, PM 512^3).  The big jobs share one
+    Zel'dovich realisation, each moved by a random periodic shift and axis
+    permutation (generating eight 256^3 fields would take minutes of host
+    time).  Returns [(config, state, particles)]."""
     rng = np.random.default_rng(seed)
-    small = ensemble_boxes(n_small, seed=seed)
-    S = J.Server(int(budget_gb * (1 << 30)))
-    parts = []
-    for bx in small:
-        st = ics.zeldovich_lattice(bx["n"], bx["L"], seed=bx["seed"])
-        S.add_job(box_config(J, bx), *st, steps=steps, dt=dt, hubble=H)
-        parts.append(2 * bx["n"] ** 3)
+    jobs = []
+    for bx in ensemble_boxes(n_small, seed=seed):
+        jobs.append((box_config(J, bx), ics.zeldovich_lattice(bx["n"], bx["L"], seed=bx["seed"]),
+                     2 * bx["n"] ** 3))
     if n_big:
-        big_base = ics.zeldovich_lattice(256, 300.0, seed=seed)
-        bigbx = dict(n=256, L=300.0, M=512, mu=19.0)
-        for b in range(n_big):
+        base = ics.zeldovich_lattice(256, 300.0, seed=seed)
+        cfg = box_config(J, dict(n=256, L=300.0, M=512, mu=19.0))
+        for _ in range(n_big):
             shift = rng.uniform(-150.0, 150.0, 3).astype(np.float32)
             perm = rng.permutation(3)
             st = []
-            for k, a in enumerate(big_base):
+            for k, a in enumerate(base):
                 a = a[:, perm]
                 if k % 2 == 0:
                     a = ((a + shift + 150.0) % 300.0 - 150.0).astype(np.float32)
                 st.append(np.ascontiguousarray(a))
-            S.add_job(box_config(J, bigbx), *st, steps=steps, dt=dt, hubble=H)
-            parts.append(2 * 256 ** 3)
-        del big_base
-    n_jobs = len(parts)
-    rate = rate_frac * capacity_ps / float(np.mean(parts))     # requests per second
-    order = np.concatenate([rng.permutation(n_jobs) for _ in range(steps)])
-    t = np.cumsum(rng.exponential(1.0 / rate, len(order)))
-    t -= t[0]
+            jobs.append((cfg, tuple(st), 2 * 256 ** 3))
+    return jobs
+
+
+def serve_once(J, jobs, steps, rate, H, dt, budget_gb, seed):
+    """One serving run: every job wants `steps` steps; requests arrive as one
+    Poisson stream of the given rate (requests/s; None = all at t = 0), request
+    k of a job in round k, jobs in a random order per round."""
+    rng = np.random.default_rng(seed)
+    S = J.Server(int(budget_gb * (1 << 30)))
+    for cfg, st, _ in jobs:
+        S.add_job(cfg, *st, steps=steps, dt=dt, hubble=H)
+    order = np.concatenate([rng.permutation(len(jobs)) for _ in range(steps)])
+    if rate is None:
+        t = np.zeros(len(order))
+    else:
+        t = np.cumsum(rng.exponential(1.0 / rate, len(order)))
+        t -= t[0]
     t0 = time.perf_counter()
     S.serve(t, order)
     wall = time.perf_counter() - t0
     st = S.stats()
     S.close()
+    return wall, st
+
+
+def run_serving(J, ics, n_small, n_big, steps, rates, H, dt, budget_gb=150.0):
+    """Serving loop: a saturated run (every request at t = 0) measures the
+    server's capacity in requests/s, then Poisson runs at the given fractions
+    of it report p50/p99 per-request latency and throughput.  The plain-path
+    estimate steps the same jobs one at a time: the small ones at the plain
+    ensemble rate measured above, a big one timed alone through a handle."""
+    import torch
+    jobs = serving_jobs(J, ics, n_small, n_big, H, dt)
+    parts = [p for _, _, p in jobs]
     total_ps = float(sum(parts) * steps)
-    return {
-        "workload": f"{n_small} ensemble-style jobs + {n_big} jobs of 2x256^3 (L=300, PM 512^3), "
-                    f"{steps} steps each, {budget_gb:g} GB HBM budget, Poisson arrivals",
-        "arrival_rate_per_s": rate, "rate_vs_capacity": rate_frac,
-        "value": total_ps / wall, "unit": UNIT, "makespan_s": wall,
-        "p50_latency_ms": 1e3 * st["p50_latency_s"], "p99_latency_ms": 1e3 * st["p99_latency_s"],
-        "max_latency_ms": 1e3 * st["max_latency_s"], "gpu_busy_frac": st["busy_s"] / wall,
-        "requests": int(st["requests_served"]), "batched_steps": int(st["batched_steps"]),
-        "max_jobs_per_step": int(st["max_jobs_per_step"]), "admission_waits": int(st["admission_waits"]),
-        "swapped_out": int(st["swapped_out"]), "peak_device_gb": st["peak_device_bytes"] / 1e9,
-    }
+    # plain path: jobs one at a time through a handle, each as a served job
+    # runs (load the state, take all its steps): a seeded sample of 16 small
+    # jobs and one big job, timed and scaled by particle-steps
+    def plain_time(sel):
+        t = 0.0
+        for cfg, st, _ in sel:
+            s = J.Solver(cfg)
+            s.set_state(*st)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            s.set_state(*st)
+            s.step(dt, H, 1.0, steps)
+            torch.cuda.synchronize()
+            t += time.perf_counter() - t0
+            s.close()
+        return t
+    small_jobs = [j for j in jobs if j[2] != 2 * 256 ** 3]
+    pick = np.random.default_rng(5).choice(len(small_jobs), min(16, len(small_jobs)), replace=False)
+    sample = [small_jobs[k] for k in pick]
+    t_small = plain_time(sample)
+    plain_s = t_small * sum(j[2] for j in small_jobs) / sum(j[2] for j in sample)
+    if n_big:
+        plain_s += n_big * plain_time([jobs[-1]])
+    out = {"workload": f"{n_small} ensemble-style jobs + {n_big} jobs of 2x256^3 (L=300, PM 512^3), "
+                       f"{steps} steps each, {budget_gb:g} GB HBM budget",
+           "particle_steps": total_ps, "plain_value_estimate": total_ps / plain_s, "runs": []}
+    wall, st = serve_once(J, jobs, steps, None, H, dt, budget_gb, seed=11)
+    cap = st["requests_served"] / wall
+    out["capacity_requests_per_s"] = cap
+    out["saturated_value"] = total_ps / wall
+    for frac in rates:
+        wall, st = serve_once(J, jobs, steps, frac * cap, H, dt, budget_gb, seed=12)
+        out["runs"].append({
+            "rate_vs_capacity": frac, "arrival_rate_per_s": frac * cap,
+            "value": total_ps / wall, "unit": UNIT, "makespan_s": wall,
+            "vs_plain": (total_ps / wall) / (total_ps / plain_s),
+            "p50_latency_ms": 1e3 * st["p50_latency_s"], "p99_latency_ms": 1e3 * st["p99_latency_s"],
+            "max_latency_ms": 1e3 * st["max_latency_s"], "gpu_busy_frac": st["busy_s"] / wall,
+            "requests": int(st["requests_served"]), "batched_steps": int(st["batched_steps"]),
+            "max_jobs_per_step": int(st["max_jobs_per_step"]),
+            "admission_waits": int(st["admission_waits"]), "swapped_out": int(st["swapped_out"]),
+            "peak_device_gb": st["peak_device_bytes"] / 1e9})
+    return out
 
 
 def run_reference(args, ws, rank):
@@ -439,15 +485,11 @@ def run_ours(args, ws, rank, local):
     if rank == 0 and ws == 1 and args.ensemble_boxes > 0:
         ensemble = run_ensemble(J, ics, args.ensemble_boxes, args.ensemble_steps, 3, H, w["dt"])
         if args.serve_jobs > 0:
-            serving = []
-            for r in args.serve_rates.split(","):
-                try:
-                    sv = run_serving(J, ics, args.serve_jobs, args.serve_big, args.serve_steps, float(r),
-                                     ensemble["value"], H, w["dt"])
-                    sv["vs_plain_ensemble"] = sv["value"] / ensemble["plain_value"]
-                except J.JanusError as e:
-                    sv = {"rate_vs_capacity": float(r), "error": str(e)}
-                serving.append(sv)
+            try:
+                serving = run_serving(J, ics, args.serve_jobs, args.serve_big, args.serve_steps,
+                                      [float(r) for r in args.serve_rates.split(",")], H, w["dt"])
+            except J.JanusError as e:
+                serving = {"error": str(e)}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K,
@@ -500,8 +542,8 @@ def main():
     ap.add_argument("--ensemble-steps", type=int, default=5)
     ap.add_argument("--serve-jobs", type=int, default=256)
     ap.add_argument("--serve-big", type=int, default=8)
-    ap.add_argument("--serve-steps", type=int, default=2)
-    ap.add_argument("--serve-rates", default="1.0")
+    ap.add_argument("--serve-steps", type=int, default=4)
+    ap.add_argument("--serve-rates", default="0.5,1.0")
     args = ap.parse_args()
     ws, rank, local = dist()
     if args.impl == "reference":

@@ -855,6 +855,33 @@ void jtb_reset_timings(jt_batch* B)
 
 int64_t jtb_phase(jt_batch* B, int i) { return B && i >= 0 && i < 4 ? B->phase[i] : 0; }
 
+int jtb_set_accel(jt_batch* B, int box_id, const float* acc_p, const float* acc_m, int mem)
+{
+    if (!box_id_ok(B, box_id) || (mem != JT_MEM_HOST && mem != JT_MEM_DEVICE)) return JT_EINVAL;
+    AllocScope scope(&B->actx);
+    jt_box_state* b = B->boxes[box_id];
+    const float* src[2] = {acc_p, acc_m};
+    for (int s = 0; s < 2; s++) {
+        const int64_t n = b->n[s];
+        if (n == 0) continue;
+        if (!src[s]) return JT_EINVAL;
+        // accelerations are stored in the state's internal order: map the
+        // caller's order through id (after an add, internal = caller order)
+        const float* d = src[s];
+        if (mem == JT_MEM_HOST) {
+            bool grew = false;
+            JT_TRY(B->stage.ensure(3 * (size_t)n, &grew));
+            JT_CU(cudaMemcpyAsync(B->stage.p, src[s], sizeof(float) * 3 * n, cudaMemcpyHostToDevice, B->st));
+            d = B->stage.p;
+        }
+        jt_launch_aos_in(d, n, b->acc[s], nullptr, B->st);
+        JT_CU(cudaStreamSynchronize(B->st));
+    }
+    JT_CU(cudaGetLastError());
+    b->acc_valid = true;
+    return JT_OK;
+}
+
 // ---------------------------------------------------------------- C ABI
 extern "C" {
 

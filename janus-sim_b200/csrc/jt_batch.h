@@ -40,3 +40,7 @@ int jtb_force_pass(jt_batch* B, const int* ids, int n_ids, int parts, float kick
 int jtb_finish(jt_batch* B);
 void jtb_reset_timings(jt_batch* B);
 int64_t jtb_phase(jt_batch* B, int i);
+// Set a box's accelerations (species AoS float3 in the caller's order, host
+// or device) and mark them valid for its current positions; used to restore
+// a box that was moved to host memory without recomputing its forces.
+int jtb_set_accel(jt_batch* B, int box_id, const float* acc_p, const float* acc_m, int mem);

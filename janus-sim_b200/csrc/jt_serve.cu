@@ -41,6 +41,8 @@ struct Job {
     jt_config cfg;
     size_t n_p = 0, n_m = 0;
     float* host = nullptr;         // pinned: pos_p, vel_p, pos_m, vel_m (3 floats each)
+    float* host_acc = nullptr;     // pinned: acc_p, acc_m of a swapped-out job
+    bool acc_saved = false;        // host_acc belongs to the state in host
     int steps_total = 0, steps_done = 0;
     jt_step_args args = {0.0, 0.0, 1.0};
     int state = kQueued;
@@ -89,6 +91,14 @@ int admit(jt_server* S, Job& j)
     int r = jt_batch_add(S->B, &j.cfg, h, h + 3 * np, np, h + 6 * np, h + 6 * np + 3 * nm, nm, JT_MEM_HOST,
                          &box);
     if (r != JT_OK) return r;
+    if (j.acc_saved) {
+        // a swapped-out job comes back with its forces: no extra force pass
+        r = jtb_set_accel(S->B, box, j.host_acc, j.host_acc + 3 * np, JT_MEM_HOST);
+        if (r != JT_OK) {
+            jt_batch_remove(S->B, box);
+            return r;
+        }
+    }
     j.box = box;
     j.state = kResident;
     S->resident_persistent += j.persistent;
@@ -106,6 +116,19 @@ int evict(jt_server* S, Job& j, bool final)
     const size_t np = j.n_p, nm = j.n_m;
     int r = jt_batch_get_state(S->B, j.box, h, h + 3 * np, h + 6 * np, h + 6 * np + 3 * nm, JT_MEM_HOST);
     if (r != JT_OK) return r;
+    j.acc_saved = false;
+    if (!final) {
+        if (!j.host_acc &&
+            cudaMallocHost((void**)&j.host_acc, sizeof(float) * 3 * (np + nm)) != cudaSuccess) {
+            j.host_acc = nullptr;
+            cudaGetLastError();
+        }
+        // keep the forces of the state being swapped out (none yet: it comes
+        // back with a force pass)
+        if (j.host_acc &&
+            jt_batch_get_accel(S->B, j.box, j.host_acc, j.host_acc + 3 * np, JT_MEM_HOST) == JT_OK)
+            j.acc_saved = true;
+    }
     r = jt_batch_remove(S->B, j.box);
     if (r != JT_OK) return r;
     j.box = -1;
@@ -274,8 +297,10 @@ void jt_server_destroy(jt_server* S)
 {
     if (!S) return;
     jt_batch_destroy(S->B);
-    for (Job& j : S->jobs)
+    for (Job& j : S->jobs) {
         if (j.host) cudaFreeHost(j.host);
+        if (j.host_acc) cudaFreeHost(j.host_acc);
+    }
     delete S;
 }
 
