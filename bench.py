@@ -296,8 +296,8 @@ def run_serving(J, ics, n_small, n_big, steps, rates, H, dt, budget_gb=150.0):
     """Serving loop: a saturated run (every request at t = 0) measures the
     server's capacity in requests/s, then Poisson runs at the given fractions
     of it report p50/p99 per-request latency and throughput.  The plain-path
-    estimate steps the same jobs one at a time: the small ones at the plain
-    ensemble rate measured above, a big one timed alone through a handle."""
+    estimate runs a seeded sample of the jobs one at a time through handles
+    (load the state, take every step) and scales it by particle-steps."""
     import torch
     jobs = serving_jobs(J, ics, n_small, n_big, H, dt)
     parts = [p for _, _, p in jobs]
