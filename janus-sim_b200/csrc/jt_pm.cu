@@ -239,18 +239,13 @@ k_b_deposit(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ 
         }
     }
     __syncthreads();
-    // flush one (grid, z, y) row per warp, lanes along x: the row index is
-    // decoded once per row, not per cell (S is a runtime value)
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-    for (int row = warp; row < NG * S * S; row += nwarps) {
-        const int g = row / (S * S), rz = row - g * S * S;
-        const int lz = rz / S, ly = rz - lz * S;
-        const float* trow = tile + (int64_t)row * S;
-        float* grow = rho + g * G + ((int64_t)((bz + lz) & mask) * M + ((by + ly) & mask)) * M;
-        for (int lx = lane; lx < S; lx += 32) {
-            const float v = trow[lx];
-            if (v != 0.0f) atomicAdd(grow + ((bx + lx) & mask), v);
-        }
+    for (int c = threadIdx.x; c < NG * S3; c += blockDim.x) {
+        float v = tile[c];
+        if (v == 0.0f) continue;
+        int g = c / S3, rem = c - g * S3;
+        int lz = rem / (S * S), ly = (rem / S) % S, lx = rem % S;
+        int64_t idx = ((int64_t)((bz + lz) & mask) * M + ((by + ly) & mask)) * M + ((bx + lx) & mask);
+        atomicAdd(rho + g * G + idx, v);
     }
 }
 
