@@ -517,6 +517,7 @@ def run_ours(args, ws, rank, local):
             "wall_ms_per_step": 1e3 * wall / K,
             "clocks": clk,
             "gpu_launches": int(launches),
+            "walk_autotune": J.walk_tuning(),
             "cpu_baseline": cpu,
             "ensemble": ensemble,
             "serving": serving,

@@ -177,6 +177,10 @@ const char* jt_strerror(int code);
  * register-only FMA kernel: the roofline denominator for the walk.  No
  * counterpart in the reference. */
 int  jt_fp32_peak(int iters, double* tflops);
+/* The walk's launch shapes picked by its autotuner so far (one entry per
+ * device and size class: register budget as blocks per SM, leaf-bucket
+ * size), as text.  No counterpart in the reference. */
+int  jt_walk_tuning(char* buf, size_t len);
 /* Library version string, e.g. "janus-treepm-b200 0.1 sm_100a". */
 const char* jt_version(void);
 

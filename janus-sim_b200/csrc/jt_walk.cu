@@ -28,8 +28,15 @@
 // evaluated without contraction, in the reference's order.
 #include "jt_internal.cuh"
 
+#include <cuda_fp16.h>
+
 #include <cmath>
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <string>
 #include <vector>
+#include <cstdio>
 
 namespace {
 
@@ -37,11 +44,7 @@ constexpr int kWarps = JT_WARPS_PER_BLOCK;
 #ifndef JT_WALK_STACK
 #define JT_WALK_STACK 384
 #endif
-#ifndef JT_WALK_BUCKET
-#define JT_WALK_BUCKET 32
-#endif
 constexpr int kStackCap = JT_WALK_STACK;   // per-warp traversal stack (node ids)
-constexpr int kBucket = JT_WALK_BUCKET;    // nodes with <= kBucket particles are streamed as ranges
 constexpr int kRangeCap = 64;     // queued ranges
 constexpr int kCandCap = 64;      // candidate particle buffer
 constexpr int kApproxCap = 64;    // queued multipole nodes
@@ -51,6 +54,9 @@ struct WalkWarpSmem {
     int2 rng[kRangeCap];          // (first sorted index, count)
     char4 rsh[kRangeCap];         // periodic shift of the range, in box lengths (-1, 0, 1)
     float4 cand[kCandCap];        // shifted candidate positions
+    // the same candidates relative to the group centre in fp16 (x, y, z
+    // arrays; pairs read as half2) for the two-at-a-time distance mask
+    __align__(16) __half hc[3][kCandCap];
     float4 acom[kApproxCap];      // shifted COM + mass
     float4 aq0[kApproxCap];       // Qxx Qyy Qzz Qxy
     float2 aq1[kApproxCap];       // Qxz Qyz
@@ -149,16 +155,49 @@ __device__ __forceinline__ unsigned chunk_mask(const float4* __restrict__ cand, 
     return m;
 }
 
+// Distance mask of a full chunk from the fp16 copies, two candidates per
+// instruction, against a cut inflated to cover fp16 rounding (rch2); the
+// evaluation loop re-tests every hit in FP32.  Candidates whose fp16
+// coordinate overflows become inf and fail the test, and they are far.
+#ifndef JT_WALK_HALF
+#define JT_WALK_HALF 1
+#endif
+__device__ __forceinline__ unsigned chunk_mask_h(const WalkWarpSmem& S, __half2 tx, __half2 ty,
+                                                 __half2 tz, __half2 rch2)
+{
+    const __half2* __restrict__ hx = reinterpret_cast<const __half2*>(S.hc[0]);
+    const __half2* __restrict__ hy = reinterpret_cast<const __half2*>(S.hc[1]);
+    const __half2* __restrict__ hz = reinterpret_cast<const __half2*>(S.hc[2]);
+    unsigned m = 0;
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        const __half2 dx = __hsub2(hx[k], tx), dy = __hsub2(hy[k], ty), dz = __hsub2(hz[k], tz);
+        const __half2 r2 = __hfma2(dz, dz, __hfma2(dy, dy, __hmul2(dx, dx)));
+        const unsigned mk = __hlt2_mask(r2, rch2);          // 0xFFFF per true half
+        m |= ((mk & 1u) | ((mk >> 15) & 2u)) << (2 * k);
+    }
+    return m;
+}
+
+struct HalfTarget {
+    __half2 tx, ty, tz, rch2;
+    bool on;                      // fp16 mask usable for this group
+};
+
 template <bool WRAP>
 __device__ __forceinline__ int eval_chunk(WalkWarpSmem& S, int cnt, int lane, float px, float py,
                                           float pz, bool valid, const jt_walk_params& P, float fac,
-                                          WalkCount& wc, Acc3& a)
+                                          WalkCount& wc, Acc3& a, const HalfTarget& H)
 {
     wc.chunks++;
     (void)lane;
     const float4* __restrict__ cand = S.cand;
-    unsigned m = cnt == 32 ? chunk_mask<WRAP, 32>(cand, 32, px, py, pz, P)
-                           : chunk_mask<WRAP, 0>(cand, cnt, px, py, pz, P);
+    unsigned m;
+    if (!WRAP && JT_WALK_HALF && cnt == 32 && H.on)
+        m = chunk_mask_h(S, H.tx, H.ty, H.tz, H.rch2);
+    else
+        m = cnt == 32 ? chunk_mask<WRAP, 32>(cand, 32, px, py, pz, P)
+                      : chunk_mask<WRAP, 0>(cand, cnt, px, py, pz, P);
     if (!valid) m = 0;
 #ifdef JT_WALK_COUNT
     {
@@ -179,7 +218,7 @@ __device__ __forceinline__ int eval_chunk(WalkWarpSmem& S, int cnt, int lane, fl
             dz = jt_wrap(dz, P.L, P.halfL);
         }
         const float r2 = dx * dx + dy * dy + dz * dz;
-        if (r2 > 0.0f) {   // not the target itself (or an exact duplicate)
+        if (r2 > 0.0f && r2 < P.rc2) {   // not the target itself; inside the cut
             hits++;
             const float rp2 = r2 + P.eps2;
             const float ri = rsqrtf(rp2);
@@ -252,7 +291,8 @@ __device__ __forceinline__ void drain_ranges(WalkWarpSmem& S, int nr, int& nc,
                                              const float4* __restrict__ tpos, int lane, float px,
                                              float py, float pz, bool valid, const jt_walk_params& P,
                                              float fac, Acc3& near, unsigned& pairs,
-                                             unsigned& cands, WalkCount& wc)
+                                             unsigned& cands, WalkCount& wc, float gcx, float gcy,
+                                             float gcz, const HalfTarget& H)
 {
     if (nr <= 0) return;
     wc.ranges += nr;
@@ -267,23 +307,37 @@ __device__ __forceinline__ void drain_ranges(WalkWarpSmem& S, int nr, int& nc,
             const int2 rn = S.rng[r + 1];
             nxt = lane < rn.y ? tpos[rn.x + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
         }
-        if (lane < rr.y) S.cand[nc + lane] = make_float4(cur.x + sh.x, cur.y + sh.y, cur.z + sh.z, 0.f);
+        if (lane < rr.y) {
+            const float4 c = make_float4(cur.x + sh.x, cur.y + sh.y, cur.z + sh.z, 0.f);
+            S.cand[nc + lane] = c;
+            if (!WRAP && JT_WALK_HALF) {
+                S.hc[0][nc + lane] = __float2half_rn(c.x - gcx);
+                S.hc[1][nc + lane] = __float2half_rn(c.y - gcy);
+                S.hc[2][nc + lane] = __float2half_rn(c.z - gcz);
+            }
+        }
         nc += rr.y;
         __syncwarp();
         if (nc >= 32) {
-            pairs += eval_chunk<WRAP>(S, 32, lane, px, py, pz, valid, P, fac, wc, near);
+            pairs += eval_chunk<WRAP>(S, 32, lane, px, py, pz, valid, P, fac, wc, near, H);
             cands += 32;
             __syncwarp();
             float4 t = S.cand[32 + lane];
+            __half h0 = S.hc[0][32 + lane], h1 = S.hc[1][32 + lane], h2 = S.hc[2][32 + lane];
             __syncwarp();
-            if (lane < nc - 32) S.cand[lane] = t;
+            if (lane < nc - 32) {
+                S.cand[lane] = t;
+                S.hc[0][lane] = h0;
+                S.hc[1][lane] = h1;
+                S.hc[2][lane] = h2;
+            }
             nc -= 32;
             __syncwarp();
         }
     }
 }
 
-template <int ORDER, int NG, bool WRAP>
+template <int ORDER, int NG, bool WRAP, int BKT>
 __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& B,
                                            const jt_walk_params& P, WalkWarpSmem& S, int s, int lane,
                                            const float4& p, bool valid, float gcx, float gcy,
@@ -293,6 +347,19 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& 
                                            WalkCount& wc)
 {
     const unsigned lt = (1u << lane) - 1u;
+    // fp16 distance mask: coordinates relative to the group centre; the cut
+    // is widened by the rounding of |coordinate| <= D (group half-diagonal
+    // + r_cut) on both sides and of the sum of squares
+    HalfTarget H;
+    {
+        const float D = sqrtf(ghx * ghx + ghy * ghy + ghz * ghz) + P.rc;
+        const float rl = (P.rc + 8.0f * 4.8828125e-4f * (D + P.rc)) * (1.0f + 8.0f * 4.8828125e-4f);
+        H.on = rl * rl < 3.0e4f;
+        H.tx = __float2half2_rn(p.x - gcx);
+        H.ty = __float2half2_rn(p.y - gcy);
+        H.tz = __float2half2_rn(p.z - gcz);
+        H.rch2 = __float2half2_rn(rl * rl);
+    }
     for (int t = 0; t < 2; t++) {
         const int tg = B.seg[t];
         if (tg < 0 || !(P.parts & 2)) continue;
@@ -364,7 +431,7 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& 
                         }
                     }
                     if (!accepted) {
-                        if (count <= kBucket) {
+                        if (count <= BKT) {
                             act = 2;
                             rg = make_int2(first, count);
                             // shift (in box lengths) that moves the node to the group's image
@@ -408,7 +475,7 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& 
             __syncwarp();
             if (nR >= 32) {
                 drain_ranges<WRAP>(S, 32, nc, tpos, lane, p.x, p.y, p.z, valid, P, fac_direct, near,
-                                   pairs, cands, wc);
+                                   pairs, cands, wc, gcx, gcy, gcz, H);
                 __syncwarp();
                 int2 r2 = S.rng[32 + lane];
                 char4 s2 = S.rsh[32 + lane];
@@ -433,10 +500,10 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& 
             }
         }
         drain_ranges<WRAP>(S, nR, nc, tpos, lane, p.x, p.y, p.z, valid, P, fac_direct, near, pairs,
-                           cands, wc);
+                           cands, wc, gcx, gcy, gcz, H);
         __syncwarp();
         if (nc > 0) {
-            pairs += eval_chunk<WRAP>(S, nc, lane, p.x, p.y, p.z, valid, P, fac_direct, wc, near);
+            pairs += eval_chunk<WRAP>(S, nc, lane, p.x, p.y, p.z, valid, P, fac_direct, wc, near, H);
             cands += nc;
         }
         if (nA > 0)
@@ -445,13 +512,13 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& 
     }
 }
 
-#ifndef JT_WALK_MINBLOCKS
-#define JT_WALK_MINBLOCKS 6
-#endif
-
-template <int ORDER, int NG>
-__global__ void __launch_bounds__(kWarps * 32, JT_WALK_MINBLOCKS) k_walk_acc(WalkArgs A)
+// MINB: resident blocks per SM the register budget is sized for (6 -> 80
+// registers); BKT: nodes with <= BKT particles are streamed as ranges
+// (<= 32: one lane per particle when a range is loaded)
+template <int ORDER, int NG, int MINB, int BKT>
+__global__ void __launch_bounds__(kWarps * 32, MINB) k_walk_acc(WalkArgs A)
 {
+    static_assert(BKT <= 32, "a range is loaded one particle per lane");
     __shared__ WalkWarpSmem smem_all[kWarps];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     WalkWarpSmem& S = smem_all[wib];
@@ -520,10 +587,10 @@ __global__ void __launch_bounds__(kWarps * 32, JT_WALK_MINBLOCKS) k_walk_acc(Wal
     // groups wider than L/8 take the minimum image per pair
     const bool wide = fmaxf(fmaxf(ghx, ghy), ghz) > 0.125f * P.L;
     if (wide)
-        walk_trees<ORDER, NG, true>(A, B, P, S, s, lane, p, valid, gcx, gcy, gcz, ghx, ghy, ghz, near,
+        walk_trees<ORDER, NG, true, BKT>(A, B, P, S, s, lane, p, valid, gcx, gcy, gcz, ghx, ghy, ghz, near,
                                     far, comp, pairs, nodes, cands, wc);
     else
-        walk_trees<ORDER, NG, false>(A, B, P, S, s, lane, p, valid, gcx, gcy, gcz, ghx, ghy, ghz, near,
+        walk_trees<ORDER, NG, false, BKT>(A, B, P, S, s, lane, p, valid, gcx, gcy, gcz, ghx, ghy, ghz, near,
                                      far, comp, pairs, nodes, cands, wc);
 
     if (valid) {
@@ -818,6 +885,106 @@ int stab_ready()
 
 }  // namespace
 
+namespace {
+
+// ---- walk autotuner --------------------------------------------------------
+// The default launch shape of the walk (80 registers, 6 blocks per SM,
+// 32-particle leaf buckets) is the best measured at 2x224^3; other densities,
+// clustering and box mixes can prefer another register budget or bucket.  For
+// the default PM scheme (TSC, interlaced) the first force-only pass of each
+// size class (device, log2 of the warp-group count) times every variant once
+// and keeps the fastest; JT_WALK_VARIANT=<k> pins variant k.  Passes that kick
+// (the walk then updates velocities) or run under stream capture use the
+// cached or the default variant.
+struct WalkVariant {
+    int minb, bkt;
+};
+constexpr WalkVariant kVariants[] = {{6, 32}, {5, 32}, {6, 24}};
+constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+
+std::mutex g_tune_mu;
+std::map<std::pair<int, int>, int> g_tuned;   // (device, log2 groups) -> variant
+
+void launch_variant(int v, unsigned g, const WalkArgs& A, cudaStream_t st)
+{
+    switch (v) {
+    case 1: k_walk_acc<3, 2, 5, 32><<<g, kWarps * 32, 0, st>>>(A); break;
+    case 2: k_walk_acc<3, 2, 6, 24><<<g, kWarps * 32, 0, st>>>(A); break;
+    default: k_walk_acc<3, 2, 6, 32><<<g, kWarps * 32, 0, st>>>(A); break;
+    }
+}
+
+int pick_variant(unsigned g, int64_t ngroups, const WalkArgs& A, cudaStream_t st)
+{
+    if (const char* e = std::getenv("JT_WALK_VARIANT")) {
+        const int v = std::atoi(e);
+        return v >= 0 && v < kNumVariants ? v : 0;
+    }
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int lg = 0;
+    while (((int64_t)1 << (lg + 1)) <= ngroups) lg++;
+    const std::pair<int, int> key(dev, lg);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tuned.find(key);
+        if (it != g_tuned.end()) return it->second;
+    }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (A.kick_frac != 0.0f || cudaStreamIsCapturing(st, &cs) != cudaSuccess ||
+        cs != cudaStreamCaptureStatusNone)
+        return 0;
+    // time each variant on this pass (force only: every run writes the same
+    // accelerations); statistics are left to the real launch
+    WalkArgs T = A;
+    T.stats = nullptr;
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess) return 0;
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return 0;
+    }
+    int best = 0;
+    float best_ms = 0.f;
+    for (int v = 0; v < kNumVariants; v++) {
+        cudaEventRecord(e0, st);
+        launch_variant(v, g, T, st);
+        cudaEventRecord(e1, st);
+        float ms = 0.f;
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+            best = 0;
+            break;
+        }
+        if (v == 0 || ms < best_ms) {
+            best = v;
+            best_ms = ms;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tuned[key] = best;
+    return best;
+}
+
+}  // namespace
+
+extern "C" int jt_walk_tuning(char* buf, size_t len)
+{
+    if (!buf || len == 0) return JT_EINVAL;
+    std::string out;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        for (const auto& kv : g_tuned) {
+            const WalkVariant& w = kVariants[kv.second];
+            out += "dev" + std::to_string(kv.first.first) + " groups~2^" + std::to_string(kv.first.second) +
+                   ": minblocks " + std::to_string(w.minb) + " bucket " + std::to_string(w.bkt) + "; ";
+        }
+    }
+    std::snprintf(buf, len, "%s", out.c_str());
+    return JT_OK;
+}
+
 int jt_b_walk(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_gprefix, int nseg,
               int64_t ngroups, const jt_tree_dev& pool, int order, int ngrid, int parts,
               float kick_frac, unsigned long long* stats, unsigned* d_err, cudaStream_t st)
@@ -835,10 +1002,10 @@ int jt_b_walk(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t
     A.stats = stats;
     A.err = d_err;
     unsigned g = (unsigned)((ngroups + kWarps - 1) / kWarps);
-    if (order == 3 && ngrid == 2) k_walk_acc<3, 2><<<g, kWarps * 32, 0, st>>>(A);
-    else if (order == 3 && ngrid == 1) k_walk_acc<3, 1><<<g, kWarps * 32, 0, st>>>(A);
-    else if (order == 2 && ngrid == 2) k_walk_acc<2, 2><<<g, kWarps * 32, 0, st>>>(A);
-    else if (order == 2 && ngrid == 1) k_walk_acc<2, 1><<<g, kWarps * 32, 0, st>>>(A);
+    if (order == 3 && ngrid == 2) launch_variant(pick_variant(g, ngroups, A, st), g, A, st);
+    else if (order == 3 && ngrid == 1) k_walk_acc<3, 1, 6, 32><<<g, kWarps * 32, 0, st>>>(A);
+    else if (order == 2 && ngrid == 2) k_walk_acc<2, 2, 6, 32><<<g, kWarps * 32, 0, st>>>(A);
+    else if (order == 2 && ngrid == 1) k_walk_acc<2, 1, 6, 32><<<g, kWarps * 32, 0, st>>>(A);
     else return JT_EINVAL;
     return cudaGetLastError() == cudaSuccess ? JT_OK : JT_ECUDA;
 }

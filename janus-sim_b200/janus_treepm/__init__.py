@@ -45,6 +45,7 @@ EXPORTED = [
     "jt_batch_trim", "jt_batch_set_graphs", "jt_server_create", "jt_server_destroy",
     "jt_server_add_job", "jt_server_request", "jt_server_clock", "jt_server_poll", "jt_server_serve",
     "jt_server_job_state", "jt_server_get_state", "jt_server_stats", "jt_server_job_need",
+    "jt_walk_tuning",
 ]
 JT_JOB_QUEUED, JT_JOB_RESIDENT, JT_JOB_DONE = 0, 1, 2
 JT_STATIC_SORT_MAX = 262144
@@ -141,6 +142,7 @@ def library():
     L.jt_batch_estimate.argtypes = [C.POINTER(jt_config), C.c_size_t, C.c_size_t, szp, szp]
     L.jt_batch_get_timings.argtypes = [H, C.POINTER(jt_timings)]
     L.jt_morton_sort_static.argtypes = [vp, C.c_size_t, C.c_double, vp, vp, vp]
+    L.jt_walk_tuning.argtypes = [C.c_char_p, C.c_size_t]
     L.jt_batch_trim.argtypes = [H]
     L.jt_batch_set_graphs.argtypes = [H, C.c_int]
     L.jt_server_create.argtypes = [C.c_size_t, C.POINTER(H)]
@@ -341,6 +343,13 @@ class Solver:
         t = jt_timings()
         _check(library().jt_get_timings(self._h, C.byref(t)), "jt_get_timings")
         return {k: getattr(t, k) for k, _ in jt_timings._fields_}
+
+
+def walk_tuning():
+    """The walk launch shapes the autotuner picked so far (text)."""
+    buf = C.create_string_buffer(4096)
+    _check(library().jt_walk_tuning(buf, 4096), "jt_walk_tuning")
+    return buf.value.decode()
 
 
 def morton_sort_static(pos_ptr, n, box_L, morton_ptr, perm_ptr, stream=None):
