@@ -58,6 +58,17 @@ def hubble_at(z):
     return expansion.state_at_redshift(z)[2]
 
 
+def max_over_ranks(value, ws, device):
+    """The largest value over all ranks (every rank's device time of the same
+    timed region; the job's time is the slowest rank's)."""
+    if ws <= 1:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -422,10 +433,7 @@ def run_ours(args, ws, rank, local):
     barrier()
     wall = time.perf_counter() - t_wall
     clk = clocks.stop()
-    if ws > 1:
-        t = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        dev_ms = float(t.item())
+    dev_ms = max_over_ranks(dev_ms, ws, "cuda")
     K = args.steps
     value = ws * 2 * n * K / (dev_ms * 1e-3)
 
@@ -444,10 +452,7 @@ def run_ours(args, ws, rank, local):
         a, b, c, d = s.get_state()
     barrier()
     e2e_t = time.perf_counter() - t0
-    if ws > 1:
-        t = torch.tensor([e2e_t], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_t = float(t.item())
+    e2e_t = max_over_ranks(e2e_t, ws, "cuda")
     e2e = ws * 2 * n * K / e2e_t
     bytes_state = 2 * n * 3 * 4 * 2     # positions + velocities, both species
 
