@@ -181,6 +181,12 @@ int  jt_fp32_peak(int iters, double* tflops);
  * device and size class: register budget as blocks per SM, leaf-bucket
  * size), as text.  No counterpart in the reference. */
 int  jt_walk_tuning(char* buf, size_t len);
+/* Failure-path self test: runs the sort's bounded look-back wait on a
+ * status word that nothing publishes, with `limit` polls (1..2^24).  Returns
+ * JT_ETIMEDOUT with *timed_out = 1 when the wait gave up and reported it (the
+ * expected outcome); the device context stays usable.  No counterpart in the
+ * reference. */
+int  jt_wait_probe(int limit, int* timed_out);
 /* Library version string, e.g. "janus-treepm-b200 0.1 sm_100a". */
 const char* jt_version(void);
 

@@ -119,6 +119,41 @@ __device__ __forceinline__ void st_relaxed(uint32_t* p, uint32_t v)
     asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// Decoupled look-back for digit t from tile p down: adds the aggregates of
+// earlier tiles until one publishes an inclusive prefix.  A status word that
+// stays empty for `limit` polls makes it give up: it sets JT_ERRBIT_LOOKBACK
+// (reported as JT_ETIMEDOUT) and returns what it has, so no wait is endless.
+__device__ __forceinline__ uint32_t lookback(const uint32_t* status, int64_t p, int t, unsigned* err,
+                                             int limit)
+{
+    uint32_t excl = 0;
+    int spins = 0;
+    for (;;) {
+        uint32_t wv = ld_relaxed(status + p * 256 + t);
+        uint32_t flag = wv & ~kValMask;
+        if (flag == 0u) {
+            if (++spins > limit) {
+                atomicOr(err, JT_ERRBIT_LOOKBACK);
+                break;
+            }
+            if (spins > 64) __nanosleep(32);
+            continue;
+        }
+        excl += wv & kValMask;
+        if (flag == kFlagInc || p == 0) break;
+        --p;
+    }
+    return excl;
+}
+
+// The same bounded wait on a status row that nothing publishes (a test of
+// the failure path: it must time out and report, and the context must stay
+// usable).
+__global__ void k_wait_probe(const uint32_t* status, unsigned* err, int limit)
+{
+    if (threadIdx.x < 32) (void)lookback(status, 0, threadIdx.x, err, limit);
+}
+
 template <typename K>
 struct SortSmem {
     uint32_t whist[kSortWarps][256];
@@ -199,20 +234,7 @@ k_onesweep(const K* __restrict__ kin, K* __restrict__ kout, const uint32_t* __re
     // decoupled look-back for digit t
     uint32_t excl = 0;
     if (tile > 0) {
-        int p = tile - 1;
-        int spins = 0;
-        for (;;) {
-            uint32_t wv = ld_relaxed(status + (int64_t)p * 256 + t);
-            uint32_t flag = wv & ~kValMask;
-            if (flag == 0u) {
-                if (++spins > kLookbackLimit) { atomicOr(err, JT_ERRBIT_LOOKBACK); break; }
-                if (spins > 64) __nanosleep(32);
-                continue;
-            }
-            excl += wv & kValMask;
-            if (flag == kFlagInc || p == 0) break;
-            --p;
-        }
+        excl = lookback(status, tile - 1, t, err, kLookbackLimit);
         st_relaxed(row + t, kFlagInc | (excl + count));
     }
     S.gofs[t] = base[t] + excl;
@@ -510,20 +532,7 @@ k_b_onesweep(const jt_seg_dev* __restrict__ segs, const int64_t* __restrict__ tp
     S.tile_start[t] = x - count + add;
     uint32_t excl = 0;
     if (tile > 0) {
-        int p = tile - 1;
-        int spins = 0;
-        for (;;) {
-            uint32_t wv = ld_relaxed(status + (int64_t)p * 256 + t);
-            uint32_t flag = wv & ~kValMask;
-            if (flag == 0u) {
-                if (++spins > kLookbackLimit) { atomicOr(err, JT_ERRBIT_LOOKBACK); break; }
-                if (spins > 64) __nanosleep(32);
-                continue;
-            }
-            excl += wv & kValMask;
-            if (flag == kFlagInc || p == 0) break;
-            --p;
-        }
+        excl = lookback(status, tile - 1, t, err, kLookbackLimit);
         st_relaxed(row + t, kFlagInc | (excl + count));
     }
     S.gofs[t] = base[t] + excl;
@@ -593,3 +602,29 @@ int jt_b_sort_reorder(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, int n
 }
 
 int jt_sort_tile_size() { return kSortTile; }
+
+extern "C" int jt_wait_probe(int limit, int* timed_out)
+{
+    if (limit <= 0 || limit > (1 << 24) || !timed_out) return JT_EINVAL;
+    *timed_out = 0;
+    uint32_t* status = nullptr;
+    unsigned* err = nullptr;
+    if (cudaMalloc(&status, 256 * sizeof(uint32_t)) != cudaSuccess) return JT_ENOMEM;
+    if (cudaMalloc(&err, sizeof(unsigned)) != cudaSuccess) {
+        cudaFree(status);
+        return JT_ENOMEM;
+    }
+    int r = JT_OK;
+    unsigned e = 0;
+    if (cudaMemset(status, 0, 256 * sizeof(uint32_t)) != cudaSuccess || cudaMemset(err, 0, sizeof(unsigned)) != cudaSuccess)
+        r = JT_ECUDA;
+    if (r == JT_OK) {
+        k_wait_probe<<<1, 32>>>(status, err, limit);
+        if (cudaMemcpy(&e, err, sizeof(unsigned), cudaMemcpyDeviceToHost) != cudaSuccess) r = JT_ECUDA;
+    }
+    cudaFree(status);
+    cudaFree(err);
+    if (r != JT_OK) return r;
+    *timed_out = (e & JT_ERRBIT_LOOKBACK) ? 1 : 0;
+    return *timed_out ? JT_ETIMEDOUT : JT_OK;
+}

@@ -45,7 +45,7 @@ EXPORTED = [
     "jt_batch_trim", "jt_batch_set_graphs", "jt_server_create", "jt_server_destroy",
     "jt_server_add_job", "jt_server_request", "jt_server_clock", "jt_server_poll", "jt_server_serve",
     "jt_server_job_state", "jt_server_get_state", "jt_server_stats", "jt_server_job_need",
-    "jt_walk_tuning",
+    "jt_walk_tuning", "jt_wait_probe",
 ]
 JT_JOB_QUEUED, JT_JOB_RESIDENT, JT_JOB_DONE = 0, 1, 2
 JT_STATIC_SORT_MAX = 262144
@@ -143,6 +143,7 @@ def library():
     L.jt_batch_get_timings.argtypes = [H, C.POINTER(jt_timings)]
     L.jt_morton_sort_static.argtypes = [vp, C.c_size_t, C.c_double, vp, vp, vp]
     L.jt_walk_tuning.argtypes = [C.c_char_p, C.c_size_t]
+    L.jt_wait_probe.argtypes = [C.c_int, C.POINTER(C.c_int)]
     L.jt_batch_trim.argtypes = [H]
     L.jt_batch_set_graphs.argtypes = [H, C.c_int]
     L.jt_server_create.argtypes = [C.c_size_t, C.POINTER(H)]
