@@ -73,3 +73,39 @@ def test_clustered_accuracy_theta_sweep():
     assert report["pm_vs_fp64_pm"][1] <= 1e-3, report
     for theta, bar in BARS.items():
         assert report[f"walk_theta_{theta}"][1] <= bar, (theta, report)
+
+
+def test_uniform_cfg0_error_split():
+    """2x32^3 uniform particles, L = 64, PM 64^3, theta 0.5,
+    mu 19, r_s = 1.25 cells, r_cut = 4.5 r_s, softening spacing/30; every 4th
+    particle as target.  Reports the walk's and the PM path's errors against
+    the FP64 split model's two parts (relative to the FP64 total), and the
+    engine's total against the FP64 split model.  Bar: total p99 <= 2e-3."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import janus_treepm as J
+    Lb, Mb, n = 64.0, 64, 32 ** 3
+    rng = np.random.default_rng(42)
+    pp = ((rng.random((n, 3)) - 0.5) * Lb).astype(np.float32)
+    pm = ((rng.random((n, 3)) - 0.5) * Lb).astype(np.float32)
+    r_s = 1.25 * Lb / Mb
+    r_cut = 4.5 * r_s
+    eps = (Lb / (2 * n) ** (1 / 3)) / 30
+    pos = np.concatenate([pp, pm]).astype(np.float64)
+    mass = np.concatenate([np.full(n, 1.0), np.full(n, 19.0)])
+    sg = np.concatenate([np.ones(n, np.int8), -np.ones(n, np.int8)])
+    idx = np.arange(0, 2 * n, 4)
+    short_ref = O.ewald_forces(pos, mass, sg, Lb, r_s, eps, r_trunc=r_cut, idx=idx, part="short")
+    long_ref = O.ewald_forces(pos, mass, sg, Lb, r_s, eps, idx=idx, part="long")
+    tot = np.linalg.norm(short_ref + long_ref, axis=1)
+    s = J.Solver(J.Config(box_L=Lb, pm_grid=Mb, theta=0.5, softening=eps, r_s=r_s, r_cut=r_cut,
+                          mu=19.0, G_mass_plus=1.0, mode=J.JT_ACCURATE))
+    s.set_state(pp, None, pm, None)
+    sh = np.concatenate(s.accel_part(J.JT_PART_SHORT))[idx]
+    lg = np.concatenate(s.accel_part(J.JT_PART_PM))[idx]
+    al = np.concatenate(s.accel())[idx]
+    s.close()
+    pct = lambda a, b: [float(x) for x in np.percentile(np.linalg.norm(a - b, axis=1) / tot, [50, 99])]
+    report = {"walk": pct(sh, short_ref), "pm": pct(lg, long_ref), "total": pct(al, short_ref + long_ref)}
+    print("ACCURACY_CFG0", json.dumps(report))
+    assert report["total"][1] <= 2e-3, report
