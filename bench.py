@@ -343,6 +343,9 @@ def run_serving(J, ics, n_small, n_big, steps, rates, H, dt, budget_gb=150.0):
     cap = st["requests_served"] / wall
     out["capacity_requests_per_s"] = cap
     out["saturated_value"] = total_ps / wall
+    out["saturated_gpu_busy_frac"] = st["busy_s"] / wall
+    out["saturated_vs_plain"] = (total_ps / wall) / (total_ps / plain_s)
+    out["saturated_swaps_trims"] = [int(st["swapped_out"]), int(st["trims"])]
     for frac in rates:
         wall, st = serve_once(J, jobs, steps, frac * cap, H, dt, budget_gb, seed=12)
         out["runs"].append({
@@ -354,6 +357,7 @@ def run_serving(J, ics, n_small, n_big, steps, rates, H, dt, budget_gb=150.0):
             "requests": int(st["requests_served"]), "batched_steps": int(st["batched_steps"]),
             "max_jobs_per_step": int(st["max_jobs_per_step"]),
             "admission_waits": int(st["admission_waits"]), "swapped_out": int(st["swapped_out"]),
+            "trims": int(st["trims"]),
             "peak_device_gb": st["peak_device_bytes"] / 1e9})
     return out
 

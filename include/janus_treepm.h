@@ -271,6 +271,7 @@ typedef struct jt_serve_stats {
     int64_t peak_device_bytes; /* batch memory after a step, maximum */
     int64_t max_jobs_per_step;
     int64_t swapped_out;       /* idle jobs moved to host to admit others */
+    int64_t trims;             /* scratch pools released to make room */
 } jt_serve_stats;
 
 #define JT_JOB_QUEUED    0

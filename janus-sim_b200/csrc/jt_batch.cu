@@ -1054,10 +1054,18 @@ int jt_batch_step(jt_batch* B, const int* ids, int n_ids, const jt_step_args* ar
     cudaEventCreate(&t0); cudaEventCreate(&t1); cudaEventCreate(&k0); cudaEventCreate(&k1);
     cudaEventRecord(t0, B->st);
     int r = JT_OK;
-    bool all_valid = true;
-    for (int id : v) all_valid = all_valid && B->boxes[id]->acc_valid;
-    if (!all_valid) {
-        r = jtb_force_pass(B, v.data(), (int)v.size(), JT_PART_ALL, 0.0f, steps.data());
+    // the opening half kick needs forces at the current positions: compute
+    // them for the boxes that lack them (new or restored boxes), not for the
+    // whole set
+    std::vector<int> need;
+    std::vector<jt_box_step> need_steps;
+    for (size_t k = 0; k < v.size(); k++)
+        if (!B->boxes[v[k]]->acc_valid) {
+            need.push_back(v[k]);
+            need_steps.push_back(steps[k]);
+        }
+    if (!need.empty()) {
+        r = jtb_force_pass(B, need.data(), (int)need.size(), JT_PART_ALL, 0.0f, need_steps.data());
         if (r == JT_OK) r = finish(B);
     }
     double kd = 0.0;

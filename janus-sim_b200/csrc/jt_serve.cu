@@ -69,6 +69,7 @@ struct jt_server {
     std::vector<double> lat;       // per served request, seconds
     double t0 = 0.0;               // clock origin of arrival times
     int64_t steps = 0, particle_steps = 0, admitted = 0, evicted = 0, refused_fit = 0, swapped = 0;
+    int64_t trims = 0;
     double busy_s = 0.0;
     size_t peak_device = 0;
     int max_resident = 0;
@@ -156,6 +157,12 @@ size_t need_of(size_t persistent, size_t scratch, size_t fft_ws)
     return persistent + scratch + scratch / 16 + fft_ws;
 }
 
+int trim(jt_server* S)
+{
+    S->trims++;
+    return jt_batch_trim(S->B);
+}
+
 bool fits(jt_server* S, const Job& j)
 {
     size_t ws = j.fft_ws;
@@ -195,13 +202,13 @@ int admit_waiting(jt_server* S)
         size_t pers = 0, scr = 0;
         jt_batch_memory(S->B, &pers, &scr);
         if (pers + j.persistent + std::max(scr, S->resident_scratch + j.scratch) > S->budget) {
-            int r = jt_batch_trim(S->B);
+            int r = trim(S);
             if (r != JT_OK) return r;
         }
         int r = admit(S, j);
         if (r == JT_ENOMEM) {
             // scratch pools held for an earlier mix: release them and retry
-            r = jt_batch_trim(S->B);
+            r = trim(S);
             if (r == JT_OK) r = admit(S, j);
         }
         if (r == JT_ENOMEM) break;     // the device disagrees with the estimate: retry later
@@ -231,7 +238,7 @@ int step_once(jt_server* S, int* served)
         // the pass could not grow its scratch (pools sized for an earlier
         // mix of jobs, fragmentation): release every pool and retry once;
         // no kernel ran before the allocation failed
-        r = jt_batch_trim(S->B);
+        r = trim(S);
         if (r == JT_OK) r = jt_batch_step(S->B, ids.data(), (int)ids.size(), args.data(), 1);
     }
     if (r != JT_OK) return r;
@@ -439,6 +446,7 @@ int jt_server_stats(jt_server* S, jt_serve_stats* out)
     s.peak_device_bytes = (int64_t)S->peak_device;
     s.max_jobs_per_step = S->max_resident;
     s.swapped_out = S->swapped;
+    s.trims = S->trims;
     *out = s;
     return JT_OK;
 }

@@ -108,4 +108,4 @@ def test_uniform_cfg0_error_split():
     pct = lambda a, b: [float(x) for x in np.percentile(np.linalg.norm(a - b, axis=1) / tot, [50, 99])]
     report = {"walk": pct(sh, short_ref), "pm": pct(lg, long_ref), "total": pct(al, short_ref + long_ref)}
     print("ACCURACY_CFG0", json.dumps(report))
-    assert report["total"][1] <= 2e-3, report
+    assert report["total"][1] <= 1e-3, report
