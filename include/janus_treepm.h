@@ -181,6 +181,25 @@ int  jt_fp32_peak(int iters, double* tflops);
  * device and size class: register budget as blocks per SM, leaf-bucket
  * size), as text.  No counterpart in the reference. */
 int  jt_walk_tuning(char* buf, size_t len);
+/* ---- in-step diagnostics (device, FP64 accumulation) ----
+ * segregation: |COM+ - COM-| / L, the reference's segregation()
+ * (src/nbody_gpu_twopass.rs:5364-5393); diff_over_poisson, corr and
+ * exc_var_minus: compute_segregation_metrics on an n_cells^3 NGP count grid
+ * (src/bin/janus_mu19_production.rs:219-276); per species the kinetic energy
+ * (1/2) sum m v^2, momentum sum m v and mean position, with m the particle
+ * mass of the config (G folded in).  Computed over the resident state with
+ * no copy of the particles. */
+typedef struct jt_diag {
+    double segregation;
+    double diff_over_poisson;   /* Var(n+ - n-) / (mean+ + mean-) */
+    double corr;                /* Corr(delta+, delta-) */
+    double exc_var_minus;       /* (Var(n-) - mean-) / mean- */
+    double kinetic[2];
+    double momentum[2][3];
+    double com[2][3];
+} jt_diag;
+int  jt_diagnostics(jt_handle* h, int n_cells, jt_diag* out);
+
 /* Failure-path self test: runs the sort's bounded look-back wait on a
  * status word that nothing publishes, with `limit` polls (1..2^24).  Returns
  * JT_ETIMEDOUT with *timed_out = 1 when the wait gave up and reported it (the
@@ -236,6 +255,8 @@ int  jt_batch_memory(jt_batch* b, size_t* persistent, size_t* scratch);
 int  jt_batch_estimate(const jt_config* cfg, size_t n_p, size_t n_m,
                        size_t* persistent, size_t* scratch);
 int  jt_batch_get_timings(jt_batch* b, jt_timings* t);
+/* jt_diagnostics of one box of a batch (jt_diag is declared above). */
+int  jt_batch_diagnostics(jt_batch* b, int box_id, int n_cells, jt_diag* out);
 
 /* on != 0: jt_batch_step replays each step as a CUDA graph, captured once
  * per set of boxes (two graphs: the reorder's ping-pong buffers alternate)

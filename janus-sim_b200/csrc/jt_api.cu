@@ -875,6 +875,16 @@ int jt_debug_tree(jt_handle* h, int species, uint32_t* morton, int32_t* perm, in
     return JT_OK;
 }
 
+int jt_diagnostics(jt_handle* h, int n_cells, jt_diag* out)
+{
+    if (!h || !out) return JT_EINVAL;
+    if (!h->have_state) return JT_ESTATE;
+    const Parts P = parts_of(h);
+    const float4* pos[2] = {P.pos[0], P.pos[1]};
+    const float4* vel[2] = {P.vel[0], P.vel[1]};
+    return jt_diag_state(pos, vel, h->n, h->mass, h->cfg.box_L, n_cells, h->st, out);
+}
+
 int jt_walk_counters(jt_handle* h, int64_t* out4)
 {
     if (!h || !out4) return JT_EINVAL;

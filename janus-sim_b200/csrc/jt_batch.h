@@ -43,4 +43,7 @@ int64_t jtb_phase(jt_batch* B, int i);
 // Set a box's accelerations (species AoS float3 in the caller's order, host
 // or device) and mark them valid for its current positions; used to restore
 // a box that was moved to host memory without recomputing its forces.
+// FP64 diagnostics of one state (jt_diag.cu)
+int jt_diag_state(const float4* const pos[2], const float4* const vel[2], const int64_t n[2],
+                  const float mass[2], double L, int n_cells, cudaStream_t st, jt_diag* out);
 int jtb_set_accel(jt_batch* B, int box_id, const float* acc_p, const float* acc_m, int mem);

@@ -45,7 +45,7 @@ EXPORTED = [
     "jt_batch_trim", "jt_batch_set_graphs", "jt_server_create", "jt_server_destroy",
     "jt_server_add_job", "jt_server_request", "jt_server_clock", "jt_server_poll", "jt_server_serve",
     "jt_server_job_state", "jt_server_get_state", "jt_server_stats", "jt_server_job_need",
-    "jt_walk_tuning", "jt_wait_probe",
+    "jt_walk_tuning", "jt_wait_probe", "jt_diagnostics", "jt_batch_diagnostics",
 ]
 JT_JOB_QUEUED, JT_JOB_RESIDENT, JT_JOB_DONE = 0, 1, 2
 JT_STATIC_SORT_MAX = 262144
@@ -81,6 +81,21 @@ class jt_timings(C.Structure):
 
 class jt_step_args(C.Structure):
     _fields_ = [("dt", C.c_double), ("hubble", C.c_double), ("dtau_per_dt", C.c_double)]
+
+
+class jt_diag(C.Structure):
+    _fields_ = [
+        ("segregation", C.c_double), ("diff_over_poisson", C.c_double), ("corr", C.c_double),
+        ("exc_var_minus", C.c_double), ("kinetic", C.c_double * 2), ("momentum", C.c_double * 6),
+        ("com", C.c_double * 6),
+    ]
+
+    def to_dict(self):
+        return {"segregation": self.segregation, "diff_over_poisson": self.diff_over_poisson,
+                "corr": self.corr, "exc_var_minus": self.exc_var_minus,
+                "kinetic": list(self.kinetic),
+                "momentum": [list(self.momentum[0:3]), list(self.momentum[3:6])],
+                "com": [list(self.com[0:3]), list(self.com[3:6])]}
 
 
 class jt_serve_stats(C.Structure):
@@ -144,6 +159,8 @@ def library():
     L.jt_morton_sort_static.argtypes = [vp, C.c_size_t, C.c_double, vp, vp, vp]
     L.jt_walk_tuning.argtypes = [C.c_char_p, C.c_size_t]
     L.jt_wait_probe.argtypes = [C.c_int, C.POINTER(C.c_int)]
+    L.jt_diagnostics.argtypes = [H, C.c_int, C.POINTER(jt_diag)]
+    L.jt_batch_diagnostics.argtypes = [H, C.c_int, C.c_int, C.POINTER(jt_diag)]
     L.jt_batch_trim.argtypes = [H]
     L.jt_batch_set_graphs.argtypes = [H, C.c_int]
     L.jt_server_create.argtypes = [C.c_size_t, C.POINTER(H)]
@@ -334,6 +351,13 @@ class Solver:
                                        _ptr(right), _ptr(parent)), "jt_debug_tree")
         return dict(morton=morton[:n], perm=perm[:n], left=left, right=right, parent=parent)
 
+    def diagnostics(self, n_cells=32):
+        """FP64 device diagnostics: segregation metrics, kinetic energy,
+        momentum and mean position per species."""
+        d = jt_diag()
+        _check(library().jt_diagnostics(self._h, n_cells, C.byref(d)), "jt_diagnostics")
+        return d.to_dict()
+
     def walk_counters(self):
         """(iterations, ranges, chunks, trips) of a -DJT_WALK_COUNT build."""
         v = (C.c_int64 * 4)()
@@ -456,6 +480,12 @@ class Batch:
         _check(library().jt_batch_get_state(self._b, box_id, *[_ptr(a) for a in out], JT_MEM_HOST),
                "jt_batch_get_state")
         return tuple(out)
+
+    def diagnostics(self, box_id, n_cells=32):
+        d = jt_diag()
+        _check(library().jt_batch_diagnostics(self._b, box_id, n_cells, C.byref(d)),
+               "jt_batch_diagnostics")
+        return d.to_dict()
 
     def memory(self):
         a, b = C.c_size_t(), C.c_size_t()

@@ -217,3 +217,46 @@ def acc_pm_forces(pos, mass, signs, M, box, r_s, k_min=0, order=2, interlace=Fal
     lib().orc_acc_pm_forces2(pos.ravel(), mass, signs, len(pos), M, box, r_s, k_min, order,
                              2 if interlace else 1, acc.ravel())
     return acc
+
+
+# ---------------------------------------------------------------------------
+# Diagnostics (numpy restatements of the reference's host-side metrics)
+# ---------------------------------------------------------------------------
+def segregation(pos, signs, box):
+    """|COM+ - COM-| / L with plain means (src/nbody_gpu_twopass.rs:5364-5393)."""
+    pos = np.asarray(pos, np.float32).astype(np.float64).reshape(-1, 3)
+    signs = np.asarray(signs)
+    cp = pos[signs > 0].mean(axis=0) if np.any(signs > 0) else np.zeros(3)
+    cm = pos[signs < 0].mean(axis=0) if np.any(signs < 0) else np.zeros(3)
+    return float(np.linalg.norm(cp - cm) / box)
+
+
+def segregation_metrics(pos, signs, box, n_cells):
+    """compute_segregation_metrics (src/bin/janus_mu19_production.rs:219-276):
+    NGP counts of each species on an n_cells^3 grid (cell of a coordinate:
+    rem_euclid(x + L/2, L) / cell, truncated, mod n_cells), then
+    (Var(n+ - n-) / (mean+ + mean-), Corr(delta+, delta-),
+     (Var(n-) - mean-) / mean-)."""
+    pos = np.asarray(pos, np.float32).astype(np.float64).reshape(-1, 3)
+    signs = np.asarray(signs)
+    cell = box / n_cells
+    r = np.mod(pos + box / 2.0, box)
+    ic = (np.floor(r / cell).astype(np.int64)) % n_cells
+    flat = (ic[:, 0] * n_cells + ic[:, 1]) * n_cells + ic[:, 2]
+    tot = n_cells ** 3
+    n_plus = np.bincount(flat[signs > 0], minlength=tot).astype(np.float64)
+    n_minus = np.bincount(flat[signs < 0], minlength=tot).astype(np.float64)
+    mp, mm = n_plus.sum() / tot, n_minus.sum() / tot
+    diff = n_plus - n_minus - (mp - mm)
+    var_diff = np.mean(diff ** 2)
+    pois = mp + mm
+    dop = var_diff / pois if pois > 0 else 0.0
+    dp = (n_plus - mp) / mp if mp > 0 else np.zeros(tot)
+    dm = (n_minus - mm) / mm if mm > 0 else np.zeros(tot)
+    var_p = np.mean(dp * dp) - np.mean(dp) ** 2
+    var_m = np.mean(dm * dm) - np.mean(dm) ** 2
+    cov = np.mean(dp * dm) - np.mean(dp) * np.mean(dm)
+    corr = cov / (np.sqrt(var_p) * np.sqrt(var_m)) if var_p > 0 and var_m > 0 else 0.0
+    var_mc = np.mean((n_minus - mm) ** 2)
+    exc = (var_mc - mm) / mm if mm > 0 else 0.0
+    return float(dop), float(corr), float(exc)
