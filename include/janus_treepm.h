@@ -200,6 +200,34 @@ typedef struct jt_diag {
 } jt_diag;
 int  jt_diagnostics(jt_handle* h, int n_cells, jt_diag* out);
 
+/* ---- snapshots (the reference's snapshot_v3 format) ----
+ * src/snapshot_v3.rs:12-47, 260-376: a 408-byte little-endian header and
+ * 36-byte particles (f32 pos[3], vel[3], mass, softening; u8 sign 1 / 255,
+ * split level, star flag, flags).  The metadata the engine does not know
+ * (expansion state, Hubble constant, seeds, label) comes from the caller. */
+typedef struct jt_snapshot_meta {
+    double   a;            /* scale factor */
+    double   t_gyr;        /* cosmic time (Gyr) */
+    double   h0;           /* Hubble constant (km/s/Mpc) */
+    double   omega_b;
+    double   z_init;       /* initial redshift of the ICs */
+    double   z_start_run;  /* start redshift of this run */
+    uint32_t seed_ic;
+    char     run_label[256];
+} jt_snapshot_meta;
+/* Write n particles (host arrays; vel may be NULL) to a snapshot file. */
+int  jt_snapshot_write(const char* path, const jt_snapshot_meta* meta, double box_L, double mu,
+                       const float* pos, const float* vel, const int8_t* signs,
+                       const float* mass, const float* eps, size_t n);
+/* Read a snapshot: *n = its particle count; pos == NULL asks for the header
+ * only; otherwise arrays of cap >= n particles (vel, mass, eps may be NULL). */
+int  jt_snapshot_read(const char* path, jt_snapshot_meta* meta, double* box_L, double* mu,
+                      float* pos, float* vel, int8_t* signs, float* mass, float* eps,
+                      size_t cap, size_t* n);
+/* Checkpoint a handle's state (caller order, signs, config masses and
+ * softening); resume with jt_snapshot_read + jt_set_state_signed. */
+int  jt_checkpoint(jt_handle* h, const char* path, const jt_snapshot_meta* meta);
+
 /* Failure-path self test: runs the sort's bounded look-back wait on a
  * status word that nothing publishes, with `limit` polls (1..2^24).  Returns
  * JT_ETIMEDOUT with *timed_out = 1 when the wait gave up and reported it (the

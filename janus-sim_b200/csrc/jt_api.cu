@@ -875,6 +875,22 @@ int jt_debug_tree(jt_handle* h, int species, uint32_t* morton, int32_t* perm, in
     return JT_OK;
 }
 
+}  // extern "C"
+
+int jth_info(jt_handle* h, jt_config* cfg, float* m_plus, float* m_minus, int8_t* signs)
+{
+    if (!h) return JT_EINVAL;
+    if (!h->have_state) return JT_ESTATE;
+    if (cfg) *cfg = h->cfg;
+    if (m_plus) *m_plus = h->mass[0];
+    if (m_minus) *m_minus = h->mass[1];
+    if (signs && cudaMemcpy(signs, h->sign_caller, (size_t)(h->n[0] + h->n[1]), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return JT_ECUDA;
+    return JT_OK;
+}
+
+extern "C" {
+
 int jt_diagnostics(jt_handle* h, int n_cells, jt_diag* out)
 {
     if (!h || !out) return JT_EINVAL;

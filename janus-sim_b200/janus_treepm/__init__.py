@@ -46,6 +46,7 @@ EXPORTED = [
     "jt_server_add_job", "jt_server_request", "jt_server_clock", "jt_server_poll", "jt_server_serve",
     "jt_server_job_state", "jt_server_get_state", "jt_server_stats", "jt_server_job_need",
     "jt_walk_tuning", "jt_wait_probe", "jt_diagnostics", "jt_batch_diagnostics",
+    "jt_snapshot_write", "jt_snapshot_read", "jt_checkpoint",
 ]
 JT_JOB_QUEUED, JT_JOB_RESIDENT, JT_JOB_DONE = 0, 1, 2
 JT_STATIC_SORT_MAX = 262144
@@ -96,6 +97,46 @@ class jt_diag(C.Structure):
                 "kinetic": list(self.kinetic),
                 "momentum": [list(self.momentum[0:3]), list(self.momentum[3:6])],
                 "com": [list(self.com[0:3]), list(self.com[3:6])]}
+
+
+class jt_snapshot_meta(C.Structure):
+    _fields_ = [("a", C.c_double), ("t_gyr", C.c_double), ("h0", C.c_double), ("omega_b", C.c_double),
+                ("z_init", C.c_double), ("z_start_run", C.c_double), ("seed_ic", C.c_uint32),
+                ("run_label", C.c_char * 256)]
+
+
+def snapshot_meta(a=1.0, t_gyr=0.0, h0=69.9, omega_b=0.05, z_init=10.0, z_start_run=10.0, seed_ic=42,
+                  run_label=""):
+    m = jt_snapshot_meta()
+    m.a, m.t_gyr, m.h0, m.omega_b, m.z_init, m.z_start_run = a, t_gyr, h0, omega_b, z_init, z_start_run
+    m.seed_ic = seed_ic
+    m.run_label = run_label.encode()[:255]
+    return m
+
+
+def snapshot_write(path, meta, box_L, mu, pos, vel, signs, mass, eps):
+    """Write the reference's snapshot_v3 file (host arrays)."""
+    pos = _f32(pos)
+    vel = None if vel is None else _f32(vel)
+    signs = np.ascontiguousarray(signs, np.int8)
+    mass = np.ascontiguousarray(mass, np.float32)
+    eps = np.ascontiguousarray(eps, np.float32)
+    _check(library().jt_snapshot_write(str(path).encode(), C.byref(meta), box_L, mu, _ptr(pos), _ptr(vel),
+                                       _ptr(signs), _ptr(mass), _ptr(eps), len(pos)), "jt_snapshot_write")
+
+
+def snapshot_read(path):
+    """Read a snapshot_v3 file: (meta, box_L, mu, pos, vel, signs, mass, eps)."""
+    L = library()
+    meta, box, mu, n = jt_snapshot_meta(), C.c_double(), C.c_double(), C.c_size_t()
+    _check(L.jt_snapshot_read(str(path).encode(), C.byref(meta), C.byref(box), C.byref(mu), None, None,
+                              None, None, None, 0, C.byref(n)), "jt_snapshot_read")
+    k = n.value
+    pos, vel = np.zeros((k, 3), np.float32), np.zeros((k, 3), np.float32)
+    sg, mass, eps = np.zeros(k, np.int8), np.zeros(k, np.float32), np.zeros(k, np.float32)
+    _check(L.jt_snapshot_read(str(path).encode(), C.byref(meta), C.byref(box), C.byref(mu), _ptr(pos),
+                              _ptr(vel), _ptr(sg), _ptr(mass), _ptr(eps), k, C.byref(n)), "jt_snapshot_read")
+    return meta, box.value, mu.value, pos, vel, sg, mass, eps
 
 
 class jt_serve_stats(C.Structure):
@@ -160,6 +201,12 @@ def library():
     L.jt_walk_tuning.argtypes = [C.c_char_p, C.c_size_t]
     L.jt_wait_probe.argtypes = [C.c_int, C.POINTER(C.c_int)]
     L.jt_diagnostics.argtypes = [H, C.c_int, C.POINTER(jt_diag)]
+    L.jt_snapshot_write.argtypes = [C.c_char_p, C.POINTER(jt_snapshot_meta), C.c_double, C.c_double,
+                                    fp, fp, vp, fp, fp, C.c_size_t]
+    L.jt_snapshot_read.argtypes = [C.c_char_p, C.POINTER(jt_snapshot_meta), C.POINTER(C.c_double),
+                                   C.POINTER(C.c_double), fp, fp, vp, fp, fp, C.c_size_t,
+                                   C.POINTER(C.c_size_t)]
+    L.jt_checkpoint.argtypes = [H, C.c_char_p, C.POINTER(jt_snapshot_meta)]
     L.jt_batch_diagnostics.argtypes = [H, C.c_int, C.c_int, C.POINTER(jt_diag)]
     L.jt_batch_trim.argtypes = [H]
     L.jt_batch_set_graphs.argtypes = [H, C.c_int]
@@ -350,6 +397,11 @@ class Solver:
         _check(library().jt_debug_tree(self._h, species, _ptr(morton), _ptr(perm), _ptr(left),
                                        _ptr(right), _ptr(parent)), "jt_debug_tree")
         return dict(morton=morton[:n], perm=perm[:n], left=left, right=right, parent=parent)
+
+    def checkpoint(self, path, meta=None):
+        """Write the state to a snapshot_v3 file (caller order, signs)."""
+        meta = meta if meta is not None else snapshot_meta()
+        _check(library().jt_checkpoint(self._h, str(path).encode(), C.byref(meta)), "jt_checkpoint")
 
     def diagnostics(self, n_cells=32):
         """FP64 device diagnostics: segregation metrics, kinetic energy,
