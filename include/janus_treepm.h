@@ -149,6 +149,19 @@ int  jt_accel_part(jt_handle* h, int part, float* acc_p, float* acc_m, int mem);
  * dtau_per_dt) (:4486-4649); r_cut comes from the config. */
 int  jt_step(jt_handle* h, double dt, double hubble, double dtau_per_dt, int nsteps);
 
+/* Yukawa screening of opposite-sign pairs: the reference's set_lambda_0 /
+ * set_current_z (src/nbody_gpu_twopass.rs:2305-2312) as its TreePM step uses
+ * them (compute_short_range_forces, :3997-4068).  With lambda_0 > 0.01 the
+ * short-range walk becomes the reference's screened full-range walk
+ * (forces_twopass_warpcoherent_screening, :911-1035): no r_cut prune and no
+ * erfc; a same-sign pair contributes m / r_p^3, an opposite-sign pair
+ * -exp(-x)(1 + x) m / r_p^3 with x = r_p / lambda(z), lambda(z) = lambda_0
+ * sqrt(1 + z) quantised down to 0.1; theta and softening are rounded to
+ * 1e-3.  The PM part is unchanged.  Compatibility mode only (JT_EINVAL for
+ * lambda_0 > 0.01 on a JT_ACCURATE handle); lambda_0 <= 0.01 turns it off.
+ * Takes effect at the next force evaluation. */
+int  jt_set_screening(jt_handle* h, double lambda_0, double z);
+
 /* Read the state back in the caller's order (get_particles, :5470).  Any
  * pointer may be NULL. */
 int  jt_get_state(jt_handle* h, float* pos_p, float* vel_p, float* pos_m,

@@ -55,6 +55,9 @@ struct jt_handle {
     jt_batch* batch = nullptr;
     int box_id = -1;
     bool dbg_ready = false;            // debug-tree buffers (accurate mode)
+    // Yukawa screening of opposite-sign pairs (compatibility mode):
+    // lambda_0 > 0.01 selects the screened walk
+    double lambda_0 = 0.0, z = 0.0;
 };
 
 namespace {
@@ -350,18 +353,27 @@ int compute_forces_rc(jt_handle* h, float kick_dt, float drag, int parts = JT_PA
     cudaEventRecord(h->ev[5], st);
     JT_FFT(cufftExecC2R(h->pm.plan_c2r, h->pm.force_k, h->pm.force));
     cudaEventRecord(h->ev[6], st);
-    float tq, sq, rq, bq;
+    float tq, sq, rq, bq, il = 0.0f;
+    const bool screened = h->lambda_0 > 0.01;
     {
         // host packing of the reference (:4079-4082, :1932-1937) and the
-        // kernel's unpacking (:1684-1694)
+        // kernel's unpacking (:1684-1694); the screened branch rounds theta
+        // and softening (:4009-4011) and packs lambda(z) = lambda_0 sqrt(1+z)
+        // with box_half (:4015, :1921-1927; unpacked at :929-936, :952)
         auto sat = [](double v) -> unsigned {
-            return v <= 0.0 ? 0u : (v >= 4294967295.0 ? 0xFFFFFFFFu : (unsigned)v);
+            return !(v > 0.0) ? 0u : (v >= 4294967295.0 ? 0xFFFFFFFFu : (unsigned)v);
         };
-        unsigned ti = sat(c.theta * 1000.0), si = sat(c.softening * 1000.0);
+        const double tv = screened ? std::round(c.theta * 1000.0) : c.theta * 1000.0;
+        const double sv = screened ? std::round(c.softening * 1000.0) : c.softening * 1000.0;
+        unsigned ti = sat(tv), si = sat(sv);
         unsigned ri = sat(c.r_cut), bi = sat(c.box_L / 2.0);
+        unsigned li = sat(h->lambda_0 * std::sqrt(1.0 + h->z) * 10.0);
         ti = ti > 0xFFFF ? 0xFFFF : ti; si = si > 0xFFFF ? 0xFFFF : si;
         ri = ri > 0xFFFF ? 0xFFFF : ri; bi = bi > 0xFFFF ? 0xFFFF : bi;
+        li = li > 0xFFFF ? 0xFFFF : li;
         tq = (float)ti / 1000.0f; sq = (float)si / 1000.0f; rq = (float)ri; bq = (float)bi;
+        const float lam = (float)li / 10.0f;
+        if (screened) il = lam > 0.01f ? 1.0f / lam : 0.0f;
     }
     jt_rc_params P;
     P.theta2 = tq * tq;
@@ -376,6 +388,8 @@ int compute_forces_rc(jt_handle* h, float kick_dt, float drag, int parts = JT_PA
     P.mass[0] = h->mass[0];
     P.mass[1] = h->mass[1];
     P.parts = parts;
+    P.screen = screened ? 1 : 0;
+    P.inv_lambda = il;
     const float4* sp2[2] = {h->pos[0], h->pos[1]};
     jt_launch_walk_rcompat(P, h->pos_caller, h->sign_caller, h->n[0] + h->n[1], sp2, h->n, h->tree,
                            h->pm.force, h->acc_caller, h->d_err, st);
@@ -801,6 +815,17 @@ int jt_step(jt_handle* h, double dt, double hubble, double dtau_per_dt, int nste
     }
     cudaEventDestroy(t0); cudaEventDestroy(t1); cudaEventDestroy(k0); cudaEventDestroy(k1);
     return r;
+}
+
+int jt_set_screening(jt_handle* h, double lambda_0, double z)
+{
+    if (!h || !(lambda_0 >= 0.0) || !(z > -1.0) || !std::isfinite(lambda_0) || !std::isfinite(z))
+        return JT_EINVAL;
+    if (h->cfg.mode != JT_RCOMPAT && lambda_0 > 0.01) return JT_EINVAL;
+    if (h->lambda_0 != lambda_0 || h->z != z) h->acc_valid = false;
+    h->lambda_0 = lambda_0;
+    h->z = z;
+    return JT_OK;
 }
 
 int jt_get_state(jt_handle* h, float* pos_p, float* vel_p, float* pos_m, float* vel_m, int mem)

@@ -279,6 +279,8 @@ struct jt_rc_params {
     int M;
     float mass[2];
     int parts;                                    // JT_PART_* bits
+    int screen;                                   // 1: Yukawa-screened full-range walk
+    float inv_lambda;                             // quantised 1/lambda(z) (0 = off)
 };
 void jt_launch_walk_rcompat(const jt_rc_params& p, const float4* pos_caller,
                             const int8_t* sign_caller, int64_t n_all,

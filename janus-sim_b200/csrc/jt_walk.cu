@@ -685,9 +685,12 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk_rc(RcArgs A)
             float dz = rc_wrap(__fsub_rn(b.z, p.z), P.box_half_q);
             float r2 = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)),
                                            __fmul_rn(dz, dz)), 1e-20f);
-            float r = __fsqrt_rn(r2);
-            bool beyond = __fsub_rn(r, b.w) > P.r_cut;
-            if (__all_sync(0xffffffffu, beyond)) continue;
+            // the screened walk (:911-1035) has no r_cut prune
+            if (!P.screen) {
+                float r = __fsqrt_rn(r2);
+                bool beyond = __fsub_rn(r, b.w) > P.r_cut;
+                if (__all_sync(0xffffffffu, beyond)) continue;
+            }
             bool approx = leaf || (__fmul_rn(__fmul_rn(4.0f, b.w), b.w) < __fmul_rn(P.theta2, r2));
             if (__all_sync(0xffffffffu, approx)) {
                 if (valid) {
@@ -697,14 +700,29 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk_rc(RcArgs A)
                     float rp2 = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy)),
                                                     __fmul_rn(ddz, ddz)), P.eps2);
                     float rp = __fsqrt_rn(rp2);
-                    float arg = __fdiv_rn(rp, __fmul_rn(2.0f, P.r_s));
-                    float ef = erfcf(arg);
-                    if (ef > 1e-6f) {
-                        float irp3 = __fdiv_rn(1.0f, __fmul_rn(rp, rp2));
-                        float f = __fmul_rn(__fmul_rn(__fmul_rn(sf, cm.w), irp3), ef);
+                    if (P.screen) {
+                        // s_i s_t S m / r_p^3, S = exp(-x)(1 + x), x = r_p / lambda,
+                        // for opposite signs (:1000-1017)
+                        float irp3 = __fdiv_rn(1.0f, __fmul_rn(rp2, rp));
+                        float scr = 1.0f;
+                        if (sf < 0.0f && P.inv_lambda > 0.0f) {
+                            float x = __fmul_rn(rp, P.inv_lambda);
+                            scr = __fmul_rn(expf(-x), __fadd_rn(1.0f, x));
+                        }
+                        float f = __fmul_rn(__fmul_rn(__fmul_rn(sf, scr), cm.w), irp3);
                         ax = __fadd_rn(ax, __fmul_rn(f, ddx));
                         ay = __fadd_rn(ay, __fmul_rn(f, ddy));
                         az = __fadd_rn(az, __fmul_rn(f, ddz));
+                    } else {
+                        float arg = __fdiv_rn(rp, __fmul_rn(2.0f, P.r_s));
+                        float ef = erfcf(arg);
+                        if (ef > 1e-6f) {
+                            float irp3 = __fdiv_rn(1.0f, __fmul_rn(rp, rp2));
+                            float f = __fmul_rn(__fmul_rn(__fmul_rn(sf, cm.w), irp3), ef);
+                            ax = __fadd_rn(ax, __fmul_rn(f, ddx));
+                            ay = __fadd_rn(ay, __fmul_rn(f, ddy));
+                            az = __fadd_rn(az, __fmul_rn(f, ddz));
+                        }
                     }
                 }
             } else {

@@ -46,7 +46,7 @@ EXPORTED = [
     "jt_server_add_job", "jt_server_request", "jt_server_clock", "jt_server_poll", "jt_server_serve",
     "jt_server_job_state", "jt_server_get_state", "jt_server_stats", "jt_server_job_need",
     "jt_walk_tuning", "jt_wait_probe", "jt_diagnostics", "jt_batch_diagnostics",
-    "jt_snapshot_write", "jt_snapshot_read", "jt_checkpoint",
+    "jt_snapshot_write", "jt_snapshot_read", "jt_checkpoint", "jt_set_screening",
 ]
 JT_JOB_QUEUED, JT_JOB_RESIDENT, JT_JOB_DONE = 0, 1, 2
 JT_STATIC_SORT_MAX = 262144
@@ -207,6 +207,7 @@ def library():
                                    C.POINTER(C.c_double), fp, fp, vp, fp, fp, C.c_size_t,
                                    C.POINTER(C.c_size_t)]
     L.jt_checkpoint.argtypes = [H, C.c_char_p, C.POINTER(jt_snapshot_meta)]
+    L.jt_set_screening.argtypes = [H, C.c_double, C.c_double]
     L.jt_batch_diagnostics.argtypes = [H, C.c_int, C.c_int, C.POINTER(jt_diag)]
     L.jt_batch_trim.argtypes = [H]
     L.jt_batch_set_graphs.argtypes = [H, C.c_int]
@@ -367,6 +368,11 @@ class Solver:
         def dp(t):
             return None if t is None else C.c_void_p(t.data_ptr())
         _check(library().jt_accel(self._h, dp(acc_p), dp(acc_m), JT_MEM_DEVICE), "jt_accel")
+
+    def set_screening(self, lambda_0, z=0.0):
+        """Yukawa screening of opposite-sign pairs (set_lambda_0 /
+        set_current_z); compatibility mode, lambda_0 > 0.01 turns it on."""
+        _check(library().jt_set_screening(self._h, lambda_0, z), "jt_set_screening")
 
     def step(self, dt, hubble=0.0, dtau_per_dt=1.0, nsteps=1):
         _check(library().jt_step(self._h, dt, hubble, dtau_per_dt, nsteps), "jt_step")

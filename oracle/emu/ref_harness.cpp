@@ -324,6 +324,40 @@ void ref_short_range(const float* pos_all, const signed char* signs_all,
     });
 }
 
+/* host packing of the screened branch of compute_short_range_forces
+ * (:4008-4016): theta and softening ROUNDED to 1e-3 (f64::round, half away
+ * from zero) before the saturating cast; lambda(z) = lambda_0 sqrt(1 + z)
+ * and box_half by pack_lambda_boxhalf (:1921-1927), truncated. */
+void ref_pack_screening(double theta, double softening, double lambda_0, double z, double box_size,
+                        float* theta_soft_packed, float* lambda_boxhalf_packed)
+{
+    unsigned ti = sat_u32(std::round(theta * 1000.0)), si = sat_u32(std::round(softening * 1000.0));
+    if (ti > 0xFFFF) ti = 0xFFFF;
+    if (si > 0xFFFF) si = 0xFFFF;
+    unsigned a = (ti << 16) | si;
+    double lz = lambda_0 * std::sqrt(1.0 + z);
+    unsigned li = sat_u32(lz * 10.0), bi = sat_u32(box_size / 2.0);
+    if (li > 0xFFFF) li = 0xFFFF;
+    if (bi > 0xFFFF) bi = 0xFFFF;
+    unsigned b = (li << 16) | bi;
+    std::memcpy(theta_soft_packed, &a, 4);
+    std::memcpy(lambda_boxhalf_packed, &b, 4);
+}
+
+/* forces_twopass_warpcoherent_screening: 256 threads/block, 4096 B dynamic
+ * shared memory, as compute_short_range_forces launches it (:4036-4073) */
+void ref_screening(const float* pos_all, const signed char* signs_all, const float* node_pos,
+                   const float* node_mass, const int* left, const int* right, const int* types,
+                   float* acc, int n_all, int tree_sign, float theta_soft_packed,
+                   float lambda_boxhalf_packed)
+{
+    emu_launch_warps(blocks_for(n_all, 256), 256, [&] {
+        forces_twopass_warpcoherent_screening(pos_all, signs_all, node_pos, node_mass, left, right,
+                                              types, acc, n_all, tree_sign, theta_soft_packed,
+                                              lambda_boxhalf_packed);
+    });
+}
+
 void ref_drift(float* pos, const float* vel, float dt, float box_half, int n)
 {
     emu_launch_serial(blocks_for(n, 256), 256, [&] { drift_f32(pos, vel, dt, box_half, n); });

@@ -100,6 +100,22 @@ void orc_ref_total_forces(const float* pos_all, const int8_t* signs_all,
 /* TreePMForce::new(r_cut, grid, box, theta, eps) + update + compute_all_forces
  * with per-particle masses (G folded in) and signs.  pos AoS f64.  Threads
  * from OpenMP (rayon in the reference). */
+/* screened branch of compute_short_range_forces (ref_walk.c) */
+void orc_ref_screen_quantize(double theta, double softening, double lambda_0, double z,
+                             double box_size, float* theta_q, float* soft_q,
+                             float* inv_lambda, float* box_half_q);
+void orc_ref_screened_walk(const float* pos_all, const int8_t* signs_all,
+                           int64_t n_all, int tree_sign,
+                           const float* node_pos, const float* node_mass,
+                           const int32_t* left, const int32_t* right,
+                           const int32_t* types,
+                           float theta, float softening, float inv_lambda,
+                           float box_half, int accumulate, float* acc);
+void orc_ref_total_forces_screened(const float* pos_all, const int8_t* signs_all,
+                                   int64_t n_all, int M, double box, double theta,
+                                   double softening, double r_cut, double mass_factor,
+                                   int k_min, double lambda_0, double z, float* acc);
+
 void orc_cpu_treepm_forces(const double* pos, const double* mass,
                            const int8_t* signs, int64_t n, double r_cut,
                            int grid, double box, double theta,

@@ -46,6 +46,12 @@ def lib():
             "orc_ref_short_range": [f32p, i8p, I64, I32, f32p, f32p, i32p, i32p, i32p,
                                     F32, F32, F32, F32, I32, f32p],
             "orc_ref_total_forces": [f32p, i8p, I64, I32, F64, F64, F64, F64, F64, I32, f32p],
+            "orc_ref_screen_quantize": [F64, F64, F64, F64, F64, C.POINTER(F32), C.POINTER(F32),
+                                        C.POINTER(F32), C.POINTER(F32)],
+            "orc_ref_screened_walk": [f32p, i8p, I64, I32, f32p, f32p, i32p, i32p, i32p,
+                                      F32, F32, F32, F32, I32, f32p],
+            "orc_ref_total_forces_screened": [f32p, i8p, I64, I32, F64, F64, F64, F64, F64, I32,
+                                              F64, F64, f32p],
             "orc_cpu_treepm_forces": [f64p, f64p, i8p, I64, F64, I32, F64, F64, F64, f64p],
             "orc_cpu_treepm_last_times": [C.POINTER(F64), C.POINTER(F64)],
             "orc_ewald_forces": [f64p, f64p, i8p, I64, i64p, I64, F64, F64, F64, F64, F64, f64p],
@@ -90,6 +96,8 @@ def ref():
             "ref_normalize": [f64p, I32, F64],
             "ref_pack_params": [F64, F64, F64, F64, C.POINTER(F32), C.POINTER(F32)],
             "ref_short_range": [f32p, i8p, f32p, f32p, i32p, i32p, i32p, f32p, I32, F32, F32],
+            "ref_pack_screening": [F64, F64, F64, F64, F64, C.POINTER(F32), C.POINTER(F32)],
+            "ref_screening": [f32p, i8p, f32p, f32p, i32p, i32p, i32p, f32p, I32, I32, F32, F32],
             "ref_drift": [f32p, f32p, F32, F32, I32],
             "ref_kick": [f32p, f32p, F32, I32, F32, F32],
         }
@@ -158,6 +166,27 @@ def ref_total_forces(pos_all, signs_all, M, box, theta, softening, r_cut,
     acc = np.zeros((len(pos_all), 3), np.float32)
     lib().orc_ref_total_forces(pos_all.ravel(), signs_all, len(pos_all), M, box,
                                theta, softening, r_cut, mass_factor, k_min, acc.ravel())
+    return acc
+
+
+def ref_screen_quantize(theta, softening, lambda_0, z, box):
+    """(theta, softening, 1/lambda, box_half) as the screened walk sees them."""
+    a, b, c, d = F32(), F32(), F32(), F32()
+    lib().orc_ref_screen_quantize(theta, softening, lambda_0, z, box, C.byref(a), C.byref(b),
+                                  C.byref(c), C.byref(d))
+    return a.value, b.value, c.value, d.value
+
+
+def ref_total_forces_screened(pos_all, signs_all, M, box, theta, softening, r_cut,
+                              mass_factor, lambda_0, z, k_min=0):
+    """Reference GPU TreePM acceleration with Yukawa screening of opposite-sign
+    pairs (lambda_0 > 0.01: PM + the full-range screened walk), FP32 out."""
+    pos_all = _c(pos_all, np.float32).reshape(-1, 3)
+    signs_all = _c(signs_all, np.int8)
+    acc = np.zeros((len(pos_all), 3), np.float32)
+    lib().orc_ref_total_forces_screened(pos_all.ravel(), signs_all, len(pos_all), M, box, theta,
+                                        softening, r_cut, mass_factor, k_min, lambda_0, z,
+                                        acc.ravel())
     return acc
 
 

@@ -94,6 +94,41 @@ def ref_short(pos_all, sg, trees, theta, eps, r_cut, L):
     return acc.reshape(n, 3)
 
 
+def ref_screened(pos_all, sg, trees, theta, eps, lambda_0, z, L):
+    """forces_twopass_warpcoherent_screening over both trees (+ overwrites, -
+    accumulates), packed as compute_short_range_forces packs it."""
+    R = O.ref()
+    n = len(pos_all)
+    a, b = C.c_float(), C.c_float()
+    R.ref_pack_screening(theta, eps, lambda_0, z, L, C.byref(a), C.byref(b))
+    acc = np.zeros(3 * n, np.float32)
+    for sgn, T in zip((1, -1), trees):
+        nn = len(T["node_mass"])
+        left = np.concatenate([T["left"], np.full(nn, -1, np.int32)])[:nn].astype(np.int32)
+        right = np.concatenate([T["right"], np.full(nn, -1, np.int32)])[:nn].astype(np.int32)
+        R.ref_screening(pos_all.ravel(), sg, T["node_pos"].ravel(), T["node_mass"], left, right,
+                        T["types"], acc, n, sgn, a.value, b.value)
+    return acc.reshape(n, 3)
+
+
+def screened_fixture():
+    """PM + Yukawa-screened walk (lambda_0 > 0.01 branch) on a mixed-sign
+    array; theta and softening chosen so that rounding and truncation of the
+    1e-3 packing differ."""
+    rng = np.random.default_rng(20261203)
+    n, M, L = 1100, 16, 32.0
+    pos = ((rng.random((n, 3)) - 0.5) * L).astype(np.float32)
+    sg = np.where(rng.random(n) < 0.4, 1, -1).astype(np.int8)
+    theta, eps, r_cut, mf, lambda_0, z = 0.5497, 0.0508, 5.7, 0.02, 1.93, 0.8
+    g_const = mf / (L / M) ** 3
+    _, _, _, _, fpm = ref_pm(pos, sg, M, L, g_const, r_cut / 3.0, 0)
+    trees = [ref_tree(np.ascontiguousarray(pos[sg == s]), L / 2, mf) for s in (1, -1)]
+    fsc = ref_screened(pos, sg, trees, theta, eps, lambda_0, z, L)
+    np.savez_compressed(os.path.join(HERE, "screened_mixed_1100.npz"), pos=pos, signs=sg, M=M, L=L,
+                        theta=theta, eps=eps, r_cut=r_cut, mass_factor=mf, lambda_0=lambda_0, z=z,
+                        pm_forces=fpm, screened=fsc, total=(fsc + fpm).astype(np.float32))
+
+
 def main():
     out = {}
     rng = np.random.default_rng(20260101)
@@ -124,6 +159,8 @@ def main():
     np.savez_compressed(os.path.join(HERE, "pm_kmin3_1200.npz"), pos=pos, signs=sg, M=M, L=L2,
                         g_const=g_const, r_s=r_cut / 3.0, phi_plus=pp2, phi_minus=pm2,
                         pm_forces=fpm2)
+    # 5. Yukawa-screened walk
+    screened_fixture()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -86,6 +86,44 @@ def test_rcompat_matches_reference_forces(n, M, L, interleave):
     s.close()
 
 
+@pytest.mark.parametrize("n,lam,z,theta,eps", [(2048, 1.93, 0.8, 0.5497, 0.0508),
+                                               (3000, 0.35, 0.0, 0.7, 0.1),
+                                               (1500, 7000.0, 9.0, 0.45, 0.02)])
+def test_rcompat_screened_matches_reference_forces(n, lam, z, theta, eps):
+    """Yukawa-screened walk (lambda_0 > 0.01) + PM against the oracle of the
+    reference's screened branch; same bars as the unscreened case (CUDA's
+    expf differs from the host's by an ulp or two)."""
+    J, O = _mods()
+    L, M, r_cut, mf = 40.0, 32, 5.0, 0.01
+    rng = np.random.default_rng(17)
+    pos = _uniform(n, L, 5)
+    sg = np.where(rng.random(n) < 0.45, 1, -1).astype(np.int8)
+    s = J.Solver(J.Config(box_L=L, pm_grid=M, theta=theta, softening=eps, r_s=r_cut / 3,
+                          r_cut=r_cut, mu=(sg < 0).sum() / (sg > 0).sum(), G_mass_plus=mf,
+                          mode=J.JT_RCOMPAT))
+    s.set_state_signed(pos, None, sg)
+    s.set_screening(lam, z)
+    got = s.accel()
+    ref = O.ref_total_forces_screened(pos, sg, M, L, theta, eps, r_cut, mf, lam, z)
+    rel = _rel(got, ref)
+    assert np.percentile(rel, 99) <= 1e-5, np.percentile(rel, [50, 99, 100])
+    assert rel.max() <= 1e-3
+    # off again: the erfc-split walk, as before
+    s.set_screening(0.0, z)
+    rel0 = _rel(s.accel(), O.ref_total_forces(pos, sg, M, L, theta, eps, r_cut, mf))
+    assert np.percentile(rel0, 99) <= 1e-5
+    s.close()
+
+
+def test_screening_is_refused_in_accurate_mode():
+    J, _ = _mods()
+    s = J.Solver(J.Config(box_L=32.0, pm_grid=16))
+    with pytest.raises(J.JanusError):
+        s.set_screening(2.0, 0.0)
+    s.set_screening(0.0, 0.0)
+    s.close()
+
+
 @pytest.mark.parametrize("n,M,L,mu", [(4096, 32, 32.0, 19.0), (8192, 64, 64.0, 1.0)])
 def test_accurate_matches_exact_split_model(n, M, L, mu):
     J, O = _mods()

@@ -104,6 +104,48 @@ def test_total_reference_force_matches_golden():
     assert rel.max() < 1e-5   # f64 FFT implementations differ in the last bits only
 
 
+def test_screened_walk_matches_golden():
+    g = load("screened_mixed_1100.npz")
+    pos, sg, L = g["pos"], g["signs"], float(g["L"])
+    tq, sq, il, bq = O.ref_screen_quantize(float(g["theta"]), float(g["eps"]), float(g["lambda_0"]),
+                                           float(g["z"]), L)
+    # rounding (screened packing) and truncation (erfc-split packing) differ here
+    assert (tq, sq) != O.ref_quantize(float(g["theta"]), float(g["eps"]), 5.0, L)[:2]
+    acc = np.zeros(3 * len(pos), np.float32)
+    for k, s in enumerate((1, -1)):
+        T = O.build_tree(np.ascontiguousarray(pos[sg == s]), np.float32(L / 2), float(g["mass_factor"]))
+        O.lib().orc_ref_screened_walk(pos.ravel(), sg, len(pos), s, T["node_pos"].ravel(),
+                                      T["node_mass"], T["left"], T["right"], T["types"],
+                                      tq, sq, il, bq, k, acc)
+    assert np.array_equal(acc.reshape(-1, 3), g["screened"])
+    tot = O.ref_total_forces_screened(pos, sg, int(g["M"]), L, float(g["theta"]), float(g["eps"]),
+                                      float(g["r_cut"]), float(g["mass_factor"]),
+                                      float(g["lambda_0"]), float(g["z"]))
+    rel = np.linalg.norm(tot - g["total"], axis=1) / np.linalg.norm(g["total"], axis=1)
+    assert rel.max() < 1e-5   # f64 FFT implementations differ in the last bits only
+
+
+def test_screening_limits():
+    """lambda_0 <= 0.01 is the unscreened erfc-split path; a huge lambda makes
+    the screening factor 1 (the plain full-range walk); tiny 1/lambda removes
+    nothing from same-sign pairs."""
+    rng = np.random.default_rng(2)
+    n, L = 600, 30.0
+    pos = ((rng.random((n, 3)) - 0.5) * L).astype(np.float32)
+    sg = np.where(rng.random(n) < 0.5, 1, -1).astype(np.int8)
+    a0 = O.ref_total_forces(pos, sg, 16, L, 0.5, 0.05, 5.0, 0.02)
+    a1 = O.ref_total_forces_screened(pos, sg, 16, L, 0.5, 0.05, 5.0, 0.02, 0.005, 0.0)
+    assert np.array_equal(a0, a1)
+    _, _, il, _ = O.ref_screen_quantize(0.5, 0.05, 6000.0, 0.0, L)
+    assert 0 < il < 2e-4
+    # screening weakens only the opposite-sign (repulsive) part: with all
+    # particles of one sign the result does not depend on lambda
+    one = np.ones(n, np.int8)
+    b1 = O.ref_total_forces_screened(pos, one, 16, L, 0.5, 0.05, 5.0, 0.02, 0.5, 0.0)
+    b2 = O.ref_total_forces_screened(pos, one, 16, L, 0.5, 0.05, 5.0, 0.02, 50.0, 3.0)
+    assert np.array_equal(b1, b2)
+
+
 # ---------------------------------------------------------------- 2. live reference
 needs_ref = pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built")
 
@@ -144,6 +186,28 @@ def test_walk_matches_reference_kernel_live():
         T = O.build_tree(np.ascontiguousarray(pos[sg == s]), np.float32(L / 2), mf)
         O.lib().orc_ref_short_range(pos.ravel(), sg, n, s, T["node_pos"].ravel(), T["node_mass"],
                                     T["left"], T["right"], T["types"], tq, sq, rq, bq, k, acc)
+    assert np.array_equal(acc.reshape(-1, 3), a_ref)
+
+
+@needs_ref
+@pytest.mark.parametrize("theta,eps,lam,z", [(0.6, 0.0305, 2.37, 1.5), (0.45, 0.1, 0.3, 0.0),
+                                            (0.7, 0.02, 6000.0, 9.0)])
+def test_screened_walk_matches_reference_kernel_live(theta, eps, lam, z):
+    import sys
+    sys.path.insert(0, GOLD)
+    from make_golden import ref_screened, ref_tree
+    rng = np.random.default_rng(13)
+    n, L, mf = 1000, 40.0, 0.1
+    pos = ((rng.random((n, 3)) - 0.5) * L).astype(np.float32)
+    sg = np.where(rng.random(n) < 0.5, 1, -1).astype(np.int8)
+    trees = [ref_tree(np.ascontiguousarray(pos[sg == s]), L / 2, mf) for s in (1, -1)]
+    a_ref = ref_screened(pos, sg, trees, theta, eps, lam, z, L)
+    tq, sq, il, bq = O.ref_screen_quantize(theta, eps, lam, z, L)
+    acc = np.zeros(3 * n, np.float32)
+    for k, s in enumerate((1, -1)):
+        T = O.build_tree(np.ascontiguousarray(pos[sg == s]), np.float32(L / 2), mf)
+        O.lib().orc_ref_screened_walk(pos.ravel(), sg, n, s, T["node_pos"].ravel(), T["node_mass"],
+                                      T["left"], T["right"], T["types"], tq, sq, il, bq, k, acc)
     assert np.array_equal(acc.reshape(-1, 3), a_ref)
 
 
