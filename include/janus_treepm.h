@@ -241,6 +241,34 @@ int  jt_snapshot_read(const char* path, jt_snapshot_meta* meta, double* box_L, d
  * softening); resume with jt_snapshot_read + jt_set_state_signed. */
 int  jt_checkpoint(jt_handle* h, const char* path, const jt_snapshot_meta* meta);
 
+/* Zel'dovich lattice initial conditions generated on the device (the host
+ * generator it replaces is the reference's generate_zeldovich_ics,
+ * src/ic_gen.rs:52-176, which builds the field with rustfft on the CPU).
+ * Per species an n_side^3 lattice of spacing a = box_L / n_side, the m-
+ * lattice offset by a/2 on every axis; displacements psi = i k / k^2 delta(k)
+ * of a Gaussian field with P(k) = A k^-2.5 exp(-(k/k_c)^2), k_c = pi / (2 a)
+ * (half the lattice Nyquist wavenumber), A such that rms |psi+| = rms_frac a;
+ * psi- = -psi evaluated on the offset lattice (delta- = -delta+); velocities
+ * v = vel_factor psi.  The white noise is Philox4x32-10 (counter = the cell
+ * index, key = seed) through Box-Muller in FP64; the Nyquist planes and k = 0
+ * are zero.  Rows are in lattice order iz n^2 + iy n + ix, AoS float3. */
+typedef struct jt_ics_params {
+    int      n_side;     /* lattice points per side per species, 4..1024 */
+    double   box_L;
+    uint64_t seed;
+    double   rms_frac;   /* rms displacement / lattice spacing (0.3) */
+    double   vel_factor; /* v = vel_factor * psi */
+} jt_ics_params;
+/* Into caller arrays of n_side^3 rows (host or device per mem; velocity
+ * pointers may be NULL); generated on the current device. */
+int  jt_ics_zeldovich(const jt_ics_params* p, float* pos_p, float* vel_p,
+                      float* pos_m, float* vel_m, int mem);
+/* Generate and load as the handle's state (as jt_set_state; no host copy). */
+int  jt_set_state_zeldovich(jt_handle* h, const jt_ics_params* p);
+/* The generator's counter-based stream on the host (Philox4x32-10 with 10
+ * rounds), for checks against its published known-answer vectors. */
+void jt_philox4x32_10(const unsigned ctr[4], const unsigned key[2], unsigned out[4]);
+
 /* Failure-path self test: runs the sort's bounded look-back wait on a
  * status word that nothing publishes, with `limit` polls (1..2^24).  Returns
  * JT_ETIMEDOUT with *timed_out = 1 when the wait gave up and reported it (the
@@ -277,6 +305,8 @@ int  jt_batch_add(jt_batch* b, const jt_config* cfg,
                   const float* pos_p, const float* vel_p, size_t n_p,
                   const float* pos_m, const float* vel_m, size_t n_m,
                   int mem, int* box_id);
+/* Add a box whose state is generated on the device (jt_ics_params). */
+int  jt_batch_add_zeldovich(jt_batch* b, const jt_config* cfg, const jt_ics_params* p, int* box_id);
 /* Free one box's device state; its id may be reused by a later add. */
 int  jt_batch_remove(jt_batch* b, int box_id);
 /* Accelerations of the listed boxes at their current positions (JT_PART_*). */

@@ -250,6 +250,8 @@ struct jt_walk_params {
     float eps2;
     float c;            // 1 / (2 r_s)
     float c2s;          // c^2 scaled to the walk's S table index (y / dy)
+    float slack;        // candidate prefilter: padding of the group's box
+    float rc2_keep;     // candidate prefilter: widened cut
     float mass[2];      // per-species particle mass (G folded in)
     int M;
     float h_inv;        // M / L

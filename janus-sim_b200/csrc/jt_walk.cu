@@ -292,10 +292,12 @@ __device__ __forceinline__ void drain_ranges(WalkWarpSmem& S, int nr, int& nc,
                                              float py, float pz, bool valid, const jt_walk_params& P,
                                              float fac, Acc3& near, unsigned& pairs,
                                              unsigned& cands, WalkCount& wc, float gcx, float gcy,
-                                             float gcz, const HalfTarget& H)
+                                             float gcz, float ghx, float ghy, float ghz,
+                                             const HalfTarget& H)
 {
     if (nr <= 0) return;
     wc.ranges += nr;
+    const unsigned lt = (1u << lane) - 1u;
     int2 r0 = S.rng[0];
     float4 nxt = lane < r0.y ? tpos[r0.x + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
     for (int r = 0; r < nr; r++) {
@@ -307,16 +309,34 @@ __device__ __forceinline__ void drain_ranges(WalkWarpSmem& S, int nr, int& nc,
             const int2 rn = S.rng[r + 1];
             nxt = lane < rn.y ? tpos[rn.x + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
         }
+        // keep only the candidates within r_cut of the group's AABB (no
+        // target can reach the others); the box is padded by P.slack and the
+        // cut by P.rc2_keep so that float rounding never drops a pair the
+        // evaluation would accept
+        const float4 c = make_float4(cur.x + sh.x, cur.y + sh.y, cur.z + sh.z, 0.f);
+        bool keep = false;
         if (lane < rr.y) {
-            const float4 c = make_float4(cur.x + sh.x, cur.y + sh.y, cur.z + sh.z, 0.f);
-            S.cand[nc + lane] = c;
+            float dx = c.x - gcx, dy = c.y - gcy, dz = c.z - gcz;
+            if (WRAP) {
+                dx = jt_wrap(dx, P.L, P.halfL);
+                dy = jt_wrap(dy, P.L, P.halfL);
+                dz = jt_wrap(dz, P.L, P.halfL);
+            }
+            const float gx = gap1(dx, ghx + P.slack), gy = gap1(dy, ghy + P.slack),
+                        gz = gap1(dz, ghz + P.slack);
+            keep = gx * gx + gy * gy + gz * gz <= P.rc2_keep;
+        }
+        const unsigned km = __ballot_sync(0xffffffffu, keep);
+        if (keep) {
+            const int at = nc + __popc(km & lt);
+            S.cand[at] = c;
             if (!WRAP && JT_WALK_HALF) {
-                S.hc[0][nc + lane] = __float2half_rn(c.x - gcx);
-                S.hc[1][nc + lane] = __float2half_rn(c.y - gcy);
-                S.hc[2][nc + lane] = __float2half_rn(c.z - gcz);
+                S.hc[0][at] = __float2half_rn(c.x - gcx);
+                S.hc[1][at] = __float2half_rn(c.y - gcy);
+                S.hc[2][at] = __float2half_rn(c.z - gcz);
             }
         }
-        nc += rr.y;
+        nc += __popc(km);
         __syncwarp();
         if (nc >= 32) {
             pairs += eval_chunk<WRAP>(S, 32, lane, px, py, pz, valid, P, fac, wc, near, H);
@@ -394,16 +414,22 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& 
             if (node >= 0) {
                 float lox, loy, loz, hix, hiy, hiz;
                 int first, count;
+                float4 cmv = make_float4(0.f, 0.f, 0.f, 0.f);
+                int2 chv = make_int2(0, 0);
                 if (node >= leaf0) {
                     first = (int)(node - leaf0);
                     count = 1;
                     float4 q = tpos[first];
                     lox = hix = q.x; loy = hiy = q.y; loz = hiz = q.z;
                 } else {
+                    // every array of an internal node is loaded at once: one
+                    // memory latency per traversal step instead of three
                     int2 r = A.pool.range[roff + node];
+                    float4 lo = A.pool.bmin[noff + node], hi = A.pool.bmax[noff + node];
+                    cmv = A.pool.com[noff + node];
+                    chv = A.pool.child[noff + node];
                     first = r.x;
                     count = r.y - r.x + 1;
-                    float4 lo = A.pool.bmin[noff + node], hi = A.pool.bmax[noff + node];
                     lox = lo.x; loy = lo.y; loz = lo.z; hix = hi.x; hiy = hi.y; hiz = hi.z;
                 }
                 float nhx = 0.5f * (hix - lox), nhy = 0.5f * (hiy - loy), nhz = 0.5f * (hiz - loz);
@@ -415,7 +441,7 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& 
                 if (gx * gx + gy * gy + gz * gz <= P.rc2) {
                     bool accepted = false;
                     if (count > 1) {
-                        float4 cm = A.pool.com[noff + node];
+                        const float4 cm = cmv;
                         float mx = jt_wrap(cm.x - gcx, P.L, P.halfL);
                         float my = jt_wrap(cm.y - gcy, P.L, P.halfL);
                         float mz = jt_wrap(cm.z - gcz, P.L, P.halfL);
@@ -439,7 +465,7 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& 
                                               rintf(((gcz + dz) - cz) / P.L), 0.f);
                         } else {
                             act = 1;
-                            ch = A.pool.child[noff + node];
+                            ch = chv;
                         }
                     }
                 }
@@ -475,7 +501,7 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& 
             __syncwarp();
             if (nR >= 32) {
                 drain_ranges<WRAP>(S, 32, nc, tpos, lane, p.x, p.y, p.z, valid, P, fac_direct, near,
-                                   pairs, cands, wc, gcx, gcy, gcz, H);
+                                   pairs, cands, wc, gcx, gcy, gcz, ghx, ghy, ghz, H);
                 __syncwarp();
                 int2 r2 = S.rng[32 + lane];
                 char4 s2 = S.rsh[32 + lane];
@@ -500,7 +526,7 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& 
             }
         }
         drain_ranges<WRAP>(S, nR, nc, tpos, lane, p.x, p.y, p.z, valid, P, fac_direct, near, pairs,
-                           cands, wc, gcx, gcy, gcz, H);
+                           cands, wc, gcx, gcy, gcz, ghx, ghy, ghz, H);
         __syncwarp();
         if (nc > 0) {
             pairs += eval_chunk<WRAP>(S, nc, lane, p.x, p.y, p.z, valid, P, fac_direct, wc, near, H);
@@ -533,6 +559,10 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_walk_acc(WalkArgs A)
     P.L = B.L; P.halfL = B.halfL; P.theta2 = B.theta2; P.rc2 = B.rc2; P.rc = sqrtf(B.rc2);
     P.eps2 = B.eps2; P.c = B.c; P.mass[0] = B.mass[0]; P.mass[1] = B.mass[1];
     P.c2s = B.c * B.c * ((float)kStab / kStabYMax);
+    // candidate prefilter margins: 8 ulp of the largest coordinate on the
+    // box, 1e-5 relative on the cut
+    P.slack = B.halfL * 9.5367431640625e-7f;
+    P.rc2_keep = B.rc2 * 1.00001f;
     P.M = B.M; P.h_inv = B.h_inv; P.order = ORDER; P.ngrid = NG; P.parts = A.parts;
     const int64_t ns = SG.n;
     const int64_t i = grp * 32 + lane;

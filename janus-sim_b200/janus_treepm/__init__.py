@@ -47,6 +47,7 @@ EXPORTED = [
     "jt_server_job_state", "jt_server_get_state", "jt_server_stats", "jt_server_job_need",
     "jt_walk_tuning", "jt_wait_probe", "jt_diagnostics", "jt_batch_diagnostics",
     "jt_snapshot_write", "jt_snapshot_read", "jt_checkpoint", "jt_set_screening",
+    "jt_ics_zeldovich", "jt_set_state_zeldovich", "jt_batch_add_zeldovich", "jt_philox4x32_10",
 ]
 JT_JOB_QUEUED, JT_JOB_RESIDENT, JT_JOB_DONE = 0, 1, 2
 JT_STATIC_SORT_MAX = 262144
@@ -139,6 +140,37 @@ def snapshot_read(path):
     return meta, box.value, mu.value, pos, vel, sg, mass, eps
 
 
+class jt_ics_params(C.Structure):
+    _fields_ = [("n_side", C.c_int), ("box_L", C.c_double), ("seed", C.c_uint64),
+                ("rms_frac", C.c_double), ("vel_factor", C.c_double)]
+
+
+def ics_params(n_side, box_L, seed=42, rms_frac=0.3, vel_factor=0.05):
+    p = jt_ics_params()
+    p.n_side, p.box_L, p.seed, p.rms_frac, p.vel_factor = n_side, box_L, seed, rms_frac, vel_factor
+    return p
+
+
+def zeldovich_device(n_side, box_L, seed=42, rms_frac=0.3, vel_factor=0.05):
+    """Zel'dovich lattice ICs generated on the current device; returns host
+    (pos_p, vel_p, pos_m, vel_m), n_side^3 rows each."""
+    n3 = n_side ** 3
+    out = [np.zeros((n3, 3), np.float32) for _ in range(4)]
+    p = ics_params(n_side, box_L, seed, rms_frac, vel_factor)
+    _check(library().jt_ics_zeldovich(C.byref(p), *[_ptr(a) for a in out], JT_MEM_HOST),
+           "jt_ics_zeldovich")
+    return tuple(out)
+
+
+def philox4x32_10(ctr, key):
+    """The IC generator's counter-based stream (host copy)."""
+    c = (C.c_uint * 4)(*ctr)
+    k = (C.c_uint * 2)(*key)
+    o = (C.c_uint * 4)()
+    library().jt_philox4x32_10(c, k, o)
+    return tuple(o)
+
+
 class jt_serve_stats(C.Structure):
     _fields_ = [
         ("requests_served", C.c_int64), ("batched_steps", C.c_int64), ("particle_steps", C.c_int64),
@@ -208,6 +240,12 @@ def library():
                                    C.POINTER(C.c_size_t)]
     L.jt_checkpoint.argtypes = [H, C.c_char_p, C.POINTER(jt_snapshot_meta)]
     L.jt_set_screening.argtypes = [H, C.c_double, C.c_double]
+    L.jt_ics_zeldovich.argtypes = [C.POINTER(jt_ics_params), fp, fp, fp, fp, C.c_int]
+    L.jt_set_state_zeldovich.argtypes = [H, C.POINTER(jt_ics_params)]
+    L.jt_batch_add_zeldovich.argtypes = [C.c_void_p, C.POINTER(jt_config), C.POINTER(jt_ics_params),
+                                         C.POINTER(C.c_int)]
+    L.jt_philox4x32_10.argtypes = [C.POINTER(C.c_uint), C.POINTER(C.c_uint), C.POINTER(C.c_uint)]
+    L.jt_philox4x32_10.restype = None
     L.jt_batch_diagnostics.argtypes = [H, C.c_int, C.c_int, C.POINTER(jt_diag)]
     L.jt_batch_trim.argtypes = [H]
     L.jt_batch_set_graphs.argtypes = [H, C.c_int]
@@ -333,6 +371,14 @@ class Solver:
         self._signed = True
         n_p = int((signs > 0).sum())
         self.n = (n_p, len(signs) - n_p)
+
+    def set_state_zeldovich(self, n_side, seed=42, rms_frac=0.3, vel_factor=0.05):
+        """Zel'dovich lattice ICs generated on the device as the state (box_L
+        from the config)."""
+        p = ics_params(n_side, self.config.box_L, seed, rms_frac, vel_factor)
+        _check(library().jt_set_state_zeldovich(self._h, C.byref(p)), "jt_set_state_zeldovich")
+        self._signed = False
+        self.n = (n_side ** 3, n_side ** 3)
 
     def set_state_device(self, pos_p, vel_p, pos_m, vel_m):
         """Device (torch CUDA float32 (n,3) contiguous) tensors; vel may be None."""
@@ -499,6 +545,16 @@ class Batch:
                                       _ptr(pos_m), _ptr(vel_m), len(pos_m), JT_MEM_HOST,
                                       C.byref(bid)), "jt_batch_add")
         self.boxes[bid.value] = (len(pos_p), len(pos_m))
+        return bid.value
+
+    def add_zeldovich(self, config: Config, n_side, seed=42, rms_frac=0.3, vel_factor=0.05):
+        """Add a box whose Zel'dovich lattice ICs are generated on the device."""
+        cfg = config.resolved().to_c()
+        p = ics_params(n_side, config.box_L, seed, rms_frac, vel_factor)
+        bid = C.c_int(-1)
+        _check(library().jt_batch_add_zeldovich(self._b, C.byref(cfg), C.byref(p), C.byref(bid)),
+               "jt_batch_add_zeldovich")
+        self.boxes[bid.value] = (n_side ** 3, n_side ** 3)
         return bid.value
 
     def remove(self, box_id):

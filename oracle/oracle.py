@@ -289,3 +289,72 @@ def segregation_metrics(pos, signs, box, n_cells):
     var_mc = np.mean((n_minus - mm) ** 2)
     exc = (var_mc - mm) / mm if mm > 0 else 0.0
     return float(dop), float(corr), float(exc)
+
+
+# ---------------------------------------------------------------- Zel'dovich ICs
+def philox4x32_10(c0, c1, c2, c3, k0, k1):
+    """Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11), vectorised over
+    uint32 counter arrays; keys are Python ints."""
+    M0, M1 = np.uint64(0xD2511F53), np.uint64(0xCD9E8D57)
+    c = [np.asarray(x, np.uint32) for x in (c0, c1, c2, c3)]
+    for _ in range(10):
+        p0 = M0 * c[0].astype(np.uint64)
+        p1 = M1 * c[2].astype(np.uint64)
+        hi0, lo0 = (p0 >> np.uint64(32)).astype(np.uint32), (p0 & np.uint64(0xFFFFFFFF)).astype(np.uint32)
+        hi1, lo1 = (p1 >> np.uint64(32)).astype(np.uint32), (p1 & np.uint64(0xFFFFFFFF)).astype(np.uint32)
+        c = [hi1 ^ c[1] ^ np.uint32(k0), lo1, hi0 ^ c[3] ^ np.uint32(k1), lo0]
+        k0 = (k0 + 0x9E3779B9) & 0xFFFFFFFF
+        k1 = (k1 + 0xBB67AE85) & 0xFFFFFFFF
+    return c
+
+
+def zeldovich_philox(n, L, seed=42, rms_frac=0.3, vel_factor=0.05):
+    """FP64 restatement of the device Zel'dovich lattice generator: the same
+    Philox noise per cell (counter = cell index, key = seed; Box-Muller), the
+    spectrum P(k) = A k^-2.5 exp(-(k/k_c)^2) with k_c = pi / (2 a), psi = i k
+    / k^2 delta(k) with k = 0 and the Nyquist planes zeroed, psi- = -psi on
+    the lattice offset by a/2, rms |psi+| = rms_frac a, v = vel_factor psi.
+    Returns (pos_p, vel_p, pos_m, vel_m) as float64 (n^3, 3) arrays, rows in
+    lattice order iz n^2 + iy n + ix."""
+    n3 = n ** 3
+    idx = np.arange(n3, dtype=np.uint64)
+    r = philox4x32_10((idx & np.uint64(0xFFFFFFFF)).astype(np.uint32),
+                      (idx >> np.uint64(32)).astype(np.uint32), np.zeros(n3, np.uint32),
+                      np.zeros(n3, np.uint32), seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF)
+    u0 = (r[0].astype(np.float64) + 0.5) * 2.0 ** -32
+    u1 = (r[1].astype(np.float64) + 0.5) * 2.0 ** -32
+    noise = (np.sqrt(-2.0 * np.log(u0)) * np.cos(2.0 * np.pi * u1)).astype(np.float32)
+    dk = np.fft.rfftn(noise.reshape(n, n, n).astype(np.float64))
+    a = L / n
+    kf = 2.0 * np.pi / L
+    k1 = kf * np.where(np.arange(n) <= (n - 1) // 2, np.arange(n), np.arange(n) - n)
+    kr = kf * np.arange(n // 2 + 1)
+    kz, ky, kx = k1[:, None, None], k1[None, :, None], kr[None, None, :]
+    k2 = kz * kz + ky * ky + kx * kx
+    kc = 0.5 * np.pi / a
+    with np.errstate(divide="ignore", invalid="ignore"):
+        amp = np.where(k2 > 0, k2 ** -0.625 * np.exp(-0.5 * k2 / kc ** 2), 0.0)
+        inv = np.where(k2 > 0, 1.0 / k2, 0.0)
+    if n % 2 == 0:
+        nyq = np.zeros((n, n, n // 2 + 1), bool)
+        nyq[n // 2, :, :] = True
+        nyq[:, n // 2, :] = True
+        nyq[:, :, n // 2] = True
+        amp = np.where(nyq, 0.0, amp)
+    shift = np.exp(1j * 0.5 * a * (kx + ky + kz))
+    psi = {}
+    for name, kc_ in (("x", kx), ("y", ky), ("z", kz)):
+        pk = 1j * kc_ * inv * amp * dk
+        psi["p" + name] = np.fft.irfftn(pk, s=(n, n, n), axes=(0, 1, 2)).ravel()
+        psi["m" + name] = -np.fft.irfftn(pk * shift, s=(n, n, n), axes=(0, 1, 2)).ravel()
+    rms = np.sqrt(np.mean(psi["px"] ** 2 + psi["py"] ** 2 + psi["pz"] ** 2))
+    scale = rms_frac * a / rms if rms > 0 else 0.0
+    i = np.arange(n3)
+    lat = np.stack([i % n, (i // n) % n, i // (n * n)], -1).astype(np.float64)
+    out = []
+    for sp, off in (("p", 0.0), ("m", 0.5 * a)):
+        d = np.stack([psi[sp + "x"], psi[sp + "y"], psi[sp + "z"]], -1) * scale
+        pos = (lat + 0.5) * a - 0.5 * L + off + d
+        pos = (pos + 0.5 * L) % L - 0.5 * L
+        out += [pos, vel_factor * d]
+    return tuple(out)
