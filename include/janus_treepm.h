@@ -241,6 +241,31 @@ int  jt_snapshot_read(const char* path, jt_snapshot_meta* meta, double* box_L, d
  * softening); resume with jt_snapshot_read + jt_set_state_signed. */
 int  jt_checkpoint(jt_handle* h, const char* path, const jt_snapshot_meta* meta);
 
+/* Energies in FP64 on the device, the reference's GpuNBodyTwoPass
+ * diagnostics (src/nbody_gpu_twopass.rs) without the host copy of the state:
+ *   kinetic    = sum |v|^2 / 2 over all particles, unit masses
+ *                (kinetic_energy, :5070-5077);
+ *   pe_plus / pe_minus = per species, a stride sample of at most n_sample
+ *                particles (rows i * (n_s / n_sample) of the species array),
+ *                -sum_{i<j} 1 / sqrt(r^2 + eps^2) with plain (non-periodic)
+ *                differences, times n_s (n_s - 1) / (ns (ns - 1))
+ *                (potential_energy_binding_sampled, :5081-5181);
+ *   pe_binding = pe_plus + pe_minus (same-species pairs only). */
+typedef struct jt_energy {
+    double  kinetic;
+    double  pe_binding;
+    double  pe_plus, pe_minus;
+    int64_t n_sampled[2];
+} jt_energy;
+int  jt_energy_sampled(jt_handle* h, size_t n_sample, jt_energy* out);
+/* virialize_sampled (:5186-5225): multiply every velocity by alpha =
+ * sqrt(|pe_binding| / (2 kinetic)) when pe_binding < 0 and kinetic >= 1e-20
+ * (else alpha = 1 and nothing changes); *alpha (may be NULL) receives it. */
+int  jt_virialize_sampled(jt_handle* h, size_t n_sample, double* alpha);
+/* energy_drift_pct (src/janus_expansion.rs:529-534): (e_now - e_initial) /
+ * |e_initial| * 100, 0 when |e_initial| < 1e-30. */
+double jt_energy_drift_pct(double e_now, double e_initial);
+
 /* Zel'dovich lattice initial conditions generated on the device (the host
  * generator it replaces is the reference's generate_zeldovich_ics,
  * src/ic_gen.rs:52-176, which builds the field with rustfft on the CPU).

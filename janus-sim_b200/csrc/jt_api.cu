@@ -902,6 +902,33 @@ int jt_debug_tree(jt_handle* h, int species, uint32_t* morton, int32_t* perm, in
 
 }  // extern "C"
 
+namespace {
+__global__ void k_scale_vel4(float4* __restrict__ v, int64_t n, float a)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 q = v[i];
+    q.x *= a;
+    q.y *= a;
+    q.z *= a;
+    v[i] = q;
+}
+}  // namespace
+
+// Multiply every velocity by a, in place (internal order: the product does
+// not depend on it).
+int jth_scale_velocities(jt_handle* h, float a)
+{
+    if (!h || !h->have_state) return JT_ESTATE;
+    Parts P = parts_of(h);
+    for (int s = 0; s < 2; s++)
+        if (h->n[s] > 0)
+            k_scale_vel4<<<(unsigned)((h->n[s] + 255) / 256), 256, 0, h->st>>>(P.vel[s], h->n[s], a);
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(h->st) != cudaSuccess) return JT_ECUDA;
+    h->tm.launches += (h->n[0] > 0) + (h->n[1] > 0);
+    return JT_OK;
+}
+
 int jth_info(jt_handle* h, jt_config* cfg, float* m_plus, float* m_minus, int8_t* signs)
 {
     if (!h) return JT_EINVAL;

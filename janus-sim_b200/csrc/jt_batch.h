@@ -45,6 +45,7 @@ int64_t jtb_phase(jt_batch* B, int i);
 // a box that was moved to host memory without recomputing its forces.
 // A handle's config, per-species particle masses and the signs of its
 // caller-order array (jt_api.cu)
+int jth_scale_velocities(jt_handle* h, float a);
 int jth_info(jt_handle* h, jt_config* cfg, float* m_plus, float* m_minus, int8_t* signs);
 // FP64 diagnostics of one state (jt_diag.cu)
 int jt_diag_state(const float4* const pos[2], const float4* const vel[2], const int64_t n[2],

@@ -48,6 +48,7 @@ EXPORTED = [
     "jt_walk_tuning", "jt_wait_probe", "jt_diagnostics", "jt_batch_diagnostics",
     "jt_snapshot_write", "jt_snapshot_read", "jt_checkpoint", "jt_set_screening",
     "jt_ics_zeldovich", "jt_set_state_zeldovich", "jt_batch_add_zeldovich", "jt_philox4x32_10",
+    "jt_energy_sampled", "jt_virialize_sampled", "jt_energy_drift_pct",
 ]
 JT_JOB_QUEUED, JT_JOB_RESIDENT, JT_JOB_DONE = 0, 1, 2
 JT_STATIC_SORT_MAX = 262144
@@ -138,6 +139,19 @@ def snapshot_read(path):
     _check(L.jt_snapshot_read(str(path).encode(), C.byref(meta), C.byref(box), C.byref(mu), _ptr(pos),
                               _ptr(vel), _ptr(sg), _ptr(mass), _ptr(eps), k, C.byref(n)), "jt_snapshot_read")
     return meta, box.value, mu.value, pos, vel, sg, mass, eps
+
+
+class jt_energy(C.Structure):
+    _fields_ = [("kinetic", C.c_double), ("pe_binding", C.c_double), ("pe_plus", C.c_double),
+                ("pe_minus", C.c_double), ("n_sampled", C.c_int64 * 2)]
+
+    def to_dict(self):
+        return dict(kinetic=self.kinetic, pe_binding=self.pe_binding, pe_plus=self.pe_plus,
+                    pe_minus=self.pe_minus, n_sampled=tuple(self.n_sampled))
+
+
+def energy_drift_pct(e_now, e_initial):
+    return library().jt_energy_drift_pct(e_now, e_initial)
 
 
 class jt_ics_params(C.Structure):
@@ -246,6 +260,10 @@ def library():
                                          C.POINTER(C.c_int)]
     L.jt_philox4x32_10.argtypes = [C.POINTER(C.c_uint), C.POINTER(C.c_uint), C.POINTER(C.c_uint)]
     L.jt_philox4x32_10.restype = None
+    L.jt_energy_sampled.argtypes = [H, C.c_size_t, C.POINTER(jt_energy)]
+    L.jt_virialize_sampled.argtypes = [H, C.c_size_t, C.POINTER(C.c_double)]
+    L.jt_energy_drift_pct.argtypes = [C.c_double, C.c_double]
+    L.jt_energy_drift_pct.restype = C.c_double
     L.jt_batch_diagnostics.argtypes = [H, C.c_int, C.c_int, C.POINTER(jt_diag)]
     L.jt_batch_trim.argtypes = [H]
     L.jt_batch_set_graphs.argtypes = [H, C.c_int]
@@ -265,7 +283,8 @@ def library():
     L.jt_server_job_need.argtypes = [C.POINTER(jt_config), C.c_size_t, C.c_size_t, C.POINTER(C.c_size_t)]
     for name in EXPORTED:
         if name not in ("jt_destroy", "jt_strerror", "jt_version", "jt_batch_destroy",
-                        "jt_server_destroy", "jt_server_clock"):
+                        "jt_server_destroy", "jt_server_clock", "jt_philox4x32_10",
+                        "jt_energy_drift_pct"):
             getattr(L, name).restype = C.c_int
     _lib = L
     return L
@@ -461,6 +480,18 @@ class Solver:
         d = jt_diag()
         _check(library().jt_diagnostics(self._h, n_cells, C.byref(d)), "jt_diagnostics")
         return d.to_dict()
+
+    def energy(self, n_sample=20000):
+        """FP64 kinetic energy and sampled same-species binding energy."""
+        e = jt_energy()
+        _check(library().jt_energy_sampled(self._h, n_sample, C.byref(e)), "jt_energy_sampled")
+        return e.to_dict()
+
+    def virialize(self, n_sample=20000):
+        """Scale velocities to 2 KE = |PE_binding|; returns alpha."""
+        a = C.c_double(1.0)
+        _check(library().jt_virialize_sampled(self._h, n_sample, C.byref(a)), "jt_virialize_sampled")
+        return a.value
 
     def walk_counters(self):
         """(iterations, ranges, chunks, trips) of a -DJT_WALK_COUNT build."""

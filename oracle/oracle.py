@@ -358,3 +358,34 @@ def zeldovich_philox(n, L, seed=42, rms_frac=0.3, vel_factor=0.05):
         pos = (pos + 0.5 * L) % L - 0.5 * L
         out += [pos, vel_factor * d]
     return tuple(out)
+
+
+# ---------------------------------------------------------------- energies
+def kinetic_energy_unit(vel_p, vel_m):
+    """kinetic_energy (src/nbody_gpu_twopass.rs:5070-5077): sum |v|^2 / 2 over
+    every particle, unit masses, f64."""
+    v = np.concatenate([np.asarray(vel_p, np.float64), np.asarray(vel_m, np.float64)])
+    return float(0.5 * np.sum(v * v))
+
+
+def pe_binding_sampled(pos_p, pos_m, n_sample, softening):
+    """potential_energy_binding_sampled (src/nbody_gpu_twopass.rs:5081-5181):
+    per species rows i * (n / n_sample) (all rows when n <= n_sample), the
+    pair sum -sum_{i<j} 1/sqrt(r^2 + eps^2) with plain differences in f64,
+    times n (n - 1) / (ns (ns - 1)).  Returns (pe_plus, pe_minus)."""
+    out = []
+    for pos in (pos_p, pos_m):
+        pos = np.asarray(pos, np.float64)
+        n = len(pos)
+        if n == 0:
+            out.append(0.0)
+            continue
+        sample = pos if n <= n_sample else pos[np.arange(n_sample) * (n // n_sample)]
+        ns = len(sample)
+        pe = 0.0
+        for i in range(ns - 1):
+            d = sample[i + 1:] - sample[i]
+            pe -= np.sum(1.0 / np.sqrt(np.sum(d * d, axis=1) + softening * softening))
+        scale = (n * (n - 1.0)) / (ns * (ns - 1.0)) if ns > 1 else 1.0
+        out.append(pe * scale)
+    return tuple(out)
