@@ -241,6 +241,17 @@ int  jt_snapshot_read(const char* path, jt_snapshot_meta* meta, double* box_L, d
  * softening); resume with jt_snapshot_read + jt_set_state_signed. */
 int  jt_checkpoint(jt_handle* h, const char* path, const jt_snapshot_meta* meta);
 
+/* The production driver's raw snapshot (save_snapshot,
+ * src/bin/janus_mu19_production.rs:198-216): u32 n, f32 box, u32 step, f32 z,
+ * then n records of f32 pos[3], f32 vel[3], i8 sign (25 bytes, little-endian,
+ * no padding).  read: pos == NULL only reads the header into n/box/step/z;
+ * otherwise cap >= n rows are filled (vel may be NULL). */
+int  jt_snapshot_write_raw(const char* path, const float* pos, const float* vel,
+                           const int8_t* signs, size_t n, double box_L, uint32_t step,
+                           double z);
+int  jt_snapshot_read_raw(const char* path, float* pos, float* vel, int8_t* signs,
+                          size_t cap, size_t* n, double* box_L, uint32_t* step, double* z);
+
 /* Energies in FP64 on the device, the reference's GpuNBodyTwoPass
  * diagnostics (src/nbody_gpu_twopass.rs) without the host copy of the state:
  *   kinetic    = sum |v|^2 / 2 over all particles, unit masses
@@ -332,6 +343,17 @@ int  jt_batch_add(jt_batch* b, const jt_config* cfg,
                   int mem, int* box_id);
 /* Add a box whose state is generated on the device (jt_ics_params). */
 int  jt_batch_add_zeldovich(jt_batch* b, const jt_config* cfg, const jt_ics_params* p, int* box_id);
+/* Checkpoint one box to a snapshot_v3 file (rows [m+ ; m-] in the caller's
+ * order) without waiting for it: the state is gathered on the batch's stream,
+ * copied to pinned host memory on a side stream and written by a host
+ * thread, so a jt_batch_step issued right after overlaps the copy and the
+ * write.  One checkpoint per batch in flight (JT_EBUSY until collected);
+ * jt_batch_checkpoint_wait collects it and returns the write's status (JT_OK
+ * when none is pending).  The reference's snapshots block on a full
+ * device-to-host copy (src/snapshot_v3.rs:260-376). */
+int  jt_batch_checkpoint_async(jt_batch* b, int box_id, const char* path,
+                               const jt_snapshot_meta* meta);
+int  jt_batch_checkpoint_wait(jt_batch* b);
 /* Free one box's device state; its id may be reused by a later add. */
 int  jt_batch_remove(jt_batch* b, int box_id);
 /* Accelerations of the listed boxes at their current positions (JT_PART_*). */

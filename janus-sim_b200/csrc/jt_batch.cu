@@ -168,6 +168,7 @@ float elapsed(cudaEvent_t a, cudaEvent_t b)
 
 struct jt_batch {
     int device = 0;
+    jt_ckpt* ckpt = nullptr;            // asynchronous checkpoint (jt_ckpt.cu)
     cudaStream_t st = nullptr;
     AllocCtx actx;                      // its memory pool and stream
     Pool<float> stage;                  // host <-> device staging of AoS arrays
@@ -853,6 +854,7 @@ void jtb_reset_timings(jt_batch* B)
     if (B) B->tm = jt_timings{};
 }
 
+jt_ckpt** jtb_ckpt_slot(jt_batch* B) { return &B->ckpt; }
 int64_t jtb_phase(jt_batch* B, int i) { return B && i >= 0 && i < 4 ? B->phase[i] : 0; }
 
 int jtb_set_accel(jt_batch* B, int box_id, const float* acc_p, const float* acc_m, int mem)
@@ -926,6 +928,7 @@ void jt_batch_destroy(jt_batch* B)
 {
     if (!B) return;
     AllocScope scope(&B->actx);
+    jt_ckpt_release(B->ckpt);
     if (B->st) cudaStreamSynchronize(B->st);
     for (auto* b : B->boxes)
         if (b) { box_release(b); delete b; }

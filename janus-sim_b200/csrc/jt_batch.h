@@ -29,6 +29,10 @@ struct jt_box_step {
 // batch's stream); n_p + n_m > 0.  The config must be ACCURATE.
 int jtb_add_empty(jt_batch* B, const jt_config* cfg, int64_t n_p, int64_t n_m, int* box_id);
 jt_box_state* jtb_box(jt_batch* B, int box_id);
+// the batch's asynchronous-checkpoint state (jt_ckpt.cu), released on destroy
+struct jt_ckpt;
+jt_ckpt** jtb_ckpt_slot(jt_batch* B);
+void jt_ckpt_release(jt_ckpt* c);
 cudaStream_t jtb_stream(jt_batch* B);
 // Enqueue one force pass (sort, trees, PM, walk) over the listed boxes;
 // kick_frac != 0 fuses the closing kick (kick_frac * dt) into the walk.  No

@@ -49,6 +49,8 @@ EXPORTED = [
     "jt_snapshot_write", "jt_snapshot_read", "jt_checkpoint", "jt_set_screening",
     "jt_ics_zeldovich", "jt_set_state_zeldovich", "jt_batch_add_zeldovich", "jt_philox4x32_10",
     "jt_energy_sampled", "jt_virialize_sampled", "jt_energy_drift_pct",
+    "jt_batch_checkpoint_async", "jt_batch_checkpoint_wait", "jt_snapshot_write_raw",
+    "jt_snapshot_read_raw",
 ]
 JT_JOB_QUEUED, JT_JOB_RESIDENT, JT_JOB_DONE = 0, 1, 2
 JT_STATIC_SORT_MAX = 262144
@@ -185,6 +187,28 @@ def philox4x32_10(ctr, key):
     return tuple(o)
 
 
+def snapshot_write_raw(path, pos, vel, signs, box_L, step, z):
+    """The production driver's raw snapshot (25-byte records)."""
+    pos = _f32(pos)
+    vel = None if vel is None else _f32(vel)
+    signs = np.ascontiguousarray(signs, np.int8)
+    _check(library().jt_snapshot_write_raw(str(path).encode(), _ptr(pos), _ptr(vel), _ptr(signs),
+                                           len(pos), box_L, step, z), "jt_snapshot_write_raw")
+
+
+def snapshot_read_raw(path):
+    """(pos, vel, signs, box_L, step, z) of a raw snapshot."""
+    L = library()
+    n, box, st, z = C.c_size_t(), C.c_double(), C.c_uint32(), C.c_double()
+    _check(L.jt_snapshot_read_raw(str(path).encode(), None, None, None, 0, C.byref(n), C.byref(box),
+                                  C.byref(st), C.byref(z)), "jt_snapshot_read_raw")
+    k = n.value
+    pos, vel, sg = np.zeros((k, 3), np.float32), np.zeros((k, 3), np.float32), np.zeros(k, np.int8)
+    _check(L.jt_snapshot_read_raw(str(path).encode(), _ptr(pos), _ptr(vel), _ptr(sg), k, C.byref(n),
+                                  C.byref(box), C.byref(st), C.byref(z)), "jt_snapshot_read_raw")
+    return pos, vel, sg, box.value, st.value, z.value
+
+
 class jt_serve_stats(C.Structure):
     _fields_ = [
         ("requests_served", C.c_int64), ("batched_steps", C.c_int64), ("particle_steps", C.c_int64),
@@ -264,6 +288,13 @@ def library():
     L.jt_virialize_sampled.argtypes = [H, C.c_size_t, C.POINTER(C.c_double)]
     L.jt_energy_drift_pct.argtypes = [C.c_double, C.c_double]
     L.jt_energy_drift_pct.restype = C.c_double
+    L.jt_batch_checkpoint_async.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.POINTER(jt_snapshot_meta)]
+    L.jt_batch_checkpoint_wait.argtypes = [C.c_void_p]
+    L.jt_snapshot_write_raw.argtypes = [C.c_char_p, fp, fp, vp, C.c_size_t, C.c_double, C.c_uint32,
+                                        C.c_double]
+    L.jt_snapshot_read_raw.argtypes = [C.c_char_p, fp, fp, vp, C.c_size_t, C.POINTER(C.c_size_t),
+                                       C.POINTER(C.c_double), C.POINTER(C.c_uint32),
+                                       C.POINTER(C.c_double)]
     L.jt_batch_diagnostics.argtypes = [H, C.c_int, C.c_int, C.POINTER(jt_diag)]
     L.jt_batch_trim.argtypes = [H]
     L.jt_batch_set_graphs.argtypes = [H, C.c_int]
@@ -577,6 +608,16 @@ class Batch:
                                       C.byref(bid)), "jt_batch_add")
         self.boxes[bid.value] = (len(pos_p), len(pos_m))
         return bid.value
+
+    def checkpoint_async(self, box_id, path, meta=None):
+        """Start a snapshot_v3 checkpoint of one box that overlaps the next
+        step; collect it with checkpoint_wait()."""
+        meta = meta if meta is not None else snapshot_meta()
+        _check(library().jt_batch_checkpoint_async(self._b, box_id, str(path).encode(), C.byref(meta)),
+               "jt_batch_checkpoint_async")
+
+    def checkpoint_wait(self):
+        _check(library().jt_batch_checkpoint_wait(self._b), "jt_batch_checkpoint_wait")
 
     def add_zeldovich(self, config: Config, n_side, seed=42, rms_frac=0.3, vel_factor=0.05):
         """Add a box whose Zel'dovich lattice ICs are generated on the device."""

@@ -192,3 +192,41 @@ def test_graph_replay_matches_plain_launches():
                 assert float(d.max()) <= VEL_TOL * rms, (k, q, float(d.max()), rms)
     A.close()
     G.close()
+
+
+def test_async_checkpoint_overlaps_the_next_step(tmp_path):
+    """A checkpoint started before a step holds the state before it, and the
+    step's result is the same as without the checkpoint."""
+    import janus_treepm as J
+    rng = np.random.default_rng(21)
+    L, n = 50.0, 6000
+    cfg = J.Config(box_L=L, pm_grid=32, softening=0.05, mu=3.0)
+    st = []
+    for _ in range(2):
+        st.append([((rng.random((n, 3)) - 0.5) * L).astype(np.float32), rng.normal(0, 0.3, (n, 3)).astype(np.float32),
+                   ((rng.random((n // 2, 3)) - 0.5) * L).astype(np.float32),
+                   rng.normal(0, 0.3, (n // 2, 3)).astype(np.float32)])
+    B = J.Batch()
+    ids = [B.add(cfg, *s) for s in st]
+    B.step(ids, 0.01, 0.0, 1.0, 2)
+    before = B.get_state(ids[0])
+    path = tmp_path / "ck.bin"
+    B.checkpoint_async(ids[0], path, J.snapshot_meta(run_label="async"))
+    B.step(ids, 0.01, 0.0, 1.0, 1)
+    B.checkpoint_wait()
+    after = B.get_state(ids[0])
+    meta, L2, mu2, pos, vel, sg, mass, eps = J.snapshot_read(path)
+    assert meta.run_label == b"async" and L2 == L and mu2 == 3.0
+    assert np.array_equal(pos, np.concatenate([before[0], before[2]]))
+    assert np.array_equal(vel, np.concatenate([before[1], before[3]]))
+    assert np.array_equal(sg, np.concatenate([np.ones(n, np.int8), -np.ones(n // 2, np.int8)]))
+    # the same step from the saved state without a checkpoint in flight
+    B2 = J.Batch()
+    i2 = [B2.add(cfg, *s) for s in st]
+    B2.step(i2, 0.01, 0.0, 1.0, 2)
+    B2.step(i2, 0.01, 0.0, 1.0, 1)
+    ref = B2.get_state(i2[0])
+    for x, y in zip(after, ref):
+        assert np.abs(x - y).max() <= 1e-5 * max(1.0, np.abs(y).max())
+    B.close()
+    B2.close()

@@ -69,3 +69,21 @@ def test_bad_magic_is_rejected(tmp_path):
     n = C.c_size_t()
     assert L.jt_snapshot_read(str(path).encode(), None, None, None, None, None, None, None, None, 0,
                               C.byref(n)) == J.JT_EINVAL
+
+
+def test_raw_driver_format(tmp_path):
+    """save_snapshot of the production driver
+    (src/bin/janus_mu19_production.rs:198-216): 16-byte header, 25-byte
+    records."""
+    pos, vel, sg, _, _ = _particles(333, seed=9)
+    path = tmp_path / "raw.bin"
+    J.snapshot_write_raw(path, pos, vel, sg, 250.0, 1234, 3.5)
+    raw = path.read_bytes()
+    assert len(raw) == 16 + 25 * 333
+    assert struct.unpack("<IfIf", raw[:16]) == (333, 250.0, 1234, 3.5)
+    rec = np.frombuffer(raw[16:], dtype=np.dtype([("pos", "<f4", 3), ("vel", "<f4", 3), ("sign", "i1")]))
+    assert np.array_equal(rec["pos"], pos) and np.array_equal(rec["vel"], vel)
+    assert np.array_equal(rec["sign"], sg)
+    p2, v2, s2, box, step, z = J.snapshot_read_raw(path)
+    assert (box, step, z) == (250.0, 1234, 3.5)
+    assert np.array_equal(p2, pos) and np.array_equal(v2, vel) and np.array_equal(s2, sg)
