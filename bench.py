@@ -441,24 +441,30 @@ def run_ours(args, ws, rank, local):
     K = args.steps
     value = ws * 2 * n * K / (dev_ms * 1e-3)
 
-    # end to end through the C ABI with pinned host buffers: upload the state,
-    # one step, read the state back, every step
+    # end to end through the C ABI with pinned host buffers: every step
+    # uploads the state a KDK step starts from (positions, velocities and the
+    # accelerations at those positions), steps once, and reads the same three
+    # back into pinned buffers, which the next step uploads again
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
-    hp, hvp, hm, hvm = pin(pp), pin(vp), pin(pm), pin(vm)
-    op = [pin(np.zeros_like(pp)) for _ in range(4)]
-    s.set_state(hp, hvp, hm, hvm)
+    cur = [pin(a) for a in (pp, vp, pm, vm)]
+    acc = [pin(np.zeros_like(pp)), pin(np.zeros_like(pm))]
+    s.set_state(*cur)
     s.step(w["dt"], H, 1.0, 1)
+    s.get_state(out=cur)
+    s.get_accel(out=acc)
     barrier()
     t0 = time.perf_counter()
     for _ in range(K):
-        s.set_state(hp, hvp, hm, hvm)
+        s.set_state(*cur)
+        s.set_accel(*acc)
         s.step(w["dt"], H, 1.0, 1)
-        a, b, c, d = s.get_state()
+        s.get_state(out=cur)
+        s.get_accel(out=acc)
     barrier()
     e2e_t = time.perf_counter() - t0
     e2e_t = max_over_ranks(e2e_t, ws, "cuda")
     e2e = ws * 2 * n * K / e2e_t
-    bytes_state = 2 * n * 3 * 4 * 2     # positions + velocities, both species
+    bytes_state = 2 * n * 3 * 4 * 3     # positions, velocities, accelerations; both species
 
     # roofline of the dominant kernel: the walk (FP32 pipe)
     walk_ms = stages["walk_ms"] / K

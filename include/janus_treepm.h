@@ -149,6 +149,16 @@ int  jt_accel_part(jt_handle* h, int part, float* acc_p, float* acc_m, int mem);
  * dtau_per_dt) (:4486-4649); r_cut comes from the config. */
 int  jt_step(jt_handle* h, double dt, double hubble, double dtau_per_dt, int nsteps);
 
+/* The accelerations a KDK step starts from, as part of the state: jt_get_accel
+ * reads the stored ones (at the current positions, as the last step or
+ * force call left them; JT_ESTATE when there are none) without computing
+ * anything, and jt_set_accel loads them after jt_set_state, so that a state
+ * taken out with jt_get_state + jt_get_accel and put back steps on without an
+ * extra force pass (the reference's DKD step needs none: it keeps no forces
+ * between steps).  Per-species layout only. */
+int  jt_set_accel(jt_handle* h, const float* acc_p, const float* acc_m, int mem);
+int  jt_get_accel(jt_handle* h, float* acc_p, float* acc_m, int mem);
+
 /* Yukawa screening of opposite-sign pairs: the reference's set_lambda_0 /
  * set_current_z (src/nbody_gpu_twopass.rs:2305-2312) as its TreePM step uses
  * them (compute_short_range_forces, :3997-4068).  With lambda_0 > 0.01 the

@@ -441,6 +441,16 @@ void set_masses(jt_handle* h)
     h->mass[1] = (float)mm;
 }
 
+// dst[i] = AoS row id[i] of src (caller order -> internal order)
+__global__ void k_aos_gather(const float* __restrict__ src, const int* __restrict__ id, int64_t n,
+                             float4* __restrict__ dst)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t k = 3 * (int64_t)id[i];
+    dst[i] = make_float4(src[k], src[k + 1], src[k + 2], 0.f);
+}
+
 int copy_in(jt_handle* h, const void* src, size_t bytes, int mem, void** dev)
 {
     if (mem == JT_MEM_DEVICE) {
@@ -815,6 +825,45 @@ int jt_step(jt_handle* h, double dt, double hubble, double dtau_per_dt, int nste
     }
     cudaEventDestroy(t0); cudaEventDestroy(t1); cudaEventDestroy(k0); cudaEventDestroy(k1);
     return r;
+}
+
+int jt_set_accel(jt_handle* h, const float* acc_p, const float* acc_m, int mem)
+{
+    if (!h || (mem != JT_MEM_HOST && mem != JT_MEM_DEVICE)) return JT_EINVAL;
+    if (!h->have_state) return JT_ESTATE;
+    if (h->signed_layout) return JT_EINVAL;
+    const float* src[2] = {acc_p, acc_m};
+    for (int s = 0; s < 2; s++)
+        if (h->n[s] > 0 && !src[s]) return JT_EINVAL;
+    const Parts P = parts_of(h);
+    for (int s = 0; s < 2; s++) {
+        const int64_t n = h->n[s];
+        if (n == 0) continue;
+        void* d = nullptr;
+        JT_TRY(copy_in(h, src[s], sizeof(float) * 3 * (size_t)n, mem, &d));
+        k_aos_gather<<<(unsigned)((n + 255) / 256), 256, 0, h->st>>>((const float*)d, P.id[s], n, P.acc[s]);
+        JT_CU(cudaGetLastError());
+        JT_CU(cudaStreamSynchronize(h->st));   // the staging buffer is reused
+    }
+    h->tm.launches += (h->n[0] > 0) + (h->n[1] > 0);
+    h->acc_valid = true;
+    if (h->batch) jtb_box(h->batch, h->box_id)->acc_valid = true;
+    return JT_OK;
+}
+
+int jt_get_accel(jt_handle* h, float* acc_p, float* acc_m, int mem)
+{
+    if (!h || (mem != JT_MEM_HOST && mem != JT_MEM_DEVICE)) return JT_EINVAL;
+    if (!h->have_state) return JT_ESTATE;
+    if (h->signed_layout) return JT_EINVAL;
+    const bool valid = h->batch ? jtb_box(h->batch, h->box_id)->acc_valid : h->acc_valid;
+    if (!valid) return JT_ESTATE;
+    const Parts P = parts_of(h);
+    JT_TRY(write_out(h, P.acc[0], P.id[0], nullptr, h->n[0], acc_p, mem));
+    if (mem == JT_MEM_HOST) JT_CU(cudaStreamSynchronize(h->st));
+    JT_TRY(write_out(h, P.acc[1], P.id[1], nullptr, h->n[1], acc_m, mem));
+    JT_CU(cudaStreamSynchronize(h->st));
+    return JT_OK;
 }
 
 int jt_set_screening(jt_handle* h, double lambda_0, double z)

@@ -629,11 +629,20 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_walk_acc(WalkArgs A)
         float az = sgn_s * pm.z + near.z + (far.z - comp.z);
         SG.acc[i] = make_float4(ax, ay, az, 0.f);
         if (A.kick_frac != 0.0f) {
-            const float drag = B.kick_drag, kdt = A.kick_frac * B.dt;
+            // kick_frac 0.5: the closing half kick; 1.0: the closing half
+            // kick and the next step's opening half kick, applied one after
+            // the other (with drag, one full kick would differ by O(H a dt^2)
+            // and make a trajectory depend on how steps are grouped in calls)
+            const float drag = B.kick_drag, h = 0.5f * B.dt;
             float4 v = SG.vel[i];
-            v.x += (ax - drag * v.x) * kdt;
-            v.y += (ay - drag * v.y) * kdt;
-            v.z += (az - drag * v.z) * kdt;
+            v.x += (ax - drag * v.x) * h;
+            v.y += (ay - drag * v.y) * h;
+            v.z += (az - drag * v.z) * h;
+            if (A.kick_frac > 0.75f) {
+                v.x += (ax - drag * v.x) * h;
+                v.y += (ay - drag * v.y) * h;
+                v.z += (az - drag * v.z) * h;
+            }
             SG.vel[i] = v;
         }
     }

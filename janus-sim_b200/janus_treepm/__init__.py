@@ -50,7 +50,7 @@ EXPORTED = [
     "jt_ics_zeldovich", "jt_set_state_zeldovich", "jt_batch_add_zeldovich", "jt_philox4x32_10",
     "jt_energy_sampled", "jt_virialize_sampled", "jt_energy_drift_pct",
     "jt_batch_checkpoint_async", "jt_batch_checkpoint_wait", "jt_snapshot_write_raw",
-    "jt_snapshot_read_raw",
+    "jt_snapshot_read_raw", "jt_set_accel", "jt_get_accel",
 ]
 JT_JOB_QUEUED, JT_JOB_RESIDENT, JT_JOB_DONE = 0, 1, 2
 JT_STATIC_SORT_MAX = 262144
@@ -278,6 +278,8 @@ def library():
                                    C.POINTER(C.c_size_t)]
     L.jt_checkpoint.argtypes = [H, C.c_char_p, C.POINTER(jt_snapshot_meta)]
     L.jt_set_screening.argtypes = [H, C.c_double, C.c_double]
+    L.jt_set_accel.argtypes = [H, fp, fp, C.c_int]
+    L.jt_get_accel.argtypes = [H, fp, fp, C.c_int]
     L.jt_ics_zeldovich.argtypes = [C.POINTER(jt_ics_params), fp, fp, fp, fp, C.c_int]
     L.jt_set_state_zeldovich.argtypes = [H, C.POINTER(jt_ics_params)]
     L.jt_batch_add_zeldovich.argtypes = [C.c_void_p, C.POINTER(jt_config), C.POINTER(jt_ics_params),
@@ -473,7 +475,25 @@ class Solver:
     def step(self, dt, hubble=0.0, dtau_per_dt=1.0, nsteps=1):
         _check(library().jt_step(self._h, dt, hubble, dtau_per_dt, nsteps), "jt_step")
 
-    def get_state(self):
+    def set_accel(self, acc_p, acc_m):
+        """Load the accelerations at the current positions (host arrays) so
+        that the next KDK step needs no opening force pass."""
+        acc_p, acc_m = _f32(acc_p), _f32(acc_m)
+        _check(library().jt_set_accel(self._h, _ptr(acc_p), _ptr(acc_m), JT_MEM_HOST), "jt_set_accel")
+
+    def get_accel(self, out=None):
+        """The stored accelerations (no force pass); out = [acc_p, acc_m]."""
+        ap, am = out if out is not None else (np.zeros((self.n[0], 3), np.float32),
+                                              np.zeros((self.n[1], 3), np.float32))
+        _check(library().jt_get_accel(self._h, _ptr(ap), _ptr(am), JT_MEM_HOST), "jt_get_accel")
+        return ap, am
+
+    def get_state(self, out=None):
+        """Positions and velocities in the caller's order; out = four
+        preallocated (pinned, say) float32 arrays to fill."""
+        if out is not None and not self._signed:
+            _check(library().jt_get_state(self._h, *[_ptr(a) for a in out], JT_MEM_HOST), "jt_get_state")
+            return tuple(out)
         if self._signed:
             pos = np.zeros((sum(self.n), 3), np.float32)
             vel = np.zeros((sum(self.n), 3), np.float32)

@@ -59,8 +59,8 @@ def zeldovich_lattice(n_side, L, seed=42, rms_frac=0.3, vel_factor=0.05):
     out = {}
     for name, comp_k in (("x", kx), ("y", ky), ("z", kz)):
         psik = (1j * comp_k * inv_k2 * dk).astype(np.complex64)
-        out[name + "p"] = np.fft.irfftn(psik, s=(n, n, n)).astype(np.float32)
-        out[name + "m"] = -np.fft.irfftn(psik * shift, s=(n, n, n)).astype(np.float32)
+        out[name + "p"] = np.fft.irfftn(psik, s=(n, n, n), axes=(0, 1, 2)).astype(np.float32)
+        out[name + "m"] = -np.fft.irfftn(psik * shift, s=(n, n, n), axes=(0, 1, 2)).astype(np.float32)
         del psik
     rms = np.sqrt(np.mean(out["xp"] ** 2 + out["yp"] ** 2 + out["zp"] ** 2))
     scale = rms_frac * a / rms
