@@ -441,6 +441,19 @@ void set_masses(jt_handle* h)
     h->mass[1] = (float)mm;
 }
 
+__global__ void k_iota(int* __restrict__ dst, int64_t n, int off)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = (int)(off + i);
+}
+
+// [m+ ; m-] signs of the per-species layout
+__global__ void k_layout_signs(int8_t* __restrict__ dst, int64_t n0, int64_t n)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = i < n0 ? (int8_t)1 : (int8_t)-1;
+}
+
 // dst[i] = AoS row id[i] of src (caller order -> internal order)
 __global__ void k_aos_gather(const float* __restrict__ src, const int* __restrict__ id, int64_t n,
                              float4* __restrict__ dst)
@@ -572,30 +585,42 @@ int jt_set_state(jt_handle* h, const float* pos_p, const float* vel_p, size_t n_
     const Parts P = parts_of(h);
     const float* pp[2] = {pos_p, pos_m};
     const float* vv[2] = {vel_p, vel_m};
-    for (int s = 0; s < 2; s++) {
-        int64_t n = h->n[s];
-        if (n == 0) continue;
-        void* d = nullptr;
-        JT_TRY(copy_in(h, pp[s], sizeof(float) * 3 * n, mem, &d));
-        jt_launch_aos_in((const float*)d, n, P.pos[s], P.id[s], h->st);
-        if (vv[s]) {
-            JT_TRY(copy_in(h, vv[s], sizeof(float) * 3 * n, mem, &d));
-            jt_launch_aos_in((const float*)d, n, P.vel[s], nullptr, h->st);
-        } else {
-            JT_CU(cudaMemsetAsync(P.vel[s], 0, sizeof(float4) * n, h->st));
+    // host arrays: all copies back to back into disjoint parts of the
+    // staging buffer (6 (n+ + n-) floats), then the conversions
+    const float* dp[2] = {pos_p, pos_m};
+    const float* dv[2] = {vel_p, vel_m};
+    if (mem == JT_MEM_HOST) {
+        float* st = (float*)h->stage;
+        size_t off = 0;
+        for (int s = 0; s < 2; s++) {
+            const size_t b = sizeof(float) * 3 * (size_t)h->n[s];
+            if (h->n[s] == 0) continue;
+            JT_CU(cudaMemcpyAsync(st + off, pp[s], b, cudaMemcpyHostToDevice, h->st));
+            dp[s] = st + off;
+            off += 3 * (size_t)h->n[s];
+            if (vv[s]) {
+                JT_CU(cudaMemcpyAsync(st + off, vv[s], b, cudaMemcpyHostToDevice, h->st));
+                dv[s] = st + off;
+                off += 3 * (size_t)h->n[s];
+            }
         }
-        // caller layout: [m+ ; m-]
-        std::vector<int> g(n);
-        for (int64_t i = 0; i < n; i++) g[i] = (int)(i + (s == 1 ? h->n[0] : 0));
-        JT_CU(cudaMemcpyAsync(h->gmap[s], g.data(), sizeof(int) * n, cudaMemcpyHostToDevice, h->st));
-        JT_CU(cudaStreamSynchronize(h->st));
     }
-    std::vector<int8_t> sg((size_t)(h->n[0] + h->n[1]));
-    for (int64_t i = 0; i < h->n[0] + h->n[1]; i++) sg[i] = i < h->n[0] ? 1 : -1;
-    if (!sg.empty())
-        JT_CU(cudaMemcpyAsync(h->sign_caller, sg.data(), sg.size(), cudaMemcpyHostToDevice, h->st));
-    JT_CU(cudaStreamSynchronize(h->st));
+    for (int s = 0; s < 2; s++) {
+        const int64_t n = h->n[s];
+        if (n == 0) continue;
+        jt_launch_aos_in(dp[s], n, P.pos[s], P.id[s], h->st);
+        if (vv[s])
+            jt_launch_aos_in(dv[s], n, P.vel[s], nullptr, h->st);
+        else
+            JT_CU(cudaMemsetAsync(P.vel[s], 0, sizeof(float4) * n, h->st));
+        // caller layout: [m+ ; m-]
+        k_iota<<<(unsigned)((n + 255) / 256), 256, 0, h->st>>>(h->gmap[s], n, s == 1 ? (int)h->n[0] : 0);
+    }
+    const int64_t na = h->n[0] + h->n[1];
+    k_layout_signs<<<(unsigned)((na + 255) / 256), 256, 0, h->st>>>(h->sign_caller, h->n[0], na);
     JT_CU(cudaGetLastError());
+    JT_CU(cudaStreamSynchronize(h->st));
+    h->tm.launches += 2 * ((h->n[0] > 0) + (h->n[1] > 0)) + 1;
     h->signed_layout = false;
     h->have_state = true;
     return JT_OK;
