@@ -43,7 +43,7 @@ UNIT = "particle-steps/s"
 # of every candidate is overhead and is not counted as useful work.
 FLOPS_PAIR = 40.0
 FLOPS_NODE = 100.0
-WALK_DRAM_BYTES_PER_PARTICLE = 615.0
+WALK_DRAM_BYTES_PER_PARTICLE = 643.0
 
 
 def workload(n_side=224, L=250.0, M=512):

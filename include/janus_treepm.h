@@ -451,6 +451,10 @@ int  jt_server_serve(jt_server* s, const double* t, const int* job, int n);
 int  jt_server_job_state(jt_server* s, int job, int* state, int* steps_done);
 int  jt_server_get_state(jt_server* s, int job, float* pos_p, float* vel_p,
                          float* pos_m, float* vel_m);
+/* The accelerations a job holds at its current positions (those of its last
+ * step; a swapped-out or finished job keeps them in pinned host memory);
+ * JT_ESTATE before its first force pass. */
+int  jt_server_get_accel(jt_server* s, int job, float* acc_p, float* acc_m);
 int  jt_server_stats(jt_server* s, jt_serve_stats* out);
 
 /* ---- allocation-free Morton sort ----

@@ -118,18 +118,17 @@ int evict(jt_server* S, Job& j, bool final)
     int r = jt_batch_get_state(S->B, j.box, h, h + 3 * np, h + 6 * np, h + 6 * np + 3 * nm, JT_MEM_HOST);
     if (r != JT_OK) return r;
     j.acc_saved = false;
-    if (!final) {
-        if (!j.host_acc &&
-            cudaMallocHost((void**)&j.host_acc, sizeof(float) * 3 * (np + nm)) != cudaSuccess) {
-            j.host_acc = nullptr;
-            cudaGetLastError();
-        }
-        // keep the forces of the state being swapped out (none yet: it comes
-        // back with a force pass)
-        if (j.host_acc &&
-            jt_batch_get_accel(S->B, j.box, j.host_acc, j.host_acc + 3 * np, JT_MEM_HOST) == JT_OK)
-            j.acc_saved = true;
+    if (!j.host_acc &&
+        cudaMallocHost((void**)&j.host_acc, sizeof(float) * 3 * (np + nm)) != cudaSuccess) {
+        j.host_acc = nullptr;
+        cudaGetLastError();
     }
+    // keep the forces of the state leaving the device (none yet: a swapped-out
+    // job then comes back with a force pass); a finished job's forces are
+    // its result as much as its state (jt_server_get_accel)
+    if (j.host_acc &&
+        jt_batch_get_accel(S->B, j.box, j.host_acc, j.host_acc + 3 * np, JT_MEM_HOST) == JT_OK)
+        j.acc_saved = true;
     r = jt_batch_remove(S->B, j.box);
     if (r != JT_OK) return r;
     j.box = -1;
@@ -425,6 +424,17 @@ int jt_server_get_state(jt_server* S, int job, float* pos_p, float* vel_p, float
     if (vel_p) std::memcpy(vel_p, h + 3 * np, sizeof(float) * 3 * np);
     if (pos_m) std::memcpy(pos_m, h + 6 * np, sizeof(float) * 3 * nm);
     if (vel_m) std::memcpy(vel_m, h + 6 * np + 3 * nm, sizeof(float) * 3 * nm);
+    return JT_OK;
+}
+
+int jt_server_get_accel(jt_server* S, int job, float* acc_p, float* acc_m)
+{
+    if (!job_ok(S, job)) return JT_EINVAL;
+    Job& j = S->jobs[job];
+    if (j.state == kResident) return jt_batch_get_accel(S->B, j.box, acc_p, acc_m, JT_MEM_HOST);
+    if (!j.acc_saved) return JT_ESTATE;
+    if (acc_p) std::memcpy(acc_p, j.host_acc, sizeof(float) * 3 * j.n_p);
+    if (acc_m) std::memcpy(acc_m, j.host_acc + 3 * j.n_p, sizeof(float) * 3 * j.n_m);
     return JT_OK;
 }
 

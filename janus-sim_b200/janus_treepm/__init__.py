@@ -50,7 +50,7 @@ EXPORTED = [
     "jt_ics_zeldovich", "jt_set_state_zeldovich", "jt_batch_add_zeldovich", "jt_philox4x32_10",
     "jt_energy_sampled", "jt_virialize_sampled", "jt_energy_drift_pct",
     "jt_batch_checkpoint_async", "jt_batch_checkpoint_wait", "jt_snapshot_write_raw",
-    "jt_snapshot_read_raw", "jt_set_accel", "jt_get_accel",
+    "jt_snapshot_read_raw", "jt_set_accel", "jt_get_accel", "jt_server_get_accel",
 ]
 JT_JOB_QUEUED, JT_JOB_RESIDENT, JT_JOB_DONE = 0, 1, 2
 JT_STATIC_SORT_MAX = 262144
@@ -279,6 +279,7 @@ def library():
     L.jt_checkpoint.argtypes = [H, C.c_char_p, C.POINTER(jt_snapshot_meta)]
     L.jt_set_screening.argtypes = [H, C.c_double, C.c_double]
     L.jt_set_accel.argtypes = [H, fp, fp, C.c_int]
+    L.jt_server_get_accel.argtypes = [H, C.c_int, fp, fp]
     L.jt_get_accel.argtypes = [H, fp, fp, C.c_int]
     L.jt_ics_zeldovich.argtypes = [C.POINTER(jt_ics_params), fp, fp, fp, fp, C.c_int]
     L.jt_set_state_zeldovich.argtypes = [H, C.POINTER(jt_ics_params)]
@@ -771,6 +772,13 @@ class Server:
         _check(library().jt_server_job_state(self._s, job, C.byref(st), C.byref(done)),
                "jt_server_job_state")
         return st.value, done.value
+
+    def get_accel(self, job):
+        """(acc_p, acc_m) the job holds at its current positions."""
+        n_p, n_m = self.jobs[job]
+        ap, am = np.zeros((n_p, 3), np.float32), np.zeros((n_m, 3), np.float32)
+        _check(library().jt_server_get_accel(self._s, job, _ptr(ap), _ptr(am)), "jt_server_get_accel")
+        return ap, am
 
     def get_state(self, job):
         n_p, n_m = self.jobs[job]
