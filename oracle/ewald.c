@@ -224,3 +224,149 @@ void orc_ewald_forces(const double* pos, const double* mass,
     for (int64_t i = 0; i < 3 * nt; i++) acc[i] += al[i];
     free(al);
 }
+
+/*
+ * Potential energy of the truncated split model (the force the engine
+ * integrates), FP64, G folded into the masses, charges q = s m:
+ *
+ *   U = U_short + U_long + U_self
+ *   U_short = -1/2 sum_{i != j, images} q_i q_j [psi(r_p) - psi(r_cp)]  for r < r_cut,
+ *             psi(r) = erfc(r / 2r_s) / r, r_p^2 = r^2 + eps^2, r_cp^2 = r_cut^2 + eps^2
+ *   U_long  = -(2 pi / V) sum_{k != 0} exp(-k^2 r_s^2) / k^2 |S(k)|^2
+ *   U_self  = +(1 / (2 r_s sqrt(pi))) sum_i q_i^2
+ *   U_bg    = +(2 pi r_s^2 / V) (sum_i q_i)^2  (the uniform background that
+ *             the missing k = 0 mode stands for; constant in the positions,
+ *             it makes U independent of r_s for a net charge)
+ *
+ * -grad_i U / m_i is the acceleration of orc_ewald_forces with r_trunc =
+ * r_cut (the shift makes the short part continuous at r_cut, so U + KE is
+ * conserved by the exact dynamics of the truncated model).  parts (may be
+ * NULL) receives U_short, U_long, U_self + U_bg.
+ */
+double orc_split_energy(const double* pos, const double* mass, const int8_t* signs, int64_t n,
+                        double box, double r_s, double eps, double r_cut, double kcut_tol,
+                        double* parts)
+{
+    double half = box / 2.0;
+    double rcp = sqrt(r_cut * r_cut + eps * eps);
+    double psi_c = erfc(rcp / (2.0 * r_s)) / rcp;
+    /* short: cell list with cells >= r_cut (falls back to all pairs) */
+    int nc = (int)floor(box / r_cut);
+    if (nc > 256) nc = 256;
+    double us = 0.0;
+    if (nc >= 3) {
+        int64_t ncell = (int64_t)nc * nc * nc;
+        int64_t* head = (int64_t*)malloc(sizeof(int64_t) * (size_t)ncell);
+        int64_t* next = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n > 0 ? n : 1));
+        for (int64_t c = 0; c < ncell; c++) head[c] = -1;
+        double cs = box / nc;
+        int* cell = (int*)malloc(sizeof(int) * 3 * (size_t)(n > 0 ? n : 1));
+        for (int64_t j = 0; j < n; j++) {
+            for (int d = 0; d < 3; d++) {
+                int gi = (int)floor((pos[3 * j + d] + half) / cs) % nc;
+                if (gi < 0) gi += nc;
+                cell[3 * j + d] = gi;
+            }
+            int64_t cid = cell[3 * j] + (int64_t)nc * (cell[3 * j + 1] + (int64_t)nc * cell[3 * j + 2]);
+            next[j] = head[cid];
+            head[cid] = j;
+        }
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : us)
+        for (int64_t i = 0; i < n; i++) {
+            double e = 0.0;
+            for (int oz = -1; oz <= 1; oz++)
+                for (int oy = -1; oy <= 1; oy++)
+                    for (int ox = -1; ox <= 1; ox++) {
+                        int cx = (cell[3 * i] + ox + nc) % nc, cy = (cell[3 * i + 1] + oy + nc) % nc,
+                            cz = (cell[3 * i + 2] + oz + nc) % nc;
+                        for (int64_t j = head[cx + (int64_t)nc * (cy + (int64_t)nc * cz)]; j >= 0; j = next[j]) {
+                            if (j == i) continue;
+                            double r2 = 0.0;
+                            for (int d = 0; d < 3; d++) {
+                                double dd = pos[3 * j + d] - pos[3 * i + d];
+                                dd -= box * floor(dd / box + 0.5);
+                                r2 += dd * dd;
+                            }
+                            if (r2 >= r_cut * r_cut) continue;
+                            double rp = sqrt(r2 + eps * eps);
+                            e += (double)signs[j] * mass[j] * (erfc(rp / (2.0 * r_s)) / rp - psi_c);
+                        }
+                    }
+            us += -0.5 * (double)signs[i] * mass[i] * e;
+        }
+        free(head);
+        free(next);
+        free(cell);
+    } else {
+        int nimg = (int)ceil(r_cut / box);
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : us)
+        for (int64_t i = 0; i < n; i++) {
+            double e = 0.0;
+            for (int64_t j = 0; j < n; j++)
+                for (int iz = -nimg; iz <= nimg; iz++)
+                    for (int iy = -nimg; iy <= nimg; iy++)
+                        for (int ix = -nimg; ix <= nimg; ix++) {
+                            if (j == i && ix == 0 && iy == 0 && iz == 0) continue;
+                            double r2 = 0.0;
+                            int sh[3] = {ix, iy, iz};
+                            for (int d = 0; d < 3; d++) {
+                                double dd = pos[3 * j + d] - pos[3 * i + d];
+                                dd -= box * floor(dd / box + 0.5);
+                                dd += sh[d] * box;
+                                r2 += dd * dd;
+                            }
+                            if (r2 >= r_cut * r_cut) continue;
+                            double rp = sqrt(r2 + eps * eps);
+                            e += (double)signs[j] * mass[j] * (erfc(rp / (2.0 * r_s)) / rp - psi_c);
+                        }
+            us += -0.5 * (double)signs[i] * mass[i] * e;
+        }
+    }
+    /* long: |S(k)|^2 over the half space of k (each pair k, -k once) */
+    double dk = 2.0 * M_PI / box;
+    double kmax = sqrt(-log(kcut_tol)) / r_s;
+    int nmax = (int)floor(kmax / dk);
+    if (nmax < 1) nmax = 1;
+    double V = box * box * box;
+    double ul = 0.0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : ul)
+    for (int nx = 0; nx <= nmax; nx++) {
+        double* cr = (double*)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+        double* ci = (double*)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+        for (int64_t j = 0; j < n; j++) {
+            double th = dk * nx * pos[3 * j];
+            cr[j] = cos(th);
+            ci[j] = sin(th);
+        }
+        for (int ny = -nmax; ny <= nmax; ny++)
+            for (int nz = -nmax; nz <= nmax; nz++) {
+                if (nx == 0 && (ny < 0 || (ny == 0 && nz <= 0))) continue;
+                double k2 = dk * dk * (double)(nx * nx + ny * ny + nz * nz);
+                if (k2 > kmax * kmax) continue;
+                double sr = 0.0, si = 0.0;
+                for (int64_t j = 0; j < n; j++) {
+                    double th = dk * (ny * pos[3 * j + 1] + nz * pos[3 * j + 2]);
+                    double c = cos(th), s = sin(th);
+                    double q = (double)signs[j] * mass[j];
+                    sr += q * (cr[j] * c - ci[j] * s);
+                    si += q * (cr[j] * s + ci[j] * c);
+                }
+                /* full-space (2 pi / V) sum = half-space (4 pi / V) sum */
+                ul += -(4.0 * M_PI / V) * exp(-k2 * r_s * r_s) / k2 * (sr * sr + si * si);
+            }
+        free(cr);
+        free(ci);
+    }
+    double q2 = 0.0, qt = 0.0;
+    for (int64_t i = 0; i < n; i++) {
+        q2 += mass[i] * mass[i];
+        qt += (double)signs[i] * mass[i];
+    }
+    double uself = q2 / (2.0 * r_s * sqrt(M_PI)) + 2.0 * M_PI * r_s * r_s * qt * qt / V;
+    if (parts) {
+        parts[0] = us;
+        parts[1] = ul;
+        parts[2] = uself;
+    }
+    return us + ul + uself;
+}

@@ -163,6 +163,11 @@ void orc_acc_pm_grids(const double* pos, const double* mass,
                       double r_s, int k_min, double* fx, double* fy,
                       double* fz);
 
+/* FP64 potential energy of the truncated split model (ewald.c) */
+double orc_split_energy(const double* pos, const double* mass, const int8_t* signs, int64_t n,
+                        double box, double r_s, double eps, double r_cut, double kcut_tol,
+                        double* parts);
+
 #ifdef __cplusplus
 }
 #endif

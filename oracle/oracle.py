@@ -389,3 +389,17 @@ def pe_binding_sampled(pos_p, pos_m, n_sample, softening):
         scale = (n * (n - 1.0)) / (ns * (ns - 1.0)) if ns > 1 else 1.0
         out.append(pe * scale)
     return tuple(out)
+
+
+def split_energy(pos, mass, signs, box, r_s, eps, r_cut, kcut_tol=1e-12):
+    """FP64 potential energy of the truncated split model (short part shifted
+    to zero at r_cut): (U, (U_short, U_long, U_self))."""
+    pos = _c(pos, np.float64).reshape(-1, 3)
+    mass = _c(mass, np.float64)
+    signs = _c(signs, np.int8)
+    parts = np.zeros(3)
+    L = lib()
+    L.orc_split_energy.argtypes = [f64p, f64p, i8p, I64, F64, F64, F64, F64, F64, f64p]
+    L.orc_split_energy.restype = F64
+    u = L.orc_split_energy(pos.ravel(), mass, signs, len(pos), box, r_s, eps, r_cut, kcut_tol, parts)
+    return u, tuple(parts)

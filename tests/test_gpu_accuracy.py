@@ -109,3 +109,50 @@ def test_uniform_cfg0_error_split():
     report = {"walk": pct(sh, short_ref), "pm": pct(lg, long_ref), "total": pct(al, short_ref + long_ref)}
     print("ACCURACY_CFG0", json.dumps(report))
     assert report["total"][1] <= 1e-3, report
+
+
+def test_energy_drift_cfg2_shape():
+    """configs[2]'s energy drift, at its density and split scale in a box
+    1/8 the side: 2x16^3 particles from 8 Plummer spheres (species
+    alternating by sphere, 20 % uniform background), L = 12.5, PM 32^3
+    (r_s = 0.488 as configs[2]), r_cut = 4.5 r_s, cold start, 100 KDK steps
+    of dt = 0.01 without Hubble drag.  E = sum m v^2 / 2 (FP64 from the state)
+    + the FP64 potential of the truncated split model (oracle/ewald.c,
+    short part shifted to zero at r_cut: E is conserved by the model's exact
+    dynamics).  Drift = (E_100 - E_0) / (KE_100 + |U_0|), reported for
+    theta 0.3 / 0.5 / 0.7.  Bar: 1e-2."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    import janus_treepm as J
+    from janus_treepm import ics
+    L, M, n = 12.5, 32, 16 ** 3
+    pp, pm = ics.plummer_spheres(n, L, n_spheres=8, seed=3)
+    r_s = 1.25 * L / M
+    r_cut = 4.5 * r_s
+    eps = (L / (2 * n) ** (1 / 3)) / 30
+    mp = 1e-3 * ((L / (2 * n) ** (1 / 3)) / 1.116) ** 3
+    report = {}
+    for theta in (0.3, 0.5, 0.7):
+        cfg = J.Config(box_L=L, pm_grid=M, theta=theta, softening=eps, r_s=r_s, r_cut=r_cut, mu=1.0,
+                       G_mass_plus=mp)
+        s = J.Solver(cfg)
+        s.set_state(pp, None, pm, None)
+        mass = np.concatenate([np.full(n, mp), np.full(n, mp)])
+        sg = np.concatenate([np.ones(n, np.int8), -np.ones(n, np.int8)])
+
+        def energy():
+            a, va, b, vb = s.get_state()
+            pos = np.concatenate([a, b]).astype(np.float64)
+            v = np.concatenate([va, vb]).astype(np.float64)
+            ke = 0.5 * float(np.sum(mass[:, None] * v * v))
+            u, _ = O.split_energy(pos, mass, sg, L, r_s, eps, r_cut)
+            return ke, u
+
+        ke0, u0 = energy()
+        s.step(0.01, 0.0, 1.0, 100)
+        ke1, u1 = energy()
+        s.close()
+        report["theta_%.1f" % theta] = [(ke1 + u1 - ke0 - u0) / (ke1 + abs(u0)), ke1 / abs(u0)]
+    print("ENERGY_DRIFT_CFG2", json.dumps(report))
+    for k, v in report.items():
+        assert abs(v[0]) <= 1e-2, report

@@ -320,3 +320,25 @@ def test_acc_pm_against_long_range_ewald(order, interlace, p50_max):
     a_ex = O.ewald_forces(pos, mass, sg, L, r_s, 0.0, part="long")
     rel = np.linalg.norm(a_pm - a_ex, axis=1) / np.linalg.norm(a_ex, axis=1)
     assert np.median(rel) < p50_max
+
+
+def test_split_energy_is_the_potential_of_the_oracle_forces():
+    """orc_split_energy: independent of r_s for an untruncated split (net
+    charge included), and -grad U / m equals orc_ewald_forces on the
+    truncated model."""
+    L = 20.0
+    pos = np.array([[0, 0, 0], [1.5, 0, 0], [3, 4, -2], [-7, 2, 9]], float)
+    m = np.array([1.0, 2.0, 0.5, 0.3])
+    s = np.array([1, 1, -1, -1], np.int8)
+    us = [O.split_energy(pos, m, s, L, rs, 0.0, 12 * rs)[0] for rs in (0.4, 0.6, 0.9)]
+    assert max(us) - min(us) <= 1e-10 * abs(us[0])
+    rs, eps, h = 0.5, 0.1, 1e-5
+    rc = 4.5 * rs
+    a = O.ewald_forces(pos, m, s, L, rs, eps, r_trunc=rc)
+    for i in range(len(pos)):
+        for d in range(3):
+            pp, pn = pos.copy(), pos.copy()
+            pp[i, d] += h
+            pn[i, d] -= h
+            g = -(O.split_energy(pp, m, s, L, rs, eps, rc)[0] - O.split_energy(pn, m, s, L, rs, eps, rc)[0]) / (2 * h) / m[i]
+            assert abs(g - a[i, d]) <= 1e-6 * max(1.0, abs(a[i, d]))
