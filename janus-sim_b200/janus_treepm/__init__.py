@@ -825,6 +825,8 @@ class GpuNBodyTwoPass:
         self._solver = None
         self._r_cut = None
         self._dirty_state = True
+        self.lambda_0 = 0.0      # Yukawa screening length at z = 0 (off)
+        self.current_z = 0.0
 
     @classmethod
     def with_custom_ics(cls, pos, vel, signs, box_size, **kw):
@@ -850,6 +852,40 @@ class GpuNBodyTwoPass:
         self.pm_k_min = int(k)
         self._solver = None
 
+    def set_lambda_0(self, lam):
+        """Yukawa screening of opposite-sign pairs (:2305-2306); lambda(z) =
+        lambda_0 sqrt(1 + z) at the next force evaluation."""
+        self.lambda_0 = float(lam)
+        if self._solver is not None:
+            self._solver.set_screening(self.lambda_0, self.current_z)
+
+    set_lambda_base = set_lambda_0   # the reference's alias (:2312)
+
+    def set_current_z(self, z):
+        self.current_z = float(z)
+        if self._solver is not None:
+            self._solver.set_screening(self.lambda_0, self.current_z)
+
+    def kinetic_energy(self):
+        """sum |v|^2 / 2, unit masses (:5070-5077), FP64 on the device."""
+        self._ensure(self._r_cut or 4.5 * 1.25 * self.box_size / self.pm_grid)
+        return self._solver.energy(1)["kinetic"]
+
+    def potential_energy_binding_sampled(self, n_sample):
+        """Sampled same-species binding energy (:5081-5181)."""
+        self._ensure(self._r_cut or 4.5 * 1.25 * self.box_size / self.pm_grid)
+        return self._solver.energy(n_sample)["pe_binding"]
+
+    def virialize_sampled(self, n_sample):
+        """Scale velocities so that 2 KE = |PE_binding| (:5186-5225)."""
+        self._ensure(self._r_cut or 4.5 * 1.25 * self.box_size / self.pm_grid)
+        return self._solver.virialize(n_sample)
+
+    def segregation(self):
+        """|COM+ - COM-| / L (:5364-5393), FP64 on the device."""
+        self._ensure(self._r_cut or 4.5 * 1.25 * self.box_size / self.pm_grid)
+        return self._solver.diagnostics(8)["segregation"]
+
     def _sync_state(self):
         if self._solver is not None:
             self._pos, self._vel = self._solver.get_state()
@@ -867,6 +903,8 @@ class GpuNBodyTwoPass:
                      integrator=self.integrator)
         self._solver = Solver(cfg)
         self._solver.set_state_signed(self._pos, self._vel, self._signs)
+        if self.lambda_0 > 0.01:
+            self._solver.set_screening(self.lambda_0, self.current_z)
         self._r_cut = r_cut
 
     def compute_forces(self, r_cut):

@@ -204,3 +204,31 @@ def test_kdk_matches_host_integration_of_device_forces():
     assert np.abs(gvm - half(v1m, a1m)).max() < 1e-4 * max(1.0, np.abs(gvm).max())
     s.close()
     s2.close()
+
+
+def test_twopass_mirror_energy_screening_and_segregation():
+    """The GpuNBodyTwoPass mirror's energy, virialization, segregation and
+    screening methods against the oracle / Solver on the same signed array."""
+    J, O = _mods()
+    L, n = 40.0, 3000
+    rng = np.random.default_rng(23)
+    pos = _uniform(n, L, 9)
+    vel = rng.normal(0, 0.2, (n, 3)).astype(np.float32)
+    sg = np.where(rng.random(n) < 0.5, 1, -1).astype(np.int8)
+    sim = J.GpuNBodyTwoPass.with_custom_ics(pos, vel, sg, L, pm_grid=32)
+    sim.set_softening(0.05)
+    ke = sim.kinetic_energy()
+    assert ke == pytest.approx(0.5 * float(np.sum(vel.astype(np.float64) ** 2)), rel=1e-10)
+    pe = sim.potential_energy_binding_sampled(1000)
+    pe_p, pe_m = O.pe_binding_sampled(pos[sg > 0], pos[sg < 0], 1000, 0.05)
+    assert pe == pytest.approx(pe_p + pe_m, rel=1e-10)
+    assert sim.segregation() == pytest.approx(O.segregation(pos, sg, L), rel=1e-9, abs=1e-15)
+    sim.set_lambda_0(1.93)
+    sim.set_current_z(0.8)
+    a = sim.compute_forces(5.0)
+    ref = O.ref_total_forces_screened(pos, sg, 32, L, 0.5, 0.05, 5.0, sim.mass_factor, 1.93, 0.8)
+    rel = _rel(a, ref)
+    assert np.percentile(rel, 99) <= 1e-5
+    alpha = sim.virialize_sampled(1000)
+    _, v2, _ = sim.get_particles()
+    assert np.allclose(v2, vel * np.float32(alpha), rtol=1e-6, atol=0)
