@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <new>
@@ -141,12 +142,21 @@ size_t grid_bytes(int64_t M, int ngrid)
 }
 
 // The tables of one pass, packed into one host buffer and uploaded once.
+// the near-field cell walk (on unless JT_WALK_CELLS=0, which keeps the tree
+// walk for every particle)
+bool cells_enabled()
+{
+    const char* e = std::getenv("JT_WALK_CELLS");
+    return !(e && e[0] == '0');
+}
+
 struct Plan {
     std::vector<int> ids;                 // boxes of this pass
     std::vector<jt_seg_dev> pre, post;    // segments before / after the reorder
     std::vector<jt_box_dev> bx;
-    std::vector<int64_t> pprefix, iprefix, tprefix, gprefix, ptprefix, kprefix;
-    int64_t npart = 0, ninternal = 0, nsorttiles = 0, ngroups = 0, npmtiles = 0, nmodes = 0;
+    std::vector<int64_t> pprefix, iprefix, tprefix, gprefix, ptprefix, kprefix, cprefix;
+    int64_t npart = 0, ninternal = 0, nsorttiles = 0, ngroups = 0, npmtiles = 0, nmodes = 0, ncells = 0;
+    bool cells = false;                   // the near-field cell walk runs (jt_b_cells)
     std::map<int, std::vector<int>> by_M; // M -> boxes (positions in ids)
     int maxT = 1;
     size_t table_bytes = 0;
@@ -154,7 +164,7 @@ struct Plan {
     const jt_seg_dev* d_post = nullptr;
     const jt_box_dev* d_bx = nullptr;
     const int64_t *d_pp = nullptr, *d_ip = nullptr, *d_tp = nullptr, *d_gp = nullptr, *d_ptp = nullptr,
-                  *d_kp = nullptr;
+                  *d_kp = nullptr, *d_cp = nullptr;
 };
 
 float elapsed(cudaEvent_t a, cudaEvent_t b)
@@ -176,6 +186,12 @@ struct jt_batch {
     int order = 0, ngrid = 0, k_min = -1;   // shared by every box of the batch
     Pool<int2> child, range;
     Pool<int> parent, flag;
+    // near-field cell list (jt_b_cells)
+    Pool<int> ccount, cstart, cbsum, ccell;
+    Pool<unsigned> cslot;
+    Pool<float4> cpos;
+    Pool<int2> cid;
+    Pool<unsigned char> tflag;
     Pool<float4> com, bmin, bmax, quad0;
     Pool<float2> quad1;
     Pool<uint32_t> m30, vals, vals_alt, keys_alt, hist, status, tickets;
@@ -420,7 +436,8 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
 
     int64_t o_node = 0, o_part = 0, o_tile = 0;
     P.pprefix.push_back(0); P.iprefix.push_back(0); P.tprefix.push_back(0); P.gprefix.push_back(0);
-    P.ptprefix.push_back(0); P.kprefix.push_back(0);
+    P.ptprefix.push_back(0); P.kprefix.push_back(0); P.cprefix.push_back(0);
+    P.cells = cells_enabled();
     P.bx.resize(nb);
     for (int k = 0; k < nb; k++) {
         jt_box_state* b = B->boxes[ids[k]];
@@ -457,6 +474,17 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
         d.tabs = b->tabs;
         d.ranges = K.ranges + (size_t)q * d.ntiles;
         d.seg[0] = d.seg[1] = -1;
+        // near-field cells of side L / nb >= r_cut (1e-4 margin against
+        // binning round-off); fewer than 3 per axis: tree walk only
+        d.nb = 0;
+        d.cbase = P.cprefix.back();
+        if (P.cells && c.r_cut > 0.0) {
+            const double q = c.box_L / (c.r_cut * 1.0001);
+            int nbc = q >= 256.0 ? 256 : (int)q;
+            if (nbc >= 3) d.nb = nbc;
+        }
+        d.cell_inv = d.nb ? (float)(d.nb / c.box_L) : 0.0f;
+        P.cprefix.push_back(P.cprefix.back() + (int64_t)d.nb * d.nb * d.nb);
         for (int s = 0; s < 2; s++) {
             const int64_t n = b->n[s];
             if (n == 0) continue;
@@ -508,12 +536,24 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
     P.ngroups = P.gprefix.back();
     P.npmtiles = P.ptprefix.back();
     P.nmodes = P.kprefix.back();
+    P.ncells = P.cprefix.back();
+    if (P.cells) {
+        JT_TRY(B->ccount.ensure((size_t)std::max<int64_t>(P.ncells, 1), &grew));
+        JT_TRY(B->cstart.ensure((size_t)P.ncells + 1, &grew));
+        JT_TRY(B->cbsum.ensure((size_t)jt_cell_scan_blocks(P.ncells) + 1, &grew));
+        JT_TRY(B->ccell.ensure((size_t)std::max<int64_t>(P.npart, 1), &grew));
+        JT_TRY(B->cslot.ensure((size_t)std::max<int64_t>(P.npart, 1), &grew));
+        JT_TRY(B->cpos.ensure((size_t)std::max<int64_t>(P.npart, 1), &grew));
+        JT_TRY(B->cid.ensure((size_t)std::max<int64_t>(P.npart, 1), &grew));
+        JT_TRY(B->tflag.ensure((size_t)std::max<int64_t>(P.npart, 1), &grew));
+    }
 
     if (grew) B->gen++;
     std::vector<unsigned char> buf;
     size_t o_pre = put(buf, P.pre), o_post = put(buf, P.post), o_bx = put(buf, P.bx);
     size_t o_pp = put(buf, P.pprefix), o_ip = put(buf, P.iprefix), o_tp = put(buf, P.tprefix);
     size_t o_gp = put(buf, P.gprefix), o_ptp = put(buf, P.ptprefix), o_kp = put(buf, P.kprefix);
+    size_t o_cp = put(buf, P.cprefix);
     JT_TRY(B->desc.ensure(buf.size(), &grew));
     // the previous upload may still read the staging buffer
     JT_CU(cudaEventSynchronize(B->desc_done));
@@ -537,6 +577,7 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
     P.d_gp = (const int64_t*)(d + o_gp);
     P.d_ptp = (const int64_t*)(d + o_ptp);
     P.d_kp = (const int64_t*)(d + o_kp);
+    P.d_cp = (const int64_t*)(d + o_cp);
     P.table_bytes = buf.size();
     return JT_OK;
 }
@@ -586,8 +627,17 @@ int force_pass(jt_batch* B, Plan& P, int parts, float kick_frac)
     pool.quad0 = B->quad0.p;
     pool.quad1 = B->quad1.p;
     pool.m30 = B->m30.p;
+    const unsigned char* tflag = nullptr;
+    if (P.cells) {
+        jt_cell_bufs cb = {B->ccount.p, B->cstart.p, B->cbsum.p, B->ccell.p, B->cslot.p,
+                           B->cpos.p, B->cid.p, B->tflag.p};
+        JT_TRY(jt_b_cells(P.d_post, P.d_bx, P.d_pp, nseg, P.npart, P.d_cp, nbox, P.ncells, cb, B->order,
+                          B->ngrid, parts, kick_frac, B->d_stats, B->d_err, st));
+        tflag = B->tflag.p;
+        B->tm.launches += P.npart > 0 ? (P.ncells > 0 ? 6 : 1) : 0;
+    }
     JT_TRY(jt_b_walk(P.d_post, P.d_bx, P.d_gp, nseg, P.ngroups, pool, B->order, B->ngrid, parts,
-                     kick_frac, B->d_stats, B->d_err, st));
+                     kick_frac, B->d_stats, B->d_err, st, P.d_pp, tflag));
     cudaEventRecord(B->ev[7], st);
     B->pending = true;
     B->tm.launches += (P.npart > 0 ? 8 : 0) + (P.ninternal > 0 ? 1 : 0) + (P.npart > 0 ? 1 : 0) +
@@ -934,6 +984,8 @@ void jt_batch_destroy(jt_batch* B)
         if (b) { box_release(b); delete b; }
     B->child.release(); B->range.release(); B->parent.release(); B->flag.release();
     B->com.release(); B->bmin.release(); B->bmax.release(); B->quad0.release(); B->quad1.release();
+    B->ccount.release(); B->cstart.release(); B->cbsum.release(); B->ccell.release(); B->cslot.release();
+    B->cpos.release(); B->cid.release(); B->tflag.release();
     B->m30.release(); B->vals.release(); B->vals_alt.release(); B->keys_alt.release();
     B->hist.release(); B->status.release(); B->tickets.release(); B->desc.release();
     drop_graphs(B);
@@ -1207,6 +1259,8 @@ int jt_batch_trim(jt_batch* B)
     drop_graphs(B);
     B->child.release(); B->range.release(); B->parent.release(); B->flag.release();
     B->com.release(); B->bmin.release(); B->bmax.release(); B->quad0.release(); B->quad1.release();
+    B->ccount.release(); B->cstart.release(); B->cbsum.release(); B->ccell.release(); B->cslot.release();
+    B->cpos.release(); B->cid.release(); B->tflag.release();
     B->m30.release(); B->vals.release(); B->vals_alt.release(); B->keys_alt.release();
     B->hist.release(); B->status.release(); B->tickets.release();
     for (auto& kv : B->buckets) kv.second.release();

@@ -100,6 +100,9 @@ struct jt_box_dev {
     float* force;         // 3*ngrid force grids
     int4* ranges;         // per-tile particle ranges of both species
     int seg[2];           // segment index of each species (-1: none)
+    int nb;               // cells per axis of the near-field cell list (0: tree walk only)
+    float cell_inv;       // nb / L
+    int64_t cbase;        // this box's first cell in the pass's cell tables
 };
 
 __device__ __forceinline__ int jt_find(const int64_t* __restrict__ prefix, int count, int64_t i)
@@ -265,8 +268,24 @@ struct jt_walk_params {
 // stats[0] pair interactions inside r_cut, [1] node (multipole) interactions,
 // [2] candidate particles distance-tested
 int jt_b_walk(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_gprefix, int nseg,
-              int64_t ngroups, const jt_tree_dev& pool, int order, int ngrid, int parts, float kick_frac,
-              unsigned long long* stats, unsigned* d_err, cudaStream_t st);
+              int64_t ngroups, const jt_tree_dev& pool, int order, int ngrid, int parts,
+              float kick_frac, unsigned long long* stats, unsigned* d_err, cudaStream_t st,
+              const int64_t* d_pprefix = nullptr, const unsigned char* tflag = nullptr);
+// Near-field cell list of a pass (cells of side >= r_cut, both species) and
+// the cell walk over it: particles of cells whose 27-cell neighbourhood holds
+// more than JT_CELL_KMAX candidates, and of boxes without a cell grid, are
+// flagged in tflag for the tree walk; the others get their acceleration (and
+// fused kick) here.  Scratch: ccount/cstart C + 1 ints, bsum, ccell/cslot,
+// cpos/cid one entry per particle.
+struct jt_cell_bufs {
+    int* ccount; int* cstart; int* bsum; int* ccell; unsigned* cslot;
+    float4* cpos; int2* cid; unsigned char* tflag;
+};
+int jt_b_cells(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_pprefix, int nseg,
+               int64_t npart, const int64_t* d_cprefix, int nbox, int64_t ncells, const jt_cell_bufs& cb,
+               int order, int ngrid, int parts, float kick_frac, unsigned long long* stats,
+               unsigned* d_err, cudaStream_t st);
+int jt_cell_scan_blocks(int64_t ncells);
 
 // kick v += (a - drag v) frac*dt and drift x += v frac*dt with each box's own
 // dt and drag (jt_box_dev)

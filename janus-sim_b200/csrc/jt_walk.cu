@@ -127,6 +127,8 @@ struct WalkArgs {
                               // of each box's dt (0 = none)
     unsigned long long* stats;
     unsigned* err;
+    const int64_t* pprefix;       // particles per segment (with tflag)
+    const unsigned char* tflag;   // non-null: only flagged particles are computed here
 };
 
 // Pair interactions of this lane's target with a chunk of candidates: a
@@ -538,6 +540,48 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& 
     }
 }
 
+// PM acceleration of a unit m+ particle at p: the deposit's stencil on every
+// grid (the interlaced grid's nodes sit half a cell higher), averaged over the
+// grids (an m- particle takes minus this)
+template <int ORDER, int NG>
+__device__ __forceinline__ Acc3 pm_interp(const jt_box_dev& B, const float4& p)
+{
+    Acc3 pm = {0.f, 0.f, 0.f};
+    {
+        const int M = B.M, mask = M - 1;
+        const int64_t G = (int64_t)M * M * M;
+        const float gx = (p.x + B.halfL) * B.h_inv, gy = (p.y + B.halfL) * B.h_inv,
+                    gz = (p.z + B.halfL) * B.h_inv;
+#pragma unroll
+        for (int b = 0; b < NG; b++) {
+            const float sh = 0.5f * b;
+            float wx[ORDER], wy[ORDER], wz[ORDER];
+            const int ix = jt_stencil<ORDER>(gx - sh, wx);
+            const int iy = jt_stencil<ORDER>(gy - sh, wy);
+            const int iz = jt_stencil<ORDER>(gz - sh, wz);
+            const float* __restrict__ F = B.force + (int64_t)b * 3 * G;
+#pragma unroll
+            for (int c = 0; c < ORDER; c++)
+#pragma unroll
+                for (int bb = 0; bb < ORDER; bb++) {
+                    const float wyz = wz[c] * wy[bb];
+                    const int64_t row = ((int64_t)((iz + c) & mask) * M + ((iy + bb) & mask)) * M;
+#pragma unroll
+                    for (int a = 0; a < ORDER; a++) {
+                        const int64_t id = row + ((ix + a) & mask);
+                        const float w = wyz * wx[a];
+                        pm.x += w * __ldg(F + id);
+                        pm.y += w * __ldg(F + G + id);
+                        pm.z += w * __ldg(F + 2 * G + id);
+                    }
+                }
+        }
+        if (NG == 2) { pm.x *= 0.5f; pm.y *= 0.5f; pm.z *= 0.5f; }
+    }
+
+    return pm;
+}
+
 // MINB: resident blocks per SM the register budget is sized for (6 -> 80
 // registers); BKT: nodes with <= BKT particles are streamed as ranges
 // (<= 32: one lane per particle when a range is loaded)
@@ -567,6 +611,9 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_walk_acc(WalkArgs A)
     const int64_t ns = SG.n;
     const int64_t i = grp * 32 + lane;
     const bool valid = i < ns;
+    // with a cell walk before this one, only its flagged particles are left
+    const bool mine = !A.tflag || (valid && A.tflag[A.pprefix[g] + i]);
+    if (A.tflag && !__any_sync(0xffffffffu, mine)) return;
     const float4 p = SG.pos[valid ? i : grp * 32];
     const float sgn_s = s == 0 ? 1.0f : -1.0f;
 
@@ -576,40 +623,7 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_walk_acc(WalkArgs A)
     float gcx = 0.5f * (lox + hix), gcy = 0.5f * (loy + hiy), gcz = 0.5f * (loz + hiz);
     float ghx = 0.5f * (hix - lox), ghy = 0.5f * (hiy - loy), ghz = 0.5f * (hiz - loz);
 
-    // PM interpolation: the deposit's stencil on every grid (the interlaced
-    // grid's nodes sit half a cell higher), averaged over the grids
-    Acc3 pm = {0.f, 0.f, 0.f};
-    if (P.parts & 1) {
-        const int M = P.M, mask = M - 1;
-        const int64_t G = (int64_t)M * M * M;
-        const float gx = (p.x + P.halfL) * P.h_inv, gy = (p.y + P.halfL) * P.h_inv,
-                    gz = (p.z + P.halfL) * P.h_inv;
-#pragma unroll
-        for (int b = 0; b < NG; b++) {
-            const float sh = 0.5f * b;
-            float wx[ORDER], wy[ORDER], wz[ORDER];
-            const int ix = jt_stencil<ORDER>(gx - sh, wx);
-            const int iy = jt_stencil<ORDER>(gy - sh, wy);
-            const int iz = jt_stencil<ORDER>(gz - sh, wz);
-            const float* __restrict__ F = B.force + (int64_t)b * 3 * G;
-#pragma unroll
-            for (int c = 0; c < ORDER; c++)
-#pragma unroll
-                for (int bb = 0; bb < ORDER; bb++) {
-                    const float wyz = wz[c] * wy[bb];
-                    const int64_t row = ((int64_t)((iz + c) & mask) * M + ((iy + bb) & mask)) * M;
-#pragma unroll
-                    for (int a = 0; a < ORDER; a++) {
-                        const int64_t id = row + ((ix + a) & mask);
-                        const float w = wyz * wx[a];
-                        pm.x += w * __ldg(F + id);
-                        pm.y += w * __ldg(F + G + id);
-                        pm.z += w * __ldg(F + 2 * G + id);
-                    }
-                }
-        }
-        if (NG == 2) { pm.x *= 0.5f; pm.y *= 0.5f; pm.z *= 0.5f; }
-    }
+    const Acc3 pm = (P.parts & 1) ? pm_interp<ORDER, NG>(B, p) : Acc3{0.f, 0.f, 0.f};
 
     Acc3 near = {0.f, 0.f, 0.f}, far = {0.f, 0.f, 0.f}, comp = {0.f, 0.f, 0.f};
     unsigned pairs = 0, nodes = 0, cands = 0;   // per lane (warp totals < 2^32)
@@ -623,7 +637,7 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_walk_acc(WalkArgs A)
         walk_trees<ORDER, NG, false, BKT>(A, B, P, S, s, lane, p, valid, gcx, gcy, gcz, ghx, ghy, ghz, near,
                                      far, comp, pairs, nodes, cands, wc);
 
-    if (valid) {
+    if (valid && mine) {
         float ax = sgn_s * pm.x + near.x + (far.x - comp.x);
         float ay = sgn_s * pm.y + near.y + (far.y - comp.y);
         float az = sgn_s * pm.z + near.z + (far.z - comp.z);
@@ -647,6 +661,7 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_walk_acc(WalkArgs A)
         }
     }
     if (A.stats) {
+        if (!mine) pairs = nodes = 0;   // those lanes' accelerations came from the cell walk
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
@@ -1042,9 +1057,357 @@ extern "C" int jt_walk_tuning(char* buf, size_t len)
     return JT_OK;
 }
 
+namespace {
+
+// ------------------------------------------------------------------ cell walk
+// The near field as a cell list: per box a grid of nb^3 cells of side
+// L / nb >= r_cut (1e-4 margin), holding both species; every pair inside
+// r_cut lies in a cell and its 26 neighbours (nb >= 3, so the 27 are
+// distinct and the shifted image is the one within r_cut).  One warp per
+// cell: its targets (both species, ~30 at the 2x224^3 density) test every
+// candidate of the 27 cells that lies within r_cut of their AABB, in dense
+// chunks of 32 where every lane evaluates every candidate with the pair
+// force selected by r^2 < r_cut^2 (no per-lane hit loop, no traversal).
+// Pairs are exactly those of the tree walk when it accepts no multipole
+// (the uniform case); cells whose neighbourhood holds more than
+// JT_CELL_KMAX candidates (clustered data) flag their particles for the
+// tree walk, which keeps its multipoles there.
+#ifndef JT_CELL_KMAX
+#define JT_CELL_KMAX 2048
+#endif
+
+struct CellArgs {
+    const jt_seg_dev* segs;
+    const jt_box_dev* boxes;
+    const int64_t* pprefix;
+    int nseg, nbox;
+    const int64_t* cprefix;       // cells per box (nbox + 1)
+    jt_cell_bufs cb;
+    int parts;
+    float kick_frac;
+    unsigned long long* stats;
+    unsigned* err;
+};
+
+__device__ __forceinline__ int cell_of(float x, float halfL, float inv, int nb)
+{
+    int c = (int)floorf((x + halfL) * inv);
+    return c < 0 ? 0 : (c >= nb ? nb - 1 : c);
+}
+
+// cell key and slot of every particle (atomics on the cell counts); boxes
+// without a grid flag their particles for the tree walk
+__global__ void k_cell_key(CellArgs A, int64_t npart)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npart) return;
+    const int g = jt_find(A.pprefix, A.nseg, i);
+    const jt_seg_dev& SG = A.segs[g];
+    const jt_box_dev& B = A.boxes[SG.box];
+    if (B.nb == 0) {
+        A.cb.tflag[i] = 1;
+        A.cb.ccell[i] = -1;
+        return;
+    }
+    const float4 p = SG.pos[i - A.pprefix[g]];
+    const int nb = B.nb;
+    const int cx = cell_of(p.x, B.halfL, B.cell_inv, nb), cy = cell_of(p.y, B.halfL, B.cell_inv, nb),
+              cz = cell_of(p.z, B.halfL, B.cell_inv, nb);
+    const int key = (int)(B.cbase + ((int64_t)cz * nb + cy) * nb + cx);
+    A.cb.cslot[i] = (unsigned)atomicAdd(A.cb.ccount + key, 1);
+    A.cb.ccell[i] = key;
+    A.cb.tflag[i] = 0;
+}
+
+// exclusive scan of n counts, 1024 per block: block-local scan and block sums
+constexpr int kScanB = 1024;
+__device__ __forceinline__ int block_excl_scan(int v, int* wsum, int& total)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int t = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        wsum[lane] = t;   // inclusive warp-total prefix
+    }
+    __syncthreads();
+    total = wsum[(blockDim.x >> 5) - 1];
+    const int before = w > 0 ? wsum[w - 1] : 0;
+    __syncthreads();
+    return before + x - v;
+}
+
+__global__ void k_scan_local(const int* __restrict__ in, int* __restrict__ out, int64_t n, int* __restrict__ bsum)
+{
+    __shared__ int wsum[32];
+    const int64_t i = (int64_t)blockIdx.x * kScanB + threadIdx.x;
+    const int v = i < n ? in[i] : 0;
+    int total;
+    const int e = block_excl_scan(v, wsum, total);
+    if (i < n) out[i] = e;
+    if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+
+// one block: exclusive scan of the block sums in place (chunks of 1024 with
+// a running carry); bsum[nblk] = grand total
+__global__ void k_scan_sums(int* __restrict__ bsum, int nblk)
+{
+    __shared__ int wsum[32];
+    int carry = 0;
+    for (int base = 0; base < nblk; base += kScanB) {
+        const int i = base + threadIdx.x;
+        const int v = i < nblk ? bsum[i] : 0;
+        int total;
+        const int e = block_excl_scan(v, wsum, total);
+        if (i < nblk) bsum[i] = carry + e;
+        carry += total;
+    }
+    if (threadIdx.x == 0) bsum[nblk] = carry;
+}
+
+__global__ void k_scan_add(int* __restrict__ out, int64_t n, const int* __restrict__ bsum, int nblk)
+{
+    const int64_t i = (int64_t)blockIdx.x * kScanB + threadIdx.x;
+    if (i < n) out[i] += bsum[blockIdx.x];
+    if (i == 0) out[n] = bsum[nblk];
+}
+
+// particles into cell order: (x, y, z, s m) and (segment, index)
+__global__ void k_cell_scatter(CellArgs A, int64_t npart)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npart) return;
+    const int key = A.cb.ccell[i];
+    if (key < 0) return;
+    const int g = jt_find(A.pprefix, A.nseg, i);
+    const jt_seg_dev& SG = A.segs[g];
+    const jt_box_dev& B = A.boxes[SG.box];
+    const int64_t idx = i - A.pprefix[g];
+    const float4 p = SG.pos[idx];
+    const float sm = SG.species == 0 ? B.mass[0] : -B.mass[1];
+    const int dst = A.cb.cstart[key] + (int)A.cb.cslot[i];
+    A.cb.cpos[dst] = make_float4(p.x, p.y, p.z, sm);
+    A.cb.cid[dst] = make_int2(g, (int)idx);
+}
+
+struct CellWarpSmem {
+    float4 cand[64];
+    int2 nrange[27];              // (first, count) of each neighbour cell
+    float4 nshift[27];            // periodic shift of its particles
+};
+
+// dense evaluation of candidates [0, cnt) for this lane's target: every pair
+// computed, the force selected by 0 < r^2 < r_cut^2
+__device__ __forceinline__ unsigned cell_chunk(const float4* __restrict__ cand, int cnt, float px, float py,
+                                               float pz, float si, float rc2, float eps2, float c2s, Acc3& a)
+{
+    unsigned hits = 0;
+#pragma unroll 4
+    for (int j = 0; j < cnt; j++) {
+        const float4 q = cand[j];
+        const float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        const bool in = r2 > 0.0f && r2 < rc2;
+        const float rp2 = r2 + eps2;
+        const float ri = rsqrtf(rp2);
+        const float t = fminf(rp2 * c2s, (float)kStab - 1.5f);   // NaN -> the bound
+        const int k = max((int)t, 0);
+        const float2 ab = __ldg(&g_stab[k]);
+        const float S = fmaf(ab.y, t - (float)k, ab.x);
+        const float g = in ? si * q.w * S * ri * ri * ri : 0.0f;
+        hits += in ? 1u : 0u;
+        a.x += g * dx;
+        a.y += g * dy;
+        a.z += g * dz;
+    }
+    return hits;
+}
+
+template <int ORDER, int NG>
+__global__ void __launch_bounds__(kWarps * 32) k_walk_cell(CellArgs A, int64_t ncells)
+{
+    __shared__ CellWarpSmem smem_all[kWarps];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    CellWarpSmem& S = smem_all[wib];
+    const int64_t gc = (int64_t)blockIdx.x * kWarps + wib;
+    if (gc >= ncells) return;   // whole warp
+    const int t0 = A.cb.cstart[gc], t1 = A.cb.cstart[gc + 1];
+    if (t0 == t1) return;
+    const int k = jt_find(A.cprefix, A.nbox, gc);
+    const jt_box_dev& B = A.boxes[k];
+    const int nb = B.nb;
+    const int64_t local = gc - A.cprefix[k];
+    const int cx = (int)(local % nb), cy = (int)((local / nb) % nb), cz = (int)(local / ((int64_t)nb * nb));
+    // the 27 neighbour cells: lane l < 27 takes offset (l % 3 - 1, l / 3 % 3 - 1, l / 9 - 1)
+    int cnt = 0;
+    if (lane < 27) {
+        int nx = cx + lane % 3 - 1, ny = cy + (lane / 3) % 3 - 1, nz = cz + lane / 9 - 1;
+        float sx = 0.f, sy = 0.f, sz = 0.f;
+        if (nx < 0) { nx += nb; sx = -B.L; } else if (nx >= nb) { nx -= nb; sx = B.L; }
+        if (ny < 0) { ny += nb; sy = -B.L; } else if (ny >= nb) { ny -= nb; sy = B.L; }
+        if (nz < 0) { nz += nb; sz = -B.L; } else if (nz >= nb) { nz -= nb; sz = B.L; }
+        const int64_t key = B.cbase + ((int64_t)nz * nb + ny) * nb + nx;
+        const int first = A.cb.cstart[key];
+        cnt = A.cb.cstart[key + 1] - first;
+        S.nrange[lane] = make_int2(first, cnt);
+        S.nshift[lane] = make_float4(sx, sy, sz, 0.f);
+    }
+    int tot = cnt;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+    if (tot > JT_CELL_KMAX) {   // clustered: the tree walk takes these targets
+        for (int t = t0 + lane; t < t1; t += 32) {
+            const int2 id = A.cb.cid[t];
+            A.cb.tflag[A.pprefix[id.x] + id.y] = 1;
+        }
+        return;
+    }
+    __syncwarp();
+    const float rc2 = B.rc2, eps2 = B.eps2, c2s = B.c * B.c * ((float)kStab / kStabYMax);
+    const float slack = B.halfL * 9.5367431640625e-7f, rc2_keep = B.rc2 * 1.00001f;
+    const unsigned lt = (1u << lane) - 1u;
+    unsigned pairs = 0, cands = 0;
+    for (int base = t0; base < t1; base += 32) {
+        const int t = base + lane;
+        const bool valid = t < t1;
+        const float4 p = A.cb.cpos[valid ? t : base];
+        const int2 id = A.cb.cid[valid ? t : base];
+        const float si = p.w > 0.f ? 1.0f : -1.0f;
+        const float lox = warp_min(p.x), loy = warp_min(p.y), loz = warp_min(p.z);
+        const float hix = warp_max(p.x), hiy = warp_max(p.y), hiz = warp_max(p.z);
+        const float gcx = 0.5f * (lox + hix), gcy = 0.5f * (loy + hiy), gcz = 0.5f * (loz + hiz);
+        const float ghx = 0.5f * (hix - lox) + slack, ghy = 0.5f * (hiy - loy) + slack,
+                    ghz = 0.5f * (hiz - loz) + slack;
+        Acc3 pm = {0.f, 0.f, 0.f};
+        if (A.parts & 1) pm = pm_interp<ORDER, NG>(B, p);
+        Acc3 near = {0.f, 0.f, 0.f};
+        if (A.parts & 2) {
+            int nc = 0;
+            for (int nbr = 0; nbr < 27; nbr++) {
+                const int2 r = S.nrange[nbr];
+                const float4 sh = S.nshift[nbr];
+                for (int o = 0; o < r.y; o += 32) {
+                    bool keep = false;
+                    float4 c = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (o + lane < r.y) {
+                        c = A.cb.cpos[r.x + o + lane];
+                        c.x += sh.x;
+                        c.y += sh.y;
+                        c.z += sh.z;
+                        const float gx = gap1(c.x - gcx, ghx), gy = gap1(c.y - gcy, ghy), gz = gap1(c.z - gcz, ghz);
+                        keep = gx * gx + gy * gy + gz * gz <= rc2_keep;
+                    }
+                    const unsigned km = __ballot_sync(0xffffffffu, keep);
+                    if (keep) S.cand[nc + __popc(km & lt)] = c;
+                    nc += __popc(km);
+                    __syncwarp();
+                    if (nc >= 32) {
+                        if (valid) pairs += cell_chunk(S.cand, 32, p.x, p.y, p.z, si, rc2, eps2, c2s, near);
+                        cands += 32;
+                        __syncwarp();
+                        const float4 t2 = S.cand[32 + lane];
+                        __syncwarp();
+                        if (lane < nc - 32) S.cand[lane] = t2;
+                        nc -= 32;
+                        __syncwarp();
+                    }
+                }
+            }
+            if (nc > 0) {
+                if (valid) pairs += cell_chunk(S.cand, nc, p.x, p.y, p.z, si, rc2, eps2, c2s, near);
+                cands += nc;
+            }
+            __syncwarp();
+        }
+        if (valid) {
+            const jt_seg_dev& SG = A.segs[id.x];
+            const float ax = si * pm.x + near.x, ay = si * pm.y + near.y, az = si * pm.z + near.z;
+            SG.acc[id.y] = make_float4(ax, ay, az, 0.f);
+            if (A.kick_frac != 0.0f) {
+                // as k_walk_acc: the closing half kick, and with kick_frac
+                // 1.0 the next step's opening half kick after it
+                const float drag = B.kick_drag, h = 0.5f * B.dt;
+                float4 v = SG.vel[id.y];
+                v.x += (ax - drag * v.x) * h;
+                v.y += (ay - drag * v.y) * h;
+                v.z += (az - drag * v.z) * h;
+                if (A.kick_frac > 0.75f) {
+                    v.x += (ax - drag * v.x) * h;
+                    v.y += (ay - drag * v.y) * h;
+                    v.z += (az - drag * v.z) * h;
+                }
+                SG.vel[id.y] = v;
+            }
+        }
+    }
+    if (A.stats) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
+        if (lane == 0) {
+            atomicAdd(A.stats, (unsigned long long)pairs);
+            atomicAdd(A.stats + 2, (unsigned long long)cands * 32ull);
+        }
+    }
+}
+
+}  // namespace
+
+int jt_cell_scan_blocks(int64_t ncells) { return (int)((ncells + kScanB - 1) / kScanB); }
+
+int jt_b_cells(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_pprefix, int nseg,
+               int64_t npart, const int64_t* d_cprefix, int nbox, int64_t ncells, const jt_cell_bufs& cb,
+               int order, int ngrid, int parts, float kick_frac, unsigned long long* stats,
+               unsigned* d_err, cudaStream_t st)
+{
+    if (npart <= 0) return JT_OK;
+    if (int r = stab_ready()) return r;
+    CellArgs A;
+    A.segs = d_segs;
+    A.boxes = d_boxes;
+    A.pprefix = d_pprefix;
+    A.nseg = nseg;
+    A.nbox = nbox;
+    A.cprefix = d_cprefix;
+    A.cb = cb;
+    A.parts = parts;
+    A.kick_frac = kick_frac;
+    A.stats = stats;
+    A.err = d_err;
+    const unsigned gp = (unsigned)((npart + 255) / 256);
+    if (ncells > 0 && cudaMemsetAsync(cb.ccount, 0, sizeof(int) * (size_t)ncells, st) != cudaSuccess)
+        return JT_ECUDA;
+    k_cell_key<<<gp, 256, 0, st>>>(A, npart);
+    if (ncells > 0) {
+        const int nblk = jt_cell_scan_blocks(ncells);
+        k_scan_local<<<nblk, kScanB, 0, st>>>(cb.ccount, cb.cstart, ncells, cb.bsum);
+        k_scan_sums<<<1, kScanB, 0, st>>>(cb.bsum, nblk);
+        k_scan_add<<<nblk, kScanB, 0, st>>>(cb.cstart, ncells, cb.bsum, nblk);
+        k_cell_scatter<<<gp, 256, 0, st>>>(A, npart);
+        const unsigned gw = (unsigned)((ncells + kWarps - 1) / kWarps);
+        if (order == 3 && ngrid == 2) k_walk_cell<3, 2><<<gw, kWarps * 32, 0, st>>>(A, ncells);
+        else if (order == 3 && ngrid == 1) k_walk_cell<3, 1><<<gw, kWarps * 32, 0, st>>>(A, ncells);
+        else if (order == 2 && ngrid == 2) k_walk_cell<2, 2><<<gw, kWarps * 32, 0, st>>>(A, ncells);
+        else if (order == 2 && ngrid == 1) k_walk_cell<2, 1><<<gw, kWarps * 32, 0, st>>>(A, ncells);
+        else return JT_EINVAL;
+    }
+    return cudaGetLastError() == cudaSuccess ? JT_OK : JT_ECUDA;
+}
+
 int jt_b_walk(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_gprefix, int nseg,
               int64_t ngroups, const jt_tree_dev& pool, int order, int ngrid, int parts,
-              float kick_frac, unsigned long long* stats, unsigned* d_err, cudaStream_t st)
+              float kick_frac, unsigned long long* stats, unsigned* d_err, cudaStream_t st,
+              const int64_t* d_pprefix, const unsigned char* tflag)
 {
     if (ngroups <= 0) return JT_OK;
     if (int r = stab_ready()) return r;
@@ -1058,6 +1421,8 @@ int jt_b_walk(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t
     A.pool = pool;
     A.stats = stats;
     A.err = d_err;
+    A.pprefix = d_pprefix;
+    A.tflag = tflag;
     unsigned g = (unsigned)((ngroups + kWarps - 1) / kWarps);
     if (order == 3 && ngrid == 2) launch_variant(pick_variant(g, ngroups, A, st), g, A, st);
     else if (order == 3 && ngrid == 1) k_walk_acc<3, 1, 6, 32><<<g, kWarps * 32, 0, st>>>(A);
