@@ -187,7 +187,7 @@ struct jt_batch {
     Pool<int2> child, range;
     Pool<int> parent, flag;
     // near-field cell list (jt_b_cells)
-    Pool<int> ccount, cstart, cbsum, ccell;
+    Pool<int> ccount, cstart, cbsum, ccell, csegflag;
     Pool<unsigned> cslot;
     Pool<float4> cpos;
     Pool<int2> cid;
@@ -546,6 +546,7 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
         JT_TRY(B->cpos.ensure((size_t)std::max<int64_t>(P.npart, 1), &grew));
         JT_TRY(B->cid.ensure((size_t)std::max<int64_t>(P.npart, 1), &grew));
         JT_TRY(B->tflag.ensure((size_t)std::max<int64_t>(P.npart, 1), &grew));
+        JT_TRY(B->csegflag.ensure((size_t)std::max<int>(nseg, 1), &grew));
     }
 
     if (grew) B->gen++;
@@ -595,7 +596,9 @@ int force_pass(jt_batch* B, Plan& P, int parts, float kick_frac)
     JT_TRY(jt_b_sort_reorder(P.d_pre, P.d_bx, nseg, P.d_pp, P.npart, P.d_tp, P.nsorttiles, B->tickets.p,
                              B->d_err, st));
     cudaEventRecord(B->ev[1], st);
-    jt_b_build_trees(P.d_post, P.d_bx, nseg, P.d_ip, P.ninternal, P.d_pp, P.npart, st);
+    // with the cell walk the trees are built after it, for the segments whose
+    // particles it flagged (none for uniform data)
+    if (!P.cells) jt_b_build_trees(P.d_post, P.d_bx, nseg, P.d_ip, P.ninternal, P.d_pp, P.npart, st);
     cudaEventRecord(B->ev[2], st);
     for (auto& kv : P.by_M) {
         const int64_t M = kv.first, G = M * M * M;
@@ -630,10 +633,11 @@ int force_pass(jt_batch* B, Plan& P, int parts, float kick_frac)
     const unsigned char* tflag = nullptr;
     if (P.cells) {
         jt_cell_bufs cb = {B->ccount.p, B->cstart.p, B->cbsum.p, B->ccell.p, B->cslot.p,
-                           B->cpos.p, B->cid.p, B->tflag.p};
+                           B->cpos.p, B->cid.p, B->tflag.p, B->csegflag.p};
         JT_TRY(jt_b_cells(P.d_post, P.d_bx, P.d_pp, nseg, P.npart, P.d_cp, nbox, P.ncells, cb, B->order,
                           B->ngrid, parts, kick_frac, B->d_stats, B->d_err, st));
         tflag = B->tflag.p;
+        jt_b_build_trees(P.d_post, P.d_bx, nseg, P.d_ip, P.ninternal, P.d_pp, P.npart, st, B->csegflag.p);
         B->tm.launches += P.npart > 0 ? (P.ncells > 0 ? 6 : 1) : 0;
     }
     JT_TRY(jt_b_walk(P.d_post, P.d_bx, P.d_gp, nseg, P.ngroups, pool, B->order, B->ngrid, parts,
@@ -985,6 +989,7 @@ void jt_batch_destroy(jt_batch* B)
     B->child.release(); B->range.release(); B->parent.release(); B->flag.release();
     B->com.release(); B->bmin.release(); B->bmax.release(); B->quad0.release(); B->quad1.release();
     B->ccount.release(); B->cstart.release(); B->cbsum.release(); B->ccell.release(); B->cslot.release();
+    B->csegflag.release();
     B->cpos.release(); B->cid.release(); B->tflag.release();
     B->m30.release(); B->vals.release(); B->vals_alt.release(); B->keys_alt.release();
     B->hist.release(); B->status.release(); B->tickets.release(); B->desc.release();
@@ -1260,6 +1265,7 @@ int jt_batch_trim(jt_batch* B)
     B->child.release(); B->range.release(); B->parent.release(); B->flag.release();
     B->com.release(); B->bmin.release(); B->bmax.release(); B->quad0.release(); B->quad1.release();
     B->ccount.release(); B->cstart.release(); B->cbsum.release(); B->ccell.release(); B->cslot.release();
+    B->csegflag.release();
     B->cpos.release(); B->cid.release(); B->tflag.release();
     B->m30.release(); B->vals.release(); B->vals_alt.release(); B->keys_alt.release();
     B->hist.release(); B->status.release(); B->tickets.release();

@@ -219,7 +219,7 @@ void jt_launch_moments_rc(jt_tree_dev t, const float4* pos, float mass, float bo
 // batched tree build over segments (jt_tree.cu)
 void jt_b_build_trees(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, int nseg,
                       const int64_t* d_iprefix, int64_t ninternal, const int64_t* d_pprefix,
-                      int64_t nleaves, cudaStream_t st);
+                      int64_t nleaves, cudaStream_t st, const int* segflag = nullptr);
 
 // RCOMPAT PM (jt_pm.cu): one CIC grid of the caller-order particles, the
 // reference's Green's function in place, C2R to the potential.
@@ -280,6 +280,7 @@ int jt_b_walk(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t
 struct jt_cell_bufs {
     int* ccount; int* cstart; int* bsum; int* ccell; unsigned* cslot;
     float4* cpos; int2* cid; unsigned char* tflag;
+    int* segflag;                 // per segment: some particle is flagged (its tree is built)
 };
 int jt_b_cells(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_pprefix, int nseg,
                int64_t npart, const int64_t* d_cprefix, int nbox, int64_t ncells, const jt_cell_bufs& cb,

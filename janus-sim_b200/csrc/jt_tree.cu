@@ -195,11 +195,12 @@ namespace {
 // parent is set to -1 and each internal node's arrival flag is cleared here,
 // so no separate reset pass is needed.
 __global__ void k_b_karras(const jt_seg_dev* __restrict__ segs, const int64_t* __restrict__ iprefix,
-                           int nseg)
+                           int nseg, const int* __restrict__ segflag)
 {
     int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= iprefix[nseg]) return;
     const int g = jt_find(iprefix, nseg, q);
+    if (segflag && !segflag[g]) return;   // no particle of this segment needs its tree
     const int64_t i = q - iprefix[g];
     const jt_seg_dev& S = segs[g];
     const jt_tree_dev& T = S.tree;
@@ -245,11 +246,12 @@ __global__ void k_b_karras(const jt_seg_dev* __restrict__ segs, const int64_t* _
 
 // leaves of every segment (particle masses from the box table)
 __global__ void k_b_moments(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ boxes,
-                            const int64_t* __restrict__ pprefix, int nseg)
+                            const int64_t* __restrict__ pprefix, int nseg, const int* __restrict__ segflag)
 {
     int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= pprefix[nseg]) return;
     const int g = jt_find(pprefix, nseg, q);
+    if (segflag && !segflag[g]) return;
     const int64_t j = q - pprefix[g];
     const jt_seg_dev& S = segs[g];
     const jt_tree_dev& T = S.tree;
@@ -301,10 +303,11 @@ __global__ void k_b_moments(const jt_seg_dev* __restrict__ segs, const jt_box_de
 
 void jt_b_build_trees(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, int nseg,
                       const int64_t* d_iprefix, int64_t ninternal, const int64_t* d_pprefix,
-                      int64_t nleaves, cudaStream_t st)
+                      int64_t nleaves, cudaStream_t st, const int* segflag)
 {
     if (ninternal > 0)
-        k_b_karras<<<(unsigned)((ninternal + 255) / 256), 256, 0, st>>>(d_segs, d_iprefix, nseg);
+        k_b_karras<<<(unsigned)((ninternal + 255) / 256), 256, 0, st>>>(d_segs, d_iprefix, nseg, segflag);
     if (nleaves > 0)
-        k_b_moments<<<(unsigned)((nleaves + 255) / 256), 256, 0, st>>>(d_segs, d_boxes, d_pprefix, nseg);
+        k_b_moments<<<(unsigned)((nleaves + 255) / 256), 256, 0, st>>>(d_segs, d_boxes, d_pprefix, nseg,
+                                                                        segflag);
 }

@@ -1107,6 +1107,9 @@ __global__ void k_cell_key(CellArgs A, int64_t npart)
     if (B.nb == 0) {
         A.cb.tflag[i] = 1;
         A.cb.ccell[i] = -1;
+        // the tree walk of a flagged particle walks both species' trees
+        if (B.seg[0] >= 0) A.cb.segflag[B.seg[0]] = 1;
+        if (B.seg[1] >= 0) A.cb.segflag[B.seg[1]] = 1;
         return;
     }
     const float4 p = SG.pos[i - A.pprefix[g]];
@@ -1271,6 +1274,9 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk_cell(CellArgs A, int64_t n
             const int2 id = A.cb.cid[t];
             A.cb.tflag[A.pprefix[id.x] + id.y] = 1;
         }
+        // the tree walk of a flagged particle walks both species' trees
+        if (lane == 0 && B.seg[0] >= 0) A.cb.segflag[B.seg[0]] = 1;
+        if (lane == 0 && B.seg[1] >= 0) A.cb.segflag[B.seg[1]] = 1;
         return;
     }
     __syncwarp();
@@ -1387,6 +1393,7 @@ int jt_b_cells(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_
     const unsigned gp = (unsigned)((npart + 255) / 256);
     if (ncells > 0 && cudaMemsetAsync(cb.ccount, 0, sizeof(int) * (size_t)ncells, st) != cudaSuccess)
         return JT_ECUDA;
+    if (cudaMemsetAsync(cb.segflag, 0, sizeof(int) * (size_t)nseg, st) != cudaSuccess) return JT_ECUDA;
     k_cell_key<<<gp, 256, 0, st>>>(A, npart);
     if (ncells > 0) {
         const int nblk = jt_cell_scan_blocks(ncells);
