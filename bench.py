@@ -37,13 +37,17 @@ sys.path.insert(0, os.path.join(ROOT, "janus-sim_b200"))
 METRIC = "TreePM particle-steps/s at 2x224^3"
 UNIT = "particle-steps/s"
 
-# flops per interaction of the walk (k_walk_acc), each exp, rcp and rsqrt
+# flops per interaction of the short-range force, each exp, rcp and rsqrt
 # counted as one flop: a particle pair inside r_cut (split kernel S(x) by
-# A&S 7.1.26) 40; a monopole + quadrupole node 100.  The 8-flop distance test
-# of every candidate is overhead and is not counted as useful work.
+# A&S 7.1.26) 40; a monopole + quadrupole node 100.  The distance test of
+# every candidate, and the force the cell walk computes and discards for
+# candidates outside r_cut, are overhead and not counted as useful work.
 FLOPS_PAIR = 40.0
 FLOPS_NODE = 100.0
-WALK_DRAM_BYTES_PER_PARTICLE = 643.0
+# DRAM bytes of one k_walk_cell launch per particle, from ncu on the 2x112^3
+# case (profiles/k_walk_cell_2x112.md: 0.520 GB read + 0.083 GB written for
+# 2,809,856 particles); it grows with N (particles and PM grids scale alike)
+WALK_DRAM_BYTES_PER_PARTICLE = 214.0
 
 
 def workload(n_side=224, L=250.0, M=512):
@@ -466,8 +470,10 @@ def run_ours(args, ws, rank, local):
     e2e = ws * 2 * n * K / e2e_t
     bytes_state = 2 * n * 3 * 4 * 3     # positions, velocities, accelerations; both species
 
-    # roofline of the dominant kernel: the walk (FP32 pipe)
-    walk_ms = stages["walk_ms"] / K
+    # roofline of the dominant kernel: the near-field cell walk (FP32 pipe),
+    # timed alone by its own events (the walk stage also holds the cell list
+    # build and the tree walk of flagged particles, none at this density)
+    walk_ms = (stages["cellwalk_ms"] if stages.get("cellwalk_ms", 0.0) > 0 else stages["walk_ms"]) / K
     pairs = stages["pair_interactions"] / K
     nodes = stages["node_interactions"] / K
     cands = stages["candidates"] / K
@@ -482,9 +488,6 @@ def run_ours(args, ws, rank, local):
         hbm_src = "measured"
     except Exception:
         hbm_src = "fallback"
-    # DRAM bytes of one walk launch per particle, from ncu on the 2x112^3 case
-    # (profiles/k_walk_acc_2x112.md: 1.728 GB for 2,809,856 particles); the
-    # walk's traffic grows with N (particles, trees and PM grids scale alike)
     walk_traffic = WALK_DRAM_BYTES_PER_PARTICLE * 2 * n if args.grid * 224 == 512 * args.n_side else None
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -518,7 +521,7 @@ def run_ours(args, ws, rank, local):
                        "parallelism": "replicas" if ws > 1 else "single"},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": bytes_state * ws,
                     "d2h_bytes_per_step": bytes_state * ws},
-            "roofline": {"bound": "fp32", "kernel": "k_walk_acc", "achieved": achieved,
+            "roofline": {"bound": "fp32", "kernel": "k_walk_cell", "achieved": achieved,
                          "peak": peak_fp32, "unit": "TFLOP/s", "frac": achieved / peak_fp32,
                          "traffic": walk_traffic,
                          "peak_source": "measured (jt_fp32_peak FMA kernel, same run)",

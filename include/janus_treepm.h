@@ -106,6 +106,7 @@ typedef struct jt_timings {
     int64_t pair_interactions;  /* particle pairs inside r_cut */
     int64_t node_interactions;  /* multipole node interactions */
     int64_t candidates;         /* particle candidates distance-tested */
+    double cellwalk_ms;  /* the near-field cell walk kernel alone (part of walk_ms) */
 } jt_timings;
 
 /* Create a handle on the current CUDA device.  Replaces the constructor and

@@ -202,7 +202,7 @@ struct jt_batch {
     std::map<int, Bucket> buckets;
     unsigned* d_err = nullptr;
     unsigned long long* d_stats = nullptr;
-    cudaEvent_t ev[8] = {};
+    cudaEvent_t ev[10] = {};            // 8, 9: around the cell walk kernel
     bool pending = false;               // a pass's events await jtb_finish
     jt_timings tm = {};
     int64_t phase[4] = {0, 0, 0, 0};
@@ -631,11 +631,14 @@ int force_pass(jt_batch* B, Plan& P, int parts, float kick_frac)
     pool.quad1 = B->quad1.p;
     pool.m30 = B->m30.p;
     const unsigned char* tflag = nullptr;
-    if (P.cells) {
+    if (!P.cells) {
+        cudaEventRecord(B->ev[8], st);
+        cudaEventRecord(B->ev[9], st);
+    } else {
         jt_cell_bufs cb = {B->ccount.p, B->cstart.p, B->cbsum.p, B->ccell.p, B->cslot.p,
                            B->cpos.p, B->cid.p, B->tflag.p, B->csegflag.p};
         JT_TRY(jt_b_cells(P.d_post, P.d_bx, P.d_pp, nseg, P.npart, P.d_cp, nbox, P.ncells, cb, B->order,
-                          B->ngrid, parts, kick_frac, B->d_stats, B->d_err, st));
+                          B->ngrid, parts, kick_frac, B->d_stats, B->d_err, st, B->ev[8], B->ev[9]));
         tflag = B->tflag.p;
         jt_b_build_trees(P.d_post, P.d_bx, nseg, P.d_ip, P.ninternal, P.d_pp, P.npart, st, B->csegflag.p);
         B->tm.launches += P.npart > 0 ? (P.ncells > 0 ? 6 : 1) : 0;
@@ -683,6 +686,7 @@ int finish(jt_batch* B)
         B->tm.fft_ms += elapsed(B->ev[3], B->ev[6]);
         B->tm.kspace_ms += elapsed(B->ev[4], B->ev[5]);
         B->tm.walk_ms += elapsed(B->ev[6], B->ev[7]);
+        B->tm.cellwalk_ms += elapsed(B->ev[8], B->ev[9]);
         B->pending = false;
     }
     B->tm.pair_interactions += (int64_t)v[0];

@@ -285,7 +285,7 @@ struct jt_cell_bufs {
 int jt_b_cells(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_pprefix, int nseg,
                int64_t npart, const int64_t* d_cprefix, int nbox, int64_t ncells, const jt_cell_bufs& cb,
                int order, int ngrid, int parts, float kick_frac, unsigned long long* stats,
-               unsigned* d_err, cudaStream_t st);
+               unsigned* d_err, cudaStream_t st, cudaEvent_t ev_walk0, cudaEvent_t ev_walk1);
 int jt_cell_scan_blocks(int64_t ncells);
 
 // kick v += (a - drag v) frac*dt and drift x += v frac*dt with each box's own

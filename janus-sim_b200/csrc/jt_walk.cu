@@ -1237,8 +1237,11 @@ __device__ __forceinline__ unsigned cell_chunk(const float4* __restrict__ cand, 
     return hits;
 }
 
+#ifndef JT_CELL_MINB
+#define JT_CELL_MINB 6
+#endif
 template <int ORDER, int NG>
-__global__ void __launch_bounds__(kWarps * 32) k_walk_cell(CellArgs A, int64_t ncells)
+__global__ void __launch_bounds__(kWarps * 32, JT_CELL_MINB) k_walk_cell(CellArgs A, int64_t ncells)
 {
     __shared__ CellWarpSmem smem_all[kWarps];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -1374,9 +1377,13 @@ int jt_cell_scan_blocks(int64_t ncells) { return (int)((ncells + kScanB - 1) / k
 int jt_b_cells(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_pprefix, int nseg,
                int64_t npart, const int64_t* d_cprefix, int nbox, int64_t ncells, const jt_cell_bufs& cb,
                int order, int ngrid, int parts, float kick_frac, unsigned long long* stats,
-               unsigned* d_err, cudaStream_t st)
+               unsigned* d_err, cudaStream_t st, cudaEvent_t ev_walk0, cudaEvent_t ev_walk1)
 {
-    if (npart <= 0) return JT_OK;
+    cudaEventRecord(ev_walk0, st);   // both recorded on every path (no stale events)
+    if (npart <= 0) {
+        cudaEventRecord(ev_walk1, st);
+        return JT_OK;
+    }
     if (int r = stab_ready()) return r;
     CellArgs A;
     A.segs = d_segs;
@@ -1395,6 +1402,7 @@ int jt_b_cells(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_
         return JT_ECUDA;
     if (cudaMemsetAsync(cb.segflag, 0, sizeof(int) * (size_t)nseg, st) != cudaSuccess) return JT_ECUDA;
     k_cell_key<<<gp, 256, 0, st>>>(A, npart);
+    if (ncells == 0) cudaEventRecord(ev_walk1, st);
     if (ncells > 0) {
         const int nblk = jt_cell_scan_blocks(ncells);
         k_scan_local<<<nblk, kScanB, 0, st>>>(cb.ccount, cb.cstart, ncells, cb.bsum);
@@ -1402,11 +1410,13 @@ int jt_b_cells(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_
         k_scan_add<<<nblk, kScanB, 0, st>>>(cb.cstart, ncells, cb.bsum, nblk);
         k_cell_scatter<<<gp, 256, 0, st>>>(A, npart);
         const unsigned gw = (unsigned)((ncells + kWarps - 1) / kWarps);
+        cudaEventRecord(ev_walk0, st);
         if (order == 3 && ngrid == 2) k_walk_cell<3, 2><<<gw, kWarps * 32, 0, st>>>(A, ncells);
         else if (order == 3 && ngrid == 1) k_walk_cell<3, 1><<<gw, kWarps * 32, 0, st>>>(A, ncells);
         else if (order == 2 && ngrid == 2) k_walk_cell<2, 2><<<gw, kWarps * 32, 0, st>>>(A, ncells);
         else if (order == 2 && ngrid == 1) k_walk_cell<2, 1><<<gw, kWarps * 32, 0, st>>>(A, ncells);
         else return JT_EINVAL;
+        cudaEventRecord(ev_walk1, st);
     }
     return cudaGetLastError() == cudaSuccess ? JT_OK : JT_ECUDA;
 }

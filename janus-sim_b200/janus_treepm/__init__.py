@@ -80,7 +80,7 @@ class jt_timings(C.Structure):
         ("kick_drift_ms", C.c_double), ("total_ms", C.c_double),
         ("interactions", C.c_int64), ("launches", C.c_int64),
         ("pair_interactions", C.c_int64), ("node_interactions", C.c_int64),
-        ("candidates", C.c_int64),
+        ("candidates", C.c_int64), ("cellwalk_ms", C.c_double),
     ]
 
 

@@ -46,7 +46,9 @@ def test_struct_layouts_match_header():
     assert C.sizeof(J.jt_config) == 96
     assert J.jt_config.G_mass_plus.offset == 56 and J.jt_config.k_min.offset == 64
     assert J.jt_config.pm_order.offset == J.jt_config.integrator.offset + 4
-    assert C.sizeof(J.jt_timings) == 8 * 8 + 8 * 5
+    # 8 doubles, 5 int64 counters, cellwalk_ms
+    assert C.sizeof(J.jt_timings) == 8 * 8 + 8 * 5 + 8
+    assert J.jt_timings.cellwalk_ms.offset == 8 * 8 + 8 * 5
 
 
 def test_strerror_and_version():
