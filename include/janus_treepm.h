@@ -422,6 +422,8 @@ typedef struct jt_serve_stats {
     int64_t max_jobs_per_step;
     int64_t swapped_out;       /* idle jobs moved to host to admit others */
     int64_t trims;             /* scratch pools released to make room */
+    double  admit_s;           /* wall time admitting jobs (state to the device) */
+    double  evict_s;           /* wall time evicting and swapping out jobs (to host) */
 } jt_serve_stats;
 
 #define JT_JOB_QUEUED    0

@@ -72,6 +72,7 @@ struct jt_server {
     int64_t trims = 0;
     double busy_s = 0.0;
     size_t peak_device = 0;
+    double admit_s = 0.0, evict_s = 0.0;   // wall time in admissions / evictions
     int max_resident = 0;
 };
 
@@ -86,6 +87,12 @@ size_t device_bytes(jt_server* S)
 
 int admit(jt_server* S, Job& j)
 {
+    const double t_in = now_s();
+    struct Clock {
+        jt_server* S;
+        double t;
+        ~Clock() { S->admit_s += now_s() - t; }
+    } clock_{S, t_in};
     const float* h = j.host;
     const size_t np = j.n_p, nm = j.n_m;
     int box = -1;
@@ -113,16 +120,16 @@ int admit(jt_server* S, Job& j)
 // and re-admitted when it has a request again).
 int evict(jt_server* S, Job& j, bool final)
 {
+    struct Clock {
+        jt_server* S;
+        double t;
+        ~Clock() { S->evict_s += now_s() - t; }
+    } clock_{S, now_s()};
     float* h = j.host;
     const size_t np = j.n_p, nm = j.n_m;
     int r = jt_batch_get_state(S->B, j.box, h, h + 3 * np, h + 6 * np, h + 6 * np + 3 * nm, JT_MEM_HOST);
     if (r != JT_OK) return r;
     j.acc_saved = false;
-    if (!j.host_acc &&
-        cudaMallocHost((void**)&j.host_acc, sizeof(float) * 3 * (np + nm)) != cudaSuccess) {
-        j.host_acc = nullptr;
-        cudaGetLastError();
-    }
     // keep the forces of the state leaving the device (none yet: a swapped-out
     // job then comes back with a force pass); a finished job's forces are
     // its result as much as its state (jt_server_get_accel)
@@ -329,7 +336,16 @@ int jt_server_add_job(jt_server* S, const jt_config* cfg, const float* pos_p, co
     j.fft_ws = fft_ws_of(*cfg);
     if (need_of(j.persistent, j.scratch, j.fft_ws) > S->budget) return JT_EBUSY;   // can never fit
     const size_t floats = 6 * (n_p + n_m);
+    // the state and, beside it, the forces a swapped-out or finished job
+    // keeps: both pinned once here (page-locking costs far more than the
+    // copies, so it stays out of the admissions and evictions)
     if (cudaMallocHost((void**)&j.host, sizeof(float) * floats) != cudaSuccess) return JT_ENOMEM;
+    if (cudaMallocHost((void**)&j.host_acc, sizeof(float) * 3 * (n_p + n_m)) != cudaSuccess) {
+        cudaFreeHost(j.host);
+        j.host = nullptr;
+        j.host_acc = nullptr;
+        return JT_ENOMEM;
+    }
     float* h = j.host;
     std::memcpy(h, pos_p, sizeof(float) * 3 * n_p);
     if (vel_p) std::memcpy(h + 3 * n_p, vel_p, sizeof(float) * 3 * n_p);
@@ -454,6 +470,8 @@ int jt_server_stats(jt_server* S, jt_serve_stats* out)
     s.max_latency_s = S->lat.empty() ? 0.0 : *std::max_element(S->lat.begin(), S->lat.end());
     s.busy_s = S->busy_s;
     s.peak_device_bytes = (int64_t)S->peak_device;
+    s.admit_s = S->admit_s;
+    s.evict_s = S->evict_s;
     s.max_jobs_per_step = S->max_resident;
     s.swapped_out = S->swapped;
     s.trims = S->trims;

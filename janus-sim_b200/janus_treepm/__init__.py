@@ -215,7 +215,8 @@ class jt_serve_stats(C.Structure):
         ("admitted", C.c_int64), ("evicted", C.c_int64), ("admission_waits", C.c_int64),
         ("p50_latency_s", C.c_double), ("p99_latency_s", C.c_double), ("max_latency_s", C.c_double),
         ("busy_s", C.c_double), ("peak_device_bytes", C.c_int64), ("max_jobs_per_step", C.c_int64),
-        ("swapped_out", C.c_int64), ("trims", C.c_int64),
+        ("swapped_out", C.c_int64), ("trims", C.c_int64), ("admit_s", C.c_double),
+        ("evict_s", C.c_double),
     ]
 
 
