@@ -336,14 +336,31 @@ int bucket_ensure(jt_batch* B, Bucket& k, int M, int count)
         JT_TRY(dalloc(&k.ranges, (size_t)count * nt));
         k.cap = count;
     }
-    // plans for the full chunk and the remainder of both transform counts
+    // plans for every power-of-two batch the executions of this count use:
+    // full chunks of fft_chunk(M) (a power of two) and the remainder's binary
+    // decomposition, so a bucket holds at most log2(chunk) + 1 plans per
+    // direction whatever counts later passes bring (creating a plan inside a
+    // pass costs more than the transforms)
     const int ch = fft_chunk(M);
     const int nr = ngrid * count, nc = 3 * ngrid * count;
-    JT_TRY(make_plan(B, k.r2c, M, std::min(ch, nr), true));
-    JT_TRY(make_plan(B, k.r2c, M, nr % ch, true));
-    JT_TRY(make_plan(B, k.c2r, M, std::min(ch, nc), false));
-    JT_TRY(make_plan(B, k.c2r, M, nc % ch, false));
+    for (int dir = 0; dir < 2; dir++) {
+        const int n = dir == 0 ? nr : nc;
+        auto& pl = dir == 0 ? k.r2c : k.c2r;
+        if (n >= ch) JT_TRY(make_plan(B, pl, M, ch, dir == 0));
+        for (int b = 1; b < ch; b <<= 1)
+            if ((n % ch) & b) JT_TRY(make_plan(B, pl, M, b, dir == 0));
+    }
     return JT_OK;
+}
+
+// largest batch of one execution for n transforms left: a full chunk, else
+// the highest power of two in n
+int fft_batch(int n, int ch)
+{
+    if (n >= ch) return ch;
+    int b = 1;
+    while (b * 2 <= n) b <<= 1;
+    return b;
 }
 
 // Run n transforms of a bucket in chunks of at most fft_chunk(M).
@@ -351,12 +368,13 @@ int exec_r2c(Bucket& K, int n)
 {
     const int64_t G = (int64_t)K.M * K.M * K.M, Gc = (int64_t)K.M * K.M * (K.M / 2 + 1);
     const int ch = fft_chunk(K.M);
-    for (int off = 0; off < n; off += ch) {
-        const int b = std::min(ch, n - off);
+    for (int off = 0; off < n;) {
+        const int b = fft_batch(n - off, ch);
         auto it = K.r2c.find(b);
         if (it == K.r2c.end()) return JT_ECUDA;   // bucket_ensure made every size a pass uses
         if (cufftExecR2C(it->second, K.rho + off * G, (cufftComplex*)(K.rho_k + off * Gc)) != CUFFT_SUCCESS)
             return JT_ECUDA;
+        off += b;
     }
     return JT_OK;
 }
@@ -365,12 +383,13 @@ int exec_c2r(Bucket& K, int n)
 {
     const int64_t G = (int64_t)K.M * K.M * K.M, Gc = (int64_t)K.M * K.M * (K.M / 2 + 1);
     const int ch = fft_chunk(K.M);
-    for (int off = 0; off < n; off += ch) {
-        const int b = std::min(ch, n - off);
+    for (int off = 0; off < n;) {
+        const int b = fft_batch(n - off, ch);
         auto it = K.c2r.find(b);
         if (it == K.c2r.end()) return JT_ECUDA;
         if (cufftExecC2R(it->second, (cufftComplex*)(K.force_k + off * Gc), K.force + off * G) != CUFFT_SUCCESS)
             return JT_ECUDA;
+        off += b;
     }
     return JT_OK;
 }
