@@ -232,3 +232,43 @@ def test_async_checkpoint_overlaps_the_next_step(tmp_path):
         assert np.abs(x - y).max() <= 1e-5 * max(1.0, np.abs(y).max())
     B.close()
     B2.close()
+
+
+def test_cell_walk_matches_the_tree_walk():
+    """The near-field cell walk against the tree walk alone (JT_WALK_CELLS=0)
+    on uniform boxes at theta = 0.1, where the tree accepts no multipole
+    inside r_cut: the same pairs, in another order (forces p99 within 2e-5
+    of rms), and the same pair count to a few borderline pairs at r_cut.  A box
+    with fewer than 3 cells per axis takes the tree walk either way."""
+    import os
+    out = {}
+    for cells in ("1", "0"):
+        os.environ["JT_WALK_CELLS"] = cells
+        try:
+            B = J.Batch()
+            ids = []
+            # the third box: r_cut = 8 in L = 20, 2 cells per axis
+            for k, (L, M, n, rc) in enumerate(((60.0, 32, 20, 0.0), (40.0, 64, 16, 0.0), (20.0, 16, 8, 8.0))):
+                rng = np.random.default_rng(70 + k)
+                pp = rng.uniform(-L / 2, L / 2, (n ** 3, 3)).astype(np.float32)
+                pm = rng.uniform(-L / 2, L / 2, (n ** 3, 3)).astype(np.float32)
+                cfg = J.Config(box_L=L, pm_grid=M, theta=0.1, softening=0.02 * L / n, mu=3.0,
+                               G_mass_plus=1e-3, r_cut=rc)
+                ids.append(B.add(cfg, pp, None, pm, None))
+            B.forces(ids)
+            out[cells] = ([B.accel(i) for i in ids], B.timings())
+            B.close()
+        finally:
+            os.environ.pop("JT_WALK_CELLS", None)
+    # a pair right at r_cut can fall on either side of the cut between the
+    # two paths' rounding (S(2.25) = 1.8 % of its Newtonian force), and the
+    # deposit's atomics differ in order: p99 and max bars, not max alone
+    for (ap, am), (bp, bm) in zip(out["1"][0], out["0"][0]):
+        for a, b in ((ap, bp), (am, bm)):
+            rms = float(np.sqrt(np.mean(np.sum(b.astype(np.float64) ** 2, axis=1))))
+            d = np.linalg.norm(a.astype(np.float64) - b, axis=1) / rms
+            assert np.percentile(d, 99) <= 2e-5 and d.max() <= 2e-3, (np.percentile(d, 99), d.max())
+    p1, p0 = out["1"][1]["pair_interactions"], out["0"][1]["pair_interactions"]
+    assert abs(p1 - p0) <= 1e-4 * p0, (p1, p0)
+    # with the cells off the cell-walk events are recorded back to back
+    assert out["1"][1]["cellwalk_ms"] > 0.0 and out["0"][1]["cellwalk_ms"] < 0.01
