@@ -168,9 +168,10 @@ int  jt_get_accel(jt_handle* h, float* acc_p, float* acc_m, int mem);
  * erfc; a same-sign pair contributes m / r_p^3, an opposite-sign pair
  * -exp(-x)(1 + x) m / r_p^3 with x = r_p / lambda(z), lambda(z) = lambda_0
  * sqrt(1 + z) quantised down to 0.1; theta and softening are rounded to
- * 1e-3.  The PM part is unchanged.  Compatibility mode only (JT_EINVAL for
- * lambda_0 > 0.01 on a JT_ACCURATE handle); lambda_0 <= 0.01 turns it off.
- * Takes effect at the next force evaluation. */
+ * 1e-3.  The PM part is unchanged.  On a JT_ACCURATE handle the screening
+ * is the split model's instead (jt_batch_set_screening, applied to the
+ * handle's box and kept across jt_set_state).  lambda_0 <= 0.01 turns it
+ * off.  Takes effect at the next force evaluation. */
 int  jt_set_screening(jt_handle* h, double lambda_0, double z);
 
 /* Read the state back in the caller's order (get_particles, :5470).  Any
@@ -365,6 +366,20 @@ int  jt_batch_add_zeldovich(jt_batch* b, const jt_config* cfg, const jt_ics_para
 int  jt_batch_checkpoint_async(jt_batch* b, int box_id, const char* path,
                                const jt_snapshot_meta* meta);
 int  jt_batch_checkpoint_wait(jt_batch* b);
+/* Yukawa screening of one box's opposite-species pairs in the split model:
+ * kappa = 1 / lambda, lambda = lambda_0 sqrt(1 + z) (no quantisation; the
+ * reference's set_lambda_0 / set_current_z, src/nbody_gpu_twopass.rs
+ * :2305-2312, screening factor :1000-1017).  Same-species pairs stay
+ * Newtonian; an opposite-species pair has the potential -e^{-kappa r} / r.
+ * The Gaussian split applies to both kernels: the box deposits the signed
+ * source D and the unsigned source S, the k-space kernel gives D
+ * (G_N + G_Y) / 2 and S (G_N - G_Y) / 2 with G_Y = 4 pi e^{-(k^2 + kappa^2)
+ * r_s^2} / (k^2 + kappa^2), and the short-range walk evaluates opposite-
+ * species pairs with the Yukawa short kernel (1 / 2r) [e^{-kappa r}
+ * erfc(r / 2r_s - kappa r_s) + e^{kappa r} erfc(r / 2r_s + kappa r_s)],
+ * directly (no multipoles).  Costs a second deposit and twice the FFT work
+ * of the box.  lambda_0 <= 0.01 turns it off. */
+int  jt_batch_set_screening(jt_batch* b, int box_id, double lambda_0, double z);
 /* Free one box's device state; its id may be reused by a later add. */
 int  jt_batch_remove(jt_batch* b, int box_id);
 /* Accelerations of the listed boxes at their current positions (JT_PART_*). */

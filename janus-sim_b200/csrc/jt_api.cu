@@ -55,8 +55,9 @@ struct jt_handle {
     jt_batch* batch = nullptr;
     int box_id = -1;
     bool dbg_ready = false;            // debug-tree buffers (accurate mode)
-    // Yukawa screening of opposite-sign pairs (compatibility mode):
-    // lambda_0 > 0.01 selects the screened walk
+    // Yukawa screening of opposite-sign pairs: lambda_0 > 0.01 selects the
+    // screened walk (compatibility mode) or the screened split (accurate
+    // mode, applied to the handle's batch box)
     double lambda_0 = 0.0, z = 0.0;
 };
 
@@ -208,6 +209,7 @@ int alloc_particles(jt_handle* h, int64_t n0, int64_t n1)
     for (int s = 0; s < 2; s++) JT_TRY(dalloc(&h->gmap[s], nn[s]));
     if (h->batch) {
         JT_TRY(jtb_add_empty(h->batch, &h->cfg, n0, n1, &h->box_id));
+        if (h->lambda_0 > 0.01) JT_TRY(jt_batch_set_screening(h->batch, h->box_id, h->lambda_0, h->z));
     } else {
         for (int s = 0; s < 2; s++) {
             int64_t n = nn[s];
@@ -896,7 +898,7 @@ int jt_set_screening(jt_handle* h, double lambda_0, double z)
 {
     if (!h || !(lambda_0 >= 0.0) || !(z > -1.0) || !std::isfinite(lambda_0) || !std::isfinite(z))
         return JT_EINVAL;
-    if (h->cfg.mode != JT_RCOMPAT && lambda_0 > 0.01) return JT_EINVAL;
+    if (h->batch && h->box_id >= 0) JT_TRY(jt_batch_set_screening(h->batch, h->box_id, lambda_0, z));
     if (h->lambda_0 != lambda_0 || h->z != z) h->acc_valid = false;
     h->lambda_0 = lambda_0;
     h->z = z;

@@ -157,7 +157,9 @@ struct Plan {
     std::vector<int64_t> pprefix, iprefix, tprefix, gprefix, ptprefix, kprefix, cprefix;
     int64_t npart = 0, ninternal = 0, nsorttiles = 0, ngroups = 0, npmtiles = 0, nmodes = 0, ncells = 0;
     bool cells = false;                   // the near-field cell walk runs (jt_b_cells)
+    bool screened = false;                // some box is screened (second source, Yukawa tables)
     std::map<int, std::vector<int>> by_M; // M -> boxes (positions in ids)
+    std::map<int, int> nslots;            // M -> bucket slots (a screened box takes two: D, then S)
     int maxT = 1;
     size_t table_bytes = 0;
     const jt_seg_dev* d_pre = nullptr;
@@ -272,6 +274,8 @@ void box_release(jt_box_state* b)
         dfree(b->id[s]); dfree(b->id_b[s]);
     }
     dfree(b->tabs);
+    dfree(b->ytab);
+    b->kappa = 0.0;
 }
 
 int tile_shift_of(int M)
@@ -436,7 +440,16 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
     JT_TRY(B->status.ensure((size_t)stiles * 4 * 256, &grew));
     JT_TRY(B->tickets.ensure(4, &grew));
     for (int k = 0; k < nb; k++) P.by_M[B->boxes[ids[k]]->M].push_back(k);
-    for (auto& kv : P.by_M) JT_TRY(bucket_ensure(B, B->buckets[kv.first], kv.first, (int)kv.second.size()));
+    std::vector<int> slot(nb);
+    for (auto& kv : P.by_M) {
+        int q = 0;
+        for (int k : kv.second) {
+            slot[k] = q;
+            q += B->boxes[ids[k]]->ytab ? 2 : 1;
+        }
+        P.nslots[kv.first] = q;
+    }
+    for (auto& kv : P.nslots) JT_TRY(bucket_ensure(B, B->buckets[kv.first], kv.first, kv.second));
     if (B->fft_dirty || B->fftws.cap < B->fft_need) {
         bool ws_grew = false;
         JT_TRY(B->fftws.ensure(B->fft_need, &ws_grew));
@@ -449,9 +462,6 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
         }
         B->fft_dirty = false;
     }
-    std::vector<int> slot(nb);
-    for (auto& kv : P.by_M)
-        for (size_t q = 0; q < kv.second.size(); q++) slot[kv.second[q]] = (int)q;
 
     int64_t o_node = 0, o_part = 0, o_tile = 0;
     P.pprefix.push_back(0); P.iprefix.push_back(0); P.tprefix.push_back(0); P.gprefix.push_back(0);
@@ -492,6 +502,17 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
         d.force = K.force + (size_t)q * 3 * b->ngrid * G;
         d.tabs = b->tabs;
         d.ranges = K.ranges + (size_t)q * d.ntiles;
+        if (b->ytab) {
+            // the unsigned source's grids sit in the next slot
+            d.rho_s = d.rho + (size_t)b->ngrid * G;
+            d.rho_s_k = d.rho_k + (size_t)b->ngrid * Gc;
+            d.force_s_k = d.force_k + (size_t)3 * b->ngrid * Gc;
+            d.force_s = d.force + (size_t)3 * b->ngrid * G;
+            d.ytab = b->ytab;
+            d.ky2 = (float)(b->kappa * b->kappa);
+            d.yfac = (float)std::exp(-b->kappa * b->kappa * c.r_s * c.r_s);
+            P.screened = true;
+        }
         d.seg[0] = d.seg[1] = -1;
         // near-field cells of side L / nb >= r_cut (1e-4 margin against
         // binning round-off); fewer than 3 per axis: tree walk only
@@ -619,23 +640,25 @@ int force_pass(jt_batch* B, Plan& P, int parts, float kick_frac)
     // particles it flagged (none for uniform data)
     if (!P.cells) jt_b_build_trees(P.d_post, P.d_bx, nseg, P.d_ip, P.ninternal, P.d_pp, P.npart, st);
     cudaEventRecord(B->ev[2], st);
-    for (auto& kv : P.by_M) {
+    for (auto& kv : P.nslots) {
         const int64_t M = kv.first, G = M * M * M;
-        JT_CU(cudaMemsetAsync(B->buckets[kv.first].rho, 0, sizeof(float) * kv.second.size() * B->ngrid * G, st));
+        JT_CU(cudaMemsetAsync(B->buckets[kv.first].rho, 0, sizeof(float) * kv.second * B->ngrid * G, st));
     }
     jt_b_tile_ranges(P.d_post, P.d_bx, P.d_ptp, nbox, P.npmtiles, st);
     JT_TRY(jt_b_deposit(P.d_post, P.d_bx, P.d_ptp, nbox, P.npmtiles, B->order, B->ngrid, P.maxT, st));
+    if (P.screened)
+        JT_TRY(jt_b_deposit(P.d_post, P.d_bx, P.d_ptp, nbox, P.npmtiles, B->order, B->ngrid, P.maxT, st, 1));
     cudaEventRecord(B->ev[3], st);
-    for (auto& kv : P.by_M) {
+    for (auto& kv : P.nslots) {
         Bucket& K = B->buckets[kv.first];
-        JT_TRY(exec_r2c(K, B->ngrid * (int)kv.second.size()));
+        JT_TRY(exec_r2c(K, B->ngrid * kv.second));
     }
     cudaEventRecord(B->ev[4], st);
     jt_b_kspace(P.d_bx, P.d_kp, nbox, P.nmodes, B->ngrid == 2, B->k_min, st);
     cudaEventRecord(B->ev[5], st);
-    for (auto& kv : P.by_M) {
+    for (auto& kv : P.nslots) {
         Bucket& K = B->buckets[kv.first];
-        JT_TRY(exec_c2r(K, 3 * B->ngrid * (int)kv.second.size()));
+        JT_TRY(exec_c2r(K, 3 * B->ngrid * kv.second));
     }
     cudaEventRecord(B->ev[6], st);
     jt_tree_dev pool = {};
@@ -657,17 +680,19 @@ int force_pass(jt_batch* B, Plan& P, int parts, float kick_frac)
         jt_cell_bufs cb = {B->ccount.p, B->cstart.p, B->cbsum.p, B->ccell.p, B->cslot.p,
                            B->cpos.p, B->cid.p, B->tflag.p, B->csegflag.p};
         JT_TRY(jt_b_cells(P.d_post, P.d_bx, P.d_pp, nseg, P.npart, P.d_cp, nbox, P.ncells, cb, B->order,
-                          B->ngrid, parts, kick_frac, B->d_stats, B->d_err, st, B->ev[8], B->ev[9]));
+                          B->ngrid, parts, kick_frac, B->d_stats, B->d_err, st, B->ev[8], B->ev[9],
+                          P.screened));
         tflag = B->tflag.p;
         jt_b_build_trees(P.d_post, P.d_bx, nseg, P.d_ip, P.ninternal, P.d_pp, P.npart, st, B->csegflag.p);
         B->tm.launches += P.npart > 0 ? (P.ncells > 0 ? 6 : 1) : 0;
     }
     JT_TRY(jt_b_walk(P.d_post, P.d_bx, P.d_gp, nseg, P.ngroups, pool, B->order, B->ngrid, parts,
-                     kick_frac, B->d_stats, B->d_err, st, P.d_pp, tflag));
+                     kick_frac, B->d_stats, B->d_err, st, P.d_pp, tflag, P.screened));
     cudaEventRecord(B->ev[7], st);
     B->pending = true;
     B->tm.launches += (P.npart > 0 ? 8 : 0) + (P.ninternal > 0 ? 1 : 0) + (P.npart > 0 ? 1 : 0) +
-                      (P.npmtiles > 0 ? 2 : 0) + (P.nmodes > 0 ? 1 : 0) + (P.ngroups > 0 ? 1 : 0);
+                      (P.npmtiles > 0 ? (P.screened ? 3 : 2) : 0) + (P.nmodes > 0 ? 1 : 0) +
+                      (P.ngroups > 0 ? 1 : 0);
     for (int id : P.ids) {
         jt_box_state* b = B->boxes[id];
         for (int s = 0; s < 2; s++) {
@@ -1082,6 +1107,34 @@ int jt_batch_add(jt_batch* B, const jt_config* cfg, const float* pos_p, const fl
         return r;
     }
     *box_id = id;
+    return JT_OK;
+}
+
+int jt_batch_set_screening(jt_batch* B, int box_id, double lambda_0, double z)
+{
+    if (!box_id_ok(B, box_id) || !(lambda_0 >= 0.0) || !(z > -1.0) || !std::isfinite(lambda_0) ||
+        !std::isfinite(z))
+        return JT_EINVAL;
+    AllocScope scope(&B->actx);
+    jt_box_state* b = B->boxes[box_id];
+    const double kappa = lambda_0 > 0.01 ? 1.0 / (lambda_0 * std::sqrt(1.0 + z)) : 0.0;
+    if (kappa == b->kappa && (kappa == 0.0) == (b->ytab == nullptr)) return JT_OK;
+    if (kappa == 0.0) {
+        dfree(b->ytab);
+        b->bytes -= sizeof(float2) * JT_STAB_N;
+    } else {
+        std::vector<float2> tab(JT_STAB_N);
+        jt_yukawa_table(kappa * b->cfg.r_s, tab.data());
+        if (!b->ytab) {
+            JT_TRY(dalloc(&b->ytab, (size_t)JT_STAB_N));
+            b->bytes += sizeof(float2) * JT_STAB_N;
+        }
+        JT_CU(cudaMemcpyAsync(b->ytab, tab.data(), sizeof(float2) * JT_STAB_N, cudaMemcpyHostToDevice, B->st));
+        JT_CU(cudaStreamSynchronize(B->st));
+    }
+    b->kappa = kappa;
+    b->acc_valid = false;
+    B->gen++;   // the pass's kernels and grid layout change
     return JT_OK;
 }
 

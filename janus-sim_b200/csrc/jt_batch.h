@@ -15,6 +15,11 @@ struct jt_box_state {
     int *id[2] = {}, *id_b[2] = {};
     float4* tabs = nullptr;      // per-axis k tables (2M float4)
     bool acc_valid = false;      // acc belongs to the current positions
+    // Yukawa screening of opposite-species pairs (jt_batch_set_screening):
+    // kappa = 1 / lambda (0: none) and the short-range split-factor table
+    // of b = kappa r_s (JT_STAB_N float2)
+    double kappa = 0.0;
+    float2* ytab = nullptr;
     int M = 0, order = 3, ngrid = 2;
     size_t bytes = 0;            // device bytes held by this box
 };

@@ -100,6 +100,18 @@ struct jt_box_dev {
     float* force;         // 3*ngrid force grids
     int4* ranges;         // per-tile particle ranges of both species
     int seg[2];           // segment index of each species (-1: none)
+    // Yukawa screening of opposite-species pairs (kappa > 0): the unsigned
+    // source S = rho+ + rho- on its own grids (rho_s ...), the signed source D
+    // takes the Green's function (G_N + G_Y) / 2 and S (G_N - G_Y) / 2, and
+    // an m+/m- particle takes s A_D + A_S; cross pairs of the short range
+    // read ytab (the Yukawa split factor) instead of the Newtonian table
+    float ky2;            // kappa^2 (0: no screening)
+    float yfac;           // exp(-kappa^2 r_s^2)
+    float* rho_s;
+    float2* rho_s_k;
+    float2* force_s_k;
+    float* force_s;
+    const float2* ytab;
     int nb;               // cells per axis of the near-field cell list (0: tree walk only)
     float cell_inv;       // nb / L
     int64_t cbase;        // this box's first cell in the pass's cell tables
@@ -240,8 +252,10 @@ int jt_pm_tile_edge(int M);
 // batched PM stages (jt_pm.cu)
 void jt_b_tile_ranges(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_tprefix,
                       int nbox, int64_t ntiles, cudaStream_t st);
+// src 0: the signed source D = sum s m W into B.rho; src 1: the unsigned
+// source S = sum m W into B.rho_s (boxes without rho_s skip the pass)
 int jt_b_deposit(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_tprefix,
-                 int nbox, int64_t ntiles, int order, int ngrid, int T, cudaStream_t st);
+                 int nbox, int64_t ntiles, int order, int ngrid, int T, cudaStream_t st, int src = 0);
 void jt_b_kspace(const jt_box_dev* d_boxes, const int64_t* d_kprefix, int nbox, int64_t nmodes,
                  int interlace, int k_min, cudaStream_t st);
 
@@ -270,7 +284,8 @@ struct jt_walk_params {
 int jt_b_walk(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_gprefix, int nseg,
               int64_t ngroups, const jt_tree_dev& pool, int order, int ngrid, int parts,
               float kick_frac, unsigned long long* stats, unsigned* d_err, cudaStream_t st,
-              const int64_t* d_pprefix = nullptr, const unsigned char* tflag = nullptr);
+              const int64_t* d_pprefix = nullptr, const unsigned char* tflag = nullptr,
+              bool screened = false);
 // Near-field cell list of a pass (cells of side >= r_cut, both species) and
 // the cell walk over it: particles of cells whose 27-cell neighbourhood holds
 // more than JT_CELL_KMAX candidates, and of boxes without a cell grid, are
@@ -285,8 +300,15 @@ struct jt_cell_bufs {
 int jt_b_cells(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_pprefix, int nseg,
                int64_t npart, const int64_t* d_cprefix, int nbox, int64_t ncells, const jt_cell_bufs& cb,
                int order, int ngrid, int parts, float kick_frac, unsigned long long* stats,
-               unsigned* d_err, cudaStream_t st, cudaEvent_t ev_walk0, cudaEvent_t ev_walk1);
+               unsigned* d_err, cudaStream_t st, cudaEvent_t ev_walk0, cudaEvent_t ev_walk1,
+               bool screened = false);
 int jt_cell_scan_blocks(int64_t ncells);
+// Yukawa split factor S_Y(y) on the walk's table grid (y = (r_p / 2 r_s)^2
+// over [0, 16], JT_STAB_N (value, next - value) entries) for b = kappa r_s.
+// A pass with a screened box (jt_box_dev.ytab) runs the walks' screened
+// instantiations (screened = true).
+void jt_yukawa_table(double b, float2* tab);
+constexpr int JT_STAB_N = 4096;
 
 // kick v += (a - drag v) frac*dt and drift x += v frac*dt with each box's own
 // dt and drag (jt_box_dev)

@@ -173,12 +173,13 @@ __global__ void k_b_tile_ranges(const jt_seg_dev* __restrict__ segs, const jt_bo
 template <int ORDER, int NG>
 __global__ void __launch_bounds__(256)
 k_b_deposit(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ boxes,
-            const int64_t* __restrict__ tprefix, int nbox)
+            const int64_t* __restrict__ tprefix, int nbox, int src)
 {
     extern __shared__ float tile[];
     const int64_t q = blockIdx.x;
     const int b = jt_find(tprefix, nbox, q);
     const jt_box_dev& B = boxes[b];
+    if (src && !B.rho_s) return;   // the unsigned source of an unscreened box: not used
     const uint32_t t = (uint32_t)(q - tprefix[b]);
     const int T = B.T, M = B.M;
     const int S = T + 3;
@@ -194,10 +195,10 @@ k_b_deposit(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ 
     const int n0 = r.y - r.x, n1 = r.w - r.z;
     const float halfL = B.halfL, hinv = B.h_inv;
     const float inv_vol = hinv * hinv * hinv;
-    const float q0 = B.mass[0] * inv_vol, q1 = -B.mass[1] * inv_vol;
+    const float q0 = B.mass[0] * inv_vol, q1 = (src ? B.mass[1] : -B.mass[1]) * inv_vol;
     const float4* pos0 = B.seg[0] >= 0 ? segs[B.seg[0]].pos : nullptr;
     const float4* pos1 = B.seg[1] >= 0 ? segs[B.seg[1]].pos : nullptr;
-    float* rho = B.rho;
+    float* rho = src ? B.rho_s : B.rho;
     for (int k = threadIdx.x; k < n0 + n1; k += blockDim.x) {
         float4 p;
         float qq;
@@ -257,6 +258,14 @@ k_b_deposit(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ 
 // With interlacing rho = (rhoA + rhoB exp(-i theta)) / 2, theta = (kx+ky+kz) h/2,
 // and the second set of force spectra is multiplied by exp(+i theta) so that
 // its C2R gives the forces at the shifted nodes.  a_d(k) = -i k_d phi(k).
+//
+// A screened box (B.ky2 = kappa^2 > 0) also has the unsigned source S on
+// rho_s_k.  With G_N the Green's function above and the Yukawa one
+// G_Y = G_N k^2 / (k^2 + kappa^2) exp(-kappa^2 r_s^2) (the long part
+// 4 pi exp(-(k^2 + kappa^2) r_s^2) / (k^2 + kappa^2) of e^{-kappa r} / r),
+// D takes (G_N + G_Y) / 2 into force_k and S takes (G_N - G_Y) / 2 into
+// force_s_k: a particle of sign s then feels s A_D + A_S, i.e. G_N from
+// its own species and -G_Y from the other.
 template <bool IL>
 __global__ void k_b_kspace(const jt_box_dev* __restrict__ boxes, const int64_t* __restrict__ kprefix,
                            int nbox, int k_min)
@@ -284,10 +293,12 @@ __global__ void k_b_kspace(const jt_box_dev* __restrict__ boxes, const int64_t* 
     const int nx = (int)ax.w, ny = (int)ay.w, nz = (int)az.w;
     const int kmax = max(max(nx, ny), nz);
     const bool keep = k2 > 0.0f && kmax >= k_min && nx != half && ny != half && nz != half;
-    float2 F0 = make_float2(0.f, 0.f), F1 = F0, F2 = F0;
+    const bool scr = B.ky2 > 0.0f;
+    float2 F0 = make_float2(0.f, 0.f), F1 = F0, F2 = F0, H0 = F0, H1 = F0, H2 = F0;
     float er = 1.0f, ei = 0.0f;
     if (keep) {
         float2 z = rho_k[idx];
+        float2 zs = scr ? B.rho_s_k[idx] : make_float2(0.f, 0.f);
         if (IL) {
             float4 bx = __ldg(&tb[kx]), by = __ldg(&tb[ky]), bz = __ldg(&tb[kz]);
             float pr = bx.x * by.x - bx.y * by.y, pi = bx.x * by.y + bx.y * by.x;
@@ -296,12 +307,30 @@ __global__ void k_b_kspace(const jt_box_dev* __restrict__ boxes, const int64_t* 
             float2 w = rho_k[Gc + idx];
             z.x = 0.5f * (z.x + (w.x * er + w.y * ei));
             z.y = 0.5f * (z.y + (w.y * er - w.x * ei));
+            if (scr) {
+                const float2 ws = B.rho_s_k[Gc + idx];
+                zs.x = 0.5f * (zs.x + (ws.x * er + ws.y * ei));
+                zs.y = 0.5f * (zs.y + (ws.y * er - ws.x * ei));
+            }
         }
         float green = -12.566370614f * norm * (ax.z * ay.z * az.z) / k2;
+        float gs = 0.0f;
+        if (scr) {
+            const float gy = green * (k2 / (k2 + B.ky2)) * B.yfac;
+            gs = 0.5f * (green - gy);
+            green = 0.5f * (green + gy);
+        }
         float pr = z.x * green, pi = z.y * green;
         F0 = make_float2(ax.y * pi, -ax.y * pr);
         F1 = make_float2(ay.y * pi, -ay.y * pr);
         F2 = make_float2(az.y * pi, -az.y * pr);
+        if (scr) {
+            pr = zs.x * gs;
+            pi = zs.y * gs;
+            H0 = make_float2(ax.y * pi, -ax.y * pr);
+            H1 = make_float2(ay.y * pi, -ay.y * pr);
+            H2 = make_float2(az.y * pi, -az.y * pr);
+        }
     }
     out[idx] = F0;
     out[Gc + idx] = F1;
@@ -310,6 +339,17 @@ __global__ void k_b_kspace(const jt_box_dev* __restrict__ boxes, const int64_t* 
         out[3 * Gc + idx] = make_float2(F0.x * er - F0.y * ei, F0.x * ei + F0.y * er);
         out[4 * Gc + idx] = make_float2(F1.x * er - F1.y * ei, F1.x * ei + F1.y * er);
         out[5 * Gc + idx] = make_float2(F2.x * er - F2.y * ei, F2.x * ei + F2.y * er);
+    }
+    if (scr) {
+        float2* os = B.force_s_k;
+        os[idx] = H0;
+        os[Gc + idx] = H1;
+        os[2 * Gc + idx] = H2;
+        if (IL) {
+            os[3 * Gc + idx] = make_float2(H0.x * er - H0.y * ei, H0.x * ei + H0.y * er);
+            os[4 * Gc + idx] = make_float2(H1.x * er - H1.y * ei, H1.x * ei + H1.y * er);
+            os[5 * Gc + idx] = make_float2(H2.x * er - H2.y * ei, H2.x * ei + H2.y * er);
+        }
     }
 }
 
@@ -324,7 +364,7 @@ void jt_b_tile_ranges(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const
 
 // all boxes of a batch share order, ngrid and the tile edge T
 int jt_b_deposit(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_tprefix,
-                 int nbox, int64_t ntiles, int order, int ngrid, int T, cudaStream_t st)
+                 int nbox, int64_t ntiles, int order, int ngrid, int T, cudaStream_t st, int src)
 {
     if (ntiles <= 0) return JT_OK;
     int S = T + 3;
@@ -337,7 +377,7 @@ int jt_b_deposit(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int6
                                  96 * 1024);                                                  \
             attr = true;                                                                      \
         }                                                                                     \
-        k_b_deposit<O, NG><<<(unsigned)ntiles, 256, smem, st>>>(d_segs, d_boxes, d_tprefix, nbox); \
+        k_b_deposit<O, NG><<<(unsigned)ntiles, 256, smem, st>>>(d_segs, d_boxes, d_tprefix, nbox, src); \
     } while (0)
     if (order == 2 && ngrid == 1) JT_BDEP(2, 1);
     else if (order == 2 && ngrid == 2) JT_BDEP(2, 2);

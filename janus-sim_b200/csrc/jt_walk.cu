@@ -111,7 +111,7 @@ __device__ __forceinline__ float gap1(float d, float ext)
 #ifndef JT_WALK_STAB
 #define JT_WALK_STAB 1
 #endif
-constexpr int kStab = 4096;
+constexpr int kStab = JT_STAB_N;
 constexpr float kStabYMax = 16.0f;
 __device__ float2 g_stab[kStab];
 
@@ -189,7 +189,8 @@ struct HalfTarget {
 template <bool WRAP>
 __device__ __forceinline__ int eval_chunk(WalkWarpSmem& S, int cnt, int lane, float px, float py,
                                           float pz, bool valid, const jt_walk_params& P, float fac,
-                                          WalkCount& wc, Acc3& a, const HalfTarget& H)
+                                          WalkCount& wc, Acc3& a, const HalfTarget& H,
+                                          const float2* __restrict__ tab)
 {
     wc.chunks++;
     (void)lane;
@@ -227,7 +228,7 @@ __device__ __forceinline__ int eval_chunk(WalkWarpSmem& S, int cnt, int lane, fl
 #if JT_WALK_STAB
             const float t = fminf(rp2 * P.c2s, (float)kStab - 1.5f);   // y / dy
             const int k = (int)t;
-            const float2 ab = __ldg(&g_stab[k]);
+            const float2 ab = __ldg(&tab[k]);
             const float S = fmaf(ab.y, t - (float)k, ab.x);
 #else
             const float S = jt_split_S(rp2 * ri * P.c);
@@ -295,7 +296,7 @@ __device__ __forceinline__ void drain_ranges(WalkWarpSmem& S, int nr, int& nc,
                                              float fac, Acc3& near, unsigned& pairs,
                                              unsigned& cands, WalkCount& wc, float gcx, float gcy,
                                              float gcz, float ghx, float ghy, float ghz,
-                                             const HalfTarget& H)
+                                             const HalfTarget& H, const float2* __restrict__ tab)
 {
     if (nr <= 0) return;
     wc.ranges += nr;
@@ -341,7 +342,7 @@ __device__ __forceinline__ void drain_ranges(WalkWarpSmem& S, int nr, int& nc,
         nc += __popc(km);
         __syncwarp();
         if (nc >= 32) {
-            pairs += eval_chunk<WRAP>(S, 32, lane, px, py, pz, valid, P, fac, wc, near, H);
+            pairs += eval_chunk<WRAP>(S, 32, lane, px, py, pz, valid, P, fac, wc, near, H, tab);
             cands += 32;
             __syncwarp();
             float4 t = S.cand[32 + lane];
@@ -359,7 +360,10 @@ __device__ __forceinline__ void drain_ranges(WalkWarpSmem& S, int nr, int& nc,
     }
 }
 
-template <int ORDER, int NG, bool WRAP, int BKT>
+// SCR: the pass holds a screened box; the other species' tree of a screened
+// box is walked with the Yukawa table and without multipoles (their
+// expansion is of the Newtonian kernel), i.e. every pair inside r_cut
+template <int ORDER, int NG, bool WRAP, int BKT, bool SCR>
 __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& B,
                                            const jt_walk_params& P, WalkWarpSmem& S, int s, int lane,
                                            const float4& p, bool valid, float gcx, float gcy,
@@ -395,6 +399,9 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& 
         const float4* __restrict__ tpos = TS.pos;
         const float sgn = (s == t) ? 1.0f : -1.0f;
         const float fac_direct = sgn * (t == 0 ? P.mass[0] : P.mass[1]);   // no dynamic index into a local array
+        const bool yuk = SCR && s != t && B.ytab != nullptr;
+        const float2* __restrict__ tab = yuk ? B.ytab : g_stab;
+        const float theta2 = yuk ? 0.0f : P.theta2;
         const int leaf0 = nt - 1;
         int sp = 1, nR = 0, nA = 0, nc = 0;
         if (lane == 0) S.stack[0] = 0;
@@ -450,7 +457,7 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& 
                         float ax = gap1(mx, ghx), ay = gap1(my, ghy), az = gap1(mz, ghz);
                         float dm2 = ax * ax + ay * ay + az * az;
                         float size = 2.0f * fmaxf(fmaxf(nhx, nhy), nhz);
-                        if (size * size < P.theta2 * dm2) {
+                        if (size * size < theta2 * dm2) {
                             accepted = true;
                             act = 3;
                             pay = make_float4(gcx + mx, gcy + my, gcz + mz, cm.w);
@@ -503,7 +510,7 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& 
             __syncwarp();
             if (nR >= 32) {
                 drain_ranges<WRAP>(S, 32, nc, tpos, lane, p.x, p.y, p.z, valid, P, fac_direct, near,
-                                   pairs, cands, wc, gcx, gcy, gcz, ghx, ghy, ghz, H);
+                                   pairs, cands, wc, gcx, gcy, gcz, ghx, ghy, ghz, H, tab);
                 __syncwarp();
                 int2 r2 = S.rng[32 + lane];
                 char4 s2 = S.rsh[32 + lane];
@@ -528,10 +535,10 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& 
             }
         }
         drain_ranges<WRAP>(S, nR, nc, tpos, lane, p.x, p.y, p.z, valid, P, fac_direct, near, pairs,
-                           cands, wc, gcx, gcy, gcz, ghx, ghy, ghz, H);
+                           cands, wc, gcx, gcy, gcz, ghx, ghy, ghz, H, tab);
         __syncwarp();
         if (nc > 0) {
-            pairs += eval_chunk<WRAP>(S, nc, lane, p.x, p.y, p.z, valid, P, fac_direct, wc, near, H);
+            pairs += eval_chunk<WRAP>(S, nc, lane, p.x, p.y, p.z, valid, P, fac_direct, wc, near, H, tab);
             cands += nc;
         }
         if (nA > 0)
@@ -540,11 +547,13 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& 
     }
 }
 
-// PM acceleration of a unit m+ particle at p: the deposit's stencil on every
-// grid (the interlaced grid's nodes sit half a cell higher), averaged over the
-// grids (an m- particle takes minus this)
+// PM acceleration of a unit m+ particle at p from one set of force grids
+// (B.force: the signed source's, which an m- particle takes with minus sign;
+// B.force_s: the unsigned source's of a screened box, taken by both): the
+// deposit's stencil on every grid (the interlaced grid's nodes sit half a
+// cell higher), averaged over the grids
 template <int ORDER, int NG>
-__device__ __forceinline__ Acc3 pm_interp(const jt_box_dev& B, const float4& p)
+__device__ __forceinline__ Acc3 pm_interp(const jt_box_dev& B, const float* __restrict__ grids, const float4& p)
 {
     Acc3 pm = {0.f, 0.f, 0.f};
     {
@@ -559,7 +568,7 @@ __device__ __forceinline__ Acc3 pm_interp(const jt_box_dev& B, const float4& p)
             const int ix = jt_stencil<ORDER>(gx - sh, wx);
             const int iy = jt_stencil<ORDER>(gy - sh, wy);
             const int iz = jt_stencil<ORDER>(gz - sh, wz);
-            const float* __restrict__ F = B.force + (int64_t)b * 3 * G;
+            const float* __restrict__ F = grids + (int64_t)b * 3 * G;
 #pragma unroll
             for (int c = 0; c < ORDER; c++)
 #pragma unroll
@@ -585,7 +594,7 @@ __device__ __forceinline__ Acc3 pm_interp(const jt_box_dev& B, const float4& p)
 // MINB: resident blocks per SM the register budget is sized for (6 -> 80
 // registers); BKT: nodes with <= BKT particles are streamed as ranges
 // (<= 32: one lane per particle when a range is loaded)
-template <int ORDER, int NG, int MINB, int BKT>
+template <int ORDER, int NG, int MINB, int BKT, bool SCR>
 __global__ void __launch_bounds__(kWarps * 32, MINB) k_walk_acc(WalkArgs A)
 {
     static_assert(BKT <= 32, "a range is loaded one particle per lane");
@@ -623,7 +632,7 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_walk_acc(WalkArgs A)
     float gcx = 0.5f * (lox + hix), gcy = 0.5f * (loy + hiy), gcz = 0.5f * (loz + hiz);
     float ghx = 0.5f * (hix - lox), ghy = 0.5f * (hiy - loy), ghz = 0.5f * (hiz - loz);
 
-    const Acc3 pm = (P.parts & 1) ? pm_interp<ORDER, NG>(B, p) : Acc3{0.f, 0.f, 0.f};
+    const Acc3 pm = (P.parts & 1) ? pm_interp<ORDER, NG>(B, B.force, p) : Acc3{0.f, 0.f, 0.f};
 
     Acc3 near = {0.f, 0.f, 0.f}, far = {0.f, 0.f, 0.f}, comp = {0.f, 0.f, 0.f};
     unsigned pairs = 0, nodes = 0, cands = 0;   // per lane (warp totals < 2^32)
@@ -631,16 +640,22 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_walk_acc(WalkArgs A)
     // groups wider than L/8 take the minimum image per pair
     const bool wide = fmaxf(fmaxf(ghx, ghy), ghz) > 0.125f * P.L;
     if (wide)
-        walk_trees<ORDER, NG, true, BKT>(A, B, P, S, s, lane, p, valid, gcx, gcy, gcz, ghx, ghy, ghz, near,
+        walk_trees<ORDER, NG, true, BKT, SCR>(A, B, P, S, s, lane, p, valid, gcx, gcy, gcz, ghx, ghy, ghz, near,
                                     far, comp, pairs, nodes, cands, wc);
     else
-        walk_trees<ORDER, NG, false, BKT>(A, B, P, S, s, lane, p, valid, gcx, gcy, gcz, ghx, ghy, ghz, near,
+        walk_trees<ORDER, NG, false, BKT, SCR>(A, B, P, S, s, lane, p, valid, gcx, gcy, gcz, ghx, ghy, ghz, near,
                                      far, comp, pairs, nodes, cands, wc);
 
     if (valid && mine) {
         float ax = sgn_s * pm.x + near.x + (far.x - comp.x);
         float ay = sgn_s * pm.y + near.y + (far.y - comp.y);
         float az = sgn_s * pm.z + near.z + (far.z - comp.z);
+        if (SCR && B.force_s && (P.parts & 1)) {
+            const Acc3 ps = pm_interp<ORDER, NG>(B, B.force_s, p);
+            ax += ps.x;
+            ay += ps.y;
+            az += ps.z;
+        }
         SG.acc[i] = make_float4(ax, ay, az, 0.f);
         if (A.kick_frac != 0.0f) {
             // kick_frac 0.5: the closing half kick; 1.0: the closing half
@@ -980,9 +995,9 @@ std::map<std::pair<int, int>, int> g_tuned;   // (device, log2 groups) -> varian
 void launch_variant(int v, unsigned g, const WalkArgs& A, cudaStream_t st)
 {
     switch (v) {
-    case 1: k_walk_acc<3, 2, 5, 32><<<g, kWarps * 32, 0, st>>>(A); break;
-    case 2: k_walk_acc<3, 2, 6, 24><<<g, kWarps * 32, 0, st>>>(A); break;
-    default: k_walk_acc<3, 2, 6, 32><<<g, kWarps * 32, 0, st>>>(A); break;
+    case 1: k_walk_acc<3, 2, 5, 32, false><<<g, kWarps * 32, 0, st>>>(A); break;
+    case 2: k_walk_acc<3, 2, 6, 24, false><<<g, kWarps * 32, 0, st>>>(A); break;
+    default: k_walk_acc<3, 2, 6, 32, false><<<g, kWarps * 32, 0, st>>>(A); break;
     }
 }
 
@@ -1213,10 +1228,12 @@ struct CellWarpSmem {
 // dense evaluation of candidates [0, cnt) for this lane's TPL targets: every
 // pair computed, the force selected by 0 < r^2 < r_cut^2 (an invalid target
 // slot counts no pair; its result is not written)
-template <int TPL>
+// SCR: opposite-species pairs read the box's Yukawa table yt.
+template <int TPL, bool SCR>
 __device__ __forceinline__ unsigned cell_chunk(const float4* __restrict__ cand, int cnt, const float4 (&p)[TPL],
                                                const float (&si)[TPL], const bool (&valid)[TPL], float rc2,
-                                               float eps2, float c2s, Acc3 (&a)[TPL])
+                                               float eps2, float c2s, Acc3 (&a)[TPL],
+                                               const float2* __restrict__ yt)
 {
     unsigned hits = 0;
 #pragma unroll (4 / TPL)
@@ -1231,7 +1248,8 @@ __device__ __forceinline__ unsigned cell_chunk(const float4* __restrict__ cand, 
             const float ri = rsqrtf(rp2);
             const float t = fminf(rp2 * c2s, (float)kStab - 1.5f);   // NaN -> the bound
             const int k = max((int)t, 0);
-            const float2 ab = __ldg(&g_stab[k]);
+            const float2* __restrict__ tb = (SCR && si[u] * q.w < 0.0f) ? yt : g_stab;
+            const float2 ab = __ldg(&tb[k]);
             const float S = fmaf(ab.y, t - (float)k, ab.x);
             const float g = in ? si[u] * q.w * S * ri * ri * ri : 0.0f;
             hits += in ? 1u : 0u;
@@ -1246,13 +1264,14 @@ __device__ __forceinline__ unsigned cell_chunk(const float4* __restrict__ cand, 
 // One batch of a cell's targets: lane l takes targets base + l + 32 u,
 // u < TPL (TPL = 2 for the cells with 33..64 targets left, so that their
 // candidates are streamed and tested once instead of twice).
-template <int ORDER, int NG, int TPL>
+template <int ORDER, int NG, int TPL, bool SCR>
 __device__ __forceinline__ void cell_batch(const CellArgs& A, const jt_box_dev& B, CellWarpSmem& S, int base,
                                            int t1, int lane, unsigned& pairs, unsigned& cands)
 {
     const unsigned lt = (1u << lane) - 1u;
     const float rc2 = B.rc2, eps2 = B.eps2, c2s = B.c * B.c * ((float)kStab / kStabYMax);
     const float slack = B.halfL * 9.5367431640625e-7f, rc2_keep = B.rc2 * 1.00001f;
+    const float2* __restrict__ yt = (SCR && B.ytab) ? B.ytab : g_stab;
     float4 p[TPL];
     int2 id[TPL];
     bool valid[TPL];
@@ -1297,7 +1316,7 @@ __device__ __forceinline__ void cell_batch(const CellArgs& A, const jt_box_dev& 
                 nc += __popc(km);
                 __syncwarp();
                 if (nc >= 32) {
-                    pairs += cell_chunk<TPL>(S.cand, 32, p, si, valid, rc2, eps2, c2s, near);
+                    pairs += cell_chunk<TPL, SCR>(S.cand, 32, p, si, valid, rc2, eps2, c2s, near, yt);
                     cands += 32 * TPL;
                     __syncwarp();
                     const float4 t2 = S.cand[32 + lane];
@@ -1309,7 +1328,7 @@ __device__ __forceinline__ void cell_batch(const CellArgs& A, const jt_box_dev& 
             }
         }
         if (nc > 0) {
-            pairs += cell_chunk<TPL>(S.cand, nc, p, si, valid, rc2, eps2, c2s, near);
+            pairs += cell_chunk<TPL, SCR>(S.cand, nc, p, si, valid, rc2, eps2, c2s, near, yt);
             cands += nc * TPL;
         }
         __syncwarp();
@@ -1318,9 +1337,15 @@ __device__ __forceinline__ void cell_batch(const CellArgs& A, const jt_box_dev& 
     for (int u = 0; u < TPL; u++) {
         if (!valid[u]) continue;
         Acc3 pm = {0.f, 0.f, 0.f};
-        if (A.parts & 1) pm = pm_interp<ORDER, NG>(B, p[u]);
+        if (A.parts & 1) pm = pm_interp<ORDER, NG>(B, B.force, p[u]);
         const jt_seg_dev& SG = A.segs[id[u].x];
-        const float ax = si[u] * pm.x + near[u].x, ay = si[u] * pm.y + near[u].y, az = si[u] * pm.z + near[u].z;
+        float ax = si[u] * pm.x + near[u].x, ay = si[u] * pm.y + near[u].y, az = si[u] * pm.z + near[u].z;
+        if (SCR && B.force_s && (A.parts & 1)) {
+            const Acc3 ps = pm_interp<ORDER, NG>(B, B.force_s, p[u]);
+            ax += ps.x;
+            ay += ps.y;
+            az += ps.z;
+        }
         SG.acc[id[u].y] = make_float4(ax, ay, az, 0.f);
         if (A.kick_frac != 0.0f) {
             // as k_walk_acc: the closing half kick, and with kick_frac 1.0
@@ -1343,7 +1368,7 @@ __device__ __forceinline__ void cell_batch(const CellArgs& A, const jt_box_dev& 
 #ifndef JT_CELL_MINB
 #define JT_CELL_MINB 6
 #endif
-template <int ORDER, int NG>
+template <int ORDER, int NG, bool SCR>
 __global__ void __launch_bounds__(kWarps * 32, JT_CELL_MINB) k_walk_cell(CellArgs A, int64_t ncells)
 {
     __shared__ CellWarpSmem smem_all[kWarps];
@@ -1389,10 +1414,10 @@ __global__ void __launch_bounds__(kWarps * 32, JT_CELL_MINB) k_walk_cell(CellArg
     unsigned pairs = 0, cands = 0;
     for (int base = t0; base < t1;) {
         if (t1 - base > 32) {
-            cell_batch<ORDER, NG, 2>(A, B, S, base, t1, lane, pairs, cands);
+            cell_batch<ORDER, NG, 2, SCR>(A, B, S, base, t1, lane, pairs, cands);
             base += 64;
         } else {
-            cell_batch<ORDER, NG, 1>(A, B, S, base, t1, lane, pairs, cands);
+            cell_batch<ORDER, NG, 1, SCR>(A, B, S, base, t1, lane, pairs, cands);
             base += 32;
         }
     }
@@ -1413,7 +1438,7 @@ int jt_cell_scan_blocks(int64_t ncells) { return (int)((ncells + kScanB - 1) / k
 int jt_b_cells(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_pprefix, int nseg,
                int64_t npart, const int64_t* d_cprefix, int nbox, int64_t ncells, const jt_cell_bufs& cb,
                int order, int ngrid, int parts, float kick_frac, unsigned long long* stats,
-               unsigned* d_err, cudaStream_t st, cudaEvent_t ev_walk0, cudaEvent_t ev_walk1)
+               unsigned* d_err, cudaStream_t st, cudaEvent_t ev_walk0, cudaEvent_t ev_walk1, bool screened)
 {
     cudaEventRecord(ev_walk0, st);   // both recorded on every path (no stale events)
     if (npart <= 0) {
@@ -1447,11 +1472,17 @@ int jt_b_cells(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_
         k_cell_scatter<<<gp, 256, 0, st>>>(A, npart);
         const unsigned gw = (unsigned)((ncells + kWarps - 1) / kWarps);
         cudaEventRecord(ev_walk0, st);
-        if (order == 3 && ngrid == 2) k_walk_cell<3, 2><<<gw, kWarps * 32, 0, st>>>(A, ncells);
-        else if (order == 3 && ngrid == 1) k_walk_cell<3, 1><<<gw, kWarps * 32, 0, st>>>(A, ncells);
-        else if (order == 2 && ngrid == 2) k_walk_cell<2, 2><<<gw, kWarps * 32, 0, st>>>(A, ncells);
-        else if (order == 2 && ngrid == 1) k_walk_cell<2, 1><<<gw, kWarps * 32, 0, st>>>(A, ncells);
+#define JT_CELL_LAUNCH(O, N)                                                         \
+    do {                                                                             \
+        if (screened) k_walk_cell<O, N, true><<<gw, kWarps * 32, 0, st>>>(A, ncells);  \
+        else k_walk_cell<O, N, false><<<gw, kWarps * 32, 0, st>>>(A, ncells);          \
+    } while (0)
+        if (order == 3 && ngrid == 2) JT_CELL_LAUNCH(3, 2);
+        else if (order == 3 && ngrid == 1) JT_CELL_LAUNCH(3, 1);
+        else if (order == 2 && ngrid == 2) JT_CELL_LAUNCH(2, 2);
+        else if (order == 2 && ngrid == 1) JT_CELL_LAUNCH(2, 1);
         else return JT_EINVAL;
+#undef JT_CELL_LAUNCH
         cudaEventRecord(ev_walk1, st);
     }
     return cudaGetLastError() == cudaSuccess ? JT_OK : JT_ECUDA;
@@ -1460,7 +1491,7 @@ int jt_b_cells(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_
 int jt_b_walk(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_gprefix, int nseg,
               int64_t ngroups, const jt_tree_dev& pool, int order, int ngrid, int parts,
               float kick_frac, unsigned long long* stats, unsigned* d_err, cudaStream_t st,
-              const int64_t* d_pprefix, const unsigned char* tflag)
+              const int64_t* d_pprefix, const unsigned char* tflag, bool screened)
 {
     if (ngroups <= 0) return JT_OK;
     if (int r = stab_ready()) return r;
@@ -1477,10 +1508,16 @@ int jt_b_walk(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t
     A.pprefix = d_pprefix;
     A.tflag = tflag;
     unsigned g = (unsigned)((ngroups + kWarps - 1) / kWarps);
-    if (order == 3 && ngrid == 2) launch_variant(pick_variant(g, ngroups, A, st), g, A, st);
-    else if (order == 3 && ngrid == 1) k_walk_acc<3, 1, 6, 32><<<g, kWarps * 32, 0, st>>>(A);
-    else if (order == 2 && ngrid == 2) k_walk_acc<2, 2, 6, 32><<<g, kWarps * 32, 0, st>>>(A);
-    else if (order == 2 && ngrid == 1) k_walk_acc<2, 1, 6, 32><<<g, kWarps * 32, 0, st>>>(A);
+    if (screened) {
+        if (order == 3 && ngrid == 2) k_walk_acc<3, 2, 6, 32, true><<<g, kWarps * 32, 0, st>>>(A);
+        else if (order == 3 && ngrid == 1) k_walk_acc<3, 1, 6, 32, true><<<g, kWarps * 32, 0, st>>>(A);
+        else if (order == 2 && ngrid == 2) k_walk_acc<2, 2, 6, 32, true><<<g, kWarps * 32, 0, st>>>(A);
+        else if (order == 2 && ngrid == 1) k_walk_acc<2, 1, 6, 32, true><<<g, kWarps * 32, 0, st>>>(A);
+        else return JT_EINVAL;
+    } else if (order == 3 && ngrid == 2) launch_variant(pick_variant(g, ngroups, A, st), g, A, st);
+    else if (order == 3 && ngrid == 1) k_walk_acc<3, 1, 6, 32, false><<<g, kWarps * 32, 0, st>>>(A);
+    else if (order == 2 && ngrid == 2) k_walk_acc<2, 2, 6, 32, false><<<g, kWarps * 32, 0, st>>>(A);
+    else if (order == 2 && ngrid == 1) k_walk_acc<2, 1, 6, 32, false><<<g, kWarps * 32, 0, st>>>(A);
     else return JT_EINVAL;
     return cudaGetLastError() == cudaSuccess ? JT_OK : JT_ECUDA;
 }
@@ -1663,4 +1700,33 @@ void jt_b_drift(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64
 {
     if (ntotal <= 0) return;
     k_b_drift<<<(unsigned)((ntotal + 255) / 256), 256, 0, st>>>(d_segs, d_boxes, d_prefix, nseg, frac);
+}
+
+// S_Y(x; b), x = r_p / (2 r_s), b = kappa r_s: r_p^2 times the force of the
+// short part of the Yukawa split, (1 / 2r) [e^{-kr} erfc(x - b) + e^{kr}
+// erfc(x + b)] with kr = 2 b x:
+//   S_Y = (Em Cm + Ep Cp) / 2 + b x (Em Cm - Ep Cp) + (2x / sqrt(pi)) e^{-x^2 - b^2},
+//   Em = e^{-2bx}, Cm = erfc(x - b), Ep = e^{2bx}, Cp = erfc(x + b);
+// b = 0 gives erfc(x) + (2x / sqrt(pi)) e^{-x^2}.  Ep Cp = e^{-x^2 - b^2}
+// erfcx(x + b) is taken from its asymptotic series where erfc underflows.
+void jt_yukawa_table(double b, float2* tab)
+{
+    const double dy = (double)kStabYMax / kStab;
+    auto S = [b](double y) {
+        const double x = std::sqrt(y);
+        const double em = std::exp(-2.0 * b * x), cm = std::erfc(x - b);
+        const double u = x + b;
+        double epcp;
+        if (u < 25.0) {
+            epcp = std::exp(2.0 * b * x) * std::erfc(u);
+        } else {
+            const double iu2 = 1.0 / (u * u);
+            epcp = std::exp(-x * x - b * b) / (u * 1.7724538509055159) * (1.0 - 0.5 * iu2 + 0.75 * iu2 * iu2);
+        }
+        return 0.5 * (em * cm + epcp) + b * x * (em * cm - epcp) + 1.1283791670955126 * x * std::exp(-x * x - b * b);
+    };
+    for (int i = 0; i < kStab; i++) {
+        const double a = S(i * dy), c = S((i + 1) * dy);
+        tab[i] = make_float2((float)a, (float)(c - a));
+    }
 }

@@ -51,6 +51,7 @@ EXPORTED = [
     "jt_energy_sampled", "jt_virialize_sampled", "jt_energy_drift_pct",
     "jt_batch_checkpoint_async", "jt_batch_checkpoint_wait", "jt_snapshot_write_raw",
     "jt_snapshot_read_raw", "jt_set_accel", "jt_get_accel", "jt_server_get_accel",
+    "jt_batch_set_screening",
 ]
 JT_JOB_QUEUED, JT_JOB_RESIDENT, JT_JOB_DONE = 0, 1, 2
 JT_STATIC_SORT_MAX = 262144
@@ -279,6 +280,7 @@ def library():
                                    C.POINTER(C.c_size_t)]
     L.jt_checkpoint.argtypes = [H, C.c_char_p, C.POINTER(jt_snapshot_meta)]
     L.jt_set_screening.argtypes = [H, C.c_double, C.c_double]
+    L.jt_batch_set_screening.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double]
     L.jt_set_accel.argtypes = [H, fp, fp, C.c_int]
     L.jt_server_get_accel.argtypes = [H, C.c_int, fp, fp]
     L.jt_get_accel.argtypes = [H, fp, fp, C.c_int]
@@ -471,7 +473,9 @@ class Solver:
 
     def set_screening(self, lambda_0, z=0.0):
         """Yukawa screening of opposite-sign pairs (set_lambda_0 /
-        set_current_z); compatibility mode, lambda_0 > 0.01 turns it on."""
+        set_current_z), lambda_0 > 0.01 turns it on: the reference's screened
+        walk in compatibility mode, the screened split model in accurate
+        mode (Batch.set_screening)."""
         _check(library().jt_set_screening(self._h, lambda_0, z), "jt_set_screening")
 
     def step(self, dt, hubble=0.0, dtau_per_dt=1.0, nsteps=1):
@@ -650,6 +654,11 @@ class Batch:
                "jt_batch_add_zeldovich")
         self.boxes[bid.value] = (n_side ** 3, n_side ** 3)
         return bid.value
+
+    def set_screening(self, box_id, lambda_0, z=0.0):
+        """Yukawa screening (kappa = 1 / (lambda_0 sqrt(1 + z))) of one box's
+        opposite-species pairs in the split model; lambda_0 <= 0.01: off."""
+        _check(library().jt_batch_set_screening(self._b, box_id, lambda_0, z), "jt_batch_set_screening")
 
     def remove(self, box_id):
         _check(library().jt_batch_remove(self._b, box_id), "jt_batch_remove")

@@ -370,3 +370,106 @@ double orc_split_energy(const double* pos, const double* mass, const int8_t* sig
     }
     return us + ul + uself;
 }
+
+/*
+ * Yukawa-screened cross-species force, FP64 split model.  Same-species pairs
+ * are Newtonian, opposite-species pairs carry the screened potential
+ * e^{-kappa r} / r (force e^{-kappa r}(1 + kappa r) / r^2, the reference's
+ * screening factor, src/nbody_gpu_twopass.rs:1000-1017).  Split with
+ * alpha = 1 / (2 r_s):
+ *   Newton: short erfc(alpha r) / r,  long 4 pi e^{-k^2 r_s^2} / k^2;
+ *   Yukawa: short (1 / 2r) [e^{-kr} erfc(alpha r - beta) + e^{kr} erfc(alpha r + beta)],
+ *           beta = kappa r_s, long 4 pi e^{-(k^2 + kappa^2) r_s^2} / (k^2 + kappa^2)
+ * (Ewald summation of the Yukawa potential).  The short-range force is the
+ * derivative of the short potential at r_p (Plummer softening), cut at
+ * r_trunc; the long part uses per-species structure factors.  kappa = 0 is
+ * orc_ewald_forces.
+ */
+static double yukawa_short_force(double r, double r_s, double kappa)
+{
+    /* -d/dr of the short potential, times r^2 (the factor S of S m / r^2) */
+    const double a = 1.0 / (2.0 * r_s), b = kappa * r_s;
+    const double em = exp(-kappa * r), ep = exp(kappa * r);
+    const double cm = erfc(a * r - b), cp = erfc(a * r + b);
+    const double phi = 0.5 * (em * cm + ep * cp) / r;
+    const double g = exp(-a * a * r * r - b * b);
+    /* d/dr [e^{-kr} erfc(ar - b) + e^{kr} erfc(ar + b)] */
+    const double dsum = -kappa * em * cm + kappa * ep * cp - 2.0 * (2.0 * a / sqrt(M_PI)) * g;
+    const double dphi = -phi / r + 0.5 * dsum / r;
+    return -dphi * r * r;
+}
+
+void orc_ewald_forces_screened(const double* pos, const double* mass, const int8_t* signs, int64_t n,
+                               const int64_t* idx, int64_t nt, double box, double r_s, double eps,
+                               double r_trunc, double kappa, double kcut_tol, double* acc)
+{
+    /* short part: all sources and the images within r_trunc */
+    const int nimg = (int)ceil(r_trunc / box);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t q = 0; q < nt; q++) {
+        const int64_t i = idx[q];
+        double a[3] = {0, 0, 0};
+        for (int64_t j = 0; j < n; j++) {
+            double r0[3];
+            for (int d = 0; d < 3; d++) {
+                double dd = pos[3 * j + d] - pos[3 * i + d];
+                dd -= box * floor(dd / box + 0.5);
+                r0[d] = dd;
+            }
+            const int same = signs[j] == signs[i];
+            for (int iz = -nimg; iz <= nimg; iz++)
+                for (int iy = -nimg; iy <= nimg; iy++)
+                    for (int ix = -nimg; ix <= nimg; ix++) {
+                        if (j == i && ix == 0 && iy == 0 && iz == 0) continue;
+                        const double r[3] = {r0[0] + ix * box, r0[1] + iy * box, r0[2] + iz * box};
+                        const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+                        if (r2 >= r_trunc * r_trunc) continue;
+                        const double rp2 = r2 + eps * eps, rp = sqrt(rp2);
+                        const double S = same || kappa == 0.0 ? short_factor(rp, r_s)
+                                                              : yukawa_short_force(rp, r_s, kappa);
+                        const double f = (same ? 1.0 : -1.0) * mass[j] * S / (rp2 * rp);
+                        a[0] += f * r[0]; a[1] += f * r[1]; a[2] += f * r[2];
+                    }
+        }
+        acc[3 * q] = a[0]; acc[3 * q + 1] = a[1]; acc[3 * q + 2] = a[2];
+    }
+    /* long part: per-species structure factors S+(k), S-(k) (masses) */
+    const double dk = 2.0 * M_PI / box, V = box * box * box;
+    const double kmax = sqrt(-log(kcut_tol)) / r_s;
+    int nmax = (int)floor(kmax / dk);
+    if (nmax < 1) nmax = 1;
+    double* al = (double*)calloc(3 * (size_t)(nt > 0 ? nt : 1), sizeof(double));
+    for (int nx = 0; nx <= nmax; nx++)
+        for (int ny = -nmax; ny <= nmax; ny++)
+            for (int nz = -nmax; nz <= nmax; nz++) {
+                if (nx == 0 && (ny < 0 || (ny == 0 && nz <= 0))) continue;
+                const double k[3] = {dk * nx, dk * ny, dk * nz};
+                const double k2 = k[0] * k[0] + k[1] * k[1] + k[2] * k[2];
+                if (k2 > kmax * kmax) continue;
+                /* half space: each term twice */
+                const double wN = 2.0 * (4.0 * M_PI / V) * exp(-k2 * r_s * r_s) / k2;
+                const double wY = 2.0 * (4.0 * M_PI / V) * exp(-(k2 + kappa * kappa) * r_s * r_s) /
+                                  (k2 + kappa * kappa);
+                double sr[2] = {0, 0}, si[2] = {0, 0};
+                for (int64_t j = 0; j < n; j++) {
+                    const double th = k[0] * pos[3 * j] + k[1] * pos[3 * j + 1] + k[2] * pos[3 * j + 2];
+                    const int s = signs[j] > 0 ? 0 : 1;
+                    sr[s] += mass[j] * cos(th);
+                    si[s] += mass[j] * sin(th);
+                }
+#pragma omp parallel for schedule(static)
+                for (int64_t q = 0; q < nt; q++) {
+                    const int64_t i = idx[q];
+                    const double th = k[0] * pos[3 * i] + k[1] * pos[3 * i + 1] + k[2] * pos[3 * i + 2];
+                    const double c = cos(th), sn = sin(th);
+                    const int me = signs[i] > 0 ? 0 : 1, ot = 1 - me;
+                    /* Im(e^{-ik.x_i} S(k)) for the same and the other species */
+                    const double im_same = c * si[me] - sn * sr[me];
+                    const double im_oth = c * si[ot] - sn * sr[ot];
+                    const double f = wN * im_same - wY * im_oth;
+                    al[3 * q] += f * k[0]; al[3 * q + 1] += f * k[1]; al[3 * q + 2] += f * k[2];
+                }
+            }
+    for (int64_t q = 0; q < 3 * nt; q++) acc[q] += al[q];
+    free(al);
+}

@@ -168,6 +168,11 @@ double orc_split_energy(const double* pos, const double* mass, const int8_t* sig
                         double box, double r_s, double eps, double r_cut, double kcut_tol,
                         double* parts);
 
+/* Yukawa-screened cross-species split model (ewald.c) */
+void orc_ewald_forces_screened(const double* pos, const double* mass, const int8_t* signs, int64_t n,
+                               const int64_t* idx, int64_t nt, double box, double r_s, double eps,
+                               double r_trunc, double kappa, double kcut_tol, double* acc);
+
 #ifdef __cplusplus
 }
 #endif

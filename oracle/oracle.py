@@ -403,3 +403,24 @@ def split_energy(pos, mass, signs, box, r_s, eps, r_cut, kcut_tol=1e-12):
     L.orc_split_energy.restype = F64
     u = L.orc_split_energy(pos.ravel(), mass, signs, len(pos), box, r_s, eps, r_cut, kcut_tol, parts)
     return u, tuple(parts)
+
+
+def ewald_forces_screened(pos, mass, signs, box, r_s, eps, kappa, r_trunc=None, idx=None,
+                          kcut_tol=1e-12):
+    """FP64 split model with Yukawa screening (kappa = 1 / lambda) of
+    opposite-species pairs; kappa = 0 is ewald_forces."""
+    pos = _c(pos, np.float64).reshape(-1, 3)
+    mass = _c(mass, np.float64)
+    signs = _c(signs, np.int8)
+    n = len(pos)
+    idx = np.arange(n, dtype=np.int64) if idx is None else _c(idx, np.int64)
+    if r_trunc is None:
+        r_trunc = 12.0 * r_s
+    acc = np.zeros((len(idx), 3), np.float64)
+    L = lib()
+    L.orc_ewald_forces_screened.argtypes = [f64p, f64p, i8p, I64, i64p, I64, F64, F64, F64, F64, F64,
+                                            F64, f64p]
+    L.orc_ewald_forces_screened.restype = None
+    L.orc_ewald_forces_screened(pos.ravel(), mass, signs, n, idx, len(idx), box, r_s, eps, r_trunc,
+                                kappa, kcut_tol, acc.ravel())
+    return acc

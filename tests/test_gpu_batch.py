@@ -272,3 +272,68 @@ def test_cell_walk_matches_the_tree_walk():
     assert abs(p1 - p0) <= 1e-4 * p0, (p1, p0)
     # with the cells off the cell-walk events are recorded back to back
     assert out["1"][1]["cellwalk_ms"] > 0.0 and out["0"][1]["cellwalk_ms"] < 0.01
+
+
+SCREEN = {0: (5.0, 0.0), 2: (3.0, 1.0), 3: (40.0, 0.5)}   # box index -> (lambda_0, z)
+
+
+def test_screened_boxes_same_alone_and_in_the_mix():
+    """Screened and unscreened boxes in one batch: each box's forces equal
+    its own single-box result, and the pass adds one launch (the unsigned
+    source's deposit).  Graph replay of screened steps matches plain
+    launches; turning screening off restores the unscreened forces."""
+    boxes = BOXES[:5]
+    B = J.Batch()
+    ids = [B.add(*make_box(*box)) for box in boxes]
+    for k, (lam, z) in SCREEN.items():
+        B.set_screening(ids[k], lam, z)
+    B.forces(ids)
+    assert B.timings()["launches"] == 21
+    for k, (bid, box) in enumerate(zip(ids, boxes)):
+        cfg, pp, vp, pm, vm = make_box(*box)
+        s = J.Solver(cfg)
+        if k in SCREEN:
+            s.set_screening(*SCREEN[k])
+        s.set_state(pp, vp, pm, vm)
+        rp, rm = s.accel()
+        s.close()
+        ap, am = B.accel(bid)
+        _cmp(ap, rp, FORCE_TOL)
+        _cmp(am, rm, FORCE_TOL)
+        if k in SCREEN:   # screening is visible at this scale
+            ref = _alone_forces(box)
+            assert np.abs(ap.astype(np.float64) - ref[0]).max() > 100 * FORCE_TOL * np.abs(ref[0]).max()
+    for k in SCREEN:
+        B.set_screening(ids[k], 0.0)
+    B.forces(ids)
+    for k, (bid, box) in enumerate(zip(ids, boxes)):
+        ap, am = B.accel(bid)
+        rp, rm = _alone_forces(box)
+        _cmp(ap, rp, FORCE_TOL)
+        _cmp(am, rm, FORCE_TOL)
+    B.close()
+
+    dts = [0.01, 0.02, 0.005, 0.01, 0.015]
+    hub = [0.0, 0.1, 0.05, 0.2, 0.0]
+    A, G = J.Batch(), J.Batch(graphs=True)
+    ia = [A.add(*make_box(*box)) for box in boxes]
+    ig = [G.add(*make_box(*box)) for box in boxes]
+    for k, (lam, z) in SCREEN.items():
+        A.set_screening(ia[k], lam, z)
+        G.set_screening(ig[k], lam, z)
+    A.step(ia, dts, hub, 1.0, nsteps=3)
+    G.step(ig, dts, hub, 1.0, nsteps=3)
+    for k, box in enumerate(boxes):
+        L = make_box(*box)[0].box_L
+        for q, (g, r) in enumerate(zip(G.get_state(ig[k]), A.get_state(ia[k]))):
+            if len(r) == 0:
+                continue
+            d = np.abs(g.astype(np.float64) - r)
+            if q % 2 == 0:
+                d = np.minimum(d, L - d)
+                assert float(d.max()) <= POS_TOL_L * L, (k, q, float(d.max()))
+            else:
+                rms = float(np.sqrt(np.mean(np.sum(r.astype(np.float64) ** 2, axis=1))))
+                assert float(d.max()) <= VEL_TOL * rms, (k, q, float(d.max()), rms)
+    A.close()
+    G.close()

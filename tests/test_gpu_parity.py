@@ -115,12 +115,76 @@ def test_rcompat_screened_matches_reference_forces(n, lam, z, theta, eps):
     s.close()
 
 
-def test_screening_is_refused_in_accurate_mode():
-    J, _ = _mods()
-    s = J.Solver(J.Config(box_L=32.0, pm_grid=16))
+@pytest.mark.parametrize("lam,z,mu,cells", [(2.0, 0.0, 19.0, "1"), (0.6, 1.5, 1.0, "1"),
+                                            (2.0, 0.0, 19.0, "0")])
+def test_accurate_screened_matches_exact_split_model(lam, z, mu, cells):
+    """Accurate mode with Yukawa screening of opposite-species pairs (kappa =
+    1 / (lambda_0 sqrt(1 + z))) against the FP64 screened split sum (Ewald
+    summation of both kernels) at the same r_cut, on 400 sampled targets;
+    the near field through the cell walk and, with JT_WALK_CELLS=0, through
+    the tree walk (no multipoles across species).  Same bars as the
+    unscreened test."""
+    import os
+    J, O = _mods()
+    n, M, L = 4096, 32, 32.0
+    pp = _uniform(n, L, 11)
+    pm = _uniform(n, L, 12)
+    r_s = 1.25 * L / M
+    r_cut = 4.5 * r_s
+    eps = (L / (2 * n) ** (1 / 3)) / 30
+    os.environ["JT_WALK_CELLS"] = cells
+    try:
+        s = J.Solver(J.Config(box_L=L, pm_grid=M, theta=0.5, softening=eps, r_s=r_s, r_cut=r_cut,
+                              mu=mu, G_mass_plus=1.0, mode=J.JT_ACCURATE))
+        s.set_screening(lam, z)   # before the state: kept when the box is made
+        s.set_state(pp, None, pm, None)
+        ap, am = s.accel()
+        s.set_screening(0.0, 0.0)
+        bp, bm = s.accel()
+        s.close()
+    finally:
+        os.environ.pop("JT_WALK_CELLS", None)
+    pos = np.concatenate([pp, pm]).astype(np.float64)
+    mass = np.concatenate([np.full(n, 1.0), np.full(n, mu)])
+    sg = np.concatenate([np.ones(n, np.int8), -np.ones(n, np.int8)])
+    idx = np.random.default_rng(5).choice(2 * n, 400, replace=False)
+    kappa = 1.0 / (lam * np.sqrt(1.0 + z))
+    ex = O.ewald_forces_screened(pos, mass, sg, L, r_s, eps, kappa, r_trunc=r_cut, idx=idx)
+    got = np.concatenate([ap, am])[idx]
+    rel = _rel(got, ex)
+    p50, p99 = np.percentile(rel, [50, 99])
+    assert p99 <= 3e-3 and p50 <= 2e-4, (p50, p99)
+    # screening changes the forces well beyond that error (the repulsion of
+    # the other species is cut off beyond lambda)
+    ex0 = O.ewald_forces_screened(pos, mass, sg, L, r_s, eps, 0.0, r_trunc=r_cut, idx=idx)
+    assert np.median(_rel(ex0, ex)) > 0.05
+    rel0 = _rel(np.concatenate([bp, bm])[idx], ex0)
+    assert np.percentile(rel0, 99) <= 3e-3
+
+
+def test_accurate_screening_limits():
+    """A screening length far beyond the box is the unscreened model (to
+    FP32 rounding of the extra terms), and lambda_0 <= 0.01 turns it off."""
+    J, O = _mods()
+    n, L = 3000, 40.0
+    pp = _uniform(n, L, 31)
+    pm = _uniform(n, L, 32)
+    s = J.Solver(J.Config(box_L=L, pm_grid=32, mu=2.0, G_mass_plus=1.0, mode=J.JT_ACCURATE))
+    s.set_state(pp, None, pm, None)
+    a0 = np.concatenate(s.accel())
+    s.set_screening(1.0e7, 0.0)
+    a1 = np.concatenate(s.accel())
+    rms = float(np.sqrt(np.mean(np.sum(a0.astype(np.float64) ** 2, axis=1))))
+    d = np.linalg.norm(a1.astype(np.float64) - a0, axis=1) / rms
+    assert np.percentile(d, 99) <= 2e-5 and d.max() <= 2e-4, (np.percentile(d, 99), d.max())
+    s.set_screening(0.005, 0.0)
+    a2 = np.concatenate(s.accel())
+    d2 = np.linalg.norm(a2.astype(np.float64) - a0, axis=1) / rms
+    assert np.percentile(d2, 99) <= 2e-5
     with pytest.raises(J.JanusError):
-        s.set_screening(2.0, 0.0)
-    s.set_screening(0.0, 0.0)
+        s.set_screening(-1.0, 0.0)
+    with pytest.raises(J.JanusError):
+        s.set_screening(2.0, -1.0)
     s.close()
 
 

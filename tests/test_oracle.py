@@ -342,3 +342,24 @@ def test_split_energy_is_the_potential_of_the_oracle_forces():
             pn[i, d] -= h
             g = -(O.split_energy(pp, m, s, L, rs, eps, rc)[0] - O.split_energy(pn, m, s, L, rs, eps, rc)[0]) / (2 * h) / m[i]
             assert abs(g - a[i, d]) <= 1e-6 * max(1.0, abs(a[i, d]))
+
+
+def test_screened_split_oracle():
+    """orc_ewald_forces_screened: kappa = 0 is the unscreened oracle; with
+    screening (eps = 0, no truncation) the split sum is independent of r_s;
+    two opposite-sign particles in a large box feel exactly
+    -m e^{-kappa r}(1 + kappa r) / r^2."""
+    rng = np.random.default_rng(3)
+    n, L = 60, 10.0
+    pos = (rng.random((n, 3)) - 0.5) * L
+    m = rng.uniform(0.5, 2.0, n)
+    s = np.where(rng.random(n) < 0.5, 1, -1).astype(np.int8)
+    a0 = O.ewald_forces(pos, m, s, L, 0.5, 0.1)
+    b0 = O.ewald_forces_screened(pos, m, s, L, 0.5, 0.1, 0.0)
+    assert np.abs(a0 - b0).max() <= 1e-14 * np.abs(a0).max()
+    for kap in (0.3, 1.0, 3.0):
+        x = [O.ewald_forces_screened(pos, m, s, L, rs, 0.0, kap) for rs in (0.4, 0.6)]
+        assert np.abs(x[0] - x[1]).max() <= 1e-12 * np.abs(x[0]).max()
+    pos2 = np.array([[0, 0, 0], [1.3, 0, 0]], float)
+    a = O.ewald_forces_screened(pos2, np.array([1.0, 2.0]), np.array([1, -1], np.int8), 40.0, 0.4, 0.0, 1.0)
+    assert a[0, 0] == pytest.approx(-2.0 * np.exp(-1.3) * 2.3 / 1.3 ** 2, rel=1e-12)
