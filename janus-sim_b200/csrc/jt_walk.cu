@@ -548,12 +548,12 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& 
 }
 
 // PM acceleration of a unit m+ particle at p from one set of force grids
-// (B.force: the signed source's, which an m- particle takes with minus sign;
-// B.force_s: the unsigned source's of a screened box, taken by both): the
-// deposit's stencil on every grid (the interlaced grid's nodes sit half a
-// cell higher), averaged over the grids
-template <int ORDER, int NG>
-__device__ __forceinline__ Acc3 pm_interp(const jt_box_dev& B, const float* __restrict__ grids, const float4& p)
+// (SG false, B.force: the signed source's, which an m- particle takes with
+// minus sign; SG true, B.force_s: the unsigned source's of a screened box,
+// taken by both): the deposit's stencil on every grid (the interlaced grid's
+// nodes sit half a cell higher), averaged over the grids
+template <int ORDER, int NG, bool SG = false>
+__device__ __forceinline__ Acc3 pm_interp(const jt_box_dev& B, const float4& p)
 {
     Acc3 pm = {0.f, 0.f, 0.f};
     {
@@ -568,7 +568,7 @@ __device__ __forceinline__ Acc3 pm_interp(const jt_box_dev& B, const float* __re
             const int ix = jt_stencil<ORDER>(gx - sh, wx);
             const int iy = jt_stencil<ORDER>(gy - sh, wy);
             const int iz = jt_stencil<ORDER>(gz - sh, wz);
-            const float* __restrict__ F = grids + (int64_t)b * 3 * G;
+            const float* __restrict__ F = (SG ? B.force_s : B.force) + (int64_t)b * 3 * G;
 #pragma unroll
             for (int c = 0; c < ORDER; c++)
 #pragma unroll
@@ -632,7 +632,7 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_walk_acc(WalkArgs A)
     float gcx = 0.5f * (lox + hix), gcy = 0.5f * (loy + hiy), gcz = 0.5f * (loz + hiz);
     float ghx = 0.5f * (hix - lox), ghy = 0.5f * (hiy - loy), ghz = 0.5f * (hiz - loz);
 
-    const Acc3 pm = (P.parts & 1) ? pm_interp<ORDER, NG>(B, B.force, p) : Acc3{0.f, 0.f, 0.f};
+    const Acc3 pm = (P.parts & 1) ? pm_interp<ORDER, NG>(B, p) : Acc3{0.f, 0.f, 0.f};
 
     Acc3 near = {0.f, 0.f, 0.f}, far = {0.f, 0.f, 0.f}, comp = {0.f, 0.f, 0.f};
     unsigned pairs = 0, nodes = 0, cands = 0;   // per lane (warp totals < 2^32)
@@ -651,7 +651,7 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_walk_acc(WalkArgs A)
         float ay = sgn_s * pm.y + near.y + (far.y - comp.y);
         float az = sgn_s * pm.z + near.z + (far.z - comp.z);
         if (SCR && B.force_s && (P.parts & 1)) {
-            const Acc3 ps = pm_interp<ORDER, NG>(B, B.force_s, p);
+            const Acc3 ps = pm_interp<ORDER, NG, true>(B, p);
             ax += ps.x;
             ay += ps.y;
             az += ps.z;
@@ -1337,11 +1337,11 @@ __device__ __forceinline__ void cell_batch(const CellArgs& A, const jt_box_dev& 
     for (int u = 0; u < TPL; u++) {
         if (!valid[u]) continue;
         Acc3 pm = {0.f, 0.f, 0.f};
-        if (A.parts & 1) pm = pm_interp<ORDER, NG>(B, B.force, p[u]);
+        if (A.parts & 1) pm = pm_interp<ORDER, NG>(B, p[u]);
         const jt_seg_dev& SG = A.segs[id[u].x];
         float ax = si[u] * pm.x + near[u].x, ay = si[u] * pm.y + near[u].y, az = si[u] * pm.z + near[u].z;
         if (SCR && B.force_s && (A.parts & 1)) {
-            const Acc3 ps = pm_interp<ORDER, NG>(B, B.force_s, p[u]);
+            const Acc3 ps = pm_interp<ORDER, NG, true>(B, p[u]);
             ax += ps.x;
             ay += ps.y;
             az += ps.z;
