@@ -451,7 +451,9 @@ def run_ours(args, ws, rank, local):
     # end to end through the C ABI with pinned host buffers: every step
     # uploads the state a KDK step starts from (positions, velocities and the
     # accelerations at those positions), steps once, and reads the same three
-    # back into pinned buffers, which the next step uploads again
+    # back into the pinned buffers, which the next step uploads again
+    # (jt_step_host: one call per step, the positions coming back during the
+    # force pass)
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
     cur = [pin(a) for a in (pp, vp, pm, vm)]
     acc = [pin(np.zeros_like(pp)), pin(np.zeros_like(pm))]
@@ -459,14 +461,11 @@ def run_ours(args, ws, rank, local):
     s.step(w["dt"], H, 1.0, 1)
     s.get_state(out=cur)
     s.get_accel(out=acc)
+    s.step_host(cur[0], cur[1], acc[0], cur[2], cur[3], acc[1], w["dt"], H, 1.0)
     barrier()
     t0 = time.perf_counter()
     for _ in range(K):
-        s.set_state(*cur)
-        s.set_accel(*acc)
-        s.step(w["dt"], H, 1.0, 1)
-        s.get_state(out=cur)
-        s.get_accel(out=acc)
+        s.step_host(cur[0], cur[1], acc[0], cur[2], cur[3], acc[1], w["dt"], H, 1.0)
     barrier()
     e2e_t = time.perf_counter() - t0
     e2e_t = max_over_ranks(e2e_t, ws, "cuda")

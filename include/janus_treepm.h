@@ -160,6 +160,21 @@ int  jt_step(jt_handle* h, double dt, double hubble, double dtau_per_dt, int nst
 int  jt_set_accel(jt_handle* h, const float* acc_p, const float* acc_m, int mem);
 int  jt_get_accel(jt_handle* h, float* acc_p, float* acc_m, int mem);
 
+/* One step of a state the host holds between steps, in one call: the host
+ * arrays (per species AoS float3, the handle's current counts; pinned for
+ * full PCIe speed) are uploaded, stepped once, and overwritten in place with
+ * the new positions, velocities and (KDK) the accelerations at the new
+ * positions.  It equals jt_set_state + jt_set_accel + jt_step(1) +
+ * jt_get_state + jt_get_accel.  In accurate KDK mode the positions, final
+ * after the drift, are copied back on a side stream while the force pass
+ * runs.  With JT_DKD_REF the acc arrays are not used (may be NULL).  The
+ * reference's drivers upload ICs once and call get_particles() after
+ * step_treepm_gpu (src/nbody_gpu_twopass.rs:4486-4649); this is that round
+ * trip for a host-resident state. */
+int  jt_step_host(jt_handle* h, float* pos_p, float* vel_p, float* acc_p,
+                  float* pos_m, float* vel_m, float* acc_m,
+                  double dt, double hubble, double dtau_per_dt);
+
 /* Yukawa screening of opposite-sign pairs: the reference's set_lambda_0 /
  * set_current_z (src/nbody_gpu_twopass.rs:2305-2312) as its TreePM step uses
  * them (compute_short_range_forces, :3997-4068).  With lambda_0 > 0.01 the

@@ -855,6 +855,37 @@ int jt_step(jt_handle* h, double dt, double hubble, double dtau_per_dt, int nste
     return r;
 }
 
+int jt_step_host(jt_handle* h, float* pos_p, float* vel_p, float* acc_p, float* pos_m, float* vel_m,
+                 float* acc_m, double dt, double hubble, double dtau_per_dt)
+{
+    if (!h || !std::isfinite(dt) || !std::isfinite(hubble) || !std::isfinite(dtau_per_dt)) return JT_EINVAL;
+    if (!h->have_state) return JT_ESTATE;
+    if (h->signed_layout) return JT_EINVAL;
+    const bool kdk = h->cfg.integrator == JT_KDK;
+    float* pos[2] = {pos_p, pos_m};
+    float* vel[2] = {vel_p, vel_m};
+    float* acc[2] = {acc_p, acc_m};
+    for (int s = 0; s < 2; s++)
+        if (h->n[s] > 0 && (!pos[s] || !vel[s] || (kdk && !acc[s]))) return JT_EINVAL;
+    if (h->batch && kdk) {
+        h->tm = jt_timings{};
+        const int r = jtb_step_host(h->batch, h->box_id, pos, vel, acc, (float)dt, (float)(hubble * dtau_per_dt));
+        jt_batch_get_timings(h->batch, &h->tm);
+        for (int i = 0; i < 4; i++) h->phase[i] = jtb_phase(h->batch, i);
+        return r;
+    }
+    // compatibility mode and the reference's DKD: the same round trip
+    // through the separate calls (no overlap)
+    JT_TRY(jt_set_state(h, pos_p, vel_p, (size_t)h->n[0], pos_m, vel_m, (size_t)h->n[1], JT_MEM_HOST));
+    if (kdk) JT_TRY(jt_set_accel(h, acc_p, acc_m, JT_MEM_HOST));
+    JT_TRY(jt_step(h, dt, hubble, dtau_per_dt, 1));
+    const jt_timings tm = h->tm;
+    JT_TRY(jt_get_state(h, pos_p, vel_p, pos_m, vel_m, JT_MEM_HOST));
+    if (kdk) JT_TRY(jt_get_accel(h, acc_p, acc_m, JT_MEM_HOST));
+    h->tm = tm;
+    return JT_OK;
+}
+
 int jt_set_accel(jt_handle* h, const float* acc_p, const float* acc_m, int mem)
 {
     if (!h || (mem != JT_MEM_HOST && mem != JT_MEM_DEVICE)) return JT_EINVAL;

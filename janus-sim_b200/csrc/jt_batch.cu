@@ -184,6 +184,11 @@ struct jt_batch {
     cudaStream_t st = nullptr;
     AllocCtx actx;                      // its memory pool and stream
     Pool<float> stage;                  // host <-> device staging of AoS arrays
+    // jtb_step_host: the uploaded and outgoing state (per species pos | vel |
+    // acc, AoS float3) and the side stream that copies positions back
+    Pool<float> io;
+    cudaStream_t io_side = nullptr;
+    cudaEvent_t io_ev = nullptr;
     std::vector<jt_box_state*> boxes;
     int order = 0, ngrid = 0, k_min = -1;   // shared by every box of the batch
     Pool<int2> child, range;
@@ -986,6 +991,101 @@ int jtb_set_accel(jt_batch* B, int box_id, const float* acc_p, const float* acc_
     return JT_OK;
 }
 
+int jtb_step_host(jt_batch* B, int box_id, float* const pos[2], float* const vel[2], float* const acc[2],
+                  float dt, float drag)
+{
+    if (!box_id_ok(B, box_id) || !std::isfinite(dt) || !std::isfinite(drag)) return JT_EINVAL;
+    AllocScope scope(&B->actx);
+    jt_box_state* b = B->boxes[box_id];
+    for (int s = 0; s < 2; s++)
+        if (b->n[s] > 0 && (!pos[s] || !vel[s] || !acc[s])) return JT_EINVAL;
+    bool grew = false;
+    JT_TRY(B->io.ensure(9 * (size_t)(b->n[0] + b->n[1]), &grew));
+    if (!B->io_side) {
+        JT_CU(cudaStreamCreateWithFlags(&B->io_side, cudaStreamNonBlocking));
+        JT_CU(cudaEventCreateWithFlags(&B->io_ev, cudaEventDisableTiming));
+    }
+    cudaStream_t st = B->st;
+    B->tm = jt_timings{};
+    cudaEvent_t t0, t1, k0, k1;
+    cudaEventCreate(&t0); cudaEventCreate(&t1); cudaEventCreate(&k0); cudaEventCreate(&k1);
+    cudaEventRecord(t0, st);
+    float* io[2] = {B->io.p, B->io.p + 9 * (size_t)b->n[0]};
+    int r = JT_OK;
+    // upload in the order the kick and the drift need the arrays; the box
+    // takes the caller's order (id = identity)
+    for (int s = 0; s < 2 && r == JT_OK; s++) {
+        const int64_t n = b->n[s];
+        if (n == 0) continue;
+        const size_t bytes = sizeof(float) * 3 * (size_t)n;
+        if (cudaMemcpyAsync(io[s] + 6 * n, acc[s], bytes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            cudaMemcpyAsync(io[s] + 3 * n, vel[s], bytes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            cudaMemcpyAsync(io[s], pos[s], bytes, cudaMemcpyHostToDevice, st) != cudaSuccess)
+            r = JT_ECUDA;
+        jt_launch_aos_in(io[s] + 6 * n, n, b->acc[s], nullptr, st);
+        jt_launch_aos_in(io[s] + 3 * n, n, b->vel[s], nullptr, st);
+        jt_launch_aos_in(io[s], n, b->pos[s], b->id[s], st);
+        B->tm.launches += 3;
+    }
+    b->acc_valid = true;
+    const jt_box_step step = {dt, drag};
+    const std::vector<int> v(1, box_id);
+    Plan& P = B->plan;
+    if (r == JT_OK) r = build_plan(B, v, &step, P);
+    double kd = 0.0;
+    if (r == JT_OK) {
+        cudaEventRecord(k0, st);
+        jt_b_kick(P.d_pre, P.d_bx, P.d_pp, (int)P.pre.size(), P.npart, 0.5f, st);
+        jt_b_drift(P.d_pre, P.d_bx, P.d_pp, (int)P.pre.size(), P.npart, 1.0f, st);
+        cudaEventRecord(k1, st);
+        B->tm.launches += 2;
+        // the positions are final: pack them into their upload slots (still
+        // in the caller's order) and copy them back while the forces run
+        for (int s = 0; s < 2; s++)
+            if (b->n[s] > 0) {
+                jt_launch_aos_out(b->pos[s], b->id[s], nullptr, b->n[s], io[s], st);
+                B->tm.launches += 1;
+            }
+        if (cudaEventRecord(B->io_ev, st) != cudaSuccess ||
+            cudaStreamWaitEvent(B->io_side, B->io_ev, 0) != cudaSuccess)
+            r = JT_ECUDA;
+        for (int s = 0; s < 2 && r == JT_OK; s++)
+            if (b->n[s] > 0 &&
+                cudaMemcpyAsync(pos[s], io[s], sizeof(float) * 3 * (size_t)b->n[s], cudaMemcpyDeviceToHost,
+                                B->io_side) != cudaSuccess)
+                r = JT_ECUDA;
+    }
+    if (r == JT_OK) r = force_pass(B, P, JT_PART_ALL, 0.5f);
+    if (r == JT_OK) {
+        // velocities (closing half kick fused into the walk) and
+        // accelerations, back to the caller's order
+        for (int s = 0; s < 2 && r == JT_OK; s++) {
+            const int64_t n = b->n[s];
+            if (n == 0) continue;
+            const size_t bytes = sizeof(float) * 3 * (size_t)n;
+            jt_launch_aos_out(b->vel[s], b->id[s], nullptr, n, io[s] + 3 * n, st);
+            jt_launch_aos_out(b->acc[s], b->id[s], nullptr, n, io[s] + 6 * n, st);
+            B->tm.launches += 2;
+            if (cudaMemcpyAsync(vel[s], io[s] + 3 * n, bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaMemcpyAsync(acc[s], io[s] + 6 * n, bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+                r = JT_ECUDA;
+        }
+        kd = elapsed(k0, k1);
+        if (r == JT_OK) r = finish(B);
+    }
+    cudaEventRecord(t1, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess && r == JT_OK) r = JT_ECUDA;
+    if (cudaStreamSynchronize(B->io_side) != cudaSuccess && r == JT_OK) r = JT_ECUDA;
+    if (r == JT_OK) {
+        B->tm.total_ms = elapsed(t0, t1);
+        B->tm.kick_drift_ms = kd;
+    } else {
+        b->acc_valid = false;
+    }
+    cudaEventDestroy(t0); cudaEventDestroy(t1); cudaEventDestroy(k0); cudaEventDestroy(k1);
+    return r;
+}
+
 // ---------------------------------------------------------------- C ABI
 extern "C" {
 
@@ -1046,6 +1146,12 @@ void jt_batch_destroy(jt_batch* B)
     for (auto& kv : B->buckets) kv.second.release();
     B->fftws.release();
     B->stage.release();
+    B->io.release();
+    if (B->io_side) {
+        cudaStreamSynchronize(B->io_side);
+        cudaStreamDestroy(B->io_side);
+    }
+    if (B->io_ev) cudaEventDestroy(B->io_ev);
     if (B->hdesc) cudaFreeHost(B->hdesc);
     if (B->d_err) cudaFree(B->d_err);
     if (B->d_stats) cudaFree(B->d_stats);

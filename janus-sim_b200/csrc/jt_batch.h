@@ -60,3 +60,11 @@ int jth_info(jt_handle* h, jt_config* cfg, float* m_plus, float* m_minus, int8_t
 int jt_diag_state(const float4* const pos[2], const float4* const vel[2], const int64_t n[2],
                   const float mass[2], double L, int n_cells, cudaStream_t st, jt_diag* out);
 int jtb_set_accel(jt_batch* B, int box_id, const float* acc_p, const float* acc_m, int mem);
+// One KDK step of one box whose state the host holds between steps: the
+// caller-order host arrays (pos, vel, acc per species; pinned for full
+// speed) are uploaded into the box (which takes the caller's order), the box
+// takes one step, and the arrays are overwritten with the new state.  The
+// positions are final after the drift: they are copied back on a side
+// stream while the force pass runs.
+int jtb_step_host(jt_batch* B, int box_id, float* const pos[2], float* const vel[2], float* const acc[2],
+                  float dt, float drag);

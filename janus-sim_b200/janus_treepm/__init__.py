@@ -51,7 +51,7 @@ EXPORTED = [
     "jt_energy_sampled", "jt_virialize_sampled", "jt_energy_drift_pct",
     "jt_batch_checkpoint_async", "jt_batch_checkpoint_wait", "jt_snapshot_write_raw",
     "jt_snapshot_read_raw", "jt_set_accel", "jt_get_accel", "jt_server_get_accel",
-    "jt_batch_set_screening",
+    "jt_batch_set_screening", "jt_step_host",
 ]
 JT_JOB_QUEUED, JT_JOB_RESIDENT, JT_JOB_DONE = 0, 1, 2
 JT_STATIC_SORT_MAX = 262144
@@ -281,6 +281,7 @@ def library():
     L.jt_checkpoint.argtypes = [H, C.c_char_p, C.POINTER(jt_snapshot_meta)]
     L.jt_set_screening.argtypes = [H, C.c_double, C.c_double]
     L.jt_batch_set_screening.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double]
+    L.jt_step_host.argtypes = [H, fp, fp, fp, fp, fp, fp, C.c_double, C.c_double, C.c_double]
     L.jt_set_accel.argtypes = [H, fp, fp, C.c_int]
     L.jt_server_get_accel.argtypes = [H, C.c_int, fp, fp]
     L.jt_get_accel.argtypes = [H, fp, fp, C.c_int]
@@ -486,6 +487,19 @@ class Solver:
         that the next KDK step needs no opening force pass."""
         acc_p, acc_m = _f32(acc_p), _f32(acc_m)
         _check(library().jt_set_accel(self._h, _ptr(acc_p), _ptr(acc_m), JT_MEM_HOST), "jt_set_accel")
+
+    def step_host(self, pos_p, vel_p, acc_p, pos_m, vel_m, acc_m, dt, hubble=0.0, dtau_per_dt=1.0):
+        """One step of a host-held state, in place (jt_step_host): the six
+        float32 (n, 3) C-contiguous arrays (pinned for full speed; acc_* may
+        be None with the DKD integrator) are uploaded, stepped once and
+        overwritten with the new state."""
+        arrs = (pos_p, vel_p, acc_p, pos_m, vel_m, acc_m)
+        for a in arrs:
+            if a is not None and (not isinstance(a, np.ndarray) or a.dtype != np.float32
+                                  or not a.flags["C_CONTIGUOUS"]):
+                raise ValueError("step_host works in place on C-contiguous float32 arrays")
+        _check(library().jt_step_host(self._h, *[_ptr(a) for a in arrs], dt, hubble, dtau_per_dt),
+               "jt_step_host")
 
     def get_accel(self, out=None):
         """The stored accelerations (no force pass); out = [acc_p, acc_m]."""
