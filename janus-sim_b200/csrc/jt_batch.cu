@@ -160,7 +160,7 @@ struct Plan {
     bool screened = false;                // some box is screened (second source, Yukawa tables)
     std::map<int, std::vector<int>> by_M; // M -> boxes (positions in ids)
     std::map<int, int> nslots;            // M -> bucket slots (a screened box takes two: D, then S)
-    int maxT = 1;
+    int maxT = 1, minT = 1 << 30;
     size_t table_bytes = 0;
     const jt_seg_dev* d_pre = nullptr;
     const jt_seg_dev* d_post = nullptr;
@@ -498,6 +498,7 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
         d.tile_shift = tile_shift_of(M);
         d.ntiles = (M / d.T) * (M / d.T) * (M / d.T);
         P.maxT = std::max(P.maxT, d.T);
+        P.minT = std::min(P.minT, d.T);
         Bucket& K = B->buckets[M];
         const int q = slot[k];
         const int64_t G = (int64_t)M * M * M, Gc = (int64_t)M * M * (M / 2 + 1);
@@ -507,6 +508,8 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
         d.force = K.force + (size_t)q * 3 * b->ngrid * G;
         d.tabs = b->tabs;
         d.ranges = K.ranges + (size_t)q * d.ntiles;
+        // the deposit flushes its tiles with 16-byte reductions
+        if (reinterpret_cast<uintptr_t>(d.rho) & 15) return JT_ECUDA;
         if (b->ytab) {
             // the unsigned source's grids sit in the next slot
             d.rho_s = d.rho + (size_t)b->ngrid * G;
@@ -650,9 +653,10 @@ int force_pass(jt_batch* B, Plan& P, int parts, float kick_frac)
         JT_CU(cudaMemsetAsync(B->buckets[kv.first].rho, 0, sizeof(float) * kv.second * B->ngrid * G, st));
     }
     jt_b_tile_ranges(P.d_post, P.d_bx, P.d_ptp, nbox, P.npmtiles, st);
-    JT_TRY(jt_b_deposit(P.d_post, P.d_bx, P.d_ptp, nbox, P.npmtiles, B->order, B->ngrid, P.maxT, st));
+    const bool t16 = P.minT == 16 && P.maxT == 16;
+    JT_TRY(jt_b_deposit(P.d_post, P.d_bx, P.d_ptp, nbox, P.npmtiles, B->order, B->ngrid, P.maxT, st, 0, t16));
     if (P.screened)
-        JT_TRY(jt_b_deposit(P.d_post, P.d_bx, P.d_ptp, nbox, P.npmtiles, B->order, B->ngrid, P.maxT, st, 1));
+        JT_TRY(jt_b_deposit(P.d_post, P.d_bx, P.d_ptp, nbox, P.npmtiles, B->order, B->ngrid, P.maxT, st, 1, t16));
     cudaEventRecord(B->ev[3], st);
     for (auto& kv : P.nslots) {
         Bucket& K = B->buckets[kv.first];

@@ -253,9 +253,11 @@ int jt_pm_tile_edge(int M);
 void jt_b_tile_ranges(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_tprefix,
                       int nbox, int64_t ntiles, cudaStream_t st);
 // src 0: the signed source D = sum s m W into B.rho; src 1: the unsigned
-// source S = sum m W into B.rho_s (boxes without rho_s skip the pass)
+// source S = sum m W into B.rho_s (boxes without rho_s skip the pass).
+// T: the largest tile edge of the pass; T16: every box's tile edge is 16.
 int jt_b_deposit(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_tprefix,
-                 int nbox, int64_t ntiles, int order, int ngrid, int T, cudaStream_t st, int src = 0);
+                 int nbox, int64_t ntiles, int order, int ngrid, int T, cudaStream_t st, int src = 0,
+                 bool T16 = false);
 void jt_b_kspace(const jt_box_dev* d_boxes, const int64_t* d_kprefix, int nbox, int64_t nmodes,
                  int interlace, int k_min, cudaStream_t st);
 

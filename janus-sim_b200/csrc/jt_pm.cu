@@ -165,34 +165,43 @@ __global__ void k_b_tile_ranges(const jt_seg_dev* __restrict__ segs, const jt_bo
 // Tiled deposit: one CTA per Morton-aligned tile of T^3 cells of one box.
 // The tile's particles are one contiguous range of each species' sorted
 // array (B.ranges); they are accumulated into a shared-memory copy of the
-// tile plus a halo (edge S = T + 3 holds every TSC stencil of a particle
-// inside the tile, including the interlaced grid's half-cell shift) with
-// shared-memory float atomics, then flushed with one global reduction per
-// non-zero cell.  Stencils that leave the halo (a particle outside its tile
-// after the drift) go straight to the grid.
-template <int ORDER, int NG>
+// tile plus a halo with shared-memory float atomics, then flushed to the
+// grid with global reductions.  The halo holds every TSC stencil of a
+// particle inside the tile, the interlaced grid's half-cell shift included:
+// S = T + 3 cells on y and z from the origin T t - 1; on x the rows start
+// 4 cells below the tile (T t - 4, a multiple of 4) and are W = T + 8 cells
+// wide, so that the flush reads and reduces four cells at a time (float4
+// shared loads, one float4 global reduction per non-zero group; 16-byte
+// aligned because M, the row start and the grid base are multiples of 4).
+// Stencils that leave the halo (a particle outside its tile after the
+// drift) go straight to the grid.  TT: the tile edge as a constant (16, the
+// edge of every grid of 16^3 and up) or 0 (read per box).
+template <int ORDER, int NG, int TT>
 __global__ void __launch_bounds__(256)
 k_b_deposit(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ boxes,
             const int64_t* __restrict__ tprefix, int nbox, int src)
 {
-    extern __shared__ float tile[];
+    extern __shared__ float4 tile4[];
+    float* tile = reinterpret_cast<float*>(tile4);
     const int64_t q = blockIdx.x;
     const int b = jt_find(tprefix, nbox, q);
     const jt_box_dev& B = boxes[b];
     if (src && !B.rho_s) return;   // the unsigned source of an unscreened box: not used
     const uint32_t t = (uint32_t)(q - tprefix[b]);
-    const int T = B.T, M = B.M;
-    const int S = T + 3;
-    const int S3 = S * S * S;
-    const int bx = (int)compact3(t) * T - 1;
+    const int T = TT > 0 ? TT : B.T, M = B.M;
+    const int S = T + 3, W = T + 8, W4 = W / 4;
+    const int SW = S * W;
+    const int ax = (int)compact3(t) * T - 4;
     const int by = (int)compact3(t >> 1) * T - 1;
     const int bz = (int)compact3(t >> 2) * T - 1;
-    for (int c = threadIdx.x; c < NG * S3; c += blockDim.x) tile[c] = 0.0f;
-    __syncthreads();
     const int4 r = B.ranges[t];
+    const int n0 = r.y - r.x, n1 = r.w - r.z;
+    if (n0 + n1 == 0) return;   // an empty tile adds nothing (whole block)
+    const int nq = NG * S * S * W4;
+    for (int c = threadIdx.x; c < nq; c += blockDim.x) tile4[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+    __syncthreads();
     const int mask = M - 1;
     const int64_t G = (int64_t)M * M * M;
-    const int n0 = r.y - r.x, n1 = r.w - r.z;
     const float halfL = B.halfL, hinv = B.h_inv;
     const float inv_vol = hinv * hinv * hinv;
     const float q0 = B.mass[0] * inv_vol, q1 = (src ? B.mass[1] : -B.mass[1]) * inv_vol;
@@ -211,17 +220,17 @@ k_b_deposit(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ 
             int ix = jt_stencil<ORDER>(gx - sh, wx);
             int iy = jt_stencil<ORDER>(gy - sh, wy);
             int iz = jt_stencil<ORDER>(gz - sh, wz);
-            int lx = ix - bx, ly = iy - by, lz = iz - bz;
-            bool inside = lx >= 0 && ly >= 0 && lz >= 0 && lx + ORDER <= S && ly + ORDER <= S &&
+            int lx = ix - ax, ly = iy - by, lz = iz - bz;
+            bool inside = lx >= 0 && ly >= 0 && lz >= 0 && lx + ORDER <= W && ly + ORDER <= S &&
                           lz + ORDER <= S;
             if (inside) {
-                float* tb_ = tile + g * S3;
+                float* tb_ = tile + g * S * SW;
 #pragma unroll
                 for (int c = 0; c < ORDER; c++)
 #pragma unroll
                     for (int bb = 0; bb < ORDER; bb++) {
                         float wyz = qq * wz[c] * wy[bb];
-                        float* row = tb_ + ((lz + c) * S + (ly + bb)) * S + lx;
+                        float* row = tb_ + (lz + c) * SW + (ly + bb) * W + lx;
 #pragma unroll
                         for (int a = 0; a < ORDER; a++) atomicAdd(row + a, wyz * wx[a]);
                     }
@@ -240,13 +249,14 @@ k_b_deposit(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ 
         }
     }
     __syncthreads();
-    for (int c = threadIdx.x; c < NG * S3; c += blockDim.x) {
-        float v = tile[c];
-        if (v == 0.0f) continue;
-        int g = c / S3, rem = c - g * S3;
-        int lz = rem / (S * S), ly = (rem / S) % S, lx = rem % S;
-        int64_t idx = ((int64_t)((bz + lz) & mask) * M + ((by + ly) & mask)) * M + ((bx + lx) & mask);
-        atomicAdd(rho + g * G + idx, v);
+    for (int c = threadIdx.x; c < nq; c += blockDim.x) {
+        const float4 v = tile4[c];
+        if (v.x == 0.0f && v.y == 0.0f && v.z == 0.0f && v.w == 0.0f) continue;
+        const int qx = c % W4, row = c / W4;
+        const int ly = row % S, gz = row / S;
+        const int lz = gz % S, g = gz / S;
+        const int64_t idx = ((int64_t)((bz + lz) & mask) * M + ((by + ly) & mask)) * M + ((ax + 4 * qx) & mask);
+        atomicAdd(reinterpret_cast<float4*>(rho + g * G + idx), v);
     }
 }
 
@@ -364,20 +374,26 @@ void jt_b_tile_ranges(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const
 
 // all boxes of a batch share order, ngrid and the tile edge T
 int jt_b_deposit(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_tprefix,
-                 int nbox, int64_t ntiles, int order, int ngrid, int T, cudaStream_t st, int src)
+                 int nbox, int64_t ntiles, int order, int ngrid, int T, cudaStream_t st, int src, bool T16)
 {
     if (ntiles <= 0) return JT_OK;
-    int S = T + 3;
-    size_t smem = sizeof(float) * (size_t)ngrid * S * S * S;
-#define JT_BDEP(O, NG)                                                                        \
+    int S = T + 3, W = T + 8;
+    size_t smem = sizeof(float) * (size_t)ngrid * S * S * W;
+    // T16: every box of the pass has the tile edge 16 (T is the largest)
+#define JT_BDEP1(O, NG, TT)                                                                   \
     do {                                                                                      \
         static bool attr = false;                                                             \
         if (!attr) {                                                                          \
-            cudaFuncSetAttribute(k_b_deposit<O, NG>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+            cudaFuncSetAttribute(k_b_deposit<O, NG, TT>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
                                  96 * 1024);                                                  \
             attr = true;                                                                      \
         }                                                                                     \
-        k_b_deposit<O, NG><<<(unsigned)ntiles, 256, smem, st>>>(d_segs, d_boxes, d_tprefix, nbox, src); \
+        k_b_deposit<O, NG, TT><<<(unsigned)ntiles, 256, smem, st>>>(d_segs, d_boxes, d_tprefix, nbox, src); \
+    } while (0)
+#define JT_BDEP(O, NG)                    \
+    do {                                  \
+        if (T16) JT_BDEP1(O, NG, 16);     \
+        else JT_BDEP1(O, NG, 0);          \
     } while (0)
     if (order == 2 && ngrid == 1) JT_BDEP(2, 1);
     else if (order == 2 && ngrid == 2) JT_BDEP(2, 2);
@@ -385,6 +401,7 @@ int jt_b_deposit(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int6
     else if (order == 3 && ngrid == 2) JT_BDEP(3, 2);
     else return JT_EINVAL;
 #undef JT_BDEP
+#undef JT_BDEP1
     return cudaGetLastError() == cudaSuccess ? JT_OK : JT_ECUDA;
 }
 
