@@ -160,7 +160,7 @@ def ensemble_boxes(n_boxes=64, seed=7):
     log-uniform in [16, 96] (N = n^3 per species), L ~ U(50, 300) Mpc, PM grid
     = next power of two >= 2n (32..256), mu ~ U(5, 30), eta ~ U(1.00, 1.10)
     (eta enters only the expansion factors, not the force path), seeded
-    Zel'dovich ICs (seed 1000 + box), cfg1's theta / r_s / r_cut / softening
+    Zel'dovich ICs (seed 1000 + box), the 2x224^3 workload's theta / r_s / r_cut / softening
     rules and mass density."""
     rng = np.random.default_rng(seed)
     boxes = []
@@ -177,7 +177,7 @@ def ensemble_boxes(n_boxes=64, seed=7):
 def box_config(J, bx):
     r_s = 1.25 * bx["L"] / bx["M"]
     spacing = bx["L"] / bx["n"]
-    # cfg1's mass per particle scaled to the same mean density
+    # the 2x224^3 workload's mass per particle scaled to the same mean density
     gm = 1.0e-3 * (spacing / (250.0 / 224.0)) ** 3
     return J.Config(box_L=bx["L"], pm_grid=bx["M"], theta=0.5,
                     softening=bx["L"] / (2 * bx["n"] ** 3) ** (1.0 / 3.0) / 30.0, r_s=r_s,

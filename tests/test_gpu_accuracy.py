@@ -1,6 +1,7 @@
-"""Force accuracy on clustered data (the configs[2] shape), theta swept.
+"""Force accuracy on clustered data (the clustered workload's shape), theta
+swept.
 
-configs[2] is 2x128^3 particles in L = 100 Mpc on a 256^3 grid: 80% in 512
+The clustered workload is 2x128^3 particles in L = 100 Mpc on a 256^3 grid: 80% in 512
 Plummer spheres (scale radii log-uniform 0.05-1 Mpc, species alternating by
 sphere) plus 20% uniform background.  Here the same density, cell size,
 r_s = 1.25 cells, r_cut = 4.5 r_s and softening in a box half the side:
@@ -75,8 +76,8 @@ def test_clustered_accuracy_theta_sweep():
         assert report[f"walk_theta_{theta}"][1] <= bar, (theta, report)
 
 
-def test_uniform_cfg0_error_split():
-    """2x32^3 uniform particles, L = 64, PM 64^3, theta 0.5,
+def test_uniform_small_workload_error_split():
+    """The small uniform workload: 2x32^3 particles, L = 64, PM 64^3, theta 0.5,
     mu 19, r_s = 1.25 cells, r_cut = 4.5 r_s, softening spacing/30; every 4th
     particle as target.  Reports the walk's and the PM path's errors against
     the FP64 split model's two parts (relative to the FP64 total), and the
@@ -111,11 +112,11 @@ def test_uniform_cfg0_error_split():
     assert report["total"][1] <= 1e-3, report
 
 
-def test_energy_drift_cfg2_shape():
-    """configs[2]'s energy drift, at its density and split scale in a box
+def test_energy_drift_clustered_shape():
+    """The clustered workload's energy drift, at its density and split scale in a box
     1/8 the side: 2x16^3 particles from 8 Plummer spheres (species
     alternating by sphere, 20 % uniform background), L = 12.5, PM 32^3
-    (r_s = 0.488 as configs[2]), r_cut = 4.5 r_s, cold start, 100 KDK steps
+    (r_s = 0.488 as the clustered workload), r_cut = 4.5 r_s, cold start, 100 KDK steps
     of dt = 0.01 without Hubble drag.  E = sum m v^2 / 2 (FP64 from the state)
     + the FP64 potential of the truncated split model (oracle/ewald.c,
     short part shifted to zero at r_cut: E is conserved by the model's exact

@@ -134,7 +134,7 @@ def test_job_that_never_fits_is_refused():
 
 
 def test_served_forces_against_the_fp64_oracle():
-    """configs[4]'s accuracy figure: a Poisson mix served under a budget that
+    """The serving workload's accuracy figure: a Poisson mix served under a budget that
     forces swap-outs; for sampled jobs, the forces each holds after its last
     step (at its final positions) against the FP64 split model (periodic
     Ewald long range + short range cut at r_cut, same r_s and softening) on
