@@ -1225,46 +1225,43 @@ struct CellWarpSmem {
     float4 nshift[27];            // periodic shift of its particles
 };
 
-// dense evaluation of candidates [0, cnt) for this lane's TPL targets: every
-// pair computed, the force selected by 0 < r^2 < r_cut^2 (an invalid target
-// slot counts no pair; its result is not written)
+// dense evaluation of candidates [0, cnt) for this lane's target: every pair
+// computed, the force selected by 0 < r^2 < r_cut^2 (an invalid target slot
+// counts no pair; its result is not written).
 // SCR: opposite-species pairs read the box's Yukawa table yt.
-template <int TPL, bool SCR>
-__device__ __forceinline__ unsigned cell_chunk(const float4* __restrict__ cand, int cnt, const float4 (&p)[TPL],
-                                               const float (&si)[TPL], const bool (&valid)[TPL], float rc2,
-                                               float eps2, float c2s, Acc3 (&a)[TPL],
+template <bool SCR>
+__device__ __forceinline__ unsigned cell_chunk(const float4* __restrict__ cand, int cnt, const float4& p, float si,
+                                               bool valid, float rc2, float eps2, float c2s, Acc3& a,
                                                const float2* __restrict__ yt)
 {
     unsigned hits = 0;
-#pragma unroll (4 / TPL)
+#pragma unroll 4
     for (int j = 0; j < cnt; j++) {
         const float4 q = cand[j];
-#pragma unroll
-        for (int u = 0; u < TPL; u++) {
-            const float dx = q.x - p[u].x, dy = q.y - p[u].y, dz = q.z - p[u].z;
-            const float r2 = dx * dx + dy * dy + dz * dz;
-            const bool in = valid[u] && r2 > 0.0f && r2 < rc2;
-            const float rp2 = r2 + eps2;
-            const float ri = rsqrtf(rp2);
-            const float t = fminf(rp2 * c2s, (float)kStab - 1.5f);   // NaN -> the bound
-            const int k = max((int)t, 0);
-            const float2* __restrict__ tb = (SCR && si[u] * q.w < 0.0f) ? yt : g_stab;
-            const float2 ab = __ldg(&tb[k]);
-            const float S = fmaf(ab.y, t - (float)k, ab.x);
-            const float g = in ? si[u] * q.w * S * ri * ri * ri : 0.0f;
-            hits += in ? 1u : 0u;
-            a[u].x += g * dx;
-            a[u].y += g * dy;
-            a[u].z += g * dz;
-        }
+        const float dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        const bool in = valid && r2 > 0.0f && r2 < rc2;
+        const float rp2 = r2 + eps2;
+        const float ri = rsqrtf(rp2);
+        const float t = fminf(rp2 * c2s, (float)kStab - 1.5f);   // NaN -> the bound
+        const int k = max((int)t, 0);
+        const float2* __restrict__ tb = (SCR && si * q.w < 0.0f) ? yt : g_stab;
+        const float2 ab = __ldg(&tb[k]);
+        const float S = fmaf(ab.y, t - (float)k, ab.x);
+        const float g = in ? si * q.w * S * ri * ri * ri : 0.0f;
+        hits += in ? 1u : 0u;
+        a.x += g * dx;
+        a.y += g * dy;
+        a.z += g * dz;
     }
     return hits;
 }
 
-// One batch of a cell's targets: lane l takes targets base + l + 32 u,
-// u < TPL (TPL = 2 for the cells with 33..64 targets left, so that their
-// candidates are streamed and tested once instead of twice).
-template <int ORDER, int NG, int TPL, bool SCR>
+// One batch of a cell's targets: lane l takes target base + l.  (Two
+// targets per lane for cells with more than 32, which streams and tests
+// their candidates once instead of twice, measured slower: its registers
+// lowered the occupancy of the whole kernel.)
+template <int ORDER, int NG, bool SCR>
 __device__ __forceinline__ void cell_batch(const CellArgs& A, const jt_box_dev& B, CellWarpSmem& S, int base,
                                            int t1, int lane, unsigned& pairs, unsigned& cands)
 {
@@ -1272,29 +1269,17 @@ __device__ __forceinline__ void cell_batch(const CellArgs& A, const jt_box_dev& 
     const float rc2 = B.rc2, eps2 = B.eps2, c2s = B.c * B.c * ((float)kStab / kStabYMax);
     const float slack = B.halfL * 9.5367431640625e-7f, rc2_keep = B.rc2 * 1.00001f;
     const float2* __restrict__ yt = (SCR && B.ytab) ? B.ytab : g_stab;
-    float4 p[TPL];
-    int2 id[TPL];
-    bool valid[TPL];
-    float si[TPL];
-    float lox = 3.0e38f, loy = 3.0e38f, loz = 3.0e38f, hix = -3.0e38f, hiy = -3.0e38f, hiz = -3.0e38f;
-#pragma unroll
-    for (int u = 0; u < TPL; u++) {
-        const int t = base + lane + 32 * u;
-        valid[u] = t < t1;
-        p[u] = A.cb.cpos[valid[u] ? t : base];
-        id[u] = A.cb.cid[valid[u] ? t : base];
-        si[u] = p[u].w > 0.f ? 1.0f : -1.0f;
-        lox = fminf(lox, p[u].x); loy = fminf(loy, p[u].y); loz = fminf(loz, p[u].z);
-        hix = fmaxf(hix, p[u].x); hiy = fmaxf(hiy, p[u].y); hiz = fmaxf(hiz, p[u].z);
-    }
-    lox = warp_min(lox); loy = warp_min(loy); loz = warp_min(loz);
-    hix = warp_max(hix); hiy = warp_max(hiy); hiz = warp_max(hiz);
+    const int t = base + lane;
+    const bool valid = t < t1;
+    const float4 p = A.cb.cpos[valid ? t : base];
+    const int2 id = A.cb.cid[valid ? t : base];
+    const float si = p.w > 0.f ? 1.0f : -1.0f;
+    const float lox = warp_min(p.x), loy = warp_min(p.y), loz = warp_min(p.z);
+    const float hix = warp_max(p.x), hiy = warp_max(p.y), hiz = warp_max(p.z);
     const float gcx = 0.5f * (lox + hix), gcy = 0.5f * (loy + hiy), gcz = 0.5f * (loz + hiz);
     const float ghx = 0.5f * (hix - lox) + slack, ghy = 0.5f * (hiy - loy) + slack,
                 ghz = 0.5f * (hiz - loz) + slack;
-    Acc3 near[TPL];
-#pragma unroll
-    for (int u = 0; u < TPL; u++) near[u] = Acc3{0.f, 0.f, 0.f};
+    Acc3 near = {0.f, 0.f, 0.f};
     if (A.parts & 2) {
         int nc = 0;
         for (int nbr = 0; nbr < 27; nbr++) {
@@ -1316,8 +1301,8 @@ __device__ __forceinline__ void cell_batch(const CellArgs& A, const jt_box_dev& 
                 nc += __popc(km);
                 __syncwarp();
                 if (nc >= 32) {
-                    pairs += cell_chunk<TPL, SCR>(S.cand, 32, p, si, valid, rc2, eps2, c2s, near, yt);
-                    cands += 32 * TPL;
+                    pairs += cell_chunk<SCR>(S.cand, 32, p, si, valid, rc2, eps2, c2s, near, yt);
+                    cands += 32;
                     __syncwarp();
                     const float4 t2 = S.cand[32 + lane];
                     __syncwarp();
@@ -1328,30 +1313,28 @@ __device__ __forceinline__ void cell_batch(const CellArgs& A, const jt_box_dev& 
             }
         }
         if (nc > 0) {
-            pairs += cell_chunk<TPL, SCR>(S.cand, nc, p, si, valid, rc2, eps2, c2s, near, yt);
-            cands += nc * TPL;
+            pairs += cell_chunk<SCR>(S.cand, nc, p, si, valid, rc2, eps2, c2s, near, yt);
+            cands += nc;
         }
         __syncwarp();
     }
-#pragma unroll
-    for (int u = 0; u < TPL; u++) {
-        if (!valid[u]) continue;
+    if (valid) {
         Acc3 pm = {0.f, 0.f, 0.f};
-        if (A.parts & 1) pm = pm_interp<ORDER, NG>(B, p[u]);
-        const jt_seg_dev& SG = A.segs[id[u].x];
-        float ax = si[u] * pm.x + near[u].x, ay = si[u] * pm.y + near[u].y, az = si[u] * pm.z + near[u].z;
+        if (A.parts & 1) pm = pm_interp<ORDER, NG>(B, p);
+        const jt_seg_dev& SG = A.segs[id.x];
+        float ax = si * pm.x + near.x, ay = si * pm.y + near.y, az = si * pm.z + near.z;
         if (SCR && B.force_s && (A.parts & 1)) {
-            const Acc3 ps = pm_interp<ORDER, NG, true>(B, p[u]);
+            const Acc3 ps = pm_interp<ORDER, NG, true>(B, p);
             ax += ps.x;
             ay += ps.y;
             az += ps.z;
         }
-        SG.acc[id[u].y] = make_float4(ax, ay, az, 0.f);
+        SG.acc[id.y] = make_float4(ax, ay, az, 0.f);
         if (A.kick_frac != 0.0f) {
             // as k_walk_acc: the closing half kick, and with kick_frac 1.0
             // the next step's opening half kick after it
             const float drag = B.kick_drag, h = 0.5f * B.dt;
-            float4 v = SG.vel[id[u].y];
+            float4 v = SG.vel[id.y];
             v.x += (ax - drag * v.x) * h;
             v.y += (ay - drag * v.y) * h;
             v.z += (az - drag * v.z) * h;
@@ -1360,7 +1343,7 @@ __device__ __forceinline__ void cell_batch(const CellArgs& A, const jt_box_dev& 
                 v.y += (ay - drag * v.y) * h;
                 v.z += (az - drag * v.z) * h;
             }
-            SG.vel[id[u].y] = v;
+            SG.vel[id.y] = v;
         }
     }
 }
@@ -1412,15 +1395,7 @@ __global__ void __launch_bounds__(kWarps * 32, JT_CELL_MINB) k_walk_cell(CellArg
     }
     __syncwarp();
     unsigned pairs = 0, cands = 0;
-    for (int base = t0; base < t1;) {
-        if (t1 - base > 32) {
-            cell_batch<ORDER, NG, 2, SCR>(A, B, S, base, t1, lane, pairs, cands);
-            base += 64;
-        } else {
-            cell_batch<ORDER, NG, 1, SCR>(A, B, S, base, t1, lane, pairs, cands);
-            base += 32;
-        }
-    }
+    for (int base = t0; base < t1; base += 32) cell_batch<ORDER, NG, SCR>(A, B, S, base, t1, lane, pairs, cands);
     if (A.stats) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
