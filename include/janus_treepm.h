@@ -381,6 +381,13 @@ int  jt_batch_add_zeldovich(jt_batch* b, const jt_config* cfg, const jt_ics_para
 int  jt_batch_checkpoint_async(jt_batch* b, int box_id, const char* path,
                                const jt_snapshot_meta* meta);
 int  jt_batch_checkpoint_wait(jt_batch* b);
+/* Create the cuFFT plans that passes over boxes of this grid size can use
+ * (one per power-of-two batch up to an execution's limit of 2^27 elements,
+ * both directions), so that no later step creates one: a plan costs more to
+ * make than its transforms take.  Steps create what they lack anyway; this
+ * moves the cost ahead (the serving loop calls it when a job with a new
+ * grid size is registered).  jt_batch_trim releases them. */
+int  jt_batch_prepare(jt_batch* b, int pm_grid);
 /* Yukawa screening of one box's opposite-species pairs in the split model:
  * kappa = 1 / lambda, lambda = lambda_0 sqrt(1 + z) (no quantisation; the
  * reference's set_lambda_0 / set_current_z, src/nbody_gpu_twopass.rs

@@ -1220,6 +1220,21 @@ int jt_batch_add(jt_batch* B, const jt_config* cfg, const float* pos_p, const fl
     return JT_OK;
 }
 
+int jt_batch_prepare(jt_batch* B, int pm_grid)
+{
+    if (!B || pm_grid < 8 || pm_grid > 1024 || (pm_grid & (pm_grid - 1))) return JT_EINVAL;
+    AllocScope scope(&B->actx);
+    Bucket& k = B->buckets[pm_grid];
+    k.M = pm_grid;
+    // every batch an execution can take: the powers of two up to the chunk
+    const int ch = fft_chunk(pm_grid);
+    for (int b = 1; b <= ch; b <<= 1) {
+        JT_TRY(make_plan(B, k.r2c, pm_grid, b, true));
+        JT_TRY(make_plan(B, k.c2r, pm_grid, b, false));
+    }
+    return JT_OK;
+}
+
 int jt_batch_set_screening(jt_batch* B, int box_id, double lambda_0, double z)
 {
     if (!box_id_ok(B, box_id) || !(lambda_0 >= 0.0) || !(z > -1.0) || !std::isfinite(lambda_0) ||

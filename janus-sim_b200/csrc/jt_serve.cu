@@ -30,6 +30,7 @@
 #include <cstring>
 #include <deque>
 #include <new>
+#include <set>
 #include <thread>
 #include <vector>
 
@@ -74,6 +75,7 @@ struct jt_server {
     size_t peak_device = 0;
     double admit_s = 0.0, evict_s = 0.0;   // wall time in admissions / evictions
     int max_resident = 0;
+    std::set<int> prepared;        // grid sizes whose cuFFT plans the batch holds (jt_batch_prepare)
 };
 
 namespace {
@@ -166,6 +168,7 @@ size_t need_of(size_t persistent, size_t scratch, size_t fft_ws)
 int trim(jt_server* S)
 {
     S->trims++;
+    S->prepared.clear();   // the trim releases the plans too
     return jt_batch_trim(S->B);
 }
 
@@ -355,6 +358,12 @@ int jt_server_add_job(jt_server* S, const jt_config* cfg, const float* pos_p, co
     else std::memset(h + 6 * n_p + 3 * n_m, 0, sizeof(float) * 3 * n_m);
     S->jobs.push_back(j);
     *job_id = (int)S->jobs.size() - 1;
+    // the cuFFT plans of a new grid size, made now rather than inside the
+    // first batched steps that use them (a failure leaves them to the steps)
+    if (S->prepared.insert(cfg->pm_grid).second && jt_batch_prepare(S->B, cfg->pm_grid) != JT_OK) {
+        S->prepared.erase(cfg->pm_grid);
+        cudaGetLastError();
+    }
     return JT_OK;
 }
 

@@ -51,7 +51,7 @@ EXPORTED = [
     "jt_energy_sampled", "jt_virialize_sampled", "jt_energy_drift_pct",
     "jt_batch_checkpoint_async", "jt_batch_checkpoint_wait", "jt_snapshot_write_raw",
     "jt_snapshot_read_raw", "jt_set_accel", "jt_get_accel", "jt_server_get_accel",
-    "jt_batch_set_screening", "jt_step_host",
+    "jt_batch_set_screening", "jt_step_host", "jt_batch_prepare",
 ]
 JT_JOB_QUEUED, JT_JOB_RESIDENT, JT_JOB_DONE = 0, 1, 2
 JT_STATIC_SORT_MAX = 262144
@@ -282,6 +282,7 @@ def library():
     L.jt_set_screening.argtypes = [H, C.c_double, C.c_double]
     L.jt_batch_set_screening.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double]
     L.jt_step_host.argtypes = [H, fp, fp, fp, fp, fp, fp, C.c_double, C.c_double, C.c_double]
+    L.jt_batch_prepare.argtypes = [C.c_void_p, C.c_int]
     L.jt_set_accel.argtypes = [H, fp, fp, C.c_int]
     L.jt_server_get_accel.argtypes = [H, C.c_int, fp, fp]
     L.jt_get_accel.argtypes = [H, fp, fp, C.c_int]
@@ -668,6 +669,11 @@ class Batch:
                "jt_batch_add_zeldovich")
         self.boxes[bid.value] = (n_side ** 3, n_side ** 3)
         return bid.value
+
+    def prepare(self, pm_grid):
+        """Create every cuFFT plan a pass over boxes of this grid size can use
+        (jt_batch_prepare), so that no later step makes one."""
+        _check(library().jt_batch_prepare(self._b, pm_grid), "jt_batch_prepare")
 
     def set_screening(self, box_id, lambda_0, z=0.0):
         """Yukawa screening (kappa = 1 / (lambda_0 sqrt(1 + z))) of one box's

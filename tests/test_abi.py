@@ -83,6 +83,7 @@ def test_null_arguments():
     assert L.jt_get_timings(None, None) == J.JT_EINVAL
     assert L.jt_set_screening(None, 2.0, 0.0) == J.JT_EINVAL
     assert L.jt_batch_set_screening(None, 0, 2.0, 0.0) == J.JT_EINVAL
+    assert L.jt_batch_prepare(None, 64) == J.JT_EINVAL
     L.jt_destroy(None)  # no-op
 
 

@@ -337,3 +337,24 @@ def test_screened_boxes_same_alone_and_in_the_mix():
                 assert float(d.max()) <= VEL_TOL * rms, (k, q, float(d.max()), rms)
     A.close()
     G.close()
+
+
+def test_prepared_plans_change_nothing():
+    """jt_batch_prepare makes the cuFFT plans of a grid size ahead: the same
+    forces as a batch that makes them in its first pass; sizes that are not
+    powers of two in [8, 1024] are refused."""
+    boxes = BOXES[:3]
+    A, P = J.Batch(), J.Batch()
+    for M in sorted({b[4] for b in boxes}):
+        P.prepare(M)
+    with pytest.raises(J.JanusError):
+        P.prepare(48)
+    ia = [A.add(*make_box(*box)) for box in boxes]
+    ip = [P.add(*make_box(*box)) for box in boxes]
+    A.forces(ia)
+    P.forces(ip)
+    for a, p in zip(ia, ip):
+        for x, y in zip(P.accel(p), A.accel(a)):
+            _cmp(x, y, FORCE_TOL)
+    A.close()
+    P.close()
