@@ -1132,7 +1132,14 @@ __global__ void k_cell_key(CellArgs A, int64_t npart)
     const int cx = cell_of(p.x, B.halfL, B.cell_inv, nb), cy = cell_of(p.y, B.halfL, B.cell_inv, nb),
               cz = cell_of(p.z, B.halfL, B.cell_inv, nb);
     const int key = (int)(B.cbase + ((int64_t)cz * nb + cy) * nb + cx);
-    A.cb.cslot[i] = (unsigned)atomicAdd(A.cb.ccount + key, 1);
+    // one atomic per distinct cell of the warp (Morton-ordered particles
+    // mostly share their lanes' cells); slots follow lane order in a group
+    const unsigned peers = __match_any_sync(__activemask(), key);
+    const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
+    unsigned base = 0;
+    if (lane == leader) base = (unsigned)atomicAdd(A.cb.ccount + key, __popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    A.cb.cslot[i] = base + (unsigned)__popc(peers & ((1u << lane) - 1u));
     A.cb.ccell[i] = key;
     A.cb.tflag[i] = 0;
 }
