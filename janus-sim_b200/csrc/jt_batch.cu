@@ -863,8 +863,7 @@ int capture_graphs(jt_batch* B, const std::vector<int>& v, const jt_box_step* st
             r = JT_ECUDA;
             break;
         }
-        jt_b_kick(P.d_pre, P.d_bx, P.d_pp, (int)P.pre.size(), P.npart, 0.5f, B->st);
-        jt_b_drift(P.d_pre, P.d_bx, P.d_pp, (int)P.pre.size(), P.npart, 1.0f, B->st);
+        jt_b_kick_drift(P.d_pre, P.d_bx, P.d_pp, (int)P.pre.size(), P.npart, 0.5f, 1.0f, B->st);
         int rf = force_pass(B, P, JT_PART_ALL, 0.5f);   // swaps the boxes' buffers and P
         cudaGraph_t g = nullptr;
         cudaError_t ec = cudaStreamEndCapture(B->st, &g);
@@ -887,7 +886,7 @@ int capture_graphs(jt_batch* B, const std::vector<int>& v, const jt_box_step* st
         drop_graphs(B);
         return r;
     }
-    B->gc.launches = per_pass / 2 + 2;
+    B->gc.launches = per_pass / 2 + 1;   // the force pass and the kick-drift
     B->gc.ids = v;
     B->gc.gen = B->gen;
     B->gc.plan = P;
@@ -1039,10 +1038,9 @@ int jtb_step_host(jt_batch* B, int box_id, float* const pos[2], float* const vel
     double kd = 0.0;
     if (r == JT_OK) {
         cudaEventRecord(k0, st);
-        jt_b_kick(P.d_pre, P.d_bx, P.d_pp, (int)P.pre.size(), P.npart, 0.5f, st);
-        jt_b_drift(P.d_pre, P.d_bx, P.d_pp, (int)P.pre.size(), P.npart, 1.0f, st);
+        jt_b_kick_drift(P.d_pre, P.d_bx, P.d_pp, (int)P.pre.size(), P.npart, 0.5f, 1.0f, st);
         cudaEventRecord(k1, st);
-        B->tm.launches += 2;
+        B->tm.launches += 1;
         // the positions are final: pack them into their upload slots (still
         // in the caller's order) and copy them back while the forces run
         for (int s = 0; s < 2; s++)
@@ -1359,9 +1357,9 @@ int jt_batch_step(jt_batch* B, const int* ids, int n_ids, const jt_step_args* ar
     if (r == JT_OK && nsteps > 0) r = build_plan(B, v, steps.data(), P);
     for (int k = 0; k < nsteps && r == JT_OK; k++) {
         cudaEventRecord(k0, B->st);
-        if (k == 0) jt_b_kick(P.d_pre, P.d_bx, P.d_pp, (int)P.pre.size(), P.npart, 0.5f, B->st);
-        jt_b_drift(P.d_pre, P.d_bx, P.d_pp, (int)P.pre.size(), P.npart, 1.0f, B->st);
-        B->tm.launches += (k == 0 ? 2 : 1);
+        if (k == 0) jt_b_kick_drift(P.d_pre, P.d_bx, P.d_pp, (int)P.pre.size(), P.npart, 0.5f, 1.0f, B->st);
+        else jt_b_drift(P.d_pre, P.d_bx, P.d_pp, (int)P.pre.size(), P.npart, 1.0f, B->st);
+        B->tm.launches += 1;
         cudaEventRecord(k1, B->st);
         // closing half kick, merged with the next step's opening half kick
         r = force_pass(B, P, JT_PART_ALL, k + 1 < nsteps ? 1.0f : 0.5f);

@@ -312,10 +312,10 @@ int jt_cell_scan_blocks(int64_t ncells);
 void jt_yukawa_table(double b, float2* tab);
 constexpr int JT_STAB_N = 4096;
 
-// kick v += (a - drag v) frac*dt and drift x += v frac*dt with each box's own
-// dt and drag (jt_box_dev)
-void jt_b_kick(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_prefix, int nseg,
-               int64_t ntotal, float frac, cudaStream_t st);
+// kick v += (a - drag v) kfrac*dt then drift x += v dfrac*dt, and the drift
+// alone, with each box's own dt and drag (jt_box_dev)
+void jt_b_kick_drift(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_prefix, int nseg,
+                     int64_t ntotal, float kfrac, float dfrac, cudaStream_t st);
 void jt_b_drift(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_prefix, int nseg,
                 int64_t ntotal, float frac, cudaStream_t st);
 

@@ -1629,20 +1629,33 @@ extern "C" int jt_fp32_peak(int iters, double* tflops)
 namespace {
 
 // v += (a - drag_b v) dt over every segment's particles (drag per box)
-__global__ void k_b_kick(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ boxes,
-                         const int64_t* __restrict__ prefix, int nseg, float frac)
+// the opening kick of kfrac dt followed by the drift of dfrac dt (below), in
+// one pass over the particles
+__global__ void k_b_kick_drift(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ boxes,
+                               const int64_t* __restrict__ prefix, int nseg, float kfrac, float dfrac)
 {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= prefix[nseg]) return;
     const int g = jt_find(prefix, nseg, i);
     const int64_t j = i - prefix[g];
     const jt_seg_dev& S = segs[g];
-    const float drag = boxes[S.box].kick_drag, dt = frac * boxes[S.box].dt;
-    float4 v = S.vel[j], a = S.acc[j];
-    v.x += (a.x - drag * v.x) * dt;
-    v.y += (a.y - drag * v.y) * dt;
-    v.z += (a.z - drag * v.z) * dt;
+    const jt_box_dev& B = boxes[S.box];
+    const float drag = B.kick_drag, dk = kfrac * B.dt, dd = dfrac * B.dt;
+    float4 v = S.vel[j], a = S.acc[j], p = S.pos[j];
+    v.x += (a.x - drag * v.x) * dk;
+    v.y += (a.y - drag * v.y) * dk;
+    v.z += (a.z - drag * v.z) * dk;
     S.vel[j] = v;
+    p.x += v.x * dd;
+    p.y += v.y * dd;
+    p.z += v.z * dd;
+    p.x = p.x > B.halfL ? p.x - B.L : p.x;
+    p.x = p.x < -B.halfL ? p.x + B.L : p.x;
+    p.y = p.y > B.halfL ? p.y - B.L : p.y;
+    p.y = p.y < -B.halfL ? p.y + B.L : p.y;
+    p.z = p.z > B.halfL ? p.z - B.L : p.z;
+    p.z = p.z < -B.halfL ? p.z + B.L : p.z;
+    S.pos[j] = p;
 }
 
 // x += v dt with one periodic wrap per axis (box side per box)
@@ -1670,11 +1683,12 @@ __global__ void k_b_drift(const jt_seg_dev* __restrict__ segs, const jt_box_dev*
 
 }  // namespace
 
-void jt_b_kick(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_prefix, int nseg,
-               int64_t ntotal, float frac, cudaStream_t st)
+void jt_b_kick_drift(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_prefix, int nseg,
+                     int64_t ntotal, float kfrac, float dfrac, cudaStream_t st)
 {
     if (ntotal <= 0) return;
-    k_b_kick<<<(unsigned)((ntotal + 255) / 256), 256, 0, st>>>(d_segs, d_boxes, d_prefix, nseg, frac);
+    k_b_kick_drift<<<(unsigned)((ntotal + 255) / 256), 256, 0, st>>>(d_segs, d_boxes, d_prefix, nseg, kfrac,
+                                                                      dfrac);
 }
 
 void jt_b_drift(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_prefix, int nseg,
