@@ -696,7 +696,8 @@ int force_pass(jt_batch* B, Plan& P, int parts, float kick_frac)
         B->tm.launches += P.npart > 0 ? (P.ncells > 0 ? 6 : 1) : 0;
     }
     JT_TRY(jt_b_walk(P.d_post, P.d_bx, P.d_gp, nseg, P.ngroups, pool, B->order, B->ngrid, parts,
-                     kick_frac, B->d_stats, B->d_err, st, P.d_pp, tflag, P.screened));
+                     kick_frac, B->d_stats, B->d_err, st, P.d_pp, tflag, P.screened,
+                     tflag ? B->csegflag.p : nullptr));
     cudaEventRecord(B->ev[7], st);
     B->pending = true;
     B->tm.launches += (P.npart > 0 ? 8 : 0) + (P.ninternal > 0 ? 1 : 0) + (P.npart > 0 ? 1 : 0) +

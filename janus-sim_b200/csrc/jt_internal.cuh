@@ -287,7 +287,7 @@ int jt_b_walk(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t
               int64_t ngroups, const jt_tree_dev& pool, int order, int ngrid, int parts,
               float kick_frac, unsigned long long* stats, unsigned* d_err, cudaStream_t st,
               const int64_t* d_pprefix = nullptr, const unsigned char* tflag = nullptr,
-              bool screened = false);
+              bool screened = false, const int* segflag = nullptr);
 // Near-field cell list of a pass (cells of side >= r_cut, both species) and
 // the cell walk over it: particles of cells whose 27-cell neighbourhood holds
 // more than JT_CELL_KMAX candidates, and of boxes without a cell grid, are

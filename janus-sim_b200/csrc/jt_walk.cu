@@ -129,6 +129,7 @@ struct WalkArgs {
     unsigned* err;
     const int64_t* pprefix;       // particles per segment (with tflag)
     const unsigned char* tflag;   // non-null: only flagged particles are computed here
+    const int* segflag;           // with tflag: per segment, some particle is flagged
 };
 
 // Pair interactions of this lane's target with a chunk of candidates: a
@@ -604,6 +605,7 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_walk_acc(WalkArgs A)
     const int64_t gw = (int64_t)blockIdx.x * kWarps + wib;
     if (gw >= A.gprefix[A.nseg]) return;  // whole warp
     const int g = jt_find(A.gprefix, A.nseg, gw);
+    if (A.segflag && A.segflag[g] == 0) return;   // whole warp: no flagged particle in this segment
     const int64_t grp = gw - A.gprefix[g];
     const jt_seg_dev& SG = A.segs[g];
     const jt_box_dev& B = A.boxes[SG.box];
@@ -1473,7 +1475,7 @@ int jt_b_cells(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_
 int jt_b_walk(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_gprefix, int nseg,
               int64_t ngroups, const jt_tree_dev& pool, int order, int ngrid, int parts,
               float kick_frac, unsigned long long* stats, unsigned* d_err, cudaStream_t st,
-              const int64_t* d_pprefix, const unsigned char* tflag, bool screened)
+              const int64_t* d_pprefix, const unsigned char* tflag, bool screened, const int* segflag)
 {
     if (ngroups <= 0) return JT_OK;
     if (int r = stab_ready()) return r;
@@ -1489,6 +1491,7 @@ int jt_b_walk(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t
     A.err = d_err;
     A.pprefix = d_pprefix;
     A.tflag = tflag;
+    A.segflag = tflag ? segflag : nullptr;
     unsigned g = (unsigned)((ngroups + kWarps - 1) / kWarps);
     if (screened) {
         if (order == 3 && ngrid == 2) k_walk_acc<3, 2, 6, 32, true><<<g, kWarps * 32, 0, st>>>(A);
