@@ -118,13 +118,11 @@ extern "C" int jt_morton_sort_static(const float* pos, size_t n, double box_L, u
     if (cudaMemsetAsync(d_err, 0, sizeof(unsigned), st) != cudaSuccess) return JT_ECUDA;
     k_morton_aos<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(pos, nn, (float)(box_L / 2.0), key64,
                                                                 ws.vals);
-    // the digits of the index (low word) first, then the 30 Morton bits
-    int shifts[8], np = 0;
-    int ib = 0;
-    while (ib < 32 && ((int64_t)1 << ib) < nn) ib++;
-    for (int s = 0; s < ib; s += 8) shifts[np++] = s;
-    for (int s = 32; s < 62; s += 8) shifts[np++] = s;
-    r = jt_radix_sort_u64(key64, ws.vals, nn, shifts, np, &ws, d_err, st);
+    // the 30 Morton bits only: the keys start in index order and every LSD
+    // pass is stable, so equal codes keep their index order (the low word)
+    // without sorting its digits
+    const int shifts[4] = {32, 40, 48, 56};
+    r = jt_radix_sort_u64(key64, ws.vals, nn, shifts, 4, &ws, d_err, st);
     if (r != JT_OK) return r;
     jt_launch_split_keys(key64, nn, morton_out, reinterpret_cast<uint32_t*>(perm_out), st);
     if (cudaGetLastError() != cudaSuccess) return JT_ECUDA;

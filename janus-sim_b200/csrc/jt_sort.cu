@@ -304,11 +304,7 @@ int radix_sort(K* keys, uint32_t* vals, int64_t n, const int* shifts, int npass,
     k_radix_hist<K><<<hb, 256, 0, st>>>(keys, n, sh, ws->hist);
     k_radix_scan<<<npass, 256, 0, st>>>(ws->hist);
     size_t smem = sizeof(SortSmem<K>);
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(k_onesweep<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr_set = true;
-    }
+    if (jt_smem_attr((const void*)k_onesweep<K>, (int)smem) != JT_OK) return JT_ECUDA;
     K* a = keys;
     K* b = reinterpret_cast<K*>(ws->keys_alt);
     uint32_t* va = vals;
@@ -592,11 +588,7 @@ int jt_b_sort_reorder(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, int n
     k_b_hist<<<(unsigned)ntiles, 256, 0, st>>>(d_segs, d_tprefix, nseg);
     k_b_scan<<<4 * nseg, 256, 0, st>>>(d_segs);
     size_t smem = sizeof(SortSmem<uint32_t>);
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_b_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
-    }
+    if (jt_smem_attr((const void*)k_b_onesweep, (int)smem) != JT_OK) return JT_ECUDA;
     for (int p = 0; p < 4; p++)
         k_b_onesweep<<<(unsigned)ntiles, kSortThreads, smem, st>>>(d_segs, d_tprefix, nseg, p,
                                                                    d_tickets + p, d_err);

@@ -53,6 +53,20 @@ def test_static_sort_matches_debug_tree_two_calls_in_a_row():
         assert np.array_equal(got_p, ref_p), (seed, n)
 
 
+def test_static_sort_ties_follow_row_order():
+    # rows in a shuffled order with many equal codes: the permutation must be
+    # the stable order of the codes (ties by row), computed by the oracle
+    import oracle as O
+    L = 80.0
+    pos = _positions(24, 50_000, L, collide=True)
+    pos = pos[np.random.default_rng(5).permutation(len(pos))]
+    codes = O.morton30(pos, np.float32(L / 2)).astype(np.uint32)
+    order = np.argsort(codes, kind="stable")
+    got_m, got_p = _static(pos, L)
+    assert np.array_equal(got_m, codes[order])
+    assert np.array_equal(got_p, order.astype(np.int32))
+
+
 def test_static_sort_limits():
     L = J.library()
     assert L.jt_morton_sort_static(None, 10, 64.0, None, None, None) == J.JT_EINVAL
