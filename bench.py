@@ -129,9 +129,9 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_treepm_step(sample_div=4, seed=42, threads=None):
+def cpu_treepm_step(sample_div=4, seed=42, threads=None, r_cut=None):
     """One reference-CPU TreePM step (update + compute_all_forces + kick/drift)
-    on a bounded sample of the workload: the same density, r_s, r_cut,
+    on a bounded sample of the workload: the same density, r_s, cut,
     softening and theta in a box of side L/sample_div (N/sample_div^3
     particles, PM grid M/sample_div).  Returns (particles, seconds, cores)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -148,11 +148,37 @@ def cpu_treepm_step(sample_div=4, seed=42, threads=None):
     mass = np.concatenate([np.full(n, 1.0), np.full(n, w["mu"])]) * 1e-3
     sg = np.concatenate([np.ones(n, np.int8), -np.ones(n, np.int8)])
     t0 = time.perf_counter()
-    acc, tu, tf = O.cpu_treepm_forces(pos, mass, sg, w["r_cut"], M, L, w["theta"], w["eps"])
+    acc, tu, tf = O.cpu_treepm_forces(pos, mass, sg, r_cut or w["r_cut"], M, L, w["theta"], w["eps"])
     vel += acc * w["dt"]
     pos += vel * w["dt"]
     dt = time.perf_counter() - t0
     return len(pos), dt, (threads or os.cpu_count())
+
+
+def reference_gpu_step(n_side, grid, steps=3):
+    """The reference's own GPU TreePM step on this GPU: its kernels (the kernel
+    text of src/nbody_gpu_twopass.rs and cuda/cufft_wrapper.cu, compiled for
+    sm_100a into oracle/_ref/libref_gpu.so) in step_treepm_gpu's launch order
+    (oracle/refgpu/replay.cu), on the same seeded workload, in a child
+    process.  A yardstick beside the CPU baseline; None when the library was
+    not built (it needs the reference checkout at build time)."""
+    lib = os.path.join(ROOT, "oracle", "_ref", "libref_gpu.so")
+    if not os.path.exists(lib):
+        return None
+    try:
+        out = subprocess.run([sys.executable, os.path.join(ROOT, "oracle", "refgpu", "time_refgpu.py"),
+                              "--n-side", str(n_side), "--grid", str(grid), "--steps", str(steps)],
+                             capture_output=True, text=True, timeout=600)
+        line = [x for x in out.stdout.splitlines() if x.startswith("{")]
+        if out.returncode != 0 or not line:
+            return {"error": (out.stderr or out.stdout)[-300:]}
+        r = json.loads(line[-1])
+        r["kind"] = "reference"
+        r["value"] = r.pop("particle_steps_per_s")
+        r["unit"] = UNIT
+        return r
+    except Exception as e:   # the yardstick never fails the bench
+        return {"error": str(e)[:300]}
 
 
 def ensemble_boxes(n_boxes=64, seed=7):
@@ -369,32 +395,75 @@ def run_serving(J, ics, n_small, n_big, steps, rates, H, dt, budget_gb=150.0):
     return out
 
 
+def config_of(w, args, short_cut, ws):
+    """The `config` object of both arms' JSON lines (the same workload)."""
+    return {"workload": f"TreePM KDK step 2x{w['n_side']}^3, L={w['L']:g} Mpc, "
+                        f"PM {w['M']}^3, mu=19, theta=0.5, r_s=1.25 cells, "
+                        f"short-range cut {short_cut / w['r_s']:.3g} r_s, accurate mode",
+            "cut_tail_ppm": args.cut_tail_ppm,
+            "l2": "inputs larger than L2 (no flush)",
+            "parallelism": "replicas" if ws > 1 else "single"}
+
+
+def short_cut_of(w, args):
+    """The engine's short-range cut for the workload (r_cut, or widened by
+    --cut-tail-ppm): the same formula as jt_config_short_cut, here without
+    loading the library (the reference arm)."""
+    from math import erfc, exp
+    if args.cut_tail_ppm <= 0:
+        return w["r_cut"]
+    tol = 1e-6 * args.cut_tail_ppm
+    lo, hi = 0.0, 8.0
+    for _ in range(80):
+        mid = 0.5 * (lo + hi)
+        if erfc(mid) + 1.1283791670955126 * mid * exp(-mid * mid) > tol:
+            lo = mid
+        else:
+            hi = mid
+    return max(w["r_cut"], 2.0 * w["r_s"] * hi)
+
+
 def run_reference(args, ws, rank):
+    """The reference's CPU TreePM path (src/treepm: TreePMForce::update +
+    compute_all_forces, then the kick and drift), restated in C with OpenMP
+    over all host cores (oracle/ref_cpu_treepm.c; the Rust crate cannot be
+    built here).  Each of the W + K steps is one full step of a bounded
+    sample of the workload (2x112^3 particles in a box half the side: the
+    same density, r_s, cut, softening and theta), so the run ends in a few
+    minutes; one full-size 2x224^3 step is timed once after them as a check
+    that the sample's rate is the workload's."""
     if rank != 0:
         return 0
-    w = workload()
+    w = workload(args.n_side, 250.0 * args.n_side / 224.0, args.grid)
     div = args.cpu_sample_div
-    for _ in range(args.warmup if args.warmup < 1 else 1):
-        cpu_treepm_step(div)
+    cut = short_cut_of(w, args)
+    for k in range(args.warmup):
+        cpu_treepm_step(div, seed=100 + k, r_cut=cut)
     tot_n, tot_t, cores = 0, 0.0, os.cpu_count()
     for k in range(args.steps):
-        n, t, cores = cpu_treepm_step(div, seed=42 + k)
+        n, t, cores = cpu_treepm_step(div, seed=42 + k, r_cut=cut)
         tot_n += n
         tot_t += t
     v = tot_n / tot_t
+    full = None
+    if not args.no_full_reference_step:
+        nf, tf, _ = cpu_treepm_step(1, seed=42, r_cut=cut)
+        full = {"particles": nf, "seconds": tf, "value": nf / tf, "unit": UNIT,
+                "what": "one full-size 2x224^3 step of the same code, outside the timed steps"}
     sample = (f"2x{w['n_side'] // div}^3 particles, L={w['L'] / div:g} Mpc, PM "
-              f"{w['M'] // div}^3 (the workload's density, r_s, r_cut, eps, theta in a box "
-              f"1/{div} the side); one full step per sample")
+              f"{w['M'] // div}^3 (the workload's density, r_s, cut, eps, theta in a box "
+              f"1/{div} the side); one full step per sample, {cores} threads")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * w["n_total"] / v,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_t / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded Zel'dovich lattice)",
-        "config": {"workload": "TreePM step 2x224^3, L=250 Mpc, PM 512^3, mu=19, theta=0.5",
-                   "reference_path": "src/treepm (TreePMForce update + compute_all_forces), "
-                                     "C restatement with OpenMP"},
+        "config": config_of(w, args, cut, ws),
+        "reference_path": "src/treepm (TreePMForce update + compute_all_forces), C restatement "
+                          "with OpenMP (oracle/ref_cpu_treepm.c)",
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": sample},
+        "full_size_step": full,
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -417,7 +486,8 @@ def run_ours(args, ws, rank, local):
     n = len(pp)
     cfg = J.Config(box_L=w["L"], pm_grid=w["M"], theta=w["theta"], softening=w["eps"],
                    r_s=w["r_s"], r_cut=w["r_cut"], mu=w["mu"], G_mass_plus=1.0e-3,
-                   mode=J.JT_ACCURATE, integrator=J.JT_KDK)
+                   mode=J.JT_ACCURATE, integrator=J.JT_KDK, cut_tail_ppm=args.cut_tail_ppm)
+    short_cut = J.short_cut(cfg)
     s = J.Solver(cfg)
     s.set_state(pp, vp, pm, vm)
     peak_fp32 = J.fp32_peak_tflops()
@@ -472,6 +542,19 @@ def run_ours(args, ws, rank, local):
     e2e = ws * 2 * n * K / e2e_t
     bytes_state = 2 * n * 3 * 4 * 3     # positions, velocities, accelerations; both species
 
+    # the PM interpolation alone: the cell walk with the pair loop off
+    # (JT_PART_PM).  Algorithmic bytes: positions in (16 B) and accelerations
+    # out (16 B) per particle, and every value of the 3 x NG force grids read
+    # once (the targets come in cell order, so the stencils' reuse stays in
+    # L1/L2)
+    interp_ms = []
+    for _ in range(3):
+        s.accel_part(J.JT_PART_PM)
+        interp_ms.append(s.timings()["cellwalk_ms"])
+    interp_ms = float(np.median(interp_ms))
+    G = w["M"] ** 3
+    interp_bytes = 32.0 * 2 * n + 4.0 * 3 * 2 * G
+
     # roofline of the dominant kernel: the near-field cell walk (FP32 pipe),
     # timed alone by its own events (the walk stage also holds the cell list
     # build and the tree walk of flagged particles, none at this density)
@@ -493,13 +576,16 @@ def run_ours(args, ws, rank, local):
     walk_traffic = WALK_DRAM_BYTES_PER_PARTICLE * 2 * n if args.grid * 224 == 512 * args.n_side else None
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        npart, tcpu, cores = cpu_treepm_step(args.cpu_sample_div)
+        npart, tcpu, cores = cpu_treepm_step(args.cpu_sample_div, r_cut=short_cut)
         cpu = {"value": npart / tcpu, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": f"one reference-CPU TreePM step (oracle/ref_cpu_treepm.c) on "
                          f"2x{w['n_side'] // args.cpu_sample_div}^3 particles in a box "
-                         f"1/{args.cpu_sample_div} the side (same density, r_s, r_cut, "
+                         f"1/{args.cpu_sample_div} the side (same density, r_s, cut, "
                          f"eps, theta), {tcpu:.1f} s"}
     launches = stages.get("launches", 0)
+    ref_gpu = None
+    if rank == 0 and ws == 1 and not args.no_reference_gpu:
+        ref_gpu = reference_gpu_step(args.n_side, args.grid)
     ensemble = None
     serving = None
     if rank == 0 and ws == 1 and args.ensemble_boxes > 0:
@@ -516,11 +602,7 @@ def run_ours(args, ws, rank, local):
             "warmup": args.warmup, "ms_per_step": dev_ms / K, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded Zel'dovich lattice)",
-            "config": {"workload": f"TreePM KDK step 2x{w['n_side']}^3, L={w['L']:g} Mpc, "
-                                   f"PM {w['M']}^3, mu=19, theta=0.5, r_s=1.25 cells, "
-                                   f"r_cut=4.5 r_s, accurate mode",
-                       "l2": "inputs larger than L2 (no flush)",
-                       "parallelism": "replicas" if ws > 1 else "single"},
+            "config": config_of(w, args, short_cut, ws),
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": bytes_state * ws,
                     "d2h_bytes_per_step": bytes_state * ws},
             "roofline": {"bound": "fp32", "kernel": "k_walk_cell", "achieved": achieved,
@@ -532,6 +614,19 @@ def run_ours(args, ws, rank, local):
             "roofline_hbm": {"bound": "hbm", "kernel": "k_kspace_acc", "achieved": ks_gbs,
                              "peak": hbm_peak, "unit": "GB/s", "frac": ks_gbs / hbm_peak,
                              "peak_source": hbm_src},
+            "roofline_deposit": {"bound": "hbm", "kernel": "k_b_deposit (+ grid zeroing, tile ranges)",
+                                 "ms": stages["deposit_ms"] / K, "bytes": 16.0 * 2 * n + 4.0 * 2 * G,
+                                 "achieved": (16.0 * 2 * n + 4.0 * 2 * G) / (stages["deposit_ms"] / K * 1e-3) / 1e9,
+                                 "peak": hbm_peak, "unit": "GB/s",
+                                 "frac": (16.0 * 2 * n + 4.0 * 2 * G) / (stages["deposit_ms"] / K * 1e-3) / 1e9
+                                 / hbm_peak,
+                                 "peak_source": hbm_src},
+            "roofline_interp": {"bound": "hbm", "kernel": "k_walk_cell (JT_PART_PM: interpolation only)",
+                                "ms": interp_ms, "bytes": interp_bytes,
+                                "achieved": interp_bytes / (interp_ms * 1e-3) / 1e9 if interp_ms > 0 else None,
+                                "peak": hbm_peak, "unit": "GB/s",
+                                "frac": interp_bytes / (interp_ms * 1e-3) / 1e9 / hbm_peak if interp_ms > 0 else None,
+                                "peak_source": hbm_src},
             "stages_ms_per_step": {k: round(v / K, 4) for k, v in stages.items()
                                    if k.endswith("_ms")},
             "wall_ms_per_step": 1e3 * wall / K,
@@ -539,6 +634,7 @@ def run_ours(args, ws, rank, local):
             "gpu_launches": int(launches),
             "walk_autotune": J.walk_tuning(),
             "cpu_baseline": cpu,
+            "reference_gpu": ref_gpu,
             "ensemble": ensemble,
             "serving": serving,
         }
@@ -565,6 +661,12 @@ def main():
     ap.add_argument("--serve-big", type=int, default=8)
     ap.add_argument("--serve-steps", type=int, default=4)
     ap.add_argument("--serve-rates", default="0.5,1.0")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip the reference's own GPU step (oracle/refgpu) beside the CPU baseline")
+    ap.add_argument("--no-full-reference-step", action="store_true",
+                    help="reference arm: skip the one full-size step timed after the samples")
+    ap.add_argument("--cut-tail-ppm", type=int, default=0,
+                    help="widen the short-range cut until S(r / 2 r_s) = ppm * 1e-6 (0: r_cut)")
     args = ap.parse_args()
     ws, rank, local = dist()
     if args.impl == "reference":

@@ -44,7 +44,7 @@ extern "C" {
 #define JT_MEM_DEVICE  1
 
 /* ---- force modes ---- */
-/* ACCURATE: signed-source PM (TSC assignment with interlacing by default,
+/* ACCURATE: signed-source PM (PCS assignment with interlacing by default,
  * deconvolved, Gaussian long-range filter, spectral gradient), short-range
  * factor erfc(x) + 2x/sqrt(pi) exp(-x^2), x = r / (2 r_s), Plummer softening,
  * monopole + quadrupole nodes, hard cut at r_cut. */
@@ -78,17 +78,33 @@ typedef struct jt_config {
     int    k_min;        /* zero modes with max(|kx|,|ky|,|kz|) < k_min; 0 = off */
     int    mode;         /* JT_ACCURATE | JT_RCOMPAT */
     int    integrator;   /* JT_KDK | JT_DKD_REF */
-    /* ACCURATE mass assignment: 0 = default (TSC), 2 = CIC, 3 = TSC.  CIC at
-     * r_s = 1.25 cells leaves ~1e-2 relative long-range force errors (FP64
-     * oracle); TSC with interlacing reaches ~5e-4 at p99. */
+    /* ACCURATE mass assignment: 0 = default (PCS), 2 = CIC, 3 = TSC, 4 = PCS
+     * (the cubic B-spline, 64 cells per particle and grid).  At r_s = 1.25
+     * cells with interlacing, on a Zel'dovich lattice (FP64 oracle, PM part
+     * relative to the total force): TSC p50 2.4e-4 / p99 2.5e-3, PCS
+     * p50 1.6e-5 / p99 2.6e-4; CIC leaves ~1e-2. */
     int    pm_order;
     /* ACCURATE interlacing (second grid shifted by half a cell, odd aliases
      * cancel): 0 = default (on), 1 = on, 2 = off. */
     int    pm_interlace;
-    int    reserved[3];  /* zero */
+    /* ACCURATE short-range tail: 0 = the walk cuts at r_cut as given; k > 0 =
+     * the walk's cut is widened (r_cut stays the floor) to the radius where
+     * the short-range factor S(r / 2 r_s) falls to k * 1e-6, so that the pairs
+     * the cut drops carry at most that fraction of their Newtonian force.
+     * With r_cut = 4.5 r_s, S(2.25) = 1.8 % sets the error floor against the
+     * full periodic sum (p99 ~7e-3 on uniform boxes); k = 440 (S = 4.4e-4,
+     * cut 6 r_s) brings that part of the error to the softening convention's
+     * floor (p99 ~3e-4) at (6 / 4.5)^3 = 2.4x the pairs. */
+    int    cut_tail_ppm;
+    int    reserved[2];  /* zero */
 } jt_config;
 
 typedef struct jt_handle jt_handle;
+
+/* The short-range cut an accurate-mode handle or batch box uses for this
+ * config: r_cut, widened by cut_tail_ppm when that is set.  No counterpart
+ * in the reference (its cut is r_cut). */
+int  jt_config_short_cut(const jt_config* cfg, double* cut);
 
 /* Stage timings of the last jt_accel / jt_step call, milliseconds of device
  * time (CUDA events on the handle's stream), summed over the call. */
@@ -497,11 +513,58 @@ int  jt_server_get_state(jt_server* s, int job, float* pos_p, float* vel_p,
 int  jt_server_get_accel(jt_server* s, int job, float* acc_p, float* acc_m);
 int  jt_server_stats(jt_server* s, jt_serve_stats* out);
 
+/* ---- Janus expansion history (FP64) ----
+ * The reference's JanusExpansion (src/janus_expansion.rs:62-266): the exact
+ * parametric solution of the positive sector, a+(mu) = alpha^2 cosh^2 mu,
+ * t+(mu) = alpha^2 (mu + sinh^2(mu) / 2) / H0, H+(mu) = H0 sinh(2 mu) /
+ * (alpha^2 cosh^2 mu (1 + sinh(2 mu) / 2)), H0 = 0.0715 / Gyr, mu0 = 1.5,
+ * alpha from H+(mu0) = H0, a+ = 1 and z = 0 at mu0.  A table of n_points
+ * states uniform in mu from z_init (clamped to 0.99 z_max, z_max = the
+ * redshift of mu = 0) to z = 0, interpolated linearly in time or redshift
+ * as the reference's at_time / at_redshift: the drivers' step schedule
+ * (t = t_start + k dt) and the kick's drag factor H (hubble of jt_step).
+ * The reference's production run builds it with z_init = 4 and 5000 rows
+ * (src/bin/janus_mu19_production.rs:46). */
+typedef struct jt_expansion_state {
+    double mu;       /* parameter mu */
+    double a_plus;   /* scale factor, 1 at z = 0 */
+    double t_gyr;    /* cosmic time (Gyr) */
+    double h_plus;   /* Hubble rate (1/Gyr) */
+    double z;        /* redshift */
+} jt_expansion_state;
+typedef struct jt_expansion_info_t {
+    double  alpha, mu_0, a_0;   /* calibration (calibrate_alpha_mu0, :247-266) */
+    double  z_max, z_init;      /* parametric limit; z_init after the clamp */
+    double  t_start, t_end;     /* table range in time (Gyr) */
+    int64_t n_points;
+} jt_expansion_info_t;
+typedef struct jt_expansion jt_expansion;
+/* JanusExpansion::new(z_init, n_points) (:62-123); n_points >= 2. */
+int  jt_expansion_create(double z_init, int n_points, jt_expansion** out);
+void jt_expansion_destroy(jt_expansion* e);
+int  jt_expansion_info(const jt_expansion* e, jt_expansion_info_t* out);
+/* at_time (:126-154): t clamped to the table, linear interpolation of the
+ * bracketing rows (t_gyr = the clamped t). */
+int  jt_expansion_at_time(const jt_expansion* e, double t_gyr, jt_expansion_state* out);
+/* at_redshift (:157-180): linear interpolation in z (z = the argument;
+ * outside the table the end row). */
+int  jt_expansion_at_redshift(const jt_expansion* e, double z, jt_expansion_state* out);
+/* compute_state (:196-230) and calibrate_alpha_mu0 (:247-266). */
+int  jt_expansion_state_at_mu(double mu, double alpha, double a_0, jt_expansion_state* out);
+int  jt_expansion_calibrate(double* alpha, double* mu_0);
+/* Cross-species factors of an eta scan: a- = a+ (1 + z)^{-(eta - 1) / eta}
+ * (src/vsl_dynamic.rs:138-142), phi = (a- / a+)^3, phi_inv = (a+ / a-)^3
+ * (src/janus_expansion.rs:449-462).  Outputs may be NULL. */
+int  jt_expansion_phi_factors(double a_plus, double eta, double* a_minus, double* phi, double* phi_inv);
+
 /* ---- allocation-free Morton sort ----
  * The reference's Morton keys of n positions already on the device (float3
- * array, box [-L/2, L/2)), sorted by the key (morton30 << 32) | index: writes
- * morton_out[n] (sorted 30-bit codes) and perm_out[n] (index of each sorted
- * position) to device memory -- the morton/perm outputs of jt_debug_tree.
+ * array, box [-L/2, L/2)), sorted by the key (morton30 << 32) | i, i = the
+ * row of the position in `pos` (equal codes keep their row order): writes
+ * morton_out[n] (sorted 30-bit codes) and perm_out[n] (row of each sorted
+ * position) to device memory.  For the species array a handle was loaded
+ * with (jt_set_state) these are the morton/perm outputs of jt_debug_tree,
+ * whose key carries each particle's index in that array in the low word.
  * Every byte of scratch of its onesweep radix sort lives in one fixed
  * file-scope static device array of JT_STATIC_SORT_BYTES (6.5 MiB); the call
  * allocates nothing (no cudaMalloc, cudaFree or allocating library call).
@@ -515,9 +578,11 @@ int  jt_server_stats(jt_server* s, jt_serve_stats* out);
  * do, stalling every other stream on it).
  * The static array keeps the last call's contents; calls that overlap in
  * time (several threads or streams) race on it and must be serialised by the
- * caller; make the first call on each device before any stream capture,
- * since that call looks up the array's address (cudaGetSymbolAddress, once
- * per device).  No counterpart in the reference. */
+ * caller.  The first call on each device looks up the array's address
+ * (cudaGetSymbolAddress, once per device): make that first call before any
+ * stream capture.  Every call copies the sort's error word to a host
+ * variable and synchronises `stream` before it returns.  No counterpart in
+ * the reference. */
 #define JT_STATIC_SORT_MAX    262144
 #define JT_STATIC_SORT_BYTES  6824448
 int  jt_morton_sort_static(const float* pos, size_t n, double box_L,

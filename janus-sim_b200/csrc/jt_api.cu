@@ -21,8 +21,26 @@
 #include <cstdlib>
 #include <cstring>
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <new>
+#include <utility>
 #include <vector>
+
+int jt_smem_attr(const void* kernel, int bytes)
+{
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, int> done;   // (device, kernel) -> bytes set
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return JT_ECUDA;
+    std::lock_guard<std::mutex> lock(mu);
+    int& have = done[std::make_pair(dev, kernel)];
+    if (have >= bytes) return JT_OK;
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess)
+        return JT_ECUDA;
+    have = bytes;
+    return JT_OK;
+}
 
 struct jt_handle {
     jt_config cfg;
@@ -132,15 +150,29 @@ int validate(const jt_config* c)
     if (!(c->softening >= 0.0) || !std::isfinite(c->softening)) return JT_EINVAL;
     if (!(c->r_cut > 0.0) || c->r_cut >= 0.5 * c->box_L) return JT_EINVAL;
     if (c->mode == JT_ACCURATE && !(c->r_s > 0.0)) return JT_EINVAL;
+    if (c->cut_tail_ppm < 0 || c->cut_tail_ppm >= 1000000) return JT_EINVAL;
+    if (c->mode == JT_ACCURATE && !(jt_short_cut(*c) < 0.5 * c->box_L)) return JT_EINVAL;
     if (!(c->mu >= 0.0) || !std::isfinite(c->mu)) return JT_EINVAL;
     if (!(c->G_mass_plus > 0.0) || !std::isfinite(c->G_mass_plus)) return JT_EINVAL;
     if (c->k_min < 0) return JT_EINVAL;
     if (c->mode != JT_ACCURATE && c->mode != JT_RCOMPAT) return JT_EINVAL;
     if (c->integrator != JT_KDK && c->integrator != JT_DKD_REF) return JT_EINVAL;
-    if (c->pm_order != 0 && c->pm_order != 2 && c->pm_order != 3) return JT_EINVAL;
+    if (c->pm_order != 0 && (c->pm_order < 2 || c->pm_order > 4)) return JT_EINVAL;
     if (c->pm_interlace < 0 || c->pm_interlace > 2) return JT_EINVAL;
     return JT_OK;
 }
+
+}  // namespace
+
+extern "C" int jt_config_short_cut(const jt_config* cfg, double* cut)
+{
+    if (!cfg || !cut) return JT_EINVAL;
+    if (int r = validate(cfg)) return r;
+    *cut = cfg->mode == JT_ACCURATE ? jt_short_cut(*cfg) : cfg->r_cut;
+    return JT_OK;
+}
+
+namespace {
 
 void free_trees(jt_handle* h)
 {

@@ -104,7 +104,7 @@ struct Pool {
     }
 };
 
-int box_order(const jt_config& c) { return c.pm_order == 0 ? 3 : c.pm_order; }
+int box_order(const jt_config& c) { return c.pm_order == 0 ? 4 : c.pm_order; }
 int box_ngrid(const jt_config& c) { return c.pm_interlace == 2 ? 1 : 2; }
 
 struct Bucket {                 // PM scratch of the boxes with grid M in a pass
@@ -483,7 +483,8 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
         d.halfL = (float)(c.box_L / 2.0);
         d.box_half = (float)(c.box_L / 2.0);
         d.h_inv = (float)(M / c.box_L);
-        d.rc2 = (float)(c.r_cut * c.r_cut);
+        const double rcut = jt_short_cut(c);
+        d.rc2 = (float)(rcut * rcut);
         d.eps2 = (float)(c.softening * c.softening);
         d.c = (float)(1.0 / (2.0 * c.r_s));
         d.theta2 = (float)(c.theta * c.theta);
@@ -526,10 +527,15 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
         // binning round-off); fewer than 3 per axis: tree walk only
         d.nb = 0;
         d.cbase = P.cprefix.back();
-        if (P.cells && c.r_cut > 0.0) {
-            const double q = c.box_L / (c.r_cut * 1.0001);
+        if (P.cells && rcut > 0.0) {
+            const double q = c.box_L / (rcut * 1.0001);
             int nbc = q >= 256.0 ? 256 : (int)q;
             if (nbc >= 3) d.nb = nbc;
+        }
+        // a widened cut scales every neighbourhood's count by (cut / r_cut)^3
+        {
+            const double w = rcut / c.r_cut;
+            d.cell_kmax = (int)std::min(1.0e6, JT_CELL_KMAX * std::max(1.0, w * w * w));
         }
         d.cell_inv = d.nb ? (float)(d.nb / c.box_L) : 0.0f;
         P.cprefix.push_back(P.cprefix.back() + (int64_t)d.nb * d.nb * d.nb);
@@ -766,6 +772,25 @@ int valid_ids(jt_batch* B, const int* ids, int n, std::vector<int>& out)
     return JT_OK;
 }
 
+}  // namespace
+
+double jt_short_cut(const jt_config& c)
+{
+    if (c.cut_tail_ppm <= 0 || !(c.r_s > 0.0)) return c.r_cut;
+    // S(x) = erfc(x) + (2 / sqrt(pi)) x e^{-x^2} decreases monotonically:
+    // bisection for S(x) = tol on [0, 8]
+    const double tol = 1e-6 * c.cut_tail_ppm;
+    auto S = [](double x) { return std::erfc(x) + 1.1283791670955126 * x * std::exp(-x * x); };
+    double lo = 0.0, hi = 8.0;
+    for (int it = 0; it < 80; it++) {
+        const double mid = 0.5 * (lo + hi);
+        if (S(mid) > tol) lo = mid; else hi = mid;
+    }
+    return std::max(c.r_cut, 2.0 * c.r_s * hi);
+}
+
+namespace {
+
 int validate_box_config(const jt_config* c)
 {
     auto pow2 = [](int m) { return m > 0 && (m & (m - 1)) == 0; };
@@ -777,10 +802,12 @@ int validate_box_config(const jt_config* c)
     if (!(c->softening >= 0.0) || !std::isfinite(c->softening)) return JT_EINVAL;
     if (!(c->r_cut > 0.0) || c->r_cut >= 0.5 * c->box_L) return JT_EINVAL;
     if (!(c->r_s > 0.0) || !std::isfinite(c->r_s)) return JT_EINVAL;
+    if (c->cut_tail_ppm < 0 || c->cut_tail_ppm >= 1000000) return JT_EINVAL;
+    if (!(jt_short_cut(*c) < 0.5 * c->box_L)) return JT_EINVAL;
     if (!(c->mu >= 0.0) || !std::isfinite(c->mu)) return JT_EINVAL;
     if (!(c->G_mass_plus > 0.0) || !std::isfinite(c->G_mass_plus)) return JT_EINVAL;
     if (c->k_min < 0) return JT_EINVAL;
-    if (c->pm_order != 0 && c->pm_order != 2 && c->pm_order != 3) return JT_EINVAL;
+    if (c->pm_order != 0 && (c->pm_order < 2 || c->pm_order > 4)) return JT_EINVAL;
     if (c->pm_interlace < 0 || c->pm_interlace > 2) return JT_EINVAL;
     return JT_OK;
 }
@@ -1243,17 +1270,18 @@ int jt_batch_set_screening(jt_batch* B, int box_id, double lambda_0, double z)
     jt_box_state* b = B->boxes[box_id];
     const double kappa = lambda_0 > 0.01 ? 1.0 / (lambda_0 * std::sqrt(1.0 + z)) : 0.0;
     if (kappa == b->kappa && (kappa == 0.0) == (b->ytab == nullptr)) return JT_OK;
+    const size_t ntab = (size_t)JT_LTAB_N;
     if (kappa == 0.0) {
         dfree(b->ytab);
-        b->bytes -= sizeof(float2) * JT_STAB_N;
+        b->bytes -= sizeof(float2) * ntab;
     } else {
-        std::vector<float2> tab(JT_STAB_N);
-        jt_yukawa_table(kappa * b->cfg.r_s, tab.data());
+        std::vector<float2> tab(ntab);
+        jt_yukawa_log_table(kappa * b->cfg.r_s, tab.data());
         if (!b->ytab) {
-            JT_TRY(dalloc(&b->ytab, (size_t)JT_STAB_N));
-            b->bytes += sizeof(float2) * JT_STAB_N;
+            JT_TRY(dalloc(&b->ytab, ntab));
+            b->bytes += sizeof(float2) * ntab;
         }
-        JT_CU(cudaMemcpyAsync(b->ytab, tab.data(), sizeof(float2) * JT_STAB_N, cudaMemcpyHostToDevice, B->st));
+        JT_CU(cudaMemcpyAsync(b->ytab, tab.data(), sizeof(float2) * ntab, cudaMemcpyHostToDevice, B->st));
         JT_CU(cudaStreamSynchronize(B->st));
     }
     b->kappa = kappa;

@@ -17,7 +17,7 @@ struct jt_box_state {
     bool acc_valid = false;      // acc belongs to the current positions
     // Yukawa screening of opposite-species pairs (jt_batch_set_screening):
     // kappa = 1 / lambda (0: none) and the short-range split-factor table
-    // of b = kappa r_s (JT_STAB_N float2)
+    // of b = kappa r_s (the log table, JT_LTAB_N float2)
     double kappa = 0.0;
     float2* ytab = nullptr;
     int M = 0, order = 3, ngrid = 2;

@@ -111,8 +111,9 @@ struct jt_box_dev {
     float2* rho_s_k;
     float2* force_s_k;
     float* force_s;
-    const float2* ytab;
+    const float2* ytab;   // the Yukawa kernel's log table (JT_LTAB_N entries)
     int nb;               // cells per axis of the near-field cell list (0: tree walk only)
+    int cell_kmax;        // a cell whose 27-cell neighbourhood holds more goes to the tree walk
     float cell_inv;       // nb / L
     int64_t cbase;        // this box's first cell in the pass's cell tables
 };
@@ -169,6 +170,9 @@ __device__ __forceinline__ jt_sfac jt_split_S2(float x, float c)
 //   ORDER 2 (CIC): nodes floor(g), +1; weights 1-f, f
 //   ORDER 3 (TSC): nodes c-1, c, c+1 with c = nearest node, d = g - c;
 //                  weights (1/2)(1/2-d)^2, 3/4-d^2, (1/2)(1/2+d)^2
+//   ORDER 4 (PCS, the cubic B-spline): nodes f-1 .. f+2 with f = floor(g),
+//                  t = g - f, s = 1 - t; weights s^3/6, 2/3 - t^2 + t^3/2,
+//                  2/3 - s^2 + s^3/2, t^3/6
 // Deposit and interpolation use the same stencil, so the scheme exerts no
 // self-force and conserves momentum.
 template <int ORDER>
@@ -180,6 +184,15 @@ __device__ __forceinline__ int jt_stencil(float g, float* w)
         w[0] = 1.0f - f;
         w[1] = f;
         return (int)f0;
+    } else if (ORDER == 4) {
+        const float f0 = floorf(g);
+        const float t = g - f0, s = 1.0f - t;
+        const float t2 = t * t, s2 = s * s;
+        w[0] = (1.0f / 6.0f) * s2 * s;
+        w[1] = fmaf(0.5f * t2, t, 2.0f / 3.0f - t2);
+        w[2] = fmaf(0.5f * s2, s, 2.0f / 3.0f - s2);
+        w[3] = (1.0f / 6.0f) * t2 * t;
+        return (int)f0 - 1;
     } else {
         float c = floorf(g + 0.5f);
         float d = g - c;
@@ -198,7 +211,25 @@ __device__ __forceinline__ float jt_wrap(float d, float L, float halfL)
     return d;
 }
 
+// Near-field cells whose 27-cell neighbourhood holds more candidates than
+// this (at the config's r_cut; scaled by (cut / r_cut)^3 for a widened cut)
+// send their targets to the tree walk: clustered data, where the dense
+// evaluation's cost grows with the square of the local count.
+#ifndef JT_CELL_KMAX
+#define JT_CELL_KMAX 2048
+#endif
+
+// The short-range cut of an accurate-mode box: r_cut, or with cut_tail_ppm
+// = k > 0 the radius where S(r / 2 r_s) = k * 1e-6 when that is larger.
+double jt_short_cut(const jt_config& c);
+
 // ---------------------------------------------------------------- launchers
+// Raise a kernel's dynamic shared-memory limit to `bytes` on the current
+// device.  cudaFuncSetAttribute applies to the device current when it runs,
+// so the setting is kept per (device, kernel) under a lock (threads driving
+// different devices, or the same one, may launch concurrently).
+int jt_smem_attr(const void* kernel, int bytes);
+
 // sort (jt_sort.cu)
 int jt_sort_ws_alloc(jt_sort_ws* ws, int64_t cap, int max_passes);
 void jt_sort_ws_free(jt_sort_ws* ws);
@@ -268,10 +299,10 @@ struct jt_walk_params {
     float rc2, rc;
     float eps2;
     float c;            // 1 / (2 r_s)
-    float c2s;          // c^2 scaled to the walk's S table index (y / dy)
+    float c2;           // c^2: the pair table's y = (r^2 + eps^2) c^2
     float slack;        // candidate prefilter: padding of the group's box
     float rc2_keep;     // candidate prefilter: widened cut
-    float mass[2];      // per-species particle mass (G folded in)
+    float mass[2];      // per-species particle mass (G folded in) times c^3
     int M;
     float h_inv;        // M / L
     int order;          // PM assignment order (2 CIC, 3 TSC)
@@ -309,8 +340,17 @@ int jt_cell_scan_blocks(int64_t ncells);
 // over [0, 16], JT_STAB_N (value, next - value) entries) for b = kappa r_s.
 // A pass with a screened box (jt_box_dev.ytab) runs the walks' screened
 // instantiations (screened = true).
-void jt_yukawa_table(double b, float2* tab);
-constexpr int JT_STAB_N = 4096;
+// The walks' pair-force table: G(y) = S(sqrt y) / y^{3/2} over
+// y = (r_p / 2 r_s)^2 in [2^-32, 2^6), piecewise linear on 512 segments per
+// octave (entry (a, b): G ~ a + b y), indexed by the float bits of y:
+// entry = (bits(y) >> 14) - JT_LTAB_BASE, clamped to the last entry (zero).
+// The pair force is then s_i s_j m_j c^3 G(y) d with c = 1 / (2 r_s): one
+// table load and one FMA in place of a reciprocal square root and the split
+// factor.  A screened box keeps the same table of the Yukawa kernel (S_Y in
+// place of S, b = kappa r_s) for its opposite-species pairs.
+constexpr int JT_LTAB_N = 38 * 512;
+constexpr unsigned JT_LTAB_BASE = (127u - 32u) * 512u;
+void jt_yukawa_log_table(double b, float2* tab);
 
 // kick v += (a - drag v) kfrac*dt then drift x += v dfrac*dt, and the drift
 // alone, with each box's own dt and drag (jt_box_dev)

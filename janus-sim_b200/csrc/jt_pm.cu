@@ -12,8 +12,8 @@
 //   * deposit: one CTA per Morton-aligned tile of T^3 cells.  Particles are
 //     kept in Morton order, so a tile's particles are one contiguous range of
 //     each species' array; the CTA accumulates them into a shared-memory copy
-//     of the tile plus a one-cell halo with shared-memory float atomics and
-//     flushes it to the grid with coalesced global reductions.  CIC (8 cells)
+//     of the tile plus a halo with shared-memory fixed-point (int32) atomics
+//     and flushes it to the grid with coalesced float4 global reductions.  CIC (8 cells)
 //     or TSC (27 cells); with interlacing a second grid whose nodes sit half a
 //     cell higher on every axis receives the same particles.
 //   * one (batched) R2C; ONE k-space kernel combines the interlaced spectra,
@@ -165,56 +165,81 @@ __global__ void k_b_tile_ranges(const jt_seg_dev* __restrict__ segs, const jt_bo
 // Tiled deposit: one CTA per Morton-aligned tile of T^3 cells of one box.
 // The tile's particles are one contiguous range of each species' sorted
 // array (B.ranges); they are accumulated into a shared-memory copy of the
-// tile plus a halo with shared-memory float atomics, then flushed to the
-// grid with global reductions.  The halo holds every TSC stencil of a
-// particle inside the tile, the interlaced grid's half-cell shift included:
-// S = T + 3 cells on y and z from the origin T t - 1; on x the rows start
-// 4 cells below the tile (T t - 4, a multiple of 4) and are W = T + 8 cells
-// wide, so that the flush reads and reduces four cells at a time (float4
-// shared loads, one float4 global reduction per non-zero group; 16-byte
-// aligned because M, the row start and the grid base are multiples of 4).
-// Stencils that leave the halo (a particle outside its tile after the
-// drift) go straight to the grid.  TT: the tile edge as a constant (16, the
-// edge of every grid of 16^3 and up) or 0 (read per box).
+// tile plus a halo, then flushed to the grid with global reductions.  The
+// halo holds every stencil of a particle inside the tile, the interlaced
+// grid's half-cell shift included: S = T + 3 cells on y and z from the origin
+// T t - 1 for CIC and TSC, S = T + 4 from T t - 2 for PCS; on x the rows start
+// 4 cells below the tile (T t - 4, a multiple of
+// 4) and are W = T + 8 cells wide, so that the flush reads and reduces four
+// cells at a time (16-byte shared loads, one float4 global reduction per
+// non-zero group; 16-byte aligned because M, the row start and the grid base
+// are multiples of 4).  Stencils that leave the halo (a particle outside its
+// tile after the drift) go straight to the grid with float atomics.
+//
+// Fixed point.  Shared-memory int32 atomicAdd runs at ~8 per clock per SM on
+// B200, float atomicAdd at ~2.5 (measured), and the deposit issues 27 (TSC)
+// per particle and grid.  So the tile accumulates integers in units u of the
+// source: every partial sum of a cell is bounded by Q = wmax sum_tile |q|
+// (wmax the stencil's largest weight product), and u = max(Q / 2^29,
+// wmax max|q| / 2^22) keeps every sum below 2^30 and every contribution below
+// 2^22, where x + 1.5 2^23 rounds it to the nearest integer in the float's
+// bits (an FMA and an integer subtract per contribution, no float-to-int
+// conversion).  Each contribution is rounded to u / 2 at most: relative to
+// the tile's bound that is 2^-30 (2^-23 of one particle's full weight in a
+// sparse tile), below the FP32 sums' own rounding of the densest cells.
+// Integer sums do not depend on the order of the atomics, so a tile's
+// values are reproducible.  TT: the tile edge as a constant (16, the edge of
+// every grid of 16^3 and up) or 0 (read per box).
 // 512 threads, 2 blocks per SM (the 69 KB tile allows 3 of 256): 32 warps
-// per SM hide more of the shared-memory atomics' latency (2.38 -> 2.30 ms at
-// 2x224^3)
+// per SM hide more of the shared-memory atomics' latency.
 template <int ORDER, int NG, int TT>
 __global__ void __launch_bounds__(512, 2)
 k_b_deposit(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ boxes,
             const int64_t* __restrict__ tprefix, int nbox, int src)
 {
-    extern __shared__ float4 tile4[];
-    float* tile = reinterpret_cast<float*>(tile4);
+    extern __shared__ int4 tile4[];
+    int* tile = reinterpret_cast<int*>(tile4);
     const int64_t q = blockIdx.x;
     const int b = jt_find(tprefix, nbox, q);
     const jt_box_dev& B = boxes[b];
     if (src && !B.rho_s) return;   // the unsigned source of an unscreened box: not used
     const uint32_t t = (uint32_t)(q - tprefix[b]);
     const int T = TT > 0 ? TT : B.T, M = B.M;
-    const int S = T + 3, W = T + 8, W4 = W / 4;
+    constexpr int kLo = ORDER == 4 ? 2 : 1;   // halo below the tile on y and z
+    const int S = T + 2 + kLo, W = T + 8, W4 = W / 4;
     const int SW = S * W;
     const int ax = (int)compact3(t) * T - 4;
-    const int by = (int)compact3(t >> 1) * T - 1;
-    const int bz = (int)compact3(t >> 2) * T - 1;
+    const int by = (int)compact3(t >> 1) * T - kLo;
+    const int bz = (int)compact3(t >> 2) * T - kLo;
     const int4 r = B.ranges[t];
     const int n0 = r.y - r.x, n1 = r.w - r.z;
     if (n0 + n1 == 0) return;   // an empty tile adds nothing (whole block)
     const int nq = NG * S * S * W4;
-    for (int c = threadIdx.x; c < nq; c += blockDim.x) tile4[c] = make_float4(0.f, 0.f, 0.f, 0.f);
-    __syncthreads();
+    for (int c = threadIdx.x; c < nq; c += blockDim.x) tile4[c] = make_int4(0, 0, 0, 0);
     const int mask = M - 1;
     const int64_t G = (int64_t)M * M * M;
     const float halfL = B.halfL, hinv = B.h_inv;
     const float inv_vol = hinv * hinv * hinv;
     const float q0 = B.mass[0] * inv_vol, q1 = (src ? B.mass[1] : -B.mass[1]) * inv_vol;
+    // the tile's fixed-point unit (see above)
+    const float wmax = ORDER == 2 ? 1.0f : (ORDER == 3 ? 0.421875f : 0.2962963f);   // (3/4)^3, (2/3)^3
+    const float qa0 = fabsf(q0), qa1 = fabsf(q1);
+    const float bound = wmax * ((float)n0 * qa0 + (float)n1 * qa1);
+    const float qmax = wmax * fmaxf(n0 ? qa0 : 0.0f, n1 ? qa1 : 0.0f);
+    const float unit = fmaxf(bound * 0x1p-29f, qmax * 0x1p-22f);
+    if (!(unit > 0.0f)) return;   // massless particles add nothing (whole block)
+    const float inv_unit = 1.0f / unit;
+    const float qs0 = q0 * inv_unit, qs1 = q1 * inv_unit;
     const float4* pos0 = B.seg[0] >= 0 ? segs[B.seg[0]].pos : nullptr;
     const float4* pos1 = B.seg[1] >= 0 ? segs[B.seg[1]].pos : nullptr;
     float* rho = src ? B.rho_s : B.rho;
+    constexpr float kRound = 12582912.0f;   // 1.5 * 2^23: x + kRound holds round(x) in its low bits
+    constexpr int kRoundBits = 0x4B400000;
+    __syncthreads();
     for (int k = threadIdx.x; k < n0 + n1; k += blockDim.x) {
         float4 p;
-        float qq;
-        if (k < n0) { p = pos0[r.x + k]; qq = q0; } else { p = pos1[r.z + k - n0]; qq = q1; }
+        float qq, qg;
+        if (k < n0) { p = pos0[r.x + k]; qq = qs0; qg = q0; } else { p = pos1[r.z + k - n0]; qq = qs1; qg = q1; }
         float gx = (p.x + halfL) * hinv, gy = (p.y + halfL) * hinv, gz = (p.z + halfL) * hinv;
 #pragma unroll
         for (int g = 0; g < NG; g++) {
@@ -227,15 +252,16 @@ k_b_deposit(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ 
             bool inside = lx >= 0 && ly >= 0 && lz >= 0 && lx + ORDER <= W && ly + ORDER <= S &&
                           lz + ORDER <= S;
             if (inside) {
-                float* tb_ = tile + g * S * SW;
+                int* tb_ = tile + g * S * SW;
 #pragma unroll
                 for (int c = 0; c < ORDER; c++)
 #pragma unroll
                     for (int bb = 0; bb < ORDER; bb++) {
                         float wyz = qq * wz[c] * wy[bb];
-                        float* row = tb_ + (lz + c) * SW + (ly + bb) * W + lx;
+                        int* row = tb_ + (lz + c) * SW + (ly + bb) * W + lx;
 #pragma unroll
-                        for (int a = 0; a < ORDER; a++) atomicAdd(row + a, wyz * wx[a]);
+                        for (int a = 0; a < ORDER; a++)
+                            atomicAdd(row + a, __float_as_int(fmaf(wyz, wx[a], kRound)) - kRoundBits);
                     }
             } else {
                 float* gb = rho + g * G;
@@ -243,7 +269,7 @@ k_b_deposit(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ 
                 for (int c = 0; c < ORDER; c++)
 #pragma unroll
                     for (int bb = 0; bb < ORDER; bb++) {
-                        float wyz = qq * wz[c] * wy[bb];
+                        float wyz = qg * wz[c] * wy[bb];
                         int64_t row = ((int64_t)((iz + c) & mask) * M + ((iy + bb) & mask)) * M;
 #pragma unroll
                         for (int a = 0; a < ORDER; a++) atomicAdd(gb + row + ((ix + a) & mask), wyz * wx[a]);
@@ -253,13 +279,14 @@ k_b_deposit(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ 
     }
     __syncthreads();
     for (int c = threadIdx.x; c < nq; c += blockDim.x) {
-        const float4 v = tile4[c];
-        if (v.x == 0.0f && v.y == 0.0f && v.z == 0.0f && v.w == 0.0f) continue;
+        const int4 v = tile4[c];
+        if ((v.x | v.y | v.z | v.w) == 0) continue;
         const int qx = c % W4, row = c / W4;
         const int ly = row % S, gz = row / S;
         const int lz = gz % S, g = gz / S;
         const int64_t idx = ((int64_t)((bz + lz) & mask) * M + ((by + ly) & mask)) * M + ((ax + 4 * qx) & mask);
-        atomicAdd(reinterpret_cast<float4*>(rho + g * G + idx), v);
+        atomicAdd(reinterpret_cast<float4*>(rho + g * G + idx),
+                  make_float4((float)v.x * unit, (float)v.y * unit, (float)v.z * unit, (float)v.w * unit));
     }
 }
 
@@ -380,17 +407,13 @@ int jt_b_deposit(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int6
                  int nbox, int64_t ntiles, int order, int ngrid, int T, cudaStream_t st, int src, bool T16)
 {
     if (ntiles <= 0) return JT_OK;
-    int S = T + 3, W = T + 8;
+    int S = T + (order == 4 ? 4 : 3), W = T + 8;
     size_t smem = sizeof(float) * (size_t)ngrid * S * S * W;
     // T16: every box of the pass has the tile edge 16 (T is the largest)
 #define JT_BDEP1(O, NG, TT)                                                                   \
     do {                                                                                      \
-        static bool attr = false;                                                             \
-        if (!attr) {                                                                          \
-            cudaFuncSetAttribute(k_b_deposit<O, NG, TT>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                 96 * 1024);                                                  \
-            attr = true;                                                                      \
-        }                                                                                     \
+        if (jt_smem_attr((const void*)k_b_deposit<O, NG, TT>, 96 * 1024) != JT_OK)            \
+            return JT_ECUDA;                                                                  \
         k_b_deposit<O, NG, TT><<<(unsigned)ntiles, 512, smem, st>>>(d_segs, d_boxes, d_tprefix, nbox, src); \
     } while (0)
 #define JT_BDEP(O, NG)                    \
@@ -402,6 +425,8 @@ int jt_b_deposit(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int6
     else if (order == 2 && ngrid == 2) JT_BDEP(2, 2);
     else if (order == 3 && ngrid == 1) JT_BDEP(3, 1);
     else if (order == 3 && ngrid == 2) JT_BDEP(3, 2);
+    else if (order == 4 && ngrid == 1) JT_BDEP(4, 1);
+    else if (order == 4 && ngrid == 2) JT_BDEP(4, 2);
     else return JT_EINVAL;
 #undef JT_BDEP
 #undef JT_BDEP1

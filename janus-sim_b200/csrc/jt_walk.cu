@@ -101,19 +101,36 @@ __device__ __forceinline__ float gap1(float d, float ext)
     return g > 0.0f ? g : 0.0f;
 }
 
-// Tabulated short-range factor for pair interactions (JT_WALK_STAB = 1):
-// S as a function of y = x^2 = (r^2 + eps^2) / (2 r_s)^2 on a uniform grid
-// of kStab points over [0, 16] (x <= 4; S(4) ~ 5e-7), each entry holding
-// (S(y_i), S(y_{i+1}) - S(y_i)) for linear interpolation.  It replaces the
-// exp and reciprocal of the closed form (two MUFU operations per pair) by
-// one L1-resident float2 load; interpolation error <= 3e-5 near y = 0 and
-// ~1e-6 elsewhere.  Filled once per device from the host's erfc and exp.
-#ifndef JT_WALK_STAB
-#define JT_WALK_STAB 1
-#endif
-constexpr int kStab = JT_STAB_N;
-constexpr float kStabYMax = 16.0f;
-__device__ float2 g_stab[kStab];
+// Pair forces of both walks read a log-indexed table of the split kernel,
+// G(y) = S(sqrt y) / y^{3/2} with y = (r_p / 2 r_s)^2 (JT_LTAB_N entries,
+// jt_internal.cuh): the force of a pair is s_i s_j m_j c^3 G(y) d,
+// c = 1 / (2 r_s).  One L1-resident float2 load and one FMA replace the
+// reciprocal square root, the exp and the reciprocal of the closed form.
+// Filled once per device from the host's erfc and exp.
+// the cell walk's log-indexed table of G(y) = S(sqrt y) / y^{3/2}
+__device__ float2 g_ltab[JT_LTAB_N];
+
+// Fill a log-indexed table of G(y) = S(sqrt y) / y^{3/2} (JT_LTAB_N entries):
+// octave e = -32..5, segment k = 0..511 covers [2^e (1 + k/512),
+// 2^e (1 + (k+1)/512)); entry (a, b) is the chord through G at its two
+// ends, so that G ~ a + b y inside it (relative error <= (h / y)^2 / 8 times
+// y^2 |G''| / G: about 2e-6 where G ~ y^{-3/2}, up to ~2e-5 at y ~ 5 where S
+// falls off as e^{-y}).  The last entry is the one every y >= 64 (and every
+// y < 2^-32, through the unsigned index wrap) is clamped to: S ~ 1e-28 there.
+template <class F>
+void fill_log_table(F S, float2* tab)
+{
+    for (int e = -32; e < 6; e++) {
+        const double base = std::ldexp(1.0, e), h = base / 512.0;
+        for (int k = 0; k < 512; k++) {
+            const double y0 = base + k * h, y1 = y0 + h;
+            const double g0 = S(y0) / (y0 * std::sqrt(y0)), g1 = S(y1) / (y1 * std::sqrt(y1));
+            const double b = (g1 - g0) / h, a = g0 - b * y0;
+            tab[(e + 32) * 512 + k] = make_float2((float)a, (float)b);
+        }
+    }
+    tab[JT_LTAB_N - 1] = make_float2(0.f, 0.f);
+}
 
 struct WalkArgs {
     const jt_seg_dev* segs;
@@ -224,17 +241,11 @@ __device__ __forceinline__ int eval_chunk(WalkWarpSmem& S, int cnt, int lane, fl
         const float r2 = dx * dx + dy * dy + dz * dz;
         if (r2 > 0.0f && r2 < P.rc2) {   // not the target itself; inside the cut
             hits++;
-            const float rp2 = r2 + P.eps2;
-            const float ri = rsqrtf(rp2);
-#if JT_WALK_STAB
-            const float t = fminf(rp2 * P.c2s, (float)kStab - 1.5f);   // y / dy
-            const int k = (int)t;
+            // fac carries s_i s_j m_j c^3: the force is fac G(y) d
+            const float y = (r2 + P.eps2) * P.c2;
+            const unsigned k = min((__float_as_uint(y) >> 14) - JT_LTAB_BASE, (unsigned)JT_LTAB_N - 1u);
             const float2 ab = __ldg(&tab[k]);
-            const float S = fmaf(ab.y, t - (float)k, ab.x);
-#else
-            const float S = jt_split_S(rp2 * ri * P.c);
-#endif
-            const float g = fac * S * ri * ri * ri;
+            const float g = fac * fmaf(ab.y, y, ab.x);
             a.x += g * dx;
             a.y += g * dy;
             a.z += g * dz;
@@ -399,9 +410,10 @@ __device__ __forceinline__ void walk_trees(const WalkArgs& A, const jt_box_dev& 
         const int roff = (int)(TS.tree.range - A.pool.range);
         const float4* __restrict__ tpos = TS.pos;
         const float sgn = (s == t) ? 1.0f : -1.0f;
-        const float fac_direct = sgn * (t == 0 ? P.mass[0] : P.mass[1]);   // no dynamic index into a local array
+        // no dynamic index into a local array (P.mass carries the table's c^3)
+        const float fac_direct = sgn * (t == 0 ? P.mass[0] : P.mass[1]);
         const bool yuk = SCR && s != t && B.ytab != nullptr;
-        const float2* __restrict__ tab = yuk ? B.ytab : g_stab;
+        const float2* __restrict__ tab = yuk ? B.ytab : g_ltab;
         const float theta2 = yuk ? 0.0f : P.theta2;
         const int leaf0 = nt - 1;
         int sp = 1, nR = 0, nA = 0, nc = 0;
@@ -612,8 +624,10 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_walk_acc(WalkArgs A)
     const int s = SG.species;
     jt_walk_params P;
     P.L = B.L; P.halfL = B.halfL; P.theta2 = B.theta2; P.rc2 = B.rc2; P.rc = sqrtf(B.rc2);
-    P.eps2 = B.eps2; P.c = B.c; P.mass[0] = B.mass[0]; P.mass[1] = B.mass[1];
-    P.c2s = B.c * B.c * ((float)kStab / kStabYMax);
+    P.eps2 = B.eps2; P.c = B.c;
+    P.c2 = B.c * B.c;
+    // particle masses times c^3, the scale of the pair table's G(y)
+    P.mass[0] = B.mass[0] * P.c2 * B.c; P.mass[1] = B.mass[1] * P.c2 * B.c;
     // candidate prefilter margins: 8 ulp of the largest coordinate on the
     // box, 1e-5 relative on the cut
     P.slack = B.halfL * 9.5367431640625e-7f;
@@ -948,27 +962,23 @@ __global__ void k_split_signed(const float* __restrict__ pos, const float* __res
 
 namespace {
 
-// Fill g_stab on the current device once (host double erfc/exp).
+// Fill g_ltab on the current device once (host double erfc/exp).
 int stab_ready()
 {
-#if JT_WALK_STAB
+    static std::mutex mu;
     static bool done[64] = {};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return JT_ECUDA;
+    std::lock_guard<std::mutex> lock(mu);
     if (done[dev]) return JT_OK;
-    std::vector<float2> tab(kStab);
-    const double dy = (double)kStabYMax / kStab;
     auto S = [](double y) {
         const double x = std::sqrt(y);
         return std::erfc(x) + 1.1283791670955126 * x * std::exp(-y);
     };
-    for (int i = 0; i < kStab; i++) {
-        const double a = S(i * dy), b = S((i + 1) * dy);
-        tab[i] = make_float2((float)a, (float)(b - a));
-    }
-    if (cudaMemcpyToSymbol(g_stab, tab.data(), sizeof(float2) * kStab) != cudaSuccess) return JT_ECUDA;
+    std::vector<float2> lt(JT_LTAB_N);
+    fill_log_table(S, lt.data());
+    if (cudaMemcpyToSymbol(g_ltab, lt.data(), sizeof(float2) * JT_LTAB_N) != cudaSuccess) return JT_ECUDA;
     done[dev] = true;
-#endif
     return JT_OK;
 }
 
@@ -980,7 +990,7 @@ namespace {
 // The default launch shape of the walk (80 registers, 6 blocks per SM,
 // 32-particle leaf buckets) is the best measured at 2x224^3; other densities,
 // clustering and box mixes can prefer another register budget or bucket.  For
-// the default PM scheme (TSC, interlaced) the first force-only pass of each
+// the default PM scheme (PCS, interlaced) the first force-only pass of each
 // size class (device, log2 of the warp-group count) times every variant once
 // and keeps the fastest; JT_WALK_VARIANT=<k> pins variant k.  Passes that kick
 // (the walk then updates velocities) or run under stream capture use the
@@ -994,12 +1004,13 @@ constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 std::mutex g_tune_mu;
 std::map<std::pair<int, int>, int> g_tuned;   // (device, log2 groups) -> variant
 
+// the variants of the default PM scheme (PCS, interlaced)
 void launch_variant(int v, unsigned g, const WalkArgs& A, cudaStream_t st)
 {
     switch (v) {
-    case 1: k_walk_acc<3, 2, 5, 32, false><<<g, kWarps * 32, 0, st>>>(A); break;
-    case 2: k_walk_acc<3, 2, 6, 24, false><<<g, kWarps * 32, 0, st>>>(A); break;
-    default: k_walk_acc<3, 2, 6, 32, false><<<g, kWarps * 32, 0, st>>>(A); break;
+    case 1: k_walk_acc<4, 2, 5, 32, false><<<g, kWarps * 32, 0, st>>>(A); break;
+    case 2: k_walk_acc<4, 2, 6, 24, false><<<g, kWarps * 32, 0, st>>>(A); break;
+    default: k_walk_acc<4, 2, 6, 32, false><<<g, kWarps * 32, 0, st>>>(A); break;
     }
 }
 
@@ -1089,9 +1100,6 @@ namespace {
 // (the uniform case); cells whose neighbourhood holds more than
 // JT_CELL_KMAX candidates (clustered data) flag their particles for the
 // tree walk, which keeps its multipoles there.
-#ifndef JT_CELL_KMAX
-#define JT_CELL_KMAX 2048
-#endif
 
 struct CellArgs {
     const jt_seg_dev* segs;
@@ -1235,12 +1243,15 @@ struct CellWarpSmem {
 };
 
 // dense evaluation of candidates [0, cnt) for this lane's target: every pair
-// computed, the force selected by 0 < r^2 < r_cut^2 (an invalid target slot
-// counts no pair; its result is not written).
+// computed, the force selected by r^2 < r_cut^2.  Per pair: y = (r^2 + eps^2)
+// c^2 indexes the log table by its float bits and G(y) = a + b y (no
+// reciprocal square root, no float-int conversion); the lane accumulates
+// q_j G(y) d, which the caller scales by s_i c^3.  The target itself (r = 0,
+// d = 0) adds nothing and is counted as a hit, which the caller removes.
 // SCR: opposite-species pairs read the box's Yukawa table yt.
 template <bool SCR>
 __device__ __forceinline__ unsigned cell_chunk(const float4* __restrict__ cand, int cnt, const float4& p, float si,
-                                               bool valid, float rc2, float eps2, float c2s, Acc3& a,
+                                               float rc2, float c2, float ye, Acc3& a,
                                                const float2* __restrict__ yt)
 {
     unsigned hits = 0;
@@ -1248,20 +1259,17 @@ __device__ __forceinline__ unsigned cell_chunk(const float4* __restrict__ cand, 
     for (int j = 0; j < cnt; j++) {
         const float4 q = cand[j];
         const float dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
-        const float r2 = dx * dx + dy * dy + dz * dz;
-        const bool in = valid && r2 > 0.0f && r2 < rc2;
-        const float rp2 = r2 + eps2;
-        const float ri = rsqrtf(rp2);
-        const float t = fminf(rp2 * c2s, (float)kStab - 1.5f);   // NaN -> the bound
-        const int k = max((int)t, 0);
-        const float2* __restrict__ tb = (SCR && si * q.w < 0.0f) ? yt : g_stab;
+        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+        const float y = fmaf(r2, c2, ye);
+        const unsigned k = min((__float_as_uint(y) >> 14) - JT_LTAB_BASE, (unsigned)JT_LTAB_N - 1u);
+        const float2* __restrict__ tb = (SCR && si * q.w < 0.0f) ? yt : g_ltab;
         const float2 ab = __ldg(&tb[k]);
-        const float S = fmaf(ab.y, t - (float)k, ab.x);
-        const float g = in ? si * q.w * S * ri * ri * ri : 0.0f;
+        const bool in = r2 < rc2;
+        const float w = in ? q.w * fmaf(ab.y, y, ab.x) : 0.0f;
         hits += in ? 1u : 0u;
-        a.x += g * dx;
-        a.y += g * dy;
-        a.z += g * dz;
+        a.x = fmaf(w, dx, a.x);
+        a.y = fmaf(w, dy, a.y);
+        a.z = fmaf(w, dz, a.z);
     }
     return hits;
 }
@@ -1275,9 +1283,9 @@ __device__ __forceinline__ void cell_batch(const CellArgs& A, const jt_box_dev& 
                                            int t1, int lane, unsigned& pairs, unsigned& cands)
 {
     const unsigned lt = (1u << lane) - 1u;
-    const float rc2 = B.rc2, eps2 = B.eps2, c2s = B.c * B.c * ((float)kStab / kStabYMax);
+    const float rc2 = B.rc2, c2 = B.c * B.c, ye = B.eps2 * c2;
     const float slack = B.halfL * 9.5367431640625e-7f, rc2_keep = B.rc2 * 1.00001f;
-    const float2* __restrict__ yt = (SCR && B.ytab) ? B.ytab : g_stab;
+    const float2* __restrict__ yt = (SCR && B.ytab) ? B.ytab : g_ltab;
     const int t = base + lane;
     const bool valid = t < t1;
     const float4 p = A.cb.cpos[valid ? t : base];
@@ -1290,6 +1298,7 @@ __device__ __forceinline__ void cell_batch(const CellArgs& A, const jt_box_dev& 
                 ghz = 0.5f * (hiz - loz) + slack;
     Acc3 near = {0.f, 0.f, 0.f};
     if (A.parts & 2) {
+        unsigned hits = 0;
         int nc = 0;
         for (int nbr = 0; nbr < 27; nbr++) {
             const int2 r = S.nrange[nbr];
@@ -1310,7 +1319,7 @@ __device__ __forceinline__ void cell_batch(const CellArgs& A, const jt_box_dev& 
                 nc += __popc(km);
                 __syncwarp();
                 if (nc >= 32) {
-                    pairs += cell_chunk<SCR>(S.cand, 32, p, si, valid, rc2, eps2, c2s, near, yt);
+                    hits += cell_chunk<SCR>(S.cand, 32, p, si, rc2, c2, ye, near, yt);
                     cands += 32;
                     __syncwarp();
                     const float4 t2 = S.cand[32 + lane];
@@ -1322,10 +1331,16 @@ __device__ __forceinline__ void cell_batch(const CellArgs& A, const jt_box_dev& 
             }
         }
         if (nc > 0) {
-            pairs += cell_chunk<SCR>(S.cand, nc, p, si, valid, rc2, eps2, c2s, near, yt);
+            hits += cell_chunk<SCR>(S.cand, nc, p, si, rc2, c2, ye, near, yt);
             cands += nc;
         }
         __syncwarp();
+        // the target met itself once (r = 0 < r_cut); an empty slot counts nothing
+        if (valid) pairs += hits - 1u;
+        const float sc = si * c2 * B.c;
+        near.x *= sc;
+        near.y *= sc;
+        near.z *= sc;
     }
     if (valid) {
         Acc3 pm = {0.f, 0.f, 0.f};
@@ -1392,7 +1407,7 @@ __global__ void __launch_bounds__(kWarps * 32, JT_CELL_MINB) k_walk_cell(CellArg
     int tot = cnt;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
-    if (tot > JT_CELL_KMAX) {   // clustered: the tree walk takes these targets
+    if (tot > B.cell_kmax) {   // clustered: the tree walk takes these targets
         for (int t = t0 + lane; t < t1; t += 32) {
             const int2 id = A.cb.cid[t];
             A.cb.tflag[A.pprefix[id.x] + id.y] = 1;
@@ -1461,7 +1476,9 @@ int jt_b_cells(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_
         if (screened) k_walk_cell<O, N, true><<<gw, kWarps * 32, 0, st>>>(A, ncells);  \
         else k_walk_cell<O, N, false><<<gw, kWarps * 32, 0, st>>>(A, ncells);          \
     } while (0)
-        if (order == 3 && ngrid == 2) JT_CELL_LAUNCH(3, 2);
+        if (order == 4 && ngrid == 2) JT_CELL_LAUNCH(4, 2);
+        else if (order == 4 && ngrid == 1) JT_CELL_LAUNCH(4, 1);
+        else if (order == 3 && ngrid == 2) JT_CELL_LAUNCH(3, 2);
         else if (order == 3 && ngrid == 1) JT_CELL_LAUNCH(3, 1);
         else if (order == 2 && ngrid == 2) JT_CELL_LAUNCH(2, 2);
         else if (order == 2 && ngrid == 1) JT_CELL_LAUNCH(2, 1);
@@ -1494,12 +1511,16 @@ int jt_b_walk(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t
     A.segflag = tflag ? segflag : nullptr;
     unsigned g = (unsigned)((ngroups + kWarps - 1) / kWarps);
     if (screened) {
-        if (order == 3 && ngrid == 2) k_walk_acc<3, 2, 6, 32, true><<<g, kWarps * 32, 0, st>>>(A);
+        if (order == 4 && ngrid == 2) k_walk_acc<4, 2, 6, 32, true><<<g, kWarps * 32, 0, st>>>(A);
+        else if (order == 4 && ngrid == 1) k_walk_acc<4, 1, 6, 32, true><<<g, kWarps * 32, 0, st>>>(A);
+        else if (order == 3 && ngrid == 2) k_walk_acc<3, 2, 6, 32, true><<<g, kWarps * 32, 0, st>>>(A);
         else if (order == 3 && ngrid == 1) k_walk_acc<3, 1, 6, 32, true><<<g, kWarps * 32, 0, st>>>(A);
         else if (order == 2 && ngrid == 2) k_walk_acc<2, 2, 6, 32, true><<<g, kWarps * 32, 0, st>>>(A);
         else if (order == 2 && ngrid == 1) k_walk_acc<2, 1, 6, 32, true><<<g, kWarps * 32, 0, st>>>(A);
         else return JT_EINVAL;
-    } else if (order == 3 && ngrid == 2) launch_variant(pick_variant(g, ngroups, A, st), g, A, st);
+    } else if (order == 4 && ngrid == 2) launch_variant(pick_variant(g, ngroups, A, st), g, A, st);
+    else if (order == 4 && ngrid == 1) k_walk_acc<4, 1, 6, 32, false><<<g, kWarps * 32, 0, st>>>(A);
+    else if (order == 3 && ngrid == 2) k_walk_acc<3, 2, 6, 32, false><<<g, kWarps * 32, 0, st>>>(A);
     else if (order == 3 && ngrid == 1) k_walk_acc<3, 1, 6, 32, false><<<g, kWarps * 32, 0, st>>>(A);
     else if (order == 2 && ngrid == 2) k_walk_acc<2, 2, 6, 32, false><<<g, kWarps * 32, 0, st>>>(A);
     else if (order == 2 && ngrid == 1) k_walk_acc<2, 1, 6, 32, false><<<g, kWarps * 32, 0, st>>>(A);
@@ -1701,31 +1722,34 @@ void jt_b_drift(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64
     k_b_drift<<<(unsigned)((ntotal + 255) / 256), 256, 0, st>>>(d_segs, d_boxes, d_prefix, nseg, frac);
 }
 
-// S_Y(x; b), x = r_p / (2 r_s), b = kappa r_s: r_p^2 times the force of the
-// short part of the Yukawa split, (1 / 2r) [e^{-kr} erfc(x - b) + e^{kr}
-// erfc(x + b)] with kr = 2 b x:
+namespace {
+
+// S_Y(x; b), x = r_p / (2 r_s), b = kappa r_s, as a function of y = x^2:
+// r_p^2 times the force of the short part of the Yukawa split,
+// (1 / 2r) [e^{-kr} erfc(x - b) + e^{kr} erfc(x + b)] with kr = 2 b x:
 //   S_Y = (Em Cm + Ep Cp) / 2 + b x (Em Cm - Ep Cp) + (2x / sqrt(pi)) e^{-x^2 - b^2},
 //   Em = e^{-2bx}, Cm = erfc(x - b), Ep = e^{2bx}, Cp = erfc(x + b);
 // b = 0 gives erfc(x) + (2x / sqrt(pi)) e^{-x^2}.  Ep Cp = e^{-x^2 - b^2}
 // erfcx(x + b) is taken from its asymptotic series where erfc underflows.
-void jt_yukawa_table(double b, float2* tab)
+double yukawa_S(double b, double y)
 {
-    const double dy = (double)kStabYMax / kStab;
-    auto S = [b](double y) {
-        const double x = std::sqrt(y);
-        const double em = std::exp(-2.0 * b * x), cm = std::erfc(x - b);
-        const double u = x + b;
-        double epcp;
-        if (u < 25.0) {
-            epcp = std::exp(2.0 * b * x) * std::erfc(u);
-        } else {
-            const double iu2 = 1.0 / (u * u);
-            epcp = std::exp(-x * x - b * b) / (u * 1.7724538509055159) * (1.0 - 0.5 * iu2 + 0.75 * iu2 * iu2);
-        }
-        return 0.5 * (em * cm + epcp) + b * x * (em * cm - epcp) + 1.1283791670955126 * x * std::exp(-x * x - b * b);
-    };
-    for (int i = 0; i < kStab; i++) {
-        const double a = S(i * dy), c = S((i + 1) * dy);
-        tab[i] = make_float2((float)a, (float)(c - a));
+    const double x = std::sqrt(y);
+    const double em = std::exp(-2.0 * b * x), cm = std::erfc(x - b);
+    const double u = x + b;
+    double epcp;
+    if (u < 25.0) {
+        epcp = std::exp(2.0 * b * x) * std::erfc(u);
+    } else {
+        const double iu2 = 1.0 / (u * u);
+        epcp = std::exp(-x * x - b * b) / (u * 1.7724538509055159) * (1.0 - 0.5 * iu2 + 0.75 * iu2 * iu2);
     }
+    return 0.5 * (em * cm + epcp) + b * x * (em * cm - epcp) + 1.1283791670955126 * x * std::exp(-x * x - b * b);
 }
+
+}  // namespace
+
+void jt_yukawa_log_table(double b, float2* tab)
+{
+    fill_log_table([b](double y) { return yukawa_S(b, y); }, tab);
+}
+

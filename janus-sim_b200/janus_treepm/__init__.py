@@ -51,7 +51,10 @@ EXPORTED = [
     "jt_energy_sampled", "jt_virialize_sampled", "jt_energy_drift_pct",
     "jt_batch_checkpoint_async", "jt_batch_checkpoint_wait", "jt_snapshot_write_raw",
     "jt_snapshot_read_raw", "jt_set_accel", "jt_get_accel", "jt_server_get_accel",
-    "jt_batch_set_screening", "jt_step_host", "jt_batch_prepare",
+    "jt_batch_set_screening", "jt_step_host", "jt_batch_prepare", "jt_config_short_cut",
+    "jt_expansion_create", "jt_expansion_destroy", "jt_expansion_info", "jt_expansion_at_time",
+    "jt_expansion_at_redshift", "jt_expansion_state_at_mu", "jt_expansion_calibrate",
+    "jt_expansion_phi_factors",
 ]
 JT_JOB_QUEUED, JT_JOB_RESIDENT, JT_JOB_DONE = 0, 1, 2
 JT_STATIC_SORT_MAX = 262144
@@ -70,7 +73,7 @@ class jt_config(C.Structure):
         ("softening", C.c_double), ("r_s", C.c_double), ("r_cut", C.c_double),
         ("mu", C.c_double), ("G_mass_plus", C.c_double), ("k_min", C.c_int),
         ("mode", C.c_int), ("integrator", C.c_int), ("pm_order", C.c_int),
-        ("pm_interlace", C.c_int), ("reserved", C.c_int * 3),
+        ("pm_interlace", C.c_int), ("cut_tail_ppm", C.c_int), ("reserved", C.c_int * 2),
     ]
 
 
@@ -83,6 +86,20 @@ class jt_timings(C.Structure):
         ("pair_interactions", C.c_int64), ("node_interactions", C.c_int64),
         ("candidates", C.c_int64), ("cellwalk_ms", C.c_double),
     ]
+
+
+class jt_expansion_state(C.Structure):
+    _fields_ = [("mu", C.c_double), ("a_plus", C.c_double), ("t_gyr", C.c_double),
+                ("h_plus", C.c_double), ("z", C.c_double)]
+
+    def to_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class jt_expansion_info_t(C.Structure):
+    _fields_ = [("alpha", C.c_double), ("mu_0", C.c_double), ("a_0", C.c_double), ("z_max", C.c_double),
+                ("z_init", C.c_double), ("t_start", C.c_double), ("t_end", C.c_double),
+                ("n_points", C.c_int64)]
 
 
 class jt_step_args(C.Structure):
@@ -251,6 +268,18 @@ def library():
     L.jt_strerror.argtypes = [C.c_int]
     L.jt_strerror.restype = C.c_char_p
     L.jt_fp32_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
+    L.jt_config_short_cut.argtypes = [C.POINTER(jt_config), C.POINTER(C.c_double)]
+    dp_ = C.POINTER(C.c_double)
+    L.jt_expansion_create.argtypes = [C.c_double, C.c_int, C.POINTER(H)]
+    L.jt_expansion_destroy.argtypes = [H]
+    L.jt_expansion_destroy.restype = None
+    L.jt_expansion_info.argtypes = [H, C.POINTER(jt_expansion_info_t)]
+    L.jt_expansion_at_time.argtypes = [H, C.c_double, C.POINTER(jt_expansion_state)]
+    L.jt_expansion_at_redshift.argtypes = [H, C.c_double, C.POINTER(jt_expansion_state)]
+    L.jt_expansion_state_at_mu.argtypes = [C.c_double, C.c_double, C.c_double,
+                                           C.POINTER(jt_expansion_state)]
+    L.jt_expansion_calibrate.argtypes = [dp_, dp_]
+    L.jt_expansion_phi_factors.argtypes = [C.c_double, C.c_double, dp_, dp_, dp_]
     L.jt_walk_counters.argtypes = [H, C.POINTER(C.c_int64)]
     L.jt_version.argtypes = []
     L.jt_version.restype = C.c_char_p
@@ -323,7 +352,7 @@ def library():
     for name in EXPORTED:
         if name not in ("jt_destroy", "jt_strerror", "jt_version", "jt_batch_destroy",
                         "jt_server_destroy", "jt_server_clock", "jt_philox4x32_10",
-                        "jt_energy_drift_pct"):
+                        "jt_energy_drift_pct", "jt_expansion_destroy"):
             getattr(L, name).restype = C.c_int
     _lib = L
     return L
@@ -366,8 +395,9 @@ class Config:
     k_min: int = 0
     mode: int = JT_ACCURATE
     integrator: int = JT_KDK
-    pm_order: int = 0           # 0 -> TSC (accurate); 2 CIC; 3 TSC
+    pm_order: int = 0           # 0 -> PCS (accurate); 2 CIC; 3 TSC; 4 PCS
     pm_interlace: int = 0       # 0 -> on (accurate); 1 on; 2 off
+    cut_tail_ppm: int = 0       # > 0: widen the short-range cut until S = ppm * 1e-6
 
     def resolved(self):
         c = Config(**self.__dict__)
@@ -384,6 +414,7 @@ class Config:
         s.r_s, s.r_cut, s.mu, s.G_mass_plus = c.r_s, c.r_cut, c.mu, c.G_mass_plus
         s.k_min, s.mode, s.integrator = c.k_min, c.mode, c.integrator
         s.pm_order, s.pm_interlace = c.pm_order, c.pm_interlace
+        s.cut_tail_ppm = c.cut_tail_ppm
         return s
 
 
@@ -1007,6 +1038,15 @@ class TreePMForce:
 
 def version():
     return library().jt_version().decode()
+
+
+def short_cut(config):
+    """The short-range cut the engine uses for this Config (r_cut, widened by
+    cut_tail_ppm in accurate mode)."""
+    c = config.to_c()
+    v = C.c_double()
+    _check(library().jt_config_short_cut(C.byref(c), C.byref(v)), "jt_config_short_cut")
+    return v.value
 
 
 def fp32_peak_tflops(iters=4096):

@@ -13,7 +13,8 @@
  *     interpolation smoothing;
  *   - the gradient is spectral (-i k phi); modes on a Nyquist plane are
  *     dropped (their weight is exp(-(pi r_s / h)^2), ~2e-7 at r_s = 1.25 h);
- *   - assignment of order 2 (CIC) or 3 (TSC, deconvolved by sinc^6 per axis);
+ *   - assignment of order 2 (CIC), 3 (TSC, deconvolved by sinc^6 per axis)
+ *     or 4 (PCS, the cubic B-spline, sinc^8);
  *   - optional interlacing: a second grid with nodes half a cell higher on
  *     every axis, the spectra averaged with the phase of that shift, the
  *     force interpolated from both grids and averaged.
@@ -26,13 +27,22 @@
 #include <stdio.h>
 
 /* stencil along one axis at grid coordinate g: first node and weights
- * (order 2 CIC: floor(g), +1; order 3 TSC: nearest node c, c-1..c+1) */
+ * (order 2 CIC: floor(g), +1; order 3 TSC: nearest node c, c-1..c+1;
+ * order 4 PCS, the cubic B-spline: f = floor(g), nodes f-1..f+2) */
 static int stencil(double g, int order, double* w)
 {
     if (order == 2) {
         double f0 = floor(g), f = g - f0;
         w[0] = 1.0 - f; w[1] = f;
         return (int)f0;
+    }
+    if (order == 4) {
+        double f0 = floor(g), t = g - f0, s = 1.0 - t;
+        w[0] = s * s * s / 6.0;
+        w[1] = 2.0 / 3.0 - t * t + 0.5 * t * t * t;
+        w[2] = 2.0 / 3.0 - s * s + 0.5 * s * s * s;
+        w[3] = t * t * t / 6.0;
+        return (int)f0 - 1;
     }
     double c = floor(g + 0.5), d = g - c;
     w[0] = 0.5 * (0.5 - d) * (0.5 - d);
@@ -46,7 +56,7 @@ static void deposit(const double* pos, const double* mass, const int8_t* signs,
 {
     double half = box / 2.0, h = box / M, inv_vol = 1.0 / (h * h * h);
     for (int64_t t = 0; t < n; t++) {
-        double w[3][3];
+        double w[3][4];
         int i0[3];
         for (int d = 0; d < 3; d++) i0[d] = stencil((pos[3 * t + d] + half) / h - shift, order, w[d]);
         double q = (double)signs[t] * mass[t] * inv_vol;
@@ -134,7 +144,7 @@ void orc_acc_pm_forces2(const double* pos, const double* mass, const int8_t* sig
     for (int64_t t = 0; t < n; t++) {
         double a[3] = {0, 0, 0};
         for (int b = 0; b < ngrid; b++) {
-            double w[3][3];
+            double w[3][4];
             int i0[3];
             for (int d = 0; d < 3; d++) i0[d] = stencil((pos[3 * t + d] + half) / h - 0.5 * b, order, w[d]);
             for (int c = 0; c < order; c++)

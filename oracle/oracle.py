@@ -72,6 +72,50 @@ def lib():
     return _lib
 
 
+_gpu = None
+
+
+def gpu_lib():
+    """The FP64 periodic force oracle on the GPU (oracle/libewald_gpu.so,
+    `make -C oracle gpu`): production-size accuracy checks."""
+    global _gpu
+    if _gpu is None:
+        path = os.path.join(HERE, "libewald_gpu.so")
+        if not os.path.exists(path):
+            raise RuntimeError("GPU oracle not built: run `make -C oracle gpu`")
+        G = C.CDLL(path)
+        u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+        G.oge_periodic_forces.argtypes = [f32p, u8p, I64, F64, F64, i64p, I64, F64, F64, F64, F64,
+                                          F64, F64, f64p, f64p]
+        G.oge_periodic_forces.restype = C.c_int
+        _gpu = G
+    return _gpu
+
+
+def periodic_forces_gpu(pos_p, pos_m, m_plus, m_minus, idx, box, eps, r_e, r_s, r_cut,
+                        kcut_tol=1e-12):
+    """FP64 accelerations of targets idx (rows of [pos_p ; pos_m]) on the GPU.
+
+    Returns (full, split): `full` the periodic sum with Plummer softening
+    (Ewald, wide split r_e, real space within 11 r_e < L/2), `split` the
+    truncated split model at r_s / r_cut (= ewald_forces(r_s, eps,
+    r_trunc=r_cut)).  Positions are the engine's FP32 inputs, taken exactly."""
+    pos = np.ascontiguousarray(np.concatenate([np.asarray(pos_p, np.float32).reshape(-1, 3),
+                                               np.asarray(pos_m, np.float32).reshape(-1, 3)]))
+    n_p = len(np.asarray(pos_p).reshape(-1, 3))
+    sp = np.zeros(len(pos), np.uint8)
+    sp[n_p:] = 1
+    idx = _c(idx, np.int64)
+    full = np.zeros((len(idx), 3), np.float64)
+    split = np.zeros((len(idx), 3), np.float64)
+    r = gpu_lib().oge_periodic_forces(pos.ravel(), sp, len(pos), float(m_plus), -float(m_minus), idx,
+                                      len(idx), box, eps, r_e, r_s, r_cut, kcut_tol, full.ravel(),
+                                      split.ravel())
+    if r != 0:
+        raise RuntimeError(f"oge_periodic_forces failed: {r}")
+    return full, split
+
+
 def ref_available():
     return os.path.exists(os.path.join(HERE, "_ref", "libref_twopass.so"))
 

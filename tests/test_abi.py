@@ -42,8 +42,10 @@ def test_python_binding_covers_the_header():
 def test_struct_layouts_match_header():
     import janus_treepm as J
     # jt_config (include/janus_treepm.h): box_L 0, pm_grid 8, theta 16 ... G_mass_plus 56,
-    # k_min 64, mode 68, integrator 72, pm_order 76, pm_interlace 80, reserved 84..96
+    # k_min 64, mode 68, integrator 72, pm_order 76, pm_interlace 80, cut_tail_ppm 84,
+    # reserved 88..96
     assert C.sizeof(J.jt_config) == 96
+    assert J.jt_config.cut_tail_ppm.offset == 84
     assert J.jt_config.G_mass_plus.offset == 56 and J.jt_config.k_min.offset == 64
     assert J.jt_config.pm_order.offset == J.jt_config.integrator.offset + 4
     # 8 doubles, 5 int64 counters, cellwalk_ms
@@ -64,7 +66,9 @@ def test_strerror_and_version():
 @pytest.mark.parametrize("field,value", [("box_L", -1.0), ("pm_grid", 48), ("pm_grid", 2048),
                                          ("theta", -0.1), ("r_cut", 40.0), ("r_s", 0.0),
                                          ("G_mass_plus", 0.0), ("mode", 7), ("integrator", 9),
-                                         ("pm_order", 4), ("pm_interlace", 3), ("k_min", -1)])
+                                         ("pm_order", 5), ("pm_order", 1), ("pm_interlace", 3),
+                                         ("k_min", -1), ("cut_tail_ppm", -1),
+                                         ("cut_tail_ppm", 1000000)])
 def test_invalid_config_is_rejected_before_device_work(field, value):
     import janus_treepm as J
     cfg = J.Config(box_L=64.0, pm_grid=64).to_c()

@@ -11,7 +11,8 @@ r_s = 1.25 cells, r_cut = 4.5 r_s and softening in a box half the side:
   the same truncated split kernel (oracle/ewald.c, part "short"), for
   theta = 0.3, 0.5, 0.7: the Barnes-Hut + FP32 error;
 * long range (JT_PART_PM) against the FP64 restatement of the same PM scheme
-  (oracle/acc_pm.c, TSC with interlacing): the FP32 error of the PM path.
+  (oracle/acc_pm.c, PCS with interlacing, the default): the FP32 error of
+  the PM path.
 
 Errors are |a - a_ref| / |a_total| per target, a_total = FP64 short + FP64
 PM.  Bars: p99 <= 1e-3 for the PM path and for the walk at theta <= 0.5;
@@ -51,7 +52,7 @@ def test_clustered_accuracy_theta_sweep():
     O, J, pp, pm, pos, mass, sg, idx, r_s, eps, n = _setup()
     r_cut = 4.5 * r_s
     short_ref = O.ewald_forces(pos, mass, sg, L, r_s, eps, r_trunc=r_cut, idx=idx, part="short")
-    pm_ref = O.acc_pm_forces(pos, mass, sg, M, L, r_s, order=3, interlace=True)[idx]
+    pm_ref = O.acc_pm_forces(pos, mass, sg, M, L, r_s, order=4, interlace=True)[idx]
     tot = np.linalg.norm(short_ref + pm_ref, axis=1)
     report = {}
     for theta in (0.3, 0.5, 0.7):

@@ -8,7 +8,7 @@ Bars:
     reference's GPU forces: p99 relative error <= 1e-5 (the engine evaluates
     the same float expressions; the PM runs in FP32 where the reference runs
     FP64, and CUDA's erfcf differs from the host's by an ulp);
-  * accurate-mode accelerations (TSC + interlacing, the default) against the
+  * accurate-mode accelerations (PCS + interlacing, the default) against the
     FP64 exact split-model sum (same r_s, softening and r_cut, no grid, no
     tree): median <= 2e-4 and p99 <= 3e-3 at theta = 0.5 (the remaining error
     is the PM grid's; measured p50 8e-5, p99 1.3e-3 at 2x32^3 particles);
@@ -296,3 +296,52 @@ def test_twopass_mirror_energy_screening_and_segregation():
     alpha = sim.virialize_sampled(1000)
     _, v2, _ = sim.get_particles()
     assert np.allclose(v2, vel * np.float32(alpha), rtol=1e-6, atol=0)
+
+
+@pytest.mark.parametrize("k_min", [2, 3])
+def test_kmin_filter_both_modes(k_min):
+    """The k_min filter (cuda/cufft_wrapper.cu:196-203: modes with
+    max(|kx|, |ky|, |kz|) < k_min zeroed) on the device, in both modes, on the
+    long-range part alone (JT_PART_PM): compatibility mode against the
+    restatement of the reference's PM (p99 <= 1e-5), accurate mode against
+    the FP64 PM of the same scheme (PCS, interlaced; p99 <= 1e-4 of the
+    unfiltered force's rms).  The filter must also change the force: without
+    it the result differs."""
+    J, O = _mods()
+    L, M, n = 48.0, 32, 3000
+    pos = _uniform(n, L, 41)
+    rng = np.random.default_rng(42)
+    sg = np.where(rng.random(n) < 0.5, 1, -1).astype(np.int8)
+    theta, eps, r_cut, mf = 0.5, 0.05, 4.5 * 1.25 * L / M, 0.01
+    # compatibility mode: the reference's Green's function with the filter
+    s = J.Solver(J.Config(box_L=L, pm_grid=M, theta=theta, softening=eps, r_s=r_cut / 3, r_cut=r_cut,
+                          mu=(sg < 0).sum() / (sg > 0).sum(), G_mass_plus=mf, k_min=k_min,
+                          mode=J.JT_RCOMPAT))
+    s.set_state_signed(pos, None, sg)
+    got = s.accel_part(J.JT_PART_PM)
+    s.close()
+    got = np.concatenate(got) if isinstance(got, tuple) else got
+    pp, pm = pos[sg > 0], pos[sg < 0]
+    ref = O.ref_pm_forces(pos, sg, M, L, mf, r_cut, k_min=k_min)
+    ref = np.concatenate([ref[sg > 0], ref[sg < 0]])
+    unf = O.ref_pm_forces(pos, sg, M, L, mf, r_cut, k_min=0)
+    unf = np.concatenate([unf[sg > 0], unf[sg < 0]])
+    rel = _rel(got, ref)
+    assert np.percentile(rel, 99) <= 1e-5, np.percentile(rel, [50, 99, 100])
+    assert np.percentile(_rel(unf, ref), 50) > 1e-3   # the filter changes the force
+    # accurate mode: FP64 PM of the same scheme with the same filter
+    r_s = 1.25 * L / M
+    mass = np.concatenate([np.full(len(pp), 1.0), np.full(len(pm), 19.0 * len(pp) / len(pm))])
+    s = J.Solver(J.Config(box_L=L, pm_grid=M, theta=theta, softening=eps, r_s=r_s, r_cut=4.5 * r_s,
+                          mu=19.0, G_mass_plus=1.0, k_min=k_min, mode=J.JT_ACCURATE))
+    s.set_state(pp, None, pm, None)
+    a = np.concatenate(s.accel_part(J.JT_PART_PM)).astype(np.float64)
+    s.close()
+    p64 = np.concatenate([pp, pm]).astype(np.float64)
+    s64 = np.concatenate([np.ones(len(pp), np.int8), -np.ones(len(pm), np.int8)])
+    ex = O.acc_pm_forces(p64, mass, s64, M, L, r_s, k_min=k_min, order=4, interlace=True)
+    ex0 = O.acc_pm_forces(p64, mass, s64, M, L, r_s, k_min=0, order=4, interlace=True)
+    rms = np.sqrt(np.mean(np.sum(ex0 ** 2, axis=1)))
+    d = np.linalg.norm(a - ex, axis=1) / rms
+    assert np.percentile(d, 99) <= 1e-4, np.percentile(d, [50, 99, 100])
+    assert np.percentile(np.linalg.norm(ex0 - ex, axis=1) / rms, 50) > 1e-3

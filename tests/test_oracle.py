@@ -306,10 +306,12 @@ def test_ewald_close_pair_is_newtonian():
 
 
 @pytest.mark.parametrize("order,interlace,p50_max", [(2, False, 2.5e-2), (2, True, 6e-3),
-                                                     (3, False, 4e-3), (3, True, 5e-4)])
+                                                     (3, False, 4e-3), (3, True, 5e-4),
+                                                     (4, False, 3e-3), (4, True, 1e-4)])
 def test_acc_pm_against_long_range_ewald(order, interlace, p50_max):
     """PM force errors against the exact long-range (Ewald reciprocal) sum at
-    r_s = 1.25 cells: CIC ~1e-2, TSC + interlacing ~2e-4 (median)."""
+    r_s = 1.25 cells: CIC ~1e-2, TSC + interlacing ~2e-4, PCS + interlacing
+    ~3e-5 (median)."""
     rng = np.random.default_rng(8)
     L, M, n = 16.0, 32, 300
     pos = (rng.random((n, 3)) - 0.5) * L
