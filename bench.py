@@ -181,6 +181,44 @@ def reference_gpu_step(n_side, grid, steps=3):
         return {"error": str(e)[:300]}
 
 
+def run_clustered(J, ics, steps, warmup, H, dt, cut_tail_ppm=0, theta=0.5):
+    """The clustered workload: 2x128^3 particles, 80 % in 512 Plummer spheres
+    (scale radii log-uniform 0.05-1 Mpc, species alternating by sphere) + 20 %
+    uniform background, L = 100 Mpc, PM 256^3, theta 0.5, mu 19, r_s = 1.25
+    cells, cut 4.5 r_s (or widened by cut_tail_ppm), softening spacing/30.
+    Most cells are too crowded for the cell walk, so the LBVH build and the
+    Barnes-Hut group walk (multipoles) do the near field.  Device time of K
+    KDK steps after W warm-up steps; the tree walk's FP32 roofline beside it."""
+    n_side, L, M = 128, 100.0, 256
+    n = n_side ** 3
+    r_s = 1.25 * L / M
+    pp, pm = ics.plummer_spheres(n, L, n_spheres=512, seed=42)
+    cfg = J.Config(box_L=L, pm_grid=M, theta=theta, softening=(L / (2 * n) ** (1 / 3)) / 30, r_s=r_s,
+                   r_cut=4.5 * r_s, mu=19.0, G_mass_plus=1.0e-3, cut_tail_ppm=cut_tail_ppm)
+    s = J.Solver(cfg)
+    s.set_state(pp, None, pm, None)
+    for _ in range(warmup):
+        s.step(dt, H, 1.0, 1)
+    dev, stages = 0.0, {}
+    for _ in range(steps):
+        s.step(dt, H, 1.0, 1)
+        tm = s.timings()
+        dev += tm["total_ms"]
+        for k, v in tm.items():
+            stages[k] = stages.get(k, 0.0) + v
+    s.close()
+    walk_ms = stages["walk_ms"] / steps - stages.get("interp_ms", 0.0) / steps
+    flops = (stages["pair_interactions"] * FLOPS_PAIR + stages["node_interactions"] * FLOPS_NODE) / steps
+    return {"workload": f"2x{n_side}^3 in 512 Plummer spheres + 20 % background, L={L:g} Mpc, PM {M}^3, "
+                        f"theta {theta}, mu 19, cut {J.short_cut(cfg) / r_s:.3g} r_s",
+            "value": 2 * n * steps / (dev * 1e-3), "unit": UNIT, "ms_per_step": dev / steps,
+            "stages_ms_per_step": {k: round(v / steps, 4) for k, v in stages.items() if k.endswith("_ms")},
+            "pairs_per_step": stages["pair_interactions"] / steps,
+            "nodes_per_step": stages["node_interactions"] / steps,
+            "walk_tflops": flops / (walk_ms * 1e-3) / 1e12 if walk_ms > 0 else None,
+            "steps": steps, "warmup": warmup}
+
+
 def ensemble_boxes(n_boxes=64, seed=7):
     """The batched-ensemble workload: n_boxes independent boxes, n per species
     log-uniform in [16, 96] (N = n^3 per species), L ~ U(50, 300) Mpc, PM grid
@@ -378,7 +416,10 @@ def run_serving(J, ics, n_small, n_big, steps, rates, H, dt, budget_gb=150.0):
     out["saturated_vs_plain"] = (total_ps / wall) / (total_ps / plain_s)
     out["saturated_swaps_trims"] = [int(st["swapped_out"]), int(st["trims"])]
     out["saturated_host_s"] = {"admit": st["admit_s"], "evict": st["evict_s"], "steps": st["busy_s"],
-                               "wall": wall}
+                               "steps_device": st["step_device_s"], "wall": wall,
+                               "batched_steps": int(st["batched_steps"]),
+                               "max_jobs_per_step": int(st["max_jobs_per_step"]),
+                               "reserved_gb": st["reserved_gb"]}
     for frac in rates:
         wall, st = serve_once(J, jobs, steps, frac * cap, H, dt, budget_gb, seed=12)
         out["runs"].append({
@@ -391,7 +432,7 @@ def run_serving(J, ics, n_small, n_big, steps, rates, H, dt, budget_gb=150.0):
             "max_jobs_per_step": int(st["max_jobs_per_step"]),
             "admission_waits": int(st["admission_waits"]), "swapped_out": int(st["swapped_out"]),
             "trims": int(st["trims"]), "admit_s": st["admit_s"], "evict_s": st["evict_s"],
-            "peak_device_gb": st["peak_device_bytes"] / 1e9})
+            "steps_device_s": st["step_device_s"], "peak_device_gb": st["peak_device_bytes"] / 1e9})
     return out
 
 
@@ -542,18 +583,13 @@ def run_ours(args, ws, rank, local):
     e2e = ws * 2 * n * K / e2e_t
     bytes_state = 2 * n * 3 * 4 * 3     # positions, velocities, accelerations; both species
 
-    # the PM interpolation alone: the cell walk with the pair loop off
-    # (JT_PART_PM).  Algorithmic bytes: positions in (16 B) and accelerations
-    # out (16 B) per particle, and every value of the 3 x NG force grids read
-    # once (the targets come in cell order, so the stencils' reuse stays in
-    # L1/L2)
-    interp_ms = []
-    for _ in range(3):
-        s.accel_part(J.JT_PART_PM)
-        interp_ms.append(s.timings()["cellwalk_ms"])
-    interp_ms = float(np.median(interp_ms))
+    # the PM interpolation (k_b_interp, timed alone by its own events inside
+    # the step).  Algorithmic bytes: positions in (16 B) and one float4 per
+    # particle and interlaced grid out, and every value of the 3 x NG force
+    # grids read once (tiles staged in shared memory)
+    interp_ms = stages.get("interp_ms", 0.0) / K
     G = w["M"] ** 3
-    interp_bytes = 32.0 * 2 * n + 4.0 * 3 * 2 * G
+    interp_bytes = 16.0 * 2 * n + 16.0 * 2 * 2 * n + 4.0 * 3 * 2 * G
 
     # roofline of the dominant kernel: the near-field cell walk (FP32 pipe),
     # timed alone by its own events (the walk stage also holds the cell list
@@ -588,6 +624,11 @@ def run_ours(args, ws, rank, local):
         ref_gpu = reference_gpu_step(args.n_side, args.grid)
     ensemble = None
     serving = None
+    clustered = None
+    if rank == 0 and ws == 1 and args.clustered_steps > 0:
+        clustered = run_clustered(J, ics, args.clustered_steps, 3, H, w["dt"], args.cut_tail_ppm)
+        if clustered.get("walk_tflops"):
+            clustered["walk_frac_fp32"] = clustered["walk_tflops"] / peak_fp32
     if rank == 0 and ws == 1 and args.ensemble_boxes > 0:
         ensemble = run_ensemble(J, ics, args.ensemble_boxes, args.ensemble_steps, 3, H, w["dt"])
         if args.serve_jobs > 0:
@@ -621,7 +662,7 @@ def run_ours(args, ws, rank, local):
                                  "frac": (16.0 * 2 * n + 4.0 * 2 * G) / (stages["deposit_ms"] / K * 1e-3) / 1e9
                                  / hbm_peak,
                                  "peak_source": hbm_src},
-            "roofline_interp": {"bound": "hbm", "kernel": "k_walk_cell (JT_PART_PM: interpolation only)",
+            "roofline_interp": {"bound": "hbm", "kernel": "k_b_interp (tiled PM interpolation)",
                                 "ms": interp_ms, "bytes": interp_bytes,
                                 "achieved": interp_bytes / (interp_ms * 1e-3) / 1e9 if interp_ms > 0 else None,
                                 "peak": hbm_peak, "unit": "GB/s",
@@ -635,6 +676,7 @@ def run_ours(args, ws, rank, local):
             "walk_autotune": J.walk_tuning(),
             "cpu_baseline": cpu,
             "reference_gpu": ref_gpu,
+            "clustered": clustered,
             "ensemble": ensemble,
             "serving": serving,
         }
@@ -661,6 +703,8 @@ def main():
     ap.add_argument("--serve-big", type=int, default=8)
     ap.add_argument("--serve-steps", type=int, default=4)
     ap.add_argument("--serve-rates", default="0.5,1.0")
+    ap.add_argument("--clustered-steps", type=int, default=5,
+                    help="steps of the clustered workload leg (0: skip)")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip the reference's own GPU step (oracle/refgpu) beside the CPU baseline")
     ap.add_argument("--no-full-reference-step", action="store_true",

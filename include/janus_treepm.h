@@ -123,6 +123,7 @@ typedef struct jt_timings {
     int64_t node_interactions;  /* multipole node interactions */
     int64_t candidates;         /* particle candidates distance-tested */
     double cellwalk_ms;  /* the near-field cell walk kernel alone (part of walk_ms) */
+    double interp_ms;    /* the tiled PM interpolation kernel alone (part of walk_ms) */
 } jt_timings;
 
 /* Create a handle on the current CUDA device.  Replaces the constructor and
@@ -477,12 +478,18 @@ typedef struct jt_serve_stats {
     int64_t trims;             /* scratch pools released to make room */
     double  admit_s;           /* wall time admitting jobs (state to the device) */
     double  evict_s;           /* wall time evicting and swapping out jobs (to host) */
+    double  step_device_s;     /* device time of the batched steps (CUDA events) */
+    double  reserved_gb;       /* memory the server's pool holds from creation (GB) */
 } jt_serve_stats;
 
 #define JT_JOB_QUEUED    0
 #define JT_JOB_RESIDENT  1
 #define JT_JOB_DONE      2
 
+/* The server reserves its budget (at most 90 % of the device's free memory)
+ * in its memory pool at creation, so that admissions and the batched steps'
+ * scratch are carved from memory already mapped, not grown by the driver
+ * while requests wait. */
 int  jt_server_create(size_t hbm_budget_bytes, jt_server** out);
 void jt_server_destroy(jt_server* s);
 /* Register a job (host arrays copied to pinned memory; nothing on the device

@@ -836,6 +836,7 @@ int jt_step(jt_handle* h, double dt, double hubble, double dtau_per_dt, int nste
         acc_tm.pair_interactions += t.pair_interactions; acc_tm.node_interactions += t.node_interactions;
         acc_tm.candidates += t.candidates;
         acc_tm.cellwalk_ms += t.cellwalk_ms;
+        acc_tm.interp_ms += t.interp_ms;
     };
     if (c.integrator == JT_KDK) {
         // RCOMPAT kick-drift-kick (the accurate handle went through the batch)

@@ -197,6 +197,7 @@ struct jt_batch {
     Pool<int> ccount, cstart, cbsum, ccell, csegflag;
     Pool<unsigned> cslot;
     Pool<float4> cpos;
+    Pool<float4> pmacc;                 // PM accelerations of the pass, per interlaced grid
     Pool<int2> cid;
     Pool<unsigned char> tflag;
     Pool<float4> com, bmin, bmax, quad0;
@@ -209,7 +210,7 @@ struct jt_batch {
     std::map<int, Bucket> buckets;
     unsigned* d_err = nullptr;
     unsigned long long* d_stats = nullptr;
-    cudaEvent_t ev[10] = {};            // 8, 9: around the cell walk kernel
+    cudaEvent_t ev[11] = {};            // 8, 9: around the cell walk kernel; 6-10: interpolation
     bool pending = false;               // a pass's events await jtb_finish
     jt_timings tm = {};
     int64_t phase[4] = {0, 0, 0, 0};
@@ -602,6 +603,7 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
         JT_TRY(B->tflag.ensure((size_t)std::max<int64_t>(P.npart, 1), &grew));
         JT_TRY(B->csegflag.ensure((size_t)std::max<int>(nseg, 1), &grew));
     }
+    if (!P.screened) JT_TRY(B->pmacc.ensure((size_t)B->ngrid * std::max<int64_t>(P.npart, 1), &grew));
 
     if (grew) B->gen++;
     std::vector<unsigned char> buf;
@@ -676,6 +678,16 @@ int force_pass(jt_batch* B, Plan& P, int parts, float kick_frac)
         JT_TRY(exec_c2r(K, 3 * B->ngrid * kv.second));
     }
     cudaEventRecord(B->ev[6], st);
+    // PM interpolation of every particle from shared-memory tiles (a pass with
+    // a screened box interpolates inside the walks: it has two sets of grids)
+    const float4* pmacc = nullptr;
+    if (!P.screened && (parts & JT_PART_PM) && P.npart > 0) {
+        JT_TRY(jt_b_interp(P.d_post, P.d_bx, P.d_ptp, P.d_pp, nbox, P.npmtiles, B->order, B->ngrid, P.maxT,
+                           P.npart, B->pmacc.p, st, t16));
+        pmacc = B->pmacc.p;
+        B->tm.launches += 1;
+    }
+    cudaEventRecord(B->ev[10], st);
     jt_tree_dev pool = {};
     pool.child = B->child.p;
     pool.range = B->range.p;
@@ -696,14 +708,14 @@ int force_pass(jt_batch* B, Plan& P, int parts, float kick_frac)
                            B->cpos.p, B->cid.p, B->tflag.p, B->csegflag.p};
         JT_TRY(jt_b_cells(P.d_post, P.d_bx, P.d_pp, nseg, P.npart, P.d_cp, nbox, P.ncells, cb, B->order,
                           B->ngrid, parts, kick_frac, B->d_stats, B->d_err, st, B->ev[8], B->ev[9],
-                          P.screened));
+                          P.screened, pmacc));
         tflag = B->tflag.p;
         jt_b_build_trees(P.d_post, P.d_bx, nseg, P.d_ip, P.ninternal, P.d_pp, P.npart, st, B->csegflag.p);
         B->tm.launches += P.npart > 0 ? (P.ncells > 0 ? 6 : 1) : 0;
     }
     JT_TRY(jt_b_walk(P.d_post, P.d_bx, P.d_gp, nseg, P.ngroups, pool, B->order, B->ngrid, parts,
                      kick_frac, B->d_stats, B->d_err, st, P.d_pp, tflag, P.screened,
-                     tflag ? B->csegflag.p : nullptr));
+                     tflag ? B->csegflag.p : nullptr, pmacc, P.npart));
     cudaEventRecord(B->ev[7], st);
     B->pending = true;
     B->tm.launches += (P.npart > 0 ? 8 : 0) + (P.ninternal > 0 ? 1 : 0) + (P.npart > 0 ? 1 : 0) +
@@ -747,6 +759,7 @@ int finish(jt_batch* B)
         B->tm.kspace_ms += elapsed(B->ev[4], B->ev[5]);
         B->tm.walk_ms += elapsed(B->ev[6], B->ev[7]);
         B->tm.cellwalk_ms += elapsed(B->ev[8], B->ev[9]);
+        B->tm.interp_ms += elapsed(B->ev[6], B->ev[10]);
         B->pending = false;
     }
     B->tm.pair_interactions += (int64_t)v[0];
@@ -1168,7 +1181,7 @@ void jt_batch_destroy(jt_batch* B)
     B->com.release(); B->bmin.release(); B->bmax.release(); B->quad0.release(); B->quad1.release();
     B->ccount.release(); B->cstart.release(); B->cbsum.release(); B->ccell.release(); B->cslot.release();
     B->csegflag.release();
-    B->cpos.release(); B->cid.release(); B->tflag.release();
+    B->cpos.release(); B->cid.release(); B->tflag.release(); B->pmacc.release();
     B->m30.release(); B->vals.release(); B->vals_alt.release(); B->keys_alt.release();
     B->hist.release(); B->status.release(); B->tickets.release(); B->desc.release();
     drop_graphs(B);
@@ -1471,7 +1484,11 @@ int jt_batch_estimate(const jt_config* cfg, size_t n_p, size_t n_m, size_t* pers
         size_t tree = 2 * n * (sizeof(int2) + sizeof(int) + 4 * sizeof(float4) + sizeof(float2)) +
                       n * (sizeof(int2) + sizeof(int));
         size_t sort = n * 4 * sizeof(uint32_t) + (n / 4096 + 2) * 4 * 256 * sizeof(uint32_t);
-        *scratch = tree + sort + grid_bytes(M, box_ngrid(*cfg));
+        // near-field cell list (cpos, cid, ccell, cslot, tflag per particle)
+        // and the interpolated PM accelerations (one float4 per grid)
+        size_t cells = n * (sizeof(float4) + sizeof(int2) + 2 * sizeof(int) + 1) +
+                       n * box_ngrid(*cfg) * sizeof(float4);
+        *scratch = tree + sort + cells + grid_bytes(M, box_ngrid(*cfg));
     }
     return JT_OK;
 }
@@ -1494,7 +1511,7 @@ int jt_batch_trim(jt_batch* B)
     B->com.release(); B->bmin.release(); B->bmax.release(); B->quad0.release(); B->quad1.release();
     B->ccount.release(); B->cstart.release(); B->cbsum.release(); B->ccell.release(); B->cslot.release();
     B->csegflag.release();
-    B->cpos.release(); B->cid.release(); B->tflag.release();
+    B->cpos.release(); B->cid.release(); B->tflag.release(); B->pmacc.release();
     B->m30.release(); B->vals.release(); B->vals_alt.release(); B->keys_alt.release();
     B->hist.release(); B->status.release(); B->tickets.release();
     for (auto& kv : B->buckets) kv.second.release();
@@ -1518,3 +1535,17 @@ int jt_batch_get_timings(jt_batch* B, jt_timings* t)
 }
 
 }  // extern "C"
+
+int jtb_reserve(jt_batch* B, size_t bytes)
+{
+    if (!B) return JT_EINVAL;
+    if (bytes == 0) return JT_OK;
+    void* p = nullptr;
+    if (cudaMallocFromPoolAsync(&p, bytes, B->actx.pool, B->st) != cudaSuccess) {
+        cudaGetLastError();
+        return JT_ENOMEM;
+    }
+    JT_CU(cudaFreeAsync(p, B->st));
+    JT_CU(cudaStreamSynchronize(B->st));
+    return JT_OK;
+}

@@ -60,6 +60,9 @@ int jth_info(jt_handle* h, jt_config* cfg, float* m_plus, float* m_minus, int8_t
 int jt_diag_state(const float4* const pos[2], const float4* const vel[2], const int64_t n[2],
                   const float mass[2], double L, int n_cells, cudaStream_t st, jt_diag* out);
 int jtb_set_accel(jt_batch* B, int box_id, const float* acc_p, const float* acc_m, int mem);
+// Map `bytes` of device memory into the batch's pool (one allocation, freed
+// at once: the pool keeps it) so that later allocations need no new mapping.
+int jtb_reserve(jt_batch* B, size_t bytes);
 // One KDK step of one box whose state the host holds between steps: the
 // caller-order host arrays (pos, vel, acc per species; pinned for full
 // speed) are uploaded into the box (which takes the caller's order), the box

@@ -291,6 +291,13 @@ int jt_b_deposit(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int6
                  bool T16 = false);
 void jt_b_kspace(const jt_box_dev* d_boxes, const int64_t* d_kprefix, int nbox, int64_t nmodes,
                  int interlace, int k_min, cudaStream_t st);
+// PM interpolation of every particle of the pass from each interlaced grid
+// (tiles staged in shared memory): pmacc[b * npart + i], i = pprefix[seg] +
+// index, the force of grid b on a unit m+ particle.  T: the largest tile edge
+// of the pass (every box's T <= it; region (T + 4)^3 x 3 floats).
+int jt_b_interp(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_tprefix,
+                const int64_t* d_pprefix, int nbox, int64_t ntiles, int order, int ngrid, int T,
+                int64_t npart, float4* pmacc, cudaStream_t st, bool T16 = false);
 
 // walk (jt_walk.cu)
 struct jt_walk_params {
@@ -318,7 +325,8 @@ int jt_b_walk(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t
               int64_t ngroups, const jt_tree_dev& pool, int order, int ngrid, int parts,
               float kick_frac, unsigned long long* stats, unsigned* d_err, cudaStream_t st,
               const int64_t* d_pprefix = nullptr, const unsigned char* tflag = nullptr,
-              bool screened = false, const int* segflag = nullptr);
+              bool screened = false, const int* segflag = nullptr, const float4* pmacc = nullptr,
+              int64_t npart = 0);
 // Near-field cell list of a pass (cells of side >= r_cut, both species) and
 // the cell walk over it: particles of cells whose 27-cell neighbourhood holds
 // more than JT_CELL_KMAX candidates, and of boxes without a cell grid, are
@@ -334,7 +342,7 @@ int jt_b_cells(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_
                int64_t npart, const int64_t* d_cprefix, int nbox, int64_t ncells, const jt_cell_bufs& cb,
                int order, int ngrid, int parts, float kick_frac, unsigned long long* stats,
                unsigned* d_err, cudaStream_t st, cudaEvent_t ev_walk0, cudaEvent_t ev_walk1,
-               bool screened = false);
+               bool screened = false, const float4* pmacc = nullptr);
 int jt_cell_scan_blocks(int64_t ncells);
 // Yukawa split factor S_Y(y) on the walk's table grid (y = (r_p / 2 r_s)^2
 // over [0, 16], JT_STAB_N (value, next - value) entries) for b = kappa r_s.

@@ -74,6 +74,8 @@ struct jt_server {
     double busy_s = 0.0;
     size_t peak_device = 0;
     double admit_s = 0.0, evict_s = 0.0;   // wall time in admissions / evictions
+    double step_device_s = 0.0;            // device time of the batched steps
+    size_t reserved = 0;                   // bytes reserved in the batch's pool at creation
     int max_resident = 0;
     std::set<int> prepared;        // grid sizes whose cuFFT plans the batch holds (jt_batch_prepare)
 };
@@ -169,7 +171,10 @@ int trim(jt_server* S)
 {
     S->trims++;
     S->prepared.clear();   // the trim releases the plans too
-    return jt_batch_trim(S->B);
+    int r = jt_batch_trim(S->B);
+    // map the reservation again (the trim returned it to the device)
+    if (r == JT_OK && S->reserved) jtb_reserve(S->B, S->reserved);
+    return r;
 }
 
 bool fits(jt_server* S, const Job& j)
@@ -253,6 +258,10 @@ int step_once(jt_server* S, int* served)
     if (r != JT_OK) return r;
     const double done = now_s();
     S->busy_s += done - a;
+    {
+        jt_timings t;
+        if (jt_batch_get_timings(S->B, &t) == JT_OK) S->step_device_s += 1e-3 * t.total_ms;
+    }
     S->steps++;
     S->max_resident = std::max(S->max_resident, (int)ids.size());
     size_t free_b = 0, total_b = 0;
@@ -304,6 +313,12 @@ int jt_server_create(size_t hbm_budget_bytes, jt_server** out)
         return r;
     }
     S->budget = hbm_budget_bytes;
+    // map the budget once, up front (see the header)
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+        const size_t want = std::min(hbm_budget_bytes, free_b / 10 * 9);
+        if (jtb_reserve(S->B, want) == JT_OK) S->reserved = want;
+    }
     S->t0 = now_s();
     *out = S;
     return JT_OK;
@@ -484,6 +499,8 @@ int jt_server_stats(jt_server* S, jt_serve_stats* out)
     s.max_jobs_per_step = S->max_resident;
     s.swapped_out = S->swapped;
     s.trims = S->trims;
+    s.step_device_s = S->step_device_s;
+    s.reserved_gb = 1e-9 * (double)S->reserved;
     *out = s;
     return JT_OK;
 }

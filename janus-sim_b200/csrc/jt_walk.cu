@@ -144,9 +144,11 @@ struct WalkArgs {
                               // of each box's dt (0 = none)
     unsigned long long* stats;
     unsigned* err;
-    const int64_t* pprefix;       // particles per segment (with tflag)
+    const int64_t* pprefix;       // particles per segment
     const unsigned char* tflag;   // non-null: only flagged particles are computed here
     const int* segflag;           // with tflag: per segment, some particle is flagged
+    const float4* pmacc;          // non-null: PM accelerations of the pass (jt_b_interp)
+    int64_t npart;                // particles of the pass (pmacc's grid stride)
 };
 
 // Pair interactions of this lane's target with a chunk of candidates: a
@@ -604,6 +606,22 @@ __device__ __forceinline__ Acc3 pm_interp(const jt_box_dev& B, const float4& p)
     return pm;
 }
 
+// The PM acceleration of a unit m+ particle computed by the tiled
+// interpolation kernel (jt_b_interp) for pass particle gi: the mean of the
+// interlaced grids' values.
+template <int NG>
+__device__ __forceinline__ Acc3 pm_from_tiles(const float4* __restrict__ pmacc, int64_t npart, int64_t gi)
+{
+    float4 a = pmacc[gi];
+    if (NG == 2) {
+        const float4 b = pmacc[npart + gi];
+        a.x = 0.5f * (a.x + b.x);
+        a.y = 0.5f * (a.y + b.y);
+        a.z = 0.5f * (a.z + b.z);
+    }
+    return Acc3{a.x, a.y, a.z};
+}
+
 // MINB: resident blocks per SM the register budget is sized for (6 -> 80
 // registers); BKT: nodes with <= BKT particles are streamed as ranges
 // (<= 32: one lane per particle when a range is loaded)
@@ -648,7 +666,8 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_walk_acc(WalkArgs A)
     float gcx = 0.5f * (lox + hix), gcy = 0.5f * (loy + hiy), gcz = 0.5f * (loz + hiz);
     float ghx = 0.5f * (hix - lox), ghy = 0.5f * (hiy - loy), ghz = 0.5f * (hiz - loz);
 
-    const Acc3 pm = (P.parts & 1) ? pm_interp<ORDER, NG>(B, p) : Acc3{0.f, 0.f, 0.f};
+    Acc3 pm = {0.f, 0.f, 0.f};
+    if ((P.parts & 1) && !A.pmacc) pm = pm_interp<ORDER, NG>(B, p);
 
     Acc3 near = {0.f, 0.f, 0.f}, far = {0.f, 0.f, 0.f}, comp = {0.f, 0.f, 0.f};
     unsigned pairs = 0, nodes = 0, cands = 0;   // per lane (warp totals < 2^32)
@@ -663,6 +682,7 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_walk_acc(WalkArgs A)
                                      far, comp, pairs, nodes, cands, wc);
 
     if (valid && mine) {
+        if ((P.parts & 1) && A.pmacc) pm = pm_from_tiles<NG>(A.pmacc, A.npart, A.pprefix[g] + i);
         float ax = sgn_s * pm.x + near.x + (far.x - comp.x);
         float ay = sgn_s * pm.y + near.y + (far.y - comp.y);
         float az = sgn_s * pm.z + near.z + (far.z - comp.z);
@@ -1112,6 +1132,8 @@ struct CellArgs {
     float kick_frac;
     unsigned long long* stats;
     unsigned* err;
+    const float4* pmacc;          // non-null: PM accelerations of the pass (jt_b_interp)
+    int64_t npart;
 };
 
 __device__ __forceinline__ int cell_of(float x, float halfL, float inv, int nb)
@@ -1263,9 +1285,12 @@ __device__ __forceinline__ unsigned cell_chunk(const float4* __restrict__ cand, 
         const float y = fmaf(r2, c2, ye);
         const unsigned k = min((__float_as_uint(y) >> 14) - JT_LTAB_BASE, (unsigned)JT_LTAB_N - 1u);
         const float2* __restrict__ tb = (SCR && si * q.w < 0.0f) ? yt : g_ltab;
-        const float2 ab = __ldg(&tb[k]);
         const bool in = r2 < rc2;
-        const float w = in ? q.w * fmaf(ab.y, y, ab.x) : 0.0f;
+        // only lanes inside the cut read the table (a predicated load: the
+        // ~4/5 of dense candidates outside it issue no L1 request)
+        float2 ab = make_float2(0.f, 0.f);
+        if (in) ab = __ldg(&tb[k]);
+        const float w = q.w * fmaf(ab.y, y, ab.x);
         hits += in ? 1u : 0u;
         a.x = fmaf(w, dx, a.x);
         a.y = fmaf(w, dy, a.y);
@@ -1344,7 +1369,8 @@ __device__ __forceinline__ void cell_batch(const CellArgs& A, const jt_box_dev& 
     }
     if (valid) {
         Acc3 pm = {0.f, 0.f, 0.f};
-        if (A.parts & 1) pm = pm_interp<ORDER, NG>(B, p);
+        if (A.parts & 1)
+            pm = A.pmacc ? pm_from_tiles<NG>(A.pmacc, A.npart, A.pprefix[id.x] + id.y) : pm_interp<ORDER, NG>(B, p);
         const jt_seg_dev& SG = A.segs[id.x];
         float ax = si * pm.x + near.x, ay = si * pm.y + near.y, az = si * pm.z + near.z;
         if (SCR && B.force_s && (A.parts & 1)) {
@@ -1437,7 +1463,8 @@ int jt_cell_scan_blocks(int64_t ncells) { return (int)((ncells + kScanB - 1) / k
 int jt_b_cells(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_pprefix, int nseg,
                int64_t npart, const int64_t* d_cprefix, int nbox, int64_t ncells, const jt_cell_bufs& cb,
                int order, int ngrid, int parts, float kick_frac, unsigned long long* stats,
-               unsigned* d_err, cudaStream_t st, cudaEvent_t ev_walk0, cudaEvent_t ev_walk1, bool screened)
+               unsigned* d_err, cudaStream_t st, cudaEvent_t ev_walk0, cudaEvent_t ev_walk1, bool screened,
+               const float4* pmacc)
 {
     cudaEventRecord(ev_walk0, st);   // both recorded on every path (no stale events)
     if (npart <= 0) {
@@ -1457,6 +1484,8 @@ int jt_b_cells(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_
     A.kick_frac = kick_frac;
     A.stats = stats;
     A.err = d_err;
+    A.pmacc = pmacc;
+    A.npart = npart;
     const unsigned gp = (unsigned)((npart + 255) / 256);
     if (ncells > 0 && cudaMemsetAsync(cb.ccount, 0, sizeof(int) * (size_t)ncells, st) != cudaSuccess)
         return JT_ECUDA;
@@ -1492,11 +1521,14 @@ int jt_b_cells(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_
 int jt_b_walk(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_gprefix, int nseg,
               int64_t ngroups, const jt_tree_dev& pool, int order, int ngrid, int parts,
               float kick_frac, unsigned long long* stats, unsigned* d_err, cudaStream_t st,
-              const int64_t* d_pprefix, const unsigned char* tflag, bool screened, const int* segflag)
+              const int64_t* d_pprefix, const unsigned char* tflag, bool screened, const int* segflag,
+              const float4* pmacc, int64_t npart)
 {
     if (ngroups <= 0) return JT_OK;
     if (int r = stab_ready()) return r;
     WalkArgs A;
+    A.pmacc = pmacc;
+    A.npart = npart;
     A.segs = d_segs;
     A.boxes = d_boxes;
     A.gprefix = d_gprefix;

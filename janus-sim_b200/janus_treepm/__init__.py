@@ -84,7 +84,7 @@ class jt_timings(C.Structure):
         ("kick_drift_ms", C.c_double), ("total_ms", C.c_double),
         ("interactions", C.c_int64), ("launches", C.c_int64),
         ("pair_interactions", C.c_int64), ("node_interactions", C.c_int64),
-        ("candidates", C.c_int64), ("cellwalk_ms", C.c_double),
+        ("candidates", C.c_int64), ("cellwalk_ms", C.c_double), ("interp_ms", C.c_double),
     ]
 
 
@@ -234,7 +234,7 @@ class jt_serve_stats(C.Structure):
         ("p50_latency_s", C.c_double), ("p99_latency_s", C.c_double), ("max_latency_s", C.c_double),
         ("busy_s", C.c_double), ("peak_device_bytes", C.c_int64), ("max_jobs_per_step", C.c_int64),
         ("swapped_out", C.c_int64), ("trims", C.c_int64), ("admit_s", C.c_double),
-        ("evict_s", C.c_double),
+        ("evict_s", C.c_double), ("step_device_s", C.c_double), ("reserved_gb", C.c_double),
     ]
 
 

@@ -48,9 +48,10 @@ def test_struct_layouts_match_header():
     assert J.jt_config.cut_tail_ppm.offset == 84
     assert J.jt_config.G_mass_plus.offset == 56 and J.jt_config.k_min.offset == 64
     assert J.jt_config.pm_order.offset == J.jt_config.integrator.offset + 4
-    # 8 doubles, 5 int64 counters, cellwalk_ms
-    assert C.sizeof(J.jt_timings) == 8 * 8 + 8 * 5 + 8
+    # 8 doubles, 5 int64 counters, cellwalk_ms, interp_ms
+    assert C.sizeof(J.jt_timings) == 8 * 8 + 8 * 5 + 16
     assert J.jt_timings.cellwalk_ms.offset == 8 * 8 + 8 * 5
+    assert J.jt_timings.interp_ms.offset == 8 * 8 + 8 * 5 + 8
 
 
 def test_strerror_and_version():

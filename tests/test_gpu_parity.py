@@ -317,15 +317,15 @@ def test_kmin_filter_both_modes(k_min):
     s = J.Solver(J.Config(box_L=L, pm_grid=M, theta=theta, softening=eps, r_s=r_cut / 3, r_cut=r_cut,
                           mu=(sg < 0).sum() / (sg > 0).sum(), G_mass_plus=mf, k_min=k_min,
                           mode=J.JT_RCOMPAT))
-    s.set_state_signed(pos, None, sg)
-    got = s.accel_part(J.JT_PART_PM)
-    s.close()
-    got = np.concatenate(got) if isinstance(got, tuple) else got
     pp, pm = pos[sg > 0], pos[sg < 0]
-    ref = O.ref_pm_forces(pos, sg, M, L, mf, r_cut, k_min=k_min)
-    ref = np.concatenate([ref[sg > 0], ref[sg < 0]])
-    unf = O.ref_pm_forces(pos, sg, M, L, mf, r_cut, k_min=0)
-    unf = np.concatenate([unf[sg > 0], unf[sg < 0]])
+    s.set_state(pp, None, pm, None)
+    got = np.concatenate(s.accel_part(J.JT_PART_PM))
+    s.close()
+    # the per-species layout is the array [m+ ; m-] with its signs
+    cat = np.concatenate([pp, pm])
+    csg = np.concatenate([np.ones(len(pp), np.int8), -np.ones(len(pm), np.int8)])
+    ref = O.ref_pm_forces(cat, csg, M, L, mf, r_cut, k_min=k_min)
+    unf = O.ref_pm_forces(cat, csg, M, L, mf, r_cut, k_min=0)
     rel = _rel(got, ref)
     assert np.percentile(rel, 99) <= 1e-5, np.percentile(rel, [50, 99, 100])
     assert np.percentile(_rel(unf, ref), 50) > 1e-3   # the filter changes the force
