@@ -519,6 +519,9 @@ int  jt_server_get_state(jt_server* s, int job, float* pos_p, float* vel_p,
  * JT_ESTATE before its first force pass. */
 int  jt_server_get_accel(jt_server* s, int job, float* acc_p, float* acc_m);
 int  jt_server_stats(jt_server* s, jt_serve_stats* out);
+/* Stage times and counts of every batched step the server ran, summed
+ * (opening force passes included); the fields as jt_get_timings'. */
+int  jt_server_get_timings(jt_server* s, jt_timings* out);
 
 /* ---- Janus expansion history (FP64) ----
  * The reference's JanusExpansion (src/janus_expansion.rs:62-266): the exact

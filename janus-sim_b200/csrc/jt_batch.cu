@@ -236,6 +236,27 @@ struct jt_batch {
 
 namespace {
 
+// Per-axis k tables of a box (index n = 0..M-1), computed on the device so
+// that adding a box needs no host-to-device copy from pageable memory (which
+// would wait for the batch's stream):
+//   ta = {k, gradient k (0 at Nyquist), exp(-k^2 r_s^2) / sinc^(2 order), |n|}
+//   tb = {cos(k h / 2), sin(k h / 2), 0, 0} (interlacing phase)
+__global__ void k_box_tabs(float4* __restrict__ tabs, int M, double L, double rs, int order)
+{
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= M) return;
+    const int ni = n <= M / 2 ? n : n - M;
+    const double dk = 2.0 * M_PI / L, hh = L / M;
+    const double k = dk * ni;
+    const double u = M_PI * ni / M;
+    const double sinc = ni == 0 ? 1.0 : sin(u) / u;
+    double w = 1.0;
+    for (int i = 0; i < 2 * order; i++) w *= sinc;
+    const double f = exp(-k * k * rs * rs) / w;
+    tabs[n] = make_float4((float)k, n == M / 2 ? 0.0f : (float)k, (float)f, (float)(ni < 0 ? -ni : ni));
+    tabs[M + n] = make_float4((float)cos(0.5 * k * hh), (float)sin(0.5 * k * hh), 0.0f, 0.0f);
+}
+
 int box_alloc(jt_box_state* b)
 {
     size_t bytes = 0;
@@ -248,27 +269,9 @@ int box_alloc(jt_box_state* b)
     }
     const int M = b->M;
     JT_TRY(dalloc(&b->tabs, 2 * (size_t)M));
-    // per-axis tables: ta = {k, gradient k (0 at Nyquist), exp(-k^2 r_s^2)/sinc^(2 order), |n|}
-    //                  tb = {cos(k h/2), sin(k h/2), 0, 0} (interlacing phase)
-    std::vector<float> tab(8 * (size_t)M);
     const jt_config& c = b->cfg;
-    double dk = 2.0 * M_PI / c.box_L, rs = c.r_s, hh = c.box_L / M;
-    for (int n = 0; n < M; n++) {
-        int ni = n <= M / 2 ? n : n - M;
-        double k = dk * ni;
-        double u = M_PI * ni / M;
-        double sinc = ni == 0 ? 1.0 : std::sin(u) / u;
-        double f = std::exp(-k * k * rs * rs) / std::pow(sinc, 2.0 * b->order);
-        tab[4 * n] = (float)k;
-        tab[4 * n + 1] = (n == M / 2) ? 0.0f : (float)k;
-        tab[4 * n + 2] = (float)f;
-        tab[4 * n + 3] = (float)(ni < 0 ? -ni : ni);
-        tab[4 * (M + n)] = (float)std::cos(0.5 * k * hh);
-        tab[4 * (M + n) + 1] = (float)std::sin(0.5 * k * hh);
-        tab[4 * (M + n) + 2] = 0.0f;
-        tab[4 * (M + n) + 3] = 0.0f;
-    }
-    JT_CU(cudaMemcpy(b->tabs, tab.data(), sizeof(float) * tab.size(), cudaMemcpyHostToDevice));
+    k_box_tabs<<<(M + 127) / 128, 128, 0, t_alloc->st>>>(b->tabs, M, c.box_L, c.r_s, b->order);
+    JT_CU(cudaGetLastError());
     b->bytes = bytes + sizeof(float4) * 2 * (size_t)M;
     return JT_OK;
 }
@@ -1032,6 +1035,63 @@ int jtb_set_accel(jt_batch* B, int box_id, const float* acc_p, const float* acc_
     }
     JT_CU(cudaGetLastError());
     b->acc_valid = true;
+    return JT_OK;
+}
+
+int jtb_upload_async(jt_batch* B, int box_id, const float* const pos[2], const float* const vel[2],
+                     const float* const acc[2])
+{
+    if (!box_id_ok(B, box_id)) return JT_EINVAL;
+    AllocScope scope(&B->actx);
+    jt_box_state* b = B->boxes[box_id];
+    for (int s = 0; s < 2; s++) {
+        const int64_t n = b->n[s];
+        if (n == 0) continue;
+        if (!pos[s] || (acc && !acc[s])) return JT_EINVAL;
+        // the kernels read the pinned host arrays through their device
+        // addresses (no staging buffer, no copy engine)
+        jt_launch_host_in(pos[s], n, b->pos[s], b->id[s], B->st);
+        if (vel && vel[s]) jt_launch_host_in(vel[s], n, b->vel[s], nullptr, B->st);
+        else JT_CU(cudaMemsetAsync(b->vel[s], 0, sizeof(float4) * (size_t)n, B->st));
+        if (acc) jt_launch_host_in(acc[s], n, b->acc[s], nullptr, B->st);
+    }
+    JT_CU(cudaGetLastError());
+    b->acc_valid = acc != nullptr;
+    return JT_OK;
+}
+
+int jtb_download_async(jt_batch* B, int box_id, float* const pos[2], float* const vel[2], float* const acc[2],
+                       bool* acc_copied)
+{
+    if (!box_id_ok(B, box_id)) return JT_EINVAL;
+    AllocScope scope(&B->actx);
+    jt_box_state* b = B->boxes[box_id];
+    const bool with_acc = acc != nullptr && b->acc_valid;
+    for (int s = 0; s < 2; s++) {
+        const int64_t n = b->n[s];
+        if (n == 0) continue;
+        // the kernels write the pinned host arrays through their device
+        // addresses, in caller order; the inverse order goes into the
+        // reorder's spare id buffer (rewritten by the next sort)
+        int* inv = b->id_b[s];
+        jt_launch_inverse(b->id[s], n, inv, B->st);
+        if (pos[s]) jt_launch_host_out(b->pos[s], inv, n, pos[s], B->st);
+        if (vel[s]) jt_launch_host_out(b->vel[s], inv, n, vel[s], B->st);
+        if (with_acc && acc[s]) jt_launch_host_out(b->acc[s], inv, n, acc[s], B->st);
+    }
+    JT_CU(cudaGetLastError());
+    if (acc_copied) *acc_copied = with_acc;
+    return JT_OK;
+}
+
+int jtb_remove_async(jt_batch* B, int box_id)
+{
+    if (!box_id_ok(B, box_id)) return JT_EINVAL;
+    AllocScope scope(&B->actx);
+    box_release(B->boxes[box_id]);   // stream-ordered frees: after the work queued on the box
+    B->gen++;
+    delete B->boxes[box_id];
+    B->boxes[box_id] = nullptr;
     return JT_OK;
 }
 

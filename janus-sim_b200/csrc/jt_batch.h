@@ -60,6 +60,22 @@ int jth_info(jt_handle* h, jt_config* cfg, float* m_plus, float* m_minus, int8_t
 int jt_diag_state(const float4* const pos[2], const float4* const vel[2], const int64_t n[2],
                   const float mass[2], double L, int n_cells, cudaStream_t st, jt_diag* out);
 int jtb_set_accel(jt_batch* B, int box_id, const float* acc_p, const float* acc_m, int mem);
+// The serving loop's transfers between a box and pinned host arrays (AoS
+// float3 per species, the caller's order), queued on the batch's stream with
+// no host synchronisation.  The pointers are the DEVICE addresses of pinned
+// host memory (cudaHostGetDevicePointer): the gather/scatter kernels read and
+// write the host arrays over the bus directly, so no staging buffer is held
+// per transfer and several admissions and evictions can be in flight behind
+// a step.  The host may read or reuse the arrays only after synchronising
+// the stream.  upload: pos required, vel (NULL: zero) and acc (NULL: none;
+// else the box's forces become valid) optional.  download: acc is written
+// only when the box holds valid forces (*acc_copied says).  remove_async:
+// frees the box's memory in stream order (no host wait).
+int jtb_upload_async(jt_batch* B, int box_id, const float* const pos[2], const float* const vel[2],
+                     const float* const acc[2]);
+int jtb_download_async(jt_batch* B, int box_id, float* const pos[2], float* const vel[2], float* const acc[2],
+                       bool* acc_copied);
+int jtb_remove_async(jt_batch* B, int box_id);
 // Map `bytes` of device memory into the batch's pool (one allocation, freed
 // at once: the pool keeps it) so that later allocations need no new mapping.
 int jtb_reserve(jt_batch* B, size_t bytes);

@@ -400,6 +400,15 @@ void jt_launch_from_caller(const float4* src_caller, const int* id, const int* g
                            float4* dst, cudaStream_t st);
 void jt_launch_aos_in(const float* src_aos, int64_t n, float4* dst, int* id,
                       cudaStream_t st);
+// Transfers through mapped pinned host memory (the host array's device
+// address): every warp reads or writes whole contiguous 128-byte lines, staged
+// through shared memory, so PCIe carries full lines.  host_in: dst[i] =
+// src_aos[3i..3i+2] (and id[i] = i when id is given).  host_out: first
+// jt_launch_inverse(id, n, inv) makes inv[id[i]] = i, then dst_aos[3k..3k+2] =
+// src[inv[k]] in caller order k.
+void jt_launch_host_in(const float* src_aos, int64_t n, float4* dst, int* id, cudaStream_t st);
+void jt_launch_inverse(const int* id, int64_t n, int* inv, cudaStream_t st);
+void jt_launch_host_out(const float4* src, const int* inv, int64_t n, float* dst_aos, cudaStream_t st);
 void jt_launch_split_signed(const float* pos_aos, const float* vel_aos, const int8_t* sg,
                             int64_t n, const int* rank, float4* pos_p, float4* vel_p,
                             int* id_p, int* gmap_p, float4* pos_m, float4* vel_m,

@@ -43,6 +43,8 @@ struct Job {
     size_t n_p = 0, n_m = 0;
     float* host = nullptr;         // pinned: pos_p, vel_p, pos_m, vel_m (3 floats each)
     float* host_acc = nullptr;     // pinned: acc_p, acc_m of a swapped-out job
+    float* dev_host = nullptr;     // device addresses of the same pinned buffers
+    float* dev_host_acc = nullptr;
     bool acc_saved = false;        // host_acc belongs to the state in host
     int steps_total = 0, steps_done = 0;
     jt_step_args args = {0.0, 0.0, 1.0};
@@ -75,6 +77,7 @@ struct jt_server {
     size_t peak_device = 0;
     double admit_s = 0.0, evict_s = 0.0;   // wall time in admissions / evictions
     double step_device_s = 0.0;            // device time of the batched steps
+    jt_timings tm_sum{};                   // their stage times and counts, summed
     size_t reserved = 0;                   // bytes reserved in the batch's pool at creation
     int max_resident = 0;
     std::set<int> prepared;        // grid sizes whose cuFFT plans the batch holds (jt_batch_prepare)
@@ -97,19 +100,21 @@ int admit(jt_server* S, Job& j)
         double t;
         ~Clock() { S->admit_s += now_s() - t; }
     } clock_{S, t_in};
-    const float* h = j.host;
+    const float* h = j.dev_host;
     const size_t np = j.n_p, nm = j.n_m;
     int box = -1;
-    int r = jt_batch_add(S->B, &j.cfg, h, h + 3 * np, np, h + 6 * np, h + 6 * np + 3 * nm, nm, JT_MEM_HOST,
-                         &box);
+    int r = jtb_add_empty(S->B, &j.cfg, (int64_t)np, (int64_t)nm, &box);
     if (r != JT_OK) return r;
-    if (j.acc_saved) {
-        // a swapped-out job comes back with its forces: no extra force pass
-        r = jtb_set_accel(S->B, box, j.host_acc, j.host_acc + 3 * np, JT_MEM_HOST);
-        if (r != JT_OK) {
-            jt_batch_remove(S->B, box);
-            return r;
-        }
+    // the state (and, for a swapped-out job, its forces: no extra force pass)
+    // read from the job's pinned buffers by kernels queued on the batch's
+    // stream, without a host wait: the next step runs after them in stream order
+    const float* pos[2] = {h, h + 6 * np};
+    const float* vel[2] = {h + 3 * np, h + 6 * np + 3 * nm};
+    const float* acc[2] = {j.dev_host_acc, j.dev_host_acc + 3 * np};
+    r = jtb_upload_async(S->B, box, pos, vel, j.acc_saved ? acc : nullptr);
+    if (r != JT_OK) {
+        jt_batch_remove(S->B, box);
+        return r;
     }
     j.box = box;
     j.state = kResident;
@@ -129,18 +134,21 @@ int evict(jt_server* S, Job& j, bool final)
         double t;
         ~Clock() { S->evict_s += now_s() - t; }
     } clock_{S, now_s()};
-    float* h = j.host;
+    float* h = j.dev_host;
     const size_t np = j.n_p, nm = j.n_m;
-    int r = jt_batch_get_state(S->B, j.box, h, h + 3 * np, h + 6 * np, h + 6 * np + 3 * nm, JT_MEM_HOST);
+    // the state and the forces at it (none yet: a swapped-out job then comes
+    // back with a force pass; a finished job's forces are its result as much
+    // as its state, jt_server_get_accel) into the job's pinned buffers, and
+    // the box's memory freed, all in the batch's stream order with no host
+    // wait; readers of the buffers synchronise the stream first
+    float* pos[2] = {h, h + 6 * np};
+    float* vel[2] = {h + 3 * np, h + 6 * np + 3 * nm};
+    float* acc[2] = {j.dev_host_acc, j.dev_host_acc + 3 * np};
+    bool got_acc = false;
+    int r = jtb_download_async(S->B, j.box, pos, vel, acc, &got_acc);
     if (r != JT_OK) return r;
-    j.acc_saved = false;
-    // keep the forces of the state leaving the device (none yet: a swapped-out
-    // job then comes back with a force pass); a finished job's forces are
-    // its result as much as its state (jt_server_get_accel)
-    if (j.host_acc &&
-        jt_batch_get_accel(S->B, j.box, j.host_acc, j.host_acc + 3 * np, JT_MEM_HOST) == JT_OK)
-        j.acc_saved = true;
-    r = jt_batch_remove(S->B, j.box);
+    j.acc_saved = got_acc;
+    r = jtb_remove_async(S->B, j.box);
     if (r != JT_OK) return r;
     j.box = -1;
     j.state = final ? kDone : kQueued;
@@ -260,7 +268,25 @@ int step_once(jt_server* S, int* served)
     S->busy_s += done - a;
     {
         jt_timings t;
-        if (jt_batch_get_timings(S->B, &t) == JT_OK) S->step_device_s += 1e-3 * t.total_ms;
+        if (jt_batch_get_timings(S->B, &t) == JT_OK) {
+            S->step_device_s += 1e-3 * t.total_ms;
+            jt_timings& a = S->tm_sum;
+            a.sort_ms += t.sort_ms;
+            a.tree_ms += t.tree_ms;
+            a.deposit_ms += t.deposit_ms;
+            a.fft_ms += t.fft_ms;
+            a.kspace_ms += t.kspace_ms;
+            a.walk_ms += t.walk_ms;
+            a.kick_drift_ms += t.kick_drift_ms;
+            a.total_ms += t.total_ms;
+            a.interactions += t.interactions;
+            a.launches += t.launches;
+            a.pair_interactions += t.pair_interactions;
+            a.node_interactions += t.node_interactions;
+            a.candidates += t.candidates;
+            a.cellwalk_ms += t.cellwalk_ms;
+            a.interp_ms += t.interp_ms;
+        }
     }
     S->steps++;
     S->max_resident = std::max(S->max_resident, (int)ids.size());
@@ -358,8 +384,12 @@ int jt_server_add_job(jt_server* S, const jt_config* cfg, const float* pos_p, co
     // keeps: both pinned once here (page-locking costs far more than the
     // copies, so it stays out of the admissions and evictions)
     if (cudaMallocHost((void**)&j.host, sizeof(float) * floats) != cudaSuccess) return JT_ENOMEM;
-    if (cudaMallocHost((void**)&j.host_acc, sizeof(float) * 3 * (n_p + n_m)) != cudaSuccess) {
+    if (cudaMallocHost((void**)&j.host_acc, sizeof(float) * 3 * (n_p + n_m)) != cudaSuccess ||
+        cudaHostGetDevicePointer((void**)&j.dev_host, j.host, 0) != cudaSuccess ||
+        cudaHostGetDevicePointer((void**)&j.dev_host_acc, j.host_acc, 0) != cudaSuccess) {
+        cudaGetLastError();
         cudaFreeHost(j.host);
+        if (j.host_acc) cudaFreeHost(j.host_acc);
         j.host = nullptr;
         j.host_acc = nullptr;
         return JT_ENOMEM;
@@ -458,6 +488,8 @@ int jt_server_get_state(jt_server* S, int job, float* pos_p, float* vel_p, float
     if (!job_ok(S, job)) return JT_EINVAL;
     Job& j = S->jobs[job];
     if (j.state == kResident) return jt_batch_get_state(S->B, j.box, pos_p, vel_p, pos_m, vel_m, JT_MEM_HOST);
+    // an eviction's copies into the pinned buffers may still be in flight
+    if (cudaStreamSynchronize(jtb_stream(S->B)) != cudaSuccess) return JT_ECUDA;
     const float* h = j.host;
     const size_t np = j.n_p, nm = j.n_m;
     if (pos_p) std::memcpy(pos_p, h, sizeof(float) * 3 * np);
@@ -473,8 +505,16 @@ int jt_server_get_accel(jt_server* S, int job, float* acc_p, float* acc_m)
     Job& j = S->jobs[job];
     if (j.state == kResident) return jt_batch_get_accel(S->B, j.box, acc_p, acc_m, JT_MEM_HOST);
     if (!j.acc_saved) return JT_ESTATE;
+    if (cudaStreamSynchronize(jtb_stream(S->B)) != cudaSuccess) return JT_ECUDA;
     if (acc_p) std::memcpy(acc_p, j.host_acc, sizeof(float) * 3 * j.n_p);
     if (acc_m) std::memcpy(acc_m, j.host_acc + 3 * j.n_p, sizeof(float) * 3 * j.n_m);
+    return JT_OK;
+}
+
+int jt_server_get_timings(jt_server* S, jt_timings* out)
+{
+    if (!S || !out) return JT_EINVAL;
+    *out = S->tm_sum;
     return JT_OK;
 }
 

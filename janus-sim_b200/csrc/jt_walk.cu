@@ -960,6 +960,48 @@ __global__ void k_aos_in(const float* __restrict__ src, int64_t n, float4* __res
     if (id) id[i] = (int)i;
 }
 
+// 256 particles (768 words) per block; the host side is touched only as
+// contiguous words t, t + 256, t + 512 of the block's span.
+__global__ void __launch_bounds__(256) k_host_in(const float* __restrict__ src, int64_t n,
+                                                 float4* __restrict__ dst, int* __restrict__ id)
+{
+    __shared__ float w[768];
+    const int64_t base = (int64_t)blockIdx.x * 256;
+    const int m = n - base < 256 ? (int)(n - base) : 256;
+    const float* s = src + 3 * base;
+    for (int k = threadIdx.x; k < 3 * m; k += 256) w[k] = s[k];
+    __syncthreads();
+    const int t = threadIdx.x;
+    if (t < m) {
+        dst[base + t] = make_float4(w[3 * t], w[3 * t + 1], w[3 * t + 2], 0.f);
+        if (id) id[base + t] = (int)(base + t);
+    }
+}
+
+__global__ void k_inverse(const int* __restrict__ id, int64_t n, int* __restrict__ inv)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) inv[id[i]] = (int)i;
+}
+
+__global__ void __launch_bounds__(256) k_host_out(const float4* __restrict__ src, const int* __restrict__ inv,
+                                                  int64_t n, float* __restrict__ dst)
+{
+    __shared__ float w[768];
+    const int64_t base = (int64_t)blockIdx.x * 256;
+    const int m = n - base < 256 ? (int)(n - base) : 256;
+    const int t = threadIdx.x;
+    if (t < m) {
+        float4 v = src[inv[base + t]];
+        w[3 * t] = v.x;
+        w[3 * t + 1] = v.y;
+        w[3 * t + 2] = v.z;
+    }
+    __syncthreads();
+    float* d = dst + 3 * base;
+    for (int k = t; k < 3 * m; k += 256) d[k] = w[k];
+}
+
 __global__ void k_split_signed(const float* __restrict__ pos, const float* __restrict__ vel,
                                const int8_t* __restrict__ sg, int64_t n, const int* __restrict__ rank,
                                float4* pos_p, float4* vel_p, int* id_p, int* gmap_p, float4* pos_m,
@@ -1258,10 +1300,19 @@ __global__ void k_cell_scatter(CellArgs A, int64_t npart)
     A.cb.cid[dst] = make_int2(g, (int)idx);
 }
 
+// A cell with more targets than one batch takes them in a spatial order:
+// sub-cell Morton code (3 bits per axis) of each target, ranked in shared
+// memory, so that each batch of 32 covers a compact part of the cell and
+// streams only the candidates its box can reach.  Cells with more than
+// kCellSortMax targets keep the list's order.
+constexpr int kCellSortMax = 256;
+
 struct CellWarpSmem {
     float4 cand[64];
     int2 nrange[27];              // (first, count) of each neighbour cell
     float4 nshift[27];            // periodic shift of its particles
+    int key[kCellSortMax];        // sub-cell code << 8 | target's rank in the list
+    int order[kCellSortMax];      // batch position -> target offset in the cell
 };
 
 // dense evaluation of candidates [0, cnt) for this lane's target: every pair
@@ -1287,7 +1338,7 @@ __device__ __forceinline__ unsigned cell_chunk(const float4* __restrict__ cand, 
         const float2* __restrict__ tb = (SCR && si * q.w < 0.0f) ? yt : g_ltab;
         const bool in = r2 < rc2;
         // only lanes inside the cut read the table (a predicated load: the
-        // ~4/5 of dense candidates outside it issue no L1 request)
+        // ~3/4 of dense candidates outside it issue no L1 request)
         float2 ab = make_float2(0.f, 0.f);
         if (in) ab = __ldg(&tb[k]);
         const float w = q.w * fmaf(ab.y, y, ab.x);
@@ -1299,22 +1350,29 @@ __device__ __forceinline__ unsigned cell_chunk(const float4* __restrict__ cand, 
     return hits;
 }
 
-// One batch of a cell's targets: lane l takes target base + l.  (Two
-// targets per lane for cells with more than 32, which streams and tests
-// their candidates once instead of twice, measured slower: its registers
-// lowered the occupancy of the whole kernel.)
+// One batch of a cell's targets: lane l takes target base + l.  Smaller
+// batches (16 or 8 targets, the warp's lanes split into 2 or 4 candidate
+// streams) test 19 % or 37 % fewer candidates, but each batch streams and
+// tests the 27 neighbour cells again: measured 5 % and 33 % slower at
+// 2x224^3.  (Two targets per lane for cells with more than 32, which streams
+// and tests their candidates once instead of twice, measured slower too: its
+// registers lowered the occupancy of the whole kernel.)
+// base: the batch's first position in the cell's target order; t0, t1: the
+// cell's range of the cell list; sorted: the order comes from S.order
 template <int ORDER, int NG, bool SCR>
 __device__ __forceinline__ void cell_batch(const CellArgs& A, const jt_box_dev& B, CellWarpSmem& S, int base,
-                                           int t1, int lane, unsigned& pairs, unsigned& cands)
+                                           int t0, int t1, bool sorted, int lane, unsigned& pairs,
+                                           unsigned& cands)
 {
     const unsigned lt = (1u << lane) - 1u;
     const float rc2 = B.rc2, c2 = B.c * B.c, ye = B.eps2 * c2;
     const float slack = B.halfL * 9.5367431640625e-7f, rc2_keep = B.rc2 * 1.00001f;
     const float2* __restrict__ yt = (SCR && B.ytab) ? B.ytab : g_ltab;
-    const int t = base + lane;
-    const bool valid = t < t1;
-    const float4 p = A.cb.cpos[valid ? t : base];
-    const int2 id = A.cb.cid[valid ? t : base];
+    const int pos_in_cell = base + lane;
+    const bool valid = t0 + pos_in_cell < t1;
+    const int t = t0 + (valid ? (sorted ? S.order[pos_in_cell] : pos_in_cell) : (sorted ? S.order[base] : base));
+    const float4 p = A.cb.cpos[t];
+    const int2 id = A.cb.cid[t];
     const float si = p.w > 0.f ? 1.0f : -1.0f;
     const float lox = warp_min(p.x), loy = warp_min(p.y), loz = warp_min(p.z);
     const float hix = warp_max(p.x), hiy = warp_max(p.y), hiz = warp_max(p.z);
@@ -1444,8 +1502,36 @@ __global__ void __launch_bounds__(kWarps * 32, JT_CELL_MINB) k_walk_cell(CellArg
         return;
     }
     __syncwarp();
+    // more than one batch: rank the targets by sub-cell code (3 bits per
+    // axis, Morton order) so that consecutive batches are compact
+    const int nt = t1 - t0;
+    const bool sorted = nt > 32 && nt <= kCellSortMax;
+    if (sorted) {
+        const float cs = B.L / (float)nb;
+        const float ox = (float)cx * cs - B.halfL, oy = (float)cy * cs - B.halfL, oz = (float)cz * cs - B.halfL;
+        const float sc = 8.0f / cs;
+        for (int i = lane; i < nt; i += 32) {
+            const float4 q = A.cb.cpos[t0 + i];
+            const int ux = min(max((int)((q.x - ox) * sc), 0), 7), uy = min(max((int)((q.y - oy) * sc), 0), 7),
+                      uz = min(max((int)((q.z - oz) * sc), 0), 7);
+            int code = 0;
+#pragma unroll
+            for (int b = 0; b < 3; b++)
+                code |= (((ux >> b) & 1) << (3 * b)) | (((uy >> b) & 1) << (3 * b + 1)) | (((uz >> b) & 1) << (3 * b + 2));
+            S.key[i] = (code << 8) | i;   // unique: ties by list order
+        }
+        __syncwarp();
+        for (int i = lane; i < nt; i += 32) {
+            const int ki = S.key[i];
+            int rank = 0;
+            for (int j = 0; j < nt; j++) rank += S.key[j] < ki ? 1 : 0;
+            S.order[rank] = i;
+        }
+        __syncwarp();
+    }
     unsigned pairs = 0, cands = 0;
-    for (int base = t0; base < t1; base += 32) cell_batch<ORDER, NG, SCR>(A, B, S, base, t1, lane, pairs, cands);
+    for (int base = 0; base < nt; base += 32)
+        cell_batch<ORDER, NG, SCR>(A, B, S, base, t0, t1, sorted, lane, pairs, cands);
     if (A.stats) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
@@ -1621,6 +1707,24 @@ void jt_launch_aos_in(const float* src_aos, int64_t n, float4* dst, int* id, cud
 {
     if (n <= 0) return;
     k_aos_in<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(src_aos, n, dst, id);
+}
+
+void jt_launch_host_in(const float* src_aos, int64_t n, float4* dst, int* id, cudaStream_t st)
+{
+    if (n <= 0) return;
+    k_host_in<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(src_aos, n, dst, id);
+}
+
+void jt_launch_inverse(const int* id, int64_t n, int* inv, cudaStream_t st)
+{
+    if (n <= 0) return;
+    k_inverse<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(id, n, inv);
+}
+
+void jt_launch_host_out(const float4* src, const int* inv, int64_t n, float* dst_aos, cudaStream_t st)
+{
+    if (n <= 0) return;
+    k_host_out<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(src, inv, n, dst_aos);
 }
 
 void jt_launch_split_signed(const float* pos_aos, const float* vel_aos, const int8_t* sg, int64_t n,

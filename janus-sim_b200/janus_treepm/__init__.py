@@ -54,7 +54,7 @@ EXPORTED = [
     "jt_batch_set_screening", "jt_step_host", "jt_batch_prepare", "jt_config_short_cut",
     "jt_expansion_create", "jt_expansion_destroy", "jt_expansion_info", "jt_expansion_at_time",
     "jt_expansion_at_redshift", "jt_expansion_state_at_mu", "jt_expansion_calibrate",
-    "jt_expansion_phi_factors",
+    "jt_expansion_phi_factors", "jt_server_get_timings",
 ]
 JT_JOB_QUEUED, JT_JOB_RESIDENT, JT_JOB_DONE = 0, 1, 2
 JT_STATIC_SORT_MAX = 262144
@@ -348,6 +348,7 @@ def library():
     L.jt_server_job_state.argtypes = [H, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.jt_server_get_state.argtypes = [H, C.c_int, fp, fp, fp, fp]
     L.jt_server_stats.argtypes = [H, C.POINTER(jt_serve_stats)]
+    L.jt_server_get_timings.argtypes = [H, C.POINTER(jt_timings)]
     L.jt_server_job_need.argtypes = [C.POINTER(jt_config), C.c_size_t, C.c_size_t, C.POINTER(C.c_size_t)]
     for name in EXPORTED:
         if name not in ("jt_destroy", "jt_strerror", "jt_version", "jt_batch_destroy",
@@ -852,6 +853,12 @@ class Server:
         st = jt_serve_stats()
         _check(library().jt_server_stats(self._s, C.byref(st)), "jt_server_stats")
         return {k: getattr(st, k) for k, _ in jt_serve_stats._fields_}
+
+    def timings(self):
+        """Stage times and counts of all batched steps so far, summed."""
+        t = jt_timings()
+        _check(library().jt_server_get_timings(self._s, C.byref(t)), "jt_server_get_timings")
+        return {k: getattr(t, k) for k, _ in jt_timings._fields_}
 
 
 # --------------------------------------------------------------------------
