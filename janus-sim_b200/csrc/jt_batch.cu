@@ -110,6 +110,10 @@ int box_ngrid(const jt_config& c) { return c.pm_interlace == 2 ? 1 : 2; }
 struct Bucket {                 // PM scratch of the boxes with grid M in a pass
     int M = 0;
     int cap = 0;                // boxes the arrays hold
+    // z transforms fused with the k-space step (jt_zfft.cu): cuFFT's plans
+    // are 2D, one transform per (x, y) plane; fixed when the bucket is made
+    bool fused = false;
+    bool decided = false;
     float* rho = nullptr;
     float2* rho_k = nullptr;
     float2* force_k = nullptr;
@@ -154,8 +158,9 @@ struct Plan {
     std::vector<int> ids;                 // boxes of this pass
     std::vector<jt_seg_dev> pre, post;    // segments before / after the reorder
     std::vector<jt_box_dev> bx;
-    std::vector<int64_t> pprefix, iprefix, tprefix, gprefix, ptprefix, kprefix, cprefix;
+    std::vector<int64_t> pprefix, iprefix, tprefix, gprefix, ptprefix, kprefix, cprefix, zprefix;
     int64_t npart = 0, ninternal = 0, nsorttiles = 0, ngroups = 0, npmtiles = 0, nmodes = 0, ncells = 0;
+    int64_t nztiles = 0;                  // CTAs of the fused z-transform kernel
     bool cells = false;                   // the near-field cell walk runs (jt_b_cells)
     bool screened = false;                // some box is screened (second source, Yukawa tables)
     std::map<int, std::vector<int>> by_M; // M -> boxes (positions in ids)
@@ -166,7 +171,7 @@ struct Plan {
     const jt_seg_dev* d_post = nullptr;
     const jt_box_dev* d_bx = nullptr;
     const int64_t *d_pp = nullptr, *d_ip = nullptr, *d_tp = nullptr, *d_gp = nullptr, *d_ptp = nullptr,
-                  *d_kp = nullptr, *d_cp = nullptr;
+                  *d_kp = nullptr, *d_cp = nullptr, *d_zp = nullptr;
 };
 
 float elapsed(cudaEvent_t a, cudaEvent_t b)
@@ -306,20 +311,24 @@ int fft_chunk(int M)
     return c < 1 ? 1 : (int)c;
 }
 
-int make_plan(jt_batch* B, std::map<int, cufftHandle>& pl, int M, int batch, bool r2c)
+// fused: the grids' (x, y) planes as 2D transforms, M per grid
+int make_plan(jt_batch* B, std::map<int, cufftHandle>& pl, int M, int batch, bool r2c, bool fused)
 {
     if (batch <= 0 || pl.count(batch)) return JT_OK;
     const int64_t G = (int64_t)M * M * M, Gc = (int64_t)M * M * (M / 2 + 1);
     int dims[3] = {M, M, M};
+    const int rank = fused ? 2 : 3;
+    const int64_t rd = fused ? (int64_t)M * M : G, cd = fused ? (int64_t)M * (M / 2 + 1) : Gc;
+    const int n = fused ? batch * M : batch;
     cufftHandle h;
     if (cufftCreate(&h) != CUFFT_SUCCESS) return JT_ECUDA;
     // the work area is the batch's shared one (set once all plans exist)
     cufftSetAutoAllocation(h, 0);
     size_t ws = 0;
-    cufftResult e = r2c ? cufftMakePlanMany(h, 3, dims, nullptr, 1, (int)G, nullptr, 1, (int)Gc, CUFFT_R2C,
-                                            batch, &ws)
-                        : cufftMakePlanMany(h, 3, dims, nullptr, 1, (int)Gc, nullptr, 1, (int)G, CUFFT_C2R,
-                                            batch, &ws);
+    cufftResult e = r2c ? cufftMakePlanMany(h, rank, dims, nullptr, 1, (int)rd, nullptr, 1, (int)cd, CUFFT_R2C,
+                                            n, &ws)
+                        : cufftMakePlanMany(h, rank, dims, nullptr, 1, (int)cd, nullptr, 1, (int)rd, CUFFT_C2R,
+                                            n, &ws);
     if (e != CUFFT_SUCCESS) {
         cufftDestroy(h);
         cudaGetLastError();
@@ -332,9 +341,22 @@ int make_plan(jt_batch* B, std::map<int, cufftHandle>& pl, int M, int batch, boo
     return JT_OK;
 }
 
+// 512^3 grids take the fused z path unless JT_ZFFT=0 (read when a bucket is
+// made: the old path stays reachable for comparisons)
+bool zfft_for(int M)
+{
+    if (jt_zfft_tiles(M) == 0) return false;
+    const char* e = std::getenv("JT_ZFFT");
+    return !(e && e[0] == '0');
+}
+
 int bucket_ensure(jt_batch* B, Bucket& k, int M, int count)
 {
     k.M = M;
+    if (!k.decided) {
+        k.fused = zfft_for(M);
+        k.decided = true;
+    }
     const int ngrid = B->ngrid;
     const int64_t G = (int64_t)M * M * M, Gc = (int64_t)M * M * (M / 2 + 1);
     if (count > k.cap) {
@@ -359,9 +381,9 @@ int bucket_ensure(jt_batch* B, Bucket& k, int M, int count)
     for (int dir = 0; dir < 2; dir++) {
         const int n = dir == 0 ? nr : nc;
         auto& pl = dir == 0 ? k.r2c : k.c2r;
-        if (n >= ch) JT_TRY(make_plan(B, pl, M, ch, dir == 0));
+        if (n >= ch) JT_TRY(make_plan(B, pl, M, ch, dir == 0, k.fused));
         for (int b = 1; b < ch; b <<= 1)
-            if ((n % ch) & b) JT_TRY(make_plan(B, pl, M, b, dir == 0));
+            if ((n % ch) & b) JT_TRY(make_plan(B, pl, M, b, dir == 0, k.fused));
     }
     return JT_OK;
 }
@@ -474,7 +496,7 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
 
     int64_t o_node = 0, o_part = 0, o_tile = 0;
     P.pprefix.push_back(0); P.iprefix.push_back(0); P.tprefix.push_back(0); P.gprefix.push_back(0);
-    P.ptprefix.push_back(0); P.kprefix.push_back(0); P.cprefix.push_back(0);
+    P.ptprefix.push_back(0); P.kprefix.push_back(0); P.cprefix.push_back(0); P.zprefix.push_back(0);
     P.cells = cells_enabled();
     P.bx.resize(nb);
     for (int k = 0; k < nb; k++) {
@@ -586,7 +608,9 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
             P.gprefix.push_back(P.gprefix.back() + (n + 31) / 32);
         }
         P.ptprefix.push_back(P.ptprefix.back() + d.ntiles);
-        P.kprefix.push_back(P.kprefix.back() + Gc);
+        // a fused bucket's boxes take the z kernel, the others k_b_kspace
+        P.kprefix.push_back(P.kprefix.back() + (K.fused ? 0 : Gc));
+        P.zprefix.push_back(P.zprefix.back() + (K.fused ? jt_zfft_tiles(M) : 0));
     }
     P.npart = P.pprefix.back();
     P.ninternal = P.iprefix.back();
@@ -594,6 +618,7 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
     P.ngroups = P.gprefix.back();
     P.npmtiles = P.ptprefix.back();
     P.nmodes = P.kprefix.back();
+    P.nztiles = P.zprefix.back();
     P.ncells = P.cprefix.back();
     if (P.cells) {
         JT_TRY(B->ccount.ensure((size_t)std::max<int64_t>(P.ncells, 1), &grew));
@@ -613,7 +638,7 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
     size_t o_pre = put(buf, P.pre), o_post = put(buf, P.post), o_bx = put(buf, P.bx);
     size_t o_pp = put(buf, P.pprefix), o_ip = put(buf, P.iprefix), o_tp = put(buf, P.tprefix);
     size_t o_gp = put(buf, P.gprefix), o_ptp = put(buf, P.ptprefix), o_kp = put(buf, P.kprefix);
-    size_t o_cp = put(buf, P.cprefix);
+    size_t o_cp = put(buf, P.cprefix), o_zp = put(buf, P.zprefix);
     JT_TRY(B->desc.ensure(buf.size(), &grew));
     // the previous upload may still read the staging buffer
     JT_CU(cudaEventSynchronize(B->desc_done));
@@ -638,6 +663,7 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
     P.d_ptp = (const int64_t*)(d + o_ptp);
     P.d_kp = (const int64_t*)(d + o_kp);
     P.d_cp = (const int64_t*)(d + o_cp);
+    P.d_zp = (const int64_t*)(d + o_zp);
     P.table_bytes = buf.size();
     return JT_OK;
 }
@@ -675,6 +701,8 @@ int force_pass(jt_batch* B, Plan& P, int parts, float kick_frac)
     }
     cudaEventRecord(B->ev[4], st);
     jt_b_kspace(P.d_bx, P.d_kp, nbox, P.nmodes, B->ngrid == 2, B->k_min, st);
+    JT_TRY(jt_b_zfft_kspace(P.d_bx, P.d_zp, nbox, P.nztiles, B->ngrid == 2, B->k_min, 0, st));
+    if (P.screened) JT_TRY(jt_b_zfft_kspace(P.d_bx, P.d_zp, nbox, P.nztiles, B->ngrid == 2, B->k_min, 1, st));
     cudaEventRecord(B->ev[5], st);
     for (auto& kv : P.nslots) {
         Bucket& K = B->buckets[kv.first];
@@ -723,6 +751,7 @@ int force_pass(jt_batch* B, Plan& P, int parts, float kick_frac)
     B->pending = true;
     B->tm.launches += (P.npart > 0 ? 8 : 0) + (P.ninternal > 0 ? 1 : 0) + (P.npart > 0 ? 1 : 0) +
                       (P.npmtiles > 0 ? (P.screened ? 3 : 2) : 0) + (P.nmodes > 0 ? 1 : 0) +
+                      (P.nztiles > 0 ? (P.screened ? 2 : 1) : 0) +
                       (P.ngroups > 0 ? 1 : 0);
     for (int id : P.ids) {
         jt_box_state* b = B->boxes[id];
@@ -897,6 +926,7 @@ int capture_graphs(jt_batch* B, const std::vector<int>& v, const jt_box_step* st
     P.d_gp = (const int64_t*)rebase(P.d_gp);
     P.d_ptp = (const int64_t*)rebase(P.d_ptp);
     P.d_kp = (const int64_t*)rebase(P.d_kp);
+    P.d_zp = (const int64_t*)rebase(P.d_zp);
     const jt_timings saved = B->tm;
     const jt_box_state* b0 = B->boxes[v[0]];
     const int sp0 = b0->n[0] > 0 ? 0 : 1;
@@ -1325,11 +1355,15 @@ int jt_batch_prepare(jt_batch* B, int pm_grid)
     AllocScope scope(&B->actx);
     Bucket& k = B->buckets[pm_grid];
     k.M = pm_grid;
+    if (!k.decided) {
+        k.fused = zfft_for(pm_grid);
+        k.decided = true;
+    }
     // every batch an execution can take: the powers of two up to the chunk
     const int ch = fft_chunk(pm_grid);
     for (int b = 1; b <= ch; b <<= 1) {
-        JT_TRY(make_plan(B, k.r2c, pm_grid, b, true));
-        JT_TRY(make_plan(B, k.c2r, pm_grid, b, false));
+        JT_TRY(make_plan(B, k.r2c, pm_grid, b, true, k.fused));
+        JT_TRY(make_plan(B, k.c2r, pm_grid, b, false, k.fused));
     }
     return JT_OK;
 }
