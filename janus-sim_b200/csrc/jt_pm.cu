@@ -314,16 +314,29 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem)
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 
+// 16-byte copy: both addresses 16-byte aligned
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
 // TT: the tile edge as a constant (16, every grid of 16^3 and up: the
-// region's index arithmetic folds) or 0 (read per box).
+// region's index arithmetic folds) or 0 (read per box).  With TT = 16 a
+// staged row of 20 nodes is stored rotated, [16 nodes of the tile | 2 above
+// | 2 below], so that the tile's 16 nodes (64-byte aligned in the grid and
+// in the row) travel as four 16-byte copies and each halo as one 8-byte
+// copy: 6 copies per row instead of 10; node lx of the row sits at
+// (lx + 18) % 20.
 template <int ORDER, int TT>
 __global__ void __launch_bounds__(512, 2)
 k_b_interp(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ boxes,
            const int64_t* __restrict__ tprefix, const int64_t* __restrict__ pprefix, int nbox,
            int64_t npart, float4* __restrict__ pmacc)
 {
-    extern __shared__ float2 reg2[];
-    const float* reg = reinterpret_cast<const float*>(reg2);
+    extern __shared__ float4 reg4[];
+    float2* reg2 = reinterpret_cast<float2*>(reg4);
+    const float* reg = reinterpret_cast<const float*>(reg4);
     const int64_t q = blockIdx.x;
     const int g = blockIdx.y;   // interlaced grid
     const int b = jt_find(tprefix, nbox, q);
@@ -340,13 +353,28 @@ k_b_interp(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ b
     const int64_t G = (int64_t)M * M * M;
     const float* __restrict__ F = B.force + (int64_t)g * 3 * G;
     const int rows = 3 * R * R;
-    // x pairs start at even nodes (ox and M even): 8-byte aligned, never split by the wrap
-    for (int k = threadIdx.x; k < rows * RH; k += blockDim.x) {
-        const int j = k % RH, row = k / RH;
-        const int y = row % R, zc = row / R;
-        const int z = zc % R, c = zc / R;
-        const int64_t gi = c * G + ((int64_t)((oz + z) & mask) * M + ((oy + y) & mask)) * M + ((ox + 2 * j) & mask);
-        cp_async8(reg2 + k, F + gi);
+    if (TT == 16) {
+        float* regw = reinterpret_cast<float*>(reg4);
+        for (int k = threadIdx.x; k < rows * 6; k += blockDim.x) {
+            const int piece = k % 6, row = k / 6;
+            const int y = row % R, zc = row / R;
+            const int z = zc % R, c = zc / R;
+            const int64_t rb = c * G + ((int64_t)((oz + z) & mask) * M + ((oy + y) & mask)) * M;
+            float* dst = regw + row * R;
+            if (piece < 4) cp_async16(dst + 4 * piece, F + rb + ox + 2 + 4 * piece);   // the tile's nodes
+            else if (piece == 4) cp_async8(dst + 16, F + rb + ((ox + 18) & mask));     // 2 above
+            else cp_async8(dst + 18, F + rb + (ox & mask));                            // 2 below
+        }
+    } else {
+        // x pairs start at even nodes (ox and M even): 8-byte aligned, never split by the wrap
+        for (int k = threadIdx.x; k < rows * RH; k += blockDim.x) {
+            const int j = k % RH, row = k / RH;
+            const int y = row % R, zc = row / R;
+            const int z = zc % R, c = zc / R;
+            const int64_t gi =
+                c * G + ((int64_t)((oz + z) & mask) * M + ((oy + y) & mask)) * M + ((ox + 2 * j) & mask);
+            cp_async8(reg2 + k, F + gi);
+        }
     }
     asm volatile("cp.async.wait_all;\n" ::: "memory");
     __syncthreads();
@@ -384,7 +412,8 @@ k_b_interp(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ b
             // rows rr (rp = 0) and rr + 1 (rp = 1): compile-time stencil
             // indices, selected by rp (no dynamic index into the weights)
             if (in) {
-                const float* base = reg + (lz * R + ly) * R + lx + cx;
+                const int xp = lx + cx;
+                const float* base = reg + (lz * R + ly) * R + (TT == 16 ? (xp >= 2 ? xp - 2 : xp + 18) : xp);
 #pragma unroll
                 for (int rr = 0; rr < ORDER * ORDER; rr += 2) {
                     constexpr int O = ORDER;
