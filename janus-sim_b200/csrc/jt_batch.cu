@@ -161,6 +161,7 @@ struct Plan {
     std::vector<int64_t> pprefix, iprefix, tprefix, gprefix, ptprefix, kprefix, cprefix, zprefix;
     int64_t npart = 0, ninternal = 0, nsorttiles = 0, ngroups = 0, npmtiles = 0, nmodes = 0, ncells = 0;
     int64_t nztiles = 0;                  // CTAs of the fused z-transform kernel
+    int zsizes = 0;                       // its grid sizes in the pass: bit 0 512^3, bit 1 256^3
     bool cells = false;                   // the near-field cell walk runs (jt_b_cells)
     bool screened = false;                // some box is screened (second source, Yukawa tables)
     std::map<int, std::vector<int>> by_M; // M -> boxes (positions in ids)
@@ -611,6 +612,7 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
         // a fused bucket's boxes take the z kernel, the others k_b_kspace
         P.kprefix.push_back(P.kprefix.back() + (K.fused ? 0 : Gc));
         P.zprefix.push_back(P.zprefix.back() + (K.fused ? jt_zfft_tiles(M) : 0));
+        if (K.fused) P.zsizes |= M == 512 ? 1 : 2;
     }
     P.npart = P.pprefix.back();
     P.ninternal = P.iprefix.back();
@@ -701,8 +703,9 @@ int force_pass(jt_batch* B, Plan& P, int parts, float kick_frac)
     }
     cudaEventRecord(B->ev[4], st);
     jt_b_kspace(P.d_bx, P.d_kp, nbox, P.nmodes, B->ngrid == 2, B->k_min, st);
-    JT_TRY(jt_b_zfft_kspace(P.d_bx, P.d_zp, nbox, P.nztiles, B->ngrid == 2, B->k_min, 0, st));
-    if (P.screened) JT_TRY(jt_b_zfft_kspace(P.d_bx, P.d_zp, nbox, P.nztiles, B->ngrid == 2, B->k_min, 1, st));
+    JT_TRY(jt_b_zfft_kspace(P.d_bx, P.d_zp, nbox, P.nztiles, B->ngrid == 2, B->k_min, 0, P.zsizes, st));
+    if (P.screened)
+        JT_TRY(jt_b_zfft_kspace(P.d_bx, P.d_zp, nbox, P.nztiles, B->ngrid == 2, B->k_min, 1, P.zsizes, st));
     cudaEventRecord(B->ev[5], st);
     for (auto& kv : P.nslots) {
         Bucket& K = B->buckets[kv.first];
@@ -751,7 +754,7 @@ int force_pass(jt_batch* B, Plan& P, int parts, float kick_frac)
     B->pending = true;
     B->tm.launches += (P.npart > 0 ? 8 : 0) + (P.ninternal > 0 ? 1 : 0) + (P.npart > 0 ? 1 : 0) +
                       (P.npmtiles > 0 ? (P.screened ? 3 : 2) : 0) + (P.nmodes > 0 ? 1 : 0) +
-                      (P.nztiles > 0 ? (P.screened ? 2 : 1) : 0) +
+                      (P.nztiles > 0 ? (P.screened ? 2 : 1) * ((P.zsizes & 1) + ((P.zsizes >> 1) & 1)) : 0) +
                       (P.ngroups > 0 ? 1 : 0);
     for (int id : P.ids) {
         jt_box_state* b = B->boxes[id];

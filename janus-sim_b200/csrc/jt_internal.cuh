@@ -289,13 +289,14 @@ void jt_b_tile_ranges(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const
 int jt_b_deposit(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_t* d_tprefix,
                  int nbox, int64_t ntiles, int order, int ngrid, int T, cudaStream_t st, int src = 0,
                  bool T16 = false);
-// The fused z transforms + k-space of 512^3 grids whose planes cuFFT
-// transforms in 2D (jt_zfft.cu): CTAs per box (0 for other grid sizes), and
-// the launch over every such box of a pass (src 1: a screened box's unsigned
-// source).
+// The fused z transforms + k-space of 512^3 and 256^3 grids whose planes
+// cuFFT transforms in 2D (jt_zfft.cu): CTAs per box (0 for other grid
+// sizes), and the launches over every such box of a pass (sizes: bit 0 if
+// the pass has 512^3 boxes, bit 1 if 256^3; src 1: a screened box's
+// unsigned source).
 int jt_zfft_tiles(int M);
 int jt_b_zfft_kspace(const jt_box_dev* d_boxes, const int64_t* d_zprefix, int nbox, int64_t ntiles, int interlace,
-                     int k_min, int src, cudaStream_t st);
+                     int k_min, int src, int sizes, cudaStream_t st);
 void jt_b_kspace(const jt_box_dev* d_boxes, const int64_t* d_kprefix, int nbox, int64_t nmodes,
                  int interlace, int k_min, cudaStream_t st);
 // PM interpolation of every particle of the pass from each interlaced grid

@@ -1,4 +1,5 @@
-// The z transforms and the k-space multiply of a 512^3 PM grid in one kernel.
+// The z transforms and the k-space multiply of a 512^3 or 256^3 PM grid in
+// one kernel.
 //
 // A 3D real FFT is separable: the batch runs the two transforms over each
 // (x, y) plane with cuFFT (a 2D R2C per plane: [z][ky][kx], kx = 0..M/2), then
@@ -11,7 +12,7 @@
 // the k-space traffic become one read of the two spectra and one write of
 // the six: 32 NG Gc bytes.
 //
-// One CTA takes 8 consecutive kx of one ky (8 columns, 512 threads: 64 per
+// At 512^3 one CTA takes 8 consecutive kx of one ky (512 threads: 64 per
 // column, the column index fastest, so that each warp's loads and stores are
 // 4 rows of 64 contiguous bytes).  A 512-point transform is three radix-8
 // stages over registers (each thread holds 8 values), with two exchanges
@@ -22,17 +23,15 @@
 //   stage 2, thread (k1, t2): DFT8 over j2 (t = t2 + 8 j2), times W64^(t2 k2)
 //   stage 3, thread (k1, k2): DFT8 over t2 -> X[k1 + 8 k2 + 64 k3], k3 = 0..7
 // and the inverse runs the stages backwards with conjugate twiddles
-// (unnormalised, as cuFFT's).  Twiddles come from sincospif of exact
-// arguments m / 256, stored as the matrices the stages read.
+// (unnormalised, as cuFFT's).  At 256^3 (fft256_fwd below) a CTA takes 16
+// columns of 32 threads and the last stage is two radix-4 DFTs per thread.
+// Twiddles come from sincospif of exact arguments 2 m / M, stored as the
+// matrices the stages read.
 #include "jt_internal.cuh"
 
 namespace {
 
-constexpr int kM = 512, kMh = kM / 2 + 1;
-constexpr int kC = 8;                           // columns per CTA
-constexpr int kNT = kC * 64;                    // threads per CTA
-constexpr int kCS = 580;                        // column stride of the exchange buffer (complex)
-constexpr int kTilesX = (kMh + kC - 1) / kC;    // 33 column tiles per ky
+constexpr int kNT = 512;   // threads per CTA (8 columns x 64 at 512^3, 16 x 32 at 256^3)
 
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
@@ -139,84 +138,187 @@ __device__ __forceinline__ void fft512_inv(float2 (&v)[8], float2* XA, float2* X
     dft8<true>(v);
 }
 
+// In-place 4-point DFT (INV: e^{+...}, unnormalised).
+template <bool INV>
+__device__ __forceinline__ void dft4(float2& a0, float2& a1, float2& a2, float2& a3)
+{
+    const float2 b0 = cadd(a0, a2), b1 = csub(a0, a2), b2 = cadd(a1, a3), b3 = mul_s<INV>(csub(a1, a3));
+    a0 = cadd(b0, b2);
+    a2 = csub(b0, b2);
+    a1 = cadd(b1, b3);
+    a3 = csub(b1, b3);
+}
+
+// The 256-point transform of 256^3 grids: 32 threads per column, each holding
+// 8 values; 256 = 8 x 8 x 4, n = t + 32 j, k = k1 + 8 k2 + 64 k3:
+//   stage 1, thread t:        DFT8 over j,  times W256^(t k1)
+//   stage 2, thread (k1, t2): DFT8 over j2 (t = t2 + 4 j2), times W32^(t2 k2)
+//   stage 3, thread u takes the pairs p = u and u + 32 (k1 = p >> 3,
+//            k2 = p & 7): DFT4 over t2 -> X[k1 + 8 k2 + 64 k3], k3 = 0..3,
+//            held as v[4 h + k3] for p = u + 32 h
+// Exchange layouts: row strides 32 and 4, column stride 257 (16 columns per
+// CTA, the column index fastest in a warp: rows of 128 bytes); twiddle
+// matrices tw1[k1 * 32 + t] = W256^(t k1), tw2[k2 * 4 + t2] = W32^(t2 k2).
+__device__ __forceinline__ void fft256_fwd(float2 (&v)[8], float2* XA, float2* XB, const float2* tw1,
+                                           const float2* tw2, int u)
+{
+    dft8<false>(v);
+#pragma unroll
+    for (int k1 = 1; k1 < 8; k1++) v[k1] = cmul(v[k1], tw1[k1 * 32 + u]);
+#pragma unroll
+    for (int k1 = 0; k1 < 8; k1++) XA[k1 * 32 + u] = v[k1];
+    __syncthreads();
+    {
+        const int k1 = u >> 2, t2 = u & 3;
+#pragma unroll
+        for (int j2 = 0; j2 < 8; j2++) v[j2] = XA[k1 * 32 + t2 + 4 * j2];
+        dft8<false>(v);
+#pragma unroll
+        for (int k2 = 1; k2 < 8; k2++) v[k2] = cmul(v[k2], tw2[k2 * 4 + t2]);
+#pragma unroll
+        for (int k2 = 0; k2 < 8; k2++) XB[(k1 * 8 + k2) * 4 + t2] = v[k2];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int p = u + 32 * h;
+#pragma unroll
+        for (int t2 = 0; t2 < 4; t2++) v[4 * h + t2] = XB[p * 4 + t2];
+        dft4<false>(v[4 * h], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
+    }
+}
+
+// Inverse of fft256_fwd (unnormalised): in v[4 h + k3]; out v[j] = x[u + 32 j].
+__device__ __forceinline__ void fft256_inv(float2 (&v)[8], float2* XA, float2* XB, const float2* tw1,
+                                           const float2* tw2, int u)
+{
+    const int k2p = u & 7;   // k2 of both pairs (p = u, u + 32)
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int p = u + 32 * h;
+        dft4<true>(v[4 * h], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
+#pragma unroll
+        for (int t2 = 0; t2 < 4; t2++) {
+            const float2 c = t2 ? cmulc(v[4 * h + t2], tw2[k2p * 4 + t2]) : v[4 * h];
+            XA[p * 4 + t2] = c;
+        }
+    }
+    __syncthreads();
+    {
+        const int k1 = u >> 2, t2 = u & 3;
+#pragma unroll
+        for (int k2 = 0; k2 < 8; k2++) v[k2] = XA[(k1 * 8 + k2) * 4 + t2];
+        dft8<true>(v);
+#pragma unroll
+        for (int j2 = 0; j2 < 8; j2++) v[j2] = cmulc(v[j2], tw1[k1 * 32 + t2 + 4 * j2]);
+#pragma unroll
+        for (int j2 = 0; j2 < 8; j2++) XB[k1 * 32 + t2 + 4 * j2] = v[j2];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k1 = 0; k1 < 8; k1++) v[k1] = XB[k1 * 32 + u];
+    dft8<true>(v);
+}
+
+// Per grid size: columns per CTA, threads per column, exchange-buffer column
+// stride (complex), twiddle entries (tw1 then tw2).
+template <int M> struct ZShape;
+template <> struct ZShape<512> {
+    static constexpr int C = 8, T = 64, CS = 580, NTW1 = 512, NTW2 = 64;
+};
+template <> struct ZShape<256> {
+    static constexpr int C = 16, T = 32, CS = 257, NTW1 = 256, NTW2 = 32;
+};
+
+template <int M> __host__ __device__ constexpr int z_tiles_x() { return (M / 2 + 1 + ZShape<M>::C - 1) / ZShape<M>::C; }
+
+// the z frequency of the value v[i] that thread t holds after a forward transform
+template <int M>
+__device__ __forceinline__ int kz_of(int t, int i)
+{
+    if (M == 512) return (t >> 3) + 8 * (t & 7) + 64 * i;
+    const int p = t + 32 * (i >> 2);
+    return (p >> 3) + 8 * (p & 7) + 64 * (i & 3);
+}
+
+// One CTA of one box: 8 (512^3) or 16 (256^3) consecutive kx of one ky.
 // src 0: the signed source (B.rho_k -> B.force_k); src 1: the unsigned source
 // of a screened box (B.rho_s_k -> B.force_s_k).  The k-space arithmetic is
 // k_b_kspace's, element by element.
-template <bool IL>
-__global__ void __launch_bounds__(kNT, 2)
-k_zfft_kspace(const jt_box_dev* __restrict__ boxes, const int64_t* __restrict__ zprefix, int nbox, int k_min,
-              int src)
+template <int M, bool IL>
+__device__ __forceinline__ void zfft_body(const jt_box_dev& B, const float2* __restrict__ in,
+                                          float2* __restrict__ out, int64_t local, int k_min, int src,
+                                          float2* zsm)
 {
-    extern __shared__ float2 zsm[];
+    using S = ZShape<M>;
+    constexpr int Mh = M / 2 + 1, C = S::C, T = S::T, CS = S::CS;
     // twiddles as the two matrices the stages read, each indexed fastest by
-    // the reading thread's own index (no bank conflicts):
-    // tw1[k1 * 64 + t] = W512^(t k1), tw2[k2 * 8 + t2] = W64^(t2 k2) (symmetric)
+    // the reading thread's own index (no bank conflicts)
     float2* tw1 = zsm;
-    float2* tw2 = zsm + kM;
-    float2* xbuf = zsm + kM + 64;     // two exchange buffers per column
-    const int64_t q = blockIdx.x;
-    const int b = jt_find(zprefix, nbox, q);
-    const jt_box_dev& B = boxes[b];
-    const float2* __restrict__ in = src ? B.rho_s_k : B.rho_k;
-    float2* __restrict__ out = src ? B.force_s_k : B.force_k;
-    if (!in) return;   // the unsigned source of an unscreened box (whole block)
-    const int64_t local = q - zprefix[b];
-    const int ky = (int)(local / kTilesX);
-    const int kx0 = (int)(local % kTilesX) * kC;
-    const int tid = threadIdx.x, col = tid & (kC - 1), t = tid >> 3;
+    float2* tw2 = zsm + S::NTW1;
+    float2* xbuf = zsm + S::NTW1 + S::NTW2;   // two exchange buffers per column
+    const int ky = (int)(local / z_tiles_x<M>());
+    const int kx0 = (int)(local % z_tiles_x<M>()) * C;
+    const int tid = threadIdx.x, col = tid & (C - 1), t = tid / C;
     const int kx = kx0 + col;
-    const bool colok = kx < kMh;
+    const bool colok = kx < Mh;
     {
-        // W512^m = e^{-2 pi i m / 512}: sincospif of the exact argument m / 256
+        // W_M^m = e^{-2 pi i m / M}: sincospif of the exact argument 2 m / M
         float s, c;
-        sincospif((float)(((tid & 63) * (tid >> 6)) & (kM - 1)) * (1.0f / 256.0f), &s, &c);
-        tw1[tid] = make_float2(c, -s);
-        if (tid < 64) {
-            sincospif((float)((8 * (tid & 7) * (tid >> 3)) & (kM - 1)) * (1.0f / 256.0f), &s, &c);
+        if (tid < S::NTW1) {
+            const int k1 = tid / T, tt = tid % T;
+            sincospif((float)((tt * k1) & (M - 1)) * (2.0f / M), &s, &c);
+            tw1[tid] = make_float2(c, -s);
+        }
+        if (tid < S::NTW2) {
+            // W(8 T)^(t2 k2) = W_M^(8 t2 k2): tw2[k2 * (T / 8) + t2]
+            const int k2 = tid / (T / 8), t2 = tid % (T / 8);
+            sincospif((float)((8 * t2 * k2) & (M - 1)) * (2.0f / M), &s, &c);
             tw2[tid] = make_float2(c, -s);
         }
     }
     __syncthreads();
-    float2* XA = xbuf + col * kCS;
-    float2* XB = xbuf + (kC + col) * kCS;
-    const int64_t Gc = (int64_t)kM * kM * kMh;
-    const int64_t sz = (int64_t)kMh * kM;   // z stride of a column
-    const int64_t cb = (int64_t)(colok ? kx : 0) + (int64_t)kMh * ky;
+    float2* XA = xbuf + col * CS;
+    float2* XB = xbuf + (C + col) * CS;
+    const int64_t Gc = (int64_t)M * M * Mh;
+    const int64_t sz = (int64_t)Mh * M;   // z stride of a column
+    const int64_t cb = (int64_t)(colok ? kx : 0) + (int64_t)Mh * ky;
     float2 P[8], v[8];
 #pragma unroll
-    for (int j = 0; j < 8; j++) v[j] = colok ? __ldcs(in + cb + (t + 64 * j) * sz) : make_float2(0.f, 0.f);
-    fft512_fwd(v, XA, XB, tw1, tw2, t);
+    for (int j = 0; j < 8; j++) v[j] = colok ? __ldcs(in + cb + (t + T * j) * sz) : make_float2(0.f, 0.f);
+    if constexpr (M == 512) fft512_fwd(v, XA, XB, tw1, tw2, t);
+    else fft256_fwd(v, XA, XB, tw1, tw2, t);
 #pragma unroll
     for (int k = 0; k < 8; k++) P[k] = v[k];
     if (IL) {
 #pragma unroll
         for (int j = 0; j < 8; j++)
-            v[j] = colok ? __ldcs(in + Gc + cb + (t + 64 * j) * sz) : make_float2(0.f, 0.f);
-        fft512_fwd(v, XA, XB, tw1, tw2, t);
+            v[j] = colok ? __ldcs(in + Gc + cb + (t + T * j) * sz) : make_float2(0.f, 0.f);
+        if constexpr (M == 512) fft512_fwd(v, XA, XB, tw1, tw2, t);
+        else fft256_fwd(v, XA, XB, tw1, tw2, t);
     }
     const float4* __restrict__ ta = B.tabs;
-    const float4* __restrict__ tb = B.tabs + kM;
+    const float4* __restrict__ tb = B.tabs + M;
     const float4 ax = __ldg(&ta[colok ? kx : 0]), ay = __ldg(&ta[ky]);
     const float4 bx = __ldg(&tb[colok ? kx : 0]), by = __ldg(&tb[ky]);
     const float2 exy = make_float2(bx.x * by.x - bx.y * by.y, bx.x * by.y + bx.y * by.x);
-    const int half = kM / 2;
+    const int half = M / 2;
     const int nx = (int)ax.w, ny = (int)ay.w;
-    const float norm = 1.0f / ((float)kM * (float)kM * (float)kM);
+    const float norm = 1.0f / ((float)M * (float)M * (float)M);
     const bool scr = B.ky2 > 0.0f;
-    const int kz0 = (t >> 3) + 8 * (t & 7);   // k1 + 8 k2; kz = kz0 + 64 k3
 #pragma unroll
-    for (int k3 = 0; k3 < 8; k3++) {
-        const int kz = kz0 + 64 * k3;
+    for (int i = 0; i < 8; i++) {
+        const int kz = kz_of<M>(t, i);
         const float4 az = __ldg(&ta[kz]);
         const float k2 = ax.x * ax.x + ay.x * ay.x + az.x * az.x;
         const int nz = (int)az.w;
         const int kmax = max(max(nx, ny), nz);
         const bool keep = colok && k2 > 0.0f && kmax >= k_min && nx != half && ny != half && nz != half;
-        float2 z = P[k3];
+        float2 z = P[i];
         if (IL) {
             const float4 bz = __ldg(&tb[kz]);
             const float er = exy.x * bz.x - exy.y * bz.y, ei = exy.x * bz.y + exy.y * bz.x;
-            const float2 u = v[k3];
+            const float2 u = v[i];
             z.x = 0.5f * (z.x + (u.x * er + u.y * ei));
             z.y = 0.5f * (z.y + (u.y * er - u.x * ei));
         }
@@ -225,7 +327,7 @@ k_zfft_kspace(const jt_box_dev* __restrict__ boxes, const int64_t* __restrict__ 
             const float gy = green * (k2 / (k2 + B.ky2)) * B.yfac;
             green = src ? 0.5f * (green - gy) : 0.5f * (green + gy);
         }
-        P[k3] = keep ? make_float2(z.x * green, z.y * green) : make_float2(0.f, 0.f);
+        P[i] = keep ? make_float2(z.x * green, z.y * green) : make_float2(0.f, 0.f);
     }
     // the six force spectra (three components, times the interlaced grid's
     // phase for the second grid), each transformed back along z
@@ -233,39 +335,70 @@ k_zfft_kspace(const jt_box_dev* __restrict__ boxes, const int64_t* __restrict__ 
     for (int s = 0; s < 3 * (IL ? 2 : 1); s++) {
         const int c = s % 3, g = s / 3;
 #pragma unroll
-        for (int k3 = 0; k3 < 8; k3++) {
-            const int kz = kz0 + 64 * k3;
-            const float d = c == 0 ? ax.y : (c == 1 ? ay.y : __ldg(&ta[kz]).y);
-            float2 f = make_float2(d * P[k3].y, -d * P[k3].x);
+        for (int i = 0; i < 8; i++) {
+            const int kz = kz_of<M>(t, i);
+            const float dd = c == 0 ? ax.y : (c == 1 ? ay.y : __ldg(&ta[kz]).y);
+            float2 f = make_float2(dd * P[i].y, -dd * P[i].x);
             if (g == 1) {
                 const float4 bz = __ldg(&tb[kz]);
                 const float2 e = make_float2(exy.x * bz.x - exy.y * bz.y, exy.x * bz.y + exy.y * bz.x);
                 f = cmul(f, e);
             }
-            v[k3] = f;
+            v[i] = f;
         }
-        fft512_inv(v, XA, XB, tw1, tw2, t);
+        if constexpr (M == 512) fft512_inv(v, XA, XB, tw1, tw2, t);
+        else fft256_inv(v, XA, XB, tw1, tw2, t);
         if (colok) {
             float2* o = out + (int64_t)s * Gc + cb;
 #pragma unroll
-            for (int j = 0; j < 8; j++) o[(t + 64 * j) * sz] = v[j];
+            for (int j = 0; j < 8; j++) o[(t + T * j) * sz] = v[j];
         }
     }
 }
 
+// One launch per grid size present in the pass (each with its own register
+// allocation); the CTAs of the other size's boxes return at once.
+template <int M, bool IL>
+__global__ void __launch_bounds__(kNT, 2)
+k_zfft_kspace(const jt_box_dev* __restrict__ boxes, const int64_t* __restrict__ zprefix, int nbox, int k_min,
+              int src)
+{
+    extern __shared__ float2 zsm[];
+    const int64_t q = blockIdx.x;
+    const int b = jt_find(zprefix, nbox, q);
+    const jt_box_dev& B = boxes[b];
+    if (B.M != M) return;   // whole block
+    const float2* __restrict__ in = src ? B.rho_s_k : B.rho_k;
+    float2* __restrict__ out = src ? B.force_s_k : B.force_k;
+    if (!in) return;   // the unsigned source of an unscreened box (whole block)
+    zfft_body<M, IL>(B, in, out, q - zprefix[b], k_min, src, zsm);
+}
+
 }  // namespace
 
-int jt_zfft_tiles(int M) { return M == kM ? kM * kTilesX : 0; }
+int jt_zfft_tiles(int M)
+{
+    if (M == 512) return 512 * z_tiles_x<512>();
+    if (M == 256) return 256 * z_tiles_x<256>();
+    return 0;
+}
 
 int jt_b_zfft_kspace(const jt_box_dev* d_boxes, const int64_t* d_zprefix, int nbox, int64_t ntiles, int interlace,
-                     int k_min, int src, cudaStream_t st)
+                     int k_min, int src, int sizes, cudaStream_t st)
 {
     if (ntiles <= 0) return JT_OK;
     const unsigned g = (unsigned)ntiles;
-    const int smem = (int)sizeof(float2) * (kM + 64 + 2 * kC * kCS);
-    const void* f = interlace ? (const void*)k_zfft_kspace<true> : (const void*)k_zfft_kspace<false>;
-    if (jt_smem_attr(f, smem) != JT_OK) return JT_ECUDA;
-    if (interlace) k_zfft_kspace<true><<<g, kNT, smem, st>>>(d_boxes, d_zprefix, nbox, k_min, src);
-    else k_zfft_kspace<false><<<g, kNT, smem, st>>>(d_boxes, d_zprefix, nbox, k_min, src);
+#define JT_ZLAUNCH(MM)                                                                                   \
+    do {                                                                                                 \
+        const int smem = (int)sizeof(float2) *                                                           \
+                         (ZShape<MM>::NTW1 + ZShape<MM>::NTW2 + 2 * ZShape<MM>::C * ZShape<MM>::CS);     \
+        const void* f = interlace ? (const void*)k_zfft_kspace<MM, true> : (const void*)k_zfft_kspace<MM, false>; \
+        if (jt_smem_attr(f, smem) != JT_OK) return JT_ECUDA;                                             \
+        if (interlace) k_zfft_kspace<MM, true><<<g, kNT, smem, st>>>(d_boxes, d_zprefix, nbox, k_min, src);   \
+        else k_zfft_kspace<MM, false><<<g, kNT, smem, st>>>(d_boxes, d_zprefix, nbox, k_min, src);          \
+    } while (0)
+    if (sizes & 1) JT_ZLAUNCH(512);
+    if (sizes & 2) JT_ZLAUNCH(256);
+#undef JT_ZLAUNCH
     return JT_OK;
 }

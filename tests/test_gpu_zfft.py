@@ -1,4 +1,4 @@
-"""The fused z transforms + k-space kernel of 512^3 grids (jt_zfft.cu) against
+"""The fused z transforms + k-space kernel of 512^3 and 256^3 grids (jt_zfft.cu) against
 the 3D path it replaces (cuFFT 3D R2C, k_b_kspace, cuFFT 3D C2R; selected
 with JT_ZFFT=0 when a handle is made).
 
@@ -43,17 +43,18 @@ def _check(a, b, tol=1e-5):
     assert np.all(np.isfinite(a)) and err <= tol, err
 
 
-@pytest.mark.parametrize("interlace,k_min", [(0, 0), (2, 0), (0, 3)])
-def test_fused_z_transforms_match_the_3d_path(interlace, k_min):
-    L, M, n = 200.0, 512, 48
+@pytest.mark.parametrize("M,interlace,k_min", [(512, 0, 0), (512, 2, 0), (512, 0, 3), (256, 0, 0), (256, 2, 3)])
+def test_fused_z_transforms_match_the_3d_path(M, interlace, k_min):
+    L, n = 200.0 * M / 512, 48
     pp, _, pm, _ = ics.zeldovich_lattice(n, L, seed=7)
     cfg = J.Config(box_L=L, pm_grid=M, theta=0.5, softening=0.02, r_s=1.25 * L / M, r_cut=4.5 * 1.25 * L / M,
                    mu=19.0, G_mass_plus=1e-3, mode=J.JT_ACCURATE, pm_interlace=interlace, k_min=k_min)
     _check(_pm(cfg, pp, pm, True), _pm(cfg, pp, pm, False))
 
 
-def test_fused_z_transforms_screened():
-    L, M, n = 150.0, 512, 40
+@pytest.mark.parametrize("M", [512, 256])
+def test_fused_z_transforms_screened(M):
+    L, n = 150.0 * M / 512, 40
     pp, pm = ics.uniform_box(n ** 3, L, seed=3)
     cfg = J.Config(box_L=L, pm_grid=M, theta=0.5, softening=0.02, r_s=1.25 * L / M, r_cut=4.5 * 1.25 * L / M,
                    mu=19.0, G_mass_plus=1e-3, mode=J.JT_ACCURATE)
