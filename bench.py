@@ -689,12 +689,12 @@ def run_ours(args, ws, rank, local):
             clustered["walk_frac_fp32"] = clustered["walk_tflops"] / peak_fp32
     if rank == 0 and ws == 1 and args.ensemble_boxes > 0:
         ensemble = run_ensemble(J, ics, args.ensemble_boxes, args.ensemble_steps, 3, H, w["dt"])
-        if args.serve_jobs > 0:
-            try:
-                serving = run_serving(J, ics, args.serve_jobs, args.serve_big, args.serve_steps,
-                                      [float(r) for r in args.serve_rates.split(",")], H, w["dt"])
-            except J.JanusError as e:
-                serving = {"error": str(e)}
+    if rank == 0 and ws == 1 and args.serve_jobs > 0:
+        try:
+            serving = run_serving(J, ics, args.serve_jobs, args.serve_big, args.serve_steps,
+                                  [float(r) for r in args.serve_rates.split(",")], H, w["dt"])
+        except J.JanusError as e:
+            serving = {"error": str(e)}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": K,

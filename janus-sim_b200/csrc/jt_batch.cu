@@ -1462,11 +1462,19 @@ int jt_batch_step(jt_batch* B, const int* ids, int n_ids, const jt_step_args* ar
             need.push_back(v[k]);
             need_steps.push_back(steps[k]);
         }
+    // its completion is awaited after the next plan is built, so that the
+    // host's plan work for the step overlaps the pass on the device (the
+    // new plan's tables reach the device in stream order, after the pass)
+    bool open_pending = false;
     if (!need.empty()) {
         r = jtb_force_pass(B, need.data(), (int)need.size(), JT_PART_ALL, 0.0f, need_steps.data());
-        if (r == JT_OK) r = finish(B);
+        open_pending = r == JT_OK;
     }
     double kd = 0.0;
+    if (open_pending && B->use_graphs) {
+        r = finish(B);
+        open_pending = false;
+    }
     if (r == JT_OK && B->use_graphs) {
         if (B->gc.gen != B->gen || B->gc.ids != v) r = capture_graphs(B, v, steps.data());
         if (r == JT_OK) {
@@ -1494,6 +1502,10 @@ int jt_batch_step(jt_batch* B, const int* ids, int n_ids, const jt_step_args* ar
     }
     Plan& P = B->plan;
     if (r == JT_OK && nsteps > 0) r = build_plan(B, v, steps.data(), P);
+    if (open_pending) {
+        const int rf = finish(B);
+        if (r == JT_OK) r = rf;
+    }
     for (int k = 0; k < nsteps && r == JT_OK; k++) {
         cudaEventRecord(k0, B->st);
         if (k == 0) jt_b_kick_drift(P.d_pre, P.d_bx, P.d_pp, (int)P.pre.size(), P.npart, 0.5f, 1.0f, B->st);
