@@ -178,3 +178,26 @@ def test_served_forces_against_the_fp64_oracle():
     for k in ("job0", "job3"):
         assert report[k][1] <= 3e-3, report
     S.close()
+
+
+def test_server_stage_timings_sum_the_batched_steps():
+    """jt_server_get_timings: the batched steps' stage times and counts,
+    summed; the stages fit inside the steps' device time and every served
+    request's pairs are counted."""
+    specs = [job_spec(sd) for sd in (401, 402, 403)]
+    S = J.Server(8 * GiB)
+    ids = [S.add_job(cfg, *st, steps=2, dt=dt, hubble=hub) for cfg, st, dt, hub in specs]
+    for _ in range(2):
+        for j in ids:
+            S.request(j)
+        while S.poll():
+            pass
+    st, tm = S.stats(), S.timings()
+    S.close()
+    assert st["requests_served"] == 6
+    assert tm["total_ms"] > 0.0
+    assert abs(tm["total_ms"] - 1e3 * st["step_device_s"]) <= 1e-6 * tm["total_ms"] + 1e-9
+    stages = sum(tm[k] for k in ("sort_ms", "tree_ms", "deposit_ms", "fft_ms", "walk_ms", "kick_drift_ms"))
+    assert 0.0 < stages <= tm["total_ms"] * (1 + 1e-6)
+    assert tm["kspace_ms"] <= tm["fft_ms"] and tm["cellwalk_ms"] <= tm["walk_ms"]
+    assert tm["pair_interactions"] > 0 and tm["launches"] > 0
