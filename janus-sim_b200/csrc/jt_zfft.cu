@@ -77,6 +77,19 @@ __device__ __forceinline__ void dft8(float2 (&v)[8])
     v[7] = csub(b3, w3);
 }
 
+// w^1 .. w^7 from w (products at most three deep: about 3 ulp), in place of
+// seven table loads (the shared-memory queue is the kernel's limit)
+__device__ __forceinline__ void powers7(float2 w, float2 (&p)[8])
+{
+    p[1] = w;
+    p[2] = cmul(w, w);
+    p[3] = cmul(p[2], w);
+    p[4] = cmul(p[2], p[2]);
+    p[5] = cmul(p[4], w);
+    p[6] = cmul(p[4], p[2]);
+    p[7] = cmul(p[4], p[3]);
+}
+
 // Forward 512-point transform of one column (thread t = 0..63 of it):
 // in v[j] = x[t + 64 j]; out v[k3] = X[k1 + 8 k2 + 64 k3], k1 = t >> 3,
 // k2 = t & 7.  XA and XB are the column's two exchange buffers (576 complex
@@ -87,8 +100,12 @@ __device__ __forceinline__ void fft512_fwd(float2 (&v)[8], float2* XA, float2* X
                                            const float2* tw2, int t)
 {
     dft8<false>(v);
+    {
+        float2 w[8];
+        powers7(tw1[64 + t], w);   // W512^(t k1), k1 = 1..7
 #pragma unroll
-    for (int k1 = 1; k1 < 8; k1++) v[k1] = cmul(v[k1], tw1[k1 * 64 + t]);
+        for (int k1 = 1; k1 < 8; k1++) v[k1] = cmul(v[k1], w[k1]);
+    }
 #pragma unroll
     for (int k1 = 0; k1 < 8; k1++) XA[k1 * 72 + t] = v[k1];
     __syncthreads();
@@ -97,8 +114,10 @@ __device__ __forceinline__ void fft512_fwd(float2 (&v)[8], float2* XA, float2* X
 #pragma unroll
         for (int j2 = 0; j2 < 8; j2++) v[j2] = XA[k1 * 72 + t2 + 8 * j2];
         dft8<false>(v);
+        float2 w[8];
+        powers7(tw2[8 + t2], w);   // W64^(t2 k2), k2 = 1..7
 #pragma unroll
-        for (int k2 = 1; k2 < 8; k2++) v[k2] = cmul(v[k2], tw2[k2 * 8 + t2]);
+        for (int k2 = 1; k2 < 8; k2++) v[k2] = cmul(v[k2], w[k2]);
 #pragma unroll
         for (int k2 = 0; k2 < 8; k2++) XB[(k1 * 8 + k2) * 9 + t2] = v[k2];
     }
@@ -115,9 +134,10 @@ __device__ __forceinline__ void fft512_inv(float2 (&v)[8], float2* XA, float2* X
 {
     dft8<true>(v);
     {
-        const int k2 = t & 7;
+        float2 w[8];
+        powers7(tw2[8 + (t & 7)], w);   // W64^(t2 k2), t2 = 1..7, k2 = t & 7
 #pragma unroll
-        for (int t2 = 1; t2 < 8; t2++) v[t2] = cmulc(v[t2], tw2[t2 * 8 + k2]);
+        for (int t2 = 1; t2 < 8; t2++) v[t2] = cmulc(v[t2], w[t2]);
     }
 #pragma unroll
     for (int t2 = 0; t2 < 8; t2++) XA[t * 9 + t2] = v[t2];
@@ -127,8 +147,15 @@ __device__ __forceinline__ void fft512_inv(float2 (&v)[8], float2* XA, float2* X
 #pragma unroll
         for (int k2 = 0; k2 < 8; k2++) v[k2] = XA[(k1 * 8 + k2) * 9 + t2];
         dft8<true>(v);
+        {
+            // W512^((t2 + 8 j2) k1) = W512^(t2 k1) (W64^k1)^j2
+            const float2 b = tw1[k1 * 64 + t2];
+            float2 s[8];
+            powers7(tw1[k1 * 64 + 8], s);
+            v[0] = cmulc(v[0], b);
 #pragma unroll
-        for (int j2 = 0; j2 < 8; j2++) v[j2] = cmulc(v[j2], tw1[k1 * 64 + t2 + 8 * j2]);
+            for (int j2 = 1; j2 < 8; j2++) v[j2] = cmulc(v[j2], cmul(b, s[j2]));
+        }
 #pragma unroll
         for (int j2 = 0; j2 < 8; j2++) XB[k1 * 72 + t2 + 8 * j2] = v[j2];
     }
@@ -163,8 +190,12 @@ __device__ __forceinline__ void fft256_fwd(float2 (&v)[8], float2* XA, float2* X
                                            const float2* tw2, int u)
 {
     dft8<false>(v);
+    {
+        float2 w[8];
+        powers7(tw1[32 + u], w);   // W256^(u k1), k1 = 1..7
 #pragma unroll
-    for (int k1 = 1; k1 < 8; k1++) v[k1] = cmul(v[k1], tw1[k1 * 32 + u]);
+        for (int k1 = 1; k1 < 8; k1++) v[k1] = cmul(v[k1], w[k1]);
+    }
 #pragma unroll
     for (int k1 = 0; k1 < 8; k1++) XA[k1 * 32 + u] = v[k1];
     __syncthreads();
@@ -173,8 +204,10 @@ __device__ __forceinline__ void fft256_fwd(float2 (&v)[8], float2* XA, float2* X
 #pragma unroll
         for (int j2 = 0; j2 < 8; j2++) v[j2] = XA[k1 * 32 + t2 + 4 * j2];
         dft8<false>(v);
+        float2 w[8];
+        powers7(tw2[4 + t2], w);   // W32^(t2 k2), k2 = 1..7
 #pragma unroll
-        for (int k2 = 1; k2 < 8; k2++) v[k2] = cmul(v[k2], tw2[k2 * 4 + t2]);
+        for (int k2 = 1; k2 < 8; k2++) v[k2] = cmul(v[k2], w[k2]);
 #pragma unroll
         for (int k2 = 0; k2 < 8; k2++) XB[(k1 * 8 + k2) * 4 + t2] = v[k2];
     }
@@ -209,8 +242,15 @@ __device__ __forceinline__ void fft256_inv(float2 (&v)[8], float2* XA, float2* X
 #pragma unroll
         for (int k2 = 0; k2 < 8; k2++) v[k2] = XA[(k1 * 8 + k2) * 4 + t2];
         dft8<true>(v);
+        {
+            // W256^((t2 + 4 j2) k1) = W256^(t2 k1) (W64^k1)^j2
+            const float2 b = tw1[k1 * 32 + t2];
+            float2 s[8];
+            powers7(tw1[k1 * 32 + 4], s);
+            v[0] = cmulc(v[0], b);
 #pragma unroll
-        for (int j2 = 0; j2 < 8; j2++) v[j2] = cmulc(v[j2], tw1[k1 * 32 + t2 + 4 * j2]);
+            for (int j2 = 1; j2 < 8; j2++) v[j2] = cmulc(v[j2], cmul(b, s[j2]));
+        }
 #pragma unroll
         for (int j2 = 0; j2 < 8; j2++) XB[k1 * 32 + t2 + 4 * j2] = v[j2];
     }
