@@ -184,6 +184,11 @@ __device__ __forceinline__ unsigned chunk_mask(const float4* __restrict__ cand, 
 #ifndef JT_WALK_HALF
 #define JT_WALK_HALF 1
 #endif
+// a full chunk whose busiest lane has at least this many hits is evaluated
+// densely (eval_chunk)
+#ifndef JT_WALK_DENSE
+#define JT_WALK_DENSE 22
+#endif
 __device__ __forceinline__ unsigned chunk_mask_h(const WalkWarpSmem& S, __half2 tx, __half2 ty,
                                                  __half2 tz, __half2 rch2)
 {
@@ -230,6 +235,34 @@ __device__ __forceinline__ int eval_chunk(WalkWarpSmem& S, int cnt, int lane, fl
     }
 #endif
     int hits = 0;
+    // dense chunks (a clump inside the cut): every lane evaluates all 32
+    // candidates, the table read predicated by the cut, instead of looping
+    // over its own hits (the warp would run the longest loop anyway, with a
+    // branch per hit)
+    if (!WRAP && cnt == 32) {
+        int mc = __popc(m);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mc = max(mc, __shfl_xor_sync(0xffffffffu, mc, o));
+        if (mc >= JT_WALK_DENSE) {
+#pragma unroll 4
+            for (int j = 0; j < 32; j++) {
+                const float4 q = cand[j];
+                const float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
+                const float r2 = dx * dx + dy * dy + dz * dz;
+                const bool in = valid && r2 > 0.0f && r2 < P.rc2;
+                const float y = (r2 + P.eps2) * P.c2;
+                const unsigned k = min((__float_as_uint(y) >> 14) - JT_LTAB_BASE, (unsigned)JT_LTAB_N - 1u);
+                float2 ab = make_float2(0.f, 0.f);
+                if (in) ab = __ldg(&tab[k]);
+                const float g = fac * fmaf(ab.y, y, ab.x);
+                hits += in ? 1 : 0;
+                a.x += g * dx;
+                a.y += g * dy;
+                a.z += g * dz;
+            }
+            return hits;
+        }
+    }
     while (m) {
         const int j = __ffs(m) - 1;
         m &= m - 1;
