@@ -71,6 +71,7 @@ struct Acc3 {
 // warp's maximum over lanes).  Compiled out of the product build.
 struct WalkCount {
     unsigned long long iters, ranges, chunks, trips;
+    bool dense;   // the warp's previous full chunk was dense (eval_chunk)
 };
 
 
@@ -211,6 +212,40 @@ struct HalfTarget {
     bool on;                      // fp16 mask usable for this group
 };
 
+// Dense evaluation of a full chunk: every lane takes all 32 candidates, the
+// table read predicated by the cut.  Returns the lane's hits.
+template <bool WRAP>
+__device__ __forceinline__ int eval_dense(const float4* __restrict__ cand, float px, float py, float pz,
+                                          bool valid, const jt_walk_params& P, float fac, Acc3& a,
+                                          const float2* __restrict__ tab)
+{
+    int hits = 0;
+#pragma unroll 4
+    for (int j = 0; j < 32; j++) {
+        const float4 q = cand[j];
+        const float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        const bool in = valid && r2 > 0.0f && r2 < P.rc2;
+        const float y = (r2 + P.eps2) * P.c2;
+        const unsigned k = min((__float_as_uint(y) >> 14) - JT_LTAB_BASE, (unsigned)JT_LTAB_N - 1u);
+        float2 ab = make_float2(0.f, 0.f);
+        if (in) ab = __ldg(&tab[k]);
+        const float g = fac * fmaf(ab.y, y, ab.x);
+        hits += in ? 1 : 0;
+        a.x += g * dx;
+        a.y += g * dy;
+        a.z += g * dz;
+    }
+    return hits;
+}
+
+__device__ __forceinline__ int warp_max_int(int v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
 template <bool WRAP>
 __device__ __forceinline__ int eval_chunk(WalkWarpSmem& S, int cnt, int lane, float px, float py,
                                           float pz, bool valid, const jt_walk_params& P, float fac,
@@ -220,6 +255,17 @@ __device__ __forceinline__ int eval_chunk(WalkWarpSmem& S, int cnt, int lane, fl
     wc.chunks++;
     (void)lane;
     const float4* __restrict__ cand = S.cand;
+    // dense chunks (a clump inside the cut): every lane evaluates all 32
+    // candidates instead of looping over its own hits (the warp would run the
+    // longest loop anyway, with a branch per hit).  Chunks come in spatial
+    // runs, so a chunk after a dense one is evaluated densely at once, without
+    // the hit mask, and its own busiest lane decides for the next; the sums
+    // are the same either way (out-of-cut candidates add exactly 0)
+    if (!WRAP && cnt == 32 && wc.dense) {
+        const int hits = eval_dense<WRAP>(cand, px, py, pz, valid, P, fac, a, tab);
+        wc.dense = warp_max_int(hits) >= JT_WALK_DENSE;
+        return hits;
+    }
     unsigned m;
     if (!WRAP && JT_WALK_HALF && cnt == 32 && H.on)
         m = chunk_mask_h(S, H.tx, H.ty, H.tz, H.rch2);
@@ -235,33 +281,9 @@ __device__ __forceinline__ int eval_chunk(WalkWarpSmem& S, int cnt, int lane, fl
     }
 #endif
     int hits = 0;
-    // dense chunks (a clump inside the cut): every lane evaluates all 32
-    // candidates, the table read predicated by the cut, instead of looping
-    // over its own hits (the warp would run the longest loop anyway, with a
-    // branch per hit)
     if (!WRAP && cnt == 32) {
-        int mc = __popc(m);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) mc = max(mc, __shfl_xor_sync(0xffffffffu, mc, o));
-        if (mc >= JT_WALK_DENSE) {
-#pragma unroll 4
-            for (int j = 0; j < 32; j++) {
-                const float4 q = cand[j];
-                const float dx = q.x - px, dy = q.y - py, dz = q.z - pz;
-                const float r2 = dx * dx + dy * dy + dz * dz;
-                const bool in = valid && r2 > 0.0f && r2 < P.rc2;
-                const float y = (r2 + P.eps2) * P.c2;
-                const unsigned k = min((__float_as_uint(y) >> 14) - JT_LTAB_BASE, (unsigned)JT_LTAB_N - 1u);
-                float2 ab = make_float2(0.f, 0.f);
-                if (in) ab = __ldg(&tab[k]);
-                const float g = fac * fmaf(ab.y, y, ab.x);
-                hits += in ? 1 : 0;
-                a.x += g * dx;
-                a.y += g * dy;
-                a.z += g * dz;
-            }
-            return hits;
-        }
+        wc.dense = warp_max_int(__popc(m)) >= JT_WALK_DENSE;
+        if (wc.dense) return eval_dense<WRAP>(cand, px, py, pz, valid, P, fac, a, tab);
     }
     while (m) {
         const int j = __ffs(m) - 1;
@@ -704,7 +726,7 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_walk_acc(WalkArgs A)
 
     Acc3 near = {0.f, 0.f, 0.f}, far = {0.f, 0.f, 0.f}, comp = {0.f, 0.f, 0.f};
     unsigned pairs = 0, nodes = 0, cands = 0;   // per lane (warp totals < 2^32)
-    WalkCount wc = {0, 0, 0, 0};
+    WalkCount wc = {0, 0, 0, 0, false};
     // groups wider than L/8 take the minimum image per pair
     const bool wide = fmaxf(fmaxf(ghx, ghy), ghz) > 0.125f * P.L;
     if (wide)
