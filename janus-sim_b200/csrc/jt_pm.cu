@@ -240,7 +240,16 @@ k_b_deposit(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ 
     constexpr float kRound = 12582912.0f;   // 1.5 * 2^23: x + kRound holds round(x) in its low bits
     constexpr int kRoundBits = 0x4B400000;
     __syncthreads();
-    for (int k = threadIdx.x; k < n0 + n1; k += blockDim.x) {
+    // A crowded tile (a clump: many particles per cell) gives each thread a
+    // run of consecutive particles, so that the lanes of a warp, whose
+    // atomics meet in one instruction, sit far apart in the tile instead of
+    // in the same few cells; integer sums do not depend on the order
+    const int ntot = n0 + n1, tid = (int)threadIdx.x, nth = (int)blockDim.x;
+    const int per = ntot > 2048 ? (ntot + nth - 1) / nth : 0;
+    const int niter = per ? per : (ntot - tid + nth - 1) / nth;
+    for (int i = 0; i < niter; i++) {
+        const int k = per ? tid * per + i : tid + i * nth;
+        if (k >= ntot) break;   // per > 0: the rest of this thread's run is past the end
         float4 p;
         float qq, qg;
         if (k < n0) { p = pos0[r.x + k]; qq = qs0; qg = q0; } else { p = pos1[r.z + k - n0]; qq = qs1; qg = q1; }
