@@ -310,13 +310,16 @@ k_b_deposit(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ 
 // the tile, the interlaced grid's half-cell shift included), are staged in
 // shared memory with asynchronous 8-byte copies (cp.async; R = 20 at
 // T = 16: 96 KB, 2 blocks per SM).  The tile's particles (one contiguous
-// range per species, B.ranges) are then interpolated by groups of 8 lanes:
-// lane (q, r) of a group takes x offset q of the stencil rows r, r + 2, ...
-// of every component, so the 32 lanes of a load instruction read 8 rows of
-// 4 consecutive floats (few bank conflicts; one lane per particle reading
-// its own 27-64 scattered nodes conflicts ~4-way; 16 lanes per particle,
-// one per (x, y) column, measured slower: 0.90 against 0.68 ms at 2x112^3),
-// and the group sums its partial forces with three shuffle steps.  A particle whose stencil leaves
+// range per species, B.ranges) are then interpolated by groups of 4 lanes:
+// lane q of a group takes x offset q of all ORDER^2 stencil rows of every
+// component (sums over y, then z, then one weight along x), so the 32 lanes
+// of a load instruction read the rows of 8 particles, 4 consecutive floats
+// each (few bank conflicts; one lane per particle reading its own 27-64
+// scattered nodes conflicts ~4-way), and the group sums its partial forces
+// with two shuffle steps.  Groups of 8 lanes (x offset and row parity)
+// repeat the stencil arithmetic of a particle on twice the lanes: 5.06
+// against 4.77 ms at 2x224^3; 16 lanes, one per (x, y) column, measured
+// slower still (0.90 against 0.68 ms at 2x112^3).  A particle whose stencil leaves
 // the region (outside its tile by the Morton key's rounding) reads the grid.
 // Output: pmacc[b * npart + i] = the interpolated force of grid b on a unit
 // m+ particle (i = the particle's index in the pass, pprefix[seg] + index);
@@ -399,12 +402,11 @@ k_b_interp(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ b
     float4* __restrict__ out = pmacc + (int64_t)g * npart;
     const int RR = R * R, RRR = RR * R;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    const int gl = lane & 7;            // lane in the particle's group
-    const int cx = gl & 3, rp = gl >> 2;
+    const int gl = lane & 3;            // lane in the particle's group: x offset of the stencil
     const int n = n0 + n1;
     // every lane of a warp runs the same number of iterations (shuffles)
-    for (int k0 = warp * 4; k0 < n; k0 += nwarp * 4) {
-        const int k = k0 + (lane >> 3);
+    for (int k0 = warp * 8; k0 < n; k0 += nwarp * 8) {
+        const int k = k0 + (lane >> 2);
         const bool valid = k < n;
         float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
         int64_t gi = 0;
@@ -418,46 +420,52 @@ k_b_interp(const jt_seg_dev* __restrict__ segs, const jt_box_dev* __restrict__ b
         const int lx = ix - ox, ly = iy - oy, lz = iz - oz;
         const bool in = lx >= 0 && ly >= 0 && lz >= 0 && lx + ORDER <= R && ly + ORDER <= R && lz + ORDER <= R;
         float ax = 0.f, ay = 0.f, az = 0.f;
-        if (valid && cx < ORDER) {
+        if (valid && gl < ORDER) {
             float wxq = wx[0];
 #pragma unroll
-            for (int a = 1; a < ORDER; a++) wxq = cx == a ? wx[a] : wxq;
-            // rows rr (rp = 0) and rr + 1 (rp = 1): compile-time stencil
-            // indices, selected by rp (no dynamic index into the weights)
+            for (int a = 1; a < ORDER; a++) wxq = gl == a ? wx[a] : wxq;
+            // the lane's column x = ix + gl of the stencil: sum over y, then z,
+            // then one weight along x
             if (in) {
-                const int xp = lx + cx;
+                const int xp = lx + gl;
                 const float* base = reg + (lz * R + ly) * R + (TT == 16 ? (xp >= 2 ? xp - 2 : xp + 18) : xp);
 #pragma unroll
-                for (int rr = 0; rr < ORDER * ORDER; rr += 2) {
-                    constexpr int O = ORDER;
-                    const int z0 = rr / O, y0 = rr % O, z1 = (rr + 1) / O, y1 = (rr + 1) % O;
-                    if (rr + 1 < O * O || rp == 0) {
-                        const float w = (rp ? wz[z1 < O ? z1 : 0] * wy[y1] : wz[z0] * wy[y0]) * wxq;
-                        const float* src = base + (rp ? (z1 * R + y1) * R : (z0 * R + y0) * R);
-                        ax = fmaf(w, src[0], ax);
-                        ay = fmaf(w, src[RRR], ay);
-                        az = fmaf(w, src[2 * RRR], az);
+                for (int zz = 0; zz < ORDER; zz++) {
+                    float bx = 0.f, by = 0.f, bz = 0.f;
+#pragma unroll
+                    for (int yy = 0; yy < ORDER; yy++) {
+                        const float* src = base + (zz * R + yy) * R;
+                        bx = fmaf(wy[yy], src[0], bx);
+                        by = fmaf(wy[yy], src[RRR], by);
+                        bz = fmaf(wy[yy], src[2 * RRR], bz);
                     }
+                    ax = fmaf(wz[zz], bx, ax);
+                    ay = fmaf(wz[zz], by, ay);
+                    az = fmaf(wz[zz], bz, az);
                 }
             } else {
+                const int64_t xg = (ix + gl) & mask;
 #pragma unroll
-                for (int rr = 0; rr < ORDER * ORDER; rr += 2) {
-                    constexpr int O = ORDER;
-                    const int z0 = rr / O, y0 = rr % O, z1 = (rr + 1) / O, y1 = (rr + 1) % O;
-                    if (rr + 1 < O * O || rp == 0) {
-                        const int czz = rp ? z1 : z0, cyy = rp ? y1 : y0;
-                        const float w = (rp ? wz[z1 < O ? z1 : 0] * wy[y1] : wz[z0] * wy[y0]) * wxq;
-                        const int64_t id = ((int64_t)((iz + czz) & mask) * M + ((iy + cyy) & mask)) * M +
-                                           ((ix + cx) & mask);
-                        ax = fmaf(w, __ldg(F + id), ax);
-                        ay = fmaf(w, __ldg(F + G + id), ay);
-                        az = fmaf(w, __ldg(F + 2 * G + id), az);
+                for (int zz = 0; zz < ORDER; zz++) {
+                    float bx = 0.f, by = 0.f, bz = 0.f;
+#pragma unroll
+                    for (int yy = 0; yy < ORDER; yy++) {
+                        const int64_t id = ((int64_t)((iz + zz) & mask) * M + ((iy + yy) & mask)) * M + xg;
+                        bx = fmaf(wy[yy], __ldg(F + id), bx);
+                        by = fmaf(wy[yy], __ldg(F + G + id), by);
+                        bz = fmaf(wy[yy], __ldg(F + 2 * G + id), bz);
                     }
+                    ax = fmaf(wz[zz], bx, ax);
+                    ay = fmaf(wz[zz], by, ay);
+                    az = fmaf(wz[zz], bz, az);
                 }
             }
+            ax *= wxq;
+            ay *= wxq;
+            az *= wxq;
         }
 #pragma unroll
-        for (int o = 1; o < 8; o <<= 1) {
+        for (int o = 1; o < 4; o <<= 1) {
             ax += __shfl_xor_sync(0xffffffffu, ax, o);
             ay += __shfl_xor_sync(0xffffffffu, ay, o);
             az += __shfl_xor_sync(0xffffffffu, az, o);
