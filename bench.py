@@ -205,6 +205,18 @@ def reference_gpu_step(n_side, grid, steps=3):
         return {"error": str(e)[:300]}
 
 
+def counted_step(s, step):
+    """One more step with the pair counters on (a diagnostic that the timed
+    steps run without: one instruction per candidate pair of the cell walk),
+    outside the timed region; its timings give the pairs, nodes and
+    candidates of a step."""
+    s.set_counters(True)
+    step()
+    tm = s.timings()
+    s.set_counters(False)
+    return tm
+
+
 def run_clustered(J, ics, steps, warmup, H, dt, cut_tail_ppm=0, theta=0.5):
     """The clustered workload: 2x128^3 particles, 80 % in 512 Plummer spheres
     (scale radii log-uniform 0.05-1 Mpc, species alternating by sphere) + 20 %
@@ -230,15 +242,16 @@ def run_clustered(J, ics, steps, warmup, H, dt, cut_tail_ppm=0, theta=0.5):
         dev += tm["total_ms"]
         for k, v in tm.items():
             stages[k] = stages.get(k, 0.0) + v
+    counted = counted_step(s, lambda: s.step(dt, H, 1.0, 1))
     s.close()
     walk_ms = stages["walk_ms"] / steps - stages.get("interp_ms", 0.0) / steps
-    flops = (stages["pair_interactions"] * FLOPS_PAIR + stages["node_interactions"] * FLOPS_NODE) / steps
+    flops = counted["pair_interactions"] * FLOPS_PAIR + counted["node_interactions"] * FLOPS_NODE
     return {"workload": f"2x{n_side}^3 in 512 Plummer spheres + 20 % background, L={L:g} Mpc, PM {M}^3, "
                         f"theta {theta}, mu 19, cut {J.short_cut(cfg) / r_s:.3g} r_s",
             "value": 2 * n * steps / (dev * 1e-3), "unit": UNIT, "ms_per_step": dev / steps,
             "stages_ms_per_step": {k: round(v / steps, 4) for k, v in stages.items() if k.endswith("_ms")},
-            "pairs_per_step": stages["pair_interactions"] / steps,
-            "nodes_per_step": stages["node_interactions"] / steps,
+            "pairs_per_step": counted["pair_interactions"],
+            "nodes_per_step": counted["node_interactions"],
             "walk_tflops": flops / (walk_ms * 1e-3) / 1e12 if walk_ms > 0 else None,
             "steps": steps, "warmup": warmup}
 
@@ -581,6 +594,7 @@ def run_ours(args, ws, rank, local):
     barrier()
     wall = time.perf_counter() - t_wall
     clk = clocks.stop()
+    counted = counted_step(s, lambda: s.step(w["dt"], H, 1.0, 1))
     dev_ms = max_over_ranks(dev_ms, ws, "cuda")
     K = args.steps
     value = ws * 2 * n * K / (dev_ms * 1e-3)
@@ -649,9 +663,9 @@ def run_ours(args, ws, rank, local):
     # timed alone by its own events (the walk stage also holds the cell list
     # build and the tree walk of flagged particles, none at this density)
     walk_ms = (stages["cellwalk_ms"] if stages.get("cellwalk_ms", 0.0) > 0 else stages["walk_ms"]) / K
-    pairs = stages["pair_interactions"] / K
-    nodes = stages["node_interactions"] / K
-    cands = stages["candidates"] / K
+    pairs = counted["pair_interactions"]
+    nodes = counted["node_interactions"]
+    cands = counted["candidates"]
     achieved = (pairs * FLOPS_PAIR + nodes * FLOPS_NODE) / (walk_ms * 1e-3) / 1e12
     Gc = w["M"] * w["M"] * (w["M"] // 2 + 1)
     ks_ms = stages["kspace_ms"] / K

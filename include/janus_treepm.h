@@ -119,12 +119,22 @@ typedef struct jt_timings {
     double total_ms;     /* whole call */
     int64_t interactions;/* pair + node interactions evaluated by the walk */
     int64_t launches;    /* kernels launched by the library (cuFFT's not counted) */
-    int64_t pair_interactions;  /* particle pairs inside r_cut */
+    int64_t pair_interactions;  /* particle pairs inside r_cut (the cell walk's
+                                   with the pair counters on: jt_set_counters) */
     int64_t node_interactions;  /* multipole node interactions */
     int64_t candidates;         /* particle candidates distance-tested */
     double cellwalk_ms;  /* the near-field cell walk kernel alone (part of walk_ms) */
     double interp_ms;    /* the tiled PM interpolation kernel alone (part of walk_ms) */
 } jt_timings;
+
+/* Pair counters, a diagnostic: with on != 0 the near-field cell walk counts
+ * its pairs inside r_cut into pair_interactions and interactions (one
+ * instruction per candidate pair, about 5 % of the walk's time).  Off by
+ * default (JT_COUNTERS=1 in the environment when a handle, batch or server
+ * is made turns them on), when those fields hold the tree walk's pairs and
+ * nodes only.  jt_batch_set_counters and jt_server_set_counters (declared
+ * with the batches and the server) do the same for their boxes. */
+int  jt_set_counters(jt_handle* h, int on);
 
 /* Create a handle on the current CUDA device.  Replaces the constructor and
  * setters of GpuNBodyTwoPass (src/nbody_gpu_twopass.rs:2159-2336) and
@@ -448,6 +458,8 @@ int  jt_batch_diagnostics(jt_batch* b, int box_id, int n_cells, jt_diag* out);
  * drift, forces + kick dt/2).  Stage timings are not collected inside
  * graphs (total_ms is). */
 int  jt_batch_set_graphs(jt_batch* b, int on);
+/* The pair counters of the batch's passes (as jt_set_counters). */
+int  jt_batch_set_counters(jt_batch* b, int on);
 /* Release the batch's per-pass scratch pools and cuFFT plans (they grow
  * back on the next pass); persistent box state is kept. */
 int  jt_batch_trim(jt_batch* b);
@@ -522,6 +534,8 @@ int  jt_server_stats(jt_server* s, jt_serve_stats* out);
 /* Stage times and counts of every batched step the server ran, summed
  * (opening force passes included); the fields as jt_get_timings'. */
 int  jt_server_get_timings(jt_server* s, jt_timings* out);
+/* The pair counters of the server's batched steps (as jt_set_counters). */
+int  jt_server_set_counters(jt_server* s, int on);
 
 /* ---- Janus expansion history (FP64) ----
  * The reference's JanusExpansion (src/janus_expansion.rs:62-266): the exact

@@ -958,6 +958,12 @@ int jt_get_accel(jt_handle* h, float* acc_p, float* acc_m, int mem)
     return JT_OK;
 }
 
+int jt_set_counters(jt_handle* h, int on)
+{
+    if (!h) return JT_EINVAL;
+    return h->batch ? jt_batch_set_counters(h->batch, on) : JT_OK;
+}
+
 int jt_set_screening(jt_handle* h, double lambda_0, double z)
 {
     if (!h || !(lambda_0 >= 0.0) || !(z > -1.0) || !std::isfinite(lambda_0) || !std::isfinite(z))

@@ -217,6 +217,7 @@ struct jt_batch {
     unsigned* d_err = nullptr;
     unsigned long long* d_stats = nullptr;
     cudaEvent_t ev[11] = {};            // 8, 9: around the cell walk kernel; 6-10: interpolation
+    bool counters = false;              // the cell walk counts its pairs (jt_batch_set_counters)
     bool pending = false;               // a pass's events await jtb_finish
     jt_timings tm = {};
     int64_t phase[4] = {0, 0, 0, 0};
@@ -742,7 +743,7 @@ int force_pass(jt_batch* B, Plan& P, int parts, float kick_frac)
                            B->cpos.p, B->cid.p, B->tflag.p, B->csegflag.p};
         JT_TRY(jt_b_cells(P.d_post, P.d_bx, P.d_pp, nseg, P.npart, P.d_cp, nbox, P.ncells, cb, B->order,
                           B->ngrid, parts, kick_frac, B->d_stats, B->d_err, st, B->ev[8], B->ev[9],
-                          P.screened, pmacc));
+                          P.screened, pmacc, B->counters));
         tflag = B->tflag.p;
         jt_b_build_trees(P.d_post, P.d_bx, nseg, P.d_ip, P.ninternal, P.d_pp, P.npart, st, B->csegflag.p);
         B->tm.launches += P.npart > 0 ? (P.ncells > 0 ? 6 : 1) : 0;
@@ -1249,6 +1250,7 @@ int jt_batch_create(jt_batch** out)
     uint64_t keep = ~(uint64_t)0;
     cudaMemPoolSetAttribute(B->actx.pool, cudaMemPoolAttrReleaseThreshold, &keep);
     B->actx.st = B->st;
+    if (const char* e = getenv("JT_COUNTERS")) B->counters = atoi(e) != 0;
     for (auto& e : B->ev) cudaEventCreate(&e);
     cudaEventCreateWithFlags(&B->desc_done, cudaEventDisableTiming);
     if (cudaMalloc(&B->d_err, sizeof(unsigned)) != cudaSuccess ||
@@ -1607,6 +1609,14 @@ int jt_batch_set_graphs(jt_batch* B, int on)
     if (!B) return JT_EINVAL;
     B->use_graphs = on != 0;
     if (!on) drop_graphs(B);
+    return JT_OK;
+}
+
+int jt_batch_set_counters(jt_batch* B, int on)
+{
+    if (!B) return JT_EINVAL;
+    if (B->counters != (on != 0)) drop_graphs(B);   // the graphs hold the walk's variant
+    B->counters = on != 0;
     return JT_OK;
 }
 

@@ -350,7 +350,7 @@ int jt_b_cells(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_
                int64_t npart, const int64_t* d_cprefix, int nbox, int64_t ncells, const jt_cell_bufs& cb,
                int order, int ngrid, int parts, float kick_frac, unsigned long long* stats,
                unsigned* d_err, cudaStream_t st, cudaEvent_t ev_walk0, cudaEvent_t ev_walk1,
-               bool screened = false, const float4* pmacc = nullptr);
+               bool screened = false, const float4* pmacc = nullptr, bool count_pairs = true);
 int jt_cell_scan_blocks(int64_t ncells);
 // Yukawa split factor S_Y(y) on the walk's table grid (y = (r_p / 2 r_s)^2
 // over [0, 16], JT_STAB_N (value, next - value) entries) for b = kappa r_s.

@@ -511,6 +511,12 @@ int jt_server_get_accel(jt_server* S, int job, float* acc_p, float* acc_m)
     return JT_OK;
 }
 
+int jt_server_set_counters(jt_server* S, int on)
+{
+    if (!S) return JT_EINVAL;
+    return jt_batch_set_counters(S->B, on);
+}
+
 int jt_server_get_timings(jt_server* S, jt_timings* out)
 {
     if (!S || !out) return JT_EINVAL;

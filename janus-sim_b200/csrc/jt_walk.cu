@@ -1377,7 +1377,12 @@ struct CellWarpSmem {
 // q_j G(y) d, which the caller scales by s_i c^3.  The target itself (r = 0,
 // d = 0) adds nothing and is counted as a hit, which the caller removes.
 // SCR: opposite-species pairs read the box's Yukawa table yt.
-template <bool SCR>
+// CNT: count the lane's pairs inside the cut (the pair counters; one
+// instruction per candidate, off unless the caller asks for them).  No
+// clamp on the table index: the caller bounds ye >= 2^-32 and
+// rc2 c2 + ye < 64, so that every y of a lane inside the cut indexes the
+// table ([2^-32, 2^6)); lanes outside it load nothing.
+template <bool SCR, bool CNT>
 __device__ __forceinline__ unsigned cell_chunk(const float4* __restrict__ cand, int cnt, const float4& p, float si,
                                                float rc2, float c2, float ye, Acc3& a,
                                                const float2* __restrict__ yt)
@@ -1389,7 +1394,7 @@ __device__ __forceinline__ unsigned cell_chunk(const float4* __restrict__ cand, 
         const float dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
         const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
         const float y = fmaf(r2, c2, ye);
-        const unsigned k = min((__float_as_uint(y) >> 14) - JT_LTAB_BASE, (unsigned)JT_LTAB_N - 1u);
+        const unsigned k = (__float_as_uint(y) >> 14) - JT_LTAB_BASE;
         const float2* __restrict__ tb = (SCR && si * q.w < 0.0f) ? yt : g_ltab;
         const bool in = r2 < rc2;
         // only lanes inside the cut read the table (a predicated load: the
@@ -1397,7 +1402,7 @@ __device__ __forceinline__ unsigned cell_chunk(const float4* __restrict__ cand, 
         float2 ab = make_float2(0.f, 0.f);
         if (in) ab = __ldg(&tb[k]);
         const float w = q.w * fmaf(ab.y, y, ab.x);
-        hits += in ? 1u : 0u;
+        if (CNT) hits += in ? 1u : 0u;
         a.x = fmaf(w, dx, a.x);
         a.y = fmaf(w, dy, a.y);
         a.z = fmaf(w, dz, a.z);
@@ -1414,13 +1419,18 @@ __device__ __forceinline__ unsigned cell_chunk(const float4* __restrict__ cand, 
 // registers lowered the occupancy of the whole kernel.)
 // base: the batch's first position in the cell's target order; t0, t1: the
 // cell's range of the cell list; sorted: the order comes from S.order
-template <int ORDER, int NG, bool SCR>
+template <int ORDER, int NG, bool SCR, bool CNT>
 __device__ __forceinline__ void cell_batch(const CellArgs& A, const jt_box_dev& B, CellWarpSmem& S, int base,
                                            int t0, int t1, bool sorted, int lane, unsigned& pairs,
                                            unsigned& cands)
 {
     const unsigned lt = (1u << lane) - 1u;
-    const float rc2 = B.rc2, c2 = B.c * B.c, ye = B.eps2 * c2;
+    // the table covers y in [2^-32, 2^6): a softening below 2^-16 (2 r_s)
+    // is raised to it, and the cut is bounded by y < 64 (16 r_s without
+    // softening), where the split factor is below 1e-27: the table's last
+    // entry, zero, held every y past it
+    const float c2 = B.c * B.c, ye = fmaxf(B.eps2 * c2, 2.3283064365386963e-10f);
+    const float rc2 = fminf(B.rc2, (64.0f * 0.99999f - ye) / c2);
     const float slack = B.halfL * 9.5367431640625e-7f, rc2_keep = B.rc2 * 1.00001f;
     const float2* __restrict__ yt = (SCR && B.ytab) ? B.ytab : g_ltab;
     const int pos_in_cell = base + lane;
@@ -1457,7 +1467,7 @@ __device__ __forceinline__ void cell_batch(const CellArgs& A, const jt_box_dev& 
                 nc += __popc(km);
                 __syncwarp();
                 if (nc >= 32) {
-                    hits += cell_chunk<SCR>(S.cand, 32, p, si, rc2, c2, ye, near, yt);
+                    hits += cell_chunk<SCR, CNT>(S.cand, 32, p, si, rc2, c2, ye, near, yt);
                     cands += 32;
                     __syncwarp();
                     const float4 t2 = S.cand[32 + lane];
@@ -1469,12 +1479,12 @@ __device__ __forceinline__ void cell_batch(const CellArgs& A, const jt_box_dev& 
             }
         }
         if (nc > 0) {
-            hits += cell_chunk<SCR>(S.cand, nc, p, si, rc2, c2, ye, near, yt);
+            hits += cell_chunk<SCR, CNT>(S.cand, nc, p, si, rc2, c2, ye, near, yt);
             cands += nc;
         }
         __syncwarp();
         // the target met itself once (r = 0 < r_cut); an empty slot counts nothing
-        if (valid) pairs += hits - 1u;
+        if (CNT && valid) pairs += hits - 1u;
         const float sc = si * c2 * B.c;
         near.x *= sc;
         near.y *= sc;
@@ -1514,7 +1524,7 @@ __device__ __forceinline__ void cell_batch(const CellArgs& A, const jt_box_dev& 
 #ifndef JT_CELL_MINB
 #define JT_CELL_MINB 6
 #endif
-template <int ORDER, int NG, bool SCR>
+template <int ORDER, int NG, bool SCR, bool CNT>
 __global__ void __launch_bounds__(kWarps * 32, JT_CELL_MINB) k_walk_cell(CellArgs A, int64_t ncells)
 {
     __shared__ CellWarpSmem smem_all[kWarps];
@@ -1586,7 +1596,7 @@ __global__ void __launch_bounds__(kWarps * 32, JT_CELL_MINB) k_walk_cell(CellArg
     }
     unsigned pairs = 0, cands = 0;
     for (int base = 0; base < nt; base += 32)
-        cell_batch<ORDER, NG, SCR>(A, B, S, base, t0, t1, sorted, lane, pairs, cands);
+        cell_batch<ORDER, NG, SCR, CNT>(A, B, S, base, t0, t1, sorted, lane, pairs, cands);
     if (A.stats) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
@@ -1605,7 +1615,7 @@ int jt_b_cells(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_
                int64_t npart, const int64_t* d_cprefix, int nbox, int64_t ncells, const jt_cell_bufs& cb,
                int order, int ngrid, int parts, float kick_frac, unsigned long long* stats,
                unsigned* d_err, cudaStream_t st, cudaEvent_t ev_walk0, cudaEvent_t ev_walk1, bool screened,
-               const float4* pmacc)
+               const float4* pmacc, bool count_pairs)
 {
     cudaEventRecord(ev_walk0, st);   // both recorded on every path (no stale events)
     if (npart <= 0) {
@@ -1641,10 +1651,12 @@ int jt_b_cells(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_
         k_cell_scatter<<<gp, 256, 0, st>>>(A, npart);
         const unsigned gw = (unsigned)((ncells + kWarps - 1) / kWarps);
         cudaEventRecord(ev_walk0, st);
-#define JT_CELL_LAUNCH(O, N)                                                         \
-    do {                                                                             \
-        if (screened) k_walk_cell<O, N, true><<<gw, kWarps * 32, 0, st>>>(A, ncells);  \
-        else k_walk_cell<O, N, false><<<gw, kWarps * 32, 0, st>>>(A, ncells);          \
+#define JT_CELL_LAUNCH(O, N)                                                                    \
+    do {                                                                                        \
+        if (screened && count_pairs) k_walk_cell<O, N, true, true><<<gw, kWarps * 32, 0, st>>>(A, ncells);   \
+        else if (screened) k_walk_cell<O, N, true, false><<<gw, kWarps * 32, 0, st>>>(A, ncells);            \
+        else if (count_pairs) k_walk_cell<O, N, false, true><<<gw, kWarps * 32, 0, st>>>(A, ncells);         \
+        else k_walk_cell<O, N, false, false><<<gw, kWarps * 32, 0, st>>>(A, ncells);                         \
     } while (0)
         if (order == 4 && ngrid == 2) JT_CELL_LAUNCH(4, 2);
         else if (order == 4 && ngrid == 1) JT_CELL_LAUNCH(4, 1);

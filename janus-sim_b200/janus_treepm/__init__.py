@@ -54,7 +54,8 @@ EXPORTED = [
     "jt_batch_set_screening", "jt_step_host", "jt_batch_prepare", "jt_config_short_cut",
     "jt_expansion_create", "jt_expansion_destroy", "jt_expansion_info", "jt_expansion_at_time",
     "jt_expansion_at_redshift", "jt_expansion_state_at_mu", "jt_expansion_calibrate",
-    "jt_expansion_phi_factors", "jt_server_get_timings",
+    "jt_expansion_phi_factors", "jt_server_get_timings", "jt_set_counters", "jt_batch_set_counters",
+    "jt_server_set_counters",
 ]
 JT_JOB_QUEUED, JT_JOB_RESIDENT, JT_JOB_DONE = 0, 1, 2
 JT_STATIC_SORT_MAX = 262144
@@ -349,6 +350,9 @@ def library():
     L.jt_server_get_state.argtypes = [H, C.c_int, fp, fp, fp, fp]
     L.jt_server_stats.argtypes = [H, C.POINTER(jt_serve_stats)]
     L.jt_server_get_timings.argtypes = [H, C.POINTER(jt_timings)]
+    L.jt_set_counters.argtypes = [H, C.c_int]
+    L.jt_batch_set_counters.argtypes = [H, C.c_int]
+    L.jt_server_set_counters.argtypes = [H, C.c_int]
     L.jt_server_job_need.argtypes = [C.POINTER(jt_config), C.c_size_t, C.c_size_t, C.POINTER(C.c_size_t)]
     for name in EXPORTED:
         if name not in ("jt_destroy", "jt_strerror", "jt_version", "jt_batch_destroy",
@@ -512,6 +516,12 @@ class Solver:
         mode (Batch.set_screening)."""
         _check(library().jt_set_screening(self._h, lambda_0, z), "jt_set_screening")
 
+    def set_counters(self, on):
+        """Pair counters (a diagnostic, off by default): the near-field cell
+        walk counts its pairs inside r_cut into timings()'s
+        pair_interactions, at about 5 % of the walk's time."""
+        _check(library().jt_set_counters(self._h, 1 if on else 0), "jt_set_counters")
+
     def step(self, dt, hubble=0.0, dtau_per_dt=1.0, nsteps=1):
         _check(library().jt_step(self._h, dt, hubble, dtau_per_dt, nsteps), "jt_step")
 
@@ -642,6 +652,10 @@ class Batch:
     def set_graphs(self, on):
         """Replay each batched step as a CUDA graph (captured per set of boxes)."""
         _check(library().jt_batch_set_graphs(self._b, 1 if on else 0), "jt_batch_set_graphs")
+
+    def set_counters(self, on):
+        """Pair counters of the batch's passes (Solver.set_counters)."""
+        _check(library().jt_batch_set_counters(self._b, 1 if on else 0), "jt_batch_set_counters")
 
     def trim(self):
         """Release the per-pass scratch pools (they regrow on the next pass)."""
@@ -853,6 +867,10 @@ class Server:
         st = jt_serve_stats()
         _check(library().jt_server_stats(self._s, C.byref(st)), "jt_server_stats")
         return {k: getattr(st, k) for k, _ in jt_serve_stats._fields_}
+
+    def set_counters(self, on):
+        """Pair counters of the server's batched steps (Solver.set_counters)."""
+        _check(library().jt_server_set_counters(self._s, 1 if on else 0), "jt_server_set_counters")
 
     def timings(self):
         """Stage times and counts of all batched steps so far, summed."""

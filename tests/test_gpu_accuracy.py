@@ -58,6 +58,7 @@ def test_clustered_accuracy_theta_sweep():
     for theta in (0.3, 0.5, 0.7):
         s = J.Solver(J.Config(box_L=L, pm_grid=M, theta=theta, softening=eps, r_s=r_s, r_cut=r_cut,
                               mu=19.0, G_mass_plus=1e-3, mode=J.JT_ACCURATE))
+        s.set_counters(True)   # the pair counts are reported
         s.set_state(pp, None, pm, None)
         sp, sm = s.accel_part(J.JT_PART_SHORT)
         short = np.concatenate([sp, sm])[idx]

@@ -96,6 +96,7 @@ def test_gpu_oracle_matches_cpu_oracle():
 
 def _engine(J, cfg, pp, pm, idx):
     s = J.Solver(cfg)
+    s.set_counters(True)   # the pair counts are reported
     s.set_state(pp, None, pm, None)
     ap, am = s.accel()
     t = s.timings()

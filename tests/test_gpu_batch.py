@@ -66,8 +66,31 @@ def _cmp(a, b, tol):
     assert err <= tol * rms, (err, rms)
 
 
+def test_pair_counters_leave_the_forces_unchanged():
+    """The cell walk's pair counters (a diagnostic, off by default) leave the
+    forces as they are, to the rounding of the summation order (neither the
+    cell list's order, filled by atomics, nor the deposit's float reductions
+    are reproducible bit for bit between runs); with them off the cell walk's
+    pairs are not counted (every target of this uniform box takes the cell
+    walk)."""
+    cfg, pp, vp, pm, vm = make_box(*BOXES[0])
+    out = []
+    for on in (False, True):
+        s = J.Solver(cfg)
+        s.set_counters(on)
+        s.set_state(pp, vp, pm, vm)
+        a = s.accel()
+        out.append((a, s.timings()))
+        s.close()
+    (a0, t0), (a1, t1) = out
+    _cmp(a0[0], a1[0].astype(np.float64), 1e-5)
+    _cmp(a0[1], a1[1].astype(np.float64), 1e-5)
+    assert t1["pair_interactions"] > 0 and t0["pair_interactions"] == 0, (t0, t1)
+
+
 def test_forces_same_alone_and_in_the_mix():
     B = J.Batch()
+    B.set_counters(True)
     ids = []
     for box in BOXES:
         cfg, pp, vp, pm, vm = make_box(*box)
@@ -247,6 +270,7 @@ def test_cell_walk_matches_the_tree_walk():
         os.environ["JT_WALK_CELLS"] = cells
         try:
             B = J.Batch()
+            B.set_counters(True)
             ids = []
             # the third box: r_cut = 8 in L = 20, 2 cells per axis
             for k, (L, M, n, rc) in enumerate(((60.0, 32, 20, 0.0), (40.0, 64, 16, 0.0), (20.0, 16, 8, 8.0))):

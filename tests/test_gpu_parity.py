@@ -210,6 +210,35 @@ def test_accurate_matches_exact_split_model(n, M, L, mu):
     s.close()
 
 
+def test_cell_walk_wide_cut_without_softening():
+    """A cut past 16 r_s, where the pair table ends (the split factor is below
+    1e-27 there), and zero softening: the cell walk bounds its cut and its
+    table index instead of clamping each pair's, and still matches the exact
+    split model (5 cells per axis of 33 particles: every target takes the cell
+    walk)."""
+    J, O = _mods()
+    n, M, L, mu = 2048, 128, 64.0, 19.0
+    pp = _uniform(n, L, 21)
+    pm = _uniform(n, L, 22)
+    r_s = 1.25 * L / M
+    r_cut = 20.0 * r_s
+    s = J.Solver(J.Config(box_L=L, pm_grid=M, theta=0.5, softening=0.0, r_s=r_s, r_cut=r_cut,
+                          mu=mu, G_mass_plus=1.0, mode=J.JT_ACCURATE))
+    s.set_counters(True)
+    s.set_state(pp, None, pm, None)
+    ap, am = s.accel()
+    t = s.timings()
+    s.close()
+    assert t["cellwalk_ms"] > 0.0 and t["node_interactions"] == 0, t
+    pos = np.concatenate([pp, pm]).astype(np.float64)
+    mass = np.concatenate([np.full(n, 1.0), np.full(n, mu)])
+    sg = np.concatenate([np.ones(n, np.int8), -np.ones(n, np.int8)])
+    ex = O.ewald_forces(pos, mass, sg, L, r_s, 0.0, r_trunc=r_cut)
+    rel = _rel(np.concatenate([ap, am]), ex)
+    p50, p99 = np.percentile(rel, [50, 99])
+    assert p99 <= 3e-3 and p50 <= 2e-4, (p50, p99)
+
+
 def test_minus_response_is_exact_sign_flip():
     J, O = _mods()
     n, L = 3000, 40.0

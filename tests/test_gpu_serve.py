@@ -186,6 +186,7 @@ def test_server_stage_timings_sum_the_batched_steps():
     request's pairs are counted."""
     specs = [job_spec(sd) for sd in (401, 402, 403)]
     S = J.Server(8 * GiB)
+    S.set_counters(True)
     ids = [S.add_job(cfg, *st, steps=2, dt=dt, hubble=hub) for cfg, st, dt, hub in specs]
     for _ in range(2):
         for j in ids:
