@@ -227,7 +227,7 @@ __device__ __forceinline__ int eval_dense(const float4* __restrict__ cand, float
         const float r2 = dx * dx + dy * dy + dz * dz;
         const bool in = valid && r2 > 0.0f && r2 < P.rc2;
         const float y = (r2 + P.eps2) * P.c2;
-        const unsigned k = min((__float_as_uint(y) >> 14) - JT_LTAB_BASE, (unsigned)JT_LTAB_N - 1u);
+        const unsigned k = (__float_as_uint(y) >> 14) - JT_LTAB_BASE;   // in range inside the cut
         float2 ab = make_float2(0.f, 0.f);
         if (in) ab = __ldg(&tab[k]);
         const float g = fac * fmaf(ab.y, y, ab.x);
@@ -300,7 +300,7 @@ __device__ __forceinline__ int eval_chunk(WalkWarpSmem& S, int cnt, int lane, fl
             hits++;
             // fac carries s_i s_j m_j c^3: the force is fac G(y) d
             const float y = (r2 + P.eps2) * P.c2;
-            const unsigned k = min((__float_as_uint(y) >> 14) - JT_LTAB_BASE, (unsigned)JT_LTAB_N - 1u);
+            const unsigned k = (__float_as_uint(y) >> 14) - JT_LTAB_BASE;   // in range inside the cut
             const float2 ab = __ldg(&tab[k]);
             const float g = fac * fmaf(ab.y, y, ab.x);
             a.x += g * dx;
@@ -696,9 +696,15 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_walk_acc(WalkArgs A)
     const jt_box_dev& B = A.boxes[SG.box];
     const int s = SG.species;
     jt_walk_params P;
-    P.L = B.L; P.halfL = B.halfL; P.theta2 = B.theta2; P.rc2 = B.rc2; P.rc = sqrtf(B.rc2);
-    P.eps2 = B.eps2; P.c = B.c;
+    P.L = B.L; P.halfL = B.halfL; P.theta2 = B.theta2; P.c = B.c;
     P.c2 = B.c * B.c;
+    // the pair table covers y = (r^2 + eps^2) c^2 in [2^-32, 2^6): a
+    // softening below 2^-16 (2 r_s) is raised to it, and the cut is bounded
+    // by y < 64 (16 r_s without softening; the split factor is below 1e-27
+    // there), so that no pair's table index needs a clamp
+    P.eps2 = fmaxf(B.eps2, 2.3285392e-10f / P.c2);
+    P.rc2 = fminf(B.rc2, 64.0f * 0.99999f / P.c2 - P.eps2);
+    P.rc = sqrtf(P.rc2);
     // particle masses times c^3, the scale of the pair table's G(y)
     P.mass[0] = B.mass[0] * P.c2 * B.c; P.mass[1] = B.mass[1] * P.c2 * B.c;
     // candidate prefilter margins: 8 ulp of the largest coordinate on the
@@ -1378,30 +1384,32 @@ struct CellWarpSmem {
 // d = 0) adds nothing and is counted as a hit, which the caller removes.
 // SCR: opposite-species pairs read the box's Yukawa table yt.
 // CNT: count the lane's pairs inside the cut (the pair counters; one
-// instruction per candidate, off unless the caller asks for them).  No
-// clamp on the table index: the caller bounds ye >= 2^-32 and
-// rc2 c2 + ye < 64, so that every y of a lane inside the cut indexes the
-// table ([2^-32, 2^6)); lanes outside it load nothing.
+// instruction per candidate, off unless the caller asks for them).
+// Positions come scaled by c = 1 / (2 r_s), so that y = |d|^2 + ye directly
+// (ye = eps^2 c^2) and the pair is inside the cut for y < yc.  No clamp on
+// the table index: the caller bounds ye >= 2^-32 and yc < 64, so that every
+// y of a lane inside the cut indexes the table ([2^-32, 2^6)); lanes outside
+// it load nothing.
 template <bool SCR, bool CNT>
 __device__ __forceinline__ unsigned cell_chunk(const float4* __restrict__ cand, int cnt, const float4& p, float si,
-                                               float rc2, float c2, float ye, Acc3& a,
-                                               const float2* __restrict__ yt)
+                                               float yc, float ye, Acc3& a, const float2* __restrict__ yt)
 {
     unsigned hits = 0;
 #pragma unroll 4
     for (int j = 0; j < cnt; j++) {
         const float4 q = cand[j];
         const float dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
-        const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-        const float y = fmaf(r2, c2, ye);
+        const float y = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, ye)));
         const unsigned k = (__float_as_uint(y) >> 14) - JT_LTAB_BASE;
         const float2* __restrict__ tb = (SCR && si * q.w < 0.0f) ? yt : g_ltab;
-        const bool in = r2 < rc2;
+        const bool in = y < yc;
         // only lanes inside the cut read the table (a predicated load: the
-        // ~3/4 of dense candidates outside it issue no L1 request)
-        float2 ab = make_float2(0.f, 0.f);
+        // ~3/4 of dense candidates outside it issue no L1 request), and the
+        // others' weight is selected to zero (one select instead of zeroing
+        // the load's registers)
+        float2 ab;
         if (in) ab = __ldg(&tb[k]);
-        const float w = q.w * fmaf(ab.y, y, ab.x);
+        const float w = in ? q.w * fmaf(ab.y, y, ab.x) : 0.0f;
         if (CNT) hits += in ? 1u : 0u;
         a.x = fmaf(w, dx, a.x);
         a.y = fmaf(w, dy, a.y);
@@ -1429,8 +1437,8 @@ __device__ __forceinline__ void cell_batch(const CellArgs& A, const jt_box_dev& 
     // is raised to it, and the cut is bounded by y < 64 (16 r_s without
     // softening), where the split factor is below 1e-27: the table's last
     // entry, zero, held every y past it
-    const float c2 = B.c * B.c, ye = fmaxf(B.eps2 * c2, 2.3283064365386963e-10f);
-    const float rc2 = fminf(B.rc2, (64.0f * 0.99999f - ye) / c2);
+    const float cc = B.c, c2 = cc * cc, ye = fmaxf(B.eps2 * c2, 2.3283064365386963e-10f);
+    const float yc = fminf(fmaf(B.rc2, c2, ye), 64.0f * 0.99999f);
     const float slack = B.halfL * 9.5367431640625e-7f, rc2_keep = B.rc2 * 1.00001f;
     const float2* __restrict__ yt = (SCR && B.ytab) ? B.ytab : g_ltab;
     const int pos_in_cell = base + lane;
@@ -1446,6 +1454,7 @@ __device__ __forceinline__ void cell_batch(const CellArgs& A, const jt_box_dev& 
                 ghz = 0.5f * (hiz - loz) + slack;
     Acc3 near = {0.f, 0.f, 0.f};
     if (A.parts & 2) {
+        const float4 ps = make_float4(p.x * cc, p.y * cc, p.z * cc, p.w);
         unsigned hits = 0;
         int nc = 0;
         for (int nbr = 0; nbr < 27; nbr++) {
@@ -1463,11 +1472,11 @@ __device__ __forceinline__ void cell_batch(const CellArgs& A, const jt_box_dev& 
                     keep = gx * gx + gy * gy + gz * gz <= rc2_keep;
                 }
                 const unsigned km = __ballot_sync(0xffffffffu, keep);
-                if (keep) S.cand[nc + __popc(km & lt)] = c;
+                if (keep) S.cand[nc + __popc(km & lt)] = make_float4(c.x * cc, c.y * cc, c.z * cc, c.w);
                 nc += __popc(km);
                 __syncwarp();
                 if (nc >= 32) {
-                    hits += cell_chunk<SCR, CNT>(S.cand, 32, p, si, rc2, c2, ye, near, yt);
+                    hits += cell_chunk<SCR, CNT>(S.cand, 32, ps, si, yc, ye, near, yt);
                     cands += 32;
                     __syncwarp();
                     const float4 t2 = S.cand[32 + lane];
@@ -1479,13 +1488,13 @@ __device__ __forceinline__ void cell_batch(const CellArgs& A, const jt_box_dev& 
             }
         }
         if (nc > 0) {
-            hits += cell_chunk<SCR, CNT>(S.cand, nc, p, si, rc2, c2, ye, near, yt);
+            hits += cell_chunk<SCR, CNT>(S.cand, nc, ps, si, yc, ye, near, yt);
             cands += nc;
         }
         __syncwarp();
         // the target met itself once (r = 0 < r_cut); an empty slot counts nothing
         if (CNT && valid) pairs += hits - 1u;
-        const float sc = si * c2 * B.c;
+        const float sc = si * c2;   // positions scaled by c: sum w (c d)
         near.x *= sc;
         near.y *= sc;
         near.z *= sc;
