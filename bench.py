@@ -61,13 +61,13 @@ ACCURACY_B200 = {
     "source": "tests/test_gpu_accuracy_full.py on B200 (recorded, not re-run by the bench)",
     "metric": "p50, p99 of |a - a_ref| / |a_ref| over 65,536 targets",
     "production_2x224": {
-        "cut_tail_440ppm_vs_full": [3.04e-05, 5.54e-04],
-        "cut_4.5rs_vs_split": [2.24e-05, 4.14e-04],
-        "cut_4.5rs_vs_full": [1.46e-03, 2.14e-02],
+        "cut_tail_440ppm_vs_full": [3.28e-05, 5.64e-04],
+        "cut_4.5rs_vs_split": [2.48e-05, 4.26e-04],
+        "cut_4.5rs_vs_full": [1.46e-03, 2.15e-02],
     },
     "clustered_2x128": {
         "theta_0.3_vs_split": [3.10e-06, 2.03e-04], "theta_0.3_tail_440ppm_vs_full": [1.23e-05, 1.61e-04],
-        "theta_0.5_vs_split": [2.81e-05, 6.71e-04], "theta_0.5_tail_440ppm_vs_full": [4.02e-05, 3.75e-04],
+        "theta_0.5_vs_split": [2.81e-05, 6.72e-04], "theta_0.5_tail_440ppm_vs_full": [4.02e-05, 3.75e-04],
         "theta_0.7_vs_split": [2.08e-04, 2.36e-03], "theta_0.7_tail_440ppm_vs_full": [2.09e-04, 2.13e-03],
     },
     "small_2x32_rcompat_vs_reference_kernels": [2.60e-07, 1.69e-06],
