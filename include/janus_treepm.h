@@ -246,7 +246,9 @@ const char* jt_strerror(int code);
 int  jt_fp32_peak(int iters, double* tflops);
 /* The walk's launch shapes picked by its autotuner so far (one entry per
  * device and size class: register budget as blocks per SM, leaf-bucket
- * size), as text.  No counterpart in the reference. */
+ * size), and the near-field cells per axis timed fastest on the first
+ * force-only pass of each box of 2^22 particles or more (the default
+ * L / r_cut and the one kept), as text.  No counterpart in the reference. */
 int  jt_walk_tuning(char* buf, size_t len);
 /* ---- in-step diagnostics (device, FP64 accumulation) ----
  * segregation: |COM+ - COM-| / L, the reference's segregation()

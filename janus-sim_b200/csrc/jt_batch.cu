@@ -24,7 +24,9 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <new>
+#include <string>
 #include <vector>
 
 namespace {
@@ -559,11 +561,15 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
             const double q = c.box_L / (rcut * 1.0001);
             int nbc = q >= 256.0 ? 256 : (int)q;
             if (nbc >= 3) d.nb = nbc;
+            if (d.nb && b->cell_nb >= 3 && b->cell_nb < d.nb) d.nb = b->cell_nb;   // timed (tune_cells)
         }
-        // a widened cut scales every neighbourhood's count by (cut / r_cut)^3
+        // a widened cut scales every neighbourhood's count by (cut / r_cut)^3,
+        // and cells wider than the default by (default nb / nb)^3
         {
             const double w = rcut / c.r_cut;
-            d.cell_kmax = (int)std::min(1.0e6, JT_CELL_KMAX * std::max(1.0, w * w * w));
+            const double q = d.nb ? c.box_L / (rcut * 1.0001) : 0.0;
+            const double v = d.nb ? std::min(256.0, std::floor(q)) / d.nb : 1.0;
+            d.cell_kmax = (int)std::min(1.0e6, JT_CELL_KMAX * std::max(1.0, w * w * w) * v * v * v);
         }
         d.cell_inv = d.nb ? (float)(d.nb / c.box_L) : 0.0f;
         P.cprefix.push_back(P.cprefix.back() + (int64_t)d.nb * d.nb * d.nb);
@@ -671,6 +677,86 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
     return JT_OK;
 }
 
+// The cell walk's cost depends on how a cell's targets fill batches of 32
+// (a lattice whose points per cell are a whole number per axis fills them
+// evenly), which no model of the mean count predicts: the first force-only
+// pass of a box of kCellTuneMin particles or more, alone in its pass, times
+// the cell walk at every nb from the default (side >= cut) down to 0.8 of it
+// and keeps the fastest for the box (nb with targets flagged for the tree
+// walk are not taken: they would time less work).  2x224^3 at cut 6 r_s:
+// 68 -> 56 cells per axis (4 lattice points, 128 particles), cell walk
+// 4 % faster.
+constexpr int64_t kCellTuneMin = (int64_t)1 << 22;
+
+std::mutex g_cell_tune_mu;
+std::string g_cell_tune_text;   // one entry per timed box (jt_cell_tuning_text)
+
+int tune_cells(jt_batch* B, Plan& P, int nseg, int parts, const float4* pmacc)
+{
+    jt_box_state* bs = B->boxes[P.ids[0]];
+    jt_box_dev& d = P.bx[0];
+    if (bs->cell_nb != 0 || d.nb < 8 || bs->n[0] + bs->n[1] < kCellTuneMin || P.screened || nseg > 2) return JT_OK;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(B->st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return JT_OK;
+    cudaStream_t st = B->st;
+    const int nmax = d.nb, kmax0 = d.cell_kmax, nmin = std::max(3, (int)std::ceil(0.8 * nmax));
+    jt_cell_bufs cb = {B->ccount.p, B->cstart.p, B->cbsum.p, B->ccell.p, B->cslot.p,
+                       B->cpos.p, B->cid.p, B->tflag.p, B->csegflag.p};
+    cudaEvent_t e0, e1;
+    JT_CU(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return JT_ECUDA;
+    }
+    auto set_nb = [&](int nb) -> int {
+        const double v = (double)nmax / nb;
+        d.nb = nb;
+        d.cell_inv = (float)(nb / (double)d.L);
+        d.cell_kmax = (int)std::min(1.0e6, kmax0 * v * v * v);
+        P.cprefix[1] = (int64_t)nb * nb * nb;
+        P.ncells = P.cprefix[1];
+        if (cudaMemcpyAsync((void*)P.d_bx, &d, sizeof(jt_box_dev), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+            cudaMemcpyAsync((void*)(P.d_cp + 1), &P.cprefix[1], sizeof(int64_t), cudaMemcpyHostToDevice, st) !=
+                cudaSuccess)
+            return JT_ECUDA;
+        return JT_OK;
+    };
+    int r = JT_OK, best = nmax;
+    float best_ms = 0.f;
+    for (int nb = nmax; nb >= nmin && r == JT_OK; nb--) {
+        r = set_nb(nb);
+        if (r == JT_OK)
+            r = jt_b_cells(P.d_post, P.d_bx, P.d_pp, nseg, P.npart, P.d_cp, 1, P.ncells, cb, B->order, B->ngrid,
+                           parts, 0.0f, nullptr, B->d_err, st, e0, e1, false, pmacc, false);
+        int flag[2] = {0, 0};
+        if (r == JT_OK && (cudaMemcpyAsync(flag, B->csegflag.p, sizeof(int) * (size_t)nseg, cudaMemcpyDeviceToHost,
+                                           st) != cudaSuccess ||
+                           cudaStreamSynchronize(st) != cudaSuccess))
+            r = JT_ECUDA;
+        float ms = 0.f;
+        if (r == JT_OK && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) r = JT_ECUDA;
+        if (r != JT_OK) break;
+        if (nb == nmax) {
+            best_ms = ms;
+            if (flag[0] || flag[1]) break;   // crowded at the default already: keep it
+        } else if (!flag[0] && !flag[1] && ms < best_ms) {
+            best = nb;
+            best_ms = ms;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (r != JT_OK) return r;
+    bs->cell_nb = best;
+    {
+        std::lock_guard<std::mutex> lock(g_cell_tune_mu);
+        if (g_cell_tune_text.size() < 4096)
+            g_cell_tune_text += "cells " + std::to_string(bs->n[0] + bs->n[1]) + " particles: " +
+                                std::to_string(nmax) + " -> " + std::to_string(best) + " per axis; ";
+    }
+    return set_nb(best);
+}
+
 // One force pass over the plan's boxes; afterwards every box's state sits in
 // its former b-buffers (pointers swapped here and in the plan).
 int force_pass(jt_batch* B, Plan& P, int parts, float kick_frac)
@@ -739,6 +825,8 @@ int force_pass(jt_batch* B, Plan& P, int parts, float kick_frac)
         cudaEventRecord(B->ev[8], st);
         cudaEventRecord(B->ev[9], st);
     } else {
+        if (kick_frac == 0.0f && nbox == 1 && P.ncells > 0 && (parts & JT_PART_SHORT))
+            JT_TRY(tune_cells(B, P, nseg, parts, pmacc));
         jt_cell_bufs cb = {B->ccount.p, B->cstart.p, B->cbsum.p, B->ccell.p, B->cslot.p,
                            B->cpos.p, B->cid.p, B->tflag.p, B->csegflag.p};
         JT_TRY(jt_b_cells(P.d_post, P.d_bx, P.d_pp, nseg, P.npart, P.d_cp, nbox, P.ncells, cb, B->order,
@@ -1667,4 +1755,10 @@ int jtb_reserve(jt_batch* B, size_t bytes)
     JT_CU(cudaFreeAsync(p, B->st));
     JT_CU(cudaStreamSynchronize(B->st));
     return JT_OK;
+}
+
+std::string jt_cell_tuning_text()
+{
+    std::lock_guard<std::mutex> lock(g_cell_tune_mu);
+    return g_cell_tune_text;
 }

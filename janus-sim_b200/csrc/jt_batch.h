@@ -22,6 +22,9 @@ struct jt_box_state {
     float2* ytab = nullptr;
     int M = 0, order = 3, ngrid = 2;
     size_t bytes = 0;            // device bytes held by this box
+    // near-field cells per axis that the box's first force-only pass timed
+    // fastest (0: not timed; the default L / r_cut is used)
+    int cell_nb = 0;
 };
 
 // Per-box step arguments of a batched force pass (kick fused into the walk).

@@ -22,6 +22,8 @@
 #include <cufft.h>
 #include <stdint.h>
 
+#include <string>
+
 #include "../../include/janus_treepm.h"
 
 #define JT_WARPS_PER_BLOCK 4
@@ -352,6 +354,10 @@ int jt_b_cells(const jt_seg_dev* d_segs, const jt_box_dev* d_boxes, const int64_
                unsigned* d_err, cudaStream_t st, cudaEvent_t ev_walk0, cudaEvent_t ev_walk1,
                bool screened = false, const float4* pmacc = nullptr, bool count_pairs = true);
 int jt_cell_scan_blocks(int64_t ncells);
+// The cell counts per axis the batches' first force-only passes timed
+// (jt_batch.cu), as text for jt_walk_tuning: "cells <n> particles: <default>
+// -> <nb> per axis; ".
+std::string jt_cell_tuning_text();
 // Yukawa split factor S_Y(y) on the walk's table grid (y = (r_p / 2 r_s)^2
 // over [0, 16], JT_STAB_N (value, next - value) entries) for b = kappa r_s.
 // A pass with a screened box (jt_box_dev.ytab) runs the walks' screened

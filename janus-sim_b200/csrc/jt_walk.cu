@@ -1204,6 +1204,7 @@ extern "C" int jt_walk_tuning(char* buf, size_t len)
                    ": minblocks " + std::to_string(w.minb) + " bucket " + std::to_string(w.bkt) + "; ";
         }
     }
+    out += jt_cell_tuning_text();
     std::snprintf(buf, len, "%s", out.c_str());
     return JT_OK;
 }
