@@ -359,6 +359,50 @@ def run_ensemble(J, ics, n_boxes, steps, warmup, H, dt):
     }
 
 
+def run_ensemble_sharded(J, ics, n_boxes, steps, warmup, H, dt, rank, ws):
+    """The ensemble sharded across the ranks (janus_treepm.shard): each rank
+    steps its share of the boxes (a cost-balanced partition every rank
+    computes alike) as one batch on its GPU, with no exchange; the device
+    time is the max over ranks, the value all boxes' particle-steps over it
+    (strong scaling: the total work stays fixed as N grows), and rank 0
+    gathers each rank's boxes, particles and time.  Every rank calls it."""
+    import torch
+    from janus_treepm import shard
+    boxes = ensemble_boxes(n_boxes)
+    costs = [shard.box_cost(2 * bx["n"] ** 3, bx["M"]) for bx in boxes]
+    shares = shard.partition(costs, ws)
+    mine = shares[rank]
+    n_part = sum(2 * bx["n"] ** 3 for bx in boxes)
+    dev = 0.0
+    if mine:
+        B = J.Batch()
+        ids = [B.add(box_config(J, boxes[i]), *ics.zeldovich_lattice(boxes[i]["n"], boxes[i]["L"],
+                                                                       seed=boxes[i]["seed"]))
+               for i in mine]
+        for _ in range(warmup):
+            B.step(ids, dt, H, 1.0, 1)
+        torch.cuda.synchronize()
+        for _ in range(steps):
+            B.step(ids, dt, H, 1.0, 1)
+            dev += B.timings()["total_ms"]
+        torch.cuda.synchronize()
+        B.close()
+    dev_max = max_over_ranks(dev, ws, "cuda")
+    metrics = shard.gather({"rank": rank, "boxes": len(mine),
+                            "particles": sum(2 * boxes[i]["n"] ** 3 for i in mine),
+                            "ms_per_step": dev / steps}, ws)
+    if rank != 0:
+        return None
+    ld = shard.loads(costs, shares)
+    return {
+        "workload": f"{n_boxes} boxes, n per species log-uniform 16..96 ({n_part} particles), "
+                    f"L U(50,300), PM 32..256, mu U(5,30), sharded by box over {ws} ranks",
+        "value": n_part * steps / (dev_max * 1e-3), "unit": UNIT, "ms_per_step": dev_max / steps,
+        "scaling": "strong", "ranks": ws, "per_rank": metrics,
+        "cost_max_over_mean": max(ld) / (sum(ld) / len(ld)), "steps": steps,
+    }
+
+
 def serving_jobs(J, ics, n_small, n_big, H, dt, seed=11):
     """The serving workload's jobs: n_small boxes sized as the ensemble's plus
     n_big boxes of 2x256^3 (L = 300 Mpc, PM 512^3).  The big jobs share one
@@ -691,10 +735,13 @@ def run_ours(args, ws, rank, local):
     # the headline handle's memory back to the device before the other legs
     # (the serving loop reserves a 150 GiB budget)
     s.close()
+    ensemble = None
+    if ws > 1 and args.ensemble_boxes > 0:   # every rank: the boxes shard across them
+        ensemble = run_ensemble_sharded(J, ics, args.ensemble_boxes, args.ensemble_steps, 3, H, w["dt"],
+                                        rank, ws)
     ref_gpu = None
     if rank == 0 and ws == 1 and not args.no_reference_gpu:
         ref_gpu = reference_gpu_step(args.n_side, args.grid)
-    ensemble = None
     serving = None
     clustered = None
     if rank == 0 and ws == 1 and args.clustered_steps > 0:
