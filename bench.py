@@ -403,6 +403,38 @@ def run_ensemble_sharded(J, ics, n_boxes, steps, warmup, H, dt, rank, ws):
     }
 
 
+def run_serving_sharded(J, ics, n_small, n_big, steps, H, dt, rank, ws, budget_gb=150.0):
+    """The serving workload's jobs sharded across the ranks
+    (janus_treepm.shard, the cost of a job from its particles and grid):
+    each rank serves its share on its GPU as a saturated run (every request
+    at t = 0) under its own budget; the makespan is the max over ranks, and
+    rank 0 gathers each rank's jobs, requests served and makespan.  Every
+    rank calls it."""
+    from janus_treepm import shard
+    jobs = serving_jobs(J, ics, n_small, n_big, H, dt)
+    costs = [shard.box_cost(p, cfg.pm_grid) for cfg, _, p in jobs]
+    shares = shard.partition(costs, ws)
+    mine = [jobs[i] for i in shares[rank]]
+    wall, served = 0.0, 0
+    if mine:
+        wall, st = serve_once(J, mine, steps, None, H, dt, budget_gb, seed=11)
+        served = int(st["requests_served"])
+    wall_max = max_over_ranks(wall, ws, "cuda")
+    metrics = shard.gather({"rank": rank, "jobs": len(mine), "requests": served, "makespan_s": wall}, ws)
+    if rank != 0:
+        return None
+    total_ps = float(sum(p for _, _, p in jobs) * steps)
+    ld = shard.loads(costs, shares)
+    return {
+        "workload": f"{n_small} ensemble-style jobs + {n_big} jobs of 2x256^3 (L=300, PM 512^3), "
+                    f"{steps} steps each, {budget_gb:g} GB HBM budget per rank, sharded by job over "
+                    f"{ws} ranks, saturated (every request at t = 0)",
+        "particle_steps": total_ps, "saturated_value": total_ps / wall_max, "unit": UNIT,
+        "makespan_s": wall_max, "scaling": "strong", "ranks": ws, "per_rank": metrics,
+        "cost_max_over_mean": max(ld) / (sum(ld) / len(ld)),
+    }
+
+
 def serving_jobs(J, ics, n_small, n_big, H, dt, seed=11):
     """The serving workload's jobs: n_small boxes sized as the ensemble's plus
     n_big boxes of 2x256^3 (L = 300 Mpc, PM 512^3).  The big jobs share one
@@ -736,13 +768,16 @@ def run_ours(args, ws, rank, local):
     # (the serving loop reserves a 150 GiB budget)
     s.close()
     ensemble = None
+    serving = None
     if ws > 1 and args.ensemble_boxes > 0:   # every rank: the boxes shard across them
         ensemble = run_ensemble_sharded(J, ics, args.ensemble_boxes, args.ensemble_steps, 3, H, w["dt"],
                                         rank, ws)
+    if ws > 1 and args.serve_jobs > 0:       # every rank: the jobs shard across them
+        serving = run_serving_sharded(J, ics, args.serve_jobs, args.serve_big, args.serve_steps, H, w["dt"],
+                                      rank, ws)
     ref_gpu = None
     if rank == 0 and ws == 1 and not args.no_reference_gpu:
         ref_gpu = reference_gpu_step(args.n_side, args.grid)
-    serving = None
     clustered = None
     if rank == 0 and ws == 1 and args.clustered_steps > 0:
         clustered = run_clustered(J, ics, args.clustered_steps, 3, H, w["dt"], args.cut_tail_ppm)

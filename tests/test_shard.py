@@ -131,3 +131,16 @@ def test_sharded_ensemble_leg_on_one_rank():
     assert r["per_rank"][0]["particles"] == n_part
     assert r["value"] > 0 and r["value"] == pytest.approx(n_part / (r["ms_per_step"] * 1e-3))
     assert r["cost_max_over_mean"] == 1.0
+
+
+@pytest.mark.gpu
+def test_sharded_serving_leg_on_one_rank():
+    """bench.run_serving_sharded on one GPU as rank 0 of 1: every job served
+    for every step."""
+    import bench
+    import janus_treepm as J
+    from janus_treepm import ics
+    w = bench.workload()
+    r = bench.run_serving_sharded(J, ics, 4, 0, 2, 0.07, w["dt"], 0, 1, budget_gb=8.0)
+    assert r["ranks"] == 1 and r["per_rank"][0]["jobs"] == 4 and r["per_rank"][0]["requests"] == 8
+    assert r["saturated_value"] > 0 and r["makespan_s"] > 0
