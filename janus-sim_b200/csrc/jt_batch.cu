@@ -685,7 +685,8 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
 // (the faster of two runs each) and keeps the fastest for the box (nb with
 // targets flagged for the tree walk are not taken: they would time less
 // work).  2x224^3 at cut 6 r_s: 68 -> 56 cells per axis (4 lattice points,
-// 128 particles), cell walk 5 % faster.
+// 128 particles), cell walk 5 % faster.  JT_CELL_TUNE=0 in the environment
+// (read once) keeps the default.
 constexpr int64_t kCellTuneMin = (int64_t)1 << 22;
 
 std::mutex g_cell_tune_mu;
@@ -696,6 +697,11 @@ int tune_cells(jt_batch* B, Plan& P, int nseg, int parts, const float4* pmacc)
     jt_box_state* bs = B->boxes[P.ids[0]];
     jt_box_dev& d = P.bx[0];
     if (bs->cell_nb != 0 || d.nb < 8 || bs->n[0] + bs->n[1] < kCellTuneMin || P.screened || nseg > 2) return JT_OK;
+    static const bool off = [] {
+        const char* e = std::getenv("JT_CELL_TUNE");
+        return e && std::atoi(e) == 0;
+    }();
+    if (off) return JT_OK;   // JT_CELL_TUNE=0: the default cell count
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(B->st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return JT_OK;
     cudaStream_t st = B->st;

@@ -383,3 +383,44 @@ def test_prepared_plans_change_nothing():
             _cmp(x, y, FORCE_TOL)
     A.close()
     P.close()
+
+
+def test_cell_count_autotuner_single_species():
+    """A box of 2^22 particles (one species) takes the cell-count autotuner on
+    its first force pass: the forces agree with the default cell count's to
+    the rounding of the summation order, and jt_walk_tuning reports the box.
+    The default run is a child process (JT_CELL_TUNE=0 is read once)."""
+    import json
+    import os
+    import subprocess
+    import sys
+    n, L, M = 1 << 22, 160.0, 256
+    code = f"""
+import sys, numpy as np
+sys.path.insert(0, {os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), 'janus-sim_b200')!r})
+import janus_treepm as J
+rng = np.random.default_rng(5)
+pp = rng.uniform(-{L} / 2, {L} / 2, ({n}, 3)).astype(np.float32)
+cfg = J.Config(box_L={L}, pm_grid={M}, theta=0.5, softening=0.02, mu=19.0, G_mass_plus=1e-3,
+               mode=J.JT_ACCURATE, cut_tail_ppm=440)
+s = J.Solver(cfg)
+s.set_state(pp, None, np.zeros((0, 3), np.float32), None)
+ap, _ = s.accel_part(J.JT_PART_SHORT)
+np.save(sys.argv[1], ap)
+print(J.walk_tuning())
+"""
+    import tempfile
+    out = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for tune in ("1", "0"):
+            f = os.path.join(tmp, f"a{tune}.npy")
+            env = dict(os.environ, JT_CELL_TUNE=tune)
+            r = subprocess.run([sys.executable, "-c", code, f], env=env, capture_output=True, text=True,
+                               timeout=600)
+            assert r.returncode == 0, r.stderr[-2000:]
+            out[tune] = (np.load(f), r.stdout)
+    a1, a0 = out["1"][0].astype(np.float64), out["0"][0].astype(np.float64)
+    rms = float(np.sqrt(np.mean(np.sum(a0 ** 2, axis=1))))
+    assert np.all(np.isfinite(a1)) and float(np.abs(a1 - a0).max()) <= 1e-4 * rms
+    assert f"cells {n} particles:" in out["1"][1]
+    assert f"cells {n} particles:" not in out["0"][1]
