@@ -220,6 +220,7 @@ struct jt_batch {
     unsigned long long* d_stats = nullptr;
     cudaEvent_t ev[11] = {};            // 8, 9: around the cell walk kernel; 6-10: interpolation
     bool counters = false;              // the cell walk counts its pairs (jt_batch_set_counters)
+    bool cell_tune = true;              // tune_cells may run (jtb_set_cell_tune)
     bool pending = false;               // a pass's events await jtb_finish
     jt_timings tm = {};
     int64_t phase[4] = {0, 0, 0, 0};
@@ -696,7 +697,9 @@ int tune_cells(jt_batch* B, Plan& P, int nseg, int parts, const float4* pmacc)
 {
     jt_box_state* bs = B->boxes[P.ids[0]];
     jt_box_dev& d = P.bx[0];
-    if (bs->cell_nb != 0 || d.nb < 8 || bs->n[0] + bs->n[1] < kCellTuneMin || P.screened || nseg > 2) return JT_OK;
+    if (!B->cell_tune || bs->cell_nb != 0 || d.nb < 8 || bs->n[0] + bs->n[1] < kCellTuneMin || P.screened ||
+        nseg > 2)
+        return JT_OK;
     static const bool off = [] {
         const char* e = std::getenv("JT_CELL_TUNE");
         return e && std::atoi(e) == 0;
@@ -1771,4 +1774,9 @@ std::string jt_cell_tuning_text()
 {
     std::lock_guard<std::mutex> lock(g_cell_tune_mu);
     return g_cell_tune_text;
+}
+
+void jtb_set_cell_tune(jt_batch* B, bool on)
+{
+    if (B) B->cell_tune = on;
 }

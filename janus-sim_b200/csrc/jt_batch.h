@@ -40,6 +40,10 @@ jt_box_state* jtb_box(jt_batch* B, int box_id);
 // the batch's asynchronous-checkpoint state (jt_ckpt.cu), released on destroy
 struct jt_ckpt;
 jt_ckpt** jtb_ckpt_slot(jt_batch* B);
+// Whether the batch's first force-only pass of a large box may time the
+// near-field cell count (tune_cells in jt_batch.cu; on by default).  The
+// server turns it off: a request must not wait for the timing runs.
+void jtb_set_cell_tune(jt_batch* B, bool on);
 void jt_ckpt_release(jt_ckpt* c);
 cudaStream_t jtb_stream(jt_batch* B);
 // Enqueue one force pass (sort, trees, PM, walk) over the listed boxes;

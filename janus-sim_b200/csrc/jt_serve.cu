@@ -338,6 +338,7 @@ int jt_server_create(size_t hbm_budget_bytes, jt_server** out)
         delete S;
         return r;
     }
+    jtb_set_cell_tune(S->B, false);   // no timing runs inside a request's step
     S->budget = hbm_budget_bytes;
     // map the budget once, up front (see the header)
     size_t free_b = 0, total_b = 0;
