@@ -109,25 +109,56 @@ struct Pool {
 int box_order(const jt_config& c) { return c.pm_order == 0 ? 4 : c.pm_order; }
 int box_ngrid(const jt_config& c) { return c.pm_interlace == 2 ? 1 : 2; }
 
-struct Bucket {                 // PM scratch of the boxes with grid M in a pass
-    int M = 0;
-    int cap = 0;                // boxes the arrays hold
-    // z transforms fused with the k-space step (jt_zfft.cu): cuFFT's plans
-    // are 2D, one transform per (x, y) plane; fixed when the bucket is made
-    bool fused = false;
-    bool decided = false;
+// One allocation of a bucket's grid arrays: `slots` boxes, each with its
+// ngrid density grids and spectra and 3 ngrid force spectra and grids.
+struct BucketChunk {
+    int slots = 0;
     float* rho = nullptr;
     float2* rho_k = nullptr;
     float2* force_k = nullptr;
     float* force = nullptr;
     int4* ranges = nullptr;
+    void free_arrays()
+    {
+        dfree(rho); dfree(rho_k); dfree(force_k); dfree(force); dfree(ranges);
+        slots = 0;
+    }
+};
+
+struct Bucket {                 // PM scratch of the boxes with grid M in a pass
+    int M = 0;
+    int cap = 0;                // boxes the chunks hold
+    // z transforms fused with the k-space step (jt_zfft.cu): cuFFT's plans
+    // are 2D, one transform per (x, y) plane; fixed when the bucket is made
+    bool fused = false;
+    bool decided = false;
+    // The grid arrays, in chunks: a pass with more boxes of this grid than
+    // the chunks hold adds one chunk for the missing slots and leaves the
+    // others in place.  (Freeing and allocating the whole bucket at the new
+    // count made the pool map several GB per 512^3 box while the step
+    // waited: up to ~1 s with the device idle when served jobs arrive a few
+    // at a time.)  Slot q of a pass is in the first chunk whose running
+    // count exceeds q; cuFFT's batches never cross a chunk.
+    std::vector<BucketChunk> chunks;
     // batched plans by transform count: r2c[b], c2r[b] transform b grids
     // per execution (at most fft_chunk(M) each, see below)
     std::map<int, cufftHandle> r2c, c2r;
     void free_arrays()
     {
-        dfree(rho); dfree(rho_k); dfree(force_k); dfree(force); dfree(ranges);
+        for (auto& c : chunks) c.free_arrays();
+        chunks.clear();
         cap = 0;
+    }
+    // the chunk holding slot q and q's index in it
+    const BucketChunk& locate(int q, int* i) const
+    {
+        size_t c = 0;
+        while (c + 1 < chunks.size() && q >= chunks[c].slots) {
+            q -= chunks[c].slots;
+            c++;
+        }
+        *i = q;
+        return chunks[c];
     }
     void release()
     {
@@ -366,14 +397,21 @@ int bucket_ensure(jt_batch* B, Bucket& k, int M, int count)
     const int64_t G = (int64_t)M * M * M, Gc = (int64_t)M * M * (M / 2 + 1);
     if (count > k.cap) {
         B->gen++;
-        k.free_arrays();
         int T = jt_pm_tile_edge(M);
         int64_t nt = (int64_t)(M / T) * (M / T) * (M / T);
-        JT_TRY(dalloc(&k.rho, (size_t)count * ngrid * G));
-        JT_TRY(dalloc(&k.rho_k, (size_t)count * ngrid * Gc));
-        JT_TRY(dalloc(&k.force_k, (size_t)count * 3 * ngrid * Gc));
-        JT_TRY(dalloc(&k.force, (size_t)count * 3 * ngrid * G));
-        JT_TRY(dalloc(&k.ranges, (size_t)count * nt));
+        const int add = count - k.cap;
+        BucketChunk c;
+        c.slots = add;
+        int r = dalloc(&c.rho, (size_t)add * ngrid * G);
+        if (r == JT_OK) r = dalloc(&c.rho_k, (size_t)add * ngrid * Gc);
+        if (r == JT_OK) r = dalloc(&c.force_k, (size_t)add * 3 * ngrid * Gc);
+        if (r == JT_OK) r = dalloc(&c.force, (size_t)add * 3 * ngrid * G);
+        if (r == JT_OK) r = dalloc(&c.ranges, (size_t)add * nt);
+        if (r != JT_OK) {
+            c.free_arrays();
+            return r;
+        }
+        k.chunks.push_back(c);
         k.cap = count;
     }
     // plans for every power-of-two batch the executions of this count use:
@@ -404,32 +442,44 @@ int fft_batch(int n, int ch)
 }
 
 // Run n transforms of a bucket in chunks of at most fft_chunk(M).
-int exec_r2c(Bucket& K, int n)
+// the density grids of the pass's first `slots` slots, chunk by chunk
+int exec_r2c(Bucket& K, int slots, int ngrid)
 {
     const int64_t G = (int64_t)K.M * K.M * K.M, Gc = (int64_t)K.M * K.M * (K.M / 2 + 1);
     const int ch = fft_chunk(K.M);
-    for (int off = 0; off < n;) {
-        const int b = fft_batch(n - off, ch);
-        auto it = K.r2c.find(b);
-        if (it == K.r2c.end()) return JT_ECUDA;   // bucket_ensure made every size a pass uses
-        if (cufftExecR2C(it->second, K.rho + off * G, (cufftComplex*)(K.rho_k + off * Gc)) != CUFFT_SUCCESS)
-            return JT_ECUDA;
-        off += b;
+    for (const BucketChunk& C : K.chunks) {
+        if (slots <= 0) break;
+        const int n = std::min(slots, C.slots) * ngrid;
+        slots -= C.slots;
+        for (int off = 0; off < n;) {
+            const int b = fft_batch(n - off, ch);
+            auto it = K.r2c.find(b);
+            if (it == K.r2c.end()) return JT_ECUDA;   // bucket_ensure made every size a pass uses
+            if (cufftExecR2C(it->second, C.rho + off * G, (cufftComplex*)(C.rho_k + off * Gc)) != CUFFT_SUCCESS)
+                return JT_ECUDA;
+            off += b;
+        }
     }
     return JT_OK;
 }
 
-int exec_c2r(Bucket& K, int n)
+// the 3 ngrid force grids of the pass's first `slots` slots, chunk by chunk
+int exec_c2r(Bucket& K, int slots, int ngrid)
 {
     const int64_t G = (int64_t)K.M * K.M * K.M, Gc = (int64_t)K.M * K.M * (K.M / 2 + 1);
     const int ch = fft_chunk(K.M);
-    for (int off = 0; off < n;) {
-        const int b = fft_batch(n - off, ch);
-        auto it = K.c2r.find(b);
-        if (it == K.c2r.end()) return JT_ECUDA;
-        if (cufftExecC2R(it->second, (cufftComplex*)(K.force_k + off * Gc), K.force + off * G) != CUFFT_SUCCESS)
-            return JT_ECUDA;
-        off += b;
+    for (const BucketChunk& C : K.chunks) {
+        if (slots <= 0) break;
+        const int n = std::min(slots, C.slots) * 3 * ngrid;
+        slots -= C.slots;
+        for (int off = 0; off < n;) {
+            const int b = fft_batch(n - off, ch);
+            auto it = K.c2r.find(b);
+            if (it == K.c2r.end()) return JT_ECUDA;
+            if (cufftExecC2R(it->second, (cufftComplex*)(C.force_k + off * Gc), C.force + off * G) != CUFFT_SUCCESS)
+                return JT_ECUDA;
+            off += b;
+        }
     }
     return JT_OK;
 }
@@ -534,20 +584,25 @@ int build_plan(jt_batch* B, const std::vector<int>& ids, const jt_box_step* step
         Bucket& K = B->buckets[M];
         const int q = slot[k];
         const int64_t G = (int64_t)M * M * M, Gc = (int64_t)M * M * (M / 2 + 1);
-        d.rho = K.rho + (size_t)q * b->ngrid * G;
-        d.rho_k = K.rho_k + (size_t)q * b->ngrid * Gc;
-        d.force_k = K.force_k + (size_t)q * 3 * b->ngrid * Gc;
-        d.force = K.force + (size_t)q * 3 * b->ngrid * G;
+        int qi = 0;
+        const BucketChunk& C = K.locate(q, &qi);
+        d.rho = C.rho + (size_t)qi * b->ngrid * G;
+        d.rho_k = C.rho_k + (size_t)qi * b->ngrid * Gc;
+        d.force_k = C.force_k + (size_t)qi * 3 * b->ngrid * Gc;
+        d.force = C.force + (size_t)qi * 3 * b->ngrid * G;
         d.tabs = b->tabs;
-        d.ranges = K.ranges + (size_t)q * d.ntiles;
+        d.ranges = C.ranges + (size_t)qi * d.ntiles;
         // the deposit flushes its tiles with 16-byte reductions
         if (reinterpret_cast<uintptr_t>(d.rho) & 15) return JT_ECUDA;
         if (b->ytab) {
-            // the unsigned source's grids sit in the next slot
-            d.rho_s = d.rho + (size_t)b->ngrid * G;
-            d.rho_s_k = d.rho_k + (size_t)b->ngrid * Gc;
-            d.force_s_k = d.force_k + (size_t)3 * b->ngrid * Gc;
-            d.force_s = d.force + (size_t)3 * b->ngrid * G;
+            // the unsigned source's grids take the next slot (in this chunk
+            // or the next)
+            int si = 0;
+            const BucketChunk& Cs = K.locate(q + 1, &si);
+            d.rho_s = Cs.rho + (size_t)si * b->ngrid * G;
+            d.rho_s_k = Cs.rho_k + (size_t)si * b->ngrid * Gc;
+            d.force_s_k = Cs.force_k + (size_t)si * 3 * b->ngrid * Gc;
+            d.force_s = Cs.force + (size_t)si * 3 * b->ngrid * G;
             d.ytab = b->ytab;
             d.ky2 = (float)(b->kappa * b->kappa);
             d.yfac = (float)std::exp(-b->kappa * b->kappa * c.r_s * c.r_s);
@@ -789,7 +844,13 @@ int force_pass(jt_batch* B, Plan& P, int parts, float kick_frac)
     cudaEventRecord(B->ev[2], st);
     for (auto& kv : P.nslots) {
         const int64_t M = kv.first, G = M * M * M;
-        JT_CU(cudaMemsetAsync(B->buckets[kv.first].rho, 0, sizeof(float) * kv.second * B->ngrid * G, st));
+        int left = kv.second;
+        for (const BucketChunk& C : B->buckets[kv.first].chunks) {
+            if (left <= 0) break;
+            const int u = std::min(left, C.slots);
+            JT_CU(cudaMemsetAsync(C.rho, 0, sizeof(float) * u * B->ngrid * G, st));
+            left -= u;
+        }
     }
     jt_b_tile_ranges(P.d_post, P.d_bx, P.d_ptp, nbox, P.npmtiles, st);
     const bool t16 = P.minT == 16 && P.maxT == 16;
@@ -799,7 +860,7 @@ int force_pass(jt_batch* B, Plan& P, int parts, float kick_frac)
     cudaEventRecord(B->ev[3], st);
     for (auto& kv : P.nslots) {
         Bucket& K = B->buckets[kv.first];
-        JT_TRY(exec_r2c(K, B->ngrid * kv.second));
+        JT_TRY(exec_r2c(K, kv.second, B->ngrid));
     }
     cudaEventRecord(B->ev[4], st);
     jt_b_kspace(P.d_bx, P.d_kp, nbox, P.nmodes, B->ngrid == 2, B->k_min, st);
@@ -809,7 +870,7 @@ int force_pass(jt_batch* B, Plan& P, int parts, float kick_frac)
     cudaEventRecord(B->ev[5], st);
     for (auto& kv : P.nslots) {
         Bucket& K = B->buckets[kv.first];
-        JT_TRY(exec_c2r(K, 3 * B->ngrid * kv.second));
+        JT_TRY(exec_c2r(K, kv.second, B->ngrid));
     }
     cudaEventRecord(B->ev[6], st);
     // PM interpolation of every particle from shared-memory tiles (a pass with
