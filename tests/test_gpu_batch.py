@@ -424,4 +424,3 @@ print(J.walk_tuning())
     assert np.all(np.isfinite(a1)) and float(np.abs(a1 - a0).max()) <= 1e-4 * rms
     assert f"cells {n} particles:" in out["1"][1]
     assert f"cells {n} particles:" not in out["0"][1]
-
