@@ -415,18 +415,25 @@ int bucket_ensure(jt_batch* B, Bucket& k, int M, int count)
         k.cap = count;
     }
     // plans for every power-of-two batch the executions of this count use:
-    // full chunks of fft_chunk(M) (a power of two) and the remainder's binary
-    // decomposition, so a bucket holds at most log2(chunk) + 1 plans per
-    // direction whatever counts later passes bring (creating a plan inside a
-    // pass costs more than the transforms)
+    // the executions run chunk by chunk (exec_r2c, exec_c2r), each chunk's
+    // share of the count as full batches of fft_chunk(M) grids (a power of
+    // two) and the remainder's binary decomposition, so a bucket holds at
+    // most log2(fft_chunk) + 1 plans per direction whatever counts later
+    // passes bring (creating a plan inside a pass costs more than the
+    // transforms; the server makes them all at registration)
     const int ch = fft_chunk(M);
-    const int nr = ngrid * count, nc = 3 * ngrid * count;
-    for (int dir = 0; dir < 2; dir++) {
-        const int n = dir == 0 ? nr : nc;
-        auto& pl = dir == 0 ? k.r2c : k.c2r;
-        if (n >= ch) JT_TRY(make_plan(B, pl, M, ch, dir == 0, k.fused));
-        for (int b = 1; b < ch; b <<= 1)
-            if ((n % ch) & b) JT_TRY(make_plan(B, pl, M, b, dir == 0, k.fused));
+    int left = count;
+    for (const BucketChunk& C : k.chunks) {
+        if (left <= 0) break;
+        const int u = std::min(left, C.slots);
+        left -= u;
+        for (int dir = 0; dir < 2; dir++) {
+            const int n = (dir == 0 ? ngrid : 3 * ngrid) * u;
+            auto& pl = dir == 0 ? k.r2c : k.c2r;
+            if (n >= ch) JT_TRY(make_plan(B, pl, M, ch, dir == 0, k.fused));
+            for (int b = 1; b < ch; b <<= 1)
+                if ((n % ch) & b) JT_TRY(make_plan(B, pl, M, b, dir == 0, k.fused));
+        }
     }
     return JT_OK;
 }
